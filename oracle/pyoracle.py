@@ -1,0 +1,283 @@
+"""ctypes access to the CPU oracles (test infrastructure only).
+
+``Oracle``    -- the project's FP64 restatement (oracle/pic_oracle.c).
+``Reference`` -- the reference program compiled by oracle/build.py
+                 (oracle/_ref/libref3d_<name>.so), driven through
+                 oracle/ref_harness.c.
+
+Both exchange grids as the reference's 18-double Grid records in
+grid[k][l][m] order and particles as rows (x, y, z, vx, vy, vz, n) + flag.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+from . import build as _build
+
+GRID_FIELDS = ["bx", "by", "bz", "b0x", "b0y", "b0z", "ex", "ey", "ez",
+               "jix", "jiy", "jiz", "jex", "jey", "jez", "ni", "ne", "phi"]
+F = {name: i for i, name in enumerate(GRID_FIELDS)}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lp = C.POINTER(C.c_long)
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def params_from_defines(d: dict) -> dict:
+    """Run-time parameter dict from an oracle.build REF_CONFIGS entry."""
+    alpha = d["ORACLE_ALPHA"]
+    alpha = math.pi / 2 if alpha == "(Pi/2.)" else float(alpha)
+    mp = d.get("ORACLE_MP", 1.67262158e-27)
+    return dict(
+        nx=d["ORACLE_NX"], ny=d["ORACLE_NY"], nz=d["ORACLE_NZ"], np=d["ORACLE_NP"],
+        thread_n=d["ORACLE_THREADS"], dx=d["ORACLE_DX"], dt=d["ORACLE_DT"],
+        q=d.get("ORACLE_Q", 1.602176487e-19), mi=mp, me=mp / d["ORACLE_MASS_RATIO"],
+        mu0=d.get("ORACLE_MU0", 1.25663706144e-6), e0=d.get("ORACLE_E0", 8.854187817e-12),
+        kb=d.get("ORACLE_KB", 1.3806504e-23), c=d.get("ORACLE_C", 2.99792458e8),
+        V=d["ORACLE_V"], Nall=d["ORACLE_NALL"], Ti=d["ORACLE_TI"], Te=d["ORACLE_TE"],
+        R=d["ORACLE_R"], I=d["ORACLE_I"], alpha=alpha, imf_x=0.0, imf_y=0.0, imf_z=0.0,
+        absorb=d["ORACLE_ABSORB"], absorb2=d["ORACLE_ABSORB2"],
+        sigma_a=d["ORACLE_SIGMA_A"], cutoff=210.0,
+    )
+
+
+_ORDER = ["nx", "ny", "nz", "np", "thread_n", "dx", "dt", "q", "mi", "me", "mu0", "e0",
+          "kb", "c", "V", "Nall", "Ti", "Te", "R", "I", "alpha", "imf_x", "imf_y", "imf_z",
+          "absorb", "absorb2", "sigma_a", "cutoff"]
+
+
+class Oracle:
+    """FP64 CPU restatement of the reference step (one domain, MPI size 1)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            path = _build.ORACLE_SO
+            if not os.path.isfile(path):
+                _build.build_oracle()
+            L = C.CDLL(path)
+            L.or_create.restype = C.c_void_p
+            L.or_create.argtypes = [_dp]
+            for name in ["or_destroy", "or_init_grid", "or_init_particle_flat", "or_add_flat",
+                         "or_renew_grid", "or_renew_b", "or_renew_e", "or_sr_b", "or_sr_e",
+                         "or_sr_current2", "or_push_j", "or_drift_n", "or_sr_particle",
+                         "or_sort"]:
+                getattr(L, name).argtypes = [C.c_void_p]
+                getattr(L, name).restype = None
+            L.or_grid_nodes.restype = C.c_long
+            L.or_grid_nodes.argtypes = [C.c_void_p]
+            L.or_get_grid.argtypes = [C.c_void_p, _dp]
+            L.or_set_grid.argtypes = [C.c_void_p, _dp]
+            L.or_get_sigma.argtypes = [C.c_void_p, _dp]
+            L.or_count.restype = C.c_long
+            L.or_count.argtypes = [C.c_void_p, C.c_int]
+            L.or_set_particles.argtypes = [C.c_void_p, C.c_int, _dp, _ip, C.c_long]
+            L.or_get_particles.restype = C.c_long
+            L.or_get_particles.argtypes = [C.c_void_p, C.c_int, _dp, _ip, C.c_long]
+            L.or_rng_counter.restype = C.c_longlong
+            L.or_rng_counter.argtypes = [C.c_void_p, C.c_int, C.c_longlong]
+            L.or_thrust.argtypes = [C.c_void_p, _dp]
+            L.or_gauss_residual.argtypes = [C.c_void_p, _dp]
+            L.or_gather.argtypes = [C.c_void_p, _dp, _dp]
+            L.or_step.argtypes = [C.c_void_p, _ip, _ip, C.c_int, C.c_int]
+            L.or_fdtd.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+            L.or_fave.argtypes = [C.c_void_p, _dp]
+            L.or_oob_count.restype = C.c_long
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self, params: dict):
+        self.p = dict(params)
+        arr = np.array([float(self.p[k]) for k in _ORDER], dtype=np.float64)
+        self.L = self.lib()
+        self.h = self.L.or_create(_ptr(arr))
+        self.shape = (self.p["nx"] + 4, self.p["ny"] + 4, self.p["nz"] + 4)
+        self.c_add = C.c_int(0)
+        self.c_thrust = C.c_int(0)
+
+    def close(self):
+        if self.h:
+            self.L.or_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def call(self, name):
+        getattr(self.L, "or_" + name)(self.h)
+
+    def grid(self) -> np.ndarray:
+        g = np.zeros(self.shape + (18,), dtype=np.float64)
+        self.L.or_get_grid(self.h, _ptr(g))
+        return g
+
+    def set_grid(self, g: np.ndarray):
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        assert g.shape == self.shape + (18,)
+        self.L.or_set_grid(self.h, _ptr(g))
+
+    def sigma(self) -> np.ndarray:
+        s = np.zeros(tuple(2 * n for n in self.shape), dtype=np.float64)
+        self.L.or_get_sigma(self.h, _ptr(s))
+        return s
+
+    def particles(self, species: int):
+        n = self.L.or_count(self.h, species)
+        rows = np.zeros((max(n, 1), 7))
+        flag = np.zeros(max(n, 1), dtype=np.int32)
+        self.L.or_get_particles(self.h, species, _ptr(rows), _ptr(flag, _ip), n)
+        return rows[:n], flag[:n]
+
+    def set_particles(self, species: int, rows: np.ndarray, flag=None):
+        rows = np.ascontiguousarray(rows, dtype=np.float64).reshape(-1, 7)
+        f = None if flag is None else np.ascontiguousarray(flag, dtype=np.int32)
+        self.L.or_set_particles(self.h, species, _ptr(rows), None if f is None else _ptr(f, _ip),
+                                rows.shape[0])
+
+    def rng_counter(self, which: int, set_to: int = -1) -> int:
+        return int(self.L.or_rng_counter(self.h, which, set_to))
+
+    def thrust(self) -> np.ndarray:
+        out = np.zeros(33)
+        self.L.or_thrust(self.h, _ptr(out))
+        return out
+
+    def gauss(self) -> np.ndarray:
+        out = np.zeros(4)
+        self.L.or_gauss_residual(self.h, _ptr(out))
+        return out
+
+    def gather(self, xyz) -> np.ndarray:
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        out = np.zeros(6)
+        self.L.or_gather(self.h, _ptr(xyz), _ptr(out))
+        return out
+
+    def step(self, sort_every=500, add_every=5):
+        self.L.or_step(self.h, C.byref(self.c_add), C.byref(self.c_thrust), sort_every, add_every)
+
+    def fdtd(self, nsteps, sort_every=500, add_every=5):
+        self.L.or_fdtd(self.h, nsteps, sort_every, add_every)
+
+    def fave(self):
+        out = np.zeros(27)
+        self.L.or_fave(self.h, _ptr(out))
+        return out
+
+
+REF_OPS = dict(renew_grid=1, renew_b=2, sr_b=3, push_j=4, drift_n=5, reduce=6,
+               sr_current=7, renew_e=8, sr_e=9, sr_particle=10, add_flat=11, sort=12,
+               thrust_f=13)
+
+
+class Reference:
+    """The reference program itself, compiled at one geometry. Its state is
+    process-global: use one instance per process."""
+
+    def __init__(self, name: str):
+        path = _build.ref_lib_path(name)
+        if not os.path.isfile(path):
+            _build.build_ref(name)
+        L = C.CDLL(path)
+        L.ref_grid_nodes.restype = C.c_long
+        L.ref_get_grid.argtypes = [_dp]
+        L.ref_set_grid.argtypes = [_dp]
+        L.ref_get_sigma.argtypes = [_dp]
+        L.ref_get_grid_thread.argtypes = [C.c_int, _dp]
+        L.ref_count.restype = C.c_long
+        L.ref_count.argtypes = [C.c_int]
+        L.ref_get_particles.restype = C.c_long
+        L.ref_get_particles.argtypes = [C.c_int, _dp, _ip, C.c_long]
+        L.ref_set_particles.argtypes = [_dp, _ip, _lp, _dp, _ip, _lp]
+        L.ref_rng_counter.restype = C.c_longlong
+        L.ref_rng_counter.argtypes = [C.c_int, C.c_int, C.c_longlong]
+        L.ref_thrust_sums.argtypes = [_dp, C.c_int]
+        L.ref_gather.argtypes = [_dp, _dp]
+        L.ref_fave.argtypes = [_dp]
+        self.L = L
+        self.name = name
+        self.defines = _build.REF_CONFIGS[name]
+        self.params = params_from_defines(self.defines)
+        d = (C.c_int * 10)()
+        L.ref_dims(d)
+        self.dims = list(d)
+        self.shape = (d[0] + 4, d[1] + 4, d[2] + 4)
+
+    def op(self, name):
+        self.L.ref_op(REF_OPS[name])
+
+    def init_grid(self):
+        self.L.ref_init_grid()
+
+    def init_particle_flat(self):
+        self.L.ref_init_particle_flat()
+
+    def init_rng(self):
+        self.L.ref_init_rng()
+
+    def grid(self) -> np.ndarray:
+        g = np.zeros(self.shape + (18,))
+        self.L.ref_get_grid(_ptr(g))
+        return g
+
+    def set_grid(self, g):
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        self.L.ref_set_grid(_ptr(g))
+
+    def sigma(self):
+        s = np.zeros(tuple(2 * n for n in self.shape))
+        self.L.ref_get_sigma(_ptr(s))
+        return s
+
+    def particles(self, species: int):
+        n = self.L.ref_count(species)
+        rows = np.zeros((max(n, 1), 7))
+        flag = np.zeros(max(n, 1), dtype=np.int32)
+        self.L.ref_get_particles(species, _ptr(rows), _ptr(flag, _ip), n)
+        return rows[:n], flag[:n]
+
+    def set_particles(self, ion_rows, electron_rows, ion_flag=None, electron_flag=None):
+        ir = np.ascontiguousarray(ion_rows, dtype=np.float64).reshape(-1, 7)
+        er = np.ascontiguousarray(electron_rows, dtype=np.float64).reshape(-1, 7)
+        ic = np.array([ir.shape[0]], dtype=np.int64)
+        ec = np.array([er.shape[0]], dtype=np.int64)
+        fi = None if ion_flag is None else np.ascontiguousarray(ion_flag, dtype=np.int32)
+        fe = None if electron_flag is None else np.ascontiguousarray(electron_flag, dtype=np.int32)
+        rc = self.L.ref_set_particles(_ptr(ir), None if fi is None else _ptr(fi, _ip), _ptr(ic, _lp),
+                                      _ptr(er), None if fe is None else _ptr(fe, _ip), _ptr(ec, _lp))
+        assert rc == 0
+
+    def rng_counter(self, which: int, set_to: int = -1) -> int:
+        return int(self.L.ref_rng_counter(0, which, set_to))
+
+    def thrust(self, include_tail=True) -> np.ndarray:
+        out = np.zeros(33)
+        self.L.ref_thrust_sums(_ptr(out), 1 if include_tail else 0)
+        return out
+
+    def gather(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        out = np.zeros(6)
+        self.L.ref_gather(_ptr(xyz), _ptr(out))
+        return out
+
+    def fdtd(self, nsteps: int):
+        self.L.ref_fdtd(nsteps)
+
+    def fave(self):
+        out = np.zeros(27)
+        self.L.ref_fave(_ptr(out))
+        return out
