@@ -1,0 +1,376 @@
+"""Benchmark of the B200 PIC step: particle-steps/s of push + deposit + FDTD
+(with boundary refill every 5 steps and a cell sort every 20) on the 3D
+solar-wind/dipole plasma of 128^3 cells x 64 particles/cell/species
+(268,435,456 particles), FP32 path, with the FP64 path timed on the same seed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU (torchrun, one process per GPU): every rank advances an independent
+replica of the workload (the single-domain path has no data exchange between
+runs); value = all ranks' particle-steps / max-over-ranks device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s (push+deposit+FDTD)"
+UNIT = "particle-steps/s"
+NX = NY = NZ = 128
+PPC = 64
+SORT_EVERY = 20
+ADD_EVERY = 5
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ CPU side
+def reference_sample(name: str, nsteps: int, warm: int, workdir: str):
+    """Times the reference program (compiled from its own source, oracle/_ref)
+    on one host core: init, the initial refill, `warm` untimed loop bodies,
+    then `nsteps` timed ones. Returns (particle-steps, seconds, particles)."""
+    from oracle.pyoracle import Reference
+
+    os.chdir(workdir)
+    R = Reference(name)
+    R.init_grid()
+    R.init_particle_flat()
+    R.op("add_flat")
+    if warm:
+        R.L.ref_loop(warm, SORT_EVERY, ADD_EVERY)
+    n0 = R.L.ref_count(0) + R.L.ref_count(1)
+    t0 = time.perf_counter()
+    R.L.ref_loop(nsteps, SORT_EVERY, ADD_EVERY)
+    dt = time.perf_counter() - t0
+    n1 = R.L.ref_count(0) + R.L.ref_count(1)
+    return 0.5 * (n0 + n1) * nsteps, dt, n0
+
+
+def _reference_worker(args):
+    name, nsteps, warm = args
+    with tempfile.TemporaryDirectory() as d:
+        return reference_sample(name, nsteps, warm, d)
+
+
+def reference_baseline(name: str, nsteps: int, warm: int, procs: int):
+    """`procs` independent single-core reference processes (spawned), summed."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_reference_worker, [(name, nsteps, warm)] * procs)
+    psteps = sum(r[0] for r in res)
+    wall = max(r[1] for r in res)
+    return psteps / wall, res
+
+
+def ensure_reference_lib(name: str) -> bool:
+    from oracle import build as obuild
+
+    if os.path.isfile(obuild.ref_lib_path(name)):
+        return True
+    if obuild.reference_available():
+        obuild.build_ref(name)
+        return True
+    return False
+
+
+# ------------------------------------------------------------------ GPU side
+def make_config(precision: int, seed: int):
+    from plasmasim_b200 import PicConfig
+
+    return PicConfig.normalized(NX, NY, NZ, PPC, precision=precision, sort_interval=SORT_EVERY,
+                                add_interval=ADD_EVERY, diag_every_step=0, seed_p=seed,
+                                seed_v=seed + 50)
+
+
+def run_gpu(precision: int, steps: int, warmup: int, seed: int, dist=None, clocks_index=0):
+    """Device-resident timing of `steps` pic_step calls after `warmup` steps."""
+    import torch
+    from plasmasim_b200 import Pic3D
+
+    P = Pic3D(make_config(precision, seed))
+    P.init_grid()
+    P.init_particle_flat()
+    P.fdtd(0)                      # fdtd's refill before its loop
+    P.step(warmup)
+    P.synchronize()
+    stream = torch.cuda.ExternalStream(P.stream_handle())
+    _, c0 = P.status()
+    P.set_timing(True)
+    _, _, launches0 = P.read_timing()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(clocks_index) as clk:
+        start.record(stream)
+        P.step(steps)
+        stop.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    phase_ms, phase_pairs, launches1 = P.read_timing()
+    P.set_timing(False)
+    rc, c1 = P.status()
+    pushed = int(c1[3] - c0[3])
+    out = dict(ms=ms, pushed=pushed, phase_ms=phase_ms, phase_pairs=phase_pairs,
+               launches=launches1 - launches0, clocks=clk.summary(), status=int(rc),
+               errors=[int(x) for x in c1[:3]])
+    return P, out
+
+
+def run_e2e(P, steps: int):
+    """The same step through the public API with host buffers: upload of the
+    particle and grid state from pinned host memory, `steps` steps each
+    followed by the thrust/energy read-back (thrust_f), download of the final
+    particle state. Returns (particle-steps/s, h2d bytes/step, d2h bytes/step)."""
+    import numpy as np
+    import torch
+
+    from plasmasim_b200 import ELECTRON, ION
+
+    rows = {}
+    for s in (ION, ELECTRON):
+        n = P.particle_count(s)
+        buf = torch.empty((n, 7), dtype=torch.float64, pin_memory=True)
+        rows[s] = buf.numpy()
+        rows[s][:] = P.particles(s)
+    g = torch.empty(P.shape + (18,), dtype=torch.float64, pin_memory=True).numpy()
+    g[:] = P.grid()
+    _, c0 = P.status()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    P.set_grid(g)
+    for s in (ION, ELECTRON):
+        P.set_particles(s, rows[s])
+    for _ in range(steps):
+        P.step(1)
+        P.thrust_f()
+    outn = 0
+    for s in (ION, ELECTRON):
+        got = P.particles(s, out=rows[s])
+        outn += got.size
+    dt = time.perf_counter() - t0
+    _, c1 = P.status()
+    pushed = int(c1[3] - c0[3])
+    h2d = g.nbytes + sum(r.nbytes for r in rows.values())
+    d2h = outn * 8 + steps * 33 * 8
+    return pushed / dt, h2d / steps, d2h / steps
+
+
+def roofline(out, npart_species, cells, rsize):
+    """Push kernel: algorithmic bytes per launch = particles x (read + write of
+    the SoA state: 4 + 6 rsize bytes each way) + cells x rsize x (6 gathered
+    field components + 4 deposited quantities)."""
+    pushes = out["pushed"]
+    launches = out["phase_pairs"]["push"] * 2
+    per_particle = 2 * (4 + 6 * rsize)
+    bytes_total = pushes * per_particle + launches * cells * rsize * 10
+    secs = out["phase_ms"]["push"] / 1e3
+    return bytes_total / secs / 1e9, bytes_total / max(launches, 1), secs / max(launches, 1)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        name = "cube32"
+        if not ensure_reference_lib(name):
+            print(json.dumps({"impl": "reference", "unavailable": "compiled reference library missing"}))
+            return
+        procs = max(1, min(os.cpu_count() or 1, 64))
+        value, res = reference_baseline(name, max(args.steps // 4, 2), min(args.warmup, 2), procs)
+        cfg = {"workload": "3D PIC solar wind + dipole, 128^3 cells x 64 ppc/species",
+               "sample": f"{procs} processes x 32^3 cells x 8 ppc/species",
+               "grid": [NX, NY, NZ], "ppc_per_species": PPC}
+        print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "higher_is_better": True, "scaling": "weak", "dtype": "f64",
+                          "data": "synthetic", "config": cfg,
+                          "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs,
+                                           "kind": "reference",
+                                           "sample": cfg["sample"] + ", fdtd loop body"},
+                          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    else:
+        torch.cuda.set_device(0)
+    from plasmasim_b200 import build as pbuild
+
+    if not os.path.isfile(pbuild.LIB):
+        pbuild.build()
+
+    seed = 1000 * rank
+    P, out = run_gpu(32, args.steps, args.warmup, seed, dist, clocks_index=local)
+    ms = out["ms"]
+    pushed = out["pushed"]
+    if dist is not None:
+        t = torch.tensor([ms, float(pushed)], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        ms_max, pushed_all = float(tmax[0]), float(t[1])
+    else:
+        ms_max, pushed_all = ms, float(pushed)
+    value = pushed_all / (ms_max / 1e3)
+    cells = (NX + 4) * (NY + 4) * (NZ + 4)
+    nsp = pushed / max(args.steps, 1) / 2
+    ach, bytes_launch, s_launch = roofline(out, nsp, cells, 4)
+    peak, peak_kind = measured_peaks()
+
+    e2e = None
+    if not args.no_e2e and world == 1:
+        try:
+            v, h2d, d2h = run_e2e(P, args.steps)
+            e2e = {"value": v, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+        except Exception as exc:  # reported, not hidden
+            log("e2e failed:", exc)
+            e2e = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
+    P.close()
+    del P
+
+    fp64 = None
+    if not args.no_fp64 and world == 1:
+        P64, o64 = run_gpu(64, args.steps, args.warmup, seed, None, clocks_index=local)
+        P64.close()
+        v64 = o64["pushed"] / (o64["ms"] / 1e3)
+        fp64 = {"value": v64, "ms_per_step": o64["ms"] / args.steps, "fp32_over_fp64": value / v64,
+                "phase_ms": o64["phase_ms"]}
+
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        if ensure_reference_lib("cube64"):
+            with tempfile.TemporaryDirectory() as d:
+                cwd = os.getcwd()
+                psteps, secs, n = reference_sample("cube64", 4, 1, d)
+                os.chdir(cwd)
+            cpu = {"value": psteps / secs, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"reference fdtd loop body, 64^3 cells x 16 ppc/species ({n} particles), 4 steps"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "compiled reference library missing"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "3D PIC solar wind + dipole (normalized units), 128^3 cells x 64 "
+                                   "particles/cell/species, sort every 20, refill every 5",
+                       "grid": [NX, NY, NZ], "ppc_per_species": PPC,
+                       "particles": int(pushed / max(args.steps, 1)),
+                       "l2": "inputs larger than L2 (7.5 GB of particle state per step)",
+                       "parallelism": f"replicas{world}"},
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "traffic": None, "kernel": "push_kernel<float,FUSED>",
+                         "peak_kind": peak_kind, "bytes_per_launch": bytes_launch,
+                         "ms_per_launch": s_launch * 1e3},
+            "phase_ms_per_step": {k: v / args.steps for k, v in out["phase_ms"].items()},
+            "clocks": out["clocks"], "gpu_launches": out["launches"],
+            "device_errors": out["errors"], "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,169 @@
+/*
+ * plasma_b200.h -- C ABI of the B200 (sm_100a) implementation of the 3D
+ * particle-in-cell time step of PLASMAsim's PIC/3d_pic458_domain.c.
+ *
+ * The reference has no library interface: its step is a set of C functions over
+ * global arrays, called in order from fdtd() (PIC/3d_pic458_domain.c:627-952),
+ * that return 0 and exit() on failure. Each entry point below replaces one of
+ * those functions (cited per declaration) for one domain at MPI size 1; the
+ * state the reference keeps in globals (grid[][][] :147, sigma[][][] :148,
+ * grid_thread :149, the particle lists owned by main_func :258-261) lives in an
+ * opaque context instead. Every call returns a status code (PIC_OK == 0) and
+ * never exits the process.
+ *
+ * Threading: one host thread per context at a time. All device work of a
+ * context is issued on its own CUDA stream (pic_get_stream); calls return
+ * when the work is queued unless they hand results back to host memory.
+ *
+ * Units are the caller's (the reference uses MKSA; normalized units work the
+ * same way); positions are absolute, ghost cells included, as in the reference
+ * (interior cell index i covers [i dx, (i+1) dx) for i in [2, N+2)).
+ */
+#ifndef PLASMA_B200_H
+#define PLASMA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIC_OK 0
+#define PIC_ERR_ARG 1        /* invalid argument or configuration */
+#define PIC_ERR_CUDA 2       /* a CUDA runtime call failed */
+#define PIC_ERR_CAPACITY 3   /* particle capacity exceeded */
+#define PIC_ERR_STATE 4      /* call out of order (e.g. step before init) */
+#define PIC_ERR_DEVICE 5     /* device-side counters report lost work (pic_status) */
+
+#define PIC_ION 0
+#define PIC_ELECTRON 1
+#define PIC_BOTH (-1)
+
+/* Number of doubles in one grid record of pic_get_grid / pic_set_grid: the
+ * reference's Grid struct (PIC/3d_pic458_domain.c:115-123) in field order
+ * bx by bz b0x b0y b0z ex ey ez jix0 jiy0 jiz0 jex0 jey0 jez0 ni ne phi. */
+#define PIC_GRID_RECORD 18
+/* Doubles per particle row of pic_set_particles / pic_get_particles:
+ * x y z vx vy vz n (the reference's Particle, :134-141, without its links). */
+#define PIC_PARTICLE_ROW 7
+#define PIC_NUM_THRUST 27    /* F[27] of thrust_f, :4950 */
+#define PIC_NUM_ENERGY 6     /* E[6] of thrust_f, :4953 */
+
+/* Run-time form of the reference's compile-time parameters (:52-103). */
+typedef struct pic_config {
+  int nx, ny, nz;          /* interior cells: Grid_Nx, Grid_Ny, Grid_Nz */
+  int np;                  /* macro-particles per cell per species: Np */
+  int precision;           /* 32: FP32 particles/fields, FP64 reductions; 64: FP64 throughout */
+  int device;              /* CUDA device ordinal */
+  double dx, dt;           /* dx, dt */
+  double q, mi, me;        /* q, mi, me (the reference: me = mi/100) */
+  double mu0, e0, kb, c;   /* mu0, e0, kb, C */
+  double v_drift;          /* V: solar-wind drift along +z */
+  double n_all;            /* Nall: plasma density; particle weight n = Nall/Np */
+  double ti, te;           /* Ti, Te */
+  double coil_r, coil_i;   /* R, I: dipole moment I*pi*R^2 */
+  double alpha;            /* alpha: moment direction (0, sin a, cos a) */
+  double imf_x, imf_y, imf_z; /* IMF_x, IMF_y, IMF_z */
+  int absorb_grid;         /* Absorb_grid: width of the field damping layer */
+  int absorb_grid2;        /* Absorb_grid2: width of the ballistic particle layer */
+  double sigma_a;          /* damping amplitude a of init_grid (:295) */
+  double dipole_cutoff;    /* external_current7 radius in cells (:4596, 210) */
+  int add_interval;        /* fdtd: add_*_flat every add_interval steps (5, :700) */
+  int sort_interval;       /* fdtd: sorting every sort_interval steps (500, :694) */
+  int diag_every_step;     /* 1: thrust_fave sums every step as fdtd does (:926) */
+  int reserved0;
+  long long capacity;      /* particle slots per species; 0 picks 1.5x the initial load */
+  unsigned long long seed_p; /* position stream key (init_particle_flat :444: 0) */
+  unsigned long long seed_v; /* velocity stream key (:445: 50) */
+} pic_config;
+
+typedef struct pic_ctx pic_ctx;
+
+/* Fills *cfg with the reference's own defaults (:52-103) for a one-domain run
+ * of nx*ny*nz cells: MKSA constants, dx = 1.5, dt = 1.5e-9, Np = 16, ... */
+int pic_config_default(pic_config *cfg, int nx, int ny, int nz);
+
+/* Allocates all device state (replaces the static arrays :147-153 and the
+ * particle lists of main_func :258-261). */
+int pic_create(const pic_config *cfg, pic_ctx **out);
+int pic_destroy(pic_ctx *ctx);
+
+/* init_grid + external_current7 (:291-410, :4579-4634): zero fields, dipole
+ * B0 on the staggered points, damping profile. */
+int pic_init_grid(pic_ctx *ctx);
+/* init_particle_flat (:412-625): Np per cell per species, uniform in the
+ * cell, drifting Maxwellian, from the position/velocity random streams. */
+int pic_init_particle_flat(pic_ctx *ctx);
+
+/* renew_grid (:2533-2578): zero currents and densities. */
+int pic_renew_grid(pic_ctx *ctx);
+/* renew_b4_2 (:2580-2611) followed by sr_b (:1001-1193) at size 1. */
+int pic_renew_b4_2(pic_ctx *ctx);
+/* renew_e4_2 (:2613-2652) followed by sr_e (:1195-1387) at size 1. */
+int pic_renew_e4_2(pic_ctx *ctx);
+/* The push loop of fdtd (:731-812): cal_track4 (:2804-2870) with the
+ * shape_func_v2 gather (:3017-3326), the ballistic branch outside the
+ * Absorb_grid2 box, and shape_func_*0_j_2 (:3397-3553). */
+int pic_push_deposit_j(pic_ctx *ctx, int species);
+/* The drift loop of fdtd (:818-867) with shape_func_*0_n_2 (:3333-3395). */
+int pic_drift_deposit_n(pic_ctx *ctx, int species);
+/* The thread reduction of fdtd (:869-886) and sr_current2 (:1805-2039) at
+ * size 1: additive periodic fold of the ghost planes of J and n. */
+int pic_reduce_current(pic_ctx *ctx);
+/* sr_particle (:2041-2531) at size 1: delete z outflow and x/y < 2 dx,
+ * wrap x/y >= (N+2) dx by -N dx. */
+int pic_sr_particle(pic_ctx *ctx);
+/* add_ion_flat then add_electron_flat (:5993-6818) at size 1. */
+int pic_add_flat(pic_ctx *ctx);
+/* sorting (:7475-7590): particles in cell order, ghost-cell particles dropped. */
+int pic_sort(pic_ctx *ctx);
+/* thrust_f sums (:4963-5101): F[27] and E[6] in FP64 on the device. */
+int pic_thrust_f(pic_ctx *ctx, double *F27, double *E6);
+/* Running mean of thrust_fave (:5124-5285): Fave[27] as accumulated since the
+ * last reset (the reference resets it every 500 steps after printing). */
+int pic_thrust_fave(pic_ctx *ctx, double *Fave27, int reset);
+/* Gauss-law residual of the current state (no reference counterpart; it is
+ * what the reference's compiled-out renew_phi3 :8315 would correct):
+ * out = [sum (div4 E - rho/e0)^2, sum (rho/e0)^2, max |div4 E - rho/e0|, cells]. */
+int pic_gauss_residual(pic_ctx *ctx, double *out4);
+
+/* nsteps iterations of fdtd's loop body (:687-949) continuing the step
+ * counters; the particle work of one step runs as one fused kernel per species. */
+int pic_step(pic_ctx *ctx, int nsteps);
+/* fdtd (:627-952) for nsteps: one add_*_flat, then pic_step(nsteps). */
+int pic_fdtd(pic_ctx *ctx, int nsteps);
+
+/* State import/export in reference units (FP64 host arrays). */
+int pic_set_particles(pic_ctx *ctx, int species, const double *rows, const int *flag,
+                      long long n);
+int pic_get_particles(pic_ctx *ctx, int species, double *rows, int *flag, long long cap,
+                      long long *n_out);
+int pic_particle_count(pic_ctx *ctx, int species, long long *n_out);
+int pic_get_grid(pic_ctx *ctx, double *records);
+int pic_set_grid(pic_ctx *ctx, const double *records);
+/* Random-stream draw counters (position, velocity) shared by init and add. */
+int pic_rng_counters(pic_ctx *ctx, long long *ctr_p, long long *ctr_v, int set);
+
+/* Device counters: errors [0] deposits or gathers skipped because the stencil
+ * left the array, [1] particles dropped with a cell outside the index range,
+ * [2] non-finite velocities after a push; work [3] particle pushes made by
+ * the push kernels since creation; [4..7] reserved. Returns PIC_ERR_DEVICE
+ * when any error counter is non-zero. */
+int pic_status(pic_ctx *ctx, long long *counters8);
+int pic_synchronize(pic_ctx *ctx);
+/* The context's cudaStream_t, for callers that time or order work around it. */
+int pic_get_stream(pic_ctx *ctx, void **stream);
+/* Per-phase CUDA-event timing of pic_step (no reference counterpart; the
+ * reference prints wall-clock times only, :684-705). While enabled, every step
+ * records event pairs on the context's stream around its phases:
+ * [0] particle push (fused kernels), [1] field updates, ghost copies and folds,
+ * [2] sort, [3] boundary refill, [4] per-step diagnostics. pic_read_timing
+ * synchronises, returns the summed milliseconds and pairs per phase, the
+ * number of kernels the context has launched since creation, and restarts. */
+int pic_set_timing(pic_ctx *ctx, int enable);
+int pic_read_timing(pic_ctx *ctx, double *ms8, long long *pairs8, long long *launches);
+const char *pic_error_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -638,7 +638,12 @@ void or_push_j(or_ctx *c)
     or_species *sp = &c->sp[s];
     for (long i = 0; i < sp->n; ++i) {
       double *p = sp->r + 7 * i;
-      if (p[0] < ax0 || p[0] > ax1 || p[1] < ay0 || p[1] > ay1 || p[2] < az0 || p[2] > az1) {
+      int bal = p[0] < ax0 || p[0] > ax1 || p[1] < ay0 || p[1] > ay1 || p[2] < az0 || p[2] > az1;
+      if (!bal && !(p[0] >= 0. && p[1] >= 0. && p[2] >= 0. && stencil_in_array(c, p))) {
+        g_oob++;  /* the gather would read outside the array: counted, pushed ballistically */
+        bal = 1;
+      }
+      if (bal) {
         p[0] += p[3] * dth; p[1] += p[4] * dth; p[2] += p[5] * dth;
       } else {
         cal_track4(c, p, s == 0 ? c->mi : -c->me);

@@ -35,7 +35,7 @@ def params_from_defines(d: dict) -> dict:
     """Run-time parameter dict from an oracle.build REF_CONFIGS entry."""
     alpha = d["ORACLE_ALPHA"]
     alpha = math.pi / 2 if alpha == "(Pi/2.)" else float(alpha)
-    mp = d.get("ORACLE_MP", 1.67262158e-27)
+    mp = d.get("ORACLE_MP", 1.672621637e-27)
     return dict(
         nx=d["ORACLE_NX"], ny=d["ORACLE_NY"], nz=d["ORACLE_NZ"], np=d["ORACLE_NP"],
         thread_n=d["ORACLE_THREADS"], dx=d["ORACLE_DX"], dt=d["ORACLE_DT"],

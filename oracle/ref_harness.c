@@ -378,5 +378,58 @@ int ref_fdtd(int nsteps)
   return h_run(h_op, &op);
 }
 
+/* The body of fdtd's loop (:688-911) repeated nsteps times with its step
+ * counters kept between calls: sorting every sort_every steps, add_*_flat every
+ * add_every steps, then the push, field and exchange functions in fdtd's order.
+ * The file output of :913-931 (output, thrust_f, thrust_fave, suspend_job) is
+ * left out so that a timing measures the step itself. */
+static int h_c_add = 0, h_c_thrust = 0;
+static int h_loop_args[3];
+static void h_loop(void *a)
+{
+  int s, i;
+  (void)a;
+  for (s = 0; s < h_loop_args[0]; s++) {
+    renew_grid();
+    if (h_c_thrust > h_loop_args[1] - 1) {
+      h_c_thrust = 0;
+      sorting(h_ion, h_ion_start);
+      sorting(h_el, h_el_start);
+    }
+    if (h_c_add > h_loop_args[2] - 1) {
+      add_ion_flat(h_ion, h_ion_start, 0, 0);
+      add_electron_flat(h_el, h_el_start, 0, 0);
+      h_c_add = 0;
+    }
+    renew_b4_2();
+    sr_b(0, 0);
+    for (i = 0; i < THREAD_N; i++) {
+      h_push_j_list(h_ion_start[i], i, 0);
+      h_push_j_list(h_el_start[i], i, 1);
+    }
+    renew_b4_2();
+    sr_b(0, 0);
+    for (i = 0; i < THREAD_N; i++) {
+      h_drift_n_list(h_ion_start[i], i, 0);
+      h_drift_n_list(h_el_start[i], i, 1);
+    }
+    h_reduce_threads();
+    sr_current2(0, 0);
+    renew_e4_2();
+    sr_e(0, 0);
+    sr_particle(h_ion, h_ion_start, h_el, h_el_start, 0, 0);
+    h_c_add++;
+    h_c_thrust++;
+  }
+}
+
+int ref_loop(int nsteps, int sort_every, int add_every)
+{
+  h_loop_args[0] = nsteps;
+  h_loop_args[1] = sort_every;
+  h_loop_args[2] = add_every;
+  return h_run(h_loop, NULL);
+}
+
 void ref_fave(double *out) { memcpy(out, Fave, sizeof(Fave)); }
 int ref_unmatched_sends(void) { return oracle_mpi_unmatched(); }

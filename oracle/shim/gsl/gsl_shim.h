@@ -35,7 +35,7 @@
 #define ORACLE_Q 1.602176487e-19
 #endif
 #ifndef ORACLE_MP
-#define ORACLE_MP 1.67262158e-27
+#define ORACLE_MP 1.672621637e-27
 #endif
 #ifndef ORACLE_ME
 #define ORACLE_ME 9.10938188e-31

@@ -1,0 +1,39 @@
+"""Builds the in-tree CUDA library plasmasim_b200/libplasmab200.so for sm_100a."""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libplasmab200.so")
+SOURCES = [os.path.join(HERE, "csrc", "api.cu")]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    cand = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    return cand if os.path.isfile(cand) else "nvcc"
+
+
+def _newest_input() -> float:
+    files = glob.glob(os.path.join(HERE, "csrc", "*")) + [os.path.join(ROOT, "include", "plasma_b200.h")]
+    return max(os.path.getmtime(f) for f in files)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and os.path.isfile(LIB) and os.path.getmtime(LIB) >= _newest_input():
+        return LIB
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
+           "-I", os.path.join(ROOT, "include"),
+           "-o", LIB, *SOURCES]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)

@@ -1,0 +1,1055 @@
+// C ABI of the B200 PIC step (declarations and reference citations in
+// include/plasma_b200.h). Host-side orchestration: one CUDA stream per
+// context, every kernel launched on it, no host synchronisation inside a step
+// except the particle count read back after a sort.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/plasma_b200.h"
+#include "common.cuh"
+#include "diag.cuh"
+#include "fields.cuh"
+#include "particles.cuh"
+
+using namespace pb;
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct Store {
+  void* mem[2] = {nullptr, nullptr};  // double-buffered for the sort
+  int cur = 0;
+  long long cap = 0;
+  long long count = 0;  // slots in use (live and empty), mirrored in *count_dev
+  int* count_dev = nullptr;
+};
+
+}  // namespace
+
+struct pic_ctx {
+  pic_config cfg{};
+  Geom g{};
+  int prec = 32;
+  size_t rsize = 4;
+  cudaStream_t stream = nullptr;
+  // fields: F_COUNT planes
+  void* field_mem = nullptr;
+  size_t plane_bytes = 0;
+  double* ramps = nullptr;  // rx[2gx], ry[2gy], rz[2gz]
+  Store sp[2];
+  // sort and scan scratch
+  int* cnt = nullptr;
+  int* offs = nullptr;
+  int* cursor = nullptr;
+  int* scan_tmp = nullptr;
+  size_t scan_tmp_len = 0;
+  long long ncells = 0;
+  // diagnostics
+  double* acc = nullptr;        // 33 thrust/energy sums, then 4 Gauss-law values
+  unsigned long long* maxbits = nullptr;
+  double* fave = nullptr;       // 27
+  unsigned long long* err = nullptr;  // ERR_COUNT
+  // import/export staging
+  void* stage = nullptr;
+  size_t stage_bytes = 0;
+  int* flags = nullptr;
+  int* pos = nullptr;
+  size_t flags_len = 0;
+  // host state
+  long long ctr_p = 0, ctr_v = 0;
+  int c_add = 0, c_thrust = 0;
+  bool grid_ready = false;
+  bool particles_ready = false;
+  // kernel launches issued by this context, and optional per-phase event timing
+  long long launches = 0;
+  bool timing = false;
+  struct Phase {
+    std::vector<cudaEvent_t> ev;  // start/stop pairs
+    size_t used = 0;
+  } phase[8];
+};
+
+#define CK(x)                                                         \
+  do {                                                                \
+    cudaError_t e_ = (x);                                             \
+    if (e_ != cudaSuccess) {                                          \
+      fprintf(stderr, "plasma_b200: %s: %s\n", #x, cudaGetErrorString(e_)); \
+      return PIC_ERR_CUDA;                                            \
+    }                                                                 \
+  } while (0)
+#define CKL()                      \
+  do {                             \
+    ++c->launches;                 \
+    CK(cudaGetLastError());        \
+  } while (0)
+#define CKR(x)                \
+  do {                        \
+    int r_ = (x);             \
+    if (r_ != PIC_OK) return r_; \
+  } while (0)
+
+namespace {
+
+template <typename real>
+Fields<real> fields(pic_ctx* c) {
+  Fields<real> F;
+  for (int q = 0; q < F_COUNT; ++q)
+    F.f[q] = (real*)((char*)c->field_mem + (size_t)q * c->plane_bytes);
+  return F;
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t store_bytes(long long cap, size_t rsize) {
+  return align256((size_t)cap * 4) + 6 * align256((size_t)cap * rsize);
+}
+
+template <typename real>
+Parts<real> parts(pic_ctx* c, int s, int buf) {
+  Parts<real> P;
+  char* base = (char*)c->sp[s].mem[buf];
+  const long long cap = c->sp[s].cap;
+  P.cell = (int*)base;
+  char* p = base + align256((size_t)cap * 4);
+  for (int a = 0; a < 3; ++a) {
+    P.o[a] = (real*)p;
+    p += align256((size_t)cap * sizeof(real));
+  }
+  for (int a = 0; a < 3; ++a) {
+    P.v[a] = (real*)p;
+    p += align256((size_t)cap * sizeof(real));
+  }
+  return P;
+}
+
+template <typename real>
+Parts<real> parts(pic_ctx* c, int s) {
+  return parts<real>(c, s, c->sp[s].cur);
+}
+
+int grid_blocks(long long n, int threads = kThreads) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+// Persistent-style grid for particle loops: enough blocks to fill the GPU.
+int particle_blocks(long long n) {
+  long long b = (n + kThreads - 1) / kThreads;
+  const long long cap = 148LL * 16;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
+
+int set_count(pic_ctx* c, int s, long long n) {
+  c->sp[s].count = n;
+  set_int_kernel<<<1, 1, 0, c->stream>>>(c->sp[s].count_dev, (int)n);
+  CKL();
+  return PIC_OK;
+}
+
+double species_mass(const pic_ctx* c, int s) { return s == 0 ? c->cfg.mi : c->cfg.me; }
+double species_weight(const pic_ctx* c) { return c->cfg.n_all / c->cfg.np; }
+
+template <typename real>
+PushConst<real> push_const(const pic_ctx* c, int s) {
+  const pic_config& k = c->cfg;
+  PushConst<real> pc;
+  const double m = s == 0 ? k.mi : -k.me;
+  pc.T = (real)(0.5 * k.q * k.dt / m);
+  pc.C = (real)k.c;
+  pc.C2 = (real)(k.c * k.c);
+  pc.hdt = (real)(0.5 * k.dt / k.dx);
+  pc.qn = (real)(k.q * species_weight(c));
+  pc.nw = (real)species_weight(c);
+  pc.ex_add = (real)(k.v_drift * k.imf_y);
+  pc.ey_add = (real)(-k.v_drift * k.imf_x);
+  pc.bal_lo = k.absorb_grid2;
+  pc.bal_hx = k.nx + 4 - k.absorb_grid2;
+  pc.bal_hy = k.ny + 4 - k.absorb_grid2;
+  pc.bal_hz = k.nz + 4 - k.absorb_grid2;
+  pc.pjx = s == 0 ? F_JIX : F_JEX;
+  pc.pjy = s == 0 ? F_JIY : F_JEY;
+  pc.pjz = s == 0 ? F_JIZ : F_JEZ;
+  pc.pn = s == 0 ? F_NI : F_NE;
+  return pc;
+}
+
+// Phases timed by pic_read_timing.
+enum { PH_PUSH = 0, PH_FIELD = 1, PH_SORT = 2, PH_ADD = 3, PH_DIAG = 4, PH_COUNT = 5 };
+
+int phase_mark(pic_ctx* c, int ph) {
+  if (!c->timing) return PIC_OK;
+  auto& p = c->phase[ph];
+  if (p.used == p.ev.size()) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    p.ev.push_back(e);
+  }
+  CK(cudaEventRecord(p.ev[p.used++], c->stream));
+  return PIC_OK;
+}
+
+Ramps ramps(const pic_ctx* c) {
+  Ramps r;
+  r.rx = c->ramps;
+  r.ry = c->ramps + 2 * c->g.gx;
+  r.rz = c->ramps + 2 * c->g.gx + 2 * c->g.gy;
+  r.a = c->cfg.sigma_a;
+  return r;
+}
+
+// ------------------------------------------------------------- fields
+template <typename real>
+int do_init_grid(pic_ctx* c) {
+  DipoleParams d{c->cfg.mu0, c->cfg.coil_i, c->cfg.coil_r, c->cfg.alpha, c->cfg.dx,
+                 c->cfg.dipole_cutoff, c->cfg.imf_x, c->cfg.imf_y, c->cfg.imf_z};
+  init_fields_kernel<real><<<grid_blocks(c->g.nodes), kThreads, 0, c->stream>>>(fields<real>(c), c->g, d);
+  CKL();
+  return PIC_OK;
+}
+
+template <typename real>
+int wrap_planes(pic_ctx* c, const int* ids, int n) {
+  PlaneSet<real> s{};
+  Fields<real> F = fields<real>(c);
+  for (int q = 0; q < n; ++q) s.p[q] = F.f[ids[q]];
+  s.count = n;
+  wrap_x_kernel<real><<<grid_blocks((long long)c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
+  CKL();
+  wrap_y_kernel<real><<<grid_blocks((long long)c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
+  CKL();
+  return PIC_OK;
+}
+
+template <typename real>
+int do_renew_b(pic_ctx* c) {
+  BParams p{1. / c->cfg.e0 * c->cfg.dt * 0.5 * 0.5, 0.5 * c->cfg.dt, 1.0 / (24.0 * c->cfg.dx)};
+  const long long nint = (long long)c->g.nx * c->g.ny * c->g.nz;
+  renew_b_kernel<real><<<grid_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, ramps(c), p);
+  CKL();
+  static const int ids[6] = {F_BX, F_BY, F_BZ, F_DBX, F_DBY, F_DBZ};
+  return wrap_planes<real>(c, ids, 6);
+}
+
+template <typename real>
+int do_renew_e(pic_ctx* c) {
+  EParams p{c->cfg.c * c->cfg.c * c->cfg.dt, c->cfg.mu0, 1.0 / (24.0 * c->cfg.dx)};
+  const long long nint = (long long)c->g.nx * c->g.ny * c->g.nz;
+  renew_e_kernel<real><<<grid_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, ramps(c), p);
+  CKL();
+  static const int ids[3] = {F_EX, F_EY, F_EZ};
+  return wrap_planes<real>(c, ids, 3);
+}
+
+template <typename real>
+int do_fold(pic_ctx* c) {
+  PlaneSet<real> s{};
+  Fields<real> F = fields<real>(c);
+  for (int q = 0; q < 8; ++q) s.p[q] = F.f[F_JIX + q];
+  s.count = 8;
+  fold_x_kernel<real><<<grid_blocks((long long)c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
+  CKL();
+  fold_y_kernel<real><<<grid_blocks((long long)c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
+  CKL();
+  return PIC_OK;
+}
+
+int do_renew_grid(pic_ctx* c) {
+  // J and n planes are contiguous (F_JIX .. F_NE)
+  CK(cudaMemsetAsync((char*)c->field_mem + (size_t)F_JIX * c->plane_bytes, 0,
+                     (size_t)(F_NE - F_JIX + 1) * c->plane_bytes, c->stream));
+  return PIC_OK;
+}
+
+// ---------------------------------------------------------- particles
+template <typename real, int MODE>
+int do_push(pic_ctx* c, int s) {
+  if (c->sp[s].count == 0) return PIC_OK;
+  push_kernel<real, MODE><<<particle_blocks(c->sp[s].count), kThreads, 0, c->stream>>>(
+      parts<real>(c, s), c->sp[s].count_dev, fields<real>(c), c->g, push_const<real>(c, s), c->err);
+  CKL();
+  return PIC_OK;
+}
+
+template <typename real>
+int do_drift_n(pic_ctx* c, int s) {
+  if (c->sp[s].count == 0) return PIC_OK;
+  drift_n_kernel<real><<<particle_blocks(c->sp[s].count), kThreads, 0, c->stream>>>(
+      parts<real>(c, s), c->sp[s].count_dev, fields<real>(c), c->g, push_const<real>(c, s), c->err);
+  CKL();
+  return PIC_OK;
+}
+
+template <typename real>
+int do_sr_particle(pic_ctx* c) {
+  for (int s = 0; s < 2; ++s) {
+    if (c->sp[s].count == 0) continue;
+    sr_particle_kernel<real><<<particle_blocks(c->sp[s].count), kThreads, 0, c->stream>>>(
+        parts<real>(c, s), c->sp[s].count_dev, c->g, c->err);
+    CKL();
+  }
+  return PIC_OK;
+}
+
+// Exclusive scan of n ints (in place allowed when in != out is not required).
+int scan_exclusive(pic_ctx* c, const int* in, int* out, long long n, int* tmp, size_t tmp_len) {
+  const long long tiles = (n + kScanTile - 1) / kScanTile;
+  if ((size_t)tiles + 1 > tmp_len) return PIC_ERR_STATE;
+  scan_tile_kernel<<<(unsigned)tiles, kScanThreads, 0, c->stream>>>(in, out, tmp, n);
+  CKL();
+  if (tiles > 1) {
+    CKR(scan_exclusive(c, tmp, tmp, tiles, tmp + tiles + 1, tmp_len - (size_t)tiles - 1));
+    scan_add_kernel<<<(unsigned)tiles, 256, 0, c->stream>>>(out, tmp, n);
+    CKL();
+  }
+  return PIC_OK;
+}
+
+__global__ void sort_total_kernel(const int* offs, const int* cnt, long long n, int* count_dev) {
+  *count_dev = offs[n - 1] + cnt[n - 1];
+}
+
+template <typename real>
+int do_sort_species(pic_ctx* c, int s) {
+  Store& st = c->sp[s];
+  if (st.count == 0) return PIC_OK;
+  CK(cudaMemsetAsync(c->cnt, 0, sizeof(int) * c->ncells, c->stream));
+  CK(cudaMemsetAsync(c->cursor, 0, sizeof(int) * c->ncells, c->stream));
+  const int blocks = particle_blocks(st.count);
+  sort_count_kernel<real><<<blocks, kThreads, 0, c->stream>>>(parts<real>(c, s), st.count_dev, c->g, c->cnt);
+  CKL();
+  CKR(scan_exclusive(c, c->cnt, c->offs, c->ncells, c->scan_tmp, c->scan_tmp_len));
+  sort_scatter_kernel<real><<<blocks, kThreads, 0, c->stream>>>(parts<real>(c, s), st.count_dev, c->g, c->offs,
+                                                               c->cursor, parts<real>(c, s, 1 - st.cur));
+  CKL();
+  sort_total_kernel<<<1, 1, 0, c->stream>>>(c->offs, c->cnt, c->ncells, st.count_dev);
+  CKL();
+  int total = 0;
+  CK(cudaMemcpyAsync(&total, st.count_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  st.cur = 1 - st.cur;
+  st.count = total;
+  return PIC_OK;
+}
+
+template <typename real>
+int do_sort(pic_ctx* c) {
+  for (int s = 0; s < 2; ++s) CKR(do_sort_species<real>(c, s));
+  return PIC_OK;
+}
+
+// Generates `total` particles of species s from the slabs into slots
+// [count, count + total), drawing from the shared position/velocity streams.
+template <typename real>
+int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0) {
+  SourceParams sp{};
+  sp.init_form = init_form;
+  long long total = 0;
+  for (int q = 0; q < nslab; ++q) {
+    sp.slab[q] = slabs[q];
+    sp.slab[q].first = total;
+    total += (long long)slabs[q].nk * slabs[q].nl * slabs[q].nm * c->cfg.np;
+  }
+  sp.nslab = nslab;
+  sp.np = c->cfg.np;
+  sp.total = total;
+  if (total == 0) return PIC_OK;
+  Store& st = c->sp[s];
+  if (st.count + total > st.cap) return PIC_ERR_CAPACITY;
+  const double T = s == 0 ? c->cfg.ti : c->cfg.te;
+  const double sig = std::sqrt(c->cfg.kb * T / species_mass(c, s));
+  sp.dx = c->cfg.dx;
+  sp.lsig = std::sqrt(sig * sig);
+  sp.vdrift = c->cfg.v_drift;
+  sp.seed_p = c->cfg.seed_p;
+  sp.seed_v = c->cfg.seed_v;
+  sp.base_p = c->ctr_p;
+  sp.base_v = c->ctr_v;
+  sp.dst = (int)st.count;
+  source_kernel<real><<<grid_blocks(total), kThreads, 0, c->stream>>>(parts<real>(c, s), sp, c->err);
+  CKL();
+  c->ctr_p += 3 * total;
+  c->ctr_v += 6 * total;
+  return set_count(c, s, st.count + total);
+}
+
+template <typename real>
+int do_add_flat(pic_ctx* c) {
+  const int Nx = c->cfg.nx, Ny = c->cfg.ny, Nz = c->cfg.nz;
+  // add_ion_flat :6037-6220 at size 1: z slabs, y slabs, the low-x slab
+  const Slab slabs[5] = {
+      {2, Nx, 2, Ny, 2, 2, 0},          {2, Nx, 2, Ny, Nz, 2, 0},
+      {2, Nx, 2, 2, 4, Nz - 4, 0},      {2, Nx, Ny, 2, 4, Nz - 4, 0},
+      {2, 2, 4, Ny - 2, 4, Nz - 4, 0},
+  };
+  for (int s = 0; s < 2; ++s) {
+    Store& st = c->sp[s];
+    if (st.count > 0) {
+      delete_shell_kernel<real><<<particle_blocks(st.count), kThreads, 0, c->stream>>>(
+          parts<real>(c, s), st.count_dev, c->g);
+      CKL();
+    }
+    CKR(do_source<real>(c, s, slabs, 5));
+  }
+  return PIC_OK;
+}
+
+template <typename real>
+int do_init_particles(pic_ctx* c) {
+  // init_particle_flat :412-625: Np per cell over the interior, cell order
+  // (k outermost, m fastest) plus the reference's extra particle, which the
+  // loop places in cell (Nx, 0, 0) of the interior numbering.
+  c->ctr_p = 0;
+  c->ctr_v = 0;
+  for (int s = 0; s < 2; ++s) {
+    CKR(set_count(c, s, 0));
+    const Slab body = {2, c->cfg.nx, 2, c->cfg.ny, 2, c->cfg.nz, 0};
+    const Slab extra_cell = {2 + c->cfg.nx, 1, 2, 1, 2, 1, 0};
+    CKR(do_source<real>(c, s, &body, 1, 1));
+    // the extra particle: one draw set from the same streams
+    SourceParams sp{};
+    sp.init_form = 1;
+    sp.nslab = 1;
+    sp.slab[0] = extra_cell;
+    sp.np = 1;
+    sp.total = 1;
+    const double T = s == 0 ? c->cfg.ti : c->cfg.te;
+    const double sig = std::sqrt(c->cfg.kb * T / species_mass(c, s));
+    sp.dx = c->cfg.dx;
+    sp.lsig = std::sqrt(sig * sig);
+    sp.vdrift = c->cfg.v_drift;
+    sp.seed_p = c->cfg.seed_p;
+    sp.seed_v = c->cfg.seed_v;
+    sp.base_p = c->ctr_p;
+    sp.base_v = c->ctr_v;
+    sp.dst = (int)c->sp[s].count;
+    if (c->sp[s].count + 1 > c->sp[s].cap) return PIC_ERR_CAPACITY;
+    source_kernel<real><<<1, 32, 0, c->stream>>>(parts<real>(c, s), sp, c->err);
+    CKL();
+    c->ctr_p += 3;
+    c->ctr_v += 6;
+    CKR(set_count(c, s, c->sp[s].count + 1));
+  }
+  return PIC_OK;
+}
+
+// -------------------------------------------------------- diagnostics
+template <typename real>
+int do_thrust_sums(pic_ctx* c) {
+  CK(cudaMemsetAsync(c->acc, 0, sizeof(double) * 33, c->stream));
+  const pic_config& k = c->cfg;
+  CellBox b{};
+  const int n3[3] = {k.nx, k.ny, k.nz};
+  for (int a = 0; a < 3; ++a) {
+    b.lo[a] = n3[a] * 0.2;
+    b.hi[a] = n3[a] * 0.8;
+  }
+  b.e0 = k.e0;
+  b.inv_mu0 = 1.0 / k.mu0;
+  const long long nint = (long long)k.nx * k.ny * k.nz;
+  field_energy_kernel<real><<<particle_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, b, c->acc);
+  CKL();
+  for (int s = 0; s < 2; ++s) {
+    if (c->sp[s].count == 0) continue;
+    ThrustParams tp{};
+    tp.xlo = (double)k.nx * k.dx * 0.2; tp.xhi = (double)k.nx * k.dx * 0.8;
+    tp.ylo = (double)k.ny * k.dx * 0.2; tp.yhi = (double)k.ny * k.dx * 0.8;
+    tp.zlo = (double)k.nz * k.dx * 0.2; tp.zhi = (double)k.nz * k.dx * 0.8;
+    tp.dx = k.dx;
+    const double sg = s == 0 ? 1.0 : -1.0;
+    const double w = k.q * species_weight(c) * k.dx * k.dx * k.dx;
+    const int o = s == 0 ? 3 : 9;
+    for (int q = 0; q < 3; ++q) { tp.idx[q] = q; tp.scale[q] = sg * w; }
+    for (int q = 0; q < 6; ++q) { tp.idx[3 + q] = o + q; tp.scale[3 + q] = sg * w; }
+    tp.idx[9] = 27 + (s == 0 ? 2 : 3);
+    tp.scale[9] = 0.5 * species_mass(c, s) * species_weight(c) * k.dx * k.dx * k.dx;
+    thrust_particles_kernel<real><<<particle_blocks(c->sp[s].count), kThreads, 0, c->stream>>>(
+        parts<real>(c, s), c->sp[s].count_dev, fields<real>(c), c->g, tp, c->acc);
+    CKL();
+  }
+  return PIC_OK;
+}
+
+template <typename real>
+int do_gauss(pic_ctx* c, double* out4) {
+  CK(cudaMemsetAsync(c->acc + 40, 0, sizeof(double) * 4, c->stream));
+  CK(cudaMemsetAsync(c->maxbits, 0, sizeof(unsigned long long), c->stream));
+  const long long nint = (long long)c->g.nx * c->g.ny * c->g.nz;
+  gauss_kernel<real><<<particle_blocks(nint), kThreads, 0, c->stream>>>(
+      fields<real>(c), c->g, 1.0 / (24.0 * c->cfg.dx), c->cfg.q / c->cfg.e0, c->acc + 40, c->maxbits);
+  CKL();
+  double h[4];
+  unsigned long long mb = 0;
+  CK(cudaMemcpyAsync(h, c->acc + 40, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&mb, c->maxbits, sizeof(mb), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double mx;
+  std::memcpy(&mx, &mb, sizeof(mx));
+  out4[0] = h[0];
+  out4[1] = h[1];
+  out4[2] = mx;
+  out4[3] = h[3];
+  return PIC_OK;
+}
+
+// ------------------------------------------------------------ a step
+template <typename real>
+int do_step(pic_ctx* c) {
+  CKR(phase_mark(c, PH_FIELD));
+  CKR(do_renew_grid(c));
+  CKR(phase_mark(c, PH_FIELD));
+  if (c->c_thrust > c->cfg.sort_interval - 1) {
+    c->c_thrust = 0;
+    CKR(phase_mark(c, PH_SORT));
+    CKR(do_sort<real>(c));
+    CKR(phase_mark(c, PH_SORT));
+  }
+  if (c->c_add > c->cfg.add_interval - 1) {
+    CKR(phase_mark(c, PH_ADD));
+    CKR(do_add_flat<real>(c));
+    CKR(phase_mark(c, PH_ADD));
+    c->c_add = 0;
+  }
+  CKR(phase_mark(c, PH_FIELD));
+  CKR(do_renew_b<real>(c));
+  CKR(phase_mark(c, PH_FIELD));
+  CKR(phase_mark(c, PH_PUSH));
+  for (int s = 0; s < 2; ++s) CKR((do_push<real, PUSH_FUSED>(c, s)));
+  CKR(phase_mark(c, PH_PUSH));
+  CKR(phase_mark(c, PH_FIELD));
+  CKR(do_renew_b<real>(c));
+  CKR(do_fold<real>(c));
+  CKR(do_renew_e<real>(c));
+  CKR(phase_mark(c, PH_FIELD));
+  if (c->cfg.diag_every_step) {
+    CKR(phase_mark(c, PH_DIAG));
+    CKR(do_thrust_sums<real>(c));
+    fave_accumulate_kernel<<<1, 32, 0, c->stream>>>(c->acc, c->fave, 1.0 / 500.0);
+    CKL();
+    CKR(phase_mark(c, PH_DIAG));
+  }
+  c->c_add++;
+  c->c_thrust++;
+  return PIC_OK;
+}
+
+// --------------------------------------------------------- import/export
+int ensure_stage(pic_ctx* c, size_t bytes) {
+  if (bytes <= c->stage_bytes) return PIC_OK;
+  if (c->stage) CK(cudaFree(c->stage));
+  c->stage = nullptr;
+  c->stage_bytes = 0;
+  CK(cudaMalloc(&c->stage, bytes));
+  c->stage_bytes = bytes;
+  return PIC_OK;
+}
+
+int ensure_flags(pic_ctx* c, size_t n) {
+  if (n <= c->flags_len) return PIC_OK;
+  if (c->flags) CK(cudaFree(c->flags));
+  if (c->pos) CK(cudaFree(c->pos));
+  c->flags = c->pos = nullptr;
+  c->flags_len = 0;
+  CK(cudaMalloc(&c->flags, sizeof(int) * n));
+  CK(cudaMalloc(&c->pos, sizeof(int) * n));
+  c->flags_len = n;
+  return PIC_OK;
+}
+
+template <typename real>
+int do_export(pic_ctx* c, int s, double* rows, long long cap, long long* n_out) {
+  Store& st = c->sp[s];
+  const long long n = st.count;
+  if (n == 0) {
+    *n_out = 0;
+    return PIC_OK;
+  }
+  CKR(ensure_flags(c, (size_t)n));
+  live_flag_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s).cell, (int)n, c->flags);
+  CKL();
+  const long long tiles = (n + kScanTile - 1) / kScanTile;
+  std::vector<int> dummy;
+  int* tmp = nullptr;
+  CK(cudaMalloc(&tmp, sizeof(int) * (size_t)(2 * tiles + 64)));
+  int rc = scan_exclusive(c, c->flags, c->pos, n, tmp, (size_t)(2 * tiles + 64));
+  if (rc != PIC_OK) {
+    cudaFree(tmp);
+    return rc;
+  }
+  int last_pos = 0, last_flag = 0;
+  CK(cudaMemcpyAsync(&last_pos, c->pos + n - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&last_flag, c->flags + n - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaFree(tmp));
+  const long long live = (long long)last_pos + last_flag;
+  *n_out = live;
+  if (rows == nullptr || cap <= 0 || live == 0) return PIC_OK;
+  CKR(ensure_stage(c, sizeof(double) * 7 * (size_t)live));
+  export_rows_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(
+      parts<real>(c, s), (int)n, c->pos, c->cfg.dx, species_weight(c), (double*)c->stage);
+  CKL();
+  const long long ncopy = live < cap ? live : cap;
+  CK(cudaMemcpyAsync(rows, c->stage, sizeof(double) * 7 * (size_t)ncopy, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIC_OK;
+}
+
+template <typename real>
+int do_import(pic_ctx* c, int s, const double* rows, long long n) {
+  Store& st = c->sp[s];
+  if (n > st.cap) return PIC_ERR_CAPACITY;
+  if (n > 0) {
+    CKR(ensure_stage(c, sizeof(double) * 7 * (size_t)n));
+    CK(cudaMemcpyAsync(c->stage, rows, sizeof(double) * 7 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    import_rows_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n,
+                                                                         (const double*)c->stage, c->cfg.dx, c->err);
+    CKL();
+  }
+  CKR(set_count(c, s, n));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIC_OK;
+}
+
+template <typename real>
+__global__ void grid_export_kernel(Fields<real> F, int nodes, double* rec) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nodes) return;
+  double* r = rec + 18 * (long long)n;
+  const int map[17] = {F_BX, F_BY, F_BZ, F_B0X, F_B0Y, F_B0Z, F_EX, F_EY, F_EZ,
+                       F_JIX, F_JIY, F_JIZ, F_JEX, F_JEY, F_JEZ, F_NI, F_NE};
+#pragma unroll
+  for (int q = 0; q < 17; ++q) r[q] = (double)F.f[map[q]][n];
+  r[17] = 0.0;
+}
+
+template <typename real>
+__global__ void grid_import_kernel(Fields<real> F, int nodes, const double* rec) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nodes) return;
+  const double* r = rec + 18 * (long long)n;
+  const int map[17] = {F_BX, F_BY, F_BZ, F_B0X, F_B0Y, F_B0Z, F_EX, F_EY, F_EZ,
+                       F_JIX, F_JIY, F_JIZ, F_JEX, F_JEY, F_JEZ, F_NI, F_NE};
+#pragma unroll
+  for (int q = 0; q < 17; ++q) F.f[map[q]][n] = (real)r[q];
+  F.f[F_DBX][n] = (real)(r[0] - r[3]);
+  F.f[F_DBY][n] = (real)(r[1] - r[4]);
+  F.f[F_DBZ][n] = (real)(r[2] - r[5]);
+}
+
+template <typename real>
+int do_get_grid(pic_ctx* c, double* records) {
+  const size_t bytes = sizeof(double) * 18 * (size_t)c->g.nodes;
+  CKR(ensure_stage(c, bytes));
+  grid_export_kernel<real><<<grid_blocks(c->g.nodes), kThreads, 0, c->stream>>>(fields<real>(c), c->g.nodes,
+                                                                                (double*)c->stage);
+  CKL();
+  CK(cudaMemcpyAsync(records, c->stage, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIC_OK;
+}
+
+template <typename real>
+int do_set_grid(pic_ctx* c, const double* records) {
+  const size_t bytes = sizeof(double) * 18 * (size_t)c->g.nodes;
+  CKR(ensure_stage(c, bytes));
+  CK(cudaMemcpyAsync(c->stage, records, bytes, cudaMemcpyHostToDevice, c->stream));
+  grid_import_kernel<real><<<grid_blocks(c->g.nodes), kThreads, 0, c->stream>>>(fields<real>(c), c->g.nodes,
+                                                                                (const double*)c->stage);
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  return PIC_OK;
+}
+
+// Dispatch on the context's precision.
+#define DISPATCH(c, call)                      \
+  ((c)->prec == 64 ? call<double> : call<float>)
+
+int check_ctx(pic_ctx* c) {
+  if (!c) return PIC_ERR_ARG;
+  if (cudaSetDevice(c->cfg.device) != cudaSuccess) return PIC_ERR_CUDA;
+  return PIC_OK;
+}
+
+double ramp_value(int idx, int n_total, int absorb) {
+  if (idx - 4 <= 2 * absorb) return (2 * absorb - (idx - 4)) / 4.;
+  if (idx - 4 >= 2 * n_total - 2 * absorb) return (idx - 4 - (2 * n_total - 2 * absorb)) / 4.;
+  return 0.;
+}
+
+}  // namespace
+
+// ================================================================= C ABI
+extern "C" {
+
+const char* pic_error_string(int code) {
+  switch (code) {
+    case PIC_OK: return "ok";
+    case PIC_ERR_ARG: return "invalid argument";
+    case PIC_ERR_CUDA: return "CUDA error";
+    case PIC_ERR_CAPACITY: return "particle capacity exceeded";
+    case PIC_ERR_STATE: return "call out of order";
+    case PIC_ERR_DEVICE: return "device counters report lost work";
+    default: return "unknown error";
+  }
+}
+
+int pic_config_default(pic_config* k, int nx, int ny, int nz) {
+  if (!k) return PIC_ERR_ARG;
+  std::memset(k, 0, sizeof(*k));
+  k->nx = nx; k->ny = ny; k->nz = nz;
+  k->np = 16;
+  k->precision = 32;
+  k->device = 0;
+  k->dx = 1.5; k->dt = 1.5e-9;
+  k->q = 1.602176487e-19;
+  k->mi = 1.672621637e-27;
+  k->me = k->mi / 100.;
+  k->mu0 = 1.25663706144e-6;
+  k->e0 = 8.854187817e-12;
+  k->kb = 1.3806504e-23;
+  k->c = 2.99792458e8;
+  k->v_drift = 1.2e7;
+  k->n_all = 5e10;
+  k->ti = 1e9; k->te = 1e9;
+  k->coil_r = 2.;
+  k->coil_i = 6.8e7;
+  k->alpha = M_PI / 2.;
+  k->absorb_grid = 32;
+  k->absorb_grid2 = 40;
+  k->sigma_a = 1e-6;
+  k->dipole_cutoff = 210.;
+  k->add_interval = 5;
+  k->sort_interval = 500;
+  k->diag_every_step = 1;
+  k->capacity = 0;
+  k->seed_p = 0;
+  k->seed_v = 50;
+  return PIC_OK;
+}
+
+int pic_create(const pic_config* cfg, pic_ctx** out) {
+  if (!cfg || !out) return PIC_ERR_ARG;
+  *out = nullptr;
+  const pic_config& k = *cfg;
+  if (k.nx < 5 || k.ny < 5 || k.nz < 5 || k.nx + 4 > kMaxDim || k.ny + 4 > kMaxDim || k.nz + 4 > kMaxDim)
+    return PIC_ERR_ARG;
+  if (k.np < 1 || !(k.dx > 0) || !(k.dt > 0) || !(k.c > 0) || !(k.mi > 0) || !(k.me > 0)) return PIC_ERR_ARG;
+  if (k.precision != 32 && k.precision != 64) return PIC_ERR_ARG;
+  if (k.add_interval < 1 || k.sort_interval < 1) return PIC_ERR_ARG;
+  if (cudaSetDevice(k.device) != cudaSuccess) return PIC_ERR_CUDA;
+  pic_ctx* c = new (std::nothrow) pic_ctx();
+  if (!c) return PIC_ERR_ARG;
+  c->cfg = k;
+  c->prec = k.precision;
+  c->rsize = k.precision == 64 ? 8 : 4;
+  Geom& g = c->g;
+  g.nx = k.nx; g.ny = k.ny; g.nz = k.nz;
+  g.gx = k.nx + 4; g.gy = k.ny + 4; g.gz = k.nz + 4;
+  g.sx = g.gy * g.gz;
+  g.nodes = g.gx * g.gy * g.gz;
+  c->ncells = (long long)k.nx * k.ny * k.nz;
+  int rc = PIC_OK;
+  auto fail = [&](int code) {
+    pic_destroy(c);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  c->plane_bytes = align256((size_t)g.nodes * c->rsize);
+  if (cudaMalloc(&c->field_mem, c->plane_bytes * F_COUNT) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  cudaMemsetAsync(c->field_mem, 0, c->plane_bytes * F_COUNT, c->stream);
+  // damping ramps of init_grid (:336-365) per axis on the doubled grid
+  {
+    std::vector<double> h(2 * (g.gx + g.gy + g.gz));
+    for (int i = 0; i < 2 * g.gx; ++i) h[i] = ramp_value(i, k.nx, k.absorb_grid);
+    for (int i = 0; i < 2 * g.gy; ++i) h[2 * g.gx + i] = ramp_value(i, k.ny, k.absorb_grid);
+    for (int i = 0; i < 2 * g.gz; ++i) h[2 * (g.gx + g.gy) + i] = ramp_value(i, k.nz, k.absorb_grid);
+    if (cudaMalloc(&c->ramps, sizeof(double) * h.size()) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    if (cudaMemcpy(c->ramps, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(PIC_ERR_CUDA);
+  }
+  long long cap = k.capacity;
+  if (cap <= 0) cap = (long long)((double)k.np * k.nx * k.ny * k.nz * 1.5) + 65536;
+  if (cap > 0x7fffffffLL) return fail(PIC_ERR_ARG);
+  for (int s = 0; s < 2; ++s) {
+    c->sp[s].cap = cap;
+    for (int b = 0; b < 2; ++b)
+      if (cudaMalloc(&c->sp[s].mem[b], store_bytes(cap, c->rsize)) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    if (cudaMalloc(&c->sp[s].count_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    cudaMemsetAsync(c->sp[s].count_dev, 0, sizeof(int), c->stream);
+  }
+  if (cudaMalloc(&c->cnt, sizeof(int) * c->ncells) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  if (cudaMalloc(&c->offs, sizeof(int) * c->ncells) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  if (cudaMalloc(&c->cursor, sizeof(int) * c->ncells) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  c->scan_tmp_len = (size_t)(c->ncells / kScanTile) * 2 + 64;
+  if (cudaMalloc(&c->scan_tmp, sizeof(int) * c->scan_tmp_len) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  if (cudaMalloc(&c->acc, sizeof(double) * 64) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  if (cudaMalloc(&c->maxbits, sizeof(unsigned long long)) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  if (cudaMalloc(&c->fave, sizeof(double) * 27) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  if (cudaMalloc(&c->err, sizeof(unsigned long long) * ERR_COUNT) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  cudaMemsetAsync(c->acc, 0, sizeof(double) * 64, c->stream);
+  cudaMemsetAsync(c->fave, 0, sizeof(double) * 27, c->stream);
+  cudaMemsetAsync(c->err, 0, sizeof(unsigned long long) * ERR_COUNT, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  (void)rc;
+  *out = c;
+  return PIC_OK;
+}
+
+int pic_destroy(pic_ctx* c) {
+  if (!c) return PIC_OK;
+  cudaSetDevice(c->cfg.device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->field_mem);
+  cudaFree(c->ramps);
+  for (int s = 0; s < 2; ++s) {
+    cudaFree(c->sp[s].mem[0]);
+    cudaFree(c->sp[s].mem[1]);
+    cudaFree(c->sp[s].count_dev);
+  }
+  cudaFree(c->cnt);
+  cudaFree(c->offs);
+  cudaFree(c->cursor);
+  cudaFree(c->scan_tmp);
+  cudaFree(c->acc);
+  cudaFree(c->maxbits);
+  cudaFree(c->fave);
+  cudaFree(c->err);
+  cudaFree(c->stage);
+  cudaFree(c->flags);
+  cudaFree(c->pos);
+  for (int p = 0; p < 8; ++p)
+    for (cudaEvent_t e : c->phase[p].ev) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return PIC_OK;
+}
+
+int pic_init_grid(pic_ctx* c) {
+  CKR(check_ctx(c));
+  CKR(DISPATCH(c, do_init_grid)(c));
+  c->grid_ready = true;
+  return PIC_OK;
+}
+
+int pic_init_particle_flat(pic_ctx* c) {
+  CKR(check_ctx(c));
+  CKR(DISPATCH(c, do_init_particles)(c));
+  c->particles_ready = true;
+  return PIC_OK;
+}
+
+int pic_renew_grid(pic_ctx* c) {
+  CKR(check_ctx(c));
+  return do_renew_grid(c);
+}
+
+int pic_renew_b4_2(pic_ctx* c) {
+  CKR(check_ctx(c));
+  return DISPATCH(c, do_renew_b)(c);
+}
+
+int pic_renew_e4_2(pic_ctx* c) {
+  CKR(check_ctx(c));
+  return DISPATCH(c, do_renew_e)(c);
+}
+
+int pic_push_deposit_j(pic_ctx* c, int species) {
+  CKR(check_ctx(c));
+  if (species < -1 || species > 1) return PIC_ERR_ARG;
+  for (int s = 0; s < 2; ++s) {
+    if (species >= 0 && s != species) continue;
+    CKR((c->prec == 64 ? do_push<double, PUSH_J>(c, s) : do_push<float, PUSH_J>(c, s)));
+  }
+  return PIC_OK;
+}
+
+int pic_drift_deposit_n(pic_ctx* c, int species) {
+  CKR(check_ctx(c));
+  if (species < -1 || species > 1) return PIC_ERR_ARG;
+  for (int s = 0; s < 2; ++s) {
+    if (species >= 0 && s != species) continue;
+    CKR((c->prec == 64 ? do_drift_n<double>(c, s) : do_drift_n<float>(c, s)));
+  }
+  return PIC_OK;
+}
+
+int pic_reduce_current(pic_ctx* c) {
+  CKR(check_ctx(c));
+  return DISPATCH(c, do_fold)(c);
+}
+
+int pic_sr_particle(pic_ctx* c) {
+  CKR(check_ctx(c));
+  return DISPATCH(c, do_sr_particle)(c);
+}
+
+int pic_add_flat(pic_ctx* c) {
+  CKR(check_ctx(c));
+  return DISPATCH(c, do_add_flat)(c);
+}
+
+int pic_sort(pic_ctx* c) {
+  CKR(check_ctx(c));
+  return DISPATCH(c, do_sort)(c);
+}
+
+int pic_thrust_f(pic_ctx* c, double* F27, double* E6) {
+  CKR(check_ctx(c));
+  CKR(DISPATCH(c, do_thrust_sums)(c));
+  double h[33];
+  CK(cudaMemcpyAsync(h, c->acc, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (F27) std::memcpy(F27, h, sizeof(double) * 27);
+  if (E6) std::memcpy(E6, h + 27, sizeof(double) * 6);
+  return PIC_OK;
+}
+
+int pic_thrust_fave(pic_ctx* c, double* Fave27, int reset) {
+  CKR(check_ctx(c));
+  if (Fave27) {
+    CK(cudaMemcpyAsync(Fave27, c->fave, sizeof(double) * 27, cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (reset) CK(cudaMemsetAsync(c->fave, 0, sizeof(double) * 27, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIC_OK;
+}
+
+int pic_gauss_residual(pic_ctx* c, double* out4) {
+  CKR(check_ctx(c));
+  if (!out4) return PIC_ERR_ARG;
+  return DISPATCH(c, do_gauss)(c, out4);
+}
+
+int pic_step(pic_ctx* c, int nsteps) {
+  CKR(check_ctx(c));
+  if (!c->grid_ready) return PIC_ERR_STATE;
+  for (int i = 0; i < nsteps; ++i) CKR(DISPATCH(c, do_step)(c));
+  return PIC_OK;
+}
+
+int pic_fdtd(pic_ctx* c, int nsteps) {
+  CKR(check_ctx(c));
+  if (!c->grid_ready) return PIC_ERR_STATE;
+  c->c_add = 0;
+  c->c_thrust = 0;
+  CKR(DISPATCH(c, do_add_flat)(c));
+  return pic_step(c, nsteps);
+}
+
+int pic_set_particles(pic_ctx* c, int species, const double* rows, const int* flag, long long n) {
+  CKR(check_ctx(c));
+  if (species < 0 || species > 1 || n < 0 || (n > 0 && !rows)) return PIC_ERR_ARG;
+  const double w = species_weight(c);
+  for (long long i = 0; i < n; ++i) {
+    if (std::fabs(rows[7 * i + 6] - w) > 1e-12 * std::fabs(w)) return PIC_ERR_ARG;
+    if (flag && flag[i] != 1) return PIC_ERR_ARG;
+  }
+  CKR(DISPATCH(c, do_import)(c, species, rows, n));
+  c->particles_ready = true;
+  return PIC_OK;
+}
+
+int pic_get_particles(pic_ctx* c, int species, double* rows, int* flag, long long cap, long long* n_out) {
+  CKR(check_ctx(c));
+  if (species < 0 || species > 1 || !n_out) return PIC_ERR_ARG;
+  CKR(DISPATCH(c, do_export)(c, species, rows, cap, n_out));
+  if (flag) {
+    const long long m = *n_out < cap ? *n_out : cap;
+    for (long long i = 0; i < m; ++i) flag[i] = 1;
+  }
+  return PIC_OK;
+}
+
+int pic_particle_count(pic_ctx* c, int species, long long* n_out) {
+  return pic_get_particles(c, species, nullptr, nullptr, 0, n_out);
+}
+
+int pic_get_grid(pic_ctx* c, double* records) {
+  CKR(check_ctx(c));
+  if (!records) return PIC_ERR_ARG;
+  return DISPATCH(c, do_get_grid)(c, records);
+}
+
+int pic_set_grid(pic_ctx* c, const double* records) {
+  CKR(check_ctx(c));
+  if (!records) return PIC_ERR_ARG;
+  CKR(DISPATCH(c, do_set_grid)(c, records));
+  c->grid_ready = true;
+  return PIC_OK;
+}
+
+int pic_rng_counters(pic_ctx* c, long long* ctr_p, long long* ctr_v, int set) {
+  if (!c || !ctr_p || !ctr_v) return PIC_ERR_ARG;
+  if (set) {
+    if (*ctr_p < 0 || *ctr_v < 0) return PIC_ERR_ARG;
+    c->ctr_p = *ctr_p;
+    c->ctr_v = *ctr_v;
+  } else {
+    *ctr_p = c->ctr_p;
+    *ctr_v = c->ctr_v;
+  }
+  return PIC_OK;
+}
+
+int pic_status(pic_ctx* c, long long* counters8) {
+  CKR(check_ctx(c));
+  unsigned long long h[ERR_COUNT];
+  CK(cudaMemcpyAsync(h, c->err, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int any = 0;
+  for (int q = 0; q < ERR_COUNT; ++q) {
+    if (counters8) counters8[q] = (long long)h[q];
+    if (q < ERR_FIRST_INFO) any |= h[q] != 0;
+  }
+  return any ? PIC_ERR_DEVICE : PIC_OK;
+}
+
+int pic_synchronize(pic_ctx* c) {
+  CKR(check_ctx(c));
+  CK(cudaStreamSynchronize(c->stream));
+  return PIC_OK;
+}
+
+int pic_get_stream(pic_ctx* c, void** stream) {
+  if (!c || !stream) return PIC_ERR_ARG;
+  *stream = (void*)c->stream;
+  return PIC_OK;
+}
+
+int pic_set_timing(pic_ctx* c, int enable) {
+  CKR(check_ctx(c));
+  CK(cudaStreamSynchronize(c->stream));
+  c->timing = enable != 0;
+  for (int p = 0; p < 8; ++p) c->phase[p].used = 0;
+  return PIC_OK;
+}
+
+int pic_read_timing(pic_ctx* c, double* ms8, long long* marks8, long long* launches) {
+  CKR(check_ctx(c));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int p = 0; p < 8; ++p) {
+    double ms = 0.0;
+    const auto& ph = c->phase[p];
+    for (size_t q = 0; q + 1 < ph.used; q += 2) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ph.ev[q], ph.ev[q + 1]));
+      ms += t;
+    }
+    if (ms8) ms8[p] = ms;
+    if (marks8) marks8[p] = (long long)(ph.used / 2);
+    c->phase[p].used = 0;
+  }
+  if (launches) *launches = c->launches;
+  return PIC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,140 @@
+// Shared device-side definitions for the B200 PIC step.
+//
+// Grid layout in HBM: one plane per field component over the padded
+// (nx+4)*(ny+4)*(nz+4) node array, node index (i*gy + j)*gz + k with k (the
+// reference's z, its solar-wind axis) fastest, as grid[k][l][m] of
+// PIC/3d_pic458_domain.c:147. Planes are padded to 256-byte boundaries.
+//
+// Particle layout: structure of arrays per species,
+//   cell : int32, (i << 20) | (j << 10) | k, the containing cell of the padded
+//          grid (i = floor(x/dx)), -1 for an empty slot
+//   ox, oy, oz : in-cell offsets in [0, 1) (x = (i + ox) dx)
+//   vx, vy, vz : velocities in the caller's units
+// 28 bytes per particle in FP32, 52 in FP64.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pb {
+
+constexpr int kCellBits = 10;
+constexpr int kCellMask = (1 << kCellBits) - 1;
+constexpr int kMaxDim = 1 << kCellBits;  // padded extent limit per axis
+
+__host__ __device__ __forceinline__ int pack_cell(int i, int j, int k) {
+  return (i << (2 * kCellBits)) | (j << kCellBits) | k;
+}
+__host__ __device__ __forceinline__ void unpack_cell(int c, int& i, int& j, int& k) {
+  i = c >> (2 * kCellBits);
+  j = (c >> kCellBits) & kCellMask;
+  k = c & kCellMask;
+}
+
+struct Geom {
+  int nx, ny, nz;   // interior cells
+  int gx, gy, gz;   // padded extents (n + 4)
+  int sx;           // node stride of i (gy * gz)
+  int nodes;        // gx * gy * gz
+};
+
+// Field components stored as planes. B is the total field used by the gather,
+// DB = B - B0 the induced part the curl updates work on.
+enum FieldId {
+  F_EX, F_EY, F_EZ, F_BX, F_BY, F_BZ, F_DBX, F_DBY, F_DBZ, F_B0X, F_B0Y, F_B0Z,
+  F_JIX, F_JIY, F_JIZ, F_JEX, F_JEY, F_JEZ, F_NI, F_NE, F_COUNT
+};
+
+template <typename real>
+struct Fields {
+  real* f[F_COUNT];
+};
+
+template <typename real>
+struct Parts {
+  int* cell;
+  real* o[3];
+  real* v[3];
+};
+
+// Device error counters (see pic_status).
+enum ErrId {
+  ERR_DEPOSIT_OOB = 0, ERR_CELL_RANGE = 1, ERR_NONFINITE = 2,
+  ERR_FIRST_INFO = 3, CNT_PUSHED = 3,  // slots from here on count work, not errors
+  ERR_COUNT = 8
+};
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): the random streams that
+// replace the reference's gsl_rng objects. Draw d of the stream keyed by seed
+// uses block d/2 and the word pair d&1; a draw is a 53-bit uniform in [0, 1).
+__host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+    c[1] = (uint32_t)p1;
+    c[3] = (uint32_t)p0;
+    c[0] = n0;
+    c[2] = n2;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+__host__ __device__ __forceinline__ double uniform53(uint64_t seed, uint64_t d) {
+  uint32_t c[4] = {(uint32_t)(d >> 1), (uint32_t)(d >> 33), 0u, 0u};
+  philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const uint32_t a = (d & 1) ? c[2] : c[0];
+  const uint32_t b = (d & 1) ? c[3] : c[1];
+  const uint64_t m = ((uint64_t)a << 21) | (uint64_t)(b >> 11);
+  return (double)m * (1.0 / 9007199254740992.0);
+}
+
+#ifdef __CUDACC__
+// a*(1-u) + b*u rounded step by step (no contraction), as the host computes it.
+__device__ __forceinline__ double flat_rn(double a, double b, double u) {
+  return __dadd_rn(__dmul_rn(a, __dadd_rn(1.0, -u)), __dmul_rn(b, u));
+}
+
+// Box-Muller from draws d and d+1 of a stream: sqrt(-2 ln(1-u1)) cos(2 pi u2).
+__device__ __forceinline__ double gauss_bm(uint64_t seed, uint64_t d) {
+  const double u1 = __dadd_rn(1.0, -uniform53(seed, d));
+  const double u2 = uniform53(seed, d + 1);
+  const double r = sqrt(__dmul_rn(-2.0, log(u1)));
+  const double ang = __dmul_rn(__dmul_rn(2.0, 3.14159265358979323846), u2);
+  return __dmul_rn(r, cos(ang));
+}
+
+// Splits an absolute coordinate in cells into (cell, offset in [0,1)).
+template <typename real>
+__device__ __forceinline__ void split_coord(double xc, int& i, real& f) {
+  double fi = floor(xc);
+  i = (int)fi;
+  f = (real)(xc - fi);
+  if (f >= (real)1) {
+    f = (real)0;
+    i += 1;
+  }
+}
+
+// Adds a displacement d (in cells) to (i, f) keeping f in [0, 1).
+template <typename real>
+__device__ __forceinline__ void advance(int& i, real& f, real d) {
+  real t = f + d;
+  if (t >= (real)1 || t < (real)0) {
+    const real fl = floor(t);
+    i += (int)fl;
+    t -= fl;
+    if (t >= (real)1) {  // t - floor(t) rounded up to 1 for a tiny negative t
+      t = (real)0;
+      i += 1;
+    }
+  }
+  f = t;
+}
+#endif
+
+}  // namespace pb

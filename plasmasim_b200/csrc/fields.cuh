@@ -1,0 +1,249 @@
+// Field kernels: dipole B0 and damping profile (init_grid), the damped
+// 4th-order B and E updates (renew_b4_2 / renew_e4_2) and the size-1 periodic
+// ghost copies and folds (sr_b / sr_e / sr_current2).
+//
+// Each update is one thread per interior node, k (z) fastest so that a warp
+// reads and writes 32 consecutive nodes of every plane it touches; the +-1/+-2
+// neighbours along i and j come from L1/L2. HBM bound: per node a B half-step
+// moves 12 words (E3 read, DB3 read, B0 3 read, DB3 + B3 written... see below)
+// and an E step 15 words.
+#pragma once
+
+#include "common.cuh"
+
+namespace pb {
+
+// Damping ramp on the doubled sub-grid (init_grid, PIC/3d_pic458_domain.c:339-365);
+// sigma = a (0.1 sqrt(x^4+y^4+z^4) + 0.01 sqrt(x^12+y^12+z^12)) (:366-367).
+__device__ __forceinline__ double sigma_of(double a, double x, double y, double z) {
+  if (x == 0.0 && y == 0.0 && z == 0.0) return 0.0;
+  const double x2 = x * x, y2 = y * y, z2 = z * z;
+  const double x4 = x2 * x2, y4 = y2 * y2, z4 = z2 * z2;
+  return a * (0.1 * sqrt(x4 + y4 + z4) + 0.01 * sqrt(x4 * x4 * x4 + y4 * y4 * y4 + z4 * z4 * z4));
+}
+
+struct Ramps {
+  const double* rx;  // 2*gx values
+  const double* ry;
+  const double* rz;
+  double a;
+};
+
+// external_current7 (:4579-4634) at rank (0,0): analytic point dipole of
+// moment I*pi*R^2 along (0, sin alpha, cos alpha), centred on node
+// ((nx+4)/2, (ny+4)/2, (nz+4)/2), each component on its own stagger.
+struct DipoleParams {
+  double mu0, I, R, alpha, dx, cutoff, imfx, imfy, imfz;
+};
+
+template <typename real>
+__global__ void init_fields_kernel(Fields<real> F, Geom g, DipoleParams d) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= g.nodes) return;
+  const int k = n / g.sx, l = (n / g.gz) % g.gy, m = n % g.gz;
+  const double Pi = 3.14159265358979323846;
+  const int cx = (g.nx + 4) / 2, cy = (g.ny + 4) / 2, cz = (g.nz + 4) / 2;
+  double x = (double)(k - cx) * d.dx, y = (double)(l - cy) * d.dx, z = (double)(m - cz) * d.dx;
+  double r = sqrt(x * x + y * y + z * z);
+  double b0x = d.imfx, b0y = d.imfy, b0z = d.imfz;
+  if (r < d.cutoff * d.dx) {
+    const double mom = d.mu0 * d.I * Pi * d.R * d.R;
+    const double sa = sin(d.alpha), ca = cos(d.alpha);
+    x = ((double)(k - cx) + 0.5) * d.dx; y = (double)(l - cy) * d.dx; z = (double)(m - cz) * d.dx;
+    r = sqrt(x * x + y * y + z * z);
+    b0x = mom * (3. * x * y * sa + 3. * x * z * ca) / (4. * Pi * pow(r, 5.0)) + d.imfx;
+    x = (double)(k - cx) * d.dx; y = ((double)(l - cy) + 0.5) * d.dx; z = (double)(m - cz) * d.dx;
+    r = sqrt(x * x + y * y + z * z);
+    b0y = mom * (3. * y * y * sa + 3. * y * z * ca - r * r * sa) / (4. * Pi * pow(r, 5.0)) + d.imfy;
+    x = (double)(k - cx) * d.dx; y = (double)(l - cy) * d.dx; z = ((double)(m - cz) + 0.5) * d.dx;
+    r = sqrt(x * x + y * y + z * z);
+    b0z = mom * (3. * y * z * sa + 3. * z * z * ca - r * r * ca) / (4. * Pi * pow(r, 5.0)) + d.imfz;
+  }
+  F.f[F_B0X][n] = (real)b0x; F.f[F_B0Y][n] = (real)b0y; F.f[F_B0Z][n] = (real)b0z;
+  F.f[F_BX][n] = (real)b0x; F.f[F_BY][n] = (real)b0y; F.f[F_BZ][n] = (real)b0z;
+  F.f[F_DBX][n] = (real)0; F.f[F_DBY][n] = (real)0; F.f[F_DBZ][n] = (real)0;
+  F.f[F_EX][n] = (real)0; F.f[F_EY][n] = (real)0; F.f[F_EZ][n] = (real)0;
+#pragma unroll
+  for (int q = F_JIX; q <= F_NE; ++q) F.f[q][n] = (real)0;
+}
+
+struct BParams {
+  double temp;   // dt / (4 e0)           (renew_b4_2 :2583)
+  double dth;    // dt / 2
+  double inv24dx;
+};
+
+struct EParams {
+  double temp;   // c^2 dt                (renew_e4_2 :2616)
+  double mu0;
+  double inv24dx;
+};
+
+// renew_b4_2 (:2580-2611) on the induced field: DB <- ca DB - cb curl4(E),
+// B = B0 + DB, with ca = (1 - s t)/(1 + s t), cb = (dt/2)/(1 + s t).
+template <typename real>
+__global__ void __launch_bounds__(256) renew_b_kernel(Fields<real> F, Geom g, Ramps rp, BParams p) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nint = g.nx * g.ny * g.nz;
+  if (t >= nint) return;
+  const int m = 2 + t % g.nz, l = 2 + (t / g.nz) % g.ny, k = 2 + t / (g.nz * g.ny);
+  const int n = k * g.sx + l * g.gz + m;
+  const int sy = g.gz, sx = g.sx;
+  const real* __restrict__ ex = F.f[F_EX];
+  const real* __restrict__ ey = F.f[F_EY];
+  const real* __restrict__ ez = F.f[F_EZ];
+  const real c24 = (real)p.inv24dx;
+  // x component at (k+1/2, l, m): sigma[2k+1][2l][2m]
+  {
+    const double s = sigma_of(rp.a, rp.rx[2 * k + 1], rp.ry[2 * l], rp.rz[2 * m]);
+    const real ca = (real)((1. - s * p.temp) / (1. + s * p.temp));
+    const real cb = (real)(p.dth / (1. + s * p.temp));
+    const real curl = ((real)27 * (ez[n] - ez[n - sy] - ey[n] + ey[n - 1]) -
+                       (ez[n + sy] - ez[n - 2 * sy] - ey[n + 1] + ey[n - 2])) * c24;
+    const real db = ca * F.f[F_DBX][n] - cb * curl;
+    F.f[F_DBX][n] = db;
+    F.f[F_BX][n] = F.f[F_B0X][n] + db;
+  }
+  {
+    const double s = sigma_of(rp.a, rp.rx[2 * k], rp.ry[2 * l + 1], rp.rz[2 * m]);
+    const real ca = (real)((1. - s * p.temp) / (1. + s * p.temp));
+    const real cb = (real)(p.dth / (1. + s * p.temp));
+    const real curl = ((real)27 * (ex[n] - ex[n - 1] - ez[n] + ez[n - sx]) -
+                       (ex[n + 1] - ex[n - 2] - ez[n + sx] + ez[n - 2 * sx])) * c24;
+    const real db = ca * F.f[F_DBY][n] - cb * curl;
+    F.f[F_DBY][n] = db;
+    F.f[F_BY][n] = F.f[F_B0Y][n] + db;
+  }
+  {
+    const double s = sigma_of(rp.a, rp.rx[2 * k], rp.ry[2 * l], rp.rz[2 * m + 1]);
+    const real ca = (real)((1. - s * p.temp) / (1. + s * p.temp));
+    const real cb = (real)(p.dth / (1. + s * p.temp));
+    const real curl = ((real)27 * (ey[n] - ey[n - sx] - ex[n] + ex[n - sy]) -
+                       (ey[n + sx] - ey[n - 2 * sx] - ex[n + sy] + ex[n - 2 * sy])) * c24;
+    const real db = ca * F.f[F_DBZ][n] - cb * curl;
+    F.f[F_DBZ][n] = db;
+    F.f[F_BZ][n] = F.f[F_B0Z][n] + db;
+  }
+}
+
+// renew_e4_2 (:2613-2652): E <- ca E + cb (curl4(DB) - mu0 (J_i - J_e)),
+// ca = (1 - mu0 s t/2)/(1 + mu0 s t/2), cb = t/(1 + mu0 s t/2), t = c^2 dt.
+template <typename real>
+__global__ void __launch_bounds__(256) renew_e_kernel(Fields<real> F, Geom g, Ramps rp, EParams p) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nint = g.nx * g.ny * g.nz;
+  if (t >= nint) return;
+  const int m = 2 + t % g.nz, l = 2 + (t / g.nz) % g.ny, k = 2 + t / (g.nz * g.ny);
+  const int n = k * g.sx + l * g.gz + m;
+  const int sy = g.gz, sx = g.sx;
+  const real* __restrict__ bx = F.f[F_DBX];
+  const real* __restrict__ by = F.f[F_DBY];
+  const real* __restrict__ bz = F.f[F_DBZ];
+  const real c24 = (real)p.inv24dx;
+  const real mu0 = (real)p.mu0;
+  {
+    const double s = sigma_of(rp.a, rp.rx[2 * k], rp.ry[2 * l + 1], rp.rz[2 * m + 1]);
+    const double h = 0.5 * p.mu0 * s * p.temp;
+    const real ca = (real)((1. - h) / (1. + h)), cb = (real)(p.temp / (1. + h));
+    const real curl = ((real)27 * ((bz[n + sy] - bz[n]) - (by[n + 1] - by[n])) -
+                       ((bz[n + 2 * sy] - bz[n - sy]) - (by[n + 2] - by[n - 1]))) * c24;
+    F.f[F_EX][n] = ca * F.f[F_EX][n] + cb * (curl - mu0 * (F.f[F_JIX][n] - F.f[F_JEX][n]));
+  }
+  {
+    const double s = sigma_of(rp.a, rp.rx[2 * k + 1], rp.ry[2 * l], rp.rz[2 * m + 1]);
+    const double h = 0.5 * p.mu0 * s * p.temp;
+    const real ca = (real)((1. - h) / (1. + h)), cb = (real)(p.temp / (1. + h));
+    const real curl = ((real)27 * ((bx[n + 1] - bx[n]) - (bz[n + sx] - bz[n])) -
+                       ((bx[n + 2] - bx[n - 1]) - (bz[n + 2 * sx] - bz[n - sx]))) * c24;
+    F.f[F_EY][n] = ca * F.f[F_EY][n] + cb * (curl - mu0 * (F.f[F_JIY][n] - F.f[F_JEY][n]));
+  }
+  {
+    const double s = sigma_of(rp.a, rp.rx[2 * k + 1], rp.ry[2 * l + 1], rp.rz[2 * m]);
+    const double h = 0.5 * p.mu0 * s * p.temp;
+    const real ca = (real)((1. - h) / (1. + h)), cb = (real)(p.temp / (1. + h));
+    const real curl = ((real)27 * ((by[n + sx] - by[n]) - (bx[n + sy] - bx[n])) -
+                       ((by[n + 2 * sx] - by[n - sx]) - (bx[n + 2 * sy] - bx[n - sy]))) * c24;
+    F.f[F_EZ][n] = ca * F.f[F_EZ][n] + cb * (curl - mu0 * (F.f[F_JIZ][n] - F.f[F_JEZ][n]));
+  }
+}
+
+// Up to 8 planes processed by one ghost kernel.
+template <typename real>
+struct PlaneSet {
+  real* p[8];
+  int count;
+};
+
+// sr_b / sr_e at size 1, x pass (:1016-1101): ghosts 0,1 <- N, N+1 and
+// N+2, N+3 <- 2, 3 for every (l, m).
+template <typename real>
+__global__ void wrap_x_kernel(PlaneSet<real> s, Geom g) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.gy * g.gz) return;
+  const int N = g.nx, sx = g.sx;
+  for (int q = 0; q < s.count; ++q) {
+    real* a = s.p[q];
+    const real v0 = a[N * sx + t], v1 = a[(N + 1) * sx + t];
+    const real v2 = a[2 * sx + t], v3 = a[3 * sx + t];
+    a[t] = v0;
+    a[sx + t] = v1;
+    a[(N + 2) * sx + t] = v2;
+    a[(N + 3) * sx + t] = v3;
+  }
+}
+
+// y pass (:1103-1190): ghosts 0,1 <- N, N+1 and N+2, N+3 <- 2, 3 for every (k, m).
+template <typename real>
+__global__ void wrap_y_kernel(PlaneSet<real> s, Geom g) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.gx * g.gz) return;
+  const int k = t / g.gz, m = t % g.gz;
+  const int N = g.ny, sy = g.gz;
+  const int base = k * g.sx + m;
+  for (int q = 0; q < s.count; ++q) {
+    real* a = s.p[q];
+    const real v0 = a[base + N * sy], v1 = a[base + (N + 1) * sy];
+    const real v2 = a[base + 2 * sy], v3 = a[base + 3 * sy];
+    a[base] = v0;
+    a[base + sy] = v1;
+    a[base + (N + 2) * sy] = v2;
+    a[base + (N + 3) * sy] = v3;
+  }
+}
+
+// sr_current2 at size 1, x pass (:1815-1935): planes 2,3 += N+2, N+3 and
+// N, N+1 += 0, 1 (sources are ghosts, targets interior: disjoint for N >= 2).
+template <typename real>
+__global__ void fold_x_kernel(PlaneSet<real> s, Geom g) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.gy * g.gz) return;
+  const int N = g.nx, sx = g.sx;
+  for (int q = 0; q < s.count; ++q) {
+    real* a = s.p[q];
+    const real g0 = a[t], g1 = a[sx + t], g2 = a[(N + 2) * sx + t], g3 = a[(N + 3) * sx + t];
+    a[2 * sx + t] += g2;
+    a[3 * sx + t] += g3;
+    a[N * sx + t] += g0;
+    a[(N + 1) * sx + t] += g1;
+  }
+}
+
+// y pass (:1937-2036), over every k including the x ghosts.
+template <typename real>
+__global__ void fold_y_kernel(PlaneSet<real> s, Geom g) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.gx * g.gz) return;
+  const int k = t / g.gz, m = t % g.gz;
+  const int N = g.ny, sy = g.gz;
+  const int base = k * g.sx + m;
+  for (int q = 0; q < s.count; ++q) {
+    real* a = s.p[q];
+    const real g0 = a[base], g1 = a[base + sy], g2 = a[base + (N + 2) * sy], g3 = a[base + (N + 3) * sy];
+    a[base + 2 * sy] += g2;
+    a[base + 3 * sy] += g3;
+    a[base + N * sy] += g0;
+    a[base + (N + 1) * sy] += g1;
+  }
+}
+
+}  // namespace pb

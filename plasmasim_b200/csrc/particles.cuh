@@ -1,0 +1,566 @@
+// Particle kernels: push with field gather, current and density deposits,
+// boundary removal/wrap, initial load and boundary injection, cell sort.
+#pragma once
+
+#include "common.cuh"
+
+namespace pb {
+
+// ------------------------------------------------------------------ shapes
+// Per-axis linear weights of shape_func_v2 (PIC/3d_pic458_domain.c:3104-3139)
+// in cell units for a coordinate (i, f), x = (i + f) dx:
+//  node-aligned components: base i,  weights (1 - f, f)
+//  half-shifted components: base (int)(x/dx - 0.5), i.e. i - 1 for f < 1/2
+//  (i itself for f >= 1/2, and for i == 0 where the cast truncates toward 0),
+//  weights (1 - p, p) with p = x/dx - (base + 1/2).
+template <typename real>
+struct Axis {
+  int a, b;          // node-aligned and half-shifted base index
+  real a0, a1, b0, b1;
+};
+
+template <typename real>
+__device__ __forceinline__ Axis<real> axis_weights(int i, real f) {
+  Axis<real> w;
+  w.a = i;
+  w.a1 = f;
+  w.a0 = (real)1 - f;
+  w.b = (f >= (real)0.5 || i == 0) ? i : i - 1;
+  w.b1 = (real)(i - w.b) - (real)0.5 + f;
+  w.b0 = (real)1 - w.b1;
+  return w;
+}
+
+template <typename real>
+__device__ __forceinline__ real ldg(const real* p) { return __ldg(p); }
+
+// Trilinear interpolation of one plane from the 2x2x2 nodes at base n.
+template <typename real>
+__device__ __forceinline__ real trilerp(const real* __restrict__ F, int n, int sx, int sy,
+                                        real x0, real x1, real y0, real y1, real z0, real z1) {
+  const real c00 = ldg(F + n) * z0 + ldg(F + n + 1) * z1;
+  const real c01 = ldg(F + n + sy) * z0 + ldg(F + n + sy + 1) * z1;
+  const real c10 = ldg(F + n + sx) * z0 + ldg(F + n + sx + 1) * z1;
+  const real c11 = ldg(F + n + sx + sy) * z0 + ldg(F + n + sx + sy + 1) * z1;
+  return (c00 * y0 + c01 * y1) * x0 + (c10 * y0 + c11 * y1) * x1;
+}
+
+// Area-weighted scatter of v onto the 2x2x2 nodes at base n.
+template <typename real>
+__device__ __forceinline__ void scatter8(real* F, int n, int sx, int sy, real v,
+                                         real x0, real x1, real y0, real y1, real z0, real z1) {
+  const real a0 = v * x0, a1 = v * x1;
+  const real a00 = a0 * y0, a01 = a0 * y1, a10 = a1 * y0, a11 = a1 * y1;
+  atomicAdd(F + n, a00 * z0);
+  atomicAdd(F + n + 1, a00 * z1);
+  atomicAdd(F + n + sy, a01 * z0);
+  atomicAdd(F + n + sy + 1, a01 * z1);
+  atomicAdd(F + n + sx, a10 * z0);
+  atomicAdd(F + n + sx + 1, a10 * z1);
+  atomicAdd(F + n + sx + sy, a11 * z0);
+  atomicAdd(F + n + sx + sy + 1, a11 * z1);
+}
+
+template <typename real>
+struct Gathered {
+  real ex, ey, ez, bx, by, bz;
+};
+
+// shape_func_v2 (:3017-3326): E and B at (i,f), each on its own stagger.
+template <typename real>
+__device__ __forceinline__ Gathered<real> gather6(const Fields<real>& F, const Geom& g,
+                                                  const Axis<real>& X, const Axis<real>& Y,
+                                                  const Axis<real>& Z) {
+  const int sx = g.sx, sy = g.gz;
+  Gathered<real> r;
+  // ex (k, l+1/2, m+1/2): x aligned, y and z shifted
+  r.ex = trilerp(F.f[F_EX], X.a * sx + Y.b * sy + Z.b, sx, sy, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
+  // ey (k+1/2, l, m+1/2)
+  r.ey = trilerp(F.f[F_EY], X.b * sx + Y.a * sy + Z.b, sx, sy, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
+  // ez (k+1/2, l+1/2, m)
+  r.ez = trilerp(F.f[F_EZ], X.b * sx + Y.b * sy + Z.a, sx, sy, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
+  // bx (k+1/2, l, m)
+  r.bx = trilerp(F.f[F_BX], X.b * sx + Y.a * sy + Z.a, sx, sy, X.b0, X.b1, Y.a0, Y.a1, Z.a0, Z.a1);
+  // by (k, l+1/2, m)
+  r.by = trilerp(F.f[F_BY], X.a * sx + Y.b * sy + Z.a, sx, sy, X.a0, X.a1, Y.b0, Y.b1, Z.a0, Z.a1);
+  // bz (k, l, m+1/2)
+  r.bz = trilerp(F.f[F_BZ], X.a * sx + Y.a * sy + Z.b, sx, sy, X.a0, X.a1, Y.a0, Y.a1, Z.b0, Z.b1);
+  return r;
+}
+
+template <typename real>
+struct PushConst {
+  real T;               // 0.5 q dt / m, m < 0 for electrons (cal_track4 :2812)
+  real C, C2;           // C, C*C
+  real hdt;             // 0.5 dt / dx: cells moved per unit velocity in half a step
+  real qn;              // q n: current per unit velocity and unit weight
+  real nw;              // n: density per unit weight
+  real ex_add, ey_add;  // V*IMF_y, -V*IMF_x (:2817-2818)
+  int bal_lo;           // Absorb_grid2: ballistic below this cell index (:642-644)
+  int bal_hx, bal_hy, bal_hz;  // N + 4 - Absorb_grid2: ballistic above (:645-647)
+  int pjx, pjy, pjz, pn;       // deposit planes of this species
+};
+
+// cal_track4 (:2804-2870) velocity update; returns the new velocity in v.
+template <typename real>
+__device__ __forceinline__ void boris4(const PushConst<real>& pc, Gathered<real> e, real& vx,
+                                       real& vy, real& vz) {
+  const real T = pc.T, C = pc.C;
+  e.ex += pc.ex_add;
+  e.ey += pc.ey_add;
+  real g1 = C / sqrt(pc.C2 - vx * vx - vy * vy - vz * vz);
+  if (isnan(g1)) g1 = (real)0;
+  real ux = g1 * vx, uy = g1 * vy, uz = g1 * vz;
+  real g2 = C / sqrt(pc.C2 + ux * ux + uy * uy + uz * uz);
+  const real bux = g2 * e.bx, buy = g2 * e.by, buz = g2 * e.bz;
+  const real S = (real)2 * T / ((real)1 + T * T * (bux * bux + buy * buy + buz * buz));
+  ux += e.ex * T;
+  uy += e.ey * T;
+  uz += e.ez * T;
+  const real uox = ux + T * (uy * buz - uz * buy);
+  const real uoy = uy + T * (uz * bux - ux * buz);
+  const real uoz = uz + T * (ux * buy - uy * bux);
+  real upx = ux + S * (uoy * buz - uoz * buy);
+  real upy = uy + S * (uoz * bux - uox * buz);
+  real upz = uz + S * (uox * buy - uoy * bux);
+  upx += e.ex * T;
+  upy += e.ey * T;
+  upz += e.ez * T;
+  g2 = C / sqrt(pc.C2 + upx * upx + upy * upy + upz * upz);
+  vx = g2 * upx;
+  vy = g2 * upy;
+  vz = g2 * upz;
+}
+
+// True when the particle lies outside the Absorb_grid2 box (fdtd :733-735):
+// x < ax0 or x > ax1 on any axis.
+template <typename real>
+__device__ __forceinline__ bool ballistic(const PushConst<real>& pc, int i, int j, int k, real fx,
+                                          real fy, real fz) {
+  return i < pc.bal_lo || j < pc.bal_lo || k < pc.bal_lo ||
+         i > pc.bal_hx || (i == pc.bal_hx && fx > (real)0) ||
+         j > pc.bal_hy || (j == pc.bal_hy && fy > (real)0) ||
+         k > pc.bal_hz || (k == pc.bal_hz && fz > (real)0);
+}
+
+// The 2x2x2 stencil of (i, j, k) lies in the padded array; the reference's
+// deposit condition 0 <= x < (N+4) dx (:747-749) also admits i = N+3, whose
+// stencil leaves the array, and such deposits are counted instead of made.
+__device__ __forceinline__ bool stencil_ok(const Geom& g, int i, int j, int k) {
+  return i >= 0 && j >= 0 && k >= 0 && i <= g.gx - 2 && j <= g.gy - 2 && k <= g.gz - 2;
+}
+__device__ __forceinline__ bool in_array(const Geom& g, int i, int j, int k) {
+  return i >= 0 && j >= 0 && k >= 0 && i < g.gx && j < g.gy && k < g.gz;
+}
+
+// shape_func_*0_j_2 (:3397-3553) at (i,f) with velocity v.
+template <typename real>
+__device__ __forceinline__ void deposit_j(const Fields<real>& F, const Geom& g,
+                                          const PushConst<real>& pc, const Axis<real>& X,
+                                          const Axis<real>& Y, const Axis<real>& Z, real vx,
+                                          real vy, real vz) {
+  const int sx = g.sx, sy = g.gz;
+  scatter8(F.f[pc.pjx], X.a * sx + Y.b * sy + Z.b, sx, sy, pc.qn * vx, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
+  scatter8(F.f[pc.pjy], X.b * sx + Y.a * sy + Z.b, sx, sy, pc.qn * vy, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
+  scatter8(F.f[pc.pjz], X.b * sx + Y.b * sy + Z.a, sx, sy, pc.qn * vz, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
+}
+
+// shape_func_*0_n_2 (:3333-3395): cell-centred density.
+template <typename real>
+__device__ __forceinline__ void deposit_n(const Fields<real>& F, const Geom& g,
+                                          const PushConst<real>& pc, const Axis<real>& X,
+                                          const Axis<real>& Y, const Axis<real>& Z) {
+  const int sx = g.sx, sy = g.gz;
+  scatter8(F.f[pc.pn], X.b * sx + Y.b * sy + Z.b, sx, sy, pc.nw, X.b0, X.b1, Y.b0, Y.b1, Z.b0, Z.b1);
+}
+
+__device__ __forceinline__ void count_err(unsigned long long* err, int id) {
+  atomicAdd(err + id, 1ull);
+}
+
+// Repacks (i,j,k) or marks the slot empty when the cell is not representable.
+__device__ __forceinline__ int repack(int i, int j, int k, unsigned long long* err) {
+  if (i < 0 || j < 0 || k < 0 || i >= kMaxDim || j >= kMaxDim || k >= kMaxDim) {
+    count_err(err, ERR_CELL_RANGE);
+    return -1;
+  }
+  return pack_cell(i, j, k);
+}
+
+// sr_particle at size 1 (:2058-2250): returns false when the particle is
+// removed; wraps x (then y) crossers by -N cells.
+__device__ __forceinline__ bool boundary(const Geom& g, int& i, int& j, int k) {
+  if (k < 2 || k >= g.nz + 2) return false;  // z outside [2dx, (Nz+2)dx)
+  if (i < 2) return false;                    // backward x packet dropped on rank 0
+  if (i >= g.nx + 2) i -= g.nx;               // forward x packet sent to itself
+  if (j < 2) return false;
+  if (j >= g.ny + 2) j -= g.ny;
+  return true;
+}
+
+enum PushMode { PUSH_J = 0, PUSH_FUSED = 1 };
+
+// The particle part of one fdtd iteration for one species.
+//  PUSH_J:     :731-812 only (push, J deposit at x^{n+1/2}).
+//  PUSH_FUSED: :731-812, then :818-867 (drift to x^{n+1}, density deposit) and
+//              sr_particle, in one pass over the particle arrays. Neither the
+//              drift, the density deposit nor the removal reads a field, so the
+//              second B half-step that the reference runs between them changes
+//              nothing they compute.
+template <typename real, int MODE>
+__global__ void __launch_bounds__(256) push_kernel(Parts<real> P, const int* __restrict__ count,
+                                                   Fields<real> F, Geom g, PushConst<real> pc,
+                                                   unsigned long long* err) {
+  const int n = *count;
+  unsigned pushed = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int c = P.cell[t];
+    if (c < 0) continue;
+    ++pushed;
+    int i, j, k;
+    unpack_cell(c, i, j, k);
+    real fx = P.o[0][t], fy = P.o[1][t], fz = P.o[2][t];
+    real vx = P.v[0][t], vy = P.v[1][t], vz = P.v[2][t];
+    bool bal = ballistic(pc, i, j, k, fx, fy, fz);
+    if (!bal && !stencil_ok(g, i, j, k)) {
+      count_err(err, ERR_DEPOSIT_OOB);
+      bal = true;
+    }
+    if (!bal) {
+      const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+      boris4(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
+      if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) count_err(err, ERR_NONFINITE);
+    }
+    advance(i, fx, vx * pc.hdt);
+    advance(j, fy, vy * pc.hdt);
+    advance(k, fz, vz * pc.hdt);
+    if (in_array(g, i, j, k)) {
+      if (stencil_ok(g, i, j, k)) {
+        const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+        deposit_j(F, g, pc, X, Y, Z, vx, vy, vz);
+      } else {
+        count_err(err, ERR_DEPOSIT_OOB);
+      }
+    }
+    int cell;
+    if (MODE == PUSH_FUSED) {
+      advance(i, fx, vx * pc.hdt);
+      advance(j, fy, vy * pc.hdt);
+      advance(k, fz, vz * pc.hdt);
+      if (in_array(g, i, j, k)) {
+        if (stencil_ok(g, i, j, k)) {
+          const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+          deposit_n(F, g, pc, X, Y, Z);
+        } else {
+          count_err(err, ERR_DEPOSIT_OOB);
+        }
+      }
+      cell = boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
+    } else {
+      cell = repack(i, j, k, err);
+    }
+    P.cell[t] = cell;
+    P.o[0][t] = fx; P.o[1][t] = fy; P.o[2][t] = fz;
+    P.v[0][t] = vx; P.v[1][t] = vy; P.v[2][t] = vz;
+  }
+  // particle pushes of this warp, one atomic per warp
+  for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
+  if ((threadIdx.x & 31) == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
+}
+
+// Drift to x^{n+1} and density deposit (fdtd :818-867).
+template <typename real>
+__global__ void __launch_bounds__(256) drift_n_kernel(Parts<real> P, const int* __restrict__ count,
+                                                      Fields<real> F, Geom g, PushConst<real> pc,
+                                                      unsigned long long* err) {
+  const int n = *count;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int c = P.cell[t];
+    if (c < 0) continue;
+    int i, j, k;
+    unpack_cell(c, i, j, k);
+    real fx = P.o[0][t], fy = P.o[1][t], fz = P.o[2][t];
+    const real vx = P.v[0][t], vy = P.v[1][t], vz = P.v[2][t];
+    advance(i, fx, vx * pc.hdt);
+    advance(j, fy, vy * pc.hdt);
+    advance(k, fz, vz * pc.hdt);
+    if (in_array(g, i, j, k)) {
+      if (stencil_ok(g, i, j, k)) {
+        const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+        deposit_n(F, g, pc, X, Y, Z);
+      } else {
+        count_err(err, ERR_DEPOSIT_OOB);
+      }
+    }
+    P.cell[t] = repack(i, j, k, err);
+    P.o[0][t] = fx; P.o[1][t] = fy; P.o[2][t] = fz;
+  }
+}
+
+// sr_particle at size 1 on its own.
+template <typename real>
+__global__ void sr_particle_kernel(Parts<real> P, const int* __restrict__ count, Geom g,
+                                   unsigned long long* err) {
+  const int n = *count;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int c = P.cell[t];
+    if (c < 0) continue;
+    int i, j, k;
+    unpack_cell(c, i, j, k);
+    P.cell[t] = boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
+  }
+}
+
+// Shell deletion of add_*_flat (:6015-6031) at size 1: x < 4dx or x > Nx dx,
+// the same in y and z.
+template <typename real>
+__global__ void delete_shell_kernel(Parts<real> P, const int* __restrict__ count, Geom g) {
+  const int n = *count;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int c = P.cell[t];
+    if (c < 0) continue;
+    int i, j, k;
+    unpack_cell(c, i, j, k);
+    bool del = i < 4 || j < 4 || k < 4 || i > g.nx || j > g.ny || k > g.nz;
+    if (!del && (i == g.nx || j == g.ny || k == g.nz)) {
+      del = (i == g.nx && P.o[0][t] > (real)0) || (j == g.ny && P.o[1][t] > (real)0) ||
+            (k == g.nz && P.o[2][t] > (real)0);
+    }
+    if (del) P.cell[t] = -1;
+  }
+}
+
+// --------------------------------------------------------------- sources
+// A refill slab of add_*_flat: cells [k0, k0+nk) x [l0, l0+nl) x [m0, m0+nm),
+// k outermost, Np particles per cell (the loop nest of :6047-6071).
+struct Slab {
+  int k0, nk, l0, nl, m0, nm;
+  long long first;  // index of the slab's first particle in the call's sequence
+};
+
+struct SourceParams {
+  int nslab;
+  Slab slab[5];
+  int np;
+  long long total;        // particles generated by this call
+  double dx;
+  double lsig;            // sqrt(sigma0^2): Cholesky factor of the covariance (:7943-7953)
+  double vdrift;          // mu[2] = V
+  uint64_t seed_p, seed_v;
+  long long base_p, base_v;  // first draw index on each stream
+  int dst;                // first slot written
+  int init_form;          // 1: cell bounds as init_particle_flat writes them, 2dx + k dx (:475)
+};
+
+// Positions: three gsl_ran_flat draws (x, y, z) on the position stream;
+// velocities: ran_multivar_gaussian = three Box-Muller normals (two draws
+// each) on the velocity stream, scaled by the Cholesky factor, plus mu.
+template <typename real>
+__global__ void source_kernel(Parts<real> P, SourceParams sp, unsigned long long* err) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= sp.total) return;
+  int s = 0;
+  while (s + 1 < sp.nslab && t >= sp.slab[s + 1].first) ++s;
+  const Slab& sl = sp.slab[s];
+  long long r = t - sl.first;
+  const int jj = (int)(r % sp.np);
+  r /= sp.np;
+  const int m = (int)(r % sl.nm);
+  r /= sl.nm;
+  const int l = (int)(r % sl.nl);
+  const int k = (int)(r / sl.nl);
+  (void)jj;
+  const double dx = sp.dx;
+  const uint64_t dp = (uint64_t)(sp.base_p + 3 * t);
+  double lo[3], hi[3];
+  const int cc[3] = {k + sl.k0, l + sl.l0, m + sl.m0};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (sp.init_form) {  // 2.*dx + k*dx with k counted from the first interior cell
+      lo[a] = __dadd_rn(__dmul_rn(2.0, dx), __dmul_rn((double)(cc[a] - 2), dx));
+      hi[a] = __dadd_rn(__dmul_rn(2.0, dx), __dmul_rn((double)(cc[a] - 1), dx));
+    } else {             // (k+2)*dx as add_*_flat writes it (:6049)
+      lo[a] = __dmul_rn((double)cc[a], dx);
+      hi[a] = __dmul_rn((double)(cc[a] + 1), dx);
+    }
+  }
+  const double x = flat_rn(lo[0], hi[0], uniform53(sp.seed_p, dp));
+  const double y = flat_rn(lo[1], hi[1], uniform53(sp.seed_p, dp + 1));
+  const double z = flat_rn(lo[2], hi[2], uniform53(sp.seed_p, dp + 2));
+  const uint64_t dv = (uint64_t)(sp.base_v + 6 * t);
+  const double g0 = gauss_bm(sp.seed_v, dv), g1 = gauss_bm(sp.seed_v, dv + 2), g2 = gauss_bm(sp.seed_v, dv + 4);
+  const double vx = __dadd_rn(__dmul_rn(sp.lsig, g0), 0.0);
+  const double vy = __dadd_rn(__dmul_rn(sp.lsig, g1), 0.0);
+  const double vz = __dadd_rn(__dmul_rn(sp.lsig, g2), sp.vdrift);
+  int ci, cj, ck;
+  real fx, fy, fz;
+  split_coord<real>(x / dx, ci, fx);
+  split_coord<real>(y / dx, cj, fy);
+  split_coord<real>(z / dx, ck, fz);
+  const int dst = sp.dst + (int)t;
+  P.cell[dst] = repack(ci, cj, ck, err);
+  P.o[0][dst] = fx; P.o[1][dst] = fy; P.o[2][dst] = fz;
+  P.v[0][dst] = (real)vx; P.v[1][dst] = (real)vy; P.v[2][dst] = (real)vz;
+}
+
+// ------------------------------------------------------------------- sort
+// sorting (:7475-7590): counting sort by interior cell, (i, j, k) order with k
+// fastest; particles outside the interior are dropped as the reference does.
+__device__ __forceinline__ int interior_key(const Geom& g, int c) {
+  if (c < 0) return -1;
+  int i, j, k;
+  unpack_cell(c, i, j, k);
+  i -= 2; j -= 2; k -= 2;
+  if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) return -1;
+  return (i * g.ny + j) * g.nz + k;
+}
+
+// Adds one to counter[key] per lane, one atomic per distinct key in the warp;
+// returns the lane's rank among lanes with the same key plus the prior value.
+__device__ __forceinline__ int warp_aggregated_inc(int* counter, int key, bool active) {
+  const unsigned mask = __ballot_sync(0xffffffffu, active);
+  int base = 0;
+  if (active) {
+    const unsigned peers = __match_any_sync(mask, key);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    int old = 0;
+    if (lane == leader) old = atomicAdd(counter + key, __popc(peers));
+    old = __shfl_sync(peers, old, leader);
+    base = old + rank;
+  }
+  return base;
+}
+
+template <typename real>
+__global__ void sort_count_kernel(Parts<real> P, const int* __restrict__ count, Geom g, int* cnt) {
+  const int n = *count;
+  const int stride = gridDim.x * blockDim.x;
+  // every lane of a warp runs the same number of iterations (warp-collective)
+  const int n_round = (n + 31) & ~31;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_round; t += stride) {
+    const int key = t < n ? interior_key(g, P.cell[t]) : -1;
+    warp_aggregated_inc(cnt, key < 0 ? 0 : key, key >= 0);
+  }
+}
+
+template <typename real>
+__global__ void sort_scatter_kernel(Parts<real> P, const int* __restrict__ count, Geom g,
+                                    const int* __restrict__ offs, int* cursor, Parts<real> Q) {
+  const int n = *count;
+  const int stride = gridDim.x * blockDim.x;
+  const int n_round = (n + 31) & ~31;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_round; t += stride) {
+    const int key = t < n ? interior_key(g, P.cell[t]) : -1;
+    const int r = warp_aggregated_inc(cursor, key < 0 ? 0 : key, key >= 0);
+    if (key >= 0) {
+      const int d = offs[key] + r;
+      Q.cell[d] = P.cell[t];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        Q.o[a][d] = P.o[a][t];
+        Q.v[a][d] = P.v[a][t];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------- scan (exclusive)
+// Block-wise exclusive scan of in[0..n) (4 items per thread, 1024 threads),
+// block totals to sums[]; a second level scans the totals.
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__global__ void __launch_bounds__(kScanThreads) scan_tile_kernel(const int* __restrict__ in, int* out,
+                                                                 int* sums, long long n) {
+  __shared__ int warp_tot[32];
+  const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int s = 0;
+#pragma unroll
+  for (int q = 0; q < kScanItems; ++q) {
+    v[q] = (base + q < n) ? in[base + q] : 0;
+    s += v[q];
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_tot[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int w = warp_tot[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    warp_tot[lane] = w;
+  }
+  __syncthreads();
+  int run = incl - s + (wid > 0 ? warp_tot[wid - 1] : 0);
+#pragma unroll
+  for (int q = 0; q < kScanItems; ++q) {
+    if (base + q < n) out[base + q] = run;
+    run += v[q];
+  }
+  if (threadIdx.x == kScanThreads - 1) sums[blockIdx.x] = run;
+}
+
+__global__ void scan_add_kernel(int* out, const int* __restrict__ add, long long n) {
+  const long long base = (long long)blockIdx.x * kScanTile;
+  const int a = add[blockIdx.x];
+  for (int q = threadIdx.x; q < kScanTile; q += blockDim.x) {
+    if (base + q < n) out[base + q] += a;
+  }
+}
+
+// -------------------------------------------------------- import / export
+// Device-side compaction of live slots for export: flags -> scan -> rows.
+template <typename real>
+__global__ void live_flag_kernel(const int* __restrict__ cell, int n, int* flag) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) flag[t] = cell[t] >= 0 ? 1 : 0;
+}
+
+template <typename real>
+__global__ void export_rows_kernel(Parts<real> P, int n, const int* __restrict__ pos, double dx,
+                                   double weight, double* rows) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int c = P.cell[t];
+  if (c < 0) return;
+  int i, j, k;
+  unpack_cell(c, i, j, k);
+  double* r = rows + 7 * (long long)pos[t];
+  r[0] = ((double)i + (double)P.o[0][t]) * dx;
+  r[1] = ((double)j + (double)P.o[1][t]) * dx;
+  r[2] = ((double)k + (double)P.o[2][t]) * dx;
+  r[3] = (double)P.v[0][t];
+  r[4] = (double)P.v[1][t];
+  r[5] = (double)P.v[2][t];
+  r[6] = weight;
+}
+
+template <typename real>
+__global__ void import_rows_kernel(Parts<real> P, int n, const double* __restrict__ rows,
+                                   double dx, unsigned long long* err) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double* r = rows + 7 * (long long)t;
+  int i, j, k;
+  real fx, fy, fz;
+  split_coord<real>(r[0] / dx, i, fx);
+  split_coord<real>(r[1] / dx, j, fy);
+  split_coord<real>(r[2] / dx, k, fz);
+  P.cell[t] = repack(i, j, k, err);
+  P.o[0][t] = fx; P.o[1][t] = fy; P.o[2][t] = fz;
+  P.v[0][t] = (real)r[3]; P.v[1][t] = (real)r[4]; P.v[2][t] = (real)r[5];
+}
+
+}  // namespace pb
