@@ -32,7 +32,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)
+    build_driver()
     return LIB
+
+
+DRIVER = os.path.join(HERE, "pic3d_main")
+
+
+def build_driver() -> str:
+    """The C host driver (plasmasim_b200/driver/pic3d_main.c) linked to the library."""
+    cmd = ["gcc", "-std=gnu11", "-O2", os.path.join(HERE, "driver", "pic3d_main.c"),
+           "-I", os.path.join(ROOT, "include"), "-L", HERE, "-lplasmab200",
+           f"-Wl,-rpath,{HERE}", "-Wl,-rpath,$ORIGIN", "-lm", "-o", DRIVER]
+    subprocess.run(cmd, check=True)
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -14,6 +14,7 @@
 #include "diag.cuh"
 #include "fields.cuh"
 #include "particles.cuh"
+#include "tiled.cuh"
 
 using namespace pb;
 
@@ -43,6 +44,12 @@ struct pic_ctx {
   double* ramps = nullptr;  // rx[2gx], ry[2gy], rz[2gz]
   Store sp[2];
   // sort and scan scratch
+  TileGeom tg{};
+  int* goff[2] = {nullptr, nullptr};  // tiled layout of each species
+  int* gmax[2] = {nullptr, nullptr};
+  int* gcap = nullptr;
+  int* total_dev = nullptr;
+  bool tiled[2] = {false, false};     // slots hold the layout of the last sort
   int* cnt = nullptr;
   int* offs = nullptr;
   int* cursor = nullptr;
@@ -150,6 +157,7 @@ int particle_blocks(long long n) {
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
 
 int set_count(pic_ctx* c, int s, long long n) {
+  if (n != c->sp[s].count) c->tiled[s] = false;  // appended or imported slots break the layout
   c->sp[s].count = n;
   set_int_kernel<<<1, 1, 0, c->stream>>>(c->sp[s].count_dev, (int)n);
   CKL();
@@ -236,8 +244,11 @@ int do_renew_b(pic_ctx* c) {
   const long long nint = (long long)c->g.nx * c->g.ny * c->g.nz;
   renew_b_kernel<real><<<grid_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, ramps(c), p);
   CKL();
-  static const int ids[6] = {F_BX, F_BY, F_BZ, F_DBX, F_DBY, F_DBZ};
-  return wrap_planes<real>(c, ids, 6);
+  wrap_b_x_kernel<real><<<grid_blocks((long long)c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(fields<real>(c), c->g);
+  CKL();
+  wrap_b_y_kernel<real><<<grid_blocks((long long)c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(fields<real>(c), c->g);
+  CKL();
+  return PIC_OK;
 }
 
 template <typename real>
@@ -280,6 +291,25 @@ int do_push(pic_ctx* c, int s) {
   return PIC_OK;
 }
 
+constexpr int kWinNodes = (kTileX + 4) * (kTileY + 4) * kWinZ;
+
+template <typename real>
+int do_push_tiled(pic_ctx* c, int s) {
+  if (!c->tiled[s]) return do_push<real, PUSH_FUSED>(c, s);
+  const int ntiles = c->tg.ntx * c->tg.nty * c->tg.ntz;
+  TileArgs ta{c->tg, c->goff[s], c->gmax[s]};
+  const size_t smem = 4 * kWinNodes * sizeof(real);
+  const bool vec = sizeof(real) == 4 && c->g.gz % 4 == 0;
+  if (vec)
+    push_tiled_kernel<real, true><<<ntiles, kTileX * kTileY * 32, smem, c->stream>>>(
+        parts<real>(c, s), ta, fields<real>(c), c->g, push_const<real>(c, s), c->err);
+  else
+    push_tiled_kernel<real, false><<<ntiles, kTileX * kTileY * 32, smem, c->stream>>>(
+        parts<real>(c, s), ta, fields<real>(c), c->g, push_const<real>(c, s), c->err);
+  CKL();
+  return PIC_OK;
+}
+
 template <typename real>
 int do_drift_n(pic_ctx* c, int s) {
   if (c->sp[s].count == 0) return PIC_OK;
@@ -318,26 +348,44 @@ __global__ void sort_total_kernel(const int* offs, const int* cnt, long long n, 
   *count_dev = offs[n - 1] + cnt[n - 1];
 }
 
+// sorting (:7475-7590) into the tiled layout of tiled.cuh: count particles per
+// interior cell, size every group by its fullest lane, scan the group sizes,
+// then scatter each particle to slot goff + 32 rank + lane. Particles outside
+// the interior are dropped, as the reference's sort drops them.
 template <typename real>
 int do_sort_species(pic_ctx* c, int s) {
   Store& st = c->sp[s];
-  if (st.count == 0) return PIC_OK;
+  const TileGeom& tg = c->tg;
+  int* goff = c->goff[s];
+  int* gmax = c->gmax[s];
   CK(cudaMemsetAsync(c->cnt, 0, sizeof(int) * c->ncells, c->stream));
   CK(cudaMemsetAsync(c->cursor, 0, sizeof(int) * c->ncells, c->stream));
   const int blocks = particle_blocks(st.count);
-  sort_count_kernel<real><<<blocks, kThreads, 0, c->stream>>>(parts<real>(c, s), st.count_dev, c->g, c->cnt);
+  if (st.count > 0) {
+    sort_count_kernel<real><<<blocks, kThreads, 0, c->stream>>>(parts<real>(c, s), st.count_dev, c->g, c->cnt);
+    CKL();
+  }
+  const int gblocks = grid_blocks((long long)tg.ngroups * 32);
+  group_size_kernel<<<gblocks, kThreads, 0, c->stream>>>(c->g, tg, c->cnt, gmax, c->gcap);
   CKL();
-  CKR(scan_exclusive(c, c->cnt, c->offs, c->ncells, c->scan_tmp, c->scan_tmp_len));
-  sort_scatter_kernel<real><<<blocks, kThreads, 0, c->stream>>>(parts<real>(c, s), st.count_dev, c->g, c->offs,
-                                                               c->cursor, parts<real>(c, s, 1 - st.cur));
-  CKL();
-  sort_total_kernel<<<1, 1, 0, c->stream>>>(c->offs, c->cnt, c->ncells, st.count_dev);
+  CKR(scan_exclusive(c, c->gcap, goff, tg.ngroups, c->scan_tmp, c->scan_tmp_len));
+  tiled_total_kernel<<<1, 1, 0, c->stream>>>(goff, c->gcap, tg.ngroups, c->total_dev);
   CKL();
   int total = 0;
-  CK(cudaMemcpyAsync(&total, st.count_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&total, c->total_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (total > st.cap) return PIC_ERR_CAPACITY;
+  Parts<real> Q = parts<real>(c, s, 1 - st.cur);
+  group_pad_kernel<<<gblocks, kThreads, 0, c->stream>>>(c->g, tg, c->cnt, goff, gmax, Q.cell);
+  CKL();
+  if (st.count > 0) {
+    tiled_scatter_kernel<real><<<blocks, kThreads, 0, c->stream>>>(parts<real>(c, s), st.count_dev, c->g, tg,
+                                                                   goff, c->cursor, Q);
+    CKL();
+  }
   st.cur = 1 - st.cur;
-  st.count = total;
+  CKR(set_count(c, s, total));
+  c->tiled[s] = true;
   return PIC_OK;
 }
 
@@ -412,6 +460,7 @@ int do_init_particles(pic_ctx* c) {
   c->ctr_v = 0;
   for (int s = 0; s < 2; ++s) {
     CKR(set_count(c, s, 0));
+    c->tiled[s] = false;
     const Slab body = {2, c->cfg.nx, 2, c->cfg.ny, 2, c->cfg.nz, 0};
     const Slab extra_cell = {2 + c->cfg.nx, 1, 2, 1, 2, 1, 0};
     CKR(do_source<real>(c, s, &body, 1, 1));
@@ -522,8 +571,14 @@ int do_step(pic_ctx* c) {
   CKR(phase_mark(c, PH_FIELD));
   CKR(do_renew_b<real>(c));
   CKR(phase_mark(c, PH_FIELD));
+  if (!c->tiled[0] || !c->tiled[1]) {  // after a refill or an import
+    CKR(phase_mark(c, PH_SORT));
+    for (int s = 0; s < 2; ++s)
+      if (!c->tiled[s]) CKR(do_sort_species<real>(c, s));
+    CKR(phase_mark(c, PH_SORT));
+  }
   CKR(phase_mark(c, PH_PUSH));
-  for (int s = 0; s < 2; ++s) CKR((do_push<real, PUSH_FUSED>(c, s)));
+  for (int s = 0; s < 2; ++s) CKR(do_push_tiled<real>(c, s));
   CKR(phase_mark(c, PH_PUSH));
   CKR(phase_mark(c, PH_FIELD));
   CKR(do_renew_b<real>(c));
@@ -615,6 +670,7 @@ int do_import(pic_ctx* c, int s, const double* rows, long long n) {
     CKL();
   }
   CKR(set_count(c, s, n));
+  c->tiled[s] = false;
   CK(cudaStreamSynchronize(c->stream));
   return PIC_OK;
 }
@@ -791,6 +847,23 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
   if (cudaMalloc(&c->cursor, sizeof(int) * c->ncells) != cudaSuccess) return fail(PIC_ERR_CUDA);
   c->scan_tmp_len = (size_t)(c->ncells / kScanTile) * 2 + 64;
   if (cudaMalloc(&c->scan_tmp, sizeof(int) * c->scan_tmp_len) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  {
+    TileGeom& t = c->tg;
+    t.ntx = (k.nx + kTileX - 1) / kTileX;
+    t.nty = (k.ny + kTileY - 1) / kTileY;
+    t.ntz = (k.nz + kLanes - 1) / kLanes;
+    t.ngroups = t.ntx * t.nty * t.ntz * kTileX * kTileY;
+    for (int s = 0; s < 2; ++s) {
+      if (cudaMalloc(&c->goff[s], sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
+      if (cudaMalloc(&c->gmax[s], sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    }
+    if (cudaMalloc(&c->gcap, sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    if (cudaMalloc(&c->total_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    const int smem64 = 4 * kWinNodes * (int)sizeof(double);
+    if (cudaFuncSetAttribute(push_tiled_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem64) != cudaSuccess)
+      return fail(PIC_ERR_CUDA);
+  }
   if (cudaMalloc(&c->acc, sizeof(double) * 64) != cudaSuccess) return fail(PIC_ERR_CUDA);
   if (cudaMalloc(&c->maxbits, sizeof(unsigned long long)) != cudaSuccess) return fail(PIC_ERR_CUDA);
   if (cudaMalloc(&c->fave, sizeof(double) * 27) != cudaSuccess) return fail(PIC_ERR_CUDA);
@@ -815,6 +888,12 @@ int pic_destroy(pic_ctx* c) {
     cudaFree(c->sp[s].mem[1]);
     cudaFree(c->sp[s].count_dev);
   }
+  for (int s = 0; s < 2; ++s) {
+    cudaFree(c->goff[s]);
+    cudaFree(c->gmax[s]);
+  }
+  cudaFree(c->gcap);
+  cudaFree(c->total_dev);
   cudaFree(c->cnt);
   cudaFree(c->offs);
   cudaFree(c->cursor);

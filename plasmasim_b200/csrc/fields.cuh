@@ -211,6 +211,57 @@ __global__ void wrap_y_kernel(PlaneSet<real> s, Geom g) {
   }
 }
 
+// sr_b at size 1 on the total field (:1016-1190): the ghost planes of B get the
+// periodic images of B, while B0 keeps its own (non-periodic) dipole values, so
+// the induced field there is B_image - B0_ghost, which the E update then sees.
+template <typename real>
+__global__ void wrap_b_x_kernel(Fields<real> F, Geom g) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.gy * g.gz) return;
+  const int N = g.nx, sx = g.sx;
+  const int dst[4] = {t, sx + t, (N + 2) * sx + t, (N + 3) * sx + t};
+  const int src[4] = {N * sx + t, (N + 1) * sx + t, 2 * sx + t, 3 * sx + t};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    real* b = F.f[F_BX + q];
+    real* db = F.f[F_DBX + q];
+    const real* b0 = F.f[F_B0X + q];
+    real v[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) v[r] = b[src[r]];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      b[dst[r]] = v[r];
+      db[dst[r]] = v[r] - b0[dst[r]];
+    }
+  }
+}
+
+template <typename real>
+__global__ void wrap_b_y_kernel(Fields<real> F, Geom g) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.gx * g.gz) return;
+  const int k = t / g.gz, m = t % g.gz;
+  const int N = g.ny, sy = g.gz;
+  const int base = k * g.sx + m;
+  const int dst[4] = {base, base + sy, base + (N + 2) * sy, base + (N + 3) * sy};
+  const int src[4] = {base + N * sy, base + (N + 1) * sy, base + 2 * sy, base + 3 * sy};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    real* b = F.f[F_BX + q];
+    real* db = F.f[F_DBX + q];
+    const real* b0 = F.f[F_B0X + q];
+    real v[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) v[r] = b[src[r]];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      b[dst[r]] = v[r];
+      db[dst[r]] = v[r] - b0[dst[r]];
+    }
+  }
+}
+
 // sr_current2 at size 1, x pass (:1815-1935): planes 2,3 += N+2, N+3 and
 // N, N+1 += 0, 1 (sources are ghosts, targets interior: disjoint for N >= 2).
 template <typename real>
