@@ -250,7 +250,13 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--grid", type=int, default=128,
+                    help="cells per axis (128 for the benchmark; smaller cases for profiling)")
+    ap.add_argument("--ppc", type=int, default=64, help="particles per cell per species")
     args = ap.parse_args()
+    global NX, NY, NZ, PPC
+    NX = NY = NZ = args.grid
+    PPC = args.ppc
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
