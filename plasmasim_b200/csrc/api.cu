@@ -45,11 +45,15 @@ struct pic_ctx {
   Store sp[2];
   // sort and scan scratch
   TileGeom tg{};
-  int* goff[2] = {nullptr, nullptr};  // tiled layout of each species
-  int* gmax[2] = {nullptr, nullptr};
+  // tiled layout of each species, double-buffered (the sort reads the old one)
+  int* goff[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int* gmax[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int lay[2] = {0, 0};                // current layout buffer
+  bool layout[2] = {false, false};    // slots [0, tiled_end) follow goff/gmax[lay]
+  long long tiled_end[2] = {0, 0};
+  bool tiled[2] = {false, false};     // layout holds every slot: the tiled push may run
   int* gcap = nullptr;
   int* total_dev = nullptr;
-  bool tiled[2] = {false, false};     // slots hold the layout of the last sort
   int* cnt = nullptr;
   int* offs = nullptr;
   int* cursor = nullptr;
@@ -297,7 +301,7 @@ template <typename real>
 int do_push_tiled(pic_ctx* c, int s) {
   if (!c->tiled[s]) return do_push<real, PUSH_FUSED>(c, s);
   const int ntiles = c->tg.ntx * c->tg.nty * c->tg.ntz;
-  TileArgs ta{c->tg, c->goff[s], c->gmax[s]};
+  TileArgs ta{c->tg, c->goff[s][c->lay[s]], c->gmax[s][c->lay[s]]};
   const size_t smem = 4 * kWinNodes * sizeof(real);
   const bool vec = sizeof(real) == 4 && c->g.gz % 4 == 0;
   if (vec)
@@ -348,43 +352,64 @@ __global__ void sort_total_kernel(const int* offs, const int* cnt, long long n, 
   *count_dev = offs[n - 1] + cnt[n - 1];
 }
 
-// sorting (:7475-7590) into the tiled layout of tiled.cuh: count particles per
-// interior cell, size every group by its fullest lane, scan the group sizes,
-// then scatter each particle to slot goff + 32 rank + lane. Particles outside
-// the interior are dropped, as the reference's sort drops them.
+// sorting (:7475-7590) into the tiled layout of tiled.cuh: count the
+// particles of every interior cell (stayers of the previous layout per lane
+// column, movers and appended particles per destination cell), size every
+// group by its fullest lane, scan the group sizes, then write stayers in their
+// previous column order and movers after them. Particles outside the interior
+// are dropped, as the reference's sort drops them.
 template <typename real>
 int do_sort_species(pic_ctx* c, int s) {
   Store& st = c->sp[s];
   const TileGeom& tg = c->tg;
-  int* goff = c->goff[s];
-  int* gmax = c->gmax[s];
-  CK(cudaMemsetAsync(c->cnt, 0, sizeof(int) * c->ncells, c->stream));
+  const int old = c->lay[s], nw = 1 - old;
+  const bool have = c->layout[s];
+  const long long first = have ? c->tiled_end[s] : 0;   // slots outside the old layout
+  int* stay = c->cnt;
+  int* moved = c->offs;
+  CK(cudaMemsetAsync(stay, 0, sizeof(int) * c->ncells, c->stream));
+  CK(cudaMemsetAsync(moved, 0, sizeof(int) * c->ncells, c->stream));
   CK(cudaMemsetAsync(c->cursor, 0, sizeof(int) * c->ncells, c->stream));
-  const int blocks = particle_blocks(st.count);
-  if (st.count > 0) {
-    sort_count_kernel<real><<<blocks, kThreads, 0, c->stream>>>(parts<real>(c, s), st.count_dev, c->g, c->cnt);
+  const int gblocks = grid_blocks((long long)tg.ngroups * 32);
+  const Parts<real> P = parts<real>(c, s);
+  if (have) {
+    tiled_count_kernel<real><<<gblocks, kThreads, 0, c->stream>>>(P, c->g, tg, c->goff[s][old], c->gmax[s][old],
+                                                                  stay, moved);
     CKL();
   }
-  const int gblocks = grid_blocks((long long)tg.ngroups * 32);
-  group_size_kernel<<<gblocks, kThreads, 0, c->stream>>>(c->g, tg, c->cnt, gmax, c->gcap);
+  if (st.count > first) {
+    append_count_kernel<real><<<particle_blocks(st.count - first), kThreads, 0, c->stream>>>(
+        P, (int)first, st.count_dev, c->g, moved);
+    CKL();
+  }
+  group_size_kernel<<<gblocks, kThreads, 0, c->stream>>>(c->g, tg, stay, moved, c->gmax[s][nw], c->gcap);
   CKL();
-  CKR(scan_exclusive(c, c->gcap, goff, tg.ngroups, c->scan_tmp, c->scan_tmp_len));
-  tiled_total_kernel<<<1, 1, 0, c->stream>>>(goff, c->gcap, tg.ngroups, c->total_dev);
+  CKR(scan_exclusive(c, c->gcap, c->goff[s][nw], tg.ngroups, c->scan_tmp, c->scan_tmp_len));
+  tiled_total_kernel<<<1, 1, 0, c->stream>>>(c->goff[s][nw], c->gcap, tg.ngroups, c->total_dev);
   CKL();
   int total = 0;
   CK(cudaMemcpyAsync(&total, c->total_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (total > st.cap) return PIC_ERR_CAPACITY;
   Parts<real> Q = parts<real>(c, s, 1 - st.cur);
-  group_pad_kernel<<<gblocks, kThreads, 0, c->stream>>>(c->g, tg, c->cnt, goff, gmax, Q.cell);
+  group_pad_kernel<<<gblocks, kThreads, 0, c->stream>>>(c->g, tg, stay, moved, c->goff[s][nw], c->gmax[s][nw],
+                                                        Q.cell);
   CKL();
-  if (st.count > 0) {
-    tiled_scatter_kernel<real><<<blocks, kThreads, 0, c->stream>>>(parts<real>(c, s), st.count_dev, c->g, tg,
-                                                                   goff, c->cursor, Q);
+  if (have) {
+    tiled_scatter_kernel<real><<<gblocks, kThreads, 0, c->stream>>>(
+        P, c->g, tg, c->goff[s][old], c->gmax[s][old], c->goff[s][nw], stay, c->cursor, Q);
+    CKL();
+  }
+  if (st.count > first) {
+    append_scatter_kernel<real><<<particle_blocks(st.count - first), kThreads, 0, c->stream>>>(
+        P, (int)first, st.count_dev, c->g, tg, c->goff[s][nw], stay, c->cursor, Q);
     CKL();
   }
   st.cur = 1 - st.cur;
+  c->lay[s] = nw;
   CKR(set_count(c, s, total));
+  c->layout[s] = true;
+  c->tiled_end[s] = total;
   c->tiled[s] = true;
   return PIC_OK;
 }
@@ -461,6 +486,7 @@ int do_init_particles(pic_ctx* c) {
   for (int s = 0; s < 2; ++s) {
     CKR(set_count(c, s, 0));
     c->tiled[s] = false;
+    c->layout[s] = false;
     const Slab body = {2, c->cfg.nx, 2, c->cfg.ny, 2, c->cfg.nz, 0};
     const Slab extra_cell = {2 + c->cfg.nx, 1, 2, 1, 2, 1, 0};
     CKR(do_source<real>(c, s, &body, 1, 1));
@@ -671,6 +697,7 @@ int do_import(pic_ctx* c, int s, const double* rows, long long n) {
   }
   CKR(set_count(c, s, n));
   c->tiled[s] = false;
+  c->layout[s] = false;
   CK(cudaStreamSynchronize(c->stream));
   return PIC_OK;
 }
@@ -854,8 +881,10 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
     t.ntz = (k.nz + kLanes - 1) / kLanes;
     t.ngroups = t.ntx * t.nty * t.ntz * kTileX * kTileY;
     for (int s = 0; s < 2; ++s) {
-      if (cudaMalloc(&c->goff[s], sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
-      if (cudaMalloc(&c->gmax[s], sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
+      for (int b = 0; b < 2; ++b) {
+        if (cudaMalloc(&c->goff[s][b], sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
+        if (cudaMalloc(&c->gmax[s][b], sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
+      }
     }
     if (cudaMalloc(&c->gcap, sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->total_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
@@ -889,8 +918,10 @@ int pic_destroy(pic_ctx* c) {
     cudaFree(c->sp[s].count_dev);
   }
   for (int s = 0; s < 2; ++s) {
-    cudaFree(c->goff[s]);
-    cudaFree(c->gmax[s]);
+    for (int b = 0; b < 2; ++b) {
+      cudaFree(c->goff[s][b]);
+      cudaFree(c->gmax[s][b]);
+    }
   }
   cudaFree(c->gcap);
   cudaFree(c->total_dev);

@@ -1,22 +1,29 @@
-// Tiled particle layout and the fused push kernel that uses it.
+// Tiled particle layout, its incremental sort, and the fused push kernel.
 //
 // Layout. The interior cells are cut into tiles of TX x TY x 32 cells (x, y,
 // z). Each (x, y) column of a tile -- 32 consecutive z cells -- is a "group"
-// handled by one warp, lane L owning cell z0 + L. A sort writes the particles
-// of a group interleaved: particle r of the cell in lane L goes to slot
-// goff[G] + 32 r + L, every lane's column padded with empty slots (cell = -1)
-// up to the group's largest cell count gmax[G]. A warp then reads 32
-// consecutive slots per step of its loop (one coalesced 128-byte line per
-// array) and its 32 lanes work on 32 different cells, so their shared-memory
-// deposits rarely hit the same address.
+// handled by one warp, lane L owning cell z0 + L (its "home" cell). A sort
+// writes the particles of a group interleaved: particle r of the cell in lane
+// L goes to slot goff[G] + 32 r + L, every lane's column padded with empty
+// slots (cell = -1) up to the group's largest cell count gmax[G]. A warp then
+// reads 32 consecutive slots per step of its loop (one coalesced 128-byte line
+// per array) and its 32 lanes work on 32 different cells.
 //
-// Deposit. Each CTA accumulates J and n of its species in a shared-memory
-// window of (TX+4) x (TY+4) x 36 nodes around its tile (the stencil of a
-// particle that has moved up to one cell from its tile since the sort), then
-// adds the window to the global planes with one vector reduction per 4 nodes.
-// Deposits whose stencil leaves the window (particles wrapped through the
-// periodic boundary, or moved farther since the sort) go straight to global
-// memory with atomics.
+// Deposit. A lane accumulates the current and density of the particles that
+// are in its home cell in registers (the 2x3x3 / 3x2x3 / 3x3x2 / 3x3x3 nodes
+// such a particle can touch) and adds them to a shared-memory window of
+// (TX+4) x (TY+4) x 36 nodes once, after its last particle. Particles that
+// have left their home cell since the sort deposit into the window with
+// shared atomics, or, when their stencil leaves the window (periodic wrap,
+// long moves), into global memory with atomics. The window is added to the
+// global planes with one vector reduction per 4 nodes.
+//
+// Sort. Between sorts most particles stay in their cell. The sort keeps the
+// order of those "stayers" within their lane column (a warp walks its columns
+// row by row, so stayers are written in order without atomics, into nearly
+// the same 128-byte lines they came from) and places the others -- movers,
+// and particles appended by a refill -- after the stayers of their new cell
+// with per-cell atomic cursors.
 #pragma once
 
 #include "common.cuh"
@@ -52,17 +59,60 @@ __device__ __forceinline__ int group_of(const Geom& g, const TileGeom& t, int i,
   return tile * (kTileX * kTileY) + wx * kTileY + wy;
 }
 
-// One warp per group: gmax = largest cell count of its 32 lanes.
-__global__ void group_size_kernel(Geom g, TileGeom t, const int* __restrict__ cnt, int* gmax,
-                                  int* gcap) {
-  const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (G >= t.ngroups) return;
+// Interior cell key of group G's lane, or -1 when the lane has no cell.
+__device__ __forceinline__ int home_key(const Geom& g, const TileGeom& t, int G, int lane) {
   const int tile = G / (kTileX * kTileY), w = G % (kTileX * kTileY);
   const int tz = tile % t.ntz, ty = (tile / t.ntz) % t.nty, tx = tile / (t.ntz * t.nty);
   const int i = tx * kTileX + w / kTileY, j = ty * kTileY + w % kTileY, k = tz * kLanes + lane;
-  int c = 0;
-  if (i < g.nx && j < g.ny && k < g.nz) c = cnt[(i * g.ny + j) * g.nz + k];
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return -1;
+  return (i * g.ny + j) * g.nz + k;
+}
+
+// Group and lane of an interior cell key.
+__device__ __forceinline__ int group_of_key(const Geom& g, const TileGeom& t, int key, int& lane) {
+  const int k = key % g.nz, j = (key / g.nz) % g.ny, i = key / (g.nz * g.ny);
+  return group_of(g, t, i + 2, j + 2, k + 2, lane);
+}
+
+// --------------------------------------------------------------- sort
+// Counting: stayers per home cell (no atomics) over the tiled slots, movers
+// and appended particles per destination cell (atomics).
+template <typename real>
+__global__ void tiled_count_kernel(Parts<real> P, Geom g, TileGeom t, const int* __restrict__ goff,
+                                   const int* __restrict__ gmax, int* stay, int* moved) {
+  const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (G >= t.ngroups) return;
+  const int home = home_key(g, t, G, lane);
+  const int base = goff[G], m = gmax[G];
+  int nstay = 0;
+  for (int r = 0; r < m; ++r) {
+    const int key = interior_key(g, P.cell[base + r * kLanes + lane]);
+    if (key < 0) continue;
+    if (key == home) ++nstay;
+    else atomicAdd(moved + key, 1);
+  }
+  if (home >= 0) stay[home] = nstay;
+}
+
+template <typename real>
+__global__ void append_count_kernel(Parts<real> P, int first, const int* __restrict__ count, Geom g,
+                                    int* moved) {
+  const int n = *count;
+  for (int s = first + blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int key = interior_key(g, P.cell[s]);
+    if (key >= 0) atomicAdd(moved + key, 1);
+  }
+}
+
+// One warp per group: gmax = largest (stayers + movers) count of its 32 lanes.
+__global__ void group_size_kernel(Geom g, TileGeom t, const int* __restrict__ stay,
+                                  const int* __restrict__ moved, int* gmax, int* gcap) {
+  const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (G >= t.ngroups) return;
+  const int home = home_key(g, t, G, lane);
+  int c = home >= 0 ? stay[home] + moved[home] : 0;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
   if (lane == 0) {
@@ -72,48 +122,71 @@ __global__ void group_size_kernel(Geom g, TileGeom t, const int* __restrict__ cn
 }
 
 // Marks the padding slots of every lane column empty.
-__global__ void group_pad_kernel(Geom g, TileGeom t, const int* __restrict__ cnt,
-                                 const int* __restrict__ goff, const int* __restrict__ gmax, int* cell) {
+__global__ void group_pad_kernel(Geom g, TileGeom t, const int* __restrict__ stay,
+                                 const int* __restrict__ moved, const int* __restrict__ goff,
+                                 const int* __restrict__ gmax, int* cell) {
   const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (G >= t.ngroups) return;
-  const int tile = G / (kTileX * kTileY), w = G % (kTileX * kTileY);
-  const int tz = tile % t.ntz, ty = (tile / t.ntz) % t.nty, tx = tile / (t.ntz * t.nty);
-  const int i = tx * kTileX + w / kTileY, j = ty * kTileY + w % kTileY, k = tz * kLanes + lane;
-  int c = 0;
-  if (i < g.nx && j < g.ny && k < g.nz) c = cnt[(i * g.ny + j) * g.nz + k];
+  const int home = home_key(g, t, G, lane);
+  const int c = home >= 0 ? stay[home] + moved[home] : 0;
   const int m = gmax[G], base = goff[G];
   for (int r = c; r < m; ++r) cell[base + r * kLanes + lane] = -1;
 }
 
 template <typename real>
-__global__ void tiled_scatter_kernel(Parts<real> P, const int* __restrict__ count, Geom g, TileGeom t,
-                                     const int* __restrict__ goff, int* cursor, Parts<real> Q) {
-  const int n = *count;
-  const int stride = gridDim.x * blockDim.x;
-  const int n_round = (n + 31) & ~31;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_round; s += stride) {
-    int key = -1, G = -1, lane = 0;
-    int c = -1;
-    if (s < n) {
-      c = P.cell[s];
-      key = interior_key(g, c);
-      if (key >= 0) {
-        int i, j, k;
-        unpack_cell(c, i, j, k);
-        G = group_of(g, t, i, j, k, lane);
-      }
-    }
-    const int r = warp_aggregated_inc(cursor, key < 0 ? 0 : key, key >= 0);
-    if (key >= 0) {
-      const int d = goff[G] + r * kLanes + lane;
-      Q.cell[d] = c;
+__device__ __forceinline__ void copy_particle(const Parts<real>& P, int s, const Parts<real>& Q, int d,
+                                              int c) {
+  Q.cell[d] = c;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        Q.o[a][d] = P.o[a][s];
-        Q.v[a][d] = P.v[a][s];
-      }
+  for (int a = 0; a < 3; ++a) {
+    Q.o[a][d] = P.o[a][s];
+    Q.v[a][d] = P.v[a][s];
+  }
+}
+
+// Scatter over the tiled slots: a stayer keeps its place in its column order;
+// a mover goes after the stayers of its new cell.
+template <typename real>
+__global__ void tiled_scatter_kernel(Parts<real> P, Geom g, TileGeom t, const int* __restrict__ goff_old,
+                                     const int* __restrict__ gmax_old, const int* __restrict__ goff_new,
+                                     const int* __restrict__ stay, int* cursor, Parts<real> Q) {
+  const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (G >= t.ngroups) return;
+  const int home = home_key(g, t, G, lane);
+  const int base = goff_old[G], m = gmax_old[G], nbase = goff_new[G];
+  int rnew = 0;
+  for (int r = 0; r < m; ++r) {
+    const int s = base + r * kLanes + lane;
+    const int c = P.cell[s];
+    const int key = interior_key(g, c);
+    if (key < 0) continue;
+    if (key == home) {
+      copy_particle(P, s, Q, nbase + rnew * kLanes + lane, c);
+      ++rnew;
+    } else {
+      int l2;
+      const int G2 = group_of_key(g, t, key, l2);
+      const int rank = stay[key] + atomicAdd(cursor + key, 1);
+      copy_particle(P, s, Q, goff_new[G2] + rank * kLanes + l2, c);
     }
+  }
+}
+
+template <typename real>
+__global__ void append_scatter_kernel(Parts<real> P, int first, const int* __restrict__ count, Geom g,
+                                      TileGeom t, const int* __restrict__ goff_new,
+                                      const int* __restrict__ stay, int* cursor, Parts<real> Q) {
+  const int n = *count;
+  for (int s = first + blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int c = P.cell[s];
+    const int key = interior_key(g, c);
+    if (key < 0) continue;
+    int l2;
+    const int G2 = group_of_key(g, t, key, l2);
+    const int rank = stay[key] + atomicAdd(cursor + key, 1);
+    copy_particle(P, s, Q, goff_new[G2] + rank * kLanes + l2, c);
   }
 }
 
@@ -152,11 +225,65 @@ __device__ __forceinline__ void scatter8_win(real* win, int wx0, int wy0, int wz
   }
 }
 
+// Half-shifted weights of a particle in its home cell h as a 3-vector over the
+// nodes h-1, h, h+1 (its base is h-1 for an offset below 1/2, h otherwise).
+template <typename real>
+struct W3 {
+  real w[3];
+};
+template <typename real>
+__device__ __forceinline__ W3<real> home3(const Axis<real>& A, int h) {
+  W3<real> r;
+  const bool up = A.b == h;
+  r.w[0] = up ? (real)0 : A.b0;
+  r.w[1] = up ? A.b0 : A.b1;
+  r.w[2] = up ? A.b1 : (real)0;
+  return r;
+}
+
+// cal_track4's square roots and divisions: exact in FP64, rsqrt/fast
+// reciprocal in FP32 (relative error ~1e-7, below the FP32 path's tolerance).
+__device__ __forceinline__ float c_over_sqrt(float c, float x) { return c * rsqrtf(x); }
+__device__ __forceinline__ double c_over_sqrt(double c, double x) { return c / sqrt(x); }
+__device__ __forceinline__ float quot(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double quot(double a, double b) { return a / b; }
+
+template <typename real>
+__device__ __forceinline__ void boris4_fast(const PushConst<real>& pc, Gathered<real> e, real& vx,
+                                            real& vy, real& vz) {
+  const real T = pc.T, C = pc.C;
+  e.ex += pc.ex_add;
+  e.ey += pc.ey_add;
+  real g1 = c_over_sqrt(C, pc.C2 - vx * vx - vy * vy - vz * vz);
+  if (isnan(g1)) g1 = (real)0;
+  real ux = g1 * vx, uy = g1 * vy, uz = g1 * vz;
+  real g2 = c_over_sqrt(C, pc.C2 + ux * ux + uy * uy + uz * uz);
+  const real bux = g2 * e.bx, buy = g2 * e.by, buz = g2 * e.bz;
+  const real S = quot((real)2 * T, (real)1 + T * T * (bux * bux + buy * buy + buz * buz));
+  ux += e.ex * T;
+  uy += e.ey * T;
+  uz += e.ez * T;
+  const real uox = ux + T * (uy * buz - uz * buy);
+  const real uoy = uy + T * (uz * bux - ux * buz);
+  const real uoz = uz + T * (ux * buy - uy * bux);
+  real upx = ux + S * (uoy * buz - uoz * buy);
+  real upy = uy + S * (uoz * bux - uox * buz);
+  real upz = uz + S * (uox * buy - uoy * bux);
+  upx += e.ex * T;
+  upy += e.ey * T;
+  upz += e.ez * T;
+  g2 = c_over_sqrt(C, pc.C2 + upx * upx + upy * upy + upz * upz);
+  vx = g2 * upx;
+  vy = g2 * upy;
+  vz = g2 * upz;
+}
+
 // The fused particle part of one step (push, J deposit at x^{n+1/2}, drift,
 // n deposit at x^{n+1}, sr_particle) for one species over the tiled layout;
-// same arithmetic as push_kernel<real, PUSH_FUSED>. One CTA per tile.
+// the same arithmetic as push_kernel<real, PUSH_FUSED> apart from the FP32
+// square roots and divisions. One CTA per tile.
 template <typename real, bool VEC_FLUSH>
-__global__ void __launch_bounds__(kTileX * kTileY * 32)
+__global__ void __launch_bounds__(kTileX * kTileY * 32, 2)
 push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc,
                   unsigned long long* err) {
   constexpr int WX = kTileX + 4, WY = kTileY + 4, WZ = kWinZ, WN = WX * WY * WZ;
@@ -172,10 +299,24 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int G = tile * (kTileX * kTileY) + warp;
   const int base = ta.goff[G], jmax = ta.gmax[G];
+  // home cell of this lane
+  const int hi = wx0 + 2 + warp / kTileY, hj = wy0 + 2 + warp % kTileY, hk = wz0 + 2 + lane;
   real* wjx = win;
   real* wjy = win + WN;
   real* wjz = win + 2 * WN;
   real* wn = win + 3 * WN;
+  real ajx[2][3][3], ajy[3][2][3], ajz[3][3][2], an[3][3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (a < 2) ajx[a][b][c] = (real)0;
+        if (b < 2) ajy[a][b][c] = (real)0;
+        if (c < 2) ajz[a][b][c] = (real)0;
+        an[a][b][c] = (real)0;
+      }
   unsigned pushed = 0;
   for (int jj = 0; jj < jmax; ++jj) {
     const int t = base + jj * kLanes + lane;
@@ -193,31 +334,73 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     }
     if (!bal) {
       const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-      boris4(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
+      boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
       if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) count_err(err, ERR_NONFINITE);
     }
     advance(i, fx, vx * pc.hdt);
     advance(j, fy, vy * pc.hdt);
     advance(k, fz, vz * pc.hdt);
-    if (in_array(g, i, j, k)) {
-      if (stencil_ok(g, i, j, k)) {
-        const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-        scatter8_win(wjx, wx0, wy0, wz0, F.f[pc.pjx], g, X.a, Y.b, Z.b, pc.qn * vx, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
-        scatter8_win(wjy, wx0, wy0, wz0, F.f[pc.pjy], g, X.b, Y.a, Z.b, pc.qn * vy, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
-        scatter8_win(wjz, wx0, wy0, wz0, F.f[pc.pjz], g, X.b, Y.b, Z.a, pc.qn * vz, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
-      } else {
-        count_err(err, ERR_DEPOSIT_OOB);
+    {  // J at x^{n+1/2}
+      const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+      if (i == hi && j == hj && k == hk) {
+        const W3<real> bx = home3(X, hi), by = home3(Y, hj), bz = home3(Z, hk);
+        const real ax[2] = {X.a0, X.a1}, ay[2] = {Y.a0, Y.a1}, az[2] = {Z.a0, Z.a1};
+        const real qx = pc.qn * vx, qy = pc.qn * vy, qz = pc.qn * vz;
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            const real yz = by.w[b] * bz.w[cc];
+            ajx[0][b][cc] += (qx * ax[0]) * yz;
+            ajx[1][b][cc] += (qx * ax[1]) * yz;
+          }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            const real xz = bx.w[a] * bz.w[cc];
+            ajy[a][0][cc] += (qy * ay[0]) * xz;
+            ajy[a][1][cc] += (qy * ay[1]) * xz;
+          }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            const real xy = bx.w[a] * by.w[b];
+            ajz[a][b][0] += (qz * az[0]) * xy;
+            ajz[a][b][1] += (qz * az[1]) * xy;
+          }
+      } else if (in_array(g, i, j, k)) {
+        if (stencil_ok(g, i, j, k)) {
+          scatter8_win(wjx, wx0, wy0, wz0, F.f[pc.pjx], g, X.a, Y.b, Z.b, pc.qn * vx, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
+          scatter8_win(wjy, wx0, wy0, wz0, F.f[pc.pjy], g, X.b, Y.a, Z.b, pc.qn * vy, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
+          scatter8_win(wjz, wx0, wy0, wz0, F.f[pc.pjz], g, X.b, Y.b, Z.a, pc.qn * vz, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
+        } else {
+          count_err(err, ERR_DEPOSIT_OOB);
+        }
       }
     }
     advance(i, fx, vx * pc.hdt);
     advance(j, fy, vy * pc.hdt);
     advance(k, fz, vz * pc.hdt);
-    if (in_array(g, i, j, k)) {
-      if (stencil_ok(g, i, j, k)) {
-        const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-        scatter8_win(wn, wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b, pc.nw, X.b0, X.b1, Y.b0, Y.b1, Z.b0, Z.b1);
-      } else {
-        count_err(err, ERR_DEPOSIT_OOB);
+    {  // n at x^{n+1}
+      const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+      if (i == hi && j == hj && k == hk) {
+        const W3<real> bx = home3(X, hi), by = home3(Y, hj), bz = home3(Z, hk);
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            const real yz = pc.nw * (by.w[b] * bz.w[cc]);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) an[a][b][cc] += bx.w[a] * yz;
+          }
+      } else if (in_array(g, i, j, k)) {
+        if (stencil_ok(g, i, j, k)) {
+          scatter8_win(wn, wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b, pc.nw, X.b0, X.b1, Y.b0, Y.b1, Z.b0, Z.b1);
+        } else {
+          count_err(err, ERR_DEPOSIT_OOB);
+        }
       }
     }
     P.cell[t] = boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
@@ -226,6 +409,22 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
   if (lane == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
+  // the lane's home-cell sums into the window (nodes h-1 .. h+1 around it)
+  if (jmax > 0) {
+    const int la = hi - 1 - wx0, lb = hj - 1 - wy0, lc = hk - 1 - wz0;  // window index of node h-1
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const int s = ((la + a) * WY + (lb + b)) * WZ + (lc + cc);
+          if (a < 2) atomicAdd(wjx + s + WY * WZ, ajx[a][b][cc]);  // x nodes h, h+1
+          if (b < 2) atomicAdd(wjy + s + WZ, ajy[a][b][cc]);       // y nodes h, h+1
+          if (cc < 2) atomicAdd(wjz + s + 1, ajz[a][b][cc]);       // z nodes h, h+1
+          atomicAdd(wn + s, an[a][b][cc]);
+        }
+  }
   __syncthreads();
   // flush the window: one reduction per 4 consecutive z nodes
   const int planes[4] = {pc.pjx, pc.pjy, pc.pjz, pc.pn};
