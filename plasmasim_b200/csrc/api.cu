@@ -15,6 +15,7 @@
 #include "fields.cuh"
 #include "particles.cuh"
 #include "tiled.cuh"
+#include "push_tiled.cuh"
 
 using namespace pb;
 
@@ -295,14 +296,12 @@ int do_push(pic_ctx* c, int s) {
   return PIC_OK;
 }
 
-constexpr int kWinNodes = (kTileX + 4) * (kTileY + 4) * kWinZ;
-
 template <typename real>
 int do_push_tiled(pic_ctx* c, int s) {
   if (!c->tiled[s]) return do_push<real, PUSH_FUSED>(c, s);
   const int ntiles = c->tg.ntx * c->tg.nty * c->tg.ntz;
   TileArgs ta{c->tg, c->goff[s][c->lay[s]], c->gmax[s][c->lay[s]]};
-  const size_t smem = 4 * kWinNodes * sizeof(real);
+  const size_t smem = PushSmem<real>::bytes;
   const bool vec = sizeof(real) == 4 && c->g.gz % 4 == 0;
   if (vec)
     push_tiled_kernel<real, true><<<ntiles, kTileX * kTileY * 32, smem, c->stream>>>(
@@ -888,9 +887,12 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
     }
     if (cudaMalloc(&c->gcap, sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->total_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
-    const int smem64 = 4 * kWinNodes * (int)sizeof(double);
     if (cudaFuncSetAttribute(push_tiled_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             smem64) != cudaSuccess)
+                             (int)PushSmem<double>::bytes) != cudaSuccess ||
+        cudaFuncSetAttribute(push_tiled_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)PushSmem<float>::bytes) != cudaSuccess ||
+        cudaFuncSetAttribute(push_tiled_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)PushSmem<float>::bytes) != cudaSuccess)
       return fail(PIC_ERR_CUDA);
   }
   if (cudaMalloc(&c->acc, sizeof(double) * 64) != cudaSuccess) return fail(PIC_ERR_CUDA);

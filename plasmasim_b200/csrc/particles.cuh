@@ -25,8 +25,9 @@ __device__ __forceinline__ Axis<real> axis_weights(int i, real f) {
   w.a = i;
   w.a1 = f;
   w.a0 = (real)1 - f;
-  w.b = (f >= (real)0.5 || i == 0) ? i : i - 1;
-  w.b1 = (real)(i - w.b) - (real)0.5 + f;
+  const bool up = f >= (real)0.5 || i == 0;
+  w.b = up ? i : i - 1;
+  w.b1 = up ? f - (real)0.5 : f + (real)0.5;
   w.b0 = (real)1 - w.b1;
   return w;
 }

@@ -1,0 +1,232 @@
+// The fused particle kernel over the tiled layout of tiled.cuh.
+#pragma once
+
+#include "common.cuh"
+#include "particles.cuh"
+#include "tiled.cuh"
+
+namespace pb {
+
+constexpr int kQueue = 64;  // per-warp queue of mover deposits (power of two)
+
+// Shared-memory plan of one CTA (8 warps): the J/n window, then per warp a
+// queue of J deposits of particles outside their home cell.
+template <typename real>
+struct PushSmem {
+  static constexpr int WX = kTileX + 4, WY = kTileY + 4, WZ = kWinZ, WN = WX * WY * WZ;
+  static constexpr int kWarps = kTileX * kTileY;
+  static constexpr size_t win_bytes = 4 * WN * sizeof(real);
+  static constexpr size_t qcell_off = (win_bytes + 15) & ~(size_t)15;
+  static constexpr size_t qdat_off = qcell_off + (size_t)kWarps * kQueue * sizeof(int);
+  static constexpr size_t bytes = qdat_off + (size_t)kWarps * kQueue * 6 * sizeof(real);
+};
+
+// Deposit of one queued J entry (a particle outside its home cell) into the
+// window, or into global memory when its stencil leaves the window.
+template <typename real>
+__device__ __forceinline__ void deposit_j_entry(real* win, int wx0, int wy0, int wz0, const Fields<real>& F,
+                                                const Geom& g, const PushConst<real>& pc, int cell,
+                                                const real* d) {
+  constexpr int WN = PushSmem<real>::WN;
+  int i, j, k;
+  unpack_cell(cell, i, j, k);
+  const Axis<real> X = axis_weights(i, d[0]), Y = axis_weights(j, d[1]), Z = axis_weights(k, d[2]);
+  scatter8_win(win, wx0, wy0, wz0, F.f[pc.pjx], g, X.a, Y.b, Z.b, d[3], X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
+  scatter8_win(win + WN, wx0, wy0, wz0, F.f[pc.pjy], g, X.b, Y.a, Z.b, d[4], X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
+  scatter8_win(win + 2 * WN, wx0, wy0, wz0, F.f[pc.pjz], g, X.b, Y.b, Z.a, d[5], X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
+}
+
+// The fused particle part of one step (push, J deposit at x^{n+1/2}, drift,
+// n deposit at x^{n+1}, sr_particle) for one species over the tiled layout;
+// the same arithmetic as push_kernel<real, PUSH_FUSED> apart from the FP32
+// square roots and divisions. One CTA per tile, one warp per group.
+//
+// J of a particle still in its lane's home cell is summed in registers; J of
+// the others is queued per warp and deposited 32 entries at a time, so that a
+// few such particles do not make the whole warp run the atomic path. The
+// density goes to the window with shared atomics (every active lane at once).
+template <typename real, bool VEC_FLUSH>
+__global__ void __launch_bounds__(kTileX * kTileY * 32, 2)
+push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc,
+                  unsigned long long* err) {
+  using S = PushSmem<real>;
+  constexpr int WY = S::WY, WZ = S::WZ, WN = S::WN, WX = S::WX;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  real* win = reinterpret_cast<real*>(smem_raw);  // [4][WN]: jx, jy, jz, n
+  const int tile = blockIdx.x;
+  const TileGeom& t = ta.t;
+  const int tz = tile % t.ntz, ty = (tile / t.ntz) % t.nty, tx = tile / (t.ntz * t.nty);
+  // window origin: two nodes below the tile's first interior cell (2 + tx*TX)
+  const int wx0 = tx * kTileX, wy0 = ty * kTileY, wz0 = tz * kLanes;
+  for (int q = threadIdx.x; q < 4 * WN; q += blockDim.x) win[q] = (real)0;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  int* qcell = reinterpret_cast<int*>(smem_raw + S::qcell_off) + warp * kQueue;
+  real* qdat = reinterpret_cast<real*>(smem_raw + S::qdat_off) + warp * kQueue * 6;
+  int qhead = 0, qtail = 0;  // warp-uniform queue counters
+  const int G = tile * (kTileX * kTileY) + warp;
+  const int base = ta.goff[G], jmax = ta.gmax[G];
+  // home cell of this lane
+  const int hi = wx0 + 2 + warp / kTileY, hj = wy0 + 2 + warp % kTileY, hk = wz0 + 2 + lane;
+  real* wn = win + 3 * WN;
+  real ajx[2][3][3], ajy[3][2][3], ajz[3][3][2];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (a < 2) ajx[a][b][c] = (real)0;
+        if (b < 2) ajy[a][b][c] = (real)0;
+        if (c < 2) ajz[a][b][c] = (real)0;
+      }
+  unsigned pushed = 0;
+  for (int jj = 0; jj < jmax; ++jj) {
+    const int t = base + jj * kLanes + lane;
+    const int c = P.cell[t];
+    const bool act = c >= 0;
+    int i = 0, j = 0, k = 0;
+    real fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
+    bool mover = false;
+    if (act) {
+      ++pushed;
+      unpack_cell(c, i, j, k);
+      fx = P.o[0][t]; fy = P.o[1][t]; fz = P.o[2][t];
+      vx = P.v[0][t]; vy = P.v[1][t]; vz = P.v[2][t];
+      bool bal = ballistic(pc, i, j, k, fx, fy, fz);
+      if (!bal && !stencil_ok(g, i, j, k)) {
+        count_err(err, ERR_DEPOSIT_OOB);
+        bal = true;
+      }
+      if (!bal) {
+        const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+        boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
+        if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) count_err(err, ERR_NONFINITE);
+      }
+      advance(i, fx, vx * pc.hdt);
+      advance(j, fy, vy * pc.hdt);
+      advance(k, fz, vz * pc.hdt);
+      // J at x^{n+1/2}
+      if (i == hi && j == hj && k == hk) {
+        const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+        const W3<real> bx = home3(X, hi), by = home3(Y, hj), bz = home3(Z, hk);
+        const real ax[2] = {X.a0, X.a1}, ay[2] = {Y.a0, Y.a1}, az[2] = {Z.a0, Z.a1};
+        const real qx = pc.qn * vx, qy = pc.qn * vy, qz = pc.qn * vz;
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            const real yz = by.w[b] * bz.w[cc];
+            ajx[0][b][cc] += (qx * ax[0]) * yz;
+            ajx[1][b][cc] += (qx * ax[1]) * yz;
+          }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            const real xz = bx.w[a] * bz.w[cc];
+            ajy[a][0][cc] += (qy * ay[0]) * xz;
+            ajy[a][1][cc] += (qy * ay[1]) * xz;
+          }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            const real xy = bx.w[a] * by.w[b];
+            ajz[a][b][0] += (qz * az[0]) * xy;
+            ajz[a][b][1] += (qz * az[1]) * xy;
+          }
+      } else if (in_array(g, i, j, k)) {
+        if (stencil_ok(g, i, j, k)) mover = true;
+        else count_err(err, ERR_DEPOSIT_OOB);
+      }
+    }
+    // queue the J deposits of movers; every lane takes part in the vote
+    const unsigned m = __ballot_sync(0xffffffffu, mover);
+    if (m) {
+      if (mover) {
+        const int p = (qtail + __popc(m & below)) & (kQueue - 1);
+        qcell[p] = pack_cell(i, j, k);
+        real* d = qdat + 6 * p;
+        d[0] = fx; d[1] = fy; d[2] = fz;
+        d[3] = pc.qn * vx; d[4] = pc.qn * vy; d[5] = pc.qn * vz;
+      }
+      qtail += __popc(m);
+      __syncwarp();
+      if (qtail - qhead >= kLanes) {
+        const int p = (qhead + lane) & (kQueue - 1);
+        deposit_j_entry(win, wx0, wy0, wz0, F, g, pc, qcell[p], qdat + 6 * p);
+        qhead += kLanes;
+        __syncwarp();
+      }
+    }
+    if (act) {
+      advance(i, fx, vx * pc.hdt);
+      advance(j, fy, vy * pc.hdt);
+      advance(k, fz, vz * pc.hdt);
+      // n at x^{n+1}
+      if (in_array(g, i, j, k)) {
+        if (stencil_ok(g, i, j, k)) {
+          const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+          scatter8_win(wn, wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b, pc.nw, X.b0, X.b1, Y.b0, Y.b1, Z.b0, Z.b1);
+        } else {
+          count_err(err, ERR_DEPOSIT_OOB);
+        }
+      }
+      P.cell[t] = boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
+      P.o[0][t] = fx; P.o[1][t] = fy; P.o[2][t] = fz;
+      P.v[0][t] = vx; P.v[1][t] = vy; P.v[2][t] = vz;
+    }
+  }
+  // the rest of the queue
+  if (qtail > qhead) {
+    if (lane < qtail - qhead) {
+      const int p = (qhead + lane) & (kQueue - 1);
+      deposit_j_entry(win, wx0, wy0, wz0, F, g, pc, qcell[p], qdat + 6 * p);
+    }
+    __syncwarp();
+  }
+  for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
+  if (lane == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
+  // the lane's home-cell sums into the window (nodes h-1 .. h+1 around it)
+  if (jmax > 0) {
+    const int la = hi - 1 - wx0, lb = hj - 1 - wy0, lc = hk - 1 - wz0;  // window index of node h-1
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const int s = ((la + a) * WY + (lb + b)) * WZ + (lc + cc);
+          if (a < 2) atomicAdd(win + s + WY * WZ, ajx[a][b][cc]);       // x nodes h, h+1
+          if (b < 2) atomicAdd(win + WN + s + WZ, ajy[a][b][cc]);       // y nodes h, h+1
+          if (cc < 2) atomicAdd(win + 2 * WN + s + 1, ajz[a][b][cc]);   // z nodes h, h+1
+        }
+  }
+  __syncthreads();
+  // flush the window: one reduction per 4 consecutive z nodes
+  const int planes[4] = {pc.pjx, pc.pjy, pc.pjz, pc.pn};
+  constexpr int NZ4 = WZ / 4;
+  for (int q4 = threadIdx.x; q4 < 4 * WX * WY * NZ4; q4 += blockDim.x) {
+    const int q = q4 / (WX * WY * NZ4);
+    const int r = q4 % (WX * WY * NZ4);
+    const int a = r / (WY * NZ4), b = (r / NZ4) % WY, c4 = r % NZ4;
+    const int ga = wx0 + a, gb = wy0 + b, gc = wz0 + 4 * c4;
+    if (ga >= g.gx || gb >= g.gy || gc >= g.gz) continue;
+    const real* src = win + q * WN + (a * WY + b) * WZ + 4 * c4;
+    const real v0 = src[0], v1 = src[1], v2 = src[2], v3 = src[3];
+    if (v0 == (real)0 && v1 == (real)0 && v2 == (real)0 && v3 == (real)0) continue;
+    real* dst = F.f[planes[q]] + ga * g.sx + gb * g.gz + gc;
+    if (VEC_FLUSH) {
+      red_add_v4(reinterpret_cast<float*>(dst), (float)v0, (float)v1, (float)v2, (float)v3);
+    } else {
+      const real v[4] = {v0, v1, v2, v3};
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (gc + e < g.gz && v[e] != (real)0) atomicAdd(dst + e, v[e]);
+    }
+  }
+}
+
+}  // namespace pb

@@ -1,4 +1,5 @@
-// Tiled particle layout, its incremental sort, and the fused push kernel.
+// Tiled particle layout and its incremental sort (the push kernel that uses
+// the layout is in push_tiled.cuh).
 //
 // Layout. The interior cells are cut into tiles of TX x TY x 32 cells (x, y,
 // z). Each (x, y) column of a tile -- 32 consecutive z cells -- is a "group"
@@ -9,13 +10,13 @@
 // reads 32 consecutive slots per step of its loop (one coalesced 128-byte line
 // per array) and its 32 lanes work on 32 different cells.
 //
-// Deposit. A lane accumulates the current and density of the particles that
-// are in its home cell in registers (the 2x3x3 / 3x2x3 / 3x3x2 / 3x3x3 nodes
-// such a particle can touch) and adds them to a shared-memory window of
-// (TX+4) x (TY+4) x 36 nodes once, after its last particle. Particles that
-// have left their home cell since the sort deposit into the window with
-// shared atomics, or, when their stencil leaves the window (periodic wrap,
-// long moves), into global memory with atomics. The window is added to the
+// Deposit. A lane accumulates the current of the particles that are in its
+// home cell in registers (the 2x3x3 / 3x2x3 / 3x3x2 nodes such a particle can
+// touch) and adds them to a shared-memory window of (TX+4) x (TY+4) x 36 nodes
+// once, after its last particle. The current of particles that have left
+// their home cell since the sort, and every density deposit, go to the window
+// with shared atomics, or, when the stencil leaves the window (periodic wrap,
+// long moves), to global memory with atomics. The window is added to the
 // global planes with one vector reduction per 4 nodes.
 //
 // Sort. Between sorts most particles stay in their cell. The sort keeps the
@@ -278,176 +279,5 @@ __device__ __forceinline__ void boris4_fast(const PushConst<real>& pc, Gathered<
   vz = g2 * upz;
 }
 
-// The fused particle part of one step (push, J deposit at x^{n+1/2}, drift,
-// n deposit at x^{n+1}, sr_particle) for one species over the tiled layout;
-// the same arithmetic as push_kernel<real, PUSH_FUSED> apart from the FP32
-// square roots and divisions. One CTA per tile.
-template <typename real, bool VEC_FLUSH>
-__global__ void __launch_bounds__(kTileX * kTileY * 32, 2)
-push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc,
-                  unsigned long long* err) {
-  constexpr int WX = kTileX + 4, WY = kTileY + 4, WZ = kWinZ, WN = WX * WY * WZ;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  real* win = reinterpret_cast<real*>(smem_raw);  // [4][WN]: jx, jy, jz, n
-  const int tile = blockIdx.x;
-  const TileGeom& t = ta.t;
-  const int tz = tile % t.ntz, ty = (tile / t.ntz) % t.nty, tx = tile / (t.ntz * t.nty);
-  // window origin: two nodes below the tile's first interior cell (2 + tx*TX)
-  const int wx0 = tx * kTileX, wy0 = ty * kTileY, wz0 = tz * kLanes;
-  for (int q = threadIdx.x; q < 4 * WN; q += blockDim.x) win[q] = (real)0;
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int G = tile * (kTileX * kTileY) + warp;
-  const int base = ta.goff[G], jmax = ta.gmax[G];
-  // home cell of this lane
-  const int hi = wx0 + 2 + warp / kTileY, hj = wy0 + 2 + warp % kTileY, hk = wz0 + 2 + lane;
-  real* wjx = win;
-  real* wjy = win + WN;
-  real* wjz = win + 2 * WN;
-  real* wn = win + 3 * WN;
-  real ajx[2][3][3], ajy[3][2][3], ajz[3][3][2], an[3][3][3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (a < 2) ajx[a][b][c] = (real)0;
-        if (b < 2) ajy[a][b][c] = (real)0;
-        if (c < 2) ajz[a][b][c] = (real)0;
-        an[a][b][c] = (real)0;
-      }
-  unsigned pushed = 0;
-  for (int jj = 0; jj < jmax; ++jj) {
-    const int t = base + jj * kLanes + lane;
-    const int c = P.cell[t];
-    if (c < 0) continue;
-    ++pushed;
-    int i, j, k;
-    unpack_cell(c, i, j, k);
-    real fx = P.o[0][t], fy = P.o[1][t], fz = P.o[2][t];
-    real vx = P.v[0][t], vy = P.v[1][t], vz = P.v[2][t];
-    bool bal = ballistic(pc, i, j, k, fx, fy, fz);
-    if (!bal && !stencil_ok(g, i, j, k)) {
-      count_err(err, ERR_DEPOSIT_OOB);
-      bal = true;
-    }
-    if (!bal) {
-      const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-      boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
-      if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) count_err(err, ERR_NONFINITE);
-    }
-    advance(i, fx, vx * pc.hdt);
-    advance(j, fy, vy * pc.hdt);
-    advance(k, fz, vz * pc.hdt);
-    {  // J at x^{n+1/2}
-      const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-      if (i == hi && j == hj && k == hk) {
-        const W3<real> bx = home3(X, hi), by = home3(Y, hj), bz = home3(Z, hk);
-        const real ax[2] = {X.a0, X.a1}, ay[2] = {Y.a0, Y.a1}, az[2] = {Z.a0, Z.a1};
-        const real qx = pc.qn * vx, qy = pc.qn * vy, qz = pc.qn * vz;
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-#pragma unroll
-          for (int cc = 0; cc < 3; ++cc) {
-            const real yz = by.w[b] * bz.w[cc];
-            ajx[0][b][cc] += (qx * ax[0]) * yz;
-            ajx[1][b][cc] += (qx * ax[1]) * yz;
-          }
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int cc = 0; cc < 3; ++cc) {
-            const real xz = bx.w[a] * bz.w[cc];
-            ajy[a][0][cc] += (qy * ay[0]) * xz;
-            ajy[a][1][cc] += (qy * ay[1]) * xz;
-          }
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            const real xy = bx.w[a] * by.w[b];
-            ajz[a][b][0] += (qz * az[0]) * xy;
-            ajz[a][b][1] += (qz * az[1]) * xy;
-          }
-      } else if (in_array(g, i, j, k)) {
-        if (stencil_ok(g, i, j, k)) {
-          scatter8_win(wjx, wx0, wy0, wz0, F.f[pc.pjx], g, X.a, Y.b, Z.b, pc.qn * vx, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
-          scatter8_win(wjy, wx0, wy0, wz0, F.f[pc.pjy], g, X.b, Y.a, Z.b, pc.qn * vy, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
-          scatter8_win(wjz, wx0, wy0, wz0, F.f[pc.pjz], g, X.b, Y.b, Z.a, pc.qn * vz, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
-        } else {
-          count_err(err, ERR_DEPOSIT_OOB);
-        }
-      }
-    }
-    advance(i, fx, vx * pc.hdt);
-    advance(j, fy, vy * pc.hdt);
-    advance(k, fz, vz * pc.hdt);
-    {  // n at x^{n+1}
-      const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-      if (i == hi && j == hj && k == hk) {
-        const W3<real> bx = home3(X, hi), by = home3(Y, hj), bz = home3(Z, hk);
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-#pragma unroll
-          for (int cc = 0; cc < 3; ++cc) {
-            const real yz = pc.nw * (by.w[b] * bz.w[cc]);
-#pragma unroll
-            for (int a = 0; a < 3; ++a) an[a][b][cc] += bx.w[a] * yz;
-          }
-      } else if (in_array(g, i, j, k)) {
-        if (stencil_ok(g, i, j, k)) {
-          scatter8_win(wn, wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b, pc.nw, X.b0, X.b1, Y.b0, Y.b1, Z.b0, Z.b1);
-        } else {
-          count_err(err, ERR_DEPOSIT_OOB);
-        }
-      }
-    }
-    P.cell[t] = boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
-    P.o[0][t] = fx; P.o[1][t] = fy; P.o[2][t] = fz;
-    P.v[0][t] = vx; P.v[1][t] = vy; P.v[2][t] = vz;
-  }
-  for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
-  if (lane == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
-  // the lane's home-cell sums into the window (nodes h-1 .. h+1 around it)
-  if (jmax > 0) {
-    const int la = hi - 1 - wx0, lb = hj - 1 - wy0, lc = hk - 1 - wz0;  // window index of node h-1
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          const int s = ((la + a) * WY + (lb + b)) * WZ + (lc + cc);
-          if (a < 2) atomicAdd(wjx + s + WY * WZ, ajx[a][b][cc]);  // x nodes h, h+1
-          if (b < 2) atomicAdd(wjy + s + WZ, ajy[a][b][cc]);       // y nodes h, h+1
-          if (cc < 2) atomicAdd(wjz + s + 1, ajz[a][b][cc]);       // z nodes h, h+1
-          atomicAdd(wn + s, an[a][b][cc]);
-        }
-  }
-  __syncthreads();
-  // flush the window: one reduction per 4 consecutive z nodes
-  const int planes[4] = {pc.pjx, pc.pjy, pc.pjz, pc.pn};
-  constexpr int NZ4 = WZ / 4;
-  for (int q4 = threadIdx.x; q4 < 4 * WX * WY * NZ4; q4 += blockDim.x) {
-    const int q = q4 / (WX * WY * NZ4);
-    const int r = q4 % (WX * WY * NZ4);
-    const int a = r / (WY * NZ4), b = (r / NZ4) % WY, c4 = r % NZ4;
-    const int ga = wx0 + a, gb = wy0 + b, gc = wz0 + 4 * c4;
-    if (ga >= g.gx || gb >= g.gy || gc >= g.gz) continue;
-    const real* src = win + q * WN + (a * WY + b) * WZ + 4 * c4;
-    const real v0 = src[0], v1 = src[1], v2 = src[2], v3 = src[3];
-    if (v0 == (real)0 && v1 == (real)0 && v2 == (real)0 && v3 == (real)0) continue;
-    real* dst = F.f[planes[q]] + ga * g.sx + gb * g.gz + gc;
-    if (VEC_FLUSH) {
-      red_add_v4(reinterpret_cast<float*>(dst), (float)v0, (float)v1, (float)v2, (float)v3);
-    } else {
-      const real v[4] = {v0, v1, v2, v3};
-#pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if (gc + e < g.gz && v[e] != (real)0) atomicAdd(dst + e, v[e]);
-    }
-  }
-}
 
 }  // namespace pb
