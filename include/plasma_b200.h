@@ -32,6 +32,7 @@ extern "C" {
 #define PIC_ERR_CAPACITY 3   /* particle capacity exceeded */
 #define PIC_ERR_STATE 4      /* call out of order (e.g. step before init) */
 #define PIC_ERR_DEVICE 5     /* device-side counters report lost work (pic_status) */
+#define PIC_ERR_TOO_LARGE 6  /* input larger than a fixed-size scratch allows */
 
 #define PIC_ION 0
 #define PIC_ELECTRON 1
@@ -160,6 +161,21 @@ int pic_get_stream(pic_ctx *ctx, void **stream);
  * number of kernels the context has launched since creation, and restarts. */
 int pic_set_timing(pic_ctx *ctx, int enable);
 int pic_read_timing(pic_ctx *ctx, double *ms8, long long *pairs8, long long *launches);
+
+/* No counterpart in the reference. The Gauss-law residual of pic_gauss_residual
+ * for callers that cannot allocate device memory (a plugin inside a host
+ * application that owns every device allocation): it takes the FP32 planes
+ * ex, ey, ez, ni, ne of a padded (nx+4)*(ny+4)*(nz+4) grid (z fastest) and a
+ * device array out4 of 4 doubles, all owned by the caller, queues its work on
+ * `stream` (a cudaStream_t, NULL for the default stream) and allocates
+ * nothing: its scratch is a static device array of 2048 x 4 doubles, which
+ * caps the input at 2048 * 256 * 64 = 33,554,432 interior cells (larger inputs
+ * return PIC_ERR_TOO_LARGE). The first call on each device sets up the
+ * scratch address; make it before any stream capture. All calls share the
+ * scratch: calls whose kernels overlap on the GPU race and must be ordered. */
+int pic_gauss_residual_noalloc(const float *ex, const float *ey, const float *ez,
+                               const float *ni, const float *ne, int nx, int ny, int nz,
+                               double dx, double q, double e0, void *stream, double *out4);
 const char *pic_error_string(int code);
 
 #ifdef __cplusplus

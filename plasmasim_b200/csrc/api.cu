@@ -780,6 +780,7 @@ const char* pic_error_string(int code) {
     case PIC_ERR_CAPACITY: return "particle capacity exceeded";
     case PIC_ERR_STATE: return "call out of order";
     case PIC_ERR_DEVICE: return "device counters report lost work";
+    case PIC_ERR_TOO_LARGE: return "input larger than the fixed-size scratch allows";
     default: return "unknown error";
   }
 }

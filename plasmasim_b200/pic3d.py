@@ -25,7 +25,8 @@ GRID_FIELDS = ["bx", "by", "bz", "b0x", "b0y", "b0z", "ex", "ey", "ez",
                "jix", "jiy", "jiz", "jex", "jey", "jez", "ni", "ne", "phi"]
 
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "particle capacity exceeded",
-          4: "call out of order", 5: "device counters report lost work"}
+          4: "call out of order", 5: "device counters report lost work",
+          6: "input larger than the fixed-size scratch allows"}
 
 
 class PicError(RuntimeError):
@@ -123,7 +124,7 @@ EXPORTED = [
     "pic_thrust_f", "pic_thrust_fave", "pic_gauss_residual", "pic_step", "pic_fdtd",
     "pic_set_particles", "pic_get_particles", "pic_particle_count", "pic_get_grid",
     "pic_set_grid", "pic_rng_counters", "pic_status", "pic_synchronize", "pic_get_stream",
-    "pic_error_string", "pic_set_timing", "pic_read_timing",
+    "pic_error_string", "pic_set_timing", "pic_read_timing", "pic_gauss_residual_noalloc",
 ]
 
 PHASES = ["push", "field", "sort", "add", "diag"]
@@ -165,6 +166,8 @@ def load_library(path: str = LIB_PATH):
     L.pic_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.pic_set_timing.argtypes = [vp, C.c_int]
     L.pic_read_timing.argtypes = [vp, _dp, _llp, _llp]
+    L.pic_gauss_residual_noalloc.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_int, C.c_int,
+                                             C.c_double, C.c_double, C.c_double, vp, vp]
     L.pic_error_string.restype = C.c_char_p
     L.pic_error_string.argtypes = [C.c_int]
     _lib = L
