@@ -7,10 +7,13 @@
 
 namespace pb {
 
-constexpr int kQueue = 64;  // per-warp queue of mover deposits (power of two)
+constexpr int kQueue = 64;   // per-warp queue of mover deposits (power of two)
+constexpr int kStages = 3;   // particle rows in flight per warp
 
-// Shared-memory plan of one CTA (8 warps): the J/n window, then per warp a
-// queue of J deposits of particles outside their home cell.
+// Shared-memory plan of one CTA (8 warps): the J/n window, per warp a queue of
+// J deposits of particles outside their home cell, and per warp a ring of
+// kStages particle rows fetched ahead with cp.async (cell words, then the six
+// coordinate arrays).
 template <typename real>
 struct PushSmem {
   static constexpr int WX = kTileX + 4, WY = kTileY + 4, WZ = kWinZ, WN = WX * WY * WZ;
@@ -18,8 +21,22 @@ struct PushSmem {
   static constexpr size_t win_bytes = 4 * WN * sizeof(real);
   static constexpr size_t qcell_off = (win_bytes + 15) & ~(size_t)15;
   static constexpr size_t qdat_off = qcell_off + (size_t)kWarps * kQueue * sizeof(int);
-  static constexpr size_t bytes = qdat_off + (size_t)kWarps * kQueue * 6 * sizeof(real);
+  static constexpr size_t pcell_off = qdat_off + (size_t)kWarps * kQueue * 6 * sizeof(real);
+  static constexpr size_t pdat_off = pcell_off + (size_t)kWarps * kStages * kLanes * sizeof(int);
+  static constexpr size_t bytes = pdat_off + (size_t)kWarps * kStages * 6 * kLanes * sizeof(real);
 };
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_n(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (BYTES == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
 
 // Deposit of one queued J entry (a particle outside its home cell) into the
 // window, or into global memory when its stencil leaves the window.
@@ -81,10 +98,32 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
         if (b < 2) ajy[a][b][c] = (real)0;
         if (c < 2) ajz[a][b][c] = (real)0;
       }
+  // ring of particle rows fetched ahead; each lane copies and reads only its
+  // own slots, so the per-thread cp.async groups need no warp barrier
+  int* pcell = reinterpret_cast<int*>(smem_raw + S::pcell_off) + warp * kStages * kLanes;
+  real* pdat = reinterpret_cast<real*>(smem_raw + S::pdat_off) + warp * kStages * 6 * kLanes;
+  auto fetch = [&](int row) {
+    if (row < jmax) {
+      const int t = base + row * kLanes + lane;
+      const int st = row % kStages;
+      cp_async_n<4>(pcell + st * kLanes + lane, P.cell + t);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        cp_async_n<sizeof(real)>(pdat + (st * 6 + a) * kLanes + lane, P.o[a] + t);
+        cp_async_n<sizeof(real)>(pdat + (st * 6 + 3 + a) * kLanes + lane, P.v[a] + t);
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int s = 0; s < kStages - 1; ++s) fetch(s);
   unsigned pushed = 0;
   for (int jj = 0; jj < jmax; ++jj) {
+    fetch(jj + kStages - 1);
+    cp_async_wait<kStages - 1>();
     const int t = base + jj * kLanes + lane;
-    const int c = P.cell[t];
+    const int st = jj % kStages;
+    const int c = pcell[st * kLanes + lane];
     const bool act = c >= 0;
     int i = 0, j = 0, k = 0;
     real fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
@@ -92,8 +131,9 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     if (act) {
       ++pushed;
       unpack_cell(c, i, j, k);
-      fx = P.o[0][t]; fy = P.o[1][t]; fz = P.o[2][t];
-      vx = P.v[0][t]; vy = P.v[1][t]; vz = P.v[2][t];
+      const real* d = pdat + st * 6 * kLanes + lane;
+      fx = d[0]; fy = d[kLanes]; fz = d[2 * kLanes];
+      vx = d[3 * kLanes]; vy = d[4 * kLanes]; vz = d[5 * kLanes];
       bool bal = ballistic(pc, i, j, k, fx, fy, fz);
       if (!bal && !stencil_ok(g, i, j, k)) {
         count_err(err, ERR_DEPOSIT_OOB);
