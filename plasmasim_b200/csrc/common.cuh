@@ -108,6 +108,13 @@ __device__ __forceinline__ double gauss_bm(uint64_t seed, uint64_t d) {
   return __dmul_rn(r, cos(ang));
 }
 
+// The same normal deviate from FP32 log/cos (for particles stored in FP32).
+__device__ __forceinline__ float gauss_bm_f32(uint64_t seed, uint64_t d) {
+  const float u1 = (float)__dadd_rn(1.0, -uniform53(seed, d));
+  const float u2 = (float)uniform53(seed, d + 1);
+  return sqrtf(-2.0f * logf(u1)) * cosf(6.28318530717958647692f * u2);
+}
+
 // Splits an absolute coordinate in cells into (cell, offset in [0,1)).
 template <typename real>
 __device__ __forceinline__ void split_coord(double xc, int& i, real& f) {

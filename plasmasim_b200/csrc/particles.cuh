@@ -389,10 +389,18 @@ __global__ void source_kernel(Parts<real> P, SourceParams sp, unsigned long long
   const double y = flat_rn(lo[1], hi[1], uniform53(sp.seed_p, dp + 1));
   const double z = flat_rn(lo[2], hi[2], uniform53(sp.seed_p, dp + 2));
   const uint64_t dv = (uint64_t)(sp.base_v + 6 * t);
-  const double g0 = gauss_bm(sp.seed_v, dv), g1 = gauss_bm(sp.seed_v, dv + 2), g2 = gauss_bm(sp.seed_v, dv + 4);
-  const double vx = __dadd_rn(__dmul_rn(sp.lsig, g0), 0.0);
-  const double vy = __dadd_rn(__dmul_rn(sp.lsig, g1), 0.0);
-  const double vz = __dadd_rn(__dmul_rn(sp.lsig, g2), sp.vdrift);
+  real vx, vy, vz;
+  if (sizeof(real) == 8) {  // the host's arithmetic, rounded step by step
+    const double g0 = gauss_bm(sp.seed_v, dv), g1 = gauss_bm(sp.seed_v, dv + 2), g2 = gauss_bm(sp.seed_v, dv + 4);
+    vx = (real)__dadd_rn(__dmul_rn(sp.lsig, g0), 0.0);
+    vy = (real)__dadd_rn(__dmul_rn(sp.lsig, g1), 0.0);
+    vz = (real)__dadd_rn(__dmul_rn(sp.lsig, g2), sp.vdrift);
+  } else {  // the same draws through FP32 log/cos: the FP32 state's own precision
+    const float ls = (float)sp.lsig;
+    vx = (real)(ls * gauss_bm_f32(sp.seed_v, dv));
+    vy = (real)(ls * gauss_bm_f32(sp.seed_v, dv + 2));
+    vz = (real)(ls * gauss_bm_f32(sp.seed_v, dv + 4) + (float)sp.vdrift);
+  }
   int ci, cj, ck;
   real fx, fy, fz;
   split_coord<real>(x / dx, ci, fx);
@@ -401,7 +409,7 @@ __global__ void source_kernel(Parts<real> P, SourceParams sp, unsigned long long
   const int dst = sp.dst + (int)t;
   P.cell[dst] = repack(ci, cj, ck, err);
   P.o[0][dst] = fx; P.o[1][dst] = fy; P.o[2][dst] = fz;
-  P.v[0][dst] = (real)vx; P.v[1][dst] = (real)vy; P.v[2][dst] = (real)vz;
+  P.v[0][dst] = vx; P.v[1][dst] = vy; P.v[2][dst] = vz;
 }
 
 // ------------------------------------------------------------------- sort

@@ -87,11 +87,18 @@ __global__ void tiled_count_kernel(Parts<real> P, Geom g, TileGeom t, const int*
   const int home = home_key(g, t, G, lane);
   const int base = goff[G], m = gmax[G];
   int nstay = 0;
-  for (int r = 0; r < m; ++r) {
-    const int key = interior_key(g, P.cell[base + r * kLanes + lane]);
-    if (key < 0) continue;
-    if (key == home) ++nstay;
-    else atomicAdd(moved + key, 1);
+  constexpr int U = 8;  // rows whose loads are in flight together
+  for (int r0 = 0; r0 < m; r0 += U) {
+    int cell[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) cell[u] = r0 + u < m ? P.cell[base + (r0 + u) * kLanes + lane] : -1;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int key = interior_key(g, cell[u]);
+      if (key < 0) continue;
+      if (key == home) ++nstay;
+      else atomicAdd(moved + key, 1);
+    }
   }
   if (home >= 0) stay[home] = nstay;
 }
@@ -158,19 +165,41 @@ __global__ void tiled_scatter_kernel(Parts<real> P, Geom g, TileGeom t, const in
   const int home = home_key(g, t, G, lane);
   const int base = goff_old[G], m = gmax_old[G], nbase = goff_new[G];
   int rnew = 0;
-  for (int r = 0; r < m; ++r) {
-    const int s = base + r * kLanes + lane;
-    const int c = P.cell[s];
-    const int key = interior_key(g, c);
-    if (key < 0) continue;
-    if (key == home) {
-      copy_particle(P, s, Q, nbase + rnew * kLanes + lane, c);
-      ++rnew;
-    } else {
-      int l2;
-      const int G2 = group_of_key(g, t, key, l2);
-      const int rank = stay[key] + atomicAdd(cursor + key, 1);
-      copy_particle(P, s, Q, goff_new[G2] + rank * kLanes + l2, c);
+  constexpr int U = 4;  // rows whose loads are in flight together
+  for (int r0 = 0; r0 < m; r0 += U) {
+    int cell[U];
+    real o[U][3], v[U][3];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int s = base + (r0 + u) * kLanes + lane;
+      const bool in = r0 + u < m;
+      cell[u] = in ? P.cell[s] : -1;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        o[u][a] = in ? P.o[a][s] : (real)0;
+        v[u][a] = in ? P.v[a][s] : (real)0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int key = interior_key(g, cell[u]);
+      if (key < 0) continue;
+      int d;
+      if (key == home) {
+        d = nbase + rnew * kLanes + lane;
+        ++rnew;
+      } else {
+        int l2;
+        const int G2 = group_of_key(g, t, key, l2);
+        const int rank = stay[key] + atomicAdd(cursor + key, 1);
+        d = goff_new[G2] + rank * kLanes + l2;
+      }
+      Q.cell[d] = cell[u];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        Q.o[a][d] = o[u][a];
+        Q.v[a][d] = v[u][a];
+      }
     }
   }
 }
