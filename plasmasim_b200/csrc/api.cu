@@ -16,6 +16,7 @@
 #include "particles.cuh"
 #include "tiled.cuh"
 #include "push_tiled.cuh"
+#include "relayout.cuh"
 
 using namespace pb;
 
@@ -55,6 +56,8 @@ struct pic_ctx {
   bool tiled[2] = {false, false};     // layout holds every slot: the tiled push may run
   int* gcap = nullptr;
   int* total_dev = nullptr;
+  int* append_dev = nullptr;          // end of the append region during a re-layout
+  int* holes = nullptr;               // per-slot scratch: hole rows of every lane column
   int* cnt = nullptr;
   int* offs = nullptr;
   int* cursor = nullptr;
@@ -287,18 +290,22 @@ int do_renew_grid(pic_ctx* c) {
 }
 
 // ---------------------------------------------------------- particles
+// The slot-order push over slots [first, count) (global-memory atomics).
 template <typename real, int MODE>
-int do_push(pic_ctx* c, int s) {
-  if (c->sp[s].count == 0) return PIC_OK;
-  push_kernel<real, MODE><<<particle_blocks(c->sp[s].count), kThreads, 0, c->stream>>>(
-      parts<real>(c, s), c->sp[s].count_dev, fields<real>(c), c->g, push_const<real>(c, s), c->err);
+int do_push(pic_ctx* c, int s, long long first = 0) {
+  if (c->sp[s].count <= first) return PIC_OK;
+  push_kernel<real, MODE><<<particle_blocks(c->sp[s].count - first), kThreads, 0, c->stream>>>(
+      parts<real>(c, s), (int)first, c->sp[s].count_dev, fields<real>(c), c->g, push_const<real>(c, s),
+      c->err);
   CKL();
   return PIC_OK;
 }
 
 template <typename real>
 int do_push_tiled(pic_ctx* c, int s) {
-  if (!c->tiled[s]) return do_push<real, PUSH_FUSED>(c, s);
+  if (!c->layout[s]) return do_push<real, PUSH_FUSED>(c, s);
+  // the slots after the layout (particles a re-layout could not place) first
+  CKR((do_push<real, PUSH_FUSED>(c, s, c->tiled_end[s])));
   const int ntiles = c->tg.ntx * c->tg.nty * c->tg.ntz;
   TileArgs ta{c->tg, c->goff[s][c->lay[s]], c->gmax[s][c->lay[s]]};
   const size_t smem = PushSmem<real>::bytes;
@@ -347,9 +354,8 @@ int scan_exclusive(pic_ctx* c, const int* in, int* out, long long n, int* tmp, s
   return PIC_OK;
 }
 
-__global__ void sort_total_kernel(const int* offs, const int* cnt, long long n, int* count_dev) {
-  *count_dev = offs[n - 1] + cnt[n - 1];
-}
+SourceParams source_params(const pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form);
+void refill_slabs(const pic_ctx* c, Slab* slabs);
 
 // sorting (:7475-7590) into the tiled layout of tiled.cuh: count the
 // particles of every interior cell (stayers of the previous layout per lane
@@ -381,7 +387,10 @@ int do_sort_species(pic_ctx* c, int s) {
         P, (int)first, st.count_dev, c->g, moved);
     CKL();
   }
-  group_size_kernel<<<gblocks, kThreads, 0, c->stream>>>(c->g, tg, stay, moved, c->gmax[s][nw], c->gcap);
+  Slab slabs[5];
+  refill_slabs(c, slabs);
+  group_size_kernel<<<gblocks, kThreads, 0, c->stream>>>(c->g, tg, stay, moved, source_params(c, s, slabs, 5, 0),
+                                                         c->gmax[s][nw], c->gcap);
   CKL();
   CKR(scan_exclusive(c, c->gcap, c->goff[s][nw], tg.ngroups, c->scan_tmp, c->scan_tmp_len));
   tiled_total_kernel<<<1, 1, 0, c->stream>>>(c->goff[s][nw], c->gcap, tg.ngroups, c->total_dev);
@@ -413,16 +422,56 @@ int do_sort_species(pic_ctx* c, int s) {
   return PIC_OK;
 }
 
+// In-place re-layout (relayout.cuh): movers and appended particles into the
+// holes of their columns; a full sort when there is no layout yet or some
+// column overflows.
+template <typename real>
+int do_relayout_species(pic_ctx* c, int s) {
+  Store& st = c->sp[s];
+  if (!c->layout[s]) return do_sort_species<real>(c, s);
+  const TileGeom& tg = c->tg;
+  const int gblocks = grid_blocks((long long)tg.ngroups * 32);
+  const Parts<real> P = parts<real>(c, s);
+  int* nholes = c->cnt;
+  CK(cudaMemsetAsync(c->cursor, 0, sizeof(int) * c->ncells, c->stream));
+  CK(cudaMemsetAsync(c->total_dev, 0, sizeof(int), c->stream));  // overflow count
+  set_int_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.count);
+  CKL();
+  classify_kernel<real><<<gblocks, kThreads, 0, c->stream>>>(P, c->g, tg, c->goff[s][c->lay[s]],
+                                                             c->gmax[s][c->lay[s]], (int)st.cap, c->holes,
+                                                             nholes, c->append_dev);
+  CKL();
+  clamp_count_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.cap, st.count_dev);
+  CKL();
+  const long long first = c->tiled_end[s];
+  const Parts<real> Q = parts<real>(c, s, 1 - st.cur);
+  place_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
+      P, (int)first, st.count_dev, c->g, tg, c->goff[s][c->lay[s]], c->holes, nholes, c->cursor, Q,
+      c->total_dev);
+  CKL();
+  unspill_kernel<real><<<particle_blocks(st.cap), kThreads, 0, c->stream>>>(Q, c->total_dev, P, (int)first);
+  CKL();
+  int nspill = 0;
+  CK(cudaMemcpyAsync(&nspill, c->total_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CKR(set_count(c, s, first + nspill));
+  c->tiled[s] = true;
+  // particles without a hole are pushed in slot order; many of them call for a sort
+  if (nspill > first / 50) return do_sort_species<real>(c, s);
+  return PIC_OK;
+}
+
 template <typename real>
 int do_sort(pic_ctx* c) {
-  for (int s = 0; s < 2; ++s) CKR(do_sort_species<real>(c, s));
+  for (int s = 0; s < 2; ++s) CKR(do_relayout_species<real>(c, s));
   return PIC_OK;
 }
 
 // Generates `total` particles of species s from the slabs into slots
 // [count, count + total), drawing from the shared position/velocity streams.
-template <typename real>
-int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0) {
+// Source description of species s for the given slabs, drawing from the
+// current position of the shared random streams.
+SourceParams source_params(const pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form) {
   SourceParams sp{};
   sp.init_form = init_form;
   long long total = 0;
@@ -434,9 +483,6 @@ int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0
   sp.nslab = nslab;
   sp.np = c->cfg.np;
   sp.total = total;
-  if (total == 0) return PIC_OK;
-  Store& st = c->sp[s];
-  if (st.count + total > st.cap) return PIC_ERR_CAPACITY;
   const double T = s == 0 ? c->cfg.ti : c->cfg.te;
   const double sig = std::sqrt(c->cfg.kb * T / species_mass(c, s));
   sp.dx = c->cfg.dx;
@@ -446,7 +492,28 @@ int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0
   sp.seed_v = c->cfg.seed_v;
   sp.base_p = c->ctr_p;
   sp.base_v = c->ctr_v;
-  sp.dst = (int)st.count;
+  sp.dst = (int)c->sp[s].count;
+  return sp;
+}
+
+// add_ion_flat :6037-6220 at size 1: z slabs, y slabs, the low-x slab.
+void refill_slabs(const pic_ctx* c, Slab* slabs) {
+  const int Nx = c->cfg.nx, Ny = c->cfg.ny, Nz = c->cfg.nz;
+  const Slab s[5] = {
+      {2, Nx, 2, Ny, 2, 2, 0},          {2, Nx, 2, Ny, Nz, 2, 0},
+      {2, Nx, 2, 2, 4, Nz - 4, 0},      {2, Nx, Ny, 2, 4, Nz - 4, 0},
+      {2, 2, 4, Ny - 2, 4, Nz - 4, 0},
+  };
+  for (int q = 0; q < 5; ++q) slabs[q] = s[q];
+}
+
+template <typename real>
+int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0) {
+  const SourceParams sp = source_params(c, s, slabs, nslab, init_form);
+  const long long total = sp.total;
+  if (total == 0) return PIC_OK;
+  Store& st = c->sp[s];
+  if (st.count + total > st.cap) return PIC_ERR_CAPACITY;
   source_kernel<real><<<grid_blocks(total), kThreads, 0, c->stream>>>(parts<real>(c, s), sp, c->err);
   CKL();
   c->ctr_p += 3 * total;
@@ -454,15 +521,11 @@ int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0
   return set_count(c, s, st.count + total);
 }
 
+
 template <typename real>
 int do_add_flat(pic_ctx* c) {
-  const int Nx = c->cfg.nx, Ny = c->cfg.ny, Nz = c->cfg.nz;
-  // add_ion_flat :6037-6220 at size 1: z slabs, y slabs, the low-x slab
-  const Slab slabs[5] = {
-      {2, Nx, 2, Ny, 2, 2, 0},          {2, Nx, 2, Ny, Nz, 2, 0},
-      {2, Nx, 2, 2, 4, Nz - 4, 0},      {2, Nx, Ny, 2, 4, Nz - 4, 0},
-      {2, 2, 4, Ny - 2, 4, Nz - 4, 0},
-  };
+  Slab slabs[5];
+  refill_slabs(c, slabs);
   for (int s = 0; s < 2; ++s) {
     Store& st = c->sp[s];
     if (st.count > 0) {
@@ -470,7 +533,7 @@ int do_add_flat(pic_ctx* c) {
           parts<real>(c, s), st.count_dev, c->g);
       CKL();
     }
-    CKR(do_source<real>(c, s, slabs, 5));
+    CKR(do_source<real>(c, s, slabs, 5));  // appended; the next step's re-layout places them
   }
   return PIC_OK;
 }
@@ -599,7 +662,7 @@ int do_step(pic_ctx* c) {
   if (!c->tiled[0] || !c->tiled[1]) {  // after a refill or an import
     CKR(phase_mark(c, PH_SORT));
     for (int s = 0; s < 2; ++s)
-      if (!c->tiled[s]) CKR(do_sort_species<real>(c, s));
+      if (!c->tiled[s]) CKR(do_relayout_species<real>(c, s));
     CKR(phase_mark(c, PH_SORT));
   }
   CKR(phase_mark(c, PH_PUSH));
@@ -840,7 +903,6 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
   g.sx = g.gy * g.gz;
   g.nodes = g.gx * g.gy * g.gz;
   c->ncells = (long long)k.nx * k.ny * k.nz;
-  int rc = PIC_OK;
   auto fail = [&](int code) {
     pic_destroy(c);
     return code;
@@ -888,6 +950,8 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
     }
     if (cudaMalloc(&c->gcap, sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->total_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    if (cudaMalloc(&c->append_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    if (cudaMalloc(&c->holes, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaFuncSetAttribute(push_tiled_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)PushSmem<double>::bytes) != cudaSuccess ||
         cudaFuncSetAttribute(push_tiled_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -904,7 +968,6 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
   cudaMemsetAsync(c->fave, 0, sizeof(double) * 27, c->stream);
   cudaMemsetAsync(c->err, 0, sizeof(unsigned long long) * ERR_COUNT, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(PIC_ERR_CUDA);
-  (void)rc;
   *out = c;
   return PIC_OK;
 }
@@ -928,6 +991,8 @@ int pic_destroy(pic_ctx* c) {
   }
   cudaFree(c->gcap);
   cudaFree(c->total_dev);
+  cudaFree(c->append_dev);
+  cudaFree(c->holes);
   cudaFree(c->cnt);
   cudaFree(c->offs);
   cudaFree(c->cursor);

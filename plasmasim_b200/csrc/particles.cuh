@@ -209,12 +209,12 @@ enum PushMode { PUSH_J = 0, PUSH_FUSED = 1 };
 //              second B half-step that the reference runs between them changes
 //              nothing they compute.
 template <typename real, int MODE>
-__global__ void __launch_bounds__(256) push_kernel(Parts<real> P, const int* __restrict__ count,
+__global__ void __launch_bounds__(256) push_kernel(Parts<real> P, int first, const int* __restrict__ count,
                                                    Fields<real> F, Geom g, PushConst<real> pc,
                                                    unsigned long long* err) {
   const int n = *count;
   unsigned pushed = 0;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+  for (int t = first + blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int c = P.cell[t];
     if (c < 0) continue;
     ++pushed;
@@ -356,25 +356,13 @@ struct SourceParams {
 // Positions: three gsl_ran_flat draws (x, y, z) on the position stream;
 // velocities: ran_multivar_gaussian = three Box-Muller normals (two draws
 // each) on the velocity stream, scaled by the Cholesky factor, plus mu.
+// Particle t of the call's sequence, in absolute cell cc, written to slot dst.
 template <typename real>
-__global__ void source_kernel(Parts<real> P, SourceParams sp, unsigned long long* err) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= sp.total) return;
-  int s = 0;
-  while (s + 1 < sp.nslab && t >= sp.slab[s + 1].first) ++s;
-  const Slab& sl = sp.slab[s];
-  long long r = t - sl.first;
-  const int jj = (int)(r % sp.np);
-  r /= sp.np;
-  const int m = (int)(r % sl.nm);
-  r /= sl.nm;
-  const int l = (int)(r % sl.nl);
-  const int k = (int)(r / sl.nl);
-  (void)jj;
+__device__ __forceinline__ void make_particle(const Parts<real>& P, const SourceParams& sp, long long t,
+                                              const int (&cc)[3], int dst, unsigned long long* err) {
   const double dx = sp.dx;
   const uint64_t dp = (uint64_t)(sp.base_p + 3 * t);
   double lo[3], hi[3];
-  const int cc[3] = {k + sl.k0, l + sl.l0, m + sl.m0};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     if (sp.init_form) {  // 2.*dx + k*dx with k counted from the first interior cell
@@ -406,10 +394,43 @@ __global__ void source_kernel(Parts<real> P, SourceParams sp, unsigned long long
   split_coord<real>(x / dx, ci, fx);
   split_coord<real>(y / dx, cj, fy);
   split_coord<real>(z / dx, ck, fz);
-  const int dst = sp.dst + (int)t;
   P.cell[dst] = repack(ci, cj, ck, err);
   P.o[0][dst] = fx; P.o[1][dst] = fy; P.o[2][dst] = fz;
   P.v[0][dst] = vx; P.v[1][dst] = vy; P.v[2][dst] = vz;
+}
+
+// Sequence number of the particles of absolute cell (i, j, k) in slab sl (the
+// first of its np), or -1 when the slab does not cover the cell.
+__device__ __forceinline__ long long slab_first(const Slab& sl, int np, int i, int j, int k) {
+  const int a = i - sl.k0, b = j - sl.l0, c = k - sl.m0;
+  if (a < 0 || b < 0 || c < 0 || a >= sl.nk || b >= sl.nl || c >= sl.nm) return -1;
+  return sl.first + ((long long)((long long)a * sl.nl + b) * sl.nm + c) * np;
+}
+
+// Particles the slabs put into absolute cell (i, j, k).
+__device__ __forceinline__ int slab_need(const SourceParams& sp, int i, int j, int k) {
+  int n = 0;
+  for (int s = 0; s < sp.nslab; ++s)
+    if (slab_first(sp.slab[s], sp.np, i, j, k) >= 0) n += sp.np;
+  return n;
+}
+
+// The call's particles, one thread each, into slots [dst, dst + total).
+template <typename real>
+__global__ void source_kernel(Parts<real> P, SourceParams sp, unsigned long long* err) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= sp.total) return;
+  int s = 0;
+  while (s + 1 < sp.nslab && t >= sp.slab[s + 1].first) ++s;
+  const Slab& sl = sp.slab[s];
+  long long r = t - sl.first;
+  r /= sp.np;
+  const int m = (int)(r % sl.nm);
+  r /= sl.nm;
+  const int l = (int)(r % sl.nl);
+  const int k = (int)(r / sl.nl);
+  const int cc[3] = {k + sl.k0, l + sl.l0, m + sl.m0};
+  make_particle(P, sp, t, cc, sp.dst + (int)t, err);
 }
 
 // ------------------------------------------------------------------- sort
@@ -440,39 +461,6 @@ __device__ __forceinline__ int warp_aggregated_inc(int* counter, int key, bool a
     base = old + rank;
   }
   return base;
-}
-
-template <typename real>
-__global__ void sort_count_kernel(Parts<real> P, const int* __restrict__ count, Geom g, int* cnt) {
-  const int n = *count;
-  const int stride = gridDim.x * blockDim.x;
-  // every lane of a warp runs the same number of iterations (warp-collective)
-  const int n_round = (n + 31) & ~31;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_round; t += stride) {
-    const int key = t < n ? interior_key(g, P.cell[t]) : -1;
-    warp_aggregated_inc(cnt, key < 0 ? 0 : key, key >= 0);
-  }
-}
-
-template <typename real>
-__global__ void sort_scatter_kernel(Parts<real> P, const int* __restrict__ count, Geom g,
-                                    const int* __restrict__ offs, int* cursor, Parts<real> Q) {
-  const int n = *count;
-  const int stride = gridDim.x * blockDim.x;
-  const int n_round = (n + 31) & ~31;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_round; t += stride) {
-    const int key = t < n ? interior_key(g, P.cell[t]) : -1;
-    const int r = warp_aggregated_inc(cursor, key < 0 ? 0 : key, key >= 0);
-    if (key >= 0) {
-      const int d = offs[key] + r;
-      Q.cell[d] = P.cell[t];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        Q.o[a][d] = P.o[a][t];
-        Q.v[a][d] = P.v[a][t];
-      }
-    }
-  }
 }
 
 // ------------------------------------------------------- scan (exclusive)

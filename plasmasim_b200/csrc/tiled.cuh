@@ -113,14 +113,41 @@ __global__ void append_count_kernel(Parts<real> P, int first, const int* __restr
   }
 }
 
-// One warp per group: gmax = largest (stayers + movers) count of its 32 lanes.
+// Absolute indices of group G's lane cell; false when the lane has no cell.
+__device__ __forceinline__ bool home_cell(const Geom& g, const TileGeom& t, int G, int lane, int& i,
+                                          int& j, int& k) {
+  const int tile = G / (kTileX * kTileY), w = G % (kTileX * kTileY);
+  const int tz = tile % t.ntz, ty = (tile / t.ntz) % t.nty, tx = tile / (t.ntz * t.nty);
+  i = tx * kTileX + w / kTileY;
+  j = ty * kTileY + w % kTileY;
+  k = tz * kLanes + lane;
+  const bool ok = i < g.nx && j < g.ny && k < g.nz;
+  i += 2; j += 2; k += 2;
+  return ok;
+}
+
+// Rows a lane column keeps for the boundary refill of its cell: the refill's
+// particle count plus an eighth and four, so that the refill fits into the
+// column's empty slots without moving other particles.
+__device__ __forceinline__ int refill_reserve(const SourceParams& sp, const Geom& g, const TileGeom& t,
+                                              int G, int lane) {
+  int i, j, k;
+  if (!home_cell(g, t, G, lane, i, j, k)) return 0;
+  const int need = slab_need(sp, i, j, k);
+  return need > 0 ? need + need / 8 + 4 : 0;
+}
+
+// One warp per group: gmax = largest (stayers + movers) count of its 32
+// lanes, or a lane's refill reserve when that is larger.
 __global__ void group_size_kernel(Geom g, TileGeom t, const int* __restrict__ stay,
-                                  const int* __restrict__ moved, int* gmax, int* gcap) {
+                                  const int* __restrict__ moved, SourceParams refill, int* gmax,
+                                  int* gcap) {
   const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (G >= t.ngroups) return;
   const int home = home_key(g, t, G, lane);
   int c = home >= 0 ? stay[home] + moved[home] : 0;
+  c = max(c, refill_reserve(refill, g, t, G, lane));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
   if (lane == 0) {

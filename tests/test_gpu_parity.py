@@ -134,6 +134,27 @@ def test_add_flat_matches_oracle(precision):
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
+def test_add_flat_into_tiled_layout_matches_oracle(precision):
+    """add_*_flat after a sort, then a second sort: the refill, appended after
+    the tiled layout, is moved into the holes the shell deletion left (the
+    in-place re-layout) and holds the same particles as the reference's."""
+    O = make_oracle("tiny")
+    O.call("init_grid")
+    O.call("init_particle_flat")
+    O.call("sort")
+    O.call("add_flat")
+    with new_pic(precision=precision) as P:
+        P.init_grid()
+        P.init_particle_flat()
+        P.sorting()
+        P.add_flat()
+        P.sorting()
+        assert list(P.rng_counters()) == [O.rng_counter(0), O.rng_counter(1)]
+        for s in (ION, ELECTRON):
+            check_rows(sort_rows(P.particles(s)), sort_rows(O.particles(s)[0]), precision, f"species {s}")
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
 def test_sort_matches_oracle(precision):
     """sorting: the same particle set in cell order (ghost-cell particles dropped)."""
     O = make_oracle("tiny")
@@ -255,7 +276,7 @@ def test_fp32_within_thrust_tolerance_of_fp64():
 def test_edge_cases(precision):
     """Empty species, particles on cell faces and box edges, the ghost-cell
     deposit that would leave the array, capacity and argument errors."""
-    with new_pic(precision=precision, diag_every_step=0, capacity=4096) as P:
+    with new_pic(precision=precision, diag_every_step=0, capacity=65536) as P:
         P.init_grid()
         P.set_particles(ION, np.zeros((0, 7)))
         P.set_particles(ELECTRON, np.zeros((0, 7)))
@@ -284,7 +305,7 @@ def test_edge_cases(precision):
         O.call("push_j")
         check_rows(P.particles(ION), O.particles(0)[0], precision, "edge push")
         with pytest.raises(Exception):
-            P.set_particles(ION, np.zeros((5000, 7)) + w)   # over capacity
+            P.set_particles(ION, np.zeros((65537, 7)) + w)  # over capacity
         bad = rows.copy()
         bad[0, 6] = 2 * w
         with pytest.raises(Exception):
