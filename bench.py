@@ -229,6 +229,13 @@ def run_e2e(P, steps: int):
     return pushed / dt, h2d / steps, d2h / steps
 
 
+# DRAM bytes (read + write) per pushed particle of push_tiled_kernel<float>,
+# from the ncu capture of a 64^3 x 64 ppc launch
+# (profiles/push_tiled_kernel_grid64_64ppc.md); at a fixed number of particles
+# per cell the traffic of a launch grows with its particles.
+PUSH_TRAFFIC_PER_PARTICLE = 61.0
+
+
 def roofline(out, npart_species, cells, rsize):
     """Push kernel: algorithmic bytes per launch = particles x (read + write of
     the SoA state: 4 + 6 rsize bytes each way) + cells x rsize x (6 gathered
@@ -320,6 +327,7 @@ def main():
     nsp = pushed / max(args.steps, 1) / 2
     ach, bytes_launch, s_launch = roofline(out, nsp, cells, 4)
     peak, peak_kind = measured_peaks()
+    step_bytes = pushed / max(args.steps, 1) * 56 + NX * NY * NZ * 200
 
     e2e = None
     if not args.no_e2e and world == 1:
@@ -365,9 +373,14 @@ def main():
                        "l2": "inputs larger than L2 (7.5 GB of particle state per step)",
                        "parallelism": f"replicas{world}"},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": ach / peak, "traffic": None, "kernel": "push_kernel<float,FUSED>",
+                         "frac": ach / peak,
+                         "traffic": PUSH_TRAFFIC_PER_PARTICLE * nsp if PPC == 64 else None,
+                         "kernel": "push_tiled_kernel<float,1> (push phase, with its tail push_kernel)",
                          "peak_kind": peak_kind, "bytes_per_launch": bytes_launch,
                          "ms_per_launch": s_launch * 1e3},
+            "step_roofline": {"bytes_per_step": step_bytes, "achieved": step_bytes / (ms_max / args.steps) / 1e6,
+                              "frac": step_bytes / (ms_max / args.steps) / 1e6 / peak, "unit": "GB/s",
+                              "bytes": "particles x 56 + cells x 200 (FP32)"},
             "phase_ms_per_step": {k: v / args.steps for k, v in out["phase_ms"].items()},
             "clocks": out["clocks"], "gpu_launches": out["launches"],
             "device_errors": out["errors"], "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu,
