@@ -56,12 +56,14 @@ __device__ __forceinline__ void deposit_j_entry(real* win, int wx0, int wy0, int
 // The fused particle part of one step (push, J deposit at x^{n+1/2}, drift,
 // n deposit at x^{n+1}, sr_particle) for one species over the tiled layout;
 // the same arithmetic as push_kernel<real, PUSH_FUSED> apart from the FP32
-// square roots and divisions. One CTA per tile, one warp per group.
+// square roots and divisions and, in FP32, the fixed-point sums of the density
+// window. One CTA per tile, one warp per group.
 //
 // J of a particle still in its lane's home cell is summed in registers; J of
 // the others is queued per warp and deposited 32 entries at a time, so that a
 // few such particles do not make the whole warp run the atomic path. The
-// density goes to the window with shared atomics (every active lane at once).
+// density goes to the window with shared reductions (every active lane at
+// once): integer ones on fixed-point sums in FP32, FP64 atomics in FP64.
 template <typename real, bool VEC_FLUSH>
 __global__ void __launch_bounds__(kTileX * kTileY * 32, 2)
 push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc,
@@ -87,6 +89,16 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   // home cell of this lane
   const int hi = wx0 + 2 + warp / kTileY, hj = wy0 + 2 + warp % kTileY, hk = wz0 + 2 + lane;
   real* wn = win + 3 * WN;
+  // FP32: the density window holds fixed-point sums (scatter8_win_fixed) at a
+  // scale that no node of this tile can overflow
+  constexpr bool kFixedN = sizeof(real) == 4;
+  float nscale = 0.f;
+  if (kFixedN) {
+    int slots = 0;
+#pragma unroll
+    for (int w = 0; w < kTileX * kTileY; ++w) slots += ta.gmax[tile * (kTileX * kTileY) + w];
+    nscale = 4294967295.f / (float)(slots * kLanes + 1);
+  }
   real ajx[2][3][3], ajy[3][2][3], ajz[3][3][2];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
@@ -209,7 +221,11 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       if (in_array(g, i, j, k)) {
         if (stencil_ok(g, i, j, k)) {
           const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-          scatter8_win(wn, wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b, pc.nw, X.b0, X.b1, Y.b0, Y.b1, Z.b0, Z.b1);
+          if constexpr (kFixedN)
+            scatter8_win_fixed(reinterpret_cast<unsigned*>(wn), wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b,
+                               pc.nw, nscale, X.b0, X.b1, Y.b0, Y.b1, Z.b0, Z.b1);
+          else
+            scatter8_win(wn, wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b, pc.nw, X.b0, X.b1, Y.b0, Y.b1, Z.b0, Z.b1);
         } else {
           count_err(err, ERR_DEPOSIT_OOB);
         }
@@ -255,7 +271,12 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     const int ga = wx0 + a, gb = wy0 + b, gc = wz0 + 4 * c4;
     if (ga >= g.gx || gb >= g.gy || gc >= g.gz) continue;
     const real* src = win + q * WN + (a * WY + b) * WZ + 4 * c4;
-    const real v0 = src[0], v1 = src[1], v2 = src[2], v3 = src[3];
+    real v0 = src[0], v1 = src[1], v2 = src[2], v3 = src[3];
+    if (kFixedN && q == 3) {  // fixed-point density sums back to weights
+      const unsigned* u = reinterpret_cast<const unsigned*>(src);
+      const real back = pc.nw / (real)nscale;
+      v0 = (real)u[0] * back; v1 = (real)u[1] * back; v2 = (real)u[2] * back; v3 = (real)u[3] * back;
+    }
     if (v0 == (real)0 && v1 == (real)0 && v2 == (real)0 && v3 == (real)0) continue;
     real* dst = F.f[planes[q]] + ga * g.sx + gb * g.gz + gc;
     if (VEC_FLUSH) {

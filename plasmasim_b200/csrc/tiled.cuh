@@ -282,6 +282,41 @@ __device__ __forceinline__ void scatter8_win(real* win, int wx0, int wy0, int wz
   }
 }
 
+// Density deposit into a fixed-point window: the 2x2x2 area weights (each in
+// [0, 1], summing to 1) scaled by `scale` and rounded, added with integer
+// shared-memory reductions, which need no compare-and-swap loop and give a sum
+// that does not depend on the order of the particles. The caller picks `scale`
+// so that no node can overflow: a node collects at most one unit of weight from
+// each particle of the tile, so scale = (2^32 - 1) / (slots + 1) is safe. With
+// 64 particles per cell this resolves 2^-17.7 of a particle's weight, as fine
+// as an FP32 sum of the same node. The stencil falls back to FP32 global
+// atomics (weight v) when it leaves the window.
+__device__ __forceinline__ void red_shared_u32(const unsigned* p, unsigned v) {
+  asm volatile("red.shared.add.u32 [%0], %1;" :: "r"((unsigned)__cvta_generic_to_shared(p)), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void scatter8_win_fixed(unsigned* win, int wx0, int wy0, int wz0, float* gplane,
+                                                   const Geom& g, int a, int b, int c, float v, float scale,
+                                                   float x0, float x1, float y0, float y1, float z0, float z1) {
+  constexpr int WY = kTileY + 4, WZ = kWinZ, WX = kTileX + 4;
+  const int la = a - wx0, lb = b - wy0, lc = c - wz0;
+  if (la >= 0 && la <= WX - 2 && lb >= 0 && lb <= WY - 2 && lc >= 0 && lc <= WZ - 2) {
+    const unsigned* s = win + (la * WY + lb) * WZ + lc;
+    const float a0 = scale * x0, a1 = scale * x1;
+    const float a00 = a0 * y0, a01 = a0 * y1, a10 = a1 * y0, a11 = a1 * y1;
+    red_shared_u32(s, __float2uint_rn(a00 * z0));
+    red_shared_u32(s + 1, __float2uint_rn(a00 * z1));
+    red_shared_u32(s + WZ, __float2uint_rn(a01 * z0));
+    red_shared_u32(s + WZ + 1, __float2uint_rn(a01 * z1));
+    red_shared_u32(s + WY * WZ, __float2uint_rn(a10 * z0));
+    red_shared_u32(s + WY * WZ + 1, __float2uint_rn(a10 * z1));
+    red_shared_u32(s + WY * WZ + WZ, __float2uint_rn(a11 * z0));
+    red_shared_u32(s + WY * WZ + WZ + 1, __float2uint_rn(a11 * z1));
+  } else {
+    scatter8(gplane, a * g.sx + b * g.gz + c, g.sx, g.gz, v, x0, x1, y0, y1, z0, z1);
+  }
+}
+
 // Half-shifted weights of a particle in its home cell h as a 3-vector over the
 // nodes h-1, h, h+1 (its base is h-1 for an offset below 1/2, h otherwise).
 template <typename real>
