@@ -132,6 +132,33 @@ int pic_step(pic_ctx *ctx, int nsteps);
 /* fdtd (:627-952) for nsteps: one add_*_flat, then pic_step(nsteps). */
 int pic_fdtd(pic_ctx *ctx, int nsteps);
 
+/* Differentiation (no counterpart in the reference).
+ *
+ * Objective: the impulse along z delivered to the dipole over nsteps loop
+ * bodies from the current state,
+ *   J = sum over steps of dt * F,  F = -sum_p s_p q n dx^3 (v x B0(x_p))_z
+ * over the particles alive after each step's sr_particle (s_p = +1 for ions,
+ * -1 for electrons; B0 gathered with the shape functions of B): the reaction
+ * to the Lorentz force of the dipole's own field on the plasma.
+ *
+ * Both calls advance the state by nsteps loop bodies of fdtd (:687-949) in a
+ * slot-stable form: no sorting (it only reorders particles), a refill that
+ * compacts the slots before it appends, and current sums in 64-bit fixed
+ * point so that every replay of a step is bit-identical.
+ *
+ * pic_objective: *J after nsteps.
+ * pic_adjoint: out3 = {J, dJ/dI, dJ/dV}, the gradient with respect to the coil
+ * current I (the dipole moment is mu0 I pi R^2; only the dipole part of B0
+ * depends on it) and the drift V (every particle created by the initial load
+ * or a refill has vz = V + thermal, so the current state must be such a load:
+ * call it after pic_init_grid, pic_init_particle_flat and pic_fdtd(ctx, 0)).
+ * The reverse pass keeps a checkpoint every checkpoint_every steps and
+ * recomputes each segment, so device memory holds nsteps/checkpoint_every
+ * full states plus checkpoint_every step inputs. The context ends in the state
+ * after the nsteps loop bodies. */
+int pic_objective(pic_ctx *ctx, int nsteps, double *J);
+int pic_adjoint(pic_ctx *ctx, int nsteps, int checkpoint_every, double *out3);
+
 /* State import/export in reference units (FP64 host arrays). */
 int pic_set_particles(pic_ctx *ctx, int species, const double *rows, const int *flag,
                       long long n);

@@ -108,10 +108,12 @@ def build_ref(name: str, force: bool = False) -> str:
 
 
 def build_oracle(force: bool = False) -> str:
-    """Compile the project's FP64 restatement of the step (oracle/pic_oracle.c)."""
-    src = os.path.join(HERE, "pic_oracle.c")
+    """Compile the project's FP64 restatement of the step (oracle/pic_oracle.c)
+    together with its tangent-linear (oracle/tangent.c, which includes it)."""
+    srcs = [os.path.join(HERE, "pic_oracle.c"), os.path.join(HERE, "tangent.c")]
+    src = srcs[1]
     if (os.path.isfile(ORACLE_SO) and not force
-            and os.path.getmtime(ORACLE_SO) >= os.path.getmtime(src)):
+            and os.path.getmtime(ORACLE_SO) >= max(os.path.getmtime(f) for f in srcs)):
         return ORACLE_SO
     cmd = ["gcc", "-std=gnu11", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-Wall",
            "-Wno-unused-function", "-I", HERE, src, os.path.join(HERE, "shim", "gsl_shim.c"),

@@ -93,6 +93,15 @@ class Oracle:
             L.or_fdtd.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
             L.or_fave.argtypes = [C.c_void_p, _dp]
             L.or_oob_count.restype = C.c_long
+            L.or_tl_create.restype = C.c_void_p
+            L.or_tl_create.argtypes = [C.c_void_p, _dp, C.c_double, C.c_double]
+            L.or_tl_destroy.argtypes = [C.c_void_p]
+            L.or_tl_result.argtypes = [C.c_void_p, _dp]
+            L.or_tl_step.argtypes = [C.c_void_p, C.c_void_p, _ip, C.c_int]
+            L.or_plain_step.restype = C.c_double
+            L.or_plain_step.argtypes = [C.c_void_p, _ip, C.c_int]
+            L.or_dipole_force.restype = C.c_double
+            L.or_dipole_force.argtypes = [C.c_void_p]
             cls._lib = L
         return cls._lib
 
@@ -176,6 +185,31 @@ class Oracle:
         out = np.zeros(27)
         self.L.or_fave(self.h, _ptr(out))
         return out
+
+    def dipole_force(self) -> float:
+        """F = -sum s q n dx^3 (v x B0(x))_z over the current particles."""
+        return float(self.L.or_dipole_force(self.h))
+
+    def plain_steps(self, nsteps, add_every=5) -> float:
+        """nsteps loop bodies without sorting; returns sum of dt * F after each."""
+        J = 0.0
+        for _ in range(nsteps):
+            J += self.L.or_plain_step(self.h, C.byref(self.c_add), add_every)
+        return J
+
+    def tangent_run(self, nsteps, dI, dV, add_every=5):
+        """FP64 tangent-linear of nsteps loop bodies (no sorting) from the
+        current state, seeded in direction (dI, dV); returns (J, dJ)."""
+        arr = np.array([float(self.p[k]) for k in _ORDER], dtype=np.float64)
+        t = self.L.or_tl_create(self.h, _ptr(arr), dI, dV)
+        try:
+            for _ in range(nsteps):
+                self.L.or_tl_step(self.h, t, C.byref(self.c_add), add_every)
+            out = np.zeros(2)
+            self.L.or_tl_result(t, _ptr(out))
+        finally:
+            self.L.or_tl_destroy(t)
+        return float(out[0]), float(out[1])
 
 
 REF_OPS = dict(renew_grid=1, renew_b=2, sr_b=3, push_j=4, drift_n=5, reduce=6,

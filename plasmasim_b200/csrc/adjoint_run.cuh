@@ -1,0 +1,365 @@
+// Host side of the adjoint run (pic_adjoint / pic_objective), included by
+// api.cu after the step functions it reuses.
+//
+// Forward: the loop body of fdtd (:687-949) in slot-stable form: the push is
+// the one-thread-per-particle fused kernel over the slots, sorting is left out
+// (it only reorders particles) and the refill compacts the slots before it
+// appends, so that a particle keeps its slot from one refill to the next and
+// the compaction's slot map is all the reverse pass needs. After every step
+// the objective kernel adds dt * F.
+//
+// Reverse: checkpoint/recompute. The forward sweep keeps the full state every
+// `every` steps; the reverse pass restores each segment's checkpoint, replays
+// its steps while keeping each step's input (particles after the refill, E,
+// B, DB), and then runs the transposed step backwards over the segment. Memory
+// is bounded by (nsteps / every) checkpoints plus `every` step inputs.
+
+struct AdjSnap {
+  long long count[2] = {0, 0};
+  void* part[2] = {nullptr, nullptr};
+  void* planes = nullptr;            // E, B, DB (nine consecutive planes from F_EX)
+  int* map[2] = {nullptr, nullptr};  // the refill's compaction map (old slot -> new slot), or null
+  long long map_n[2] = {0, 0};
+  long long kept[2] = {0, 0};        // slots before the refill's appended particles
+  long long ctr_p = 0, ctr_v = 0;
+  int c_add = 0, c_thrust = 0;
+};
+
+struct AdjRun {
+  std::vector<void*> owned;
+  int* scan_tmp = nullptr;
+  size_t scan_len = 0;
+  void* lam[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [species][buffer]: lx[3] lv[3]
+  int lcur[2] = {0, 0};
+  void* lfield = nullptr;  // lE 3, lDB 3, lJ 3, W 3
+  unsigned long long* j64 = nullptr;  // fixed-point J sums of one species (3 planes)
+  double* acc = nullptr;   // [0] J, [1] dJ/dI, [2] dJ/dV
+};
+
+constexpr int kSnapPlanes = 9;  // F_EX .. F_DBZ
+
+static_assert(F_EY == F_EX + 1 && F_EZ == F_EX + 2 && F_BX == F_EX + 3 && F_DBX == F_EX + 6 &&
+                  F_DBZ == F_EX + 8,
+              "E, B and DB planes are consecutive");
+
+int adj_alloc(pic_ctx* c, AdjRun& R, void** p, size_t bytes) {
+  CK(cudaMalloc(p, bytes < 256 ? 256 : bytes));
+  R.owned.push_back(*p);
+  return PIC_OK;
+}
+
+void adj_free(AdjRun& R) {
+  for (void* p : R.owned) cudaFree(p);
+  R.owned.clear();
+}
+
+// Snapshot memory is returned as soon as a segment is done with it.
+int snap_alloc(pic_ctx* c, void** p, size_t bytes) {
+  CK(cudaMalloc(p, bytes < 256 ? 256 : bytes));
+  return PIC_OK;
+}
+
+void snap_free(AdjSnap& S) {
+  for (int s = 0; s < 2; ++s) {
+    cudaFree(S.part[s]);
+    cudaFree(S.map[s]);
+    S.part[s] = nullptr;
+    S.map[s] = nullptr;
+  }
+  cudaFree(S.planes);
+  S.planes = nullptr;
+}
+
+template <typename real>
+Parts<real> parts_at(void* base, long long cap) {
+  Parts<real> P;
+  char* b = (char*)base;
+  P.cell = (int*)b;
+  char* p = b + align256((size_t)cap * 4);
+  for (int a = 0; a < 3; ++a) {
+    P.o[a] = (real*)p;
+    p += align256((size_t)cap * sizeof(real));
+  }
+  for (int a = 0; a < 3; ++a) {
+    P.v[a] = (real*)p;
+    p += align256((size_t)cap * sizeof(real));
+  }
+  return P;
+}
+
+template <typename real>
+int copy_parts(pic_ctx* c, Parts<real> dst, Parts<real> src, long long n) {
+  if (n <= 0) return PIC_OK;
+  CK(cudaMemcpyAsync(dst.cell, src.cell, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
+  for (int a = 0; a < 3; ++a) {
+    CK(cudaMemcpyAsync(dst.o[a], src.o[a], sizeof(real) * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(dst.v[a], src.v[a], sizeof(real) * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  return PIC_OK;
+}
+
+// The context's particles, fields (E, B, DB), random-stream counters and step
+// counters into a new snapshot.
+template <typename real>
+int adj_save(pic_ctx* c, AdjSnap& S) {
+  for (int s = 0; s < 2; ++s) {
+    S.count[s] = c->sp[s].count;
+    CKR(snap_alloc(c, &S.part[s], store_bytes(S.count[s] > 0 ? S.count[s] : 1, c->rsize)));
+    CKR(copy_parts<real>(c, parts_at<real>(S.part[s], S.count[s] > 0 ? S.count[s] : 1), parts<real>(c, s),
+                         S.count[s]));
+  }
+  CKR(snap_alloc(c, &S.planes, kSnapPlanes * c->plane_bytes));
+  CK(cudaMemcpyAsync(S.planes, (char*)c->field_mem + (size_t)F_EX * c->plane_bytes,
+                     kSnapPlanes * c->plane_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  S.ctr_p = c->ctr_p;
+  S.ctr_v = c->ctr_v;
+  S.c_add = c->c_add;
+  S.c_thrust = c->c_thrust;
+  return PIC_OK;
+}
+
+template <typename real>
+int adj_restore(pic_ctx* c, const AdjSnap& S) {
+  for (int s = 0; s < 2; ++s) {
+    if (S.count[s] > c->sp[s].cap) return PIC_ERR_CAPACITY;
+    CKR(copy_parts<real>(c, parts<real>(c, s), parts_at<real>(S.part[s], S.count[s] > 0 ? S.count[s] : 1),
+                         S.count[s]));
+    CKR(set_count(c, s, S.count[s]));
+    c->tiled[s] = false;
+    c->layout[s] = false;
+  }
+  CK(cudaMemcpyAsync((char*)c->field_mem + (size_t)F_EX * c->plane_bytes, S.planes,
+                     kSnapPlanes * c->plane_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  c->ctr_p = S.ctr_p;
+  c->ctr_v = S.ctr_v;
+  c->c_add = S.c_add;
+  c->c_thrust = S.c_thrust;
+  return PIC_OK;
+}
+
+AdjConst adj_const(const pic_ctx* c, int s) {
+  const pic_config& k = c->cfg;
+  AdjConst a;
+  a.K = (s == 0 ? 1.0 : -1.0) * k.q * species_weight(c) * k.dx * k.dx * k.dx;
+  a.dt = k.dt;
+  a.inv_I = k.coil_i != 0.0 ? 1.0 / k.coil_i : 0.0;
+  a.imf[0] = k.imf_x; a.imf[1] = k.imf_y; a.imf[2] = k.imf_z;
+  a.jsign = s == 0 ? 1.0 : -1.0;
+  return a;
+}
+
+// Removes the empty slots of species s, keeping the order of the rest, and
+// records the slot map in `map` when it is not null.
+template <typename real>
+int adj_compact(pic_ctx* c, AdjRun& R, int s, int* map) {
+  Store& st = c->sp[s];
+  const long long n = st.count;
+  if (n == 0) return PIC_OK;
+  CKR(ensure_flags(c, (size_t)n));
+  live_flag_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s).cell, (int)n, c->flags);
+  CKL();
+  const long long tiles = (n + kScanTile - 1) / kScanTile;
+  if ((size_t)(2 * tiles + 64) > R.scan_len) return PIC_ERR_STATE;
+  CKR(scan_exclusive(c, c->flags, c->pos, n, R.scan_tmp, R.scan_len));
+  compact_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, c->pos,
+                                                                    parts<real>(c, s, 1 - st.cur), map);
+  CKL();
+  int h[2] = {0, 0};
+  CK(cudaMemcpyAsync(&h[0], c->pos + n - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&h[1], c->flags + n - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  st.cur = 1 - st.cur;
+  return set_count(c, s, (long long)h[0] + h[1]);
+}
+
+// One slot-stable loop body; with `rec`, the step input goes into it.
+template <typename real>
+int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
+  CKR(do_renew_grid(c));
+  long long kept[2] = {c->sp[0].count, c->sp[1].count};
+  if (c->c_add > c->cfg.add_interval - 1) {
+    Slab slabs[5];
+    refill_slabs(c, slabs);
+    for (int s = 0; s < 2; ++s) {
+      Store& st = c->sp[s];
+      if (st.count > 0) {
+        delete_shell_kernel<real><<<particle_blocks(st.count), kThreads, 0, c->stream>>>(parts<real>(c, s),
+                                                                                         st.count_dev, c->g);
+        CKL();
+      }
+      int* map = nullptr;
+      if (rec && st.count > 0) {
+        CKR(snap_alloc(c, (void**)&map, sizeof(int) * (size_t)st.count));
+        rec->map[s] = map;
+        rec->map_n[s] = st.count;
+      }
+      CKR(adj_compact<real>(c, R, s, map));
+      kept[s] = st.count;
+      CKR(do_source<real>(c, s, slabs, 5));
+    }
+    c->c_add = 0;
+  }
+  if (rec) {
+    CKR(adj_save<real>(c, *rec));
+    rec->kept[0] = kept[0];
+    rec->kept[1] = kept[1];
+  }
+  CKR(do_renew_b<real>(c));
+  const int nodes = c->g.nodes;
+  Fields<real> F = fields<real>(c);
+  for (int s = 0; s < 2; ++s) {
+    const long long n = c->sp[s].count;
+    if (n == 0) continue;
+    const PushConst<real> pc = push_const<real>(c, s);
+    CK(cudaMemsetAsync(R.j64, 0, sizeof(unsigned long long) * 3 * (size_t)nodes, c->stream));
+    push_fixed_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
+        parts<real>(c, s), (int)n, F, c->g, pc, R.j64, R.j64 + nodes, R.j64 + 2 * (size_t)nodes,
+        (real)(kJFixed / c->cfg.c), c->err);
+    CKL();
+    jconvert_kernel<real><<<grid_blocks(nodes), kThreads, 0, c->stream>>>(
+        R.j64, nodes, F.f[pc.pjx], F.f[pc.pjy], F.f[pc.pjz], c->cfg.q * species_weight(c) * c->cfg.c / kJFixed);
+    CKL();
+  }
+  CKR(do_renew_b<real>(c));
+  CKR(do_fold<real>(c));
+  CKR(do_renew_e<real>(c));
+  for (int s = 0; s < 2; ++s) {
+    const long long n = c->sp[s].count;
+    if (n == 0) continue;
+    objective_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n,
+                                                                          fields<real>(c), c->g,
+                                                                          adj_const(c, s), R.acc);
+    CKL();
+  }
+  c->c_add++;
+  c->c_thrust++;
+  return PIC_OK;
+}
+
+template <typename real>
+AdjPart<real> adj_part(pic_ctx* c, AdjRun& R, int s, int buf) {
+  AdjPart<real> A;
+  const long long cap = c->sp[s].cap;
+  char* p = (char*)R.lam[s][buf];
+  for (int q = 0; q < 3; ++q) { A.lx[q] = (real*)p; p += align256((size_t)cap * sizeof(real)); }
+  for (int q = 0; q < 3; ++q) { A.lv[q] = (real*)p; p += align256((size_t)cap * sizeof(real)); }
+  real* lf = (real*)R.lfield;
+  const size_t pl = c->plane_bytes / sizeof(real);
+  for (int q = 0; q < 3; ++q) {
+    A.le[q] = lf + q * pl;
+    A.ldb[q] = lf + (3 + q) * pl;
+    A.lj[q] = lf + (6 + q) * pl;
+  }
+  return A;
+}
+
+template <typename real>
+AdjField<real> adj_field(pic_ctx* c, AdjRun& R) {
+  AdjField<real> A;
+  real* lf = (real*)R.lfield;
+  const size_t pl = c->plane_bytes / sizeof(real);
+  for (int q = 0; q < 3; ++q) {
+    A.le[q] = lf + q * pl;
+    A.ldb[q] = lf + (3 + q) * pl;
+    A.lj[q] = lf + (6 + q) * pl;
+    A.w[q] = lf + (9 + q) * pl;
+  }
+  return A;
+}
+
+template <typename real>
+PlaneSet<real> plane_set(real* const* p, int n) {
+  PlaneSet<real> s{};
+  for (int q = 0; q < n; ++q) s.p[q] = p[q];
+  s.count = n;
+  return s;
+}
+
+// Transpose of renew_b4_2 + sr_b on (lE, lDB).
+template <typename real>
+int adj_renew_b(pic_ctx* c, AdjRun& R) {
+  AdjField<real> A = adj_field<real>(c, R);
+  const Geom& g = c->g;
+  const double inv_I = c->cfg.coil_i != 0.0 ? 1.0 / c->cfg.coil_i : 0.0;
+  wrap_b_adjoint<real><<<grid_blocks((long long)g.gx * g.gz), kThreads, 0, c->stream>>>(fields<real>(c), A, g, 1,
+                                                                                         inv_I, R.acc);
+  CKL();
+  wrap_b_adjoint<real><<<grid_blocks((long long)g.gy * g.gz), kThreads, 0, c->stream>>>(fields<real>(c), A, g, 0,
+                                                                                         inv_I, R.acc);
+  CKL();
+  BParams p{1. / c->cfg.e0 * c->cfg.dt * 0.5 * 0.5, 0.5 * c->cfg.dt, 1.0 / (24.0 * c->cfg.dx)};
+  const long long nint = (long long)g.nx * g.ny * g.nz;
+  renew_b_adjoint_point<real><<<grid_blocks(nint), kThreads, 0, c->stream>>>(A, g, ramps(c), p);
+  CKL();
+  renew_b_adjoint_curl<real><<<grid_blocks(g.nodes), kThreads, 0, c->stream>>>(A, g);
+  CKL();
+  return PIC_OK;
+}
+
+// Transpose of renew_e4_2 + sr_e and of the sr_current2 fold: lE in, lJ out.
+template <typename real>
+int adj_renew_e(pic_ctx* c, AdjRun& R) {
+  AdjField<real> A = adj_field<real>(c, R);
+  const Geom& g = c->g;
+  wrap_y_adjoint<real><<<grid_blocks((long long)g.gx * g.gz), kThreads, 0, c->stream>>>(plane_set(A.le, 3), g);
+  CKL();
+  wrap_x_adjoint<real><<<grid_blocks((long long)g.gy * g.gz), kThreads, 0, c->stream>>>(plane_set(A.le, 3), g);
+  CKL();
+  CK(cudaMemsetAsync(A.lj[0], 0, 3 * c->plane_bytes, c->stream));
+  EParams p{c->cfg.c * c->cfg.c * c->cfg.dt, c->cfg.mu0, 1.0 / (24.0 * c->cfg.dx)};
+  const long long nint = (long long)g.nx * g.ny * g.nz;
+  renew_e_adjoint_point<real><<<grid_blocks(nint), kThreads, 0, c->stream>>>(A, g, ramps(c), p);
+  CKL();
+  renew_e_adjoint_curl<real><<<grid_blocks(g.nodes), kThreads, 0, c->stream>>>(A, g);
+  CKL();
+  fold_y_adjoint<real><<<grid_blocks((long long)g.gx * g.gz), kThreads, 0, c->stream>>>(plane_set(A.lj, 3), g);
+  CKL();
+  fold_x_adjoint<real><<<grid_blocks((long long)g.gy * g.gz), kThreads, 0, c->stream>>>(plane_set(A.lj, 3), g);
+  CKL();
+  return PIC_OK;
+}
+
+// The transposed step n, given the adjoint of its output state; `in` is the
+// step's recorded input.
+template <typename real>
+int adj_reverse_step(pic_ctx* c, AdjRun& R, const AdjSnap& in) {
+  // the fields the push gathered: E at the step start, B after the first half-step
+  CK(cudaMemcpyAsync((char*)c->field_mem + (size_t)F_EX * c->plane_bytes, in.planes, kSnapPlanes * c->plane_bytes,
+                     cudaMemcpyDeviceToDevice, c->stream));
+  CKR(do_renew_b<real>(c));
+  CKR(adj_renew_e<real>(c, R));
+  CKR(adj_renew_b<real>(c, R));  // second B half-step
+  for (int s = 0; s < 2; ++s) {
+    const long long n = in.count[s];
+    if (n == 0) continue;
+    push_adjoint_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
+        parts_at<real>(in.part[s], n), (int)n, fields<real>(c), c->g, push_const<real>(c, s),
+        adj_part<real>(c, R, s, R.lcur[s]), adj_const(c, s), R.acc);
+    CKL();
+  }
+  CKR(adj_renew_b<real>(c, R));  // first B half-step
+  return PIC_OK;
+}
+
+// Transpose of the refill at the start of the recorded step: the appended
+// particles were created with vz = V + thermal, and the slots before the
+// compaction take the adjoints of their new slots through its map.
+template <typename real>
+int adj_unrefill(pic_ctx* c, AdjRun& R, const AdjSnap& in) {
+  for (int s = 0; s < 2; ++s) {
+    if (in.count[s] > in.kept[s]) {
+      const AdjPart<real> A = adj_part<real>(c, R, s, R.lcur[s]);
+      drift_grad_kernel<real><<<particle_blocks(in.count[s] - in.kept[s]), kThreads, 0, c->stream>>>(
+          parts_at<real>(in.part[s], in.count[s]).cell, A.lv[2], (int)in.kept[s], (int)in.count[s], R.acc);
+      CKL();
+    }
+    if (in.map[s]) {
+      const int nb = 1 - R.lcur[s];
+      uncompact_adjoint_kernel<real><<<grid_blocks(in.map_n[s]), kThreads, 0, c->stream>>>(
+          in.map[s], (int)in.map_n[s], adj_part<real>(c, R, s, R.lcur[s]), adj_part<real>(c, R, s, nb));
+      CKL();
+      R.lcur[s] = nb;
+    }
+  }
+  return PIC_OK;
+}

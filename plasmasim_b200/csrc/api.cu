@@ -17,6 +17,7 @@
 #include "tiled.cuh"
 #include "push_tiled.cuh"
 #include "relayout.cuh"
+#include "adjoint.cuh"
 
 using namespace pb;
 
@@ -814,6 +815,83 @@ int do_set_grid(pic_ctx* c, const double* records) {
   return PIC_OK;
 }
 
+#include "adjoint_run.cuh"
+
+// nsteps slot-stable loop bodies from the current state with the objective;
+// with `grad`, the reverse pass as well. out = {J, dJ/dI, dJ/dV}.
+template <typename real>
+int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
+  AdjRun R;
+  std::vector<AdjSnap> ck;
+  AdjSnap fin;
+  auto run = [&]() -> int {
+    const long long capmax = c->sp[0].cap > c->sp[1].cap ? c->sp[0].cap : c->sp[1].cap;
+    R.scan_len = (size_t)(2 * ((capmax + kScanTile - 1) / kScanTile) + 64);
+    CKR(adj_alloc(c, R, (void**)&R.scan_tmp, sizeof(int) * R.scan_len));
+    CKR(adj_alloc(c, R, (void**)&R.acc, sizeof(double) * 4));
+    CKR(adj_alloc(c, R, (void**)&R.j64, sizeof(unsigned long long) * 3 * (size_t)c->g.nodes));
+    CK(cudaMemsetAsync(R.acc, 0, sizeof(double) * 4, c->stream));
+    // forward sweep, keeping a checkpoint every `every` steps
+    for (int n = 0; n < nsteps; ++n) {
+      if (grad && n % every == 0) {
+        ck.emplace_back();
+        CKR(adj_save<real>(c, ck.back()));
+      }
+      CKR(adj_forward_step<real>(c, R, nullptr));
+    }
+    double h[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(h, R.acc, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out[0] = h[0];
+    if (!grad) return PIC_OK;
+    CKR(adj_save<real>(c, fin));
+    // adjoint state: zero for the final state (the objective terms enter in the reverse kernels)
+    for (int s = 0; s < 2; ++s)
+      for (int b = 0; b < 2; ++b) {
+        const size_t bytes = 6 * align256((size_t)c->sp[s].cap * sizeof(real));
+        CKR(adj_alloc(c, R, &R.lam[s][b], bytes));
+        CK(cudaMemsetAsync(R.lam[s][b], 0, bytes, c->stream));
+      }
+    CKR(adj_alloc(c, R, &R.lfield, 12 * c->plane_bytes));
+    CK(cudaMemsetAsync(R.lfield, 0, 12 * c->plane_bytes, c->stream));
+    CK(cudaMemsetAsync(R.acc, 0, sizeof(double) * 4, c->stream));
+    for (int seg = (int)ck.size() - 1; seg >= 0; --seg) {
+      const int n0 = seg * every, n1 = n0 + every < nsteps ? n0 + every : nsteps;
+      CKR(adj_restore<real>(c, ck[seg]));
+      std::vector<AdjSnap> rec((size_t)(n1 - n0));
+      int rc = PIC_OK;
+      for (int n = n0; n < n1 && rc == PIC_OK; ++n) rc = adj_forward_step<real>(c, R, &rec[n - n0]);
+      for (int n = n1 - 1; n >= n0 && rc == PIC_OK; --n) {
+        rc = adj_reverse_step<real>(c, R, rec[n - n0]);
+        if (rc == PIC_OK) rc = adj_unrefill<real>(c, R, rec[n - n0]);
+      }
+      CK(cudaStreamSynchronize(c->stream));
+      for (auto& S : rec) snap_free(S);
+      if (rc != PIC_OK) return rc;
+    }
+    // the initial particles were created with vz = V + thermal
+    for (int s = 0; s < 2; ++s) {
+      const long long n = ck[0].count[s];
+      if (n == 0) continue;
+      const AdjPart<real> A = adj_part<real>(c, R, s, R.lcur[s]);
+      drift_grad_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
+          parts_at<real>(ck[0].part[s], n).cell, A.lv[2], 0, (int)n, R.acc);
+      CKL();
+    }
+    CK(cudaMemcpyAsync(h, R.acc, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out[1] = h[1];
+    out[2] = h[2];
+    return adj_restore<real>(c, fin);
+  };
+  const int rc = run();
+  cudaStreamSynchronize(c->stream);
+  for (auto& S : ck) snap_free(S);
+  snap_free(fin);
+  adj_free(R);
+  return rc;
+}
+
 // Dispatch on the context's precision.
 #define DISPATCH(c, call)                      \
   ((c)->prec == 64 ? call<double> : call<float>)
@@ -1098,6 +1176,26 @@ int pic_thrust_fave(pic_ctx* c, double* Fave27, int reset) {
   }
   if (reset) CK(cudaMemsetAsync(c->fave, 0, sizeof(double) * 27, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return PIC_OK;
+}
+
+int pic_objective(pic_ctx* c, int nsteps, double* J) {
+  CKR(check_ctx(c));
+  if (!J || nsteps < 0) return PIC_ERR_ARG;
+  if (!c->grid_ready) return PIC_ERR_STATE;
+  double out[3] = {0, 0, 0};
+  CKR(DISPATCH(c, do_adjoint)(c, nsteps, 1, false, out));
+  *J = out[0];
+  return PIC_OK;
+}
+
+int pic_adjoint(pic_ctx* c, int nsteps, int checkpoint_every, double* out3) {
+  CKR(check_ctx(c));
+  if (!out3 || nsteps < 1 || checkpoint_every < 1) return PIC_ERR_ARG;
+  if (!c->grid_ready) return PIC_ERR_STATE;
+  double out[3] = {0, 0, 0};
+  CKR(DISPATCH(c, do_adjoint)(c, nsteps, checkpoint_every, true, out));
+  for (int q = 0; q < 3; ++q) out3[q] = out[q];
   return PIC_OK;
 }
 

@@ -125,6 +125,7 @@ EXPORTED = [
     "pic_set_particles", "pic_get_particles", "pic_particle_count", "pic_get_grid",
     "pic_set_grid", "pic_rng_counters", "pic_status", "pic_synchronize", "pic_get_stream",
     "pic_error_string", "pic_set_timing", "pic_read_timing", "pic_gauss_residual_noalloc",
+    "pic_objective", "pic_adjoint",
 ]
 
 PHASES = ["push", "field", "sort", "add", "diag"]
@@ -154,6 +155,8 @@ def load_library(path: str = LIB_PATH):
     L.pic_thrust_f.argtypes = [vp, _dp, _dp]
     L.pic_thrust_fave.argtypes = [vp, _dp, C.c_int]
     L.pic_gauss_residual.argtypes = [vp, _dp]
+    L.pic_objective.argtypes = [vp, C.c_int, _dp]
+    L.pic_adjoint.argtypes = [vp, C.c_int, C.c_int, _dp]
     L.pic_step.argtypes = [vp, C.c_int]
     L.pic_fdtd.argtypes = [vp, C.c_int]
     L.pic_set_particles.argtypes = [vp, C.c_int, _dp, _ip, C.c_longlong]
@@ -264,6 +267,18 @@ class Pic3D:
         out = np.zeros(4)
         self._call("pic_gauss_residual", _ptr(out))
         return out
+
+    def objective(self, nsteps: int) -> float:
+        """Impulse along z delivered to the dipole over nsteps slot-stable steps."""
+        out = np.zeros(1)
+        self._call("pic_objective", nsteps, _ptr(out))
+        return float(out[0])
+
+    def adjoint(self, nsteps: int, checkpoint_every: int = 20):
+        """(J, dJ/dI, dJ/dV) over nsteps steps by the reverse pass."""
+        out = np.zeros(3)
+        self._call("pic_adjoint", nsteps, checkpoint_every, _ptr(out))
+        return float(out[0]), float(out[1]), float(out[2])
 
     def step(self, nsteps: int = 1):
         self._call("pic_step", nsteps)
