@@ -71,7 +71,8 @@ typedef struct pic_config {
   int sort_interval;       /* fdtd: sorting every sort_interval steps (500, :694) */
   int diag_every_step;     /* 1: thrust_fave sums every step as fdtd does (:926) */
   int reserved0;
-  long long capacity;      /* particle slots per species; 0 picks 1.5x the initial load */
+  long long capacity;      /* particle slots per species; 0 sizes it for the tiled layout:
+                              (1.125 (np + 3 sqrt(np) + 2) + 6) slots per cell + 65536 */
   unsigned long long seed_p; /* position stream key (init_particle_flat :444: 0) */
   unsigned long long seed_v; /* velocity stream key (:445: 50) */
 } pic_config;

@@ -1000,7 +1000,13 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
       return fail(PIC_ERR_CUDA);
   }
   long long cap = k.capacity;
-  if (cap <= 0) cap = (long long)((double)k.np * k.nx * k.ny * k.nz * 1.5) + 65536;
+  if (cap <= 0) {
+    // the tiled layout gives every lane column room for its fullest cell plus
+    // a refill reserve (refill_reserve): about np + 3 sqrt(np) + 2 slots per
+    // cell, plus an eighth, plus 4; a few more for the unplaced tail
+    const double per_cell = 1.125 * (k.np + 3.0 * std::sqrt((double)k.np) + 2.0) + 6.0;
+    cap = (long long)(per_cell * k.nx * k.ny * k.nz) + 65536;
+  }
   if (cap > 0x7fffffffLL) return fail(PIC_ERR_ARG);
   for (int s = 0; s < 2; ++s) {
     c->sp[s].cap = cap;
