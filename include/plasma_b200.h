@@ -206,6 +206,68 @@ int pic_gauss_residual_noalloc(const float *ex, const float *ey, const float *ez
                                double dx, double q, double e0, void *stream, double *out4);
 const char *pic_error_string(int code);
 
+/* ------------------------------------------------------------------------
+ * Batched 2D runs of PIC2D/2d_pic278_mpi.c (the x-z model with the coil's
+ * line currents), MPI size 1: many independent runs of uneven sizes advanced
+ * together on one GPU. The reference runs one such simulation per program
+ * (main :129-188, main_func :201-222, fdtd :527-1019); here a batch replaces
+ * them, each run keeping the reference's step.
+ * ------------------------------------------------------------------------ */
+
+/* Run-time form of the 2D reference's compile-time parameters (:31-87). */
+typedef struct pic2d_config {
+  int nx, nz;              /* Grid_Nx, Grid_Nz (interior cells along x, z) */
+  int np;                  /* Np: Np*Np macro-particles per cell per species */
+  int add_interval;        /* add_ion5 / add_electron5 every add_interval steps (250, :645);
+                              the same for every run of a batch */
+  double dx, dt;           /* dx, dtf (= dti = dte) */
+  double q, mi, me, mu0, e0, kb, c;
+  double v_drift;          /* V: drift along +z */
+  double n_all, ti, te;    /* Nall, Ti, Te; particle weight N0i = N0e = Nall/Np/Np */
+  double coil_i;           /* I: the coil's two line currents +-I/dx^2 (:2238-2268) */
+  double imf_x, imf_y, imf_z;
+  int absorb_grid;         /* Absorb_grid: field damping layer */
+  int absorb_grid2;        /* Absorb_grid2: ballistic particle margin */
+  int absorb_grid3;        /* Absorb_grid3: margin left out of renew_phi's source (>= 2) */
+  int reserved;
+  double sigma_a;          /* damping amplitude a of init_grid (:228) */
+  unsigned long long seed_p, seed_v;  /* position / velocity stream keys (:406-407: 0, 50) */
+  long long capacity;      /* particle slots per species of this run; 0 sizes it */
+} pic2d_config;
+
+typedef struct pic2d_batch pic2d_batch;
+
+/* Normalized-units defaults (c = e0 = mu0 = q = m_e = dx = 1, m_i = 100, dt at
+ * half of the 2D stability limit of the 4th-order stencil), the reference's
+ * absorb widths (32, 16, 32) and refill interval (250). */
+int pic2d_config_normalized(pic2d_config *cfg, int nx, int nz, int np);
+/* precision 32 (FP32 fields and particles, FP64 thrust sums) or 64. */
+int pic2d_create(const pic2d_config *cfgs, int nruns, int precision, int device, pic2d_batch **out);
+int pic2d_destroy(pic2d_batch *b);
+/* init_grid (:224-387) and init_particle (:389-525) of every run, then fdtd's
+ * set-up before its loop (:583-625: density, sr_density, sr_grid, renew_phi). */
+int pic2d_init(pic2d_batch *b);
+/* nsteps bodies of fdtd's loop (:627-1015) for every run; plain steps replay
+ * a captured CUDA graph. */
+int pic2d_step(pic2d_batch *b, int nsteps);
+/* thrust_F (:2304-2387) of every run: out3[3 r + {0, 1, 2}] = Fx, Fz, My. */
+int pic2d_thrust(pic2d_batch *b, double *out3);
+int pic2d_particle_count(pic2d_batch *b, int run, int species, long long *n);
+/* Rows x z vx vy vz n (FP64, absolute positions with ghost cells). */
+int pic2d_get_particles(pic2d_batch *b, int run, int species, double *rows6, long long cap, long long *n);
+/* The run's grid as the reference's Grid records (:104-112: b0x b0y b0z bx by
+ * bz ex ey ez jix0 jiy0 jiz0 jex0 jey0 jez0 ni ne phi), (nx+4)*(nz+4) nodes,
+ * z fastest. */
+int pic2d_get_grid(pic2d_batch *b, int run, double *records);
+/* No counterpart in the reference. Tunes the push launch shape on the batch's
+ * next steps (ordinary steps of the runs); choice2 = {block size, blocks}. */
+int pic2d_autotune(pic2d_batch *b, int *choice2);
+int pic2d_set_graph(pic2d_batch *b, int enable);
+/* counters8: [0..2] device errors as pic_status, [3] particle pushes,
+ * [4] steps taken, [5] kernels launched. */
+int pic2d_status(pic2d_batch *b, long long *counters8);
+int pic2d_get_stream(pic2d_batch *b, void **stream);
+
 #ifdef __cplusplus
 }
 #endif

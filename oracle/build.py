@@ -71,6 +71,61 @@ REF_CONFIGS = {
 }
 
 
+# The 2D reference (PIC2D/2d_pic278_mpi.c) in normalized units: c = e0 = mu0 =
+# q = m_e = dx = 1, m_i = 100; dt at half of the 2D stability limit of the
+# (27/24, -1/24) stencil, 6/(7 sqrt 2) dx/c; drift 0.1 c, v_th,e = 0.05 c.
+REF2D_SRC = os.path.join(REF_ROOT, "PIC2D", "2d_pic278_mpi.c")
+DT2D_NORM = 0.5 * 6.0 / (7.0 * math.sqrt(2.0))
+NORMALIZED_2D = dict(
+    ORACLE_Q=1.0, ORACLE_MI=100.0, ORACLE_ME=1.0, ORACLE_MU0=1.0, ORACLE_E0=1.0, ORACLE_KB=1.0,
+    ORACLE_C=1.0, ORACLE_DX=1.0, ORACLE_DT=DT2D_NORM, ORACLE_V=0.1, ORACLE_NALL=0.01,
+    ORACLE_TI=0.0025, ORACLE_TE=0.0025, ORACLE_R=2.0, ORACLE_I=12.0, ORACLE_ALPHA=0.0,
+    ORACLE_SIGMA_A=1e-6,
+)
+
+
+def _geom2d(nx, nz, np_, absorb, absorb2, absorb3, pack=20000):
+    return dict(ORACLE_NX=nx, ORACLE_NZ=nz, ORACLE_NP=np_, ORACLE_ABSORB=absorb,
+                ORACLE_ABSORB2=absorb2, ORACLE_ABSORB3=absorb3, ORACLE_PACK_N=pack)
+
+
+REF2D_CONFIGS = {
+    # a small strip: 16 x 32 cells, 2 x 2 particles per cell per species
+    "strip": {**NORMALIZED_2D, **_geom2d(16, 32, 2, 4, 2, 4)},
+    # 64 x 64 cells, 4 x 4 particles per cell: a batch run of the smallest size
+    "sq64": {**NORMALIZED_2D, **_geom2d(64, 64, 4, 8, 4, 8)},
+    # 32 x 128 cells, 3 x 3 particles per cell, a different current and drift
+    "rect": {**NORMALIZED_2D, **_geom2d(32, 128, 3, 6, 3, 6), "ORACLE_I": 20.0, "ORACLE_V": 0.15},
+}
+
+
+def ref2d_lib_path(name: str) -> str:
+    return os.path.join(REF_OUT, f"libref2d_{name}.so")
+
+
+def build_ref2d(name: str, force: bool = False) -> str:
+    """Compile the 2D reference at geometry ``name`` (size-1 MPI and GSL-subset
+    shims, harness oracle/ref2d_harness.c); returns the library path."""
+    out = ref2d_lib_path(name)
+    if os.path.isfile(out) and not force:
+        return out
+    if not os.path.isfile(REF2D_SRC):
+        raise FileNotFoundError(f"2D reference source not found at {REF2D_SRC}")
+    os.makedirs(REF_OUT, exist_ok=True)
+    defs = [f"-D{k}={_fmt(v)}" for k, v in REF2D_CONFIGS[name].items()]
+    sed = subprocess.run(["sed", "-f", os.path.join(HERE, "ref2d_patch.sed"), REF2D_SRC],
+                         check=True, capture_output=True)
+    with open(os.path.join(HERE, "ref2d_harness.c"), "rb") as f:
+        tu = sed.stdout + b"\n" + f.read()
+    cmd = ["gcc", "-x", "c", "-", "-x", "none",
+           os.path.join(HERE, "shim", "gsl_shim.c"), os.path.join(HERE, "shim", "mpi_shim.c"),
+           "-std=gnu11", "-O2", "-ffp-contract=off", "-fgnu89-inline", "-fPIC", "-shared", "-w",
+           "-I", os.path.join(HERE, "shim"), "-include", os.path.join(HERE, "ref_pre.h"),
+           *defs, "-lm", "-o", out]
+    subprocess.run(cmd, input=tu, check=True)
+    return out
+
+
 def ref_lib_path(name: str) -> str:
     return os.path.join(REF_OUT, f"libref3d_{name}.so")
 
@@ -127,6 +182,9 @@ def build_all(force: bool = False) -> None:
     if reference_available():
         for name in REF_CONFIGS:
             build_ref(name, force)
+    if os.path.isfile(REF2D_SRC):
+        for name in REF2D_CONFIGS:
+            build_ref2d(name, force)
 
 
 if __name__ == "__main__":

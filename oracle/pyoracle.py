@@ -315,3 +315,66 @@ class Reference:
         out = np.zeros(27)
         self.L.ref_fave(_ptr(out))
         return out
+
+
+GRID2D_FIELDS = ["b0x", "b0y", "b0z", "bx", "by", "bz", "ex", "ey", "ez",
+                 "jix", "jiy", "jiz", "jex", "jey", "jez", "ni", "ne", "phi"]
+F2 = {name: i for i, name in enumerate(GRID2D_FIELDS)}
+
+
+class Reference2D:
+    """The 2D reference program (PIC2D/2d_pic278_mpi.c) compiled at one
+    geometry by oracle/build.py, driven through oracle/ref2d_harness.c. Its
+    state is process-global: use one instance per process (or per test that
+    re-initialises it). Particle rows: x, z, vx, vy, vz, n."""
+
+    def __init__(self, name: str):
+        path = _build.ref2d_lib_path(name)
+        if not os.path.isfile(path):
+            _build.build_ref2d(name)
+        L = C.CDLL(path)
+        L.ref2d_grid_nodes.restype = C.c_long
+        L.ref2d_get_grid.argtypes = [_dp]
+        L.ref2d_set_grid.argtypes = [_dp]
+        L.ref2d_count.restype = C.c_long
+        L.ref2d_count.argtypes = [C.c_int]
+        L.ref2d_get_particles.restype = C.c_long
+        L.ref2d_get_particles.argtypes = [C.c_int, _dp, _ip, C.c_long]
+        L.ref2d_step.argtypes = [C.c_int]
+        L.ref2d_thrust.argtypes = [_dp]
+        L.ref2d_sinft.argtypes = [C.c_int, _dp]
+        L.ref2d_dims.argtypes = [_ip]
+        self.L = L
+        d = np.zeros(10, dtype=np.int32)
+        L.ref2d_dims(_ptr(d, _ip))
+        self.nx, self.nz, self.np = int(d[0]), int(d[1]), int(d[2])
+        self.shape = (self.nx + 4, self.nz + 4)
+        self.params = dict(_build.REF2D_CONFIGS[name])
+
+    def init(self):
+        self.L.ref2d_init()
+
+    def step(self, add_every=250):
+        self.L.ref2d_step(add_every)
+
+    def grid(self) -> np.ndarray:
+        g = np.zeros(self.shape + (18,), dtype=np.float64)
+        self.L.ref2d_get_grid(_ptr(g))
+        return g
+
+    def particles(self, species: int):
+        n = self.L.ref2d_count(species)
+        rows = np.zeros((max(n, 1), 6))
+        flag = np.zeros(max(n, 1), dtype=np.int32)
+        self.L.ref2d_get_particles(species, _ptr(rows), _ptr(flag, _ip), n)
+        return rows[:n], flag[:n]
+
+    def thrust(self) -> np.ndarray:
+        out = np.zeros(3)
+        self.L.ref2d_thrust(_ptr(out))
+        return out
+
+    def sinft(self, y) -> np.ndarray:
+        y = np.array(y, dtype=np.float64)
+        self.L.ref2d_sinft(len(y), _ptr(y))
+        return y

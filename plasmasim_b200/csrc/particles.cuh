@@ -470,7 +470,7 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
-__global__ void __launch_bounds__(kScanThreads) scan_tile_kernel(const int* __restrict__ in, int* out,
+static __global__ void __launch_bounds__(kScanThreads) scan_tile_kernel(const int* __restrict__ in, int* out,
                                                                  int* sums, long long n) {
   __shared__ int warp_tot[32];
   const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
@@ -509,7 +509,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_tile_kernel(const int* __re
   if (threadIdx.x == kScanThreads - 1) sums[blockIdx.x] = run;
 }
 
-__global__ void scan_add_kernel(int* out, const int* __restrict__ add, long long n) {
+static __global__ void scan_add_kernel(int* out, const int* __restrict__ add, long long n) {
   const long long base = (long long)blockIdx.x * kScanTile;
   const int a = add[blockIdx.x];
   for (int q = threadIdx.x; q < kScanTile; q += blockDim.x) {

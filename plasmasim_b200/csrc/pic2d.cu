@@ -1,0 +1,1577 @@
+// Batched 2D particle-in-cell runs of PIC2D/2d_pic278_mpi.c (the x-z sail
+// model) at MPI size 1: many independent runs of uneven grid sizes advanced
+// together, every phase of the step one batched kernel over all runs, the
+// step replayed from CUDA graphs.
+//
+// Per run the step is fdtd's loop body (:627-1015): renew_grid; add_ion5 /
+// add_electron5 every add_interval steps (:645-653, :3311-3566); renew_b4
+// (:1391-1417) + sr_grid; the push loop (cal_track_c4 :1520-1560 with the
+// bilinear gathers :1948-2016, the ballistic margins :682-686, the J deposit
+// :2018-2145); sr_current (:1073-1144) and external_current_perp (:2238-2268);
+// renew_b4 + sr_grid; the drift loop with the density deposit (:762-828) and
+// sr_density (:1146-1209); renew_e4 (:1419-1449) + sr_grid; renew_phi
+// (:2589-2771) + sr_grid; the x exchange and the removal (:861-960).
+// thrust_F (:2304-2387) on request.
+//
+// Layout: runs are concatenated. Fields: per run 18 planes of (nx+4)(nz+4)
+// nodes, z fastest. Particles: per species one pool, run r owning slots
+// [poff_r, poff_r + cap_r): cell (i << 16 | k), the in-cell offsets along x
+// and z, and vx vy vz. Work lists map persistent blocks onto (run, chunk)
+// items so that one launch covers every run whatever its size.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/plasma_b200.h"
+#include "common.cuh"
+#include "particles.cuh"
+
+using namespace pb;
+
+namespace p2 {
+
+enum Plane {
+  P_EX, P_EY, P_EZ, P_BX, P_BY, P_BZ, P_B0X, P_B0Y, P_B0Z,
+  P_JIX, P_JIY, P_JIZ, P_JEX, P_JEY, P_JEZ, P_NI, P_NE, P_PHI, P_COUNT
+};
+
+constexpr int kChunk = 2048;     // particle slots per work item
+constexpr int kCellShift = 16;   // cell = (i << 16) | k
+
+__host__ __device__ __forceinline__ int pack2(int i, int k) { return (i << kCellShift) | k; }
+__host__ __device__ __forceinline__ void unpack2(int c, int& i, int& k) {
+  i = c >> kCellShift;
+  k = c & ((1 << kCellShift) - 1);
+}
+
+// Constant description of one run on the device.
+template <typename real>
+struct Run {
+  int nx, nz, gx, gz, nodes;
+  int np;                 // particles per cell per axis (Np); Np*Np per cell
+  long long foff;         // first node of the run's field block (18 planes)
+  long long poff;         // first slot in each species pool
+  long long cap;          // slots per species
+  int a1, a2, a3;         // Absorb_grid (fields), Absorb_grid2 (particles), Absorb_grid3 (phi)
+  double dx, dt, q, e0, mu0, c;
+  double sigma_a;
+  double coil_i;
+  double vdrift, sig[2];  // drift and thermal spread per species
+  double nw;              // N0i = N0e = Nall / Np / Np
+  double T[2];            // 0.5 q dt / m, m < 0 for electrons
+  double ex_add, ey_add;  // V IMF_y, -V IMF_x
+  unsigned long long seed_p, seed_v;
+  int add_interval;
+  int sz_dst;             // offset of the run's sine tables (Nx then Nz)
+  long long roff;         // offset of the run's Poisson buffers (nx * nz)
+};
+
+struct Pools {
+  int* cell[2];
+  void* o[2][2];  // [species][axis x, z]
+  void* v[2][3];
+};
+
+template <typename real>
+struct PView {
+  int* cell;
+  real* ox;
+  real* oz;
+  real* vx;
+  real* vy;
+  real* vz;
+};
+
+template <typename real>
+__device__ __forceinline__ PView<real> pview(const Pools& P, int s) {
+  PView<real> v;
+  v.cell = P.cell[s];
+  v.ox = (real*)P.o[s][0];
+  v.oz = (real*)P.o[s][1];
+  v.vx = (real*)P.v[s][0];
+  v.vy = (real*)P.v[s][1];
+  v.vz = (real*)P.v[s][2];
+  return v;
+}
+
+// Mutable per-run device state.
+struct State {
+  int count[2];
+  int live[2];
+  unsigned long long ctr_p, ctr_v;  // random-stream draw counters
+  double thrust[3];                 // Fx, Fz, My of the last pic2d_thrust
+};
+
+// ------------------------------------------------------------ helpers
+__device__ __forceinline__ double ramp2(int idx, int n, int absorb) {
+  if (idx - 4 <= 2 * absorb) return (2 * absorb - (idx - 4)) / 4.;
+  if (idx - 4 >= 2 * n - 2 * absorb) return ((idx - 4) - (2 * n - 2 * absorb)) / 4.;
+  return 0.;
+}
+
+// init_grid's damping profile (:252-276) on the doubled grid.
+__device__ __forceinline__ double sigma2(double a, int kk, int mm, int nx, int nz, int absorb) {
+  const double x = ramp2(kk, nx, absorb), z = ramp2(mm, nz, absorb);
+  return a * (0.1 * sqrt(pow(x, 4) + pow(z, 4)) + 0.01 * sqrt(pow(x, 12) + pow(z, 12)));
+}
+
+template <typename real>
+__device__ __forceinline__ real* plane(real* F, const Run<real>& R, int p) {
+  return F + R.foff + (long long)p * R.nodes;
+}
+
+// Work item lists: run index and a first row/slot per item.
+struct Item {
+  int run;
+  int first;
+};
+
+// ------------------------------------------------------------ grid
+// renew_b4 (:1391-1417) on the interior of every run; item = (run, row k).
+template <typename real>
+__global__ void renew_b4_kernel(real* F, const Run<real>* __restrict__ runs, const Item* __restrict__ items, int nitems) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Run<real> R = runs[items[it].run];
+    const int k = items[it].first;
+    const real* ex = plane(F, R, P_EX);
+    const real* ey = plane(F, R, P_EY);
+    const real* ez = plane(F, R, P_EZ);
+    real* bx = plane(F, R, P_BX);
+    real* by = plane(F, R, P_BY);
+    real* bz = plane(F, R, P_BZ);
+    const real* b0x = plane(F, R, P_B0X);
+    const real* b0y = plane(F, R, P_B0Y);
+    const real* b0z = plane(F, R, P_B0Z);
+    const int G = R.gz;
+    const double t = 1. / R.e0 * R.dt * 0.5 * 0.5;
+    for (int m = 2 + threadIdx.x; m < R.nz + 2; m += blockDim.x) {
+      const int n = k * G + m;
+      double s = sigma2(R.sigma_a, 2 * k + 1, 2 * m, R.nx, R.nz, R.a1);
+      bx[n] = (real)((double)b0x[n] + (1. - s * t) / (1. + s * t) * ((double)bx[n] - (double)b0x[n]) +
+                     0.5 * R.dt / (1. + s * t) * (1. / 24.) *
+                         (27. * ((double)ey[n] - (double)ey[n - 1]) - ((double)ey[n + 1] - (double)ey[n - 2])) / R.dx);
+      s = sigma2(R.sigma_a, 2 * k, 2 * m, R.nx, R.nz, R.a1);
+      by[n] = (real)((double)b0y[n] + (1. - s * t) / (1. + s * t) * ((double)by[n] - (double)b0y[n]) -
+                     R.dt * 0.5 / (1. + s * t) *
+                         ((1. / 24.) * (27. * ((double)ex[n] - (double)ex[n - 1]) - ((double)ex[n + 1] - (double)ex[n - 2])) / R.dx -
+                          (1. / 24.) * (27. * ((double)ez[n] - (double)ez[n - G]) - ((double)ez[n + G] - (double)ez[n - 2 * G])) / R.dx));
+      s = sigma2(R.sigma_a, 2 * k, 2 * m + 1, R.nx, R.nz, R.a1);
+      bz[n] = (real)((double)b0z[n] + (1. - s * t) / (1. + s * t) * ((double)bz[n] - (double)b0z[n]) -
+                     R.dt * 0.5 / (1. + s * t) * (1. / 24.) *
+                         (27. * ((double)ey[n] - (double)ey[n - G]) - ((double)ey[n + G] - (double)ey[n - 2 * G])) / R.dx);
+    }
+  }
+}
+
+// renew_e4 (:1419-1449); item = (run, row k).
+template <typename real>
+__global__ void renew_e4_kernel(real* F, const Run<real>* __restrict__ runs, const Item* __restrict__ items, int nitems) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Run<real> R = runs[items[it].run];
+    const int k = items[it].first;
+    real* ex = plane(F, R, P_EX);
+    real* ey = plane(F, R, P_EY);
+    real* ez = plane(F, R, P_EZ);
+    const real* bx = plane(F, R, P_BX);
+    const real* by = plane(F, R, P_BY);
+    const real* bz = plane(F, R, P_BZ);
+    const real* b0x = plane(F, R, P_B0X);
+    const real* b0y = plane(F, R, P_B0Y);
+    const real* b0z = plane(F, R, P_B0Z);
+    const real* jix = plane(F, R, P_JIX);
+    const real* jiy = plane(F, R, P_JIY);
+    const real* jiz = plane(F, R, P_JIZ);
+    const real* jex = plane(F, R, P_JEX);
+    const real* jey = plane(F, R, P_JEY);
+    const real* jez = plane(F, R, P_JEZ);
+    const int G = R.gz;
+    const double cc = R.c * R.c * R.dt;
+    auto dby = [&](int n) { return (double)by[n] - (double)b0y[n]; };
+    auto dbx = [&](int n) { return (double)bx[n] - (double)b0x[n]; };
+    auto dbz = [&](int n) { return (double)bz[n] - (double)b0z[n]; };
+    for (int m = 2 + threadIdx.x; m < R.nz + 2; m += blockDim.x) {
+      const int n = k * G + m;
+      double s = sigma2(R.sigma_a, 2 * k, 2 * m + 1, R.nx, R.nz, R.a1);
+      double h = 0.5 * R.mu0 * s * cc;
+      ex[n] = (real)((1. - h) / (1. + h) * (double)ex[n] +
+                     cc / (1. + h) *
+                         (-1. / 24. * (27. * (dby(n + 1) - dby(n)) - (dby(n + 2) - dby(n - 1))) / R.dx -
+                          R.mu0 * ((double)jix[n] - (double)jex[n])));
+      s = sigma2(R.sigma_a, 2 * k + 1, 2 * m, R.nx, R.nz, R.a1);
+      h = 0.5 * R.mu0 * s * cc;
+      ez[n] = (real)((1. - h) / (1. + h) * (double)ez[n] +
+                     cc / (1. + h) *
+                         (1. / 24. * (27. * (dby(n + G) - dby(n)) - (dby(n + 2 * G) - dby(n - G))) / R.dx -
+                          R.mu0 * ((double)jiz[n] - (double)jez[n])));
+      s = sigma2(R.sigma_a, 2 * k + 1, 2 * m + 1, R.nx, R.nz, R.a1);
+      h = 0.5 * R.mu0 * s * cc;
+      ey[n] = (real)((1. - h) / (1. + h) * (double)ey[n] +
+                     cc / (1. + h) *
+                         (1. / 24. * (27. * (dbx(n + 1) - dbx(n)) - (dbx(n + 2) - dbx(n - 1))) / R.dx -
+                          1. / 24. * (27. * (dbz(n + G) - dbz(n)) - (dbz(n + 2 * G) - dbz(n - G))) / R.dx -
+                          R.mu0 * ((double)jiy[n] - (double)jey[n])));
+    }
+  }
+}
+
+// sr_grid at size 1 (:1021-1071): columns 0,1 <- N, N+1 and N+2, N+3 <- 2, 3
+// of every plane (the whole Grid record); one block per run.
+template <typename real>
+__global__ void sr_grid_kernel(real* F, const Run<real>* __restrict__ runs, int nruns) {
+  for (int r = blockIdx.x; r < nruns; r += gridDim.x) {
+    const Run<real> R = runs[r];
+    const int G = R.gz, N = R.nx;
+    for (int q = threadIdx.x; q < P_COUNT * G; q += blockDim.x) {
+      real* a = plane(F, R, q / G);
+      const int m = q % G;
+      const real v0 = a[N * G + m], v1 = a[(N + 1) * G + m], v2 = a[2 * G + m], v3 = a[3 * G + m];
+      a[m] = v0;
+      a[G + m] = v1;
+      a[(N + 2) * G + m] = v2;
+      a[(N + 3) * G + m] = v3;
+    }
+  }
+}
+
+// sr_current / sr_density at size 1 (:1073-1209): column 2 += column N+2,
+// column N+1 += column 1, for planes [p0, p0 + np).
+template <typename real>
+__global__ void fold_kernel(real* F, const Run<real>* __restrict__ runs, int nruns, int p0, int np) {
+  for (int r = blockIdx.x; r < nruns; r += gridDim.x) {
+    const Run<real> R = runs[r];
+    const int G = R.gz, N = R.nx;
+    for (int q = threadIdx.x; q < np * G; q += blockDim.x) {
+      real* a = plane(F, R, p0 + q / G);
+      const int m = q % G;
+      a[2 * G + m] += a[(N + 2) * G + m];
+      a[(N + 1) * G + m] += a[G + m];
+    }
+  }
+}
+
+// external_current_perp (:2238-2268) at rank p/2 = 0: the coil's two line
+// currents, ramped up over the first 10000 steps.
+template <typename real>
+__global__ void coil_kernel(real* F, const Run<real>* __restrict__ runs, int nruns, const int* __restrict__ step) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nruns) return;
+  const Run<real> R = runs[r];
+  const int c = *step;
+  const double Pi = 3.14159265358979323846;
+  const double w = Pi / 10000.;
+  real* jiy = plane(F, R, P_JIY);
+  const int G = R.gz;
+  const int lo = 3 * G + (R.nz + 4) / 2 - 3, hi = 3 * G + (R.nz + 4) / 2 + 2;
+  if (c < 10000) {
+    jiy[lo] = (real)(-R.coil_i / R.dx / R.dx * (1. + cos(w * c - Pi)) / 2.);
+    jiy[hi] = (real)(R.coil_i / R.dx / R.dx * (1. + cos(w * c - Pi)) / 2.);
+  } else {
+    jiy[lo] = (real)(-R.coil_i / R.dx / R.dx);
+    jiy[hi] = (real)(R.coil_i / R.dx / R.dx);
+  }
+}
+
+// renew_grid (:1348-1389): J, n and phi of every run to zero (the last nine
+// planes of each run's block); one block per run.
+template <typename real>
+__global__ void zero_sources_kernel(real* F, const Run<real>* __restrict__ runs, int nruns) {
+  for (int r = blockIdx.x; r < nruns; r += gridDim.x) {
+    const Run<real> R = runs[r];
+    real* base = F + R.foff + (long long)P_JIX * R.nodes;
+    const long long n = (long long)(P_COUNT - P_JIX) * R.nodes;
+    for (long long q = threadIdx.x; q < n; q += blockDim.x) base[q] = (real)0;
+  }
+}
+
+__global__ void step_advance_kernel(int* step) { *step += 1; }
+
+// ------------------------------------------------------------ particles
+// Bilinear weights of one axis in cell units (shape_func_*3, :1948-2016):
+// node-aligned base i with (1 - f, f); half-shifted base (int)(x - 0.5).
+template <typename real>
+struct Ax2 {
+  int a, b;
+  real a0, a1, b0, b1;
+};
+
+template <typename real>
+__device__ __forceinline__ Ax2<real> ax2(int i, real f) {
+  Ax2<real> w;
+  w.a = i;
+  w.a1 = f;
+  w.a0 = (real)1 - f;
+  const bool up = f >= (real)0.5 || i == 0;
+  w.b = up ? i : i - 1;
+  w.b1 = up ? f - (real)0.5 : f + (real)0.5;
+  w.b0 = (real)1 - w.b1;
+  return w;
+}
+
+template <typename real>
+__device__ __forceinline__ real bil(const real* P, int G, int i, int k, real x0, real x1, real z0, real z1) {
+  return (P[i * G + k] * (x0 * z0) + P[(i + 1) * G + k] * (x1 * z0)) +
+         (P[i * G + k + 1] * (x0 * z1) + P[(i + 1) * G + k + 1] * (x1 * z1));
+}
+
+template <typename real>
+__device__ __forceinline__ void dep4(real* P, int G, int i, int k, real v, real x0, real x1, real z0, real z1) {
+  atomicAdd(P + i * G + k, v * (x0 * z0));
+  atomicAdd(P + (i + 1) * G + k, v * (x1 * z0));
+  atomicAdd(P + i * G + k + 1, v * (x0 * z1));
+  atomicAdd(P + (i + 1) * G + k + 1, v * (x1 * z1));
+}
+
+// The particle part of one step for every run and species (the push loop,
+// the drift loop and the x exchange + removal in one pass). item = (run*2 +
+// species, first slot relative to the run).
+template <typename real, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, const Run<real>* __restrict__ runs,
+                                                       const State* __restrict__ st, const Item* __restrict__ items,
+                                                       int nitems, int chunk, unsigned long long* err) {
+  unsigned pushed = 0;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int rs = items[it].run;
+    const int r = rs >> 1, s = rs & 1;
+    const Run<real> R = runs[r];
+    const int n = st[r].count[s];
+    const int first = items[it].first;
+    if (first >= n) continue;
+    const int last = min(first + chunk, n);
+    const PView<real> P = pview<real>(pools, s);
+    const int G = R.gz;
+    const real T = (real)R.T[s];
+    const real hdt = (real)(0.5 * R.dt / R.dx);
+    const real qn = (real)(R.q * R.nw);
+    const real nw = (real)R.nw;
+    real* jx = plane(F, R, s == 0 ? P_JIX : P_JEX);
+    real* jy = plane(F, R, s == 0 ? P_JIY : P_JEY);
+    real* jz = plane(F, R, s == 0 ? P_JIZ : P_JEZ);
+    real* dn = plane(F, R, s == 0 ? P_NI : P_NE);
+    const real* Ex = plane(F, R, P_EX);
+    const real* Ey = plane(F, R, P_EY);
+    const real* Ez = plane(F, R, P_EZ);
+    const real* Bx = plane(F, R, P_BX);
+    const real* By = plane(F, R, P_BY);
+    const real* Bz = plane(F, R, P_BZ);
+    for (int q = first + threadIdx.x; q < last; q += BLOCK) {
+      const long long t = R.poff + q;
+      const int c = P.cell[t];
+      if (c < 0) continue;
+      ++pushed;
+      int i, k;
+      unpack2(c, i, k);
+      real fx = P.ox[t], fz = P.oz[t];
+      real vx = P.vx[t], vy = P.vy[t], vz = P.vz[t];
+      // ballistic margins (:682-686): z < A2, z > Nz+4-A2, x < A2, x > Nx+4-A2 (cells)
+      const int hz = R.nz + 4 - R.a2, hx = R.nx + 4 - R.a2;
+      const bool bal = k < R.a2 || i < R.a2 || k > hz || (k == hz && fz > (real)0) || i > hx ||
+                       (i == hx && fx > (real)0);
+      if (!bal) {
+        if (i < 1 || k < 1 || i > R.gx - 2 || k > R.gz - 2) {
+          atomicAdd(err + ERR_DEPOSIT_OOB, 1ull);
+        } else {
+          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+          // ex, bz: x aligned, z shifted; ez, bx: x shifted, z aligned; ey: both shifted; by: both aligned
+          real ex = bil(Ex, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1) + (real)R.ex_add;
+          real bz = bil(Bz, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
+          real ey = bil(Ey, G, X.b, Z.b, X.b0, X.b1, Z.b0, Z.b1) + (real)R.ey_add;
+          real ez = bil(Ez, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
+          real bx = bil(Bx, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
+          real by = bil(By, G, X.a, Z.a, X.a0, X.a1, Z.a0, Z.a1);
+          // cal_track_c4 (:1520-1560)
+          const real S = (real)2 * T / ((real)1 + T * T * (bx * bx + by * by + bz * bz));
+          const real ux = vx + ex * T, uy = vy + ey * T, uz = vz + ez * T;
+          const real uox = ux + T * (uy * bz - uz * by);
+          const real uoy = uy + T * (uz * bx - ux * bz);
+          const real uoz = uz + T * (ux * by - uy * bx);
+          vx = ux + S * (uoy * bz - uoz * by) + ex * T;
+          vy = uy + S * (uoz * bx - uox * bz) + ey * T;
+          vz = uz + S * (uox * by - uoy * bx) + ez * T;
+        }
+      }
+      advance(i, fx, vx * hdt);
+      advance(k, fz, vz * hdt);
+      // J deposit at x^{n+1/2} for dx <= x < (Nx+3) dx, 2 dx <= z < (Nz+2) dx
+      if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
+        const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+        dep4(jx, G, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1);
+        dep4(jy, G, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1);
+        dep4(jz, G, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1);
+      }
+      advance(i, fx, vx * hdt);
+      advance(k, fz, vz * hdt);
+      if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
+        const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+        dep4(dn, G, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1);
+      }
+      // x exchange at size 1: forward crossers wrap, backward ones are dropped; then removal
+      if (i == R.nx + 2 && k >= 2 && k < R.nz + 2) i -= R.nx;
+      const bool keep = i >= 2 && i < R.nx + 2 && k >= 2 && k < R.nz + 2;
+      P.cell[t] = keep ? pack2(i, k) : -1;
+      P.ox[t] = fx; P.oz[t] = fz;
+      P.vx[t] = vx; P.vy[t] = vy; P.vz[t] = vz;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
+  if ((threadIdx.x & 31) == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
+}
+
+// Density deposit of every particle (fdtd's set-up, :583-607).
+template <typename real>
+__global__ void density2d_kernel(Pools pools, real* F, const Run<real>* __restrict__ runs, const State* __restrict__ st,
+                                 const Item* __restrict__ items, int nitems, int chunk) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int rs = items[it].run;
+    const int r = rs >> 1, s = rs & 1;
+    const Run<real> R = runs[r];
+    const int n = st[r].count[s];
+    const int first = items[it].first;
+    if (first >= n) continue;
+    const int last = min(first + chunk, n);
+    const PView<real> P = pview<real>(pools, s);
+    real* dn = plane(F, R, s == 0 ? P_NI : P_NE);
+    for (int q = first + threadIdx.x; q < last; q += blockDim.x) {
+      const long long t = R.poff + q;
+      const int c = P.cell[t];
+      if (c < 0) continue;
+      int i, k;
+      unpack2(c, i, k);
+      if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
+        const Ax2<real> X = ax2(i, P.ox[t]), Z = ax2(k, P.oz[t]);
+        dep4(dn, R.gz, X.b, Z.b, (real)R.nw, X.b0, X.b1, Z.b0, Z.b1);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ sources
+// A source block: `count` particles uniform in [x0, x1) x [z0, z1) (absolute
+// units), drifting Maxwellian, drawing x, z from the position stream and vx,
+// vz (two normals, vy = 0) from the velocity stream, in order.
+struct Slab2 {
+  double x0, x1, z0, z1;
+  long long count;
+};
+
+struct SourceSet {
+  Slab2 slab[4];
+  int nslab;
+  long long total;
+};
+
+// Particles of species s for every run: slab blocks of run r appended after
+// the run's current count; the stream counters advance by 2 and 4 draws per
+// particle. item = (run, first particle index of the source set).
+template <typename real>
+__global__ void source2d_kernel(Pools pools, const Run<real>* __restrict__ runs, State* st, const SourceSet* __restrict__ sets,
+                                const Item* __restrict__ items, int nitems, int chunk, int s, unsigned long long* err) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int r = items[it].run;
+    const Run<real> R = runs[r];
+    const SourceSet S = sets[r];
+    const long long first = items[it].first;
+    const long long last = min(first + (long long)chunk, S.total);
+    const PView<real> P = pview<real>(pools, s);
+    const int base = st[r].count[s];
+    const unsigned long long bp = st[r].ctr_p, bv = st[r].ctr_v;
+    for (long long j = first + threadIdx.x; j < last; j += blockDim.x) {
+      if (base + j >= R.cap) {
+        atomicAdd(err + ERR_CELL_RANGE, 1ull);
+        continue;
+      }
+      long long rem = j;
+      int q = 0;
+      while (q < S.nslab - 1 && rem >= S.slab[q].count) rem -= S.slab[q].count, ++q;
+      const Slab2& sl = S.slab[q];
+      const double x = flat_rn(sl.x0, sl.x1, uniform53(R.seed_p, bp + 2 * j));
+      const double z = flat_rn(sl.z0, sl.z1, uniform53(R.seed_p, bp + 2 * j + 1));
+      const double vx = R.sig[s] * gauss_bm(R.seed_v, bv + 4 * j);
+      const double vz = R.vdrift + R.sig[s] * gauss_bm(R.seed_v, bv + 4 * j + 2);
+      const long long t = R.poff + base + j;
+      int i, k;
+      real fx, fz;
+      split_coord(x / R.dx, i, fx);
+      split_coord(z / R.dx, k, fz);
+      P.cell[t] = pack2(i, k);
+      P.ox[t] = fx;
+      P.oz[t] = fz;
+      P.vx[t] = (real)vx;
+      P.vy[t] = (real)0;
+      P.vz[t] = (real)vz;
+    }
+  }
+}
+
+// After a source launch: counts and stream counters of every run advance.
+template <typename real>
+__global__ void source2d_commit_kernel(const Run<real>* __restrict__ runs, State* st, const SourceSet* __restrict__ sets,
+                                       int nruns, int s) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nruns) return;
+  const long long total = sets[r].total;
+  const long long n = min((long long)st[r].count[s] + total, runs[r].cap);
+  st[r].count[s] = (int)n;
+  st[r].ctr_p += 2ull * total;
+  st[r].ctr_v += 4ull * total;
+}
+
+// add_ion5 / add_electron5's removal (:3317-3332) at size 1: z < 3 dx,
+// z > (Nz+1) dx, x < 3 dx, x > (Nx+1) dx.
+template <typename real>
+__global__ void delete5_kernel(Pools pools, const Run<real>* __restrict__ runs, const State* __restrict__ st,
+                               const Item* __restrict__ items, int nitems, int chunk) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int rs = items[it].run;
+    const int r = rs >> 1, s = rs & 1;
+    const Run<real> R = runs[r];
+    const int n = st[r].count[s];
+    const int first = items[it].first;
+    if (first >= n) continue;
+    const int last = min(first + chunk, n);
+    const PView<real> P = pview<real>(pools, s);
+    for (int q = first + threadIdx.x; q < last; q += blockDim.x) {
+      const long long t = R.poff + q;
+      const int c = P.cell[t];
+      if (c < 0) continue;
+      int i, k;
+      unpack2(c, i, k);
+      const real fx = P.ox[t], fz = P.oz[t];
+      const bool del = k < 3 || k > R.nz + 1 || (k == R.nz + 1 && fz > (real)0) || i < 3 || i > R.nx + 1 ||
+                       (i == R.nx + 1 && fx > (real)0);
+      if (del) P.cell[t] = -1;
+    }
+  }
+}
+
+// Stable compaction of every run's slots: flags -> per-run exclusive scan ->
+// scatter into the second pool; counts become the live totals.
+template <typename real>
+__global__ void live2d_kernel(Pools pools, const Run<real>* __restrict__ runs, const State* __restrict__ st,
+                              const Item* __restrict__ items, int nitems, int chunk, int s, int* flags, long long pool_cap) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int rs = items[it].run;
+    if ((rs & 1) != s) continue;
+    const int r = rs >> 1;
+    const Run<real> R = runs[r];
+    const int n = st[r].count[s];
+    const int first = items[it].first;
+    const int last = (int)min((long long)first + chunk, R.cap);
+    for (int q = first + threadIdx.x; q < last; q += blockDim.x) {
+      const long long t = R.poff + q;
+      flags[t] = (q < n && pools.cell[s][t] >= 0) ? 1 : 0;
+    }
+  }
+}
+
+template <typename real>
+__global__ void compact2d_kernel(Pools src, Pools dst, const Run<real>* __restrict__ runs, State* st,
+                                 const Item* __restrict__ items, int nitems, int chunk, int s, const int* __restrict__ pos,
+                                 const int* __restrict__ flags) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int rs = items[it].run;
+    if ((rs & 1) != s) continue;
+    const int r = rs >> 1;
+    const Run<real> R = runs[r];
+    const int base = pos[R.poff];
+    const int first = items[it].first;
+    const int last = (int)min((long long)first + chunk, R.cap);
+    const PView<real> A = pview<real>(src, s), B = pview<real>(dst, s);
+    for (int q = first + threadIdx.x; q < last; q += blockDim.x) {
+      const long long t = R.poff + q;
+      if (!flags[t]) continue;
+      const long long d = R.poff + (pos[t] - base);
+      B.cell[d] = A.cell[t];
+      B.ox[d] = A.ox[t]; B.oz[d] = A.oz[t];
+      B.vx[d] = A.vx[t]; B.vy[d] = A.vy[t]; B.vz[d] = A.vz[t];
+    }
+  }
+}
+
+template <typename real>
+__global__ void compact2d_count_kernel(const Run<real>* __restrict__ runs, State* st, int nruns, int s,
+                                       const int* __restrict__ pos, const int* __restrict__ flags) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nruns) return;
+  const Run<real> R = runs[r];
+  const long long e = R.poff + R.cap - 1;
+  st[r].count[s] = pos[e] + flags[e] - pos[R.poff];
+}
+
+// ------------------------------------------------------------ renew_phi
+// rho of renew_phi (:2608-2638, the rank-0 branch at size 1): the Gauss-law
+// residual on grid rows [Absorb_grid3, Nx+2) x columns [Absorb_grid3,
+// Nz+4-Absorb_grid3), zero elsewhere; buffer [nx][nz].
+template <typename real>
+__global__ void phi_rho_kernel(real* F, const Run<real>* __restrict__ runs, const Item* __restrict__ items, int nitems,
+                               real* rho) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Run<real> R = runs[items[it].run];
+    const int kk = items[it].first;  // rho row 0..nx-1 (grid row kk + 2)
+    const int k = kk + 2;
+    const int G = R.gz;
+    const real* ex = plane(F, R, P_EX);
+    const real* ez = plane(F, R, P_EZ);
+    const real* ni = plane(F, R, P_NI);
+    const real* ne = plane(F, R, P_NE);
+    real* out = rho + R.roff + (long long)kk * R.nz;
+    for (int mm = threadIdx.x; mm < R.nz; mm += blockDim.x) {
+      const int m = mm + 2;
+      double v = 0.0;
+      if (k >= R.a3 && k < R.nx + 2 && m >= R.a3 && m < R.nz + 4 - R.a3) {
+        const int n = k * G + m;
+        v = -(-R.q * ((double)ni[n] - (double)ne[n]) / R.e0 + ((double)ex[n + G] - (double)ex[n]) / R.dx +
+              ((double)ez[n + 1] - (double)ez[n]) / R.dx);
+      }
+      out[mm] = (real)v;
+    }
+  }
+}
+
+// Batched small GEMM C = alpha * op(A B) over every run (row-major, the run's
+// sizes): 32x32 output tiles, K staged through shared memory. mode selects the
+// operands of the four sine transforms:
+//  0: C[nx][nz] = A[nx][nz] * S_nz        (transform along z)
+//  1: C[nx][nz] = S_nx * A[nx][nz], then / eigenvalue  (along x, solve)
+//  2: C[nx][nz] = (2/nx) S_nx * A          (inverse along x)
+//  3: C[nx][nz] = (2/nz) A * S_nz          (inverse along z)
+// S_n[i][j] = sin(pi i j / n); its row and column 0 vanish, so the transforms
+// skip the first element as the reference's sinft does (y[1] = 0, :2902).
+template <typename real>
+__global__ void __launch_bounds__(256) dst_gemm_kernel(const Run<real>* __restrict__ runs, const Item* __restrict__ items,
+                                                       int nitems, const real* __restrict__ A, real* C,
+                                                       const real* __restrict__ sines, int mode) {
+  __shared__ real As[32][33];
+  __shared__ real Bs[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Run<real> R = runs[items[it].run];
+    const int nx = R.nx, nz = R.nz;
+    const int tiles_n = (nz + 31) / 32;
+    const int ti = items[it].first / tiles_n, tj = items[it].first % tiles_n;
+    const real* a = A + R.roff;
+    real* cmat = C + R.roff;
+    const real* Sx = sines + R.sz_dst;
+    const real* Sz = sines + R.sz_dst + (long long)nx * nx;
+    const bool left = mode == 1 || mode == 2;  // S * A (K = nx) or A * S (K = nz)
+    const int K = left ? nx : nz;
+    real acc[4] = {0, 0, 0, 0};
+    for (int k0 = 0; k0 < K; k0 += 32) {
+      // left operand tile [32 rows of C][32 of K], right operand tile [32 of K][32 cols of C]
+      for (int q = ty; q < 32; q += 8) {
+        const int row = ti * 32 + q, kc = k0 + tx;
+        real lv = 0, rv = 0;
+        if (left) {
+          if (row < nx && kc < nx) lv = Sx[(long long)row * nx + kc];
+          const int kr = k0 + q, col = tj * 32 + tx;
+          if (kr < nx && col < nz) rv = a[(long long)kr * nz + col];
+        } else {
+          if (row < nx && kc < nz) lv = a[(long long)row * nz + kc];
+          const int kr = k0 + q, col = tj * 32 + tx;
+          if (kr < nz && col < nz) rv = Sz[(long long)kr * nz + col];
+        }
+        As[q][tx] = lv;
+        Bs[q][tx] = rv;
+      }
+      __syncthreads();
+#pragma unroll 8
+      for (int kk = 0; kk < 32; ++kk) {
+        const real b = Bs[kk][tx];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[u] += As[ty + 8 * u][kk] * b;
+      }
+      __syncthreads();
+    }
+    const double Pi = 3.14159265358979323846;
+    for (int u = 0; u < 4; ++u) {
+      const int row = ti * 32 + ty + 8 * u, col = tj * 32 + tx;
+      if (row >= nx || col >= nz) continue;
+      real v = acc[u];
+      if (mode == 1) {
+        // renew_phi's eigenvalue (:2680-2690): row = x wave number, col = z wave number
+        const double sz = sin(Pi * (double)col / (double)nz / 2.), sx = sin(Pi * (double)row / (double)nx / 2.);
+        const double Aev = -(sz * sz + sx * sx) / ((R.dx / 2.) * (R.dx / 2.));
+        v = Aev == 0. ? (real)0 : (real)((double)v / Aev);
+      } else if (mode == 2) {
+        v = (real)(2. * (double)v / nx);
+      } else if (mode == 3) {
+        v = (real)(2. * (double)v / nz);
+      }
+      cmat[(long long)row * nz + col] = v;
+    }
+  }
+}
+
+// renew_phi's correction (:2749-2768): ex += d(phi)/dx (periodic at size 1:
+// the left neighbour of row 0 is row Nx-1), ez += d(phi)/dz (zero below
+// column 0), phi stored.
+template <typename real>
+__global__ void phi_apply_kernel(real* F, const Run<real>* __restrict__ runs, const Item* __restrict__ items, int nitems,
+                                 const real* __restrict__ rho) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Run<real> R = runs[items[it].run];
+    const int kk = items[it].first;
+    const int G = R.gz;
+    real* ex = plane(F, R, P_EX);
+    real* ez = plane(F, R, P_EZ);
+    real* phi = plane(F, R, P_PHI);
+    const real* row = rho + R.roff + (long long)kk * R.nz;
+    const real* left = rho + R.roff + (long long)(kk == 0 ? R.nx - 1 : kk - 1) * R.nz;
+    for (int mm = threadIdx.x; mm < R.nz; mm += blockDim.x) {
+      const int n = (kk + 2) * G + mm + 2;
+      const double v = row[mm];
+      ex[n] = (real)((double)ex[n] + (v - (double)left[mm]) / R.dx);
+      phi[n] = (real)v;
+      ez[n] = (real)((double)ez[n] + (v - (mm == 0 ? 0.0 : (double)row[mm - 1])) / R.dx);
+    }
+  }
+}
+
+// ------------------------------------------------------------ thrust_F
+// thrust_F (:2304-2387) per run, FP64. Where the reference's test
+// (x != xf0 && z != zf0) fails it keeps the previous node's terms: for the row
+// x == xf0 those of the last node of the row before, elsewhere those of the
+// node before in z. One block per run.
+__device__ __forceinline__ void coil_terms(double jy, double x, double z, double x0, double z0, double K, double& fx,
+                                           double& fz) {
+  const double Pi = 3.14159265358979323846;
+  const double d = 2. * Pi * ((x - x0) * (x - x0) + (z - z0) * (z - z0));
+  fx = K * jy * (x - x0) / d;
+  fz = K * jy * (z - z0) / d;
+}
+
+template <typename real>
+__global__ void thrust2d_kernel(const real* __restrict__ F, const Run<real>* __restrict__ runs, int nruns, State* st) {
+  __shared__ double red[3][32];
+  for (int r = blockIdx.x; r < nruns; r += gridDim.x) {
+    const Run<real> R = runs[r];
+    const real* jiy = plane((real*)F, R, P_JIY);
+    const real* jey = plane((real*)F, R, P_JEY);
+    const int G = R.gz;
+    const double dx = R.dx;
+    const double xf0 = 1.5 * dx, zf0 = -2.5 * dx, xb0 = 1.5 * dx, zb0 = 2.5 * dx;
+    const double K = R.mu0 * R.coil_i * dx * dx;
+    auto xs = [&](int k) { return ((double)(k - 2) + 0.5) * dx - dx * 1 * R.nx / 2.; };
+    auto zs = [&](int m) { return (double)(m - 2) * dx - (double)(R.nz / 2) * dx + 0.5 * dx; };
+    auto terms = [&](int k, int m, double& fx0, double& fz0, double& fx1, double& fz1) {
+      const double x = xs(k), z = zs(m);
+      const double jy = (double)jiy[k * G + m] - (double)jey[k * G + m];
+      coil_terms(jy, x, z, xf0, zf0, -K, fx0, fz0);
+      coil_terms(jy, x, z, xb0, zb0, K, fx1, fz1);
+    };
+    double s[3] = {0, 0, 0};
+    const int tot = R.nx * R.nz;
+    for (int q = threadIdx.x; q < tot; q += blockDim.x) {
+      const int k = 2 + q / R.nz, m = 2 + q % R.nz;
+      double fx0, fz0, fx1, fz1, a, b;
+      terms(k, m, fx0, fz0, fx1, fz1);
+      const double x = xs(k), z = zs(m);
+      if (!(x != xf0 && z != zf0)) {
+        if (x == xf0) terms(k - 1, R.nz + 1, fx0, fz0, a, b);
+        else terms(k, m - 1, fx0, fz0, a, b);
+      }
+      if (!(x != xb0 && z != zb0)) {
+        if (x == xb0) terms(k - 1, R.nz + 1, a, b, fx1, fz1);
+        else terms(k, m - 1, a, b, fx1, fz1);
+      }
+      s[0] += fx0 + fx1;
+      s[1] += fz0 + fz1;
+      s[2] += (-(zf0 + 0.5 * dx) * fx0 + xf0 * fz0) + (-(zb0 + 0.5 * dx) * fx1 + xb0 * fz1);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int q = 0; q < 3; ++q) {
+      double v = s[q];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) red[q][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      double v = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+      st[r].thrust[threadIdx.x] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------ exports
+template <typename real>
+__global__ void grid2d_export_kernel(const real* F, Run<real> R, double* rec) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= R.nodes) return;
+  // the reference's Grid record order (:104-112)
+  const int map[18] = {P_B0X, P_B0Y, P_B0Z, P_BX, P_BY, P_BZ, P_EX, P_EY, P_EZ,
+                       P_JIX, P_JIY, P_JIZ, P_JEX, P_JEY, P_JEZ, P_NI, P_NE, P_PHI};
+  for (int q = 0; q < 18; ++q) rec[18LL * n + q] = (double)F[R.foff + (long long)map[q] * R.nodes + n];
+}
+
+template <typename real>
+__global__ void parts2d_export_kernel(Pools pools, Run<real> R, int s, int n, const int* __restrict__ pos, double* rows) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const PView<real> P = pview<real>(pools, s);
+  const long long t = R.poff + q;
+  const int c = P.cell[t];
+  if (c < 0) return;
+  int i, k;
+  unpack2(c, i, k);
+  double* r = rows + 6LL * pos[q];
+  r[0] = ((double)i + (double)P.ox[t]) * R.dx;
+  r[1] = ((double)k + (double)P.oz[t]) * R.dx;
+  r[2] = (double)P.vx[t];
+  r[3] = (double)P.vy[t];
+  r[4] = (double)P.vz[t];
+  r[5] = R.nw;
+}
+
+__global__ void flag_kernel(const int* __restrict__ cell, long long off, int n, int* flags) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) flags[q] = cell[off + q] >= 0 ? 1 : 0;
+}
+
+}  // namespace p2
+
+// ================================================================ host
+using namespace p2;
+
+struct pic2d_batch {
+  int prec = 32;
+  int device = 0;
+  size_t rsize = 4;
+  int nruns = 0;
+  std::vector<pic2d_config> cfg;
+  cudaStream_t stream = nullptr;
+  void* runs_dev = nullptr;       // Run<real>[nruns]
+  std::vector<char> runs_host;    // same, host copy (bytes)
+  State* st = nullptr;            // device State[nruns]
+  void* field = nullptr;
+  long long field_nodes = 0;
+  Pools pool[2]{};                // double-buffered particle pools
+  int cur = 0;
+  long long pool_slots = 0;
+  void* sines = nullptr;
+  void* rho = nullptr;
+  void* rho2 = nullptr;
+  long long rho_len = 0;
+  // work lists
+  Item* row_items = nullptr;   int n_row = 0;    // (run, interior row k)
+  Item* rho_items = nullptr;   int n_rhorow = 0; // (run, rho row 0..nx-1)
+  Item* part_items = nullptr;  int n_part = 0;   // (run*2+s, first slot) over [0, cap)
+  Item* tile_items = nullptr;  int n_tile = 0;   // (run, 32x32 tile of nx x nz)
+  Item* src_items[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [init/add][species]
+  int n_src[2][2] = {{0, 0}, {0, 0}};
+  SourceSet* sets[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int* flags = nullptr;
+  int* pos = nullptr;
+  int* scan_tmp = nullptr;
+  size_t scan_len = 0;
+  int* step_dev = nullptr;
+  unsigned long long* err = nullptr;
+  int c_add = 0;
+  long long step = 0;
+  bool ready = false;
+  // launch configuration (tuned)
+  int push_block = 256;
+  int push_blocks = 148 * 8;
+  // graphs
+  bool use_graph = true;
+  cudaGraphExec_t graph[1] = {nullptr};  // the plain step on the current pool
+  long long graph_launches = 0;          // kernels in that graph
+  long long launches = 0;
+};
+
+namespace {
+
+#define CK2(x)                                                                   \
+  do {                                                                           \
+    cudaError_t e_ = (x);                                                        \
+    if (e_ != cudaSuccess) {                                                     \
+      fprintf(stderr, "plasma_b200 (2d): %s: %s\n", #x, cudaGetErrorString(e_)); \
+      return PIC_ERR_CUDA;                                                       \
+    }                                                                            \
+  } while (0)
+#define CKL2()                \
+  do {                        \
+    ++b->launches;            \
+    CK2(cudaGetLastError());  \
+  } while (0)
+#define CKR2(x)                  \
+  do {                           \
+    int r_ = (x);                \
+    if (r_ != PIC_OK) return r_; \
+  } while (0)
+
+
+int persistent(long long items, int per_sm = 8) {
+  long long b = std::min<long long>(items, 148LL * per_sm);
+  return (int)std::max<long long>(b, 1);
+}
+
+template <typename real>
+const Run<real>* runs_of(pic2d_batch* b) { return (const Run<real>*)b->runs_dev; }
+template <typename real>
+Run<real>* runs_host(pic2d_batch* b) { return (Run<real>*)b->runs_host.data(); }
+
+// The source sets of every run: the initial load (init_particle :389-525) or
+// the refill of add_ion5 / add_electron5 (:3311-3566) at size 1.
+template <typename real>
+void make_sets(pic2d_batch* b, int which, std::vector<SourceSet>& sets) {
+  sets.assign(b->nruns, SourceSet{});
+  for (int r = 0; r < b->nruns; ++r) {
+    const pic2d_config& k = b->cfg[r];
+    const double dx = k.dx;
+    const long long Np = k.np, Nx = k.nx, Nz = k.nz;
+    SourceSet& S = sets[r];
+    if (which == 0) {
+      // N * Step_p / THREAD_N + 1 particles uniform over the interior
+      S.slab[0] = {2. * dx, 2. * dx + Nx * dx, 2. * dx, 2. * dx + Nz * dx, Np * Nx * Np * Nz + 1};
+      S.nslab = 1;
+    } else {
+      S.slab[0] = {2 * dx, (Nx + 2) * dx, 2 * dx, 3 * dx, Np * Nx * Np};
+      S.slab[1] = {2 * dx, (Nx + 2) * dx, (Nz + 1) * dx, (Nz + 2) * dx, Np * Nx * Np};
+      S.slab[2] = {2 * dx, 3 * dx, 3 * dx, (Nz + 1) * dx, (Np * Nz - 2) * Np};
+      S.slab[3] = {(Nx + 1) * dx, (Nx + 2) * dx, 3 * dx, (Nz + 1) * dx, (Np * Nz - 2) * Np};
+      S.nslab = 4;
+    }
+    S.total = 0;
+    for (int q = 0; q < S.nslab; ++q) S.total += S.slab[q].count;
+  }
+}
+
+template <typename real>
+int run_sources(pic2d_batch* b, int which) {
+  for (int s = 0; s < 2; ++s) {
+    if (b->n_src[which][s] > 0) {
+      source2d_kernel<real><<<persistent(b->n_src[which][s]), 256, 0, b->stream>>>(
+          b->pool[b->cur], runs_of<real>(b), b->st, b->sets[which][s], b->src_items[which][s], b->n_src[which][s], kChunk, s,
+          b->err);
+      CKL2();
+    }
+    source2d_commit_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(runs_of<real>(b), b->st, b->sets[which][s],
+                                                                                b->nruns, s);
+    CKL2();
+  }
+  return PIC_OK;
+}
+
+int scan_excl(pic2d_batch* b, const int* in, int* out, long long n, int* tmp, size_t tmp_len) {
+  const long long tiles = (n + kScanTile - 1) / kScanTile;
+  if ((size_t)tiles + 1 > tmp_len) return PIC_ERR_STATE;
+  scan_tile_kernel<<<(unsigned)tiles, kScanThreads, 0, b->stream>>>(in, out, tmp, n);
+  CKL2();
+  if (tiles > 1) {
+    CKR2(scan_excl(b, tmp, tmp, tiles, tmp + tiles + 1, tmp_len - (size_t)tiles - 1));
+    scan_add_kernel<<<(unsigned)tiles, 256, 0, b->stream>>>(out, tmp, n);
+    CKL2();
+  }
+  return PIC_OK;
+}
+
+// Removes every run's empty slots, keeping order (into the other pool).
+template <typename real>
+int compact(pic2d_batch* b) {
+  const int nb = 1 - b->cur;
+  for (int s = 0; s < 2; ++s) {
+    live2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], runs_of<real>(b), b->st,
+                                                                      b->part_items, b->n_part, kChunk, s, b->flags,
+                                                                      b->pool_slots);
+    CKL2();
+    CKR2(scan_excl(b, b->flags, b->pos, b->pool_slots, b->scan_tmp, b->scan_len));
+    compact2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], b->pool[nb], runs_of<real>(b),
+                                                                         b->st, b->part_items, b->n_part, kChunk, s,
+                                                                         b->pos, b->flags);
+    CKL2();
+    compact2d_count_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(runs_of<real>(b), b->st, b->nruns, s,
+                                                                                b->pos, b->flags);
+    CKL2();
+  }
+  b->cur = nb;
+  return PIC_OK;
+}
+
+template <typename real>
+int sr_grid(pic2d_batch* b) {
+  sr_grid_kernel<real><<<persistent(b->nruns), 256, 0, b->stream>>>((real*)b->field, runs_of<real>(b), b->nruns);
+  CKL2();
+  return PIC_OK;
+}
+
+template <typename real>
+int renew_phi(pic2d_batch* b) {
+  real* rho = (real*)b->rho;
+  real* tmp = (real*)b->rho2;
+  const Run<real>* R = runs_of<real>(b);
+  phi_rho_kernel<real><<<persistent(b->n_rhorow), 128, 0, b->stream>>>((real*)b->field, R, b->rho_items, b->n_rhorow, rho);
+  CKL2();
+  const real* S = (const real*)b->sines;
+  dst_gemm_kernel<real><<<persistent(b->n_tile), 256, 0, b->stream>>>(R, b->tile_items, b->n_tile, rho, tmp, S, 0);
+  CKL2();
+  dst_gemm_kernel<real><<<persistent(b->n_tile), 256, 0, b->stream>>>(R, b->tile_items, b->n_tile, tmp, rho, S, 1);
+  CKL2();
+  dst_gemm_kernel<real><<<persistent(b->n_tile), 256, 0, b->stream>>>(R, b->tile_items, b->n_tile, rho, tmp, S, 2);
+  CKL2();
+  dst_gemm_kernel<real><<<persistent(b->n_tile), 256, 0, b->stream>>>(R, b->tile_items, b->n_tile, tmp, rho, S, 3);
+  CKL2();
+  phi_apply_kernel<real><<<persistent(b->n_rhorow), 128, 0, b->stream>>>((real*)b->field, R, b->rho_items, b->n_rhorow, rho);
+  CKL2();
+  return PIC_OK;
+}
+
+template <typename real>
+int push(pic2d_batch* b) {
+  const Run<real>* R = runs_of<real>(b);
+  real* F = (real*)b->field;
+  switch (b->push_block) {
+    case 128:
+      push2d_kernel<real, 128><<<b->push_blocks, 128, 0, b->stream>>>(b->pool[b->cur], F, R, b->st, b->part_items,
+                                                                       b->n_part, kChunk, b->err);
+      break;
+    case 512:
+      push2d_kernel<real, 512><<<b->push_blocks, 512, 0, b->stream>>>(b->pool[b->cur], F, R, b->st, b->part_items,
+                                                                       b->n_part, kChunk, b->err);
+      break;
+    default:
+      push2d_kernel<real, 256><<<b->push_blocks, 256, 0, b->stream>>>(b->pool[b->cur], F, R, b->st, b->part_items,
+                                                                       b->n_part, kChunk, b->err);
+  }
+  CKL2();
+  return PIC_OK;
+}
+
+// Zero J, n and phi of every run (renew_grid, :1348-1389).
+template <typename real>
+int renew_grid(pic2d_batch* b) {
+  zero_sources_kernel<real><<<persistent(b->nruns), 256, 0, b->stream>>>((real*)b->field, runs_of<real>(b), b->nruns);
+  CKL2();
+  return PIC_OK;
+}
+
+// One loop body for every run (fdtd :627-1015).
+template <typename real>
+int step_body(pic2d_batch* b, bool refill) {
+  const Run<real>* R = runs_of<real>(b);
+  real* F = (real*)b->field;
+  CKR2(renew_grid<real>(b));
+  if (refill) {
+    delete5_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], R, b->st, b->part_items,
+                                                                        b->n_part, kChunk);
+    CKL2();
+    CKR2(compact<real>(b));
+    CKR2(run_sources<real>(b, 1));
+  }
+  renew_b4_kernel<real><<<persistent(b->n_row), 128, 0, b->stream>>>(F, R, b->row_items, b->n_row);
+  CKL2();
+  CKR2(sr_grid<real>(b));
+  CKR2(push<real>(b));
+  fold_kernel<real><<<persistent(b->nruns), 256, 0, b->stream>>>(F, R, b->nruns, P_JIX, 6);
+  CKL2();
+  fold_kernel<real><<<persistent(b->nruns), 256, 0, b->stream>>>(F, R, b->nruns, P_NI, 2);
+  CKL2();
+  coil_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(F, R, b->nruns, b->step_dev);
+  CKL2();
+  renew_b4_kernel<real><<<persistent(b->n_row), 128, 0, b->stream>>>(F, R, b->row_items, b->n_row);
+  CKL2();
+  CKR2(sr_grid<real>(b));
+  renew_e4_kernel<real><<<persistent(b->n_row), 128, 0, b->stream>>>(F, R, b->row_items, b->n_row);
+  CKL2();
+  CKR2(sr_grid<real>(b));
+  CKR2(renew_phi<real>(b));
+  CKR2(sr_grid<real>(b));
+  step_advance_kernel<<<1, 1, 0, b->stream>>>(b->step_dev);
+  CKL2();
+  return PIC_OK;
+}
+
+void drop_graphs(pic2d_batch* b) {
+  for (auto& g : b->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+// nsteps loop bodies. A plain step is replayed from a CUDA graph captured on
+// first use; a step with a refill (every add_interval steps) runs directly,
+// since its compaction moves the particles to the other pool, after which
+// the plain-step graph is captured again for the new pool.
+template <typename real>
+int run_steps(pic2d_batch* b, int nsteps) {
+  for (int i = 0; i < nsteps; ++i) {
+    const bool refill = b->c_add > b->cfg[0].add_interval - 1;
+    if (refill || !b->use_graph) {
+      CKR2(step_body<real>(b, refill));
+      if (refill) drop_graphs(b);
+    } else {
+      if (!b->graph[0]) {
+        cudaGraph_t graph;
+        CK2(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        const long long l0 = b->launches;
+        const int rc = step_body<real>(b, false);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        graph = g;
+        if (rc != PIC_OK) {
+          if (graph) cudaGraphDestroy(graph);
+          return rc;
+        }
+        CK2(e);
+        b->graph_launches = b->launches - l0;
+        b->launches = l0;
+        const cudaError_t ei = cudaGraphInstantiate(&b->graph[0], graph, 0);
+        cudaGraphDestroy(graph);
+        CK2(ei);
+      }
+      CK2(cudaGraphLaunch(b->graph[0], b->stream));
+      b->launches += b->graph_launches;
+    }
+    if (refill) b->c_add = 0;
+    b->c_add++;
+    b->step++;
+  }
+  return PIC_OK;
+}
+
+template <typename real>
+int do_init(pic2d_batch* b) {
+  real* F = (real*)b->field;
+  const Run<real>* R = runs_of<real>(b);
+  const Run<real>* H = runs_host<real>(b);
+  // init_grid (:224-387): fields zero apart from B0 = B = IMF (the dipole terms
+  // are zeroed in the reference, :368, :385), so the whole block is cleared
+  CK2(cudaMemsetAsync(F, 0, sizeof(real) * (size_t)b->field_nodes, b->stream));
+  for (int r = 0; r < b->nruns; ++r) {
+    const pic2d_config& k = b->cfg[r];
+    // b0y = by = IMF_y everywhere; bx, bz, b0x, b0z = IMF_x / IMF_z on the interior
+    std::vector<real> h((size_t)H[r].nodes);
+    std::fill(h.begin(), h.end(), (real)k.imf_y);
+    CK2(cudaMemcpyAsync(F + H[r].foff + (long long)P_BY * H[r].nodes, h.data(), sizeof(real) * h.size(),
+                        cudaMemcpyHostToDevice, b->stream));
+    CK2(cudaMemcpyAsync(F + H[r].foff + (long long)P_B0Y * H[r].nodes, h.data(), sizeof(real) * h.size(),
+                        cudaMemcpyHostToDevice, b->stream));
+    for (int comp = 0; comp < 2; ++comp) {
+      const double imf = comp == 0 ? k.imf_x : k.imf_z;
+      if (imf == 0.0) continue;
+      std::fill(h.begin(), h.end(), (real)0);
+      for (int kk = 2; kk < k.nx + 2; ++kk)
+        for (int m = 2; m < k.nz + 2; ++m) h[(size_t)kk * (k.nz + 4) + m] = (real)imf;
+      const int pa = comp == 0 ? P_BX : P_BZ, pb0 = comp == 0 ? P_B0X : P_B0Z;
+      CK2(cudaMemcpyAsync(F + H[r].foff + (long long)pa * H[r].nodes, h.data(), sizeof(real) * h.size(),
+                          cudaMemcpyHostToDevice, b->stream));
+      CK2(cudaMemcpyAsync(F + H[r].foff + (long long)pb0 * H[r].nodes, h.data(), sizeof(real) * h.size(),
+                          cudaMemcpyHostToDevice, b->stream));
+    }
+    CK2(cudaStreamSynchronize(b->stream));
+  }
+  // particles (init_particle :389-525)
+  CK2(cudaMemsetAsync(b->st, 0, sizeof(State) * b->nruns, b->stream));
+  for (int p = 0; p < 2; ++p) CK2(cudaMemsetAsync(b->pool[p].cell[0], 0xff, sizeof(int) * b->pool_slots, b->stream));
+  for (int p = 0; p < 2; ++p) CK2(cudaMemsetAsync(b->pool[p].cell[1], 0xff, sizeof(int) * b->pool_slots, b->stream));
+  CKR2(run_sources<real>(b, 0));
+  // fdtd's set-up (:583-625)
+  CKR2(renew_grid<real>(b));
+  density2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], F, R, b->st, b->part_items,
+                                                                        b->n_part, kChunk);
+  CKL2();
+  fold_kernel<real><<<persistent(b->nruns), 256, 0, b->stream>>>(F, R, b->nruns, P_NI, 2);
+  CKL2();
+  CKR2(sr_grid<real>(b));
+  CK2(cudaMemsetAsync(b->step_dev, 0, sizeof(int), b->stream));
+  CKR2(renew_phi<real>(b));
+  CKR2(sr_grid<real>(b));
+  CK2(cudaStreamSynchronize(b->stream));
+  b->c_add = 0;
+  b->step = 0;
+  b->ready = true;
+  drop_graphs(b);
+  return PIC_OK;
+}
+
+template <typename real>
+int do_create(pic2d_batch* b) {
+  const int n = b->nruns;
+  b->runs_host.assign(sizeof(Run<real>) * n, 0);
+  Run<real>* H = runs_host<real>(b);
+  long long foff = 0, poff = 0, roff = 0;
+  std::vector<int> sine_sizes;
+  std::vector<std::pair<int, long long>> sine_off;  // size -> offset
+  std::vector<double> sines;
+  auto sine_table = [&](int m) -> long long {
+    for (auto& p : sine_off)
+      if (p.first == m) return p.second;
+    const long long o = (long long)sines.size();
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < m; ++j) sines.push_back(std::sin(3.14159265358979323846 * (double)i * (double)j / (double)m));
+    sine_off.push_back({m, o});
+    return o;
+  };
+  for (int r = 0; r < n; ++r) {
+    const pic2d_config& k = b->cfg[r];
+    Run<real>& R = H[r];
+    R.nx = k.nx; R.nz = k.nz; R.gx = k.nx + 4; R.gz = k.nz + 4; R.nodes = R.gx * R.gz;
+    R.np = k.np;
+    R.foff = foff;
+    foff += (long long)P_COUNT * R.nodes;
+    foff = (foff + 63) & ~63LL;
+    const long long load = (long long)k.np * k.np * k.nx * k.nz + 1;
+    const long long refill = 2LL * k.np * k.nx * k.np + 2LL * (k.np * (long long)k.nz - 2) * k.np;
+    R.cap = k.capacity > 0 ? k.capacity : (long long)(load * 1.25) + 2 * refill + 4096;
+    R.cap = (R.cap + kChunk - 1) / kChunk * kChunk;
+    R.poff = poff;
+    poff += R.cap;
+    R.a1 = k.absorb_grid; R.a2 = k.absorb_grid2; R.a3 = k.absorb_grid3;
+    R.dx = k.dx; R.dt = k.dt; R.q = k.q; R.e0 = k.e0; R.mu0 = k.mu0; R.c = k.c;
+    R.sigma_a = k.sigma_a;
+    R.coil_i = k.coil_i;
+    R.vdrift = k.v_drift;
+    R.sig[0] = std::sqrt(k.kb * k.ti / k.mi);
+    R.sig[1] = std::sqrt(k.kb * k.te / k.me);
+    R.nw = k.n_all / k.np / k.np;
+    R.T[0] = 0.5 * k.q * k.dt / k.mi;
+    R.T[1] = 0.5 * k.q * k.dt / -k.me;
+    R.ex_add = k.v_drift * k.imf_y;
+    R.ey_add = -k.v_drift * k.imf_x;
+    R.seed_p = k.seed_p;
+    R.seed_v = k.seed_v;
+    R.add_interval = k.add_interval;
+    R.sz_dst = 0;
+    R.roff = roff;
+    roff += (long long)k.nx * k.nz;
+    const long long sx = sine_table(k.nx);
+    const long long sz = sine_table(k.nz);
+    // the kernel expects S_nx then S_nz back to back: store a pair when they are not
+    if (sz != sx + (long long)k.nx * k.nx) {
+      const long long o = (long long)sines.size();
+      for (long long q = 0; q < (long long)k.nx * k.nx; ++q) sines.push_back(sines[sx + q]);
+      for (long long q = 0; q < (long long)k.nz * k.nz; ++q) sines.push_back(sines[sz + q]);
+      R.sz_dst = (int)o;
+    } else {
+      R.sz_dst = (int)sx;
+    }
+  }
+  b->field_nodes = foff;
+  b->pool_slots = poff;
+  b->rho_len = roff;
+  CK2(cudaMalloc(&b->runs_dev, sizeof(Run<real>) * n));
+  CK2(cudaMemcpy(b->runs_dev, H, sizeof(Run<real>) * n, cudaMemcpyHostToDevice));
+  CK2(cudaMalloc(&b->st, sizeof(State) * n));
+  CK2(cudaMemset(b->st, 0, sizeof(State) * n));
+  CK2(cudaMalloc(&b->field, sizeof(real) * (size_t)foff));
+  for (int p = 0; p < 2; ++p)
+    for (int s = 0; s < 2; ++s) {
+      CK2(cudaMalloc(&b->pool[p].cell[s], sizeof(int) * (size_t)poff));
+      for (int a = 0; a < 2; ++a) CK2(cudaMalloc(&b->pool[p].o[s][a], sizeof(real) * (size_t)poff));
+      for (int a = 0; a < 3; ++a) CK2(cudaMalloc(&b->pool[p].v[s][a], sizeof(real) * (size_t)poff));
+    }
+  std::vector<real> sr(sines.begin(), sines.end());
+  CK2(cudaMalloc(&b->sines, sizeof(real) * std::max<size_t>(sr.size(), 1)));
+  CK2(cudaMemcpy(b->sines, sr.data(), sizeof(real) * sr.size(), cudaMemcpyHostToDevice));
+  CK2(cudaMalloc(&b->rho, sizeof(real) * (size_t)roff));
+  CK2(cudaMalloc(&b->rho2, sizeof(real) * (size_t)roff));
+  // work lists
+  std::vector<Item> rows, rhos, parts, tiles;
+  for (int r = 0; r < n; ++r) {
+    for (int k = 2; k < H[r].nx + 2; ++k) rows.push_back({r, k});
+    for (int k = 0; k < H[r].nx; ++k) rhos.push_back({r, k});
+    for (int s = 0; s < 2; ++s)
+      for (long long q = 0; q < H[r].cap; q += kChunk) parts.push_back({2 * r + s, (int)q});
+    const int tn = (H[r].nz + 31) / 32, tm = (H[r].nx + 31) / 32;
+    for (int t = 0; t < tn * tm; ++t) tiles.push_back({r, t});
+  }
+  auto upload = [&](const std::vector<Item>& v, Item** dst, int* cnt) -> int {
+    *cnt = (int)v.size();
+    CK2(cudaMalloc(dst, sizeof(Item) * std::max<size_t>(v.size(), 1)));
+    CK2(cudaMemcpy(*dst, v.data(), sizeof(Item) * v.size(), cudaMemcpyHostToDevice));
+    return PIC_OK;
+  };
+  CKR2(upload(rows, &b->row_items, &b->n_row));
+  CKR2(upload(rhos, &b->rho_items, &b->n_rhorow));
+  CKR2(upload(parts, &b->part_items, &b->n_part));
+  CKR2(upload(tiles, &b->tile_items, &b->n_tile));
+  for (int which = 0; which < 2; ++which) {
+    std::vector<SourceSet> sets;
+    make_sets<real>(b, which, sets);
+    for (int s = 0; s < 2; ++s) {
+      CK2(cudaMalloc(&b->sets[which][s], sizeof(SourceSet) * n));
+      CK2(cudaMemcpy(b->sets[which][s], sets.data(), sizeof(SourceSet) * n, cudaMemcpyHostToDevice));
+      std::vector<Item> it;
+      for (int r = 0; r < n; ++r)
+        for (long long q = 0; q < sets[r].total; q += kChunk) it.push_back({r, (int)q});
+      CKR2(upload(it, &b->src_items[which][s], &b->n_src[which][s]));
+    }
+  }
+  CK2(cudaMalloc(&b->flags, sizeof(int) * (size_t)poff));
+  CK2(cudaMalloc(&b->pos, sizeof(int) * (size_t)poff));
+  b->scan_len = (size_t)(2 * ((poff + kScanTile - 1) / kScanTile) + 64);
+  CK2(cudaMalloc(&b->scan_tmp, sizeof(int) * b->scan_len));
+  CK2(cudaMalloc(&b->step_dev, sizeof(int)));
+  CK2(cudaMemset(b->step_dev, 0, sizeof(int)));
+  CK2(cudaMalloc(&b->err, sizeof(unsigned long long) * ERR_COUNT));
+  CK2(cudaMemset(b->err, 0, sizeof(unsigned long long) * ERR_COUNT));
+  b->push_blocks = persistent(b->n_part, 8);
+  return PIC_OK;
+}
+
+void free_batch(pic2d_batch* b) {
+  drop_graphs(b);
+  cudaFree(b->runs_dev); cudaFree(b->st); cudaFree(b->field);
+  for (int p = 0; p < 2; ++p)
+    for (int s = 0; s < 2; ++s) {
+      cudaFree(b->pool[p].cell[s]);
+      for (int a = 0; a < 2; ++a) cudaFree(b->pool[p].o[s][a]);
+      for (int a = 0; a < 3; ++a) cudaFree(b->pool[p].v[s][a]);
+    }
+  cudaFree(b->sines); cudaFree(b->rho); cudaFree(b->rho2);
+  cudaFree(b->row_items); cudaFree(b->rho_items); cudaFree(b->part_items); cudaFree(b->tile_items);
+  for (int w = 0; w < 2; ++w)
+    for (int s = 0; s < 2; ++s) { cudaFree(b->src_items[w][s]); cudaFree(b->sets[w][s]); }
+  cudaFree(b->flags); cudaFree(b->pos); cudaFree(b->scan_tmp); cudaFree(b->step_dev); cudaFree(b->err);
+  if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+#define DISPATCH2(b, call) ((b)->prec == 64 ? call<double> : call<float>)
+
+int valid(const pic2d_config& k) {
+  if (k.nx < 8 || k.nz < 8 || k.np < 1 || k.nx + 4 >= (1 << kCellShift) || k.nz + 4 >= (1 << kCellShift)) return 0;
+  if (k.dx <= 0 || k.dt <= 0 || k.mi <= 0 || k.me <= 0 || k.e0 <= 0 || k.c <= 0) return 0;
+  if (k.absorb_grid3 < 2 || k.add_interval < 1) return 0;
+  return 1;
+}
+
+template <typename real>
+int do_get_particles(pic2d_batch* b, int run, int s, double* rows, long long cap, long long* n_out) {
+  const Run<real>& R = runs_host<real>(b)[run];
+  State S;
+  CK2(cudaMemcpyAsync(&S, b->st + run, sizeof(State), cudaMemcpyDeviceToHost, b->stream));
+  CK2(cudaStreamSynchronize(b->stream));
+  const int n = S.count[s];
+  if (n == 0) {
+    *n_out = 0;
+    return PIC_OK;
+  }
+  int* flags = nullptr;
+  int* pos = nullptr;
+  int* tmp = nullptr;
+  const size_t tl = (size_t)(2 * ((n + kScanTile - 1) / kScanTile) + 64);
+  CK2(cudaMalloc(&flags, sizeof(int) * n));
+  CK2(cudaMalloc(&pos, sizeof(int) * n));
+  CK2(cudaMalloc(&tmp, sizeof(int) * tl));
+  flag_kernel<<<(n + 255) / 256, 256, 0, b->stream>>>(b->pool[b->cur].cell[s], R.poff, n, flags);
+  int rc = scan_excl(b, flags, pos, n, tmp, tl);
+  int lp = 0, lf = 0;
+  double* dev = nullptr;
+  if (rc == PIC_OK) {
+    cudaMemcpyAsync(&lp, pos + n - 1, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    cudaMemcpyAsync(&lf, flags + n - 1, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    cudaStreamSynchronize(b->stream);
+    const long long live = (long long)lp + lf;
+    *n_out = live;
+    if (rows && cap > 0 && live > 0) {
+      cudaMalloc(&dev, sizeof(double) * 6 * (size_t)live);
+      parts2d_export_kernel<real><<<(n + 255) / 256, 256, 0, b->stream>>>(b->pool[b->cur], R, s, n, pos, dev);
+      cudaMemcpyAsync(rows, dev, sizeof(double) * 6 * (size_t)std::min(live, cap), cudaMemcpyDeviceToHost, b->stream);
+      cudaStreamSynchronize(b->stream);
+    }
+  }
+  cudaFree(dev); cudaFree(flags); cudaFree(pos); cudaFree(tmp);
+  CK2(cudaGetLastError());
+  return rc;
+}
+
+template <typename real>
+int do_get_grid(pic2d_batch* b, int run, double* rec) {
+  const Run<real>& R = runs_host<real>(b)[run];
+  double* dev = nullptr;
+  CK2(cudaMalloc(&dev, sizeof(double) * 18 * (size_t)R.nodes));
+  grid2d_export_kernel<real><<<(R.nodes + 255) / 256, 256, 0, b->stream>>>((const real*)b->field, R, dev);
+  cudaError_t e = cudaMemcpyAsync(rec, dev, sizeof(double) * 18 * (size_t)R.nodes, cudaMemcpyDeviceToHost, b->stream);
+  cudaStreamSynchronize(b->stream);
+  cudaFree(dev);
+  CK2(e);
+  CK2(cudaGetLastError());
+  return PIC_OK;
+}
+
+template <typename real>
+int do_thrust(pic2d_batch* b, double* out) {
+  thrust2d_kernel<real><<<persistent(b->nruns), 256, 0, b->stream>>>((const real*)b->field, runs_of<real>(b), b->nruns,
+                                                                       b->st);
+  CKL2();
+  std::vector<State> S(b->nruns);
+  CK2(cudaMemcpyAsync(S.data(), b->st, sizeof(State) * b->nruns, cudaMemcpyDeviceToHost, b->stream));
+  CK2(cudaStreamSynchronize(b->stream));
+  for (int r = 0; r < b->nruns; ++r)
+    for (int q = 0; q < 3; ++q) out[3 * r + q] = S[r].thrust[q];
+  return PIC_OK;
+}
+
+// Online tuning: the next steps of the run itself try each push launch shape
+// (block size x persistent blocks per SM), timing whole loop bodies, and the
+// fastest shape is kept; the steps taken are ordinary steps of the run.
+template <typename real>
+int do_autotune(pic2d_batch* b, int* choice) {
+  const int blocks[3] = {128, 256, 512};
+  const int per_sm[3] = {2, 4, 8};  // resident blocks of 256 threads per SM
+  float best = 1e30f;
+  int bb = b->push_block, bs = b->push_blocks;
+  cudaEvent_t e0, e1;
+  CK2(cudaEventCreate(&e0));
+  CK2(cudaEventCreate(&e1));
+  int rc = PIC_OK;
+  for (int i = 0; i < 3 && rc == PIC_OK; ++i)
+    for (int j = 0; j < 3 && rc == PIC_OK; ++j) {
+      b->push_block = blocks[i];
+      b->push_blocks = persistent(b->n_part, per_sm[j] * 256 / blocks[i]);
+      const bool g = b->use_graph;
+      b->use_graph = false;
+      cudaEventRecord(e0, b->stream);
+      rc = run_steps<real>(b, 2);
+      cudaEventRecord(e1, b->stream);
+      b->use_graph = g;
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = PIC_ERR_CUDA;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rc == PIC_OK && ms < best) {
+        best = ms;
+        bb = blocks[i];
+        bs = b->push_blocks;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->push_block = bb;
+  b->push_blocks = bs;
+  drop_graphs(b);
+  if (choice) {
+    choice[0] = bb;
+    choice[1] = bs;
+  }
+  return rc;
+}
+
+}  // namespace
+
+// ================================================================ C ABI
+extern "C" {
+
+int pic2d_config_normalized(pic2d_config* k, int nx, int nz, int np) {
+  if (!k) return PIC_ERR_ARG;
+  std::memset(k, 0, sizeof(*k));
+  k->nx = nx; k->nz = nz; k->np = np;
+  k->dx = 1.0; k->dt = 0.5 * 6.0 / (7.0 * std::sqrt(2.0));
+  k->q = 1.0; k->mi = 100.0; k->me = 1.0; k->mu0 = 1.0; k->e0 = 1.0; k->kb = 1.0; k->c = 1.0;
+  k->v_drift = 0.1; k->n_all = 0.01; k->ti = 0.0025; k->te = 0.0025; k->coil_i = 12.0;
+  k->absorb_grid = 32; k->absorb_grid2 = 16; k->absorb_grid3 = 32;
+  k->sigma_a = 1e-6;
+  k->add_interval = 250;
+  k->seed_p = 0; k->seed_v = 50;
+  return PIC_OK;
+}
+
+int pic2d_create(const pic2d_config* cfgs, int nruns, int precision, int device, pic2d_batch** out) {
+  if (!cfgs || !out || nruns < 1 || (precision != 32 && precision != 64)) return PIC_ERR_ARG;
+  for (int r = 0; r < nruns; ++r) {
+    if (!valid(cfgs[r])) return PIC_ERR_ARG;
+    if (cfgs[r].add_interval != cfgs[0].add_interval) return PIC_ERR_ARG;  // runs step together
+  }
+  *out = nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) return PIC_ERR_CUDA;
+  pic2d_batch* b = new (std::nothrow) pic2d_batch();
+  if (!b) return PIC_ERR_ARG;
+  b->prec = precision;
+  b->device = device;
+  b->rsize = precision == 64 ? 8 : 4;
+  b->nruns = nruns;
+  b->cfg.assign(cfgs, cfgs + nruns);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete b;
+    return PIC_ERR_CUDA;
+  }
+  const int rc = DISPATCH2(b, do_create)(b);
+  if (rc != PIC_OK) {
+    free_batch(b);
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return PIC_OK;
+}
+
+int pic2d_destroy(pic2d_batch* b) {
+  if (!b) return PIC_ERR_ARG;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  free_batch(b);
+  delete b;
+  return PIC_OK;
+}
+
+int pic2d_init(pic2d_batch* b) {
+  if (!b) return PIC_ERR_ARG;
+  if (cudaSetDevice(b->device) != cudaSuccess) return PIC_ERR_CUDA;
+  return DISPATCH2(b, do_init)(b);
+}
+
+int pic2d_step(pic2d_batch* b, int nsteps) {
+  if (!b || nsteps < 0) return PIC_ERR_ARG;
+  if (!b->ready) return PIC_ERR_STATE;
+  if (cudaSetDevice(b->device) != cudaSuccess) return PIC_ERR_CUDA;
+  return DISPATCH2(b, run_steps)(b, nsteps);
+}
+
+int pic2d_thrust(pic2d_batch* b, double* out3) {
+  if (!b || !out3) return PIC_ERR_ARG;
+  if (!b->ready) return PIC_ERR_STATE;
+  return DISPATCH2(b, do_thrust)(b, out3);
+}
+
+int pic2d_particle_count(pic2d_batch* b, int run, int species, long long* n) {
+  if (!b || !n || run < 0 || run >= b->nruns || species < 0 || species > 1) return PIC_ERR_ARG;
+  return (b->prec == 64 ? do_get_particles<double> : do_get_particles<float>)(b, run, species, nullptr, 0, n);
+}
+
+int pic2d_get_particles(pic2d_batch* b, int run, int species, double* rows6, long long cap, long long* n) {
+  if (!b || !n || run < 0 || run >= b->nruns || species < 0 || species > 1) return PIC_ERR_ARG;
+  return (b->prec == 64 ? do_get_particles<double> : do_get_particles<float>)(b, run, species, rows6, cap, n);
+}
+
+int pic2d_get_grid(pic2d_batch* b, int run, double* records) {
+  if (!b || !records || run < 0 || run >= b->nruns) return PIC_ERR_ARG;
+  return (b->prec == 64 ? do_get_grid<double> : do_get_grid<float>)(b, run, records);
+}
+
+int pic2d_autotune(pic2d_batch* b, int* choice2) {
+  if (!b) return PIC_ERR_ARG;
+  if (!b->ready) return PIC_ERR_STATE;
+  return DISPATCH2(b, do_autotune)(b, choice2);
+}
+
+int pic2d_set_graph(pic2d_batch* b, int enable) {
+  if (!b) return PIC_ERR_ARG;
+  b->use_graph = enable != 0;
+  drop_graphs(b);
+  return PIC_OK;
+}
+
+int pic2d_status(pic2d_batch* b, long long* counters8) {
+  if (!b || !counters8) return PIC_ERR_ARG;
+  unsigned long long h[ERR_COUNT];
+  if (cudaMemcpy(h, b->err, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return PIC_ERR_CUDA;
+  for (int q = 0; q < 8; ++q) counters8[q] = (long long)h[q];
+  counters8[4] = b->step;
+  counters8[5] = b->launches;
+  return (h[0] | h[1] | h[2]) ? PIC_ERR_DEVICE : PIC_OK;
+}
+
+int pic2d_get_stream(pic2d_batch* b, void** stream) {
+  if (!b || !stream) return PIC_ERR_ARG;
+  *stream = (void*)b->stream;
+  return PIC_OK;
+}
+
+}  // extern "C"

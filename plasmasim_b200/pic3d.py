@@ -126,6 +126,9 @@ EXPORTED = [
     "pic_set_grid", "pic_rng_counters", "pic_status", "pic_synchronize", "pic_get_stream",
     "pic_error_string", "pic_set_timing", "pic_read_timing", "pic_gauss_residual_noalloc",
     "pic_objective", "pic_adjoint",
+    "pic2d_config_normalized", "pic2d_create", "pic2d_destroy", "pic2d_init", "pic2d_step",
+    "pic2d_thrust", "pic2d_particle_count", "pic2d_get_particles", "pic2d_get_grid",
+    "pic2d_autotune", "pic2d_set_graph", "pic2d_status", "pic2d_get_stream",
 ]
 
 PHASES = ["push", "field", "sort", "add", "diag"]

@@ -10,6 +10,7 @@ import pytest
 
 import plasmasim_b200 as pb
 from plasmasim_b200 import build as pbuild
+from plasmasim_b200.pic2d import _C2Config
 from plasmasim_b200.pic3d import _CConfig
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -24,7 +25,7 @@ def lib():
 
 def declared_functions():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^(?:int|const char \*)\s*(pic_\w+)\(", text, re.M)))
+    return sorted(set(re.findall(r"^(?:int|const char \*)\s*(pic(?:2d)?_\w+)\(", text, re.M)))
 
 
 def test_exports_every_declared_function(lib):
@@ -35,20 +36,21 @@ def test_exports_every_declared_function(lib):
     assert sorted(pb.pic3d.EXPORTED) == names
 
 
-def test_config_layout_matches_header(tmp_path):
-    fields = [f[0] for f in _CConfig._fields_]
+@pytest.mark.parametrize("struct,mirror", [("pic_config", _CConfig), ("pic2d_config", _C2Config)])
+def test_config_layout_matches_header(tmp_path, struct, mirror):
+    fields = [f[0] for f in mirror._fields_]
     src = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', 'int main(void){',
-           'printf("%zu\\n", sizeof(pic_config));']
-    src += [f'printf("%zu\\n", offsetof(pic_config, {f}));' for f in fields]
+           f'printf("%zu\\n", sizeof({struct}));']
+    src += [f'printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
     src += ['return 0;}']
     c = tmp_path / "layout.c"
     c.write_text("\n".join(src))
     exe = tmp_path / "layout"
     subprocess.run(["gcc", str(c), "-o", str(exe)], check=True)
     out = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
-    assert out[0] == C.sizeof(_CConfig)
+    assert out[0] == C.sizeof(mirror)
     for f, off in zip(fields, out[1:]):
-        assert getattr(_CConfig, f).offset == off, f
+        assert getattr(mirror, f).offset == off, f
 
 
 def test_error_strings(lib):
