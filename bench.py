@@ -248,6 +248,137 @@ def roofline(out, npart_species, cells, rsize):
     return bytes_total / secs / 1e9, bytes_total / max(launches, 1), secs / max(launches, 1)
 
 
+def batch2d_configs(nruns: int, seed: int = 7):
+    """The batched 2D workload: nruns x-z runs with grid sides uniform in
+    [64, 256] (even), Np uniform in [4, 8] (16-64 particles per cell per
+    species), coil current uniform in [6, 25] (x0.5-x2 of the current giving
+    |B| = 0.5 at 4 cells) and drift uniform in [0.05, 0.2] c; absorb widths
+    8 / 4 / 8 cells; each run its own random streams."""
+    import numpy as np
+
+    from plasmasim_b200 import Pic2DConfig
+
+    rng = np.random.default_rng(seed)
+    cfgs = []
+    for r in range(nruns):
+        nx, nz = (int(v) // 2 * 2 for v in rng.integers(64, 257, size=2))
+        cfgs.append(Pic2DConfig(nx=nx, nz=nz, np=int(rng.integers(4, 9)), coil_i=float(rng.uniform(6, 25)),
+                                v_drift=float(rng.uniform(0.05, 0.2)), absorb_grid=8, absorb_grid2=4,
+                                absorb_grid3=8, seed_p=1000 * r, seed_v=1000 * r + 50))
+    return cfgs
+
+
+def run_batch2d(nruns: int, steps: int, warmup: int):
+    """Device-timed steps of the batched 2D workload (FP32), after init, the
+    online launch tuning and `warmup` further steps."""
+    import torch
+
+    from plasmasim_b200 import Pic2DBatch
+
+    cfgs = batch2d_configs(nruns)
+    B = Pic2DBatch(cfgs, precision=32)
+    B.init()
+    choice = B.autotune()
+    B.step(warmup)
+    stream = torch.cuda.ExternalStream(B.stream_handle())
+    _, c0 = B.status()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    B.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    rc, c1 = B.status()
+    pushed = int(c1[3] - c0[3])
+    B.close()
+    return {"workload": f"{nruns} independent x-z runs (PIC2D), grid sides uniform in [64, 256], "
+                        "16-64 particles/cell/species, coil current and drift seeded-random",
+            "value": pushed / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+            "particles": pushed // max(steps, 1), "launch_shape": list(choice), "graph": True,
+            "kernels_per_step": int(c1[5] - c0[5]) // max(steps, 1), "device_errors": [int(x) for x in c1[:3]]}
+
+
+def batch2d_cpu_sample(steps: int = 3):
+    """The 2D reference compiled at 64 x 64 cells x 16 ppc (oracle/_ref), one core."""
+    from oracle import build as obuild
+    from oracle.pyoracle import Reference2D
+
+    if not os.path.isfile(obuild.ref2d_lib_path("sq64")):
+        if not os.path.isfile(obuild.REF2D_SRC):
+            return None
+        obuild.build_ref2d("sq64")
+    R = Reference2D("sq64")
+    R.init()
+    n0 = len(R.particles(0)[0]) + len(R.particles(1)[0])
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        R.step(250)
+    dt = time.perf_counter() - t0
+    return {"value": n0 * steps / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"2D reference loop body, 64 x 64 cells x 16 ppc/species ({n0} particles), {steps} steps"}
+
+
+def run_adjoint(nsteps: int = 200, every: int = 20):
+    """The adjoint of configs' differentiable run: 64^3 cells x 16 ppc/species,
+    nsteps steps with a checkpoint every `every` steps (FP32): wall times of
+    the production step, the slot-stable forward and the adjoint, and the
+    adjoint against central differences (h = 1e-3 relative) at growing
+    horizons."""
+    import torch
+
+    from plasmasim_b200 import Pic3D, PicConfig
+
+    def ctx(I=32.0, V=0.1):
+        cfg = PicConfig.normalized(64, 64, 64, 16, precision=32, diag_every_step=0, sort_interval=20,
+                                   add_interval=5)
+        cfg.coil_i, cfg.v_drift = I, V
+        P = Pic3D(cfg)
+        P.init_grid()
+        P.init_particle_flat()
+        P.fdtd(0)
+        P.synchronize()
+        return P
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+
+    P = ctx()
+    P.step(3)
+    _, t_step = timed(lambda: P.step(nsteps))
+    P.close()
+    P = ctx()
+    _, t_fwd = timed(lambda: P.objective(nsteps))
+    P.close()
+    P = ctx()
+    out, t_adj = timed(lambda: P.adjoint(nsteps, every))
+    P.close()
+    checks = []
+    h = 1e-3
+    for T in (5, 20, 50, nsteps):
+        P = ctx()
+        J, dI, dV = P.adjoint(T, min(every, T))
+        P.close()
+        vals = []
+        for I, V in ((32 * (1 + h), 0.1), (32 * (1 - h), 0.1), (32, 0.1 * (1 + h)), (32, 0.1 * (1 - h))):
+            P = ctx(I, V)
+            vals.append(P.objective(T))
+            P.close()
+        fdI = (vals[0] - vals[1]) / (2 * h * 32)
+        fdV = (vals[2] - vals[3]) / (2 * h * 0.1)
+        checks.append({"steps": T, "dJ_dI": dI, "fd_dJ_dI": fdI, "rel_err_I": abs(dI / fdI - 1),
+                       "dJ_dV": dV, "fd_dJ_dV": fdV, "rel_err_V": abs(dV / fdV - 1)})
+    return {"workload": f"64^3 cells x 16 ppc/species, {nsteps} steps, checkpoint every {every}, FP32",
+            "objective": "impulse along z delivered to the dipole", "J": out[0], "dJ_dI": out[1], "dJ_dV": out[2],
+            "step_ms": t_step / nsteps * 1e3, "forward_ms": t_fwd / nsteps * 1e3, "adjoint_ms": t_adj / nsteps * 1e3,
+            "adjoint_over_step": t_adj / t_step, "adjoint_over_forward": t_adj / t_fwd,
+            "fd_checks": checks}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -260,6 +391,9 @@ def main():
     ap.add_argument("--grid", type=int, default=128,
                     help="cells per axis (128 for the benchmark; smaller cases for profiling)")
     ap.add_argument("--ppc", type=int, default=64, help="particles per cell per species")
+    ap.add_argument("--no-batch2d", action="store_true", help="skip the batched 2D runs")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
+    ap.add_argument("--runs2d", type=int, default=256, help="runs of the batched 2D workload")
     args = ap.parse_args()
     global NX, NY, NZ, PPC
     NX = NY = NZ = args.grid
@@ -348,6 +482,24 @@ def main():
         fp64 = {"value": v64, "ms_per_step": o64["ms"] / args.steps, "fp32_over_fp64": value / v64,
                 "phase_ms": o64["phase_ms"]}
 
+    batch2d = None
+    if not args.no_batch2d and world == 1:
+        try:
+            batch2d = run_batch2d(args.runs2d, args.steps, args.warmup)
+            if not args.no_cpu:
+                batch2d["cpu_baseline"] = batch2d_cpu_sample()
+        except Exception as exc:  # reported, not hidden
+            log("batch2d failed:", exc)
+            batch2d = {"error": str(exc)[:200]}
+
+    adjoint = None
+    if not args.no_adjoint and world == 1:
+        try:
+            adjoint = run_adjoint()
+        except Exception as exc:
+            log("adjoint failed:", exc)
+            adjoint = {"error": str(exc)[:200]}
+
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         if ensure_reference_lib("cube64"):
@@ -384,6 +536,7 @@ def main():
             "phase_ms_per_step": {k: v / args.steps for k, v in out["phase_ms"].items()},
             "clocks": out["clocks"], "gpu_launches": out["launches"],
             "device_errors": out["errors"], "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu,
+            "batch2d": batch2d, "adjoint": adjoint,
         }
         print(json.dumps(line))
     if dist is not None:
