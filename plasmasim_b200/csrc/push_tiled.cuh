@@ -11,20 +11,53 @@ constexpr int kQueue = 64;   // per-warp queue of mover deposits (power of two)
 constexpr int kStages = 3;   // particle rows in flight per warp
 
 // Shared-memory plan of one CTA (8 warps): the J/n window, per warp a queue of
-// J deposits of particles outside their home cell, and per warp a ring of
+// J deposits of particles outside their home cell, per warp a ring of
 // kStages particle rows fetched ahead with cp.async (cell words, then the six
-// coordinate arrays).
+// coordinate arrays) and, in FP32, the tile's E and B over the same window
+// (the gather reads them there; FP64 gathers from global memory, its window
+// would not leave room for two CTAs per SM).
 template <typename real>
 struct PushSmem {
   static constexpr int WX = kTileX + 4, WY = kTileY + 4, WZ = kWinZ, WN = WX * WY * WZ;
   static constexpr int kWarps = kTileX * kTileY;
+  static constexpr bool kFieldWin = sizeof(real) == 4;
   static constexpr size_t win_bytes = 4 * WN * sizeof(real);
   static constexpr size_t qcell_off = (win_bytes + 15) & ~(size_t)15;
   static constexpr size_t qdat_off = qcell_off + (size_t)kWarps * kQueue * sizeof(int);
   static constexpr size_t pcell_off = qdat_off + (size_t)kWarps * kQueue * 6 * sizeof(real);
   static constexpr size_t pdat_off = pcell_off + (size_t)kWarps * kStages * kLanes * sizeof(int);
-  static constexpr size_t bytes = pdat_off + (size_t)kWarps * kStages * 6 * kLanes * sizeof(real);
+  static constexpr size_t fwin_off = pdat_off + (size_t)kWarps * kStages * 6 * kLanes * sizeof(real);
+  static constexpr size_t bytes = fwin_off + (kFieldWin ? (size_t)6 * WN * sizeof(real) : 0);
 };
+
+// Trilinear interpolation from a window plane with compile-time strides (the
+// 2x2x2 nodes at window index n).
+template <int WY, int WZ>
+__device__ __forceinline__ float trilerp_win(const float* __restrict__ w, int n, float x0, float x1, float y0,
+                                             float y1, float z0, float z1) {
+  const float c00 = w[n] * z0 + w[n + 1] * z1;
+  const float c01 = w[n + WZ] * z0 + w[n + WZ + 1] * z1;
+  const float c10 = w[n + WY * WZ] * z0 + w[n + WY * WZ + 1] * z1;
+  const float c11 = w[n + WY * WZ + WZ] * z0 + w[n + WY * WZ + WZ + 1] * z1;
+  return (c00 * y0 + c01 * y1) * x0 + (c10 * y0 + c11 * y1) * x1;
+}
+
+// gather6 from the tile's field window (planes ex ey ez bx by bz of WN nodes,
+// origin (wx0, wy0, wz0)); the caller checks that the stencil lies inside.
+template <int WY, int WZ, int WN>
+__device__ __forceinline__ Gathered<float> gather6_win(const float* __restrict__ fw, int wx0, int wy0, int wz0,
+                                                       const Axis<float>& X, const Axis<float>& Y,
+                                                       const Axis<float>& Z) {
+  const int ax = X.a - wx0, bx = X.b - wx0, ay = Y.a - wy0, by = Y.b - wy0, az = Z.a - wz0, bz = Z.b - wz0;
+  Gathered<float> r;
+  r.ex = trilerp_win<WY, WZ>(fw, (ax * WY + by) * WZ + bz, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
+  r.ey = trilerp_win<WY, WZ>(fw + WN, (bx * WY + ay) * WZ + bz, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
+  r.ez = trilerp_win<WY, WZ>(fw + 2 * WN, (bx * WY + by) * WZ + az, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
+  r.bx = trilerp_win<WY, WZ>(fw + 3 * WN, (bx * WY + ay) * WZ + az, X.b0, X.b1, Y.a0, Y.a1, Z.a0, Z.a1);
+  r.by = trilerp_win<WY, WZ>(fw + 4 * WN, (ax * WY + by) * WZ + az, X.a0, X.a1, Y.b0, Y.b1, Z.a0, Z.a1);
+  r.bz = trilerp_win<WY, WZ>(fw + 5 * WN, (ax * WY + ay) * WZ + bz, X.a0, X.a1, Y.a0, Y.a1, Z.b0, Z.b1);
+  return r;
+}
 
 template <int BYTES>
 __device__ __forceinline__ void cp_async_n(void* smem, const void* gmem) {
@@ -78,6 +111,32 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   // window origin: two nodes below the tile's first interior cell (2 + tx*TX)
   const int wx0 = tx * kTileX, wy0 = ty * kTileY, wz0 = tz * kLanes;
   for (int q = threadIdx.x; q < 4 * WN; q += blockDim.x) win[q] = (real)0;
+  // FP32: E and B (planes F_EX..F_BZ) over the window, zero outside the array
+  float* fw = reinterpret_cast<float*>(smem_raw + S::fwin_off);
+  if constexpr (S::kFieldWin) {
+    constexpr int NZ4 = WZ / 4;
+    for (int q4 = threadIdx.x; q4 < 6 * WX * WY * NZ4; q4 += blockDim.x) {
+      const int p = q4 / (WX * WY * NZ4);
+      const int r = q4 % (WX * WY * NZ4);
+      const int a = r / (WY * NZ4), b = (r / NZ4) % WY, c4 = r % NZ4;
+      const int ga = wx0 + a, gb = wy0 + b, gc = wz0 + 4 * c4;
+      float v[4] = {0.f, 0.f, 0.f, 0.f};
+      if (ga < g.gx && gb < g.gy) {
+        const real* src = F.f[p] + ga * g.sx + gb * g.gz + gc;
+        if (VEC_FLUSH && gc + 3 < g.gz) {
+          const float4 f4 = __ldg(reinterpret_cast<const float4*>(src));
+          v[0] = f4.x; v[1] = f4.y; v[2] = f4.z; v[3] = f4.w;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (gc + e < g.gz) v[e] = (float)src[e];
+        }
+      }
+      float* dst = fw + p * WN + (a * WY + b) * WZ + 4 * c4;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) dst[e] = v[e];
+    }
+  }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
@@ -153,7 +212,17 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       }
       if (!bal) {
         const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-        boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
+        if constexpr (S::kFieldWin) {
+          // the stencil spans nodes i-1 .. i+1 on each axis
+          const bool inside = i - 1 >= wx0 && i + 1 < wx0 + WX && j - 1 >= wy0 && j + 1 < wy0 + WY &&
+                              k - 1 >= wz0 && k + 1 < wz0 + WZ;
+          if (inside)
+            boris4_fast(pc, gather6_win<WY, WZ, WN>(fw, wx0, wy0, wz0, X, Y, Z), vx, vy, vz);
+          else
+            boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
+        } else {
+          boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
+        }
         if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) count_err(err, ERR_NONFINITE);
       }
       advance(i, fx, vx * pc.hdt);
