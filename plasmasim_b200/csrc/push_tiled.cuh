@@ -7,11 +7,9 @@
 
 namespace pb {
 
-constexpr int kQueue = 64;   // per-warp queue of mover deposits (power of two)
 constexpr int kStages = 3;   // particle rows in flight per warp
 
-// Shared-memory plan of one CTA (8 warps): the J/n window, per warp a queue of
-// J deposits of particles outside their home cell, per warp a ring of
+// Shared-memory plan of one CTA (8 warps): the J/n window, per warp a ring of
 // kStages particle rows fetched ahead with cp.async (cell words, then the six
 // coordinate arrays) and, in FP32, the tile's E and B over the same window
 // (the gather reads them there; FP64 gathers from global memory, its window
@@ -22,9 +20,7 @@ struct PushSmem {
   static constexpr int kWarps = kTileX * kTileY;
   static constexpr bool kFieldWin = sizeof(real) == 4;
   static constexpr size_t win_bytes = 4 * WN * sizeof(real);
-  static constexpr size_t qcell_off = (win_bytes + 15) & ~(size_t)15;
-  static constexpr size_t qdat_off = qcell_off + (size_t)kWarps * kQueue * sizeof(int);
-  static constexpr size_t pcell_off = qdat_off + (size_t)kWarps * kQueue * 6 * sizeof(real);
+  static constexpr size_t pcell_off = (win_bytes + 15) & ~(size_t)15;
   static constexpr size_t pdat_off = pcell_off + (size_t)kWarps * kStages * kLanes * sizeof(int);
   static constexpr size_t fwin_off = pdat_off + (size_t)kWarps * kStages * 6 * kLanes * sizeof(real);
   static constexpr size_t bytes = fwin_off + (kFieldWin ? (size_t)6 * WN * sizeof(real) : 0);
@@ -71,32 +67,17 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
 
-// Deposit of one queued J entry (a particle outside its home cell) into the
-// window, or into global memory when its stencil leaves the window.
-template <typename real>
-__device__ __forceinline__ void deposit_j_entry(real* win, int wx0, int wy0, int wz0, const Fields<real>& F,
-                                                const Geom& g, const PushConst<real>& pc, int cell,
-                                                const real* d) {
-  constexpr int WN = PushSmem<real>::WN;
-  int i, j, k;
-  unpack_cell(cell, i, j, k);
-  const Axis<real> X = axis_weights(i, d[0]), Y = axis_weights(j, d[1]), Z = axis_weights(k, d[2]);
-  scatter8_win(win, wx0, wy0, wz0, F.f[pc.pjx], g, X.a, Y.b, Z.b, d[3], X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
-  scatter8_win(win + WN, wx0, wy0, wz0, F.f[pc.pjy], g, X.b, Y.a, Z.b, d[4], X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
-  scatter8_win(win + 2 * WN, wx0, wy0, wz0, F.f[pc.pjz], g, X.b, Y.b, Z.a, d[5], X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
-}
-
 // The fused particle part of one step (push, J deposit at x^{n+1/2}, drift,
 // n deposit at x^{n+1}, sr_particle) for one species over the tiled layout;
 // the same arithmetic as push_kernel<real, PUSH_FUSED> apart from the FP32
 // square roots and divisions and, in FP32, the fixed-point sums of the density
 // window. One CTA per tile, one warp per group.
 //
-// J of a particle still in its lane's home cell is summed in registers; J of
-// the others is queued per warp and deposited 32 entries at a time, so that a
-// few such particles do not make the whole warp run the atomic path. The
-// density goes to the window with shared reductions (every active lane at
-// once): integer ones on fixed-point sums in FP32, FP64 atomics in FP64.
+// J of a particle in its lane's home cell at x^{n+1/2} is summed in registers;
+// the others add theirs to global memory with reductions (FP32 shared atomics
+// would be compare-and-swap loops). The density goes to the window with shared
+// reductions (every active lane at once): integer ones on fixed-point sums in
+// FP32, FP64 atomics in FP64.
 template <typename real, bool VEC_FLUSH>
 __global__ void __launch_bounds__(kTileX * kTileY * 32, 2)
 push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc,
@@ -139,10 +120,6 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const unsigned below = (1u << lane) - 1u;
-  int* qcell = reinterpret_cast<int*>(smem_raw + S::qcell_off) + warp * kQueue;
-  real* qdat = reinterpret_cast<real*>(smem_raw + S::qdat_off) + warp * kQueue * 6;
-  int qhead = 0, qtail = 0;  // warp-uniform queue counters
   const int G = tile * (kTileX * kTileY) + warp;
   const int base = ta.goff[G], jmax = ta.gmax[G];
   // home cell of this lane
@@ -198,7 +175,6 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     const bool act = c >= 0;
     int i = 0, j = 0, k = 0;
     real fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
-    bool mover = false;
     if (act) {
       ++pushed;
       unpack_cell(c, i, j, k);
@@ -259,27 +235,12 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
             ajz[a][b][1] += (qz * az[1]) * xy;
           }
       } else if (in_array(g, i, j, k)) {
-        if (stencil_ok(g, i, j, k)) mover = true;
-        else count_err(err, ERR_DEPOSIT_OOB);
-      }
-    }
-    // queue the J deposits of movers; every lane takes part in the vote
-    const unsigned m = __ballot_sync(0xffffffffu, mover);
-    if (m) {
-      if (mover) {
-        const int p = (qtail + __popc(m & below)) & (kQueue - 1);
-        qcell[p] = pack_cell(i, j, k);
-        real* d = qdat + 6 * p;
-        d[0] = fx; d[1] = fy; d[2] = fz;
-        d[3] = pc.qn * vx; d[4] = pc.qn * vy; d[5] = pc.qn * vz;
-      }
-      qtail += __popc(m);
-      __syncwarp();
-      if (qtail - qhead >= kLanes) {
-        const int p = (qhead + lane) & (kQueue - 1);
-        deposit_j_entry(win, wx0, wy0, wz0, F, g, pc, qcell[p], qdat + 6 * p);
-        qhead += kLanes;
-        __syncwarp();
+        if (stencil_ok(g, i, j, k)) {
+          const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+          deposit_j(F, g, pc, X, Y, Z, vx, vy, vz);
+        } else {
+          count_err(err, ERR_DEPOSIT_OOB);
+        }
       }
     }
     if (act) {
@@ -303,14 +264,6 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       P.o[0][t] = fx; P.o[1][t] = fy; P.o[2][t] = fz;
       P.v[0][t] = vx; P.v[1][t] = vy; P.v[2][t] = vz;
     }
-  }
-  // the rest of the queue
-  if (qtail > qhead) {
-    if (lane < qtail - qhead) {
-      const int p = (qhead + lane) & (kQueue - 1);
-      deposit_j_entry(win, wx0, wy0, wz0, F, g, pc, qcell[p], qdat + 6 * p);
-    }
-    __syncwarp();
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
   if (lane == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
