@@ -160,6 +160,29 @@ int pic_fdtd(pic_ctx *ctx, int nsteps);
 int pic_objective(pic_ctx *ctx, int nsteps, double *J);
 int pic_adjoint(pic_ctx *ctx, int nsteps, int checkpoint_every, double *out3);
 
+/* The reference's files, byte-compatible, in directory dir (NULL: the working
+ * directory); rank is the file-name rank (myrank_x + myrank_y * PROCESS_Nx).
+ *
+ * pic_save_checkpoint: suspend_job (:7629-7674): suspend-<rank>-field.dat, the
+ * Grid records of every node (z fastest), and suspend-<rank>-<t>-ion.dat /
+ * -electron.dat for t < nthreads, the 80-byte Particle structs (list links
+ * written as zero), the particles split in nthreads consecutive parts.
+ * pic_load_checkpoint: continue_job (:7676-7911): reads those files (as the
+ * reference or pic_save_checkpoint wrote them) into the context and restarts
+ * the random streams from their seeds as continue_job does; continue with
+ * pic_fdtd, as the reference continues with fdtd. Every particle must carry
+ * the species weight Nall/Np and flag 1.
+ * pic_write_output: output (:4834-4883): fdtd458-0-0-<step>.dat, 23 columns
+ * per interior node.
+ * pic_append_thrust: the line thrust_f appends to thrust458.txt (:5111-5119).
+ * pic_append_thrust_ave: when step % 500 == 0, the line thrust_fave appends to
+ * thrust458_ave.txt (:5266-5276), then the running mean restarts. */
+int pic_save_checkpoint(pic_ctx *ctx, const char *dir, int rank, int nthreads);
+int pic_load_checkpoint(pic_ctx *ctx, const char *dir, int rank, int nthreads);
+int pic_write_output(pic_ctx *ctx, const char *dir, int step);
+int pic_append_thrust(pic_ctx *ctx, const char *dir, int step);
+int pic_append_thrust_ave(pic_ctx *ctx, const char *dir, int step);
+
 /* State import/export in reference units (FP64 host arrays). */
 int pic_set_particles(pic_ctx *ctx, int species, const double *rows, const int *flag,
                       long long n);

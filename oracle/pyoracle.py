@@ -253,6 +253,18 @@ class Reference:
     def op(self, name):
         self.L.ref_op(REF_OPS[name])
 
+    def suspend(self):
+        """suspend_job: the reference's checkpoint files in the working directory."""
+        self.L.ref_suspend()
+
+    def continue_job(self):
+        """continue_job: the state from checkpoint files in the working directory."""
+        self.L.ref_continue()
+
+    def output(self, step: int):
+        """output(): fdtd458-0-0-<step>.dat in the working directory."""
+        self.L.ref_output(step)
+
     def init_grid(self):
         self.L.ref_init_grid()
 

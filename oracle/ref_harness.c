@@ -433,3 +433,25 @@ int ref_loop(int nsteps, int sort_every, int add_every)
 
 void ref_fave(double *out) { memcpy(out, Fave, sizeof(Fave)); }
 int ref_unmatched_sends(void) { return oracle_mpi_unmatched(); }
+
+/* --- the reference's own file writers and reader ----------------------- */
+/* suspend_job (:7629-7674) and continue_job (:7676-7911) in the working
+ * directory, on the harness's particle lists. */
+static void h_suspend(void *a) { (void)a; suspend_job(h_ion, h_ion_start, h_el, h_el_start, 0, 0); }
+int ref_suspend(void) { return h_run(h_suspend, NULL); }
+static void h_continue(void *a)
+{
+  (void)a;
+  continue_job(h_ion, h_ion_start, h_el, h_el_start, 0, 0);
+}
+int ref_continue(void)
+{
+  h_free_all();
+  int rc = h_run(h_continue, NULL);
+  h_have_particles = 1;
+  return rc;
+}
+/* output (:4834-4883): fdtd458-0-0-<c>.dat in the working directory. */
+static int h_output_c;
+static void h_output(void *a) { (void)a; output(0, 0, h_output_c); }
+int ref_output(int c) { h_output_c = c; return h_run(h_output, NULL); }

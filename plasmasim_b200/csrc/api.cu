@@ -1335,3 +1335,5 @@ int pic_read_timing(pic_ctx* c, double* ms8, long long* marks8, long long* launc
 }
 
 }  // extern "C"
+
+#include "files.cuh"

@@ -125,7 +125,8 @@ EXPORTED = [
     "pic_set_particles", "pic_get_particles", "pic_particle_count", "pic_get_grid",
     "pic_set_grid", "pic_rng_counters", "pic_status", "pic_synchronize", "pic_get_stream",
     "pic_error_string", "pic_set_timing", "pic_read_timing", "pic_gauss_residual_noalloc",
-    "pic_objective", "pic_adjoint",
+    "pic_objective", "pic_adjoint", "pic_save_checkpoint", "pic_load_checkpoint", "pic_write_output",
+    "pic_append_thrust", "pic_append_thrust_ave",
     "pic2d_config_normalized", "pic2d_create", "pic2d_destroy", "pic2d_init", "pic2d_step",
     "pic2d_thrust", "pic2d_particle_count", "pic2d_get_particles", "pic2d_get_grid",
     "pic2d_autotune", "pic2d_set_graph", "pic2d_status", "pic2d_get_stream",
@@ -159,6 +160,10 @@ def load_library(path: str = LIB_PATH):
     L.pic_thrust_fave.argtypes = [vp, _dp, C.c_int]
     L.pic_gauss_residual.argtypes = [vp, _dp]
     L.pic_objective.argtypes = [vp, C.c_int, _dp]
+    for name in ["pic_save_checkpoint", "pic_load_checkpoint"]:
+        getattr(L, name).argtypes = [vp, C.c_char_p, C.c_int, C.c_int]
+    for name in ["pic_write_output", "pic_append_thrust", "pic_append_thrust_ave"]:
+        getattr(L, name).argtypes = [vp, C.c_char_p, C.c_int]
     L.pic_adjoint.argtypes = [vp, C.c_int, C.c_int, _dp]
     L.pic_step.argtypes = [vp, C.c_int]
     L.pic_fdtd.argtypes = [vp, C.c_int]
@@ -270,6 +275,26 @@ class Pic3D:
         out = np.zeros(4)
         self._call("pic_gauss_residual", _ptr(out))
         return out
+
+    def save_checkpoint(self, directory: str, rank: int = 0, nthreads: int = 1):
+        """suspend_job's files (suspend-<rank>-field.dat, suspend-<rank>-<t>-{ion,electron}.dat)."""
+        self._call("pic_save_checkpoint", directory.encode(), rank, nthreads)
+
+    def load_checkpoint(self, directory: str, rank: int = 0, nthreads: int = 1):
+        """continue_job: the state from suspend_job's files."""
+        self._call("pic_load_checkpoint", directory.encode(), rank, nthreads)
+
+    def write_output(self, directory: str, step: int):
+        """output(): fdtd458-0-0-<step>.dat."""
+        self._call("pic_write_output", directory.encode(), step)
+
+    def append_thrust(self, directory: str, step: int):
+        """thrust_f's line in thrust458.txt."""
+        self._call("pic_append_thrust", directory.encode(), step)
+
+    def append_thrust_ave(self, directory: str, step: int):
+        """thrust_fave's line in thrust458_ave.txt (every 500 steps)."""
+        self._call("pic_append_thrust_ave", directory.encode(), step)
 
     def objective(self, nsteps: int) -> float:
         """Impulse along z delivered to the dipole over nsteps slot-stable steps."""
