@@ -233,7 +233,7 @@ def run_e2e(P, steps: int):
 # from the ncu capture of a 64^3 x 64 ppc launch
 # (profiles/push_tiled_kernel_grid64_64ppc.md); at a fixed number of particles
 # per cell the traffic of a launch grows with its particles.
-PUSH_TRAFFIC_PER_PARTICLE = 61.0
+PUSH_TRAFFIC_PER_PARTICLE = 61.1
 
 
 def roofline(out, npart_species, cells, rsize):
@@ -518,11 +518,12 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "3D PIC solar wind + dipole (normalized units), 128^3 cells x 64 "
-                                   "particles/cell/species, sort every 20, refill every 5",
+            "config": {"workload": f"3D PIC solar wind + dipole (normalized units), {NX}x{NY}x{NZ} cells x "
+                                   f"{PPC} particles/cell/species, sort every 20, refill every 5",
                        "grid": [NX, NY, NZ], "ppc_per_species": PPC,
                        "particles": int(pushed / max(args.steps, 1)),
-                       "l2": "inputs larger than L2 (7.5 GB of particle state per step)",
+                       "l2": f"inputs larger than L2 ({28 * pushed / max(args.steps, 1) / 1e9:.2f} GB of "
+                             "particle state per step)",
                        "parallelism": f"replicas{world}"},
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak,
