@@ -70,11 +70,15 @@ typedef struct pic_config {
   int add_interval;        /* fdtd: add_*_flat every add_interval steps (5, :700) */
   int sort_interval;       /* fdtd: sorting every sort_interval steps (500, :694) */
   int diag_every_step;     /* 1: thrust_fave sums every step as fdtd does (:926) */
-  int reserved0;
+  int poisson_clean;       /* 1: renew_phi3 + sr_phi + sr_e after each renew_e4_2 and after the
+                              first add_*_flat, as a build with the PHI blocks (:107, :676-681,
+                              :901-907); 0: as the reference ships (PHI compiled out) */
   long long capacity;      /* particle slots per species; 0 sizes it for the tiled layout:
                               (1.125 (np + 3 sqrt(np) + 2) + 6) slots per cell + 65536 */
   unsigned long long seed_p; /* position stream key (init_particle_flat :444: 0) */
   unsigned long long seed_v; /* velocity stream key (:445: 50) */
+  int absorb_grid3;        /* Absorb_grid3 (:97, 40): cells of each boundary left out of renew_phi3's residual */
+  int reserved1;
 } pic_config;
 
 typedef struct pic_ctx pic_ctx;
@@ -126,6 +130,12 @@ int pic_thrust_fave(pic_ctx *ctx, double *Fave27, int reset);
  * what the reference's compiled-out renew_phi3 :8315 would correct):
  * out = [sum (div4 E - rho/e0)^2, sum (rho/e0)^2, max |div4 E - rho/e0|, cells]. */
 int pic_gauss_residual(pic_ctx *ctx, double *out4);
+/* renew_phi3 (:8315-8665) + sr_phi (:1389-1574) + sr_e at size 1, the block a
+ * build with the PHI blocks runs after renew_e4_2 (:901-907): phi solves
+ * lap(phi) = -(div4 E - q (ni - ne)/e0) on the cells Absorb_grid3 leaves in, by
+ * sine transforms; E += the 4th-order gradient of phi. pic_config.poisson_clean
+ * runs it inside pic_step and pic_fdtd. */
+int pic_poisson_clean(pic_ctx *ctx);
 
 /* nsteps iterations of fdtd's loop body (:687-949) continuing the step
  * counters; the particle work of one step runs as one fused kernel per species. */

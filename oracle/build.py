@@ -51,10 +51,11 @@ MKSA = dict(
 )
 
 
-def _geom(nx, ny, nz, np_, absorb=0, absorb2=0, threads=1, pack=20000):
+def _geom(nx, ny, nz, np_, absorb=0, absorb2=0, threads=1, pack=20000, absorb3=40, phi=0):
     return dict(ORACLE_NX=nx, ORACLE_NY=ny, ORACLE_NZ=nz, ORACLE_NP=np_,
                 ORACLE_ABSORB=absorb, ORACLE_ABSORB2=absorb2,
-                ORACLE_THREADS=threads, ORACLE_PACK_N=pack)
+                ORACLE_THREADS=threads, ORACLE_PACK_N=pack,
+                ORACLE_ABSORB3=absorb3, ORACLE_PHI=phi)
 
 
 REF_CONFIGS = {
@@ -68,6 +69,12 @@ REF_CONFIGS = {
     "cube32": {**NORMALIZED, **_geom(32, 32, 32, 8, pack=80000)},
     # 64^3 cells, 16 particles/cell/species: CPU throughput sample
     "cube64": {**NORMALIZED, **_geom(64, 64, 64, 16, pack=400000)},
+    # the tiny cube with the reference's PHI blocks compiled in (renew_phi3,
+    # sr_phi, sr_e after each renew_e4_2 and after the first add_*_flat);
+    # Absorb_grid3 = 0 and 1 (the reference ships 40, which leaves no cell of
+    # an 8^3 grid)
+    "tiny_phi": {**NORMALIZED, **_geom(8, 8, 8, 4, absorb3=0, phi=1)},
+    "tiny_phi1": {**NORMALIZED, **_geom(8, 8, 8, 4, absorb3=1, phi=1)},
 }
 
 

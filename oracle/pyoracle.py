@@ -212,6 +212,78 @@ class Oracle:
         return float(out[0]), float(out[1])
 
 
+def sine_matrix(n: int) -> np.ndarray:
+    """S[k][j] = sin(pi j k / n): the transform of the reference's sinft
+    (PIC/3d_pic458_domain.c:8182-8210) on data[1..n] = rho[0..n-1], which
+    sets data[1] = 0, so row and column 0 vanish."""
+    j = np.arange(n, dtype=np.float64)
+    return np.sin(np.pi * np.outer(j, j) / n)
+
+
+def renew_phi3(grid: np.ndarray, dx: float, q: float, e0: float, absorb3: int) -> np.ndarray:
+    """renew_phi3 + sr_phi + sr_e at MPI size 1 (PIC/3d_pic458_domain.c
+    :8315-8665, :1389-1574, and the E wrap of sr_e), restated with numpy on a
+    grid of records [x][y][z][18]; returns the new grid.
+
+    - rho (:8338-8355): on interior cells (k, l, m) with 0 < k-2 < Nx - A3 ... the
+      Gauss residual -( -q (ni - ne)/e0 + div4 E ), div4 the (27, -1)/24 stencil
+      of E's forward differences; zero elsewhere (A3 = Absorb_grid3).
+    - sine transforms along z, y, x (fft_z/y/x :7990-8084), division by
+      A = -(sin^2(pi ky/2Ny) + sin^2(pi kz/2Nz) + sin^2(pi kx/2Nx)) / (dx/2)^2
+      (zero where A = 0, :8502-8511), inverse transforms with 2/N (:8086-8180).
+    - phi on the interior (:8655-8661); sr_phi wraps its two ghost planes in x,
+      then in y over all x; E += the (27, -1)/24 backward gradient of phi on
+      the interior (:1563-1572); sr_e wraps E's ghost planes in x, then y."""
+    EX, EY, EZ, NI, NE, PHI = 6, 7, 8, 15, 16, 17
+    g = grid.copy()
+    gx, gy, gz = g.shape[:3]
+    nx, ny, nz = gx - 4, gy - 4, gz - 4
+    I = slice(2, nx + 2)
+    Jy = slice(2, ny + 2)
+    K = slice(2, nz + 2)
+
+    def sh(a, dk=0, dl=0, dm=0):
+        return a[2 + dk:nx + 2 + dk, 2 + dl:ny + 2 + dl, 2 + dm:nz + 2 + dm]
+
+    ex, ey, ez = g[..., EX], g[..., EY], g[..., EZ]
+    div = ((-sh(ex, 2) + 27 * sh(ex, 1) - 27 * sh(ex) + sh(ex, -1))
+           + (-sh(ey, 0, 2) + 27 * sh(ey, 0, 1) - 27 * sh(ey) + sh(ey, 0, -1))
+           + (-sh(ez, 0, 0, 2) + 27 * sh(ez, 0, 0, 1) - 27 * sh(ez) + sh(ez, 0, 0, -1))) / (24. * dx)
+    rho = -(-q * (g[I, Jy, K, NI] - g[I, Jy, K, NE]) / e0 + div)
+    kx = np.arange(nx)[:, None, None]
+    ky = np.arange(ny)[None, :, None]
+    kz = np.arange(nz)[None, None, :]
+    mask = ((kx > absorb3) & (kx < nx - absorb3) & (ky > absorb3) & (ky < ny - absorb3)
+            & (kz >= absorb3) & (kz < nz - absorb3))
+    rho = np.where(mask, rho, 0.0)
+    Sx, Sy, Sz = sine_matrix(nx), sine_matrix(ny), sine_matrix(nz)
+    t = np.einsum("xyz,cz->xyc", rho, Sz)
+    t = np.einsum("xyz,by->xbz", t, Sy)
+    t = np.einsum("xyz,ax->ayz", t, Sx)
+    A = -(np.sin(np.pi * ky / ny / 2.) ** 2 + np.sin(np.pi * kz / nz / 2.) ** 2
+          + np.sin(np.pi * kx / nx / 2.) ** 2) / (dx / 2.) ** 2
+    t = np.where(A == 0., 0.0, t / np.where(A == 0., 1.0, A))
+    t = 2. * np.einsum("xyz,ax->ayz", t, Sx) / nx
+    t = 2. * np.einsum("xyz,by->xbz", t, Sy) / ny
+    t = 2. * np.einsum("xyz,cz->xyc", t, Sz) / nz
+    g[I, Jy, K, PHI] = t
+    # sr_phi at size 1: x planes (all y, z), then y planes (all x, z)
+    g[0:2, :, :, PHI] = g[nx:nx + 2, :, :, PHI]
+    g[nx + 2:nx + 4, :, :, PHI] = g[2:4, :, :, PHI]
+    g[:, 0:2, :, PHI] = g[:, ny:ny + 2, :, PHI]
+    g[:, ny + 2:ny + 4, :, PHI] = g[:, 2:4, :, PHI]
+    phi = g[..., PHI]
+    g[I, Jy, K, EX] += (-sh(phi, 1) + 27 * sh(phi) - 27 * sh(phi, -1) + sh(phi, -2)) / (24. * dx)
+    g[I, Jy, K, EY] += (-sh(phi, 0, 1) + 27 * sh(phi) - 27 * sh(phi, 0, -1) + sh(phi, 0, -2)) / (24. * dx)
+    g[I, Jy, K, EZ] += (-sh(phi, 0, 0, 1) + 27 * sh(phi) - 27 * sh(phi, 0, 0, -1) + sh(phi, 0, 0, -2)) / (24. * dx)
+    for f in (EX, EY, EZ):
+        g[0:2, :, :, f] = g[nx:nx + 2, :, :, f]
+        g[nx + 2:nx + 4, :, :, f] = g[2:4, :, :, f]
+        g[:, 0:2, :, f] = g[:, ny:ny + 2, :, f]
+        g[:, ny + 2:ny + 4, :, f] = g[:, 2:4, :, f]
+    return g
+
+
 REF_OPS = dict(renew_grid=1, renew_b=2, sr_b=3, push_j=4, drift_n=5, reduce=6,
                sr_current=7, renew_e=8, sr_e=9, sr_particle=10, add_flat=11, sort=12,
                thrust_f=13)
@@ -264,6 +336,11 @@ class Reference:
     def output(self, step: int):
         """output(): fdtd458-0-0-<step>.dat in the working directory."""
         self.L.ref_output(step)
+
+    def renew_phi3(self):
+        """renew_phi3 + sr_phi + sr_e (a geometry built with the PHI blocks)."""
+        if self.L.ref_renew_phi3() != 0:
+            raise RuntimeError(f"reference geometry {self.name} has no PHI blocks")
 
     def init_grid(self):
         self.L.ref_init_grid()

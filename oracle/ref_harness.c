@@ -455,3 +455,23 @@ int ref_continue(void)
 static int h_output_c;
 static void h_output(void *a) { (void)a; output(0, 0, h_output_c); }
 int ref_output(int c) { h_output_c = c; return h_run(h_output, NULL); }
+
+/* renew_phi3 (:8315-8665), sr_phi (:1389-1574) and sr_e, as fdtd runs them
+ * after renew_e4_2 when the PHI blocks are compiled in (:901-907). */
+static void h_renew_phi3(void *a)
+{
+  (void)a;
+#if ORACLE_PHI
+  renew_phi3(0, 0);
+  sr_phi(0, 0);
+  sr_e(0, 0);
+#endif
+}
+int ref_renew_phi3(void)
+{
+#if ORACLE_PHI
+  return h_run(h_renew_phi3, NULL);
+#else
+  return -1;
+#endif
+}

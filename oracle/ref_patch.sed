@@ -24,3 +24,5 @@ s|^#define PROCESS_Nx 128$|#define PROCESS_Nx 1|
 s|^#define PROCESS_Ny 128$|#define PROCESS_Ny 1|
 s|^#define PACK_N 80000$|#define PACK_N ORACLE_PACK_N|
 s|^  const double a=1e-6;$|  const double a=ORACLE_SIGMA_A;|
+s|^#define Absorb_grid3 40  //particle$|#define Absorb_grid3 ORACLE_ABSORB3|
+s|^#define PHI(x) $|#if ORACLE_PHI\n#define PHI(...) __VA_ARGS__\n#else\n#define PHI(...)\n#endif|

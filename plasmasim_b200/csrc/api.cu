@@ -18,6 +18,7 @@
 #include "push_tiled.cuh"
 #include "relayout.cuh"
 #include "adjoint.cuh"
+#include "poisson3d.cuh"
 
 using namespace pb;
 
@@ -69,6 +70,11 @@ struct pic_ctx {
   double* acc = nullptr;        // 33 thrust/energy sums, then 4 Gauss-law values
   unsigned long long* maxbits = nullptr;
   double* fave = nullptr;       // 27
+  // Poisson cleaning (renew_phi3): two interior-sized work arrays, the sine
+  // tables of the three axes and their sin^2 eigenvalue terms
+  void* phi_w = nullptr;
+  void* phi_sines = nullptr;
+  double* phi_sin2 = nullptr;
   unsigned long long* err = nullptr;  // ERR_COUNT
   // import/export staging
   void* stage = nullptr;
@@ -281,6 +287,92 @@ int do_fold(pic_ctx* c) {
   fold_y_kernel<real><<<grid_blocks((long long)c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
   CKL();
   return PIC_OK;
+}
+
+// renew_phi3 + sr_phi + sr_e (:8315-8665, :1389-1574): the Gauss residual,
+// three sine transforms, the eigenvalue division, three inverse transforms,
+// phi on the interior, its ghost planes wrapped, E corrected and wrapped.
+template <typename real>
+int do_poisson(pic_ctx* c) {
+  const Geom& g = c->g;
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  const int ns[3] = {g.nx, g.ny, g.nz};
+  long long soff[3];
+  soff[0] = 0;
+  soff[1] = (long long)g.nx * g.nx;
+  soff[2] = soff[1] + (long long)g.ny * g.ny;
+  const long long stotal = soff[2] + (long long)g.nz * g.nz;
+  if (!c->phi_w) {
+    CK(cudaMalloc(&c->phi_w, 2 * (size_t)n * sizeof(real)));
+    CK(cudaMalloc(&c->phi_sines, (size_t)stotal * sizeof(real)));
+    CK(cudaMalloc(&c->phi_sin2, (size_t)(g.nx + g.ny + g.nz) * sizeof(double)));
+    const double Pi = 3.14159265358979323846;
+    std::vector<real> S((size_t)stotal);
+    std::vector<double> s2;
+    for (int a = 0; a < 3; ++a) {
+      const int m = ns[a];
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) S[soff[a] + (long long)i * m + j] = (real)std::sin(Pi * (double)i * (double)j / (double)m);
+      for (int i = 0; i < m; ++i) {
+        const double v = std::sin(Pi * (double)i / (double)m / 2.);  // :8502-8504
+        s2.push_back(v * v);
+      }
+    }
+    CK(cudaMemcpy(c->phi_sines, S.data(), S.size() * sizeof(real), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->phi_sin2, s2.data(), s2.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  real* w0 = (real*)c->phi_w;
+  real* w1 = w0 + n;
+  const real* S = (const real*)c->phi_sines;
+  const double d24 = 24. * c->cfg.dx;
+  Fields<real> F = fields<real>(c);
+  phi3_rho_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(F, g, d24, c->cfg.q, c->cfg.e0,
+                                                                     c->cfg.absorb_grid3, w0);
+  CKL();
+  auto gemm = [&](DstGemm<real> a) -> int {
+    const long long tiles = (long long)((a.M + kDstTile - 1) / kDstTile) * ((a.N + kDstTile - 1) / kDstTile) * a.B;
+    const int blocks = (int)std::min<long long>(tiles, 148LL * 8);
+    a.sin2 = c->phi_sin2;
+    a.nx = g.nx; a.ny = g.ny; a.nz = g.nz;
+    a.h2 = (c->cfg.dx / 2.) * (c->cfg.dx / 2.);
+    dst3_gemm_kernel<real><<<blocks, 256, 0, c->stream>>>(a);
+    CKL();
+    return PIC_OK;
+  };
+  const long long yz = (long long)g.ny * g.nz;
+  // C = mul * L R / div. z: [x*y][z] x S_z; y: S_y x [y][z] per x; x: S_x x [x][y*z]
+  auto zpass = [&](const real* in, real* out, double mul, double div) {
+    DstGemm<real> a{};
+    a.L = in; a.lm = g.nz; a.R = S + soff[2]; a.rk = g.nz; a.C = out; a.cm = g.nz;
+    a.M = g.nx * g.ny; a.N = g.nz; a.K = g.nz; a.B = 1; a.mul = mul; a.div = div;
+    return gemm(a);
+  };
+  auto ypass = [&](const real* in, real* out, double mul, double div) {
+    DstGemm<real> a{};
+    a.L = S + soff[1]; a.lm = g.ny; a.R = in; a.rb = yz; a.rk = g.nz; a.C = out; a.cb = yz; a.cm = g.nz;
+    a.M = g.ny; a.N = g.nz; a.K = g.ny; a.B = g.nx; a.mul = mul; a.div = div;
+    return gemm(a);
+  };
+  auto xpass = [&](const real* in, real* out, double mul, double div, int solve) {
+    DstGemm<real> a{};
+    a.L = S + soff[0]; a.lm = g.nx; a.R = in; a.rk = yz; a.C = out; a.cm = yz;
+    a.M = g.nx; a.N = (int)yz; a.K = g.nx; a.B = 1; a.mul = mul; a.div = div; a.solve = solve;
+    return gemm(a);
+  };
+  CKR(zpass(w0, w1, 1., 1.));                    // fft_z
+  CKR(ypass(w1, w0, 1., 1.));                    // fft_y
+  CKR(xpass(w0, w1, 1., 1., 1));                 // fft_x and the division by A
+  CKR(xpass(w1, w0, 2., (double)g.nx, 0));       // inv_fft_x
+  CKR(ypass(w0, w1, 2., (double)g.ny));          // inv_fft_y
+  CKR(zpass(w1, w0, 2., (double)g.nz));          // inv_fft_z
+  phi3_store_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(F, g, w0);
+  CKL();
+  static const int phi_id[1] = {F_PHI};
+  CKR(wrap_planes<real>(c, phi_id, 1));          // sr_phi's exchange
+  phi3_grad_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(F, g, d24);
+  CKL();
+  static const int e_ids[3] = {F_EX, F_EY, F_EZ};
+  return wrap_planes<real>(c, e_ids, 3);         // sr_e
 }
 
 int do_renew_grid(pic_ctx* c) {
@@ -673,6 +765,7 @@ int do_step(pic_ctx* c) {
   CKR(do_renew_b<real>(c));
   CKR(do_fold<real>(c));
   CKR(do_renew_e<real>(c));
+  if (c->cfg.poisson_clean) CKR(do_poisson<real>(c));
   CKR(phase_mark(c, PH_FIELD));
   if (c->cfg.diag_every_step) {
     CKR(phase_mark(c, PH_DIAG));
@@ -774,7 +867,7 @@ __global__ void grid_export_kernel(Fields<real> F, int nodes, double* rec) {
                        F_JIX, F_JIY, F_JIZ, F_JEX, F_JEY, F_JEZ, F_NI, F_NE};
 #pragma unroll
   for (int q = 0; q < 17; ++q) r[q] = (double)F.f[map[q]][n];
-  r[17] = 0.0;
+  r[17] = (double)F.f[F_PHI][n];
 }
 
 template <typename real>
@@ -786,6 +879,7 @@ __global__ void grid_import_kernel(Fields<real> F, int nodes, const double* rec)
                        F_JIX, F_JIY, F_JIZ, F_JEX, F_JEY, F_JEZ, F_NI, F_NE};
 #pragma unroll
   for (int q = 0; q < 17; ++q) F.f[map[q]][n] = (real)r[q];
+  F.f[F_PHI][n] = (real)r[17];
   F.f[F_DBX][n] = (real)(r[0] - r[3]);
   F.f[F_DBY][n] = (real)(r[1] - r[4]);
   F.f[F_DBZ][n] = (real)(r[2] - r[5]);
@@ -954,6 +1048,8 @@ int pic_config_default(pic_config* k, int nx, int ny, int nz) {
   k->add_interval = 5;
   k->sort_interval = 500;
   k->diag_every_step = 1;
+  k->poisson_clean = 0;
+  k->absorb_grid3 = 40;
   k->capacity = 0;
   k->seed_p = 0;
   k->seed_v = 50;
@@ -969,6 +1065,7 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
   if (k.np < 1 || !(k.dx > 0) || !(k.dt > 0) || !(k.c > 0) || !(k.mi > 0) || !(k.me > 0)) return PIC_ERR_ARG;
   if (k.precision != 32 && k.precision != 64) return PIC_ERR_ARG;
   if (k.add_interval < 1 || k.sort_interval < 1) return PIC_ERR_ARG;
+  if (k.absorb_grid3 < 0 || (k.poisson_clean != 0 && k.poisson_clean != 1)) return PIC_ERR_ARG;
   if (cudaSetDevice(k.device) != cudaSuccess) return PIC_ERR_CUDA;
   pic_ctx* c = new (std::nothrow) pic_ctx();
   if (!c) return PIC_ERR_ARG;
@@ -1084,6 +1181,9 @@ int pic_destroy(pic_ctx* c) {
   cudaFree(c->acc);
   cudaFree(c->maxbits);
   cudaFree(c->fave);
+  cudaFree(c->phi_w);
+  cudaFree(c->phi_sines);
+  cudaFree(c->phi_sin2);
   cudaFree(c->err);
   cudaFree(c->stage);
   cudaFree(c->flags);
@@ -1185,9 +1285,16 @@ int pic_thrust_fave(pic_ctx* c, double* Fave27, int reset) {
   return PIC_OK;
 }
 
+int pic_poisson_clean(pic_ctx* c) {
+  CKR(check_ctx(c));
+  if (!c->grid_ready) return PIC_ERR_STATE;
+  return DISPATCH(c, do_poisson)(c);
+}
+
 int pic_objective(pic_ctx* c, int nsteps, double* J) {
   CKR(check_ctx(c));
   if (!J || nsteps < 0) return PIC_ERR_ARG;
+  if (c->cfg.poisson_clean) return PIC_ERR_ARG;  // the adjoint does not differentiate the cleaning
   if (!c->grid_ready) return PIC_ERR_STATE;
   double out[3] = {0, 0, 0};
   CKR(DISPATCH(c, do_adjoint)(c, nsteps, 1, false, out));
@@ -1198,6 +1305,7 @@ int pic_objective(pic_ctx* c, int nsteps, double* J) {
 int pic_adjoint(pic_ctx* c, int nsteps, int checkpoint_every, double* out3) {
   CKR(check_ctx(c));
   if (!out3 || nsteps < 1 || checkpoint_every < 1) return PIC_ERR_ARG;
+  if (c->cfg.poisson_clean) return PIC_ERR_ARG;
   if (!c->grid_ready) return PIC_ERR_STATE;
   double out[3] = {0, 0, 0};
   CKR(DISPATCH(c, do_adjoint)(c, nsteps, checkpoint_every, true, out));
@@ -1224,6 +1332,7 @@ int pic_fdtd(pic_ctx* c, int nsteps) {
   c->c_add = 0;
   c->c_thrust = 0;
   CKR(DISPATCH(c, do_add_flat)(c));
+  if (c->cfg.poisson_clean) CKR(DISPATCH(c, do_poisson)(c));  // :676-681
   return pic_step(c, nsteps);
 }
 

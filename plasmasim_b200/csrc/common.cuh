@@ -42,7 +42,7 @@ struct Geom {
 // DB = B - B0 the induced part the curl updates work on.
 enum FieldId {
   F_EX, F_EY, F_EZ, F_BX, F_BY, F_BZ, F_DBX, F_DBY, F_DBZ, F_B0X, F_B0Y, F_B0Z,
-  F_JIX, F_JIY, F_JIZ, F_JEX, F_JEY, F_JEZ, F_NI, F_NE, F_COUNT
+  F_JIX, F_JIY, F_JIZ, F_JEX, F_JEY, F_JEZ, F_NI, F_NE, F_PHI, F_COUNT
 };
 
 template <typename real>

@@ -65,6 +65,7 @@ __global__ void init_fields_kernel(Fields<real> F, Geom g, DipoleParams d) {
   F.f[F_EX][n] = (real)0; F.f[F_EY][n] = (real)0; F.f[F_EZ][n] = (real)0;
 #pragma unroll
   for (int q = F_JIX; q <= F_NE; ++q) F.f[q][n] = (real)0;
+  F.f[F_PHI][n] = (real)0;  // :325
 }
 
 struct BParams {

@@ -48,8 +48,9 @@ class _CConfig(C.Structure):
         ("absorb_grid", C.c_int), ("absorb_grid2", C.c_int),
         ("sigma_a", C.c_double), ("dipole_cutoff", C.c_double),
         ("add_interval", C.c_int), ("sort_interval", C.c_int),
-        ("diag_every_step", C.c_int), ("reserved0", C.c_int),
+        ("diag_every_step", C.c_int), ("poisson_clean", C.c_int),
         ("capacity", C.c_longlong), ("seed_p", C.c_ulonglong), ("seed_v", C.c_ulonglong),
+        ("absorb_grid3", C.c_int), ("reserved1", C.c_int),
     ]
 
 
@@ -88,9 +89,11 @@ class PicConfig:
     add_interval: int = 5
     sort_interval: int = 500
     diag_every_step: int = 1
+    poisson_clean: int = 0
     capacity: int = 0
     seed_p: int = 0
     seed_v: int = 50
+    absorb_grid3: int = 40
 
     @classmethod
     def normalized(cls, nx, ny, nz, np_, **kw) -> "PicConfig":
@@ -126,7 +129,7 @@ EXPORTED = [
     "pic_set_grid", "pic_rng_counters", "pic_status", "pic_synchronize", "pic_get_stream",
     "pic_error_string", "pic_set_timing", "pic_read_timing", "pic_gauss_residual_noalloc",
     "pic_objective", "pic_adjoint", "pic_save_checkpoint", "pic_load_checkpoint", "pic_write_output",
-    "pic_append_thrust", "pic_append_thrust_ave",
+    "pic_append_thrust", "pic_append_thrust_ave", "pic_poisson_clean",
     "pic2d_config_normalized", "pic2d_create", "pic2d_destroy", "pic2d_init", "pic2d_step",
     "pic2d_thrust", "pic2d_particle_count", "pic2d_get_particles", "pic2d_get_grid",
     "pic2d_autotune", "pic2d_set_graph", "pic2d_status", "pic2d_get_stream",
@@ -159,6 +162,7 @@ def load_library(path: str = LIB_PATH):
     L.pic_thrust_f.argtypes = [vp, _dp, _dp]
     L.pic_thrust_fave.argtypes = [vp, _dp, C.c_int]
     L.pic_gauss_residual.argtypes = [vp, _dp]
+    L.pic_poisson_clean.argtypes = [vp]
     L.pic_objective.argtypes = [vp, C.c_int, _dp]
     for name in ["pic_save_checkpoint", "pic_load_checkpoint"]:
         getattr(L, name).argtypes = [vp, C.c_char_p, C.c_int, C.c_int]
@@ -270,6 +274,10 @@ class Pic3D:
         F = np.zeros(27)
         self._call("pic_thrust_fave", _ptr(F), 1 if reset else 0)
         return F
+
+    def poisson_clean(self):
+        """renew_phi3 + sr_phi + sr_e: the Poisson correction of E."""
+        self._call("pic_poisson_clean")
 
     def gauss_residual(self):
         out = np.zeros(4)
