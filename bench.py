@@ -379,6 +379,42 @@ def run_adjoint(nsteps: int = 200, every: int = 20):
             "fd_checks": checks}
 
 
+def run_poisson(reps: int = 10):
+    """Poisson cleaning (pic_poisson_clean: renew_phi3 + sr_phi + sr_e) on the
+    bench grid, FP32, timed with CUDA events on the context's stream. FLOPs:
+    the six sine-transform GEMMs, 2 * 2 * N * (nx + ny + nz) for N interior
+    cells (forward and inverse along each axis)."""
+    import torch
+
+    from plasmasim_b200 import Pic3D
+
+    cfg = make_config(32, 0)
+    cfg.absorb_grid3 = 0
+    P = Pic3D(cfg)
+    P.init_grid()
+    P.init_particle_flat()
+    P.fdtd(0)
+    P.step(2)
+    P.poisson_clean()
+    P.synchronize()
+    stream = torch.cuda.ExternalStream(P.stream_handle())
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(reps):
+        P.poisson_clean()
+    stop.record(stream)
+    stop.synchronize()
+    ms = start.elapsed_time(stop) / reps
+    P.close()
+    n = NX * NY * NZ
+    flop = 4.0 * n * (NX + NY + NZ)
+    # nominal FP32 CUDA-core peak: 148 SMs x 128 FMA/clock x 2 x 1.965 GHz
+    fp32_peak = 148 * 128 * 2 * 1.965e9
+    return {"workload": f"{NX}x{NY}x{NZ} interior cells, FP32, Absorb_grid3 = 0", "ms": ms,
+            "gflop": flop / 1e9, "tflops": flop / ms / 1e9, "fp32_simt_peak_tflops": fp32_peak / 1e12,
+            "frac_of_fp32_simt_peak": flop / (ms * 1e-3) / fp32_peak}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -393,6 +429,7 @@ def main():
     ap.add_argument("--ppc", type=int, default=64, help="particles per cell per species")
     ap.add_argument("--no-batch2d", action="store_true", help="skip the batched 2D runs")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
+    ap.add_argument("--no-poisson", action="store_true", help="skip the Poisson cleaning measurement")
     ap.add_argument("--runs2d", type=int, default=256, help="runs of the batched 2D workload")
     args = ap.parse_args()
     global NX, NY, NZ, PPC
@@ -500,6 +537,15 @@ def main():
             log("adjoint failed:", exc)
             adjoint = {"error": str(exc)[:200]}
 
+    poisson = None
+    if not args.no_poisson and world == 1:
+        try:
+            poisson = run_poisson()
+            poisson["over_step"] = poisson["ms"] / (ms_max / args.steps)
+        except Exception as exc:
+            log("poisson failed:", exc)
+            poisson = {"error": str(exc)[:200]}
+
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         if ensure_reference_lib("cube64"):
@@ -537,7 +583,7 @@ def main():
             "phase_ms_per_step": {k: v / args.steps for k, v in out["phase_ms"].items()},
             "clocks": out["clocks"], "gpu_launches": out["launches"],
             "device_errors": out["errors"], "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu,
-            "batch2d": batch2d, "adjoint": adjoint,
+            "batch2d": batch2d, "adjoint": adjoint, "poisson": poisson,
         }
         print(json.dumps(line))
     if dist is not None:
