@@ -33,6 +33,7 @@ extern "C" {
 #define PIC_ERR_STATE 4      /* call out of order (e.g. step before init) */
 #define PIC_ERR_DEVICE 5     /* device-side counters report lost work (pic_status) */
 #define PIC_ERR_TOO_LARGE 6  /* input larger than a fixed-size scratch allows */
+#define PIC_ERR_COMM 7       /* an exchange between ranks failed (transport error or timeout) */
 
 #define PIC_ION 0
 #define PIC_ELECTRON 1
@@ -78,10 +79,57 @@ typedef struct pic_config {
   unsigned long long seed_p; /* position stream key (init_particle_flat :444: 0) */
   unsigned long long seed_v; /* velocity stream key (:445: 50) */
   int absorb_grid3;        /* Absorb_grid3 (:97, 40): cells of each boundary left out of renew_phi3's residual */
+  int procs_x, procs_y;    /* PROCESS_Nx, PROCESS_Ny (:100-101): the x-y decomposition, 1 x 1 by default;
+                              nx, ny are then the cells of one rank (Grid_Nx, Grid_Ny) */
+  int rank_x, rank_y;      /* myrank_x, myrank_y (:205-206) of this context */
   int reserved1;
 } pic_config;
 
 typedef struct pic_ctx pic_ctx;
+
+/* Domain decomposition (PROCESS_Nx x PROCESS_Ny > 1). Every exchange of the
+ * reference's MPI code -- sr_b, sr_e, sr_current2, sr_particle (:1001-2555)
+ * and thrust_f's MPI_Allreduce -- goes through a transport that the caller
+ * provides; ranks are numbered myrank_y * procs_x + myrank_x, as main() does.
+ * All ranks make the same calls in the same order (one host thread per rank).
+ *  sendrecv: send `send_bytes` of device memory at `send` to rank `dest` and
+ *            receive `recv_bytes` of device memory into `recv` from rank `src`
+ *            (a rank may name itself); both ordered on `stream` (the context's
+ *            cudaStream_t): the send reads what the stream's earlier work
+ *            wrote, later work on the stream sees the received bytes.
+ *  allreduce_sum_f64: in-place sum of n doubles in device memory over all
+ *            ranks, ordered on `stream`; every rank gets the same bits.
+ * Both return 0 on success. */
+typedef struct pic_transport {
+  void *user;
+  int (*sendrecv)(void *user, const void *send, size_t send_bytes, int dest,
+                  void *recv, size_t recv_bytes, int src, void *stream);
+  int (*allreduce_sum_f64)(void *user, double *buf, int n, void *stream);
+} pic_transport;
+
+/* Installs the transport of a context whose configuration has
+ * procs_x * procs_y > 1 (or a single-rank context that should exchange
+ * through it instead of its in-place wraps); the transport must outlive the
+ * context's use of it. */
+int pic_set_transport(pic_ctx *ctx, const pic_transport *t);
+
+/* In-process transport: the ranks are contexts of one process, each driven by
+ * its own host thread, on one GPU or several; device-to-device copies ordered
+ * with CUDA events, rendezvous on the host (a wait that sees no partner for
+ * 60 s fails with PIC_ERR_COMM instead of blocking). */
+typedef struct pic_group pic_group;
+int pic_group_create(int nranks, pic_group **out);
+int pic_group_destroy(pic_group *group);
+int pic_group_transport(pic_group *group, int rank, pic_transport *out);
+
+/* NCCL transport: one process (or thread) per GPU. pic_nccl_unique_id fills
+ * the 128-byte id on one rank; the caller shares it (e.g. through
+ * torch.distributed's store) and every rank calls
+ * pic_nccl_transport_create with it. libnccl.so.2 is loaded at run time. */
+int pic_nccl_unique_id(unsigned char id[128]);
+int pic_nccl_transport_create(const unsigned char id[128], int nranks, int rank, int device,
+                              pic_transport *out);
+int pic_nccl_transport_destroy(pic_transport *t);
 
 /* Fills *cfg with the reference's own defaults (:52-103) for a one-domain run
  * of nx*ny*nz cells: MKSA constants, dx = 1.5, dt = 1.5e-9, Np = 16, ... */

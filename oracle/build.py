@@ -51,11 +51,11 @@ MKSA = dict(
 )
 
 
-def _geom(nx, ny, nz, np_, absorb=0, absorb2=0, threads=1, pack=20000, absorb3=40, phi=0):
+def _geom(nx, ny, nz, np_, absorb=0, absorb2=0, threads=1, pack=20000, absorb3=40, phi=0, pnx=1, pny=1):
     return dict(ORACLE_NX=nx, ORACLE_NY=ny, ORACLE_NZ=nz, ORACLE_NP=np_,
                 ORACLE_ABSORB=absorb, ORACLE_ABSORB2=absorb2,
                 ORACLE_THREADS=threads, ORACLE_PACK_N=pack,
-                ORACLE_ABSORB3=absorb3, ORACLE_PHI=phi)
+                ORACLE_ABSORB3=absorb3, ORACLE_PHI=phi, ORACLE_PNX=pnx, ORACLE_PNY=pny)
 
 
 REF_CONFIGS = {
@@ -75,6 +75,12 @@ REF_CONFIGS = {
     # an 8^3 grid)
     "tiny_phi": {**NORMALIZED, **_geom(8, 8, 8, 4, absorb3=0, phi=1)},
     "tiny_phi1": {**NORMALIZED, **_geom(8, 8, 8, 4, absorb3=1, phi=1)},
+    # the reference as an MPI job of 2 x 1 and 2 x 2 ranks of 8^3 cells each
+    # (oracle/shim/mpi_shim.c runs the ranks as processes; oracle/multirank.py
+    # drives them); absorbing layers 2 and 3 cells wide on the global domain
+    "tiny_2x1": {**NORMALIZED, **_geom(8, 8, 8, 4, pnx=2, pny=1)},
+    "tiny_2x2": {**NORMALIZED, **_geom(8, 8, 8, 4, pnx=2, pny=2)},
+    "damped_2x2": {**NORMALIZED, **_geom(8, 8, 10, 2, absorb=2, absorb2=3, pnx=2, pny=2), "ORACLE_SIGMA_A": 0.05},
 }
 
 

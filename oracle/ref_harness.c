@@ -58,6 +58,11 @@ static int h_run(void (*fn)(void *), void *arg)
   return 0;
 }
 
+/* This process's rank coordinates (myrank_x, myrank_y of main :205-206); 0, 0
+ * in a build with PROCESS_Nx = PROCESS_Ny = 1. */
+static int h_rx(void) { int r = 0; MPI_Comm_rank(MPI_COMM_WORLD, &r); return r % PROCESS_Nx; }
+static int h_ry(void) { int r = 0; MPI_Comm_rank(MPI_COMM_WORLD, &r); return r / PROCESS_Nx; }
+
 /* --- grid access --------------------------------------------------------- */
 long ref_grid_nodes(void) { return (long)(Grid_Nx + 4) * (Grid_Ny + 4) * (Grid_Nz + 4); }
 void ref_get_grid(double *out) { memcpy(out, grid, sizeof(grid)); }
@@ -65,7 +70,7 @@ void ref_set_grid(const double *in) { memcpy(grid, in, sizeof(grid)); }
 void ref_get_sigma(double *out) { memcpy(out, sigma, sizeof(sigma)); }
 void ref_get_grid_thread(int t, double *out) { memcpy(out, grid_thread[t], sizeof(grid_thread[t])); }
 
-static void h_init_grid(void *a) { (void)a; init_grid(0, 0); }
+static void h_init_grid(void *a) { (void)a; init_grid(h_rx(), h_ry()); }
 int ref_init_grid(void) { return h_run(h_init_grid, NULL); }
 
 /* --- RNG streams: the same seeds as init_particle_flat (:437-446) -------- */
@@ -76,8 +81,8 @@ void ref_init_rng(void)
     if (!rnd_p[i]) rnd_p[i] = gsl_rng_alloc(gsl_rng_rand);
     if (!rnd_v[i]) rnd_v[i] = gsl_rng_alloc(gsl_rng_rand);
     if (!rnd_i[i]) rnd_i[i] = gsl_rng_alloc(gsl_rng_rand);
-    gsl_rng_set(rnd_p[i], (0 * PROCESS_Nx + 0) * 10000 + i * 100);
-    gsl_rng_set(rnd_v[i], (0 * PROCESS_Nx + 0) * 10000 + i * 100 + 50);
+    gsl_rng_set(rnd_p[i], (h_ry() * PROCESS_Nx + h_rx()) * 10000 + i * 100);
+    gsl_rng_set(rnd_v[i], (h_ry() * PROCESS_Nx + h_rx()) * 10000 + i * 100 + 50);
     gsl_rng_set(rnd_i[i], i * 10);
     particle_flag[i] = 1;
   }
@@ -114,7 +119,7 @@ static void h_free_all(void)
   h_have_particles = 0;
 }
 
-static void h_init_particles(void *a) { (void)a; init_particle_flat(h_ion, h_ion_start, h_el, h_el_start, 0, 0); }
+static void h_init_particles(void *a) { (void)a; init_particle_flat(h_ion, h_ion_start, h_el, h_el_start, h_rx(), h_ry()); }
 int ref_init_particle_flat(void)
 {
   h_free_all();
@@ -195,9 +200,11 @@ long ref_get_particles(int species, double *rows, int *flag, long cap)
 /* Push + J deposit loop, restated from fdtd PIC/3d_pic458_domain.c:731-812. */
 static void h_push_j_list(Particle *start, int thread, int electron)
 {
-  const double ax0 = Absorb_grid2 * dx, ay0 = Absorb_grid2 * dx, az0 = Absorb_grid2 * dx;
-  const double ax1 = (PROCESS_Nx * Grid_Nx + 4 - Absorb_grid2) * dx;
-  const double ay1 = (PROCESS_Ny * Grid_Ny + 4 - Absorb_grid2) * dx;
+  const int rx = h_rx(), ry = h_ry();
+  const double ax0 = Absorb_grid2 * dx - rx * Grid_Nx * dx, ay0 = Absorb_grid2 * dx - ry * Grid_Ny * dx;
+  const double az0 = Absorb_grid2 * dx;
+  const double ax1 = (PROCESS_Nx * Grid_Nx + 4 - Absorb_grid2) * dx - rx * Grid_Nx * dx;
+  const double ay1 = (PROCESS_Ny * Grid_Ny + 4 - Absorb_grid2) * dx - ry * Grid_Ny * dx;
   const double az1 = (Grid_Nz + 4 - Absorb_grid2) * dx;
   const double d3x = (Grid_Nx + 4) * dx, d3y = (Grid_Ny + 4) * dx, d3z = (Grid_Nz + 4) * dx;
   const double dx0 = 0.;
@@ -209,7 +216,7 @@ static void h_push_j_list(Particle *start, int thread, int electron)
       p->y += p->vy * dth;
       p->z += p->vz * dth;
     } else {
-      cal_track4(p, electron ? -me : mi, 0, 0);
+      cal_track4(p, electron ? -me : mi, h_rx(), h_ry());
     }
     if (p->x < d3x && p->x >= dx0 && p->y < d3y && p->y >= dx0 && p->z < d3z && p->z >= dx0) {
       if (electron) shape_func_electron0_j_2(p, thread);
@@ -271,13 +278,14 @@ void ref_thrust_sums(double *out, int include_tail)
 {
   int i, k, l, m, s;
   double F[27], E[6];
+  const int rx = h_rx(), ry = h_ry();  /* this rank's part of the sums (thrust_f :4971, :4984) */
   for (i = 0; i < 27; i++) F[i] = 0.;
   for (i = 0; i < 6; i++) E[i] = 0.;
   for (k = 2; k < Grid_Nx + 2; k++)
     for (l = 2; l < Grid_Ny + 2; l++)
       for (m = 2; m < Grid_Nz + 2; m++)
-        if (k - 2 < PROCESS_Nx * Grid_Nx * 0.8 && k - 2 > PROCESS_Nx * Grid_Nx * 0.2 &&
-            l - 2 < PROCESS_Ny * Grid_Ny * 0.8 && l - 2 > PROCESS_Ny * Grid_Ny * 0.2 &&
+        if (rx * Grid_Nx + k - 2 < PROCESS_Nx * Grid_Nx * 0.8 && rx * Grid_Nx + k - 2 > PROCESS_Nx * Grid_Nx * 0.2 &&
+            ry * Grid_Ny + l - 2 < PROCESS_Ny * Grid_Ny * 0.8 && ry * Grid_Ny + l - 2 > PROCESS_Ny * Grid_Ny * 0.2 &&
             m - 2 < Grid_Nz * 0.8 && m - 2 > Grid_Nz * 0.2) {
           E[0] += 0.5 * (grid[k][l][m].ex * grid[k][l][m].ex + grid[k][l][m].ey * grid[k][l][m].ey + grid[k][l][m].ez * grid[k][l][m].ez) * e0;
           E[1] += 0.5 * (grid[k][l][m].bx * grid[k][l][m].bx + grid[k][l][m].by * grid[k][l][m].by + grid[k][l][m].bz * grid[k][l][m].bz) / mu0;
@@ -290,8 +298,10 @@ void ref_thrust_sums(double *out, int include_tail)
       Particle *p = s == 0 ? h_ion_start[i] : h_el_start[i];
       for (; p && (include_tail || p->next_particle != NULL); p = p->next_particle) {
         double ex, ey, ez, bx, by, bz;
-        if (!(p->x < PROCESS_Nx * Grid_Nx * dx * 0.8 && p->x > PROCESS_Nx * Grid_Nx * dx * 0.2 &&
-              p->y < PROCESS_Ny * Grid_Ny * dx * 0.8 && p->y > PROCESS_Ny * Grid_Ny * dx * 0.2 &&
+        if (!(rx * Grid_Nx * dx + p->x < PROCESS_Nx * Grid_Nx * dx * 0.8 &&
+              rx * Grid_Nx * dx + p->x > PROCESS_Nx * Grid_Nx * dx * 0.2 &&
+              ry * Grid_Ny * dx + p->y < PROCESS_Ny * Grid_Ny * dx * 0.8 &&
+              ry * Grid_Ny * dx + p->y > PROCESS_Ny * Grid_Ny * dx * 0.2 &&
               p->z < Grid_Nz * dx * 0.8 && p->z > Grid_Nz * dx * 0.2)) continue;
         shape_func_v2(p, &ex, &ey, &ez, &bx, &by, &bz);
         F[0] += sg * q * (ex + p->vy * bz - p->vz * by) * p->n * dx * dx * dx;
@@ -330,7 +340,7 @@ static void h_op(void *arg)
   switch (op) {
   case REF_RENEW_GRID: renew_grid(); break;
   case REF_RENEW_B: renew_b4_2(); break;
-  case REF_SR_B: sr_b(0, 0); break;
+  case REF_SR_B: sr_b(h_rx(), h_ry()); break;
   case REF_PUSH_J:
     for (i = 0; i < THREAD_N; i++) {
       h_push_j_list(h_ion_start[i], i, 0);
@@ -344,23 +354,23 @@ static void h_op(void *arg)
     }
     break;
   case REF_REDUCE: h_reduce_threads(); break;
-  case REF_SR_CURRENT: sr_current2(0, 0); break;
+  case REF_SR_CURRENT: sr_current2(h_rx(), h_ry()); break;
   case REF_RENEW_E: renew_e4_2(); break;
-  case REF_SR_E: sr_e(0, 0); break;
-  case REF_SR_PARTICLE: sr_particle(h_ion, h_ion_start, h_el, h_el_start, 0, 0); break;
+  case REF_SR_E: sr_e(h_rx(), h_ry()); break;
+  case REF_SR_PARTICLE: sr_particle(h_ion, h_ion_start, h_el, h_el_start, h_rx(), h_ry()); break;
   case REF_ADD_FLAT:
-    add_ion_flat(h_ion, h_ion_start, 0, 0);
-    add_electron_flat(h_el, h_el_start, 0, 0);
+    add_ion_flat(h_ion, h_ion_start, h_rx(), h_ry());
+    add_electron_flat(h_el, h_el_start, h_rx(), h_ry());
     break;
   case REF_SORT:
     sorting(h_ion, h_ion_start);
     sorting(h_el, h_el_start);
     break;
   case REF_THRUST_F:
-    thrust_f(0, 0, 0, h_ion, h_ion_start, h_el, h_el_start);
+    thrust_f(h_rx(), h_ry(), 0, h_ion, h_ion_start, h_el, h_el_start);
     break;
   case REF_FDTD:
-    fdtd(h_ion, h_ion_start, h_el, h_el_start, 0, 0, 0);
+    fdtd(h_ion, h_ion_start, h_el, h_el_start, h_rx(), h_ry(), 0);
     break;
   default: break;
   }
@@ -397,27 +407,27 @@ static void h_loop(void *a)
       sorting(h_el, h_el_start);
     }
     if (h_c_add > h_loop_args[2] - 1) {
-      add_ion_flat(h_ion, h_ion_start, 0, 0);
-      add_electron_flat(h_el, h_el_start, 0, 0);
+      add_ion_flat(h_ion, h_ion_start, h_rx(), h_ry());
+      add_electron_flat(h_el, h_el_start, h_rx(), h_ry());
       h_c_add = 0;
     }
     renew_b4_2();
-    sr_b(0, 0);
+    sr_b(h_rx(), h_ry());
     for (i = 0; i < THREAD_N; i++) {
       h_push_j_list(h_ion_start[i], i, 0);
       h_push_j_list(h_el_start[i], i, 1);
     }
     renew_b4_2();
-    sr_b(0, 0);
+    sr_b(h_rx(), h_ry());
     for (i = 0; i < THREAD_N; i++) {
       h_drift_n_list(h_ion_start[i], i, 0);
       h_drift_n_list(h_el_start[i], i, 1);
     }
     h_reduce_threads();
-    sr_current2(0, 0);
+    sr_current2(h_rx(), h_ry());
     renew_e4_2();
-    sr_e(0, 0);
-    sr_particle(h_ion, h_ion_start, h_el, h_el_start, 0, 0);
+    sr_e(h_rx(), h_ry());
+    sr_particle(h_ion, h_ion_start, h_el, h_el_start, h_rx(), h_ry());
     h_c_add++;
     h_c_thrust++;
   }
@@ -437,12 +447,12 @@ int ref_unmatched_sends(void) { return oracle_mpi_unmatched(); }
 /* --- the reference's own file writers and reader ----------------------- */
 /* suspend_job (:7629-7674) and continue_job (:7676-7911) in the working
  * directory, on the harness's particle lists. */
-static void h_suspend(void *a) { (void)a; suspend_job(h_ion, h_ion_start, h_el, h_el_start, 0, 0); }
+static void h_suspend(void *a) { (void)a; suspend_job(h_ion, h_ion_start, h_el, h_el_start, h_rx(), h_ry()); }
 int ref_suspend(void) { return h_run(h_suspend, NULL); }
 static void h_continue(void *a)
 {
   (void)a;
-  continue_job(h_ion, h_ion_start, h_el, h_el_start, 0, 0);
+  continue_job(h_ion, h_ion_start, h_el, h_el_start, h_rx(), h_ry());
 }
 int ref_continue(void)
 {
@@ -453,7 +463,7 @@ int ref_continue(void)
 }
 /* output (:4834-4883): fdtd458-0-0-<c>.dat in the working directory. */
 static int h_output_c;
-static void h_output(void *a) { (void)a; output(0, 0, h_output_c); }
+static void h_output(void *a) { (void)a; output(h_rx(), h_ry(), h_output_c); }
 int ref_output(int c) { h_output_c = c; return h_run(h_output, NULL); }
 
 /* renew_phi3 (:8315-8665), sr_phi (:1389-1574) and sr_e, as fdtd runs them
@@ -462,9 +472,9 @@ static void h_renew_phi3(void *a)
 {
   (void)a;
 #if ORACLE_PHI
-  renew_phi3(0, 0);
-  sr_phi(0, 0);
-  sr_e(0, 0);
+  renew_phi3(h_rx(), h_ry());
+  sr_phi(h_rx(), h_ry());
+  sr_e(h_rx(), h_ry());
 #endif
 }
 int ref_renew_phi3(void)

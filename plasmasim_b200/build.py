@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libplasmab200.so")
 SOURCES = [os.path.join(HERE, "csrc", "api.cu"), os.path.join(HERE, "csrc", "noalloc.cu"),
-           os.path.join(HERE, "csrc", "pic2d.cu")]
+           os.path.join(HERE, "csrc", "pic2d.cu"), os.path.join(HERE, "csrc", "transport.cu")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -19,6 +19,7 @@
 #include "relayout.cuh"
 #include "adjoint.cuh"
 #include "poisson3d.cuh"
+#include "halo.cuh"
 
 using namespace pb;
 
@@ -75,6 +76,15 @@ struct pic_ctx {
   void* phi_w = nullptr;
   void* phi_sines = nullptr;
   double* phi_sin2 = nullptr;
+  // decomposed runs: the transport, the ghost-plane buffers and the particle
+  // packet lists of sr_particle (kMig lists of mig_cap records, counters)
+  pic_transport xport{};
+  bool has_xport = false;
+  void* halo_buf[2] = {nullptr, nullptr};  // send, receive
+  size_t halo_bytes = 0;
+  void* mig = nullptr;
+  int* mig_cnt = nullptr;
+  int mig_cap = 0;
   unsigned long long* err = nullptr;  // ERR_COUNT
   // import/export staging
   void* stage = nullptr;
@@ -195,10 +205,19 @@ PushConst<real> push_const(const pic_ctx* c, int s) {
   pc.nw = (real)species_weight(c);
   pc.ex_add = (real)(k.v_drift * k.imf_y);
   pc.ey_add = (real)(-k.v_drift * k.imf_x);
-  pc.bal_lo = k.absorb_grid2;
-  pc.bal_hx = k.nx + 4 - k.absorb_grid2;
-  pc.bal_hy = k.ny + 4 - k.absorb_grid2;
+  const Geom& g = c->g;
+  pc.bal_lx = k.absorb_grid2 - g.ox;
+  pc.bal_ly = k.absorb_grid2 - g.oy;
+  pc.bal_lz = k.absorb_grid2;
+  pc.bal_hx = g.gnx + 4 - k.absorb_grid2 - g.ox;
+  pc.bal_hy = g.gny + 4 - k.absorb_grid2 - g.oy;
   pc.bal_hz = k.nz + 4 - k.absorb_grid2;
+  pc.out = Outbox<real>{nullptr, 0, nullptr};
+  if (c->has_xport && c->mig) {  // list s of the packet lists is species s's outbox
+    pc.out.count = c->mig_cnt + s;
+    pc.out.cap = c->mig_cap;
+    pc.out.rec = (MigRec<real>*)c->mig + (size_t)s * c->mig_cap;
+  }
   pc.pjx = s == 0 ? F_JIX : F_JEX;
   pc.pjy = s == 0 ? F_JIY : F_JEY;
   pc.pjz = s == 0 ? F_JIZ : F_JEZ;
@@ -240,12 +259,184 @@ int do_init_grid(pic_ctx* c) {
   return PIC_OK;
 }
 
+// ------------------------------------------------- exchanges between ranks
+// Rank number of process-grid coordinates (periodic), as main() numbers them.
+int rank_at(const pic_ctx* c, int rx, int ry) {
+  const int px = c->cfg.procs_x, py = c->cfg.procs_y;
+  return ((ry % py + py) % py) * px + ((rx % px + px) % px);
+}
+
+int xfer(pic_ctx* c, const void* send, size_t sbytes, int dest, void* recv, size_t rbytes, int src) {
+  if (c->xport.sendrecv(c->xport.user, send, sbytes, dest, recv, rbytes, src, (void*)c->stream) != 0)
+    return PIC_ERR_COMM;
+  return PIC_OK;
+}
+
+// One transfer of two layers of every plane of s along `axis`: layers
+// send_layer, +1 to rank `dest`; from rank `src` into recv_layer, +1.
+template <typename real>
+int halo_exchange(pic_ctx* c, const PlaneSet<real>& s, const PlaneSet<real>& aux, int axis, int send_layer, int dest,
+                  int recv_layer, int src, int mode) {
+  const Geom& g = c->g;
+  const size_t n = (size_t)s.count * 2 * (size_t)std::max(g.gy * g.gz, g.gx * g.gz);
+  if (n * sizeof(real) > c->halo_bytes) {
+    cudaFree(c->halo_buf[0]);
+    cudaFree(c->halo_buf[1]);
+    c->halo_buf[0] = c->halo_buf[1] = nullptr;
+    c->halo_bytes = 0;
+    const size_t bytes = (size_t)8 * 2 * std::max(g.gy * g.gz, g.gx * g.gz) * sizeof(real);
+    CK(cudaMalloc(&c->halo_buf[0], bytes));
+    CK(cudaMalloc(&c->halo_buf[1], bytes));
+    c->halo_bytes = bytes;
+  }
+  const long long elems = (long long)s.count * 2 * halo_layer_nodes(g, axis);
+  real* sb = (real*)c->halo_buf[0];
+  real* rb = (real*)c->halo_buf[1];
+  halo_pack_kernel<real><<<grid_blocks(elems), kThreads, 0, c->stream>>>(s, g, axis, send_layer, sb);
+  CKL();
+  CKR(xfer(c, sb, elems * sizeof(real), dest, rb, elems * sizeof(real), src));
+  halo_unpack_kernel<real><<<grid_blocks(elems), kThreads, 0, c->stream>>>(s, aux, g, axis, recv_layer, rb, mode);
+  CKL();
+  return PIC_OK;
+}
+
+// sr_b / sr_e / sr_phi at any size (:1001-1387, :1389-1574): per axis (x, then
+// y over every x), layers N, N+1 to the next rank's ghosts 0, 1 and layers
+// 2, 3 to the previous rank's ghosts N+2, N+3, periodic over the ranks.
+template <typename real>
+int halo_ghosts(pic_ctx* c, const PlaneSet<real>& s, const PlaneSet<real>& aux, int mode) {
+  const int rx = c->cfg.rank_x, ry = c->cfg.rank_y;
+  for (int axis = 0; axis < 2; ++axis) {
+    const int N = axis == 0 ? c->g.nx : c->g.ny;
+    const int next = axis == 0 ? rank_at(c, rx + 1, ry) : rank_at(c, rx, ry + 1);
+    const int prev = axis == 0 ? rank_at(c, rx - 1, ry) : rank_at(c, rx, ry - 1);
+    CKR(halo_exchange<real>(c, s, aux, axis, N, next, 0, prev, mode));
+    CKR(halo_exchange<real>(c, s, aux, axis, 2, prev, N + 2, next, mode));
+  }
+  return PIC_OK;
+}
+
+// sr_current2 at any size (:1805-2039): per axis, ghosts N+2, N+3 added to
+// the next rank's layers 2, 3; ghosts 0, 1 added to the previous rank's N, N+1.
+template <typename real>
+int halo_fold(pic_ctx* c, const PlaneSet<real>& s) {
+  const int rx = c->cfg.rank_x, ry = c->cfg.rank_y;
+  for (int axis = 0; axis < 2; ++axis) {
+    const int N = axis == 0 ? c->g.nx : c->g.ny;
+    const int next = axis == 0 ? rank_at(c, rx + 1, ry) : rank_at(c, rx, ry + 1);
+    const int prev = axis == 0 ? rank_at(c, rx - 1, ry) : rank_at(c, rx, ry - 1);
+    CKR(halo_exchange<real>(c, s, s, axis, N + 2, next, 2, prev, HALO_ADD));
+    CKR(halo_exchange<real>(c, s, s, axis, 0, prev, N, next, HALO_ADD));
+  }
+  return PIC_OK;
+}
+
+// Particle packet lists of sr_particle: 0, 1 the species' outboxes, then the
+// split and received lists of the x and y passes.
+enum { MIG_OUT0 = 0, MIG_OUT1 = 1, MIG_XF, MIG_XB, MIG_YS, MIG_YF, MIG_YB, MIG_FIN, MIG_RA, MIG_RB, kMig };
+
+template <typename real>
+int ensure_mig(pic_ctx* c) {
+  if (c->mig) return PIC_OK;
+  const Geom& g = c->g;
+  // packets of one step: at most the particles of the outer two cell layers
+  // of the x and y faces; a list that overflows counts ERR_MIGRATION
+  const long long face = 2LL * ((long long)g.gy * g.gz + (long long)g.gx * g.gz);
+  const long long cap = std::min<long long>(face * std::max(c->cfg.np, 1) + 65536, 1LL << 30);
+  c->mig_cap = (int)cap;
+  CK(cudaMalloc(&c->mig, (size_t)kMig * cap * sizeof(MigRec<real>)));
+  CK(cudaMalloc(&c->mig_cnt, sizeof(int) * 16));
+  CK(cudaMemsetAsync(c->mig_cnt, 0, sizeof(int) * 16, c->stream));
+  return PIC_OK;
+}
+
+template <typename real>
+MigRec<real>* mig_list(pic_ctx* c, int q) {
+  return (MigRec<real>*)c->mig + (size_t)q * c->mig_cap;
+}
+
+// sr_particle between ranks (:2041-2555) for species s, after the push has
+// written the particles that left the rank's x-y interior to its outbox: the
+// x pass (forward and backward packets to the x neighbours, received packets
+// shifted by -/+ Nx cells), then the y pass over the particles still outside
+// in y, then the settled packets appended after the particle slots.
+template <typename real>
+int do_migrate_species(pic_ctx* c, int s) {
+  const Geom& g = c->g;
+  const int rx = c->cfg.rank_x, ry = c->cfg.rank_y;
+  int* cnt = c->mig_cnt;
+  const size_t rec = sizeof(MigRec<real>);
+  CK(cudaMemsetAsync(cnt + MIG_XF, 0, sizeof(int) * (kMig - MIG_XF), c->stream));
+  int h[16];
+  const int blocks = particle_blocks(c->mig_cap);
+  int in_list = MIG_OUT0 + s;
+  for (int axis = 0; axis < 2; ++axis) {
+    const int F = axis == 0 ? MIG_XF : MIG_YF, B = axis == 0 ? MIG_XB : MIG_YB;
+    const int S = axis == 0 ? MIG_YS : MIG_FIN;
+    const bool lo = axis == 0 ? g.xlo : g.ylo, hi = axis == 0 ? g.xhi : g.yhi;
+    // rank 0 drops its backward packets, the last rank (when it is not also
+    // rank 0) its forward ones (:2137-2146, :2237-2246)
+    mig_split_kernel<real><<<blocks, kThreads, 0, c->stream>>>(
+        mig_list<real>(c, in_list), cnt + in_list, g, axis, lo ? 1 : 0, (hi && !lo) ? 1 : 0, mig_list<real>(c, F),
+        cnt + F, mig_list<real>(c, B), cnt + B, mig_list<real>(c, S), cnt + S, c->mig_cap, c->err);
+    CKL();
+    const int next = axis == 0 ? rank_at(c, rx + 1, ry) : rank_at(c, rx, ry + 1);
+    const int prev = axis == 0 ? rank_at(c, rx - 1, ry) : rank_at(c, rx, ry - 1);
+    // counts first (the receiver sizes its copy), then the packets
+    CKR(xfer(c, cnt + F, sizeof(int), next, cnt + MIG_RA, sizeof(int), prev));
+    CKR(xfer(c, cnt + B, sizeof(int), prev, cnt + MIG_RB, sizeof(int), next));
+    CK(cudaMemcpyAsync(h, cnt, sizeof(int) * kMig, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const int nf = std::min(h[F], c->mig_cap), nb = std::min(h[B], c->mig_cap);
+    const int ra = std::min(h[MIG_RA], c->mig_cap), rb = std::min(h[MIG_RB], c->mig_cap);
+    CKR(xfer(c, mig_list<real>(c, F), nf * rec, next, mig_list<real>(c, MIG_RA), ra * rec, prev));
+    CKR(xfer(c, mig_list<real>(c, B), nb * rec, prev, mig_list<real>(c, MIG_RB), rb * rec, next));
+    const int N = axis == 0 ? g.nx : g.ny;
+    // a forward packet arrives from the previous rank (:2374-2378)
+    if (ra > 0) {
+      mig_receive_kernel<real><<<particle_blocks(ra), kThreads, 0, c->stream>>>(
+          mig_list<real>(c, MIG_RA), ra, axis, -N, mig_list<real>(c, S), cnt + S, c->mig_cap, c->err);
+      CKL();
+    }
+    if (rb > 0) {
+      mig_receive_kernel<real><<<particle_blocks(rb), kThreads, 0, c->stream>>>(
+          mig_list<real>(c, MIG_RB), rb, axis, N, mig_list<real>(c, S), cnt + S, c->mig_cap, c->err);
+      CKL();
+    }
+    in_list = S;
+  }
+  CK(cudaMemcpyAsync(h, cnt, sizeof(int) * kMig, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const int nfin = std::min(h[MIG_FIN], c->mig_cap);
+  Store& st = c->sp[s];
+  if (st.count + nfin > st.cap) return PIC_ERR_CAPACITY;
+  if (nfin > 0) {
+    mig_append_kernel<real><<<particle_blocks(nfin), kThreads, 0, c->stream>>>(
+        mig_list<real>(c, MIG_FIN), nfin, parts<real>(c, s), (int)st.count);
+    CKL();
+    // appended after the slots the layout and its tail cover: the slot-order
+    // push handles them until the next re-layout, so the layout stays valid
+    st.count += nfin;
+    set_int_kernel<<<1, 1, 0, c->stream>>>(st.count_dev, (int)st.count);
+    CKL();
+  }
+  CK(cudaMemsetAsync(cnt + MIG_OUT0 + s, 0, sizeof(int), c->stream));
+  return PIC_OK;
+}
+
+template <typename real>
+int do_migrate(pic_ctx* c) {
+  for (int s = 0; s < 2; ++s) CKR(do_migrate_species<real>(c, s));
+  return PIC_OK;
+}
+
 template <typename real>
 int wrap_planes(pic_ctx* c, const int* ids, int n) {
   PlaneSet<real> s{};
   Fields<real> F = fields<real>(c);
   for (int q = 0; q < n; ++q) s.p[q] = F.f[ids[q]];
   s.count = n;
+  if (c->has_xport) return halo_ghosts<real>(c, s, s, HALO_COPY);
   wrap_x_kernel<real><<<grid_blocks((long long)c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
   CKL();
   wrap_y_kernel<real><<<grid_blocks((long long)c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
@@ -259,6 +450,18 @@ int do_renew_b(pic_ctx* c) {
   const long long nint = (long long)c->g.nx * c->g.ny * c->g.nz;
   renew_b_kernel<real><<<grid_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, ramps(c), p);
   CKL();
+  if (c->has_xport) {
+    Fields<real> F = fields<real>(c);
+    PlaneSet<real> s{}, aux{};
+    for (int q = 0; q < 3; ++q) {
+      s.p[q] = F.f[F_BX + q];
+      aux.p[q] = F.f[F_DBX + q];
+      aux.p[3 + q] = F.f[F_B0X + q];
+    }
+    s.count = 3;
+    aux.count = 6;
+    return halo_ghosts<real>(c, s, aux, HALO_BTOTAL);
+  }
   wrap_b_x_kernel<real><<<grid_blocks((long long)c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(fields<real>(c), c->g);
   CKL();
   wrap_b_y_kernel<real><<<grid_blocks((long long)c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(fields<real>(c), c->g);
@@ -282,6 +485,7 @@ int do_fold(pic_ctx* c) {
   Fields<real> F = fields<real>(c);
   for (int q = 0; q < 8; ++q) s.p[q] = F.f[F_JIX + q];
   s.count = 8;
+  if (c->has_xport) return halo_fold<real>(c, s);
   fold_x_kernel<real><<<grid_blocks((long long)c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
   CKL();
   fold_y_kernel<real><<<grid_blocks((long long)c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
@@ -424,12 +628,14 @@ int do_drift_n(pic_ctx* c, int s) {
 
 template <typename real>
 int do_sr_particle(pic_ctx* c) {
+  if (c->has_xport) CKR(ensure_mig<real>(c));
   for (int s = 0; s < 2; ++s) {
     if (c->sp[s].count == 0) continue;
     sr_particle_kernel<real><<<particle_blocks(c->sp[s].count), kThreads, 0, c->stream>>>(
-        parts<real>(c, s), c->sp[s].count_dev, c->g, c->err);
+        parts<real>(c, s), c->sp[s].count_dev, c->g, push_const<real>(c, s).out, c->err);
     CKL();
   }
+  if (c->has_xport) CKR(do_migrate<real>(c));
   return PIC_OK;
 }
 
@@ -448,7 +654,7 @@ int scan_exclusive(pic_ctx* c, const int* in, int* out, long long n, int* tmp, s
 }
 
 SourceParams source_params(const pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form);
-void refill_slabs(const pic_ctx* c, Slab* slabs);
+int refill_slabs(const pic_ctx* c, Slab* slabs);
 
 // sorting (:7475-7590) into the tiled layout of tiled.cuh: count the
 // particles of every interior cell (stayers of the previous layout per lane
@@ -590,14 +796,22 @@ SourceParams source_params(const pic_ctx* c, int s, const Slab* slabs, int nslab
 }
 
 // add_ion_flat :6037-6220 at size 1: z slabs, y slabs, the low-x slab.
-void refill_slabs(const pic_ctx* c, Slab* slabs) {
+int refill_slabs(const pic_ctx* c, Slab* slabs) {
   const int Nx = c->cfg.nx, Ny = c->cfg.ny, Nz = c->cfg.nz;
-  const Slab s[5] = {
-      {2, Nx, 2, Ny, 2, 2, 0},          {2, Nx, 2, Ny, Nz, 2, 0},
-      {2, Nx, 2, 2, 4, Nz - 4, 0},      {2, Nx, Ny, 2, 4, Nz - 4, 0},
-      {2, 2, 4, Ny - 2, 4, Nz - 4, 0},
-  };
-  for (int q = 0; q < 5; ++q) slabs[q] = s[q];
+  const Geom& g = c->g;
+  int n = 0;
+  slabs[n++] = {2, Nx, 2, Ny, 2, 2, 0};                  // z = 2, 3 (:6035-6071)
+  slabs[n++] = {2, Nx, 2, Ny, Nz, 2, 0};                 // z = Nz, Nz+1 (:6072-6108)
+  if (g.ylo) slabs[n++] = {2, Nx, 2, 2, 4, Nz - 4, 0};   // y = 2, 3 on the low-y ranks (:6109-6145)
+  if (g.yhi) slabs[n++] = {2, Nx, Ny, 2, 4, Nz - 4, 0};  // y = Ny, Ny+1 on the high-y ranks (:6147-6183)
+  // one x slab, by the first branch of the chain at :6185-6401 that holds
+  if (g.xlo && g.ylo) slabs[n++] = {2, 2, 4, Ny - 2, 4, Nz - 4, 0};
+  else if (g.xlo && g.yhi) slabs[n++] = {2, 2, 2, Ny - 2, 4, Nz - 4, 0};
+  else if (g.xhi && g.ylo) slabs[n++] = {Nx, 2, 4, Ny - 2, 4, Nz - 4, 0};
+  else if (g.xhi && g.yhi) slabs[n++] = {Nx, 2, 2, Ny - 2, 4, Nz - 4, 0};
+  else if (g.xlo) slabs[n++] = {2, 2, 2, Ny, 4, Nz - 4, 0};
+  else if (g.xhi) slabs[n++] = {Nx, 2, 2, Ny, 4, Nz - 4, 0};
+  return n;
 }
 
 template <typename real>
@@ -618,7 +832,7 @@ int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0
 template <typename real>
 int do_add_flat(pic_ctx* c) {
   Slab slabs[5];
-  refill_slabs(c, slabs);
+  const int nslab = refill_slabs(c, slabs);
   for (int s = 0; s < 2; ++s) {
     Store& st = c->sp[s];
     if (st.count > 0) {
@@ -626,7 +840,7 @@ int do_add_flat(pic_ctx* c) {
           parts<real>(c, s), st.count_dev, c->g);
       CKL();
     }
-    CKR(do_source<real>(c, s, slabs, 5));  // appended; the next step's re-layout places them
+    CKR(do_source<real>(c, s, slabs, nslab));  // appended; the next step's re-layout places them
   }
   return PIC_OK;
 }
@@ -678,22 +892,26 @@ int do_thrust_sums(pic_ctx* c) {
   CK(cudaMemsetAsync(c->acc, 0, sizeof(double) * 33, c->stream));
   const pic_config& k = c->cfg;
   CellBox b{};
-  const int n3[3] = {k.nx, k.ny, k.nz};
+  const int n3[3] = {c->g.gnx, c->g.gny, k.nz};  // PROCESS_N Grid_N (:4971-4973)
   for (int a = 0; a < 3; ++a) {
     b.lo[a] = n3[a] * 0.2;
     b.hi[a] = n3[a] * 0.8;
   }
   b.e0 = k.e0;
   b.inv_mu0 = 1.0 / k.mu0;
+  b.ox = c->g.ox;
+  b.oy = c->g.oy;
   const long long nint = (long long)k.nx * k.ny * k.nz;
   field_energy_kernel<real><<<particle_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, b, c->acc);
   CKL();
   for (int s = 0; s < 2; ++s) {
     if (c->sp[s].count == 0) continue;
     ThrustParams tp{};
-    tp.xlo = (double)k.nx * k.dx * 0.2; tp.xhi = (double)k.nx * k.dx * 0.8;
-    tp.ylo = (double)k.ny * k.dx * 0.2; tp.yhi = (double)k.ny * k.dx * 0.8;
+    tp.xlo = (double)c->g.gnx * k.dx * 0.2; tp.xhi = (double)c->g.gnx * k.dx * 0.8;
+    tp.ylo = (double)c->g.gny * k.dx * 0.2; tp.yhi = (double)c->g.gny * k.dx * 0.8;
     tp.zlo = (double)k.nz * k.dx * 0.2; tp.zhi = (double)k.nz * k.dx * 0.8;
+    tp.ox = (double)c->g.ox * k.dx;
+    tp.oy = (double)c->g.oy * k.dx;
     tp.dx = k.dx;
     const double sg = s == 0 ? 1.0 : -1.0;
     const double w = k.q * species_weight(c) * k.dx * k.dx * k.dx;
@@ -706,6 +924,8 @@ int do_thrust_sums(pic_ctx* c) {
         parts<real>(c, s), c->sp[s].count_dev, fields<real>(c), c->g, tp, c->acc);
     CKL();
   }
+  // thrust_f's MPI_Allreduce of F and E over the ranks (:5103-5108)
+  if (c->has_xport && c->xport.allreduce_sum_f64(c->xport.user, c->acc, 33, (void*)c->stream) != 0) return PIC_ERR_COMM;
   return PIC_OK;
 }
 
@@ -759,7 +979,9 @@ int do_step(pic_ctx* c) {
     CKR(phase_mark(c, PH_SORT));
   }
   CKR(phase_mark(c, PH_PUSH));
+  if (c->has_xport) CKR(ensure_mig<real>(c));
   for (int s = 0; s < 2; ++s) CKR(do_push_tiled<real>(c, s));
+  if (c->has_xport) CKR(do_migrate<real>(c));  // sr_particle's exchange between ranks
   CKR(phase_mark(c, PH_PUSH));
   CKR(phase_mark(c, PH_FIELD));
   CKR(do_renew_b<real>(c));
@@ -1066,6 +1288,10 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
   if (k.precision != 32 && k.precision != 64) return PIC_ERR_ARG;
   if (k.add_interval < 1 || k.sort_interval < 1) return PIC_ERR_ARG;
   if (k.absorb_grid3 < 0 || (k.poisson_clean != 0 && k.poisson_clean != 1)) return PIC_ERR_ARG;
+  if (k.procs_x < 1 || k.procs_y < 1 || k.rank_x < 0 || k.rank_y < 0 || k.rank_x >= k.procs_x ||
+      k.rank_y >= k.procs_y)
+    return PIC_ERR_ARG;
+  if ((k.procs_x > 1 || k.procs_y > 1) && k.poisson_clean) return PIC_ERR_ARG;  // single domain only
   if (cudaSetDevice(k.device) != cudaSuccess) return PIC_ERR_CUDA;
   pic_ctx* c = new (std::nothrow) pic_ctx();
   if (!c) return PIC_ERR_ARG;
@@ -1077,6 +1303,14 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
   g.gx = k.nx + 4; g.gy = k.ny + 4; g.gz = k.nz + 4;
   g.sx = g.gy * g.gz;
   g.nodes = g.gx * g.gy * g.gz;
+  g.ox = k.rank_x * k.nx;
+  g.oy = k.rank_y * k.ny;
+  g.gnx = k.procs_x * k.nx;
+  g.gny = k.procs_y * k.ny;
+  g.xlo = k.rank_x == 0;
+  g.xhi = k.rank_x == k.procs_x - 1;
+  g.ylo = k.rank_y == 0;
+  g.yhi = k.rank_y == k.procs_y - 1;
   c->ncells = (long long)k.nx * k.ny * k.nz;
   auto fail = [&](int code) {
     pic_destroy(c);
@@ -1089,8 +1323,9 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
   // damping ramps of init_grid (:336-365) per axis on the doubled grid
   {
     std::vector<double> h(2 * (g.gx + g.gy + g.gz));
-    for (int i = 0; i < 2 * g.gx; ++i) h[i] = ramp_value(i, k.nx, k.absorb_grid);
-    for (int i = 0; i < 2 * g.gy; ++i) h[2 * g.gx + i] = ramp_value(i, k.ny, k.absorb_grid);
+    // k + 2 myrank_x Grid_Nx on the doubled grid of PROCESS_Nx Grid_Nx cells (:338-349)
+    for (int i = 0; i < 2 * g.gx; ++i) h[i] = ramp_value(i + 2 * g.ox, g.gnx, k.absorb_grid);
+    for (int i = 0; i < 2 * g.gy; ++i) h[2 * g.gx + i] = ramp_value(i + 2 * g.oy, g.gny, k.absorb_grid);
     for (int i = 0; i < 2 * g.gz; ++i) h[2 * (g.gx + g.gy) + i] = ramp_value(i, k.nz, k.absorb_grid);
     if (cudaMalloc(&c->ramps, sizeof(double) * h.size()) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMemcpy(c->ramps, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -1184,6 +1419,10 @@ int pic_destroy(pic_ctx* c) {
   cudaFree(c->phi_w);
   cudaFree(c->phi_sines);
   cudaFree(c->phi_sin2);
+  cudaFree(c->halo_buf[0]);
+  cudaFree(c->halo_buf[1]);
+  cudaFree(c->mig);
+  cudaFree(c->mig_cnt);
   cudaFree(c->err);
   cudaFree(c->stage);
   cudaFree(c->flags);
@@ -1285,9 +1524,19 @@ int pic_thrust_fave(pic_ctx* c, double* Fave27, int reset) {
   return PIC_OK;
 }
 
+int pic_set_transport(pic_ctx* c, const pic_transport* t) {
+  CKR(check_ctx(c));
+  if (!t || !t->sendrecv || !t->allreduce_sum_f64) return PIC_ERR_ARG;
+  if (c->cfg.poisson_clean) return PIC_ERR_STATE;
+  c->xport = *t;
+  c->has_xport = true;
+  return PIC_OK;
+}
+
 int pic_poisson_clean(pic_ctx* c) {
   CKR(check_ctx(c));
   if (!c->grid_ready) return PIC_ERR_STATE;
+  if (c->has_xport || c->cfg.procs_x * c->cfg.procs_y > 1) return PIC_ERR_STATE;  // single domain only
   return DISPATCH(c, do_poisson)(c);
 }
 
@@ -1295,6 +1544,7 @@ int pic_objective(pic_ctx* c, int nsteps, double* J) {
   CKR(check_ctx(c));
   if (!J || nsteps < 0) return PIC_ERR_ARG;
   if (c->cfg.poisson_clean) return PIC_ERR_ARG;  // the adjoint does not differentiate the cleaning
+  if (c->has_xport || c->cfg.procs_x * c->cfg.procs_y > 1) return PIC_ERR_ARG;  // single domain only
   if (!c->grid_ready) return PIC_ERR_STATE;
   double out[3] = {0, 0, 0};
   CKR(DISPATCH(c, do_adjoint)(c, nsteps, 1, false, out));
@@ -1306,6 +1556,7 @@ int pic_adjoint(pic_ctx* c, int nsteps, int checkpoint_every, double* out3) {
   CKR(check_ctx(c));
   if (!out3 || nsteps < 1 || checkpoint_every < 1) return PIC_ERR_ARG;
   if (c->cfg.poisson_clean) return PIC_ERR_ARG;
+  if (c->has_xport || c->cfg.procs_x * c->cfg.procs_y > 1) return PIC_ERR_ARG;
   if (!c->grid_ready) return PIC_ERR_STATE;
   double out[3] = {0, 0, 0};
   CKR(DISPATCH(c, do_adjoint)(c, nsteps, checkpoint_every, true, out));
@@ -1399,7 +1650,7 @@ int pic_status(pic_ctx* c, long long* counters8) {
   int any = 0;
   for (int q = 0; q < ERR_COUNT; ++q) {
     if (counters8) counters8[q] = (long long)h[q];
-    if (q < ERR_FIRST_INFO) any |= h[q] != 0;
+    if (q < ERR_FIRST_INFO || q == ERR_MIGRATION) any |= h[q] != 0;
   }
   return any ? PIC_ERR_DEVICE : PIC_OK;
 }

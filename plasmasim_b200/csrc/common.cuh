@@ -36,6 +36,12 @@ struct Geom {
   int gx, gy, gz;   // padded extents (n + 4)
   int sx;           // node stride of i (gy * gz)
   int nodes;        // gx * gy * gz
+  // the x-y decomposition (PROCESS_Nx x PROCESS_Ny, :100-101): this rank's
+  // first global cell (myrank_x Grid_Nx, myrank_y Grid_Ny), the global
+  // interior, and whether the rank holds the global low / high face of x, y
+  int ox, oy;
+  int gnx, gny;
+  int xlo, xhi, ylo, yhi;
 };
 
 // Field components stored as planes. B is the total field used by the gather,
@@ -61,6 +67,7 @@ struct Parts {
 enum ErrId {
   ERR_DEPOSIT_OOB = 0, ERR_CELL_RANGE = 1, ERR_NONFINITE = 2,
   ERR_FIRST_INFO = 3, CNT_PUSHED = 3,  // slots from here on count work, not errors
+  ERR_MIGRATION = 4,  // sr_particle packets lost to a full exchange buffer (an error)
   ERR_COUNT = 8
 };
 

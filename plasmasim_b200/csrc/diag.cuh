@@ -35,6 +35,7 @@ __device__ __forceinline__ void block_reduce_add(double (&v)[N], double* out, co
 
 struct ThrustParams {
   double xlo, xhi, ylo, yhi, zlo, zhi;  // open box (0.2 N dx, 0.8 N dx) per axis (:4986-4988)
+  double ox, oy;                        // myrank_x Grid_Nx dx, myrank_y Grid_Ny dx (:4984-4985)
   double dx;
   int idx[10];      // output slot per partial sum (F0..F2, F[o..o+5], E[oe])
   double scale[10];
@@ -59,7 +60,9 @@ __global__ void __launch_bounds__(256) thrust_particles_kernel(Parts<real> P, co
     const double x = ((double)i + (double)fx) * tp.dx;
     const double y = ((double)j + (double)fy) * tp.dx;
     const double z = ((double)k + (double)fz) * tp.dx;
-    if (!(x < tp.xhi && x > tp.xlo && y < tp.yhi && y > tp.ylo && z < tp.zhi && z > tp.zlo)) continue;
+    if (!(tp.ox + x < tp.xhi && tp.ox + x > tp.xlo && tp.oy + y < tp.yhi && tp.oy + y > tp.ylo && z < tp.zhi &&
+          z > tp.zlo))
+      continue;
     if (!stencil_ok(g, i, j, k)) continue;
     const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
     const Gathered<real> e = gather6(F, g, X, Y, Z);
@@ -76,6 +79,7 @@ __global__ void __launch_bounds__(256) thrust_particles_kernel(Parts<real> P, co
 
 struct CellBox {
   double lo[3], hi[3];   // open box on k-2, l-2, m-2 (:4965-4967)
+  int ox, oy;            // myrank_x Grid_Nx, myrank_y Grid_Ny (:4971-4972)
   double e0, inv_mu0;
 };
 
@@ -87,7 +91,8 @@ __global__ void __launch_bounds__(256) field_energy_kernel(Fields<real> F, Geom 
   const int nint = g.nx * g.ny * g.nz;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
     const int m = t % g.nz, l = (t / g.nz) % g.ny, k = t / (g.nz * g.ny);
-    if (!(k < b.hi[0] && k > b.lo[0] && l < b.hi[1] && l > b.lo[1] && m < b.hi[2] && m > b.lo[2])) continue;
+    const int kg = b.ox + k, lg = b.oy + l;
+    if (!(kg < b.hi[0] && kg > b.lo[0] && lg < b.hi[1] && lg > b.lo[1] && m < b.hi[2] && m > b.lo[2])) continue;
     const int n = (k + 2) * g.sx + (l + 2) * g.gz + (m + 2);
     const double ex = F.f[F_EX][n], ey = F.f[F_EY][n], ez = F.f[F_EZ][n];
     const double bx = F.f[F_BX][n], by = F.f[F_BY][n], bz = F.f[F_BZ][n];

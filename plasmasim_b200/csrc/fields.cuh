@@ -42,7 +42,8 @@ __global__ void init_fields_kernel(Fields<real> F, Geom g, DipoleParams d) {
   if (n >= g.nodes) return;
   const int k = n / g.sx, l = (n / g.gz) % g.gy, m = n % g.gz;
   const double Pi = 3.14159265358979323846;
-  const int cx = (g.nx + 4) / 2, cy = (g.ny + 4) / 2, cz = (g.nz + 4) / 2;
+  // k + myrank_x Grid_Nx - (PROCESS_Nx Grid_Nx + 4)/2 (:4588-4589)
+  const int cx = (g.gnx + 4) / 2 - g.ox, cy = (g.gny + 4) / 2 - g.oy, cz = (g.nz + 4) / 2;
   double x = (double)(k - cx) * d.dx, y = (double)(l - cy) * d.dx, z = (double)(m - cz) * d.dx;
   double r = sqrt(x * x + y * y + z * z);
   double b0x = d.imfx, b0y = d.imfy, b0z = d.imfz;

@@ -89,6 +89,25 @@ __device__ __forceinline__ Gathered<real> gather6(const Fields<real>& F, const G
   return r;
 }
 
+// sr_particle's packets between ranks: one record per particle, in the
+// sending rank's cell indices (the receiver shifts them, :2374-2380).
+template <typename real>
+struct MigRec {
+  int cell;
+  int pad;
+  real o[3];
+  real v[3];
+};
+
+// Where the push writes the particles that leave a rank's x-y interior in a
+// decomposed run; count is null for a single domain.
+template <typename real>
+struct Outbox {
+  int* count;
+  int cap;
+  MigRec<real>* rec;
+};
+
 template <typename real>
 struct PushConst {
   real T;               // 0.5 q dt / m, m < 0 for electrons (cal_track4 :2812)
@@ -97,9 +116,12 @@ struct PushConst {
   real qn;              // q n: current per unit velocity and unit weight
   real nw;              // n: density per unit weight
   real ex_add, ey_add;  // V*IMF_y, -V*IMF_x (:2817-2818)
-  int bal_lo;           // Absorb_grid2: ballistic below this cell index (:642-644)
-  int bal_hx, bal_hy, bal_hz;  // N + 4 - Absorb_grid2: ballistic above (:645-647)
+  // ballistic region of fdtd (:642-647) in this rank's cell indices:
+  // Absorb_grid2 - offset below, N_global + 4 - Absorb_grid2 - offset above
+  int bal_lx, bal_ly, bal_lz;
+  int bal_hx, bal_hy, bal_hz;
   int pjx, pjy, pjz, pn;       // deposit planes of this species
+  Outbox<real> out;            // decomposed runs: particles leaving the rank's x-y interior
 };
 
 // cal_track4 (:2804-2870) velocity update; returns the new velocity in v.
@@ -138,7 +160,7 @@ __device__ __forceinline__ void boris4(const PushConst<real>& pc, Gathered<real>
 template <typename real>
 __device__ __forceinline__ bool ballistic(const PushConst<real>& pc, int i, int j, int k, real fx,
                                           real fy, real fz) {
-  return i < pc.bal_lo || j < pc.bal_lo || k < pc.bal_lo ||
+  return i < pc.bal_lx || j < pc.bal_ly || k < pc.bal_lz ||
          i > pc.bal_hx || (i == pc.bal_hx && fx > (real)0) ||
          j > pc.bal_hy || (j == pc.bal_hy && fy > (real)0) ||
          k > pc.bal_hz || (k == pc.bal_hz && fz > (real)0);
@@ -199,6 +221,32 @@ __device__ __forceinline__ bool boundary(const Geom& g, int& i, int& j, int k) {
   return true;
 }
 
+// The slot's cell after sr_particle. A single domain applies `boundary`. A
+// decomposed run keeps particles inside the rank's x-y interior, deletes
+// those outside z (:2067-2104), and writes the rest to the outbox as packets
+// for the exchange between ranks, leaving the slot empty.
+template <typename real>
+__device__ __forceinline__ int settle(const Geom& g, const Outbox<real>& ob, int i, int j, int k, real fx, real fy,
+                                      real fz, real vx, real vy, real vz, unsigned long long* err) {
+  if (!ob.count) return boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
+  if (k < 2 || k >= g.nz + 2) return -1;
+  if (i >= 2 && i < g.nx + 2 && j >= 2 && j < g.ny + 2) return repack(i, j, k, err);
+  const int c = repack(i, j, k, err);
+  if (c < 0) return -1;
+  const int q = atomicAdd(ob.count, 1);
+  if (q < ob.cap) {
+    MigRec<real> r;
+    r.cell = c;
+    r.pad = 0;
+    r.o[0] = fx; r.o[1] = fy; r.o[2] = fz;
+    r.v[0] = vx; r.v[1] = vy; r.v[2] = vz;
+    ob.rec[q] = r;
+  } else {
+    count_err(err, ERR_MIGRATION);
+  }
+  return -1;
+}
+
 enum PushMode { PUSH_J = 0, PUSH_FUSED = 1 };
 
 // The particle part of one fdtd iteration for one species.
@@ -256,7 +304,7 @@ __global__ void __launch_bounds__(256) push_kernel(Parts<real> P, int first, con
           count_err(err, ERR_DEPOSIT_OOB);
         }
       }
-      cell = boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
+      cell = settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
     } else {
       cell = repack(i, j, k, err);
     }
@@ -300,7 +348,7 @@ __global__ void __launch_bounds__(256) drift_n_kernel(Parts<real> P, const int* 
 
 // sr_particle at size 1 on its own.
 template <typename real>
-__global__ void sr_particle_kernel(Parts<real> P, const int* __restrict__ count, Geom g,
+__global__ void sr_particle_kernel(Parts<real> P, const int* __restrict__ count, Geom g, Outbox<real> ob,
                                    unsigned long long* err) {
   const int n = *count;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
@@ -308,12 +356,13 @@ __global__ void sr_particle_kernel(Parts<real> P, const int* __restrict__ count,
     if (c < 0) continue;
     int i, j, k;
     unpack_cell(c, i, j, k);
-    P.cell[t] = boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
+    P.cell[t] = settle(g, ob, i, j, k, P.o[0][t], P.o[1][t], P.o[2][t], P.v[0][t], P.v[1][t], P.v[2][t], err);
   }
 }
 
-// Shell deletion of add_*_flat (:6015-6031) at size 1: x < 4dx or x > Nx dx,
-// the same in y and z.
+// Shell deletion of add_*_flat (:6015-6031): x < 4dx on the rank of the
+// global low x face, x > Nx dx on the rank of the high face, the same in y;
+// z < 4dx or z > Nz dx everywhere (at size 1 the one rank holds every face).
 template <typename real>
 __global__ void delete_shell_kernel(Parts<real> P, const int* __restrict__ count, Geom g) {
   const int n = *count;
@@ -322,11 +371,12 @@ __global__ void delete_shell_kernel(Parts<real> P, const int* __restrict__ count
     if (c < 0) continue;
     int i, j, k;
     unpack_cell(c, i, j, k);
-    bool del = i < 4 || j < 4 || k < 4 || i > g.nx || j > g.ny || k > g.nz;
-    if (!del && (i == g.nx || j == g.ny || k == g.nz)) {
-      del = (i == g.nx && P.o[0][t] > (real)0) || (j == g.ny && P.o[1][t] > (real)0) ||
-            (k == g.nz && P.o[2][t] > (real)0);
-    }
+    // the x and y shells only on the ranks that hold that face of the global domain
+    const bool xl = g.xlo && i < 4, yl = g.ylo && j < 4;
+    const bool xh = g.xhi && (i > g.nx || (i == g.nx && P.o[0][t] > (real)0));
+    const bool yh = g.yhi && (j > g.ny || (j == g.ny && P.o[1][t] > (real)0));
+    const bool zs = k < 4 || k > g.nz || (k == g.nz && P.o[2][t] > (real)0);
+    const bool del = xl || yl || xh || yh || zs;
     if (del) P.cell[t] = -1;
   }
 }

@@ -260,7 +260,7 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
           count_err(err, ERR_DEPOSIT_OOB);
         }
       }
-      P.cell[t] = boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
+      P.cell[t] = settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
       P.o[0][t] = fx; P.o[1][t] = fy; P.o[2][t] = fz;
       P.v[0][t] = vx; P.v[1][t] = vy; P.v[2][t] = vz;
     }

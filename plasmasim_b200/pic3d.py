@@ -50,7 +50,8 @@ class _CConfig(C.Structure):
         ("add_interval", C.c_int), ("sort_interval", C.c_int),
         ("diag_every_step", C.c_int), ("poisson_clean", C.c_int),
         ("capacity", C.c_longlong), ("seed_p", C.c_ulonglong), ("seed_v", C.c_ulonglong),
-        ("absorb_grid3", C.c_int), ("reserved1", C.c_int),
+        ("absorb_grid3", C.c_int), ("procs_x", C.c_int), ("procs_y", C.c_int),
+        ("rank_x", C.c_int), ("rank_y", C.c_int), ("reserved1", C.c_int),
     ]
 
 
@@ -94,6 +95,10 @@ class PicConfig:
     seed_p: int = 0
     seed_v: int = 50
     absorb_grid3: int = 40
+    procs_x: int = 1
+    procs_y: int = 1
+    rank_x: int = 0
+    rank_y: int = 0
 
     @classmethod
     def normalized(cls, nx, ny, nz, np_, **kw) -> "PicConfig":
@@ -116,6 +121,12 @@ class PicConfig:
         return c
 
 
+class _CTransport(C.Structure):
+    """pic_transport: the exchange callbacks of a decomposed run (C function
+    pointers, held opaque here)."""
+    _fields_ = [("user", C.c_void_p), ("sendrecv", C.c_void_p), ("allreduce_sum_f64", C.c_void_p)]
+
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 _llp = C.POINTER(C.c_longlong)
@@ -130,6 +141,8 @@ EXPORTED = [
     "pic_error_string", "pic_set_timing", "pic_read_timing", "pic_gauss_residual_noalloc",
     "pic_objective", "pic_adjoint", "pic_save_checkpoint", "pic_load_checkpoint", "pic_write_output",
     "pic_append_thrust", "pic_append_thrust_ave", "pic_poisson_clean",
+    "pic_set_transport", "pic_group_create", "pic_group_destroy", "pic_group_transport",
+    "pic_nccl_unique_id", "pic_nccl_transport_create", "pic_nccl_transport_destroy",
     "pic2d_config_normalized", "pic2d_create", "pic2d_destroy", "pic2d_init", "pic2d_step",
     "pic2d_thrust", "pic2d_particle_count", "pic2d_get_particles", "pic2d_get_grid",
     "pic2d_autotune", "pic2d_set_graph", "pic2d_status", "pic2d_get_stream",
@@ -163,6 +176,13 @@ def load_library(path: str = LIB_PATH):
     L.pic_thrust_fave.argtypes = [vp, _dp, C.c_int]
     L.pic_gauss_residual.argtypes = [vp, _dp]
     L.pic_poisson_clean.argtypes = [vp]
+    L.pic_set_transport.argtypes = [vp, C.POINTER(_CTransport)]
+    L.pic_group_create.argtypes = [C.c_int, C.POINTER(vp)]
+    L.pic_group_destroy.argtypes = [vp]
+    L.pic_group_transport.argtypes = [vp, C.c_int, C.POINTER(_CTransport)]
+    L.pic_nccl_unique_id.argtypes = [C.c_char_p]
+    L.pic_nccl_transport_create.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(_CTransport)]
+    L.pic_nccl_transport_destroy.argtypes = [C.POINTER(_CTransport)]
     L.pic_objective.argtypes = [vp, C.c_int, _dp]
     for name in ["pic_save_checkpoint", "pic_load_checkpoint"]:
         getattr(L, name).argtypes = [vp, C.c_char_p, C.c_int, C.c_int]
@@ -274,6 +294,12 @@ class Pic3D:
         F = np.zeros(27)
         self._call("pic_thrust_fave", _ptr(F), 1 if reset else 0)
         return F
+
+    def set_transport(self, transport: "_CTransport"):
+        """Exchanges of a decomposed run go through `transport` (which must
+        outlive this context's use of it)."""
+        self._transport = transport
+        self._call("pic_set_transport", C.byref(transport))
 
     def poisson_clean(self):
         """renew_phi3 + sr_phi + sr_e: the Poisson correction of E."""
