@@ -379,6 +379,20 @@ def run_adjoint(nsteps: int = 200, every: int = 20):
             "fd_checks": checks}
 
 
+def combine_over_ranks(ms: float, pushed: float, dist=None, device: str = "cuda"):
+    """Whole-job numbers of the replicas: the slowest rank's time and the
+    particle pushes of all ranks (max and sum over the process group)."""
+    if dist is None:
+        return ms, float(pushed)
+    import torch
+
+    tmax = torch.tensor([ms], dtype=torch.float64, device=device)
+    tsum = torch.tensor([float(pushed)], dtype=torch.float64, device=device)
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return float(tmax[0]), float(tsum[0])
+
+
 def run_poisson(reps: int = 10):
     """Poisson cleaning (pic_poisson_clean: renew_phi3 + sr_phi + sr_e) on the
     bench grid, FP32, timed with CUDA events on the context's stream. FLOPs:
@@ -485,14 +499,7 @@ def main():
     P, out = run_gpu(32, args.steps, args.warmup, seed, dist, clocks_index=local)
     ms = out["ms"]
     pushed = out["pushed"]
-    if dist is not None:
-        t = torch.tensor([ms, float(pushed)], dtype=torch.float64, device="cuda")
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        ms_max, pushed_all = float(tmax[0]), float(t[1])
-    else:
-        ms_max, pushed_all = ms, float(pushed)
+    ms_max, pushed_all = combine_over_ranks(ms, pushed, dist)
     value = pushed_all / (ms_max / 1e3)
     cells = (NX + 4) * (NY + 4) * (NZ + 4)
     nsp = pushed / max(args.steps, 1) / 2

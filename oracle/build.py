@@ -79,6 +79,8 @@ REF_CONFIGS = {
     # (oracle/shim/mpi_shim.c runs the ranks as processes; oracle/multirank.py
     # drives them); absorbing layers 2 and 3 cells wide on the global domain
     "tiny_2x1": {**NORMALIZED, **_geom(8, 8, 8, 4, pnx=2, pny=1)},
+    # one rank over the 2 x 1 job's global grid (16 x 8 x 8)
+    "wide16": {**NORMALIZED, **_geom(16, 8, 8, 4)},
     "tiny_2x2": {**NORMALIZED, **_geom(8, 8, 8, 4, pnx=2, pny=2)},
     "damped_2x2": {**NORMALIZED, **_geom(8, 8, 10, 2, absorb=2, absorb2=3, pnx=2, pny=2), "ORACLE_SIGMA_A": 0.05},
 }

@@ -66,15 +66,21 @@ class NcclTransport:
     """pic_nccl_transport_create for this process's rank; rank 0 creates the
     NCCL unique id and publishes it in `store` (a torch.distributed Store)."""
 
-    def __init__(self, store, nranks: int, rank: int, device: int, key: str = "plasma_b200_nccl_id"):
-        self.L = load_library()
+    @staticmethod
+    def share_unique_id(store, rank: int, key: str = "plasma_b200_nccl_id") -> bytes:
+        """Rank 0 makes the NCCL unique id and sets it in the store; every
+        rank returns it from the store."""
         if rank == 0:
             buf = C.create_string_buffer(128)
-            rc = self.L.pic_nccl_unique_id(buf)
+            rc = load_library().pic_nccl_unique_id(buf)
             if rc:
                 raise PicError(rc, "pic_nccl_unique_id")
             store.set(key, bytes(buf.raw))
-        uid = store.get(key)
+        return bytes(store.get(key))
+
+    def __init__(self, store, nranks: int, rank: int, device: int, key: str = "plasma_b200_nccl_id"):
+        self.L = load_library()
+        uid = self.share_unique_id(store, rank, key)
         self.t = _CTransport()
         rc = self.L.pic_nccl_transport_create(uid, nranks, rank, device, C.byref(self.t))
         if rc:
