@@ -41,6 +41,7 @@ template <typename real>
 __global__ void classify_kernel(Parts<real> P, Geom g, TileGeom t, const int* __restrict__ goff,
                                 const int* __restrict__ gmax, int cap, int* holes, int* nholes,
                                 int* append_at) {
+  constexpr int U = 4;  // rows whose loads are in flight together
   const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (G >= t.ngroups) return;  // warp-uniform
@@ -49,33 +50,61 @@ __global__ void classify_kernel(Parts<real> P, Geom g, TileGeom t, const int* __
   const int base = goff[G], m = gmax[G];
   int nh = 0;
   int blk = 0, used = kAppendBlock;  // current block of append slots (warp-uniform)
-  for (int r = 0; r < m; ++r) {
-    const int s = base + r * kLanes + lane;
-    const int c = P.cell[s];
-    const int key = interior_key(g, c);
-    const bool leaves = c >= 0 && key != home;
-    const bool mover = leaves && key >= 0;
-    const unsigned mm = __ballot_sync(0xffffffffu, mover);
-    const int nm = __popc(mm);
-    if (nm > kAppendBlock - used) {  // close the block, take a new one
-      for (int q = used + lane; q < kAppendBlock; q += kLanes)
-        if (blk + q < cap) P.cell[blk + q] = -1;
-      int nb = 0;
-      if (lane == 0) nb = atomicAdd(append_at, kAppendBlock);
-      blk = __shfl_sync(0xffffffffu, nb, 0);
-      used = 0;
+  for (int r0 = 0; r0 < m; r0 += U) {
+    int c[U], d[U];
+    bool moved[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) c[u] = r0 + u < m ? P.cell[base + (r0 + u) * kLanes + lane] : -1;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int r = r0 + u;
+      const int key = interior_key(g, c[u]);
+      const bool leaves = c[u] >= 0 && key != home;
+      const bool mover = leaves && key >= 0;
+      const unsigned mm = __ballot_sync(0xffffffffu, mover);
+      const int nm = __popc(mm);
+      if (nm > kAppendBlock - used) {  // close the block, take a new one
+        for (int q = used + lane; q < kAppendBlock; q += kLanes)
+          if (blk + q < cap) P.cell[blk + q] = -1;
+        int nb = 0;
+        if (lane == 0) nb = atomicAdd(append_at, kAppendBlock);
+        blk = __shfl_sync(0xffffffffu, nb, 0);
+        used = 0;
+      }
+      d[u] = blk + used + __popc(mm & below);
+      used += nm;
+      // a mover that finds the append region full stays where it is
+      moved[u] = mover && d[u] < cap;
+      const bool hole = c[u] < 0 || (leaves && (moved[u] || !mover));
+      if (hole && c[u] >= 0 && !moved[u]) P.cell[base + r * kLanes + lane] = -1;
+      if (hole && r < m) {
+        holes[base + nh * kLanes + lane] = r;
+        ++nh;
+      }
     }
-    const int d = blk + used + __popc(mm & below);
-    used += nm;
-    // a mover that finds the append region full stays where it is
-    const bool moved = mover && d < cap;
-    if (moved) copy_slot(P, s, P, d, c);
-    const bool hole = c < 0 || (leaves && (moved || !mover));
-    if (hole && c >= 0) P.cell[s] = -1;
-    if (hole) {
-      holes[base + nh * kLanes + lane] = r;
-      ++nh;
-    }
+    // the movers of the U rows: their loads issued together, then the copies
+    real o[U][3], v[U][3];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (moved[u]) {
+        const int s = base + (r0 + u) * kLanes + lane;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          o[u][a] = P.o[a][s];
+          v[u][a] = P.v[a][s];
+        }
+      }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (moved[u]) {
+        P.cell[d[u]] = c[u];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          P.o[a][d[u]] = o[u][a];
+          P.v[a][d[u]] = v[u][a];
+        }
+        P.cell[base + (r0 + u) * kLanes + lane] = -1;
+      }
   }
   for (int q = used + lane; q < kAppendBlock; q += kLanes)
     if (blk + q < cap && used < kAppendBlock) P.cell[blk + q] = -1;
@@ -87,41 +116,92 @@ __global__ void clamp_count_kernel(const int* append_at, int cap, int* count_dev
 }
 
 // Each appended particle takes the next hole of its cell's column; the rest
-// go, compacted, to the spare buffer Q.
+// go, compacted, to the spare buffer Q. A warp takes U rows of 32 appended
+// slots at a time and issues their loads, cursor atomics and hole lookups
+// together, so that the chain of dependent memory accesses of one particle
+// overlaps those of the others.
 template <typename real>
 __global__ void place_kernel(Parts<real> P, int first, const int* __restrict__ count, Geom g, TileGeom t,
                              const int* __restrict__ goff, const int* __restrict__ holes,
                              const int* __restrict__ nholes, int* cursor, Parts<real> Q, int* nspill) {
+  constexpr int U = 4;
   const int n = *count;
-  const int stride = gridDim.x * blockDim.x;
   const int span = n - first;
-  const int span_round = (span + 31) & ~31;
   const int lane = threadIdx.x & 31;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < span_round; q += stride) {
-    const int s = first + q;
-    int c = -1, key = -1;
-    if (q < span) {
-      c = P.cell[s];
-      key = interior_key(g, c);
+  const unsigned below = (1u << lane) - 1u;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int w0 = warp * (U * kLanes); w0 < span; w0 += nwarps * (U * kLanes)) {  // warp-uniform
+    int s[U], c[U], key[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int q = w0 + u * kLanes + lane;
+      s[u] = first + q;
+      c[u] = q < span ? P.cell[s[u]] : -1;
     }
-    const int rank = warp_aggregated_inc(cursor, key < 0 ? 0 : key, key >= 0);
-    const bool spill = key >= 0 && rank >= nholes[key];
-    const unsigned ms = __ballot_sync(0xffffffffu, spill);
-    int sb = 0;
-    if (lane == 0 && ms) sb = atomicAdd(nspill, __popc(ms));
-    sb = __shfl_sync(0xffffffffu, sb, 0);
-    if (q >= span) continue;
-    if (key < 0) {
-      P.cell[s] = -1;  // empty slot, or outside the interior: dropped
-    } else if (spill) {
-      copy_slot(P, s, Q, sb + __popc(ms & ((1u << lane) - 1u)), c);
-      P.cell[s] = -1;
-    } else {
-      int l2;
-      const int G = group_of_key(g, t, key, l2);
-      const int d = goff[G] + holes[goff[G] + rank * kLanes + l2] * kLanes + l2;
-      copy_slot(P, s, P, d, c);
-      P.cell[s] = -1;
+    real o[U][3], v[U][3];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      key[u] = interior_key(g, c[u]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        o[u][a] = key[u] >= 0 ? P.o[a][s[u]] : (real)0;
+        v[u][a] = key[u] >= 0 ? P.v[a][s[u]] : (real)0;
+      }
+    }
+    // per slot: holes of the destination cell and its column's first slot
+    int nh[U], gb[U], l2[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      nh[u] = 0;
+      gb[u] = 0;
+      l2[u] = 0;
+      if (key[u] >= 0) {
+        nh[u] = nholes[key[u]];
+        gb[u] = goff[group_of_key(g, t, key[u], l2[u])];
+      }
+    }
+    // warp-aggregated cursor increments: one atomic per distinct key and row
+    unsigned peers[U];
+    int old[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      peers[u] = __match_any_sync(0xffffffffu, key[u] >= 0 ? key[u] : -1 - lane);
+      old[u] = 0;
+      if (key[u] >= 0 && lane == __ffs(peers[u]) - 1) old[u] = atomicAdd(cursor + key[u], __popc(peers[u]));
+    }
+    int rank[U], sb[U];
+    unsigned ms[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      rank[u] = __shfl_sync(0xffffffffu, old[u], __ffs(peers[u]) - 1) + __popc(peers[u] & below);
+      const bool spill = key[u] >= 0 && rank[u] >= nh[u];
+      ms[u] = __ballot_sync(0xffffffffu, spill);
+      sb[u] = 0;
+      if (lane == 0 && ms[u]) sb[u] = atomicAdd(nspill, __popc(ms[u]));
+    }
+    int hrow[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      sb[u] = __shfl_sync(0xffffffffu, sb[u], 0);
+      const bool spill = (ms[u] >> lane) & 1u;
+      hrow[u] = (key[u] >= 0 && !spill) ? holes[gb[u] + rank[u] * kLanes + l2[u]] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (w0 + u * kLanes + lane >= span) continue;
+      if (key[u] >= 0) {
+        const bool spill = (ms[u] >> lane) & 1u;
+        const Parts<real>& D = spill ? Q : P;
+        const int d = spill ? sb[u] + __popc(ms[u] & below) : gb[u] + hrow[u] * kLanes + l2[u];
+        D.cell[d] = c[u];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          D.o[a][d] = o[u][a];
+          D.v[a][d] = v[u][a];
+        }
+      }
+      P.cell[s[u]] = -1;  // empty slot, outside the interior (dropped), or moved
     }
   }
 }
