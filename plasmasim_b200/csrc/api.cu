@@ -1063,12 +1063,30 @@ int do_export(pic_ctx* c, int s, double* rows, long long cap, long long* n_out) 
 }
 
 template <typename real>
-int do_import(pic_ctx* c, int s, const double* rows, long long n) {
+int do_import(pic_ctx* c, int s, const double* rows, const int* flag, long long n) {
   Store& st = c->sp[s];
   if (n > st.cap) return PIC_ERR_CAPACITY;
   if (n > 0) {
     CKR(ensure_stage(c, sizeof(double) * 7 * (size_t)n));
     CK(cudaMemcpyAsync(c->stage, rows, sizeof(double) * 7 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    // every row carries the species' weight and flag 1: checked on the device
+    // before the store changes (a host loop over the rows would read them all
+    // a second time through the host's memory)
+    const int* fdev = nullptr;
+    if (flag) {
+      CKR(ensure_flags(c, (size_t)n));
+      CK(cudaMemcpyAsync(c->flags, flag, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+      fdev = c->flags;
+    }
+    const double w = species_weight(c);
+    CK(cudaMemsetAsync(c->maxbits, 0, sizeof(unsigned long long), c->stream));
+    import_check_kernel<<<particle_blocks(n), kThreads, 0, c->stream>>>((const double*)c->stage, n, w,
+                                                                        1e-12 * std::fabs(w), fdev, c->maxbits);
+    CKL();
+    unsigned long long bad = 0;
+    CK(cudaMemcpyAsync(&bad, c->maxbits, sizeof(bad), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (bad) return PIC_ERR_ARG;
     import_rows_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n,
                                                                          (const double*)c->stage, c->cfg.dx, c->err);
     CKL();
@@ -1590,12 +1608,7 @@ int pic_fdtd(pic_ctx* c, int nsteps) {
 int pic_set_particles(pic_ctx* c, int species, const double* rows, const int* flag, long long n) {
   CKR(check_ctx(c));
   if (species < 0 || species > 1 || n < 0 || (n > 0 && !rows)) return PIC_ERR_ARG;
-  const double w = species_weight(c);
-  for (long long i = 0; i < n; ++i) {
-    if (std::fabs(rows[7 * i + 6] - w) > 1e-12 * std::fabs(w)) return PIC_ERR_ARG;
-    if (flag && flag[i] != 1) return PIC_ERR_ARG;
-  }
-  CKR(DISPATCH(c, do_import)(c, species, rows, n));
+  CKR(DISPATCH(c, do_import)(c, species, rows, flag, n));
   c->particles_ready = true;
   return PIC_OK;
 }

@@ -594,6 +594,19 @@ __global__ void export_rows_kernel(Parts<real> P, int n, const int* __restrict__
   r[6] = weight;
 }
 
+// Rows that pic_set_particles refuses: a weight other than the species' n
+// (:83-84) or a flag other than 1 (the only value the reference assigns,
+// :510); counted, so that the caller can reject the import before it
+// changes the store.
+static __global__ void import_check_kernel(const double* __restrict__ rows, long long n, double w, double tol,
+                                           const int* __restrict__ flag, unsigned long long* bad) {
+  unsigned long long nb = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    nb += (fabs(rows[7 * i + 6] - w) > tol || (flag && flag[i] != 1)) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) nb += __shfl_down_sync(0xffffffffu, nb, o);
+  if ((threadIdx.x & 31) == 0 && nb) atomicAdd(bad, nb);
+}
+
 template <typename real>
 __global__ void import_rows_kernel(Parts<real> P, int n, const double* __restrict__ rows,
                                    double dx, unsigned long long* err) {
