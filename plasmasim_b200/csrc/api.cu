@@ -1002,25 +1002,31 @@ int do_step(pic_ctx* c) {
 }
 
 // --------------------------------------------------------- import/export
+// The staging buffer grows with an eighth of headroom, so that a particle
+// count that grows by a refill between two exports does not reallocate it.
 int ensure_stage(pic_ctx* c, size_t bytes) {
   if (bytes <= c->stage_bytes) return PIC_OK;
   if (c->stage) CK(cudaFree(c->stage));
   c->stage = nullptr;
   c->stage_bytes = 0;
-  CK(cudaMalloc(&c->stage, bytes));
-  c->stage_bytes = bytes;
+  const size_t want = bytes + bytes / 8;
+  CK(cudaMalloc(&c->stage, want));
+  c->stage_bytes = want;
   return PIC_OK;
 }
 
+// Flags and positions of the export's compaction: sized once for the larger
+// particle store, since the count changes every refill.
 int ensure_flags(pic_ctx* c, size_t n) {
   if (n <= c->flags_len) return PIC_OK;
   if (c->flags) CK(cudaFree(c->flags));
   if (c->pos) CK(cudaFree(c->pos));
   c->flags = c->pos = nullptr;
   c->flags_len = 0;
-  CK(cudaMalloc(&c->flags, sizeof(int) * n));
-  CK(cudaMalloc(&c->pos, sizeof(int) * n));
-  c->flags_len = n;
+  const size_t want = std::max<size_t>(n, (size_t)std::max(c->sp[0].cap, c->sp[1].cap));
+  CK(cudaMalloc(&c->flags, sizeof(int) * want));
+  CK(cudaMalloc(&c->pos, sizeof(int) * want));
+  c->flags_len = want;
   return PIC_OK;
 }
 
