@@ -27,15 +27,19 @@ struct PushSmem {
 };
 
 // Trilinear interpolation from a window plane with compile-time strides (the
-// 2x2x2 nodes at window index n).
+// 2x2x2 nodes at window index n). The two x planes travel as one packed pair
+// through the z and y steps, two-wide multiplies and FMAs of sm_100 (one
+// instruction for both planes); Z0 = (z0, z0) and so on.
 template <int WY, int WZ>
-__device__ __forceinline__ float trilerp_win(const float* __restrict__ w, int n, float x0, float x1, float y0,
-                                             float y1, float z0, float z1) {
-  const float c00 = w[n] * z0 + w[n + 1] * z1;
-  const float c01 = w[n + WZ] * z0 + w[n + WZ + 1] * z1;
-  const float c10 = w[n + WY * WZ] * z0 + w[n + WY * WZ + 1] * z1;
-  const float c11 = w[n + WY * WZ + WZ] * z0 + w[n + WY * WZ + WZ + 1] * z1;
-  return (c00 * y0 + c01 * y1) * x0 + (c10 * y0 + c11 * y1) * x1;
+__device__ __forceinline__ float trilerp_win(const float* __restrict__ w, int n, float x0, float x1, float2 Y0,
+                                             float2 Y1, float2 Z0, float2 Z1) {
+  constexpr int P = WY * WZ;  // next x plane
+  const float2 n00 = make_float2(w[n], w[n + P]), n01 = make_float2(w[n + 1], w[n + P + 1]);
+  const float2 n10 = make_float2(w[n + WZ], w[n + P + WZ]), n11 = make_float2(w[n + WZ + 1], w[n + P + WZ + 1]);
+  const float2 cy0 = __ffma2_rn(n01, Z1, __fmul2_rn(n00, Z0));  // (c00, c10)
+  const float2 cy1 = __ffma2_rn(n11, Z1, __fmul2_rn(n10, Z0));  // (c01, c11)
+  const float2 cx = __ffma2_rn(cy1, Y1, __fmul2_rn(cy0, Y0));   // the two x planes
+  return cx.x * x0 + cx.y * x1;
 }
 
 // gather6 from the tile's field window (planes ex ey ez bx by bz of WN nodes,
@@ -45,13 +49,17 @@ __device__ __forceinline__ Gathered<float> gather6_win(const float* __restrict__
                                                        const Axis<float>& X, const Axis<float>& Y,
                                                        const Axis<float>& Z) {
   const int ax = X.a - wx0, bx = X.b - wx0, ay = Y.a - wy0, by = Y.b - wy0, az = Z.a - wz0, bz = Z.b - wz0;
+  const float2 ya0 = make_float2(Y.a0, Y.a0), ya1 = make_float2(Y.a1, Y.a1);
+  const float2 yb0 = make_float2(Y.b0, Y.b0), yb1 = make_float2(Y.b1, Y.b1);
+  const float2 za0 = make_float2(Z.a0, Z.a0), za1 = make_float2(Z.a1, Z.a1);
+  const float2 zb0 = make_float2(Z.b0, Z.b0), zb1 = make_float2(Z.b1, Z.b1);
   Gathered<float> r;
-  r.ex = trilerp_win<WY, WZ>(fw, (ax * WY + by) * WZ + bz, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
-  r.ey = trilerp_win<WY, WZ>(fw + WN, (bx * WY + ay) * WZ + bz, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
-  r.ez = trilerp_win<WY, WZ>(fw + 2 * WN, (bx * WY + by) * WZ + az, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
-  r.bx = trilerp_win<WY, WZ>(fw + 3 * WN, (bx * WY + ay) * WZ + az, X.b0, X.b1, Y.a0, Y.a1, Z.a0, Z.a1);
-  r.by = trilerp_win<WY, WZ>(fw + 4 * WN, (ax * WY + by) * WZ + az, X.a0, X.a1, Y.b0, Y.b1, Z.a0, Z.a1);
-  r.bz = trilerp_win<WY, WZ>(fw + 5 * WN, (ax * WY + ay) * WZ + bz, X.a0, X.a1, Y.a0, Y.a1, Z.b0, Z.b1);
+  r.ex = trilerp_win<WY, WZ>(fw, (ax * WY + by) * WZ + bz, X.a0, X.a1, yb0, yb1, zb0, zb1);
+  r.ey = trilerp_win<WY, WZ>(fw + WN, (bx * WY + ay) * WZ + bz, X.b0, X.b1, ya0, ya1, zb0, zb1);
+  r.ez = trilerp_win<WY, WZ>(fw + 2 * WN, (bx * WY + by) * WZ + az, X.b0, X.b1, yb0, yb1, za0, za1);
+  r.bx = trilerp_win<WY, WZ>(fw + 3 * WN, (bx * WY + ay) * WZ + az, X.b0, X.b1, ya0, ya1, za0, za1);
+  r.by = trilerp_win<WY, WZ>(fw + 4 * WN, (ax * WY + by) * WZ + az, X.a0, X.a1, yb0, yb1, za0, za1);
+  r.bz = trilerp_win<WY, WZ>(fw + 5 * WN, (ax * WY + ay) * WZ + bz, X.a0, X.a1, ya0, ya1, zb0, zb1);
   return r;
 }
 
