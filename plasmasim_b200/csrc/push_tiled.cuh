@@ -63,6 +63,101 @@ __device__ __forceinline__ Gathered<float> gather6_win(const float* __restrict__
   return r;
 }
 
+// The current of the particles that are in a lane's home cell, summed in
+// registers over the 2x3x3 / 3x2x3 / 3x3x2 nodes such a particle can touch:
+// x(a, b, c) is the jx sum at node (h-1+a+1, h-1+b, h-1+c) of the window flush
+// below, and so on for y and z.
+template <typename real>
+struct HomeJ {
+  real jx[2][3][3], jy[3][2][3], jz[3][3][2];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (a < 2) jx[a][b][c] = (real)0;
+          if (b < 2) jy[a][b][c] = (real)0;
+          if (c < 2) jz[a][b][c] = (real)0;
+        }
+  }
+  __device__ __forceinline__ void add(real qx, real qy, real qz, const Axis<real>& X, const Axis<real>& Y,
+                                      const Axis<real>& Z, const W3<real>& bx, const W3<real>& by,
+                                      const W3<real>& bz) {
+    const real ax[2] = {X.a0, X.a1}, ay[2] = {Y.a0, Y.a1}, az[2] = {Z.a0, Z.a1};
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const real yz = by.w[b] * bz.w[c];
+        jx[0][b][c] += (qx * ax[0]) * yz;
+        jx[1][b][c] += (qx * ax[1]) * yz;
+      }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const real xz = bx.w[a] * bz.w[c];
+        jy[a][0][c] += (qy * ay[0]) * xz;
+        jy[a][1][c] += (qy * ay[1]) * xz;
+      }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const real xy = bx.w[a] * by.w[b];
+        jz[a][b][0] += (qz * az[0]) * xy;
+        jz[a][b][1] += (qz * az[1]) * xy;
+      }
+  }
+  __device__ __forceinline__ real x(int a, int b, int c) const { return jx[a][b][c]; }
+  __device__ __forceinline__ real y(int a, int b, int c) const { return jy[a][b][c]; }
+  __device__ __forceinline__ real z(int a, int b, int c) const { return jz[a][b][c]; }
+};
+
+// FP32: the two nodes of each component's unshifted axis as one packed pair,
+// updated with the two-wide multiplies and FMAs of sm_100.
+template <>
+struct HomeJ<float> {
+  float2 jx[3][3], jy[3][3], jz[3][3];  // jx[b][c] = (a = 0, a = 1); jy[a][c] = (b = 0, 1); jz[a][b] = (c = 0, 1)
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) jx[a][b] = jy[a][b] = jz[a][b] = make_float2(0.f, 0.f);
+  }
+  __device__ __forceinline__ void add(float qx, float qy, float qz, const Axis<float>& X, const Axis<float>& Y,
+                                      const Axis<float>& Z, const W3<float>& bx, const W3<float>& by,
+                                      const W3<float>& bz) {
+    const float2 qxa = make_float2(qx * X.a0, qx * X.a1);
+    const float2 qya = make_float2(qy * Y.a0, qy * Y.a1);
+    const float2 qza = make_float2(qz * Z.a0, qz * Z.a1);
+    float2 dx[3], dy[3], dz[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      dx[q] = make_float2(bx.w[q], bx.w[q]);
+      dy[q] = make_float2(by.w[q], by.w[q]);
+      dz[q] = make_float2(bz.w[q], bz.w[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const float2 tx = __fmul2_rn(qxa, dy[q]);  // jx: b = q
+      const float2 ty = __fmul2_rn(qya, dx[q]);  // jy: a = q
+      const float2 tz = __fmul2_rn(qza, dx[q]);  // jz: a = q
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        jx[q][r] = __ffma2_rn(tx, dz[r], jx[q][r]);  // c = r
+        jy[q][r] = __ffma2_rn(ty, dz[r], jy[q][r]);  // c = r
+        jz[q][r] = __ffma2_rn(tz, dy[r], jz[q][r]);  // b = r
+      }
+    }
+  }
+  __device__ __forceinline__ float x(int a, int b, int c) const { return a ? jx[b][c].y : jx[b][c].x; }
+  __device__ __forceinline__ float y(int a, int b, int c) const { return b ? jy[a][c].y : jy[a][c].x; }
+  __device__ __forceinline__ float z(int a, int b, int c) const { return c ? jz[a][b].y : jz[a][b].x; }
+};
+
 template <int BYTES>
 __device__ __forceinline__ void cp_async_n(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -143,17 +238,8 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     for (int w = 0; w < kTileX * kTileY; ++w) slots += ta.gmax[tile * (kTileX * kTileY) + w];
     nscale = 4294967295.f / (float)(slots * kLanes + 1);
   }
-  real ajx[2][3][3], ajy[3][2][3], ajz[3][3][2];
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (a < 2) ajx[a][b][c] = (real)0;
-        if (b < 2) ajy[a][b][c] = (real)0;
-        if (c < 2) ajz[a][b][c] = (real)0;
-      }
+  HomeJ<real> acc;
+  acc.zero();
   // ring of particle rows fetched ahead; each lane copies and reads only its
   // own slots, so the per-thread cp.async groups need no warp barrier
   int* pcell = reinterpret_cast<int*>(smem_raw + S::pcell_off) + warp * kStages * kLanes;
@@ -216,32 +302,7 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       if (i == hi && j == hj && k == hk) {
         const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
         const W3<real> bx = home3(X, hi), by = home3(Y, hj), bz = home3(Z, hk);
-        const real ax[2] = {X.a0, X.a1}, ay[2] = {Y.a0, Y.a1}, az[2] = {Z.a0, Z.a1};
-        const real qx = pc.qn * vx, qy = pc.qn * vy, qz = pc.qn * vz;
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-#pragma unroll
-          for (int cc = 0; cc < 3; ++cc) {
-            const real yz = by.w[b] * bz.w[cc];
-            ajx[0][b][cc] += (qx * ax[0]) * yz;
-            ajx[1][b][cc] += (qx * ax[1]) * yz;
-          }
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int cc = 0; cc < 3; ++cc) {
-            const real xz = bx.w[a] * bz.w[cc];
-            ajy[a][0][cc] += (qy * ay[0]) * xz;
-            ajy[a][1][cc] += (qy * ay[1]) * xz;
-          }
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            const real xy = bx.w[a] * by.w[b];
-            ajz[a][b][0] += (qz * az[0]) * xy;
-            ajz[a][b][1] += (qz * az[1]) * xy;
-          }
+        acc.add(pc.qn * vx, pc.qn * vy, pc.qn * vz, X, Y, Z, bx, by, bz);
       } else if (in_array(g, i, j, k)) {
         if (stencil_ok(g, i, j, k)) {
           const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
@@ -285,9 +346,9 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
           const int s = ((la + a) * WY + (lb + b)) * WZ + (lc + cc);
-          if (a < 2) atomicAdd(win + s + WY * WZ, ajx[a][b][cc]);       // x nodes h, h+1
-          if (b < 2) atomicAdd(win + WN + s + WZ, ajy[a][b][cc]);       // y nodes h, h+1
-          if (cc < 2) atomicAdd(win + 2 * WN + s + 1, ajz[a][b][cc]);   // z nodes h, h+1
+          if (a < 2) atomicAdd(win + s + WY * WZ, acc.x(a, b, cc));       // x nodes h, h+1
+          if (b < 2) atomicAdd(win + WN + s + WZ, acc.y(a, b, cc));       // y nodes h, h+1
+          if (cc < 2) atomicAdd(win + 2 * WN + s + 1, acc.z(a, b, cc));   // z nodes h, h+1
         }
   }
   __syncthreads();
