@@ -236,7 +236,8 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     int slots = 0;
 #pragma unroll
     for (int w = 0; w < kTileX * kTileY; ++w) slots += ta.gmax[tile * (kTileX * kTileY) + w];
-    nscale = 4294967295.f / (float)(slots * kLanes + 1);
+    // below 2^23 as well, where scatter8_win_fixed's rounding by an added 2^23 is exact
+    nscale = fminf(4294967295.f / (float)(slots * kLanes + 1), 8388607.f);
   }
   HomeJ<real> acc;
   acc.zero();

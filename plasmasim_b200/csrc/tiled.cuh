@@ -287,9 +287,10 @@ __device__ __forceinline__ void scatter8_win(real* win, int wx0, int wy0, int wz
 // shared-memory reductions, which need no compare-and-swap loop and give a sum
 // that does not depend on the order of the particles. The caller picks `scale`
 // so that no node can overflow: a node collects at most one unit of weight from
-// each particle of the tile, so scale = (2^32 - 1) / (slots + 1) is safe. With
-// 64 particles per cell this resolves 2^-17.7 of a particle's weight, as fine
-// as an FP32 sum of the same node. The stencil falls back to FP32 global
+// each particle of the tile, so scale = (2^32 - 1) / (slots + 1) is safe; it is
+// also kept below 2^23 for the rounding below. With 64 particles per cell this
+// resolves 2^-17.7 of a particle's weight, as fine as an FP32 sum of the same
+// node. The stencil falls back to FP32 global
 // atomics (weight v) when it leaves the window.
 __device__ __forceinline__ void red_shared_u32(const unsigned* p, unsigned v) {
   asm volatile("red.shared.add.u32 [%0], %1;" :: "r"((unsigned)__cvta_generic_to_shared(p)), "r"(v) : "memory");
@@ -302,16 +303,27 @@ __device__ __forceinline__ void scatter8_win_fixed(unsigned* win, int wx0, int w
   const int la = a - wx0, lb = b - wy0, lc = c - wz0;
   if (la >= 0 && la <= WX - 2 && lb >= 0 && lb <= WY - 2 && lc >= 0 && lc <= WZ - 2) {
     const unsigned* s = win + (la * WY + lb) * WZ + lc;
-    const float a0 = scale * x0, a1 = scale * x1;
-    const float a00 = a0 * y0, a01 = a0 * y1, a10 = a1 * y0, a11 = a1 * y1;
-    red_shared_u32(s, __float2uint_rn(a00 * z0));
-    red_shared_u32(s + 1, __float2uint_rn(a00 * z1));
-    red_shared_u32(s + WZ, __float2uint_rn(a01 * z0));
-    red_shared_u32(s + WZ + 1, __float2uint_rn(a01 * z1));
-    red_shared_u32(s + WY * WZ, __float2uint_rn(a10 * z0));
-    red_shared_u32(s + WY * WZ + 1, __float2uint_rn(a10 * z1));
-    red_shared_u32(s + WY * WZ + WZ, __float2uint_rn(a11 * z0));
-    red_shared_u32(s + WY * WZ + WZ + 1, __float2uint_rn(a11 * z1));
+    // the eight node weights (each in [0, scale], scale < 2^23) rounded to
+    // integers by adding 2^23 in the FMA: the sum's low mantissa bits are then
+    // the rounded weight, with no float-to-integer conversion; the two x
+    // planes travel as one packed pair
+    constexpr float kM = 8388608.f;                 // 2^23
+    constexpr unsigned kMBits = 0x4B000000u;        // its bit pattern
+    const float2 M = make_float2(kM, kM);
+    const float2 ax = __fmul2_rn(make_float2(x0, x1), make_float2(scale, scale));
+    const float2 ay0 = __fmul2_rn(ax, make_float2(y0, y0));  // (a00, a10)
+    const float2 ay1 = __fmul2_rn(ax, make_float2(y1, y1));  // (a01, a11)
+    const float2 Z0 = make_float2(z0, z0), Z1 = make_float2(z1, z1);
+    const float2 t00 = __ffma2_rn(ay0, Z0, M), t01 = __ffma2_rn(ay0, Z1, M);
+    const float2 t10 = __ffma2_rn(ay1, Z0, M), t11 = __ffma2_rn(ay1, Z1, M);
+    red_shared_u32(s, __float_as_uint(t00.x) - kMBits);
+    red_shared_u32(s + 1, __float_as_uint(t01.x) - kMBits);
+    red_shared_u32(s + WZ, __float_as_uint(t10.x) - kMBits);
+    red_shared_u32(s + WZ + 1, __float_as_uint(t11.x) - kMBits);
+    red_shared_u32(s + WY * WZ, __float_as_uint(t00.y) - kMBits);
+    red_shared_u32(s + WY * WZ + 1, __float_as_uint(t01.y) - kMBits);
+    red_shared_u32(s + WY * WZ + WZ, __float_as_uint(t10.y) - kMBits);
+    red_shared_u32(s + WY * WZ + WZ + 1, __float_as_uint(t11.y) - kMBits);
   } else {
     scatter8(gplane, a * g.sx + b * g.gz + c, g.sx, g.gz, v, x0, x1, y0, y1, z0, z1);
   }
