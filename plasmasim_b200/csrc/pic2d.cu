@@ -328,13 +328,55 @@ __device__ __forceinline__ void dep4(real* P, int G, int i, int k, real v, real 
   atomicAdd(P + (i + 1) * G + k + 1, v * (x1 * z1));
 }
 
+// dep4 for a whole warp: lanes whose four nodes coincide (particles in the
+// same cell and half-cell) are found with a match, their values summed by the
+// lowest such lane through the warp's scratch rows, and only that lane adds
+// the sums to the plane. Every lane of the warp calls it; `active` selects the
+// lanes that deposit.
+template <typename real>
+__device__ __forceinline__ void dep4_warp(real* P, int G, bool active, int i, int k, real v, real x0, real x1,
+                                          real z0, real z1, real (*ws)[4]) {
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(0xffffffffu, active ? i * G + k : -1 - lane);
+  const int leader = __ffs(peers) - 1;
+  real w0 = v * (x0 * z0), w1 = v * (x1 * z0), w2 = v * (x0 * z1), w3 = v * (x1 * z1);
+  if (__any_sync(0xffffffffu, __popc(peers) > 1)) {
+    ws[lane][0] = w0;
+    ws[lane][1] = w1;
+    ws[lane][2] = w2;
+    ws[lane][3] = w3;
+    __syncwarp();
+    if (lane == leader)
+      for (unsigned m = peers & (peers - 1); m; m &= m - 1) {  // the other members, in lane order
+        const int o = __ffs(m) - 1;
+        w0 += ws[o][0];
+        w1 += ws[o][1];
+        w2 += ws[o][2];
+        w3 += ws[o][3];
+      }
+    __syncwarp();
+  }
+  if (active && lane == leader) {
+    atomicAdd(P + i * G + k, w0);
+    atomicAdd(P + (i + 1) * G + k, w1);
+    atomicAdd(P + i * G + k + 1, w2);
+    atomicAdd(P + (i + 1) * G + k + 1, w3);
+  }
+}
+
 // The particle part of one step for every run and species (the push loop,
 // the drift loop and the x exchange + removal in one pass). item = (run*2 +
-// species, first slot relative to the run).
+// species, first slot relative to the run). A block walks its chunk in rows of
+// BLOCK slots with every lane present, so that the deposits can sum the lanes
+// of a warp that share nodes before their atomics: slots follow the cells the
+// particles were created in, so neighbouring lanes often deposit on the same
+// nodes.
 template <typename real, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, const Run<real>* __restrict__ runs,
                                                        const State* __restrict__ st, const Item* __restrict__ items,
                                                        int nitems, int chunk, unsigned long long* err) {
+  __shared__ real scratch[BLOCK / 32][32][4];
+  real(*ws)[4] = scratch[threadIdx.x >> 5];
   unsigned pushed = 0;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int rs = items[it].run;
@@ -342,7 +384,7 @@ __global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, con
     const Run<real> R = runs[r];
     const int n = st[r].count[s];
     const int first = items[it].first;
-    if (first >= n) continue;
+    if (first >= n) continue;  // block-uniform
     const int last = min(first + chunk, n);
     const PView<real> P = pview<real>(pools, s);
     const int G = R.gz;
@@ -360,63 +402,76 @@ __global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, con
     const real* Bx = plane(F, R, P_BX);
     const real* By = plane(F, R, P_BY);
     const real* Bz = plane(F, R, P_BZ);
-    for (int q = first + threadIdx.x; q < last; q += BLOCK) {
+    for (int qb = first; qb < last; qb += BLOCK) {  // block-uniform
+      const int q = qb + threadIdx.x;
       const long long t = R.poff + q;
-      const int c = P.cell[t];
-      if (c < 0) continue;
-      ++pushed;
-      int i, k;
-      unpack2(c, i, k);
-      real fx = P.ox[t], fz = P.oz[t];
-      real vx = P.vx[t], vy = P.vy[t], vz = P.vz[t];
-      // ballistic margins (:682-686): z < A2, z > Nz+4-A2, x < A2, x > Nx+4-A2 (cells)
-      const int hz = R.nz + 4 - R.a2, hx = R.nx + 4 - R.a2;
-      const bool bal = k < R.a2 || i < R.a2 || k > hz || (k == hz && fz > (real)0) || i > hx ||
-                       (i == hx && fx > (real)0);
-      if (!bal) {
-        if (i < 1 || k < 1 || i > R.gx - 2 || k > R.gz - 2) {
-          atomicAdd(err + ERR_DEPOSIT_OOB, 1ull);
-        } else {
-          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-          // ex, bz: x aligned, z shifted; ez, bx: x shifted, z aligned; ey: both shifted; by: both aligned
-          real ex = bil(Ex, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1) + (real)R.ex_add;
-          real bz = bil(Bz, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
-          real ey = bil(Ey, G, X.b, Z.b, X.b0, X.b1, Z.b0, Z.b1) + (real)R.ey_add;
-          real ez = bil(Ez, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
-          real bx = bil(Bx, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
-          real by = bil(By, G, X.a, Z.a, X.a0, X.a1, Z.a0, Z.a1);
-          // cal_track_c4 (:1520-1560)
-          const real S = (real)2 * T / ((real)1 + T * T * (bx * bx + by * by + bz * bz));
-          const real ux = vx + ex * T, uy = vy + ey * T, uz = vz + ez * T;
-          const real uox = ux + T * (uy * bz - uz * by);
-          const real uoy = uy + T * (uz * bx - ux * bz);
-          const real uoz = uz + T * (ux * by - uy * bx);
-          vx = ux + S * (uoy * bz - uoz * by) + ex * T;
-          vy = uy + S * (uoz * bx - uox * bz) + ey * T;
-          vz = uz + S * (uox * by - uoy * bx) + ez * T;
+      const int c = q < last ? P.cell[t] : -1;
+      const bool act = c >= 0;
+      int i = 0, k = 0;
+      real fx = 0, fz = 0, vx = 0, vy = 0, vz = 0;
+      if (act) {
+        ++pushed;
+        unpack2(c, i, k);
+        fx = P.ox[t];
+        fz = P.oz[t];
+        vx = P.vx[t];
+        vy = P.vy[t];
+        vz = P.vz[t];
+        // ballistic margins (:682-686): z < A2, z > Nz+4-A2, x < A2, x > Nx+4-A2 (cells)
+        const int hz = R.nz + 4 - R.a2, hx = R.nx + 4 - R.a2;
+        const bool bal = k < R.a2 || i < R.a2 || k > hz || (k == hz && fz > (real)0) || i > hx ||
+                         (i == hx && fx > (real)0);
+        if (!bal) {
+          if (i < 1 || k < 1 || i > R.gx - 2 || k > R.gz - 2) {
+            atomicAdd(err + ERR_DEPOSIT_OOB, 1ull);
+          } else {
+            const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+            // ex, bz: x aligned, z shifted; ez, bx: x shifted, z aligned; ey: both shifted; by: both aligned
+            real ex = bil(Ex, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1) + (real)R.ex_add;
+            real bz = bil(Bz, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
+            real ey = bil(Ey, G, X.b, Z.b, X.b0, X.b1, Z.b0, Z.b1) + (real)R.ey_add;
+            real ez = bil(Ez, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
+            real bx = bil(Bx, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
+            real by = bil(By, G, X.a, Z.a, X.a0, X.a1, Z.a0, Z.a1);
+            // cal_track_c4 (:1520-1560)
+            const real S = (real)2 * T / ((real)1 + T * T * (bx * bx + by * by + bz * bz));
+            const real ux = vx + ex * T, uy = vy + ey * T, uz = vz + ez * T;
+            const real uox = ux + T * (uy * bz - uz * by);
+            const real uoy = uy + T * (uz * bx - ux * bz);
+            const real uoz = uz + T * (ux * by - uy * bx);
+            vx = ux + S * (uoy * bz - uoz * by) + ex * T;
+            vy = uy + S * (uoz * bx - uox * bz) + ey * T;
+            vz = uz + S * (uox * by - uoy * bx) + ez * T;
+          }
         }
+        advance(i, fx, vx * hdt);
+        advance(k, fz, vz * hdt);
       }
-      advance(i, fx, vx * hdt);
-      advance(k, fz, vz * hdt);
       // J deposit at x^{n+1/2} for dx <= x < (Nx+3) dx, 2 dx <= z < (Nz+2) dx
-      if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
+      {
+        const bool dep = act && i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2;
         const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-        dep4(jx, G, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1);
-        dep4(jy, G, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1);
-        dep4(jz, G, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1);
+        dep4_warp(jx, G, dep, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1, ws);
+        dep4_warp(jy, G, dep, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1, ws);
+        dep4_warp(jz, G, dep, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1, ws);
       }
-      advance(i, fx, vx * hdt);
-      advance(k, fz, vz * hdt);
-      if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
+      if (act) {
+        advance(i, fx, vx * hdt);
+        advance(k, fz, vz * hdt);
+      }
+      {
+        const bool dep = act && i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2;
         const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-        dep4(dn, G, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1);
+        dep4_warp(dn, G, dep, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1, ws);
       }
-      // x exchange at size 1: forward crossers wrap, backward ones are dropped; then removal
-      if (i == R.nx + 2 && k >= 2 && k < R.nz + 2) i -= R.nx;
-      const bool keep = i >= 2 && i < R.nx + 2 && k >= 2 && k < R.nz + 2;
-      P.cell[t] = keep ? pack2(i, k) : -1;
-      P.ox[t] = fx; P.oz[t] = fz;
-      P.vx[t] = vx; P.vy[t] = vy; P.vz[t] = vz;
+      if (act) {
+        // x exchange at size 1: forward crossers wrap, backward ones are dropped; then removal
+        if (i == R.nx + 2 && k >= 2 && k < R.nz + 2) i -= R.nx;
+        const bool keep = i >= 2 && i < R.nx + 2 && k >= 2 && k < R.nz + 2;
+        P.cell[t] = keep ? pack2(i, k) : -1;
+        P.ox[t] = fx; P.oz[t] = fz;
+        P.vx[t] = vx; P.vy[t] = vy; P.vz[t] = vz;
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
@@ -871,6 +926,9 @@ struct pic2d_batch {
   int* pos = nullptr;
   int* scan_tmp = nullptr;
   size_t scan_len = 0;
+  int* ccnt = nullptr;   // cell sort: particles per cell, first slot per cell, cursors (rho_len each)
+  int* coffs = nullptr;
+  int* ccur = nullptr;
   int* step_dev = nullptr;
   unsigned long long* err = nullptr;
   int c_add = 0;
@@ -973,6 +1031,119 @@ int scan_excl(pic2d_batch* b, const int* in, int* out, long long n, int* tmp, si
   return PIC_OK;
 }
 
+// ---------------------------------------------------------- cell sort
+// The reference draws its particles uniformly over each source slab, so their
+// order in the lists says nothing about where they are; deposited in that
+// order, every lane of a warp adds to different nodes and the L2 reductions
+// bound the step. A counting sort of every run's particles by cell (into the
+// other pool, empty slots dropped) lets neighbouring lanes share nodes, which
+// push2d_kernel's deposits then sum before their atomics. Keys index the
+// run's interior cells from R.roff (the nx * nz layout of its Poisson buffer).
+__device__ __forceinline__ int warp_add_count(int* counter, int key, bool active) {
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(0xffffffffu, active ? key : -1 - lane);
+  const int leader = __ffs(peers) - 1;
+  int old = 0;
+  if (active && lane == leader) old = atomicAdd(counter + key, __popc(peers));
+  old = __shfl_sync(0xffffffffu, old, leader);
+  return old + __popc(peers & ((1u << lane) - 1u));
+}
+
+template <typename real>
+__device__ __forceinline__ int sort_key(const Run<real>& R, int c) {
+  if (c < 0) return -1;
+  int i, k;
+  unpack2(c, i, k);
+  i -= 2;
+  k -= 2;
+  if (i < 0 || k < 0 || i >= R.nx || k >= R.nz) return -1;
+  return (int)R.roff + i * R.nz + k;
+}
+
+// Particles per cell of species s (every lane of a block walks its chunk in rows).
+template <typename real>
+__global__ void cellcount2d_kernel(Pools pools, const Run<real>* __restrict__ runs, const State* __restrict__ st,
+                                   const Item* __restrict__ items, int nitems, int chunk, int s, int* cnt) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int rs = items[it].run;
+    if ((rs & 1) != s) continue;
+    const Run<real> R = runs[rs >> 1];
+    const int n = st[rs >> 1].count[s];
+    const int first = items[it].first;
+    const int last = min(first + chunk, n);
+    const int* cell = pools.cell[s];
+    for (int qb = first; qb < last; qb += blockDim.x) {  // block-uniform
+      const int q = qb + threadIdx.x;
+      const int key = q < last ? sort_key(R, cell[R.poff + q]) : -1;
+      warp_add_count(cnt, key < 0 ? 0 : key, key >= 0);
+    }
+  }
+}
+
+// Each particle to slot (cell's first slot + its rank) of the other pool.
+template <typename real>
+__global__ void cellscatter2d_kernel(Pools src, Pools dst, const Run<real>* __restrict__ runs,
+                                     const State* __restrict__ st, const Item* __restrict__ items, int nitems,
+                                     int chunk, int s, const int* __restrict__ offs, int* cursor) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int rs = items[it].run;
+    if ((rs & 1) != s) continue;
+    const Run<real> R = runs[rs >> 1];
+    const int n = st[rs >> 1].count[s];
+    const int first = items[it].first;
+    const int last = min(first + chunk, n);
+    const PView<real> A = pview<real>(src, s), B = pview<real>(dst, s);
+    const int base = offs[R.roff];
+    for (int qb = first; qb < last; qb += blockDim.x) {  // block-uniform
+      const int q = qb + threadIdx.x;
+      const long long t = R.poff + q;
+      const int c = q < last ? A.cell[t] : -1;
+      const int key = q < last ? sort_key(R, c) : -1;
+      const int rank = warp_add_count(cursor, key < 0 ? 0 : key, key >= 0);
+      if (key < 0) continue;
+      const long long d = R.poff + (offs[key] - base) + rank;
+      B.cell[d] = c;
+      B.ox[d] = A.ox[t]; B.oz[d] = A.oz[t];
+      B.vx[d] = A.vx[t]; B.vy[d] = A.vy[t]; B.vz[d] = A.vz[t];
+    }
+  }
+}
+
+// Live particles of every run after the sort.
+template <typename real>
+__global__ void cellsort_count_kernel(const Run<real>* __restrict__ runs, State* st, int nruns, int s,
+                                      const int* __restrict__ offs, const int* __restrict__ cnt) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nruns) return;
+  const Run<real> R = runs[r];
+  const long long e = R.roff + (long long)R.nx * R.nz - 1;
+  st[r].count[s] = offs[e] + cnt[e] - offs[R.roff];
+}
+
+// Every run's particles by cell into the other pool, empty slots dropped.
+template <typename real>
+int cellsort(pic2d_batch* b) {
+  const int nb = 1 - b->cur;
+  const long long nc = b->rho_len;
+  const Run<real>* R = runs_of<real>(b);
+  for (int s = 0; s < 2; ++s) {
+    CK2(cudaMemsetAsync(b->ccnt, 0, sizeof(int) * (size_t)nc, b->stream));
+    CK2(cudaMemsetAsync(b->ccur, 0, sizeof(int) * (size_t)nc, b->stream));
+    cellcount2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], R, b->st, b->part_items,
+                                                                            b->n_part, kChunk, s, b->ccnt);
+    CKL2();
+    CKR2(scan_excl(b, b->ccnt, b->coffs, nc, b->scan_tmp, b->scan_len));
+    cellscatter2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(
+        b->pool[b->cur], b->pool[nb], R, b->st, b->part_items, b->n_part, kChunk, s, b->coffs, b->ccur);
+    CKL2();
+    cellsort_count_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(R, b->st, b->nruns, s, b->coffs,
+                                                                               b->ccnt);
+    CKL2();
+  }
+  b->cur = nb;
+  return PIC_OK;
+}
+
 // Removes every run's empty slots, keeping order (into the other pool).
 template <typename real>
 int compact(pic2d_batch* b) {
@@ -1054,7 +1225,7 @@ int renew_grid(pic2d_batch* b) {
 
 // One loop body for every run (fdtd :627-1015).
 template <typename real>
-int step_body(pic2d_batch* b, bool refill) {
+int step_body(pic2d_batch* b, bool refill, bool sort = false) {
   const Run<real>* R = runs_of<real>(b);
   real* F = (real*)b->field;
   CKR2(renew_grid<real>(b));
@@ -1062,8 +1233,10 @@ int step_body(pic2d_batch* b, bool refill) {
     delete5_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], R, b->st, b->part_items,
                                                                         b->n_part, kChunk);
     CKL2();
-    CKR2(compact<real>(b));
+    CKR2(cellsort<real>(b));  // drops the deleted slots as a compaction would
     CKR2(run_sources<real>(b, 1));
+  } else if (sort) {
+    CKR2(cellsort<real>(b));
   }
   renew_b4_kernel<real><<<persistent(b->n_row), 128, 0, b->stream>>>(F, R, b->row_items, b->n_row);
   CKL2();
@@ -1104,9 +1277,11 @@ template <typename real>
 int run_steps(pic2d_batch* b, int nsteps) {
   for (int i = 0; i < nsteps; ++i) {
     const bool refill = b->c_add > b->cfg[0].add_interval - 1;
-    if (refill || !b->use_graph) {
-      CKR2(step_body<real>(b, refill));
-      if (refill) drop_graphs(b);
+    const int si = b->cfg[0].sort_interval;
+    const bool sort = !refill && si > 0 && b->step > 0 && b->step % si == 0;
+    if (refill || sort || !b->use_graph) {
+      CKR2(step_body<real>(b, refill, sort));
+      if (refill || sort) drop_graphs(b);
     } else {
       if (!b->graph[0]) {
         cudaGraph_t graph;
@@ -1173,6 +1348,7 @@ int do_init(pic2d_batch* b) {
   for (int p = 0; p < 2; ++p) CK2(cudaMemsetAsync(b->pool[p].cell[0], 0xff, sizeof(int) * b->pool_slots, b->stream));
   for (int p = 0; p < 2; ++p) CK2(cudaMemsetAsync(b->pool[p].cell[1], 0xff, sizeof(int) * b->pool_slots, b->stream));
   CKR2(run_sources<real>(b, 0));
+  CKR2(cellsort<real>(b));  // the particles by cell (only their order changes)
   // fdtd's set-up (:583-625)
   CKR2(renew_grid<real>(b));
   density2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], F, R, b->st, b->part_items,
@@ -1309,6 +1485,9 @@ int do_create(pic2d_batch* b) {
   CK2(cudaMalloc(&b->pos, sizeof(int) * (size_t)poff));
   b->scan_len = (size_t)(2 * ((poff + kScanTile - 1) / kScanTile) + 64);
   CK2(cudaMalloc(&b->scan_tmp, sizeof(int) * b->scan_len));
+  CK2(cudaMalloc(&b->ccnt, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
+  CK2(cudaMalloc(&b->coffs, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
+  CK2(cudaMalloc(&b->ccur, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
   CK2(cudaMalloc(&b->step_dev, sizeof(int)));
   CK2(cudaMemset(b->step_dev, 0, sizeof(int)));
   CK2(cudaMalloc(&b->err, sizeof(unsigned long long) * ERR_COUNT));
@@ -1331,6 +1510,7 @@ void free_batch(pic2d_batch* b) {
   for (int w = 0; w < 2; ++w)
     for (int s = 0; s < 2; ++s) { cudaFree(b->src_items[w][s]); cudaFree(b->sets[w][s]); }
   cudaFree(b->flags); cudaFree(b->pos); cudaFree(b->scan_tmp); cudaFree(b->step_dev); cudaFree(b->err);
+  cudaFree(b->ccnt); cudaFree(b->coffs); cudaFree(b->ccur);
   if (b->stream) cudaStreamDestroy(b->stream);
 }
 
@@ -1469,6 +1649,7 @@ int pic2d_config_normalized(pic2d_config* k, int nx, int nz, int np) {
   k->absorb_grid = 32; k->absorb_grid2 = 16; k->absorb_grid3 = 32;
   k->sigma_a = 1e-6;
   k->add_interval = 250;
+  k->sort_interval = 20;
   k->seed_p = 0; k->seed_v = 50;
   return PIC_OK;
 }
@@ -1478,6 +1659,7 @@ int pic2d_create(const pic2d_config* cfgs, int nruns, int precision, int device,
   for (int r = 0; r < nruns; ++r) {
     if (!valid(cfgs[r])) return PIC_ERR_ARG;
     if (cfgs[r].add_interval != cfgs[0].add_interval) return PIC_ERR_ARG;  // runs step together
+    if (cfgs[r].sort_interval != cfgs[0].sort_interval || cfgs[r].sort_interval < 0) return PIC_ERR_ARG;
   }
   *out = nullptr;
   if (cudaSetDevice(device) != cudaSuccess) return PIC_ERR_CUDA;

@@ -26,7 +26,7 @@ class _C2Config(C.Structure):
         ("c", C.c_double), ("v_drift", C.c_double), ("n_all", C.c_double), ("ti", C.c_double),
         ("te", C.c_double), ("coil_i", C.c_double), ("imf_x", C.c_double), ("imf_y", C.c_double),
         ("imf_z", C.c_double), ("absorb_grid", C.c_int), ("absorb_grid2", C.c_int),
-        ("absorb_grid3", C.c_int), ("reserved", C.c_int), ("sigma_a", C.c_double),
+        ("absorb_grid3", C.c_int), ("sort_interval", C.c_int), ("sigma_a", C.c_double),
         ("seed_p", C.c_ulonglong), ("seed_v", C.c_ulonglong), ("capacity", C.c_longlong),
     ]
 
@@ -57,7 +57,7 @@ class Pic2DConfig:
     absorb_grid: int = 32
     absorb_grid2: int = 16
     absorb_grid3: int = 32
-    reserved: int = 0
+    sort_interval: int = 20
     sigma_a: float = 1e-6
     seed_p: int = 0
     seed_v: int = 50
