@@ -328,35 +328,38 @@ __device__ __forceinline__ void dep4(real* P, int G, int i, int k, real v, real 
   atomicAdd(P + (i + 1) * G + k + 1, v * (x1 * z1));
 }
 
-// dep4 for a whole warp: lanes whose four nodes coincide (particles in the
-// same cell and half-cell) are found with a match, their values summed by the
-// lowest such lane through the warp's scratch rows, and only that lane adds
-// the sums to the plane. Every lane of the warp calls it; `active` selects the
-// lanes that deposit.
+// dep4 for a whole warp: runs of neighbouring lanes whose four nodes coincide
+// (particles of one cell and half-cell, adjacent after the cell sort) are
+// summed with a segmented shuffle reduction, and the first lane of each run
+// adds the sums to the plane. Every lane of the warp calls it; `active`
+// selects the lanes that deposit. A warp without such runs adds directly.
 template <typename real>
 __device__ __forceinline__ void dep4_warp(real* P, int G, bool active, int i, int k, real v, real x0, real x1,
-                                          real z0, real z1, real (*ws)[4]) {
+                                          real z0, real z1) {
   const int lane = threadIdx.x & 31;
-  const unsigned peers = __match_any_sync(0xffffffffu, active ? i * G + k : -1 - lane);
-  const int leader = __ffs(peers) - 1;
+  const int key = active ? i * G + k : -1 - lane;
+  const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+  const bool head = lane == 0 || prev != key;
+  const unsigned heads = __ballot_sync(0xffffffffu, head);
   real w0 = v * (x0 * z0), w1 = v * (x1 * z0), w2 = v * (x0 * z1), w3 = v * (x1 * z1);
-  if (__any_sync(0xffffffffu, __popc(peers) > 1)) {
-    ws[lane][0] = w0;
-    ws[lane][1] = w1;
-    ws[lane][2] = w2;
-    ws[lane][3] = w3;
-    __syncwarp();
-    if (lane == leader)
-      for (unsigned m = peers & (peers - 1); m; m &= m - 1) {  // the other members, in lane order
-        const int o = __ffs(m) - 1;
-        w0 += ws[o][0];
-        w1 += ws[o][1];
-        w2 += ws[o][2];
-        w3 += ws[o][3];
+  if (heads != 0xffffffffu) {  // warp-uniform
+    const unsigned after = lane == 31 ? 0u : heads & (0xffffffffu << (lane + 1));
+    const int end = after ? __ffs(after) - 2 : 31;  // last lane of this lane's run
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const real o0 = __shfl_down_sync(0xffffffffu, w0, off);
+      const real o1 = __shfl_down_sync(0xffffffffu, w1, off);
+      const real o2 = __shfl_down_sync(0xffffffffu, w2, off);
+      const real o3 = __shfl_down_sync(0xffffffffu, w3, off);
+      if (lane + off <= end) {
+        w0 += o0;
+        w1 += o1;
+        w2 += o2;
+        w3 += o3;
       }
-    __syncwarp();
+    }
   }
-  if (active && lane == leader) {
+  if (active && head) {
     atomicAdd(P + i * G + k, w0);
     atomicAdd(P + (i + 1) * G + k, w1);
     atomicAdd(P + i * G + k + 1, w2);
@@ -368,15 +371,12 @@ __device__ __forceinline__ void dep4_warp(real* P, int G, bool active, int i, in
 // the drift loop and the x exchange + removal in one pass). item = (run*2 +
 // species, first slot relative to the run). A block walks its chunk in rows of
 // BLOCK slots with every lane present, so that the deposits can sum the lanes
-// of a warp that share nodes before their atomics: slots follow the cells the
-// particles were created in, so neighbouring lanes often deposit on the same
-// nodes.
+// of a warp that share nodes before their atomics: after the cell sort,
+// neighbouring lanes mostly deposit on the same nodes.
 template <typename real, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, const Run<real>* __restrict__ runs,
                                                        const State* __restrict__ st, const Item* __restrict__ items,
                                                        int nitems, int chunk, unsigned long long* err) {
-  __shared__ real scratch[BLOCK / 32][32][4];
-  real(*ws)[4] = scratch[threadIdx.x >> 5];
   unsigned pushed = 0;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int rs = items[it].run;
@@ -451,9 +451,9 @@ __global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, con
       {
         const bool dep = act && i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2;
         const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-        dep4_warp(jx, G, dep, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1, ws);
-        dep4_warp(jy, G, dep, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1, ws);
-        dep4_warp(jz, G, dep, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1, ws);
+        dep4_warp(jx, G, dep, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1);
+        dep4_warp(jy, G, dep, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1);
+        dep4_warp(jz, G, dep, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1);
       }
       if (act) {
         advance(i, fx, vx * hdt);
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, con
       {
         const bool dep = act && i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2;
         const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-        dep4_warp(dn, G, dep, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1, ws);
+        dep4_warp(dn, G, dep, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1);
       }
       if (act) {
         // x exchange at size 1: forward crossers wrap, backward ones are dropped; then removal
