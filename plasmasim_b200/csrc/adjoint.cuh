@@ -390,11 +390,11 @@ __global__ void __launch_bounds__(256) push_adjoint_kernel(Parts<real> P, int n,
 // acc[2] += sum of dJ/dvz over slots [first, n): particles created with
 // vz = V + thermal (by the initial load or a refill).
 template <typename real>
-__global__ void __launch_bounds__(256) drift_grad_kernel(const int* __restrict__ cell, const real* __restrict__ lvz,
+__global__ void __launch_bounds__(256) drift_grad_kernel(Parts<real> P, const real* __restrict__ lvz,
                                                          int first, int n, double* acc) {
   double s[1] = {0.0};
   for (int t = first + blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-    if (cell[t] >= 0) s[0] += (double)lvz[t];
+    if (P.cell[t] >= 0) s[0] += (double)lvz[t];
   const int idx[1] = {2};
   const double scale[1] = {1.0};
   block_reduce_add<1>(s, acc, idx, scale);

@@ -72,29 +72,15 @@ void snap_free(AdjSnap& S) {
 
 template <typename real>
 Parts<real> parts_at(void* base, long long cap) {
-  Parts<real> P;
   char* b = (char*)base;
-  P.cell = (int*)b;
-  char* p = b + align256((size_t)cap * 4);
-  for (int a = 0; a < 3; ++a) {
-    P.o[a] = (real*)p;
-    p += align256((size_t)cap * sizeof(real));
-  }
-  for (int a = 0; a < 3; ++a) {
-    P.v[a] = (real*)p;
-    p += align256((size_t)cap * sizeof(real));
-  }
-  return P;
+  return make_parts<real>((real*)b, (real*)(b + parts_record_bytes(cap, sizeof(real))));
 }
 
 template <typename real>
 int copy_parts(pic_ctx* c, Parts<real> dst, Parts<real> src, long long n) {
   if (n <= 0) return PIC_OK;
-  CK(cudaMemcpyAsync(dst.cell, src.cell, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
-  for (int a = 0; a < 3; ++a) {
-    CK(cudaMemcpyAsync(dst.o[a], src.o[a], sizeof(real) * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
-    CK(cudaMemcpyAsync(dst.v[a], src.v[a], sizeof(real) * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
-  }
+  CK(cudaMemcpyAsync(dst.ra, src.ra, 4 * sizeof(real) * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(dst.rb, src.rb, 4 * sizeof(real) * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
   return PIC_OK;
 }
 
@@ -156,7 +142,7 @@ int adj_compact(pic_ctx* c, AdjRun& R, int s, int* map) {
   const long long n = st.count;
   if (n == 0) return PIC_OK;
   CKR(ensure_flags(c, (size_t)n));
-  live_flag_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s).cell, (int)n, c->flags);
+  live_flag_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, c->flags);
   CKL();
   const long long tiles = (n + kScanTile - 1) / kScanTile;
   if ((size_t)(2 * tiles + 64) > R.scan_len) return PIC_ERR_STATE;
@@ -350,7 +336,7 @@ int adj_unrefill(pic_ctx* c, AdjRun& R, const AdjSnap& in) {
     if (in.count[s] > in.kept[s]) {
       const AdjPart<real> A = adj_part<real>(c, R, s, R.lcur[s]);
       drift_grad_kernel<real><<<particle_blocks(in.count[s] - in.kept[s]), kThreads, 0, c->stream>>>(
-          parts_at<real>(in.part[s], in.count[s]).cell, A.lv[2], (int)in.kept[s], (int)in.count[s], R.acc);
+          parts_at<real>(in.part[s], in.count[s]), A.lv[2], (int)in.kept[s], (int)in.count[s], R.acc);
       CKL();
     }
     if (in.map[s]) {

@@ -137,26 +137,12 @@ Fields<real> fields(pic_ctx* c) {
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-size_t store_bytes(long long cap, size_t rsize) {
-  return align256((size_t)cap * 4) + 6 * align256((size_t)cap * rsize);
-}
+size_t store_bytes(long long cap, size_t rsize) { return 2 * parts_record_bytes(cap, rsize); }
 
 template <typename real>
 Parts<real> parts(pic_ctx* c, int s, int buf) {
-  Parts<real> P;
   char* base = (char*)c->sp[s].mem[buf];
-  const long long cap = c->sp[s].cap;
-  P.cell = (int*)base;
-  char* p = base + align256((size_t)cap * 4);
-  for (int a = 0; a < 3; ++a) {
-    P.o[a] = (real*)p;
-    p += align256((size_t)cap * sizeof(real));
-  }
-  for (int a = 0; a < 3; ++a) {
-    P.v[a] = (real*)p;
-    p += align256((size_t)cap * sizeof(real));
-  }
-  return P;
+  return make_parts<real>((real*)base, (real*)(base + parts_record_bytes(c->sp[s].cap, sizeof(real))));
 }
 
 template <typename real>
@@ -1039,7 +1025,7 @@ int do_export(pic_ctx* c, int s, double* rows, long long cap, long long* n_out) 
     return PIC_OK;
   }
   CKR(ensure_flags(c, (size_t)n));
-  live_flag_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s).cell, (int)n, c->flags);
+  live_flag_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, c->flags);
   CKL();
   const long long tiles = (n + kScanTile - 1) / kScanTile;
   std::vector<int> dummy;
@@ -1215,7 +1201,7 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
       if (n == 0) continue;
       const AdjPart<real> A = adj_part<real>(c, R, s, R.lcur[s]);
       drift_grad_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
-          parts_at<real>(ck[0].part[s], n).cell, A.lv[2], 0, (int)n, R.acc);
+          parts_at<real>(ck[0].part[s], n), A.lv[2], 0, (int)n, R.acc);
       CKL();
     }
     CK(cudaMemcpyAsync(h, R.acc, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));

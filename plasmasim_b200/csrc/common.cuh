@@ -56,12 +56,43 @@ struct Fields {
   real* f[F_COUNT];
 };
 
+// Element t of an array whose elements lie S values of T apart.
+template <typename T, int S>
+struct Strided {
+  T* p;
+  __host__ __device__ __forceinline__ T& operator[](long long t) const { return p[t * S]; }
+};
+
 template <typename real>
 struct Parts {
-  int* cell;
-  real* o[3];
-  real* v[3];
+  // two 4-value records per particle: A = (cell, ox, oy, oz), the cell index
+  // in A's first 4 bytes, and B = (vx, vy, vz, unused); 16 bytes each in FP32,
+  // 32 in FP64, so that a particle moves with two vector copies
+  static constexpr int kCellStride = 4 * (int)sizeof(real) / (int)sizeof(int);
+  real* ra;
+  real* rb;
+  Strided<int, kCellStride> cell;  // cell[t], o[a][t], v[a][t]: one quantity of particle t
+  Strided<real, 4> o[3];
+  Strided<real, 4> v[3];
 };
+
+template <typename real>
+__host__ __device__ __forceinline__ Parts<real> make_parts(real* ra, real* rb) {
+  Parts<real> P;
+  P.ra = ra;
+  P.rb = rb;
+  P.cell.p = reinterpret_cast<int*>(ra);
+  for (int a = 0; a < 3; ++a) {
+    P.o[a].p = ra + 1 + a;
+    P.v[a].p = rb + a;
+  }
+  return P;
+}
+
+// Bytes of the records of `cap` particles (A array, then B array).
+__host__ __device__ __forceinline__ size_t parts_record_bytes(long long cap, size_t rsize) {
+  return (((size_t)cap * 4 * rsize + 255) & ~(size_t)255);
+}
 
 // Device error counters (see pic_status).
 enum ErrId {

@@ -89,6 +89,29 @@ __device__ __forceinline__ Gathered<real> gather6(const Fields<real>& F, const G
   return r;
 }
 
+// Particle s of S to slot d of D with cell index c: two vector copies.
+__device__ __forceinline__ void copy_record(const Parts<float>& S, long long s, const Parts<float>& D, long long d,
+                                            int c) {
+  float4 a = reinterpret_cast<const float4*>(S.ra)[s];
+  a.x = __int_as_float(c);
+  reinterpret_cast<float4*>(D.ra)[d] = a;
+  reinterpret_cast<float4*>(D.rb)[d] = reinterpret_cast<const float4*>(S.rb)[s];
+}
+__device__ __forceinline__ void copy_record(const Parts<double>& S, long long s, const Parts<double>& D,
+                                            long long d, int c) {
+  const double2* a = reinterpret_cast<const double2*>(S.ra + 4 * s);
+  const double2* b = reinterpret_cast<const double2*>(S.rb + 4 * s);
+  double2 a0 = a[0];
+  const double2 a1 = a[1], b0 = b[0], b1 = b[1];
+  a0.x = __hiloint2double(0, c);
+  double2* da = reinterpret_cast<double2*>(D.ra + 4 * d);
+  double2* db = reinterpret_cast<double2*>(D.rb + 4 * d);
+  da[0] = a0;
+  da[1] = a1;
+  db[0] = b0;
+  db[1] = b1;
+}
+
 // sr_particle's packets between ranks: one record per particle, in the
 // sending rank's cell indices (the receiver shifts them, :2374-2380).
 template <typename real>
@@ -570,9 +593,9 @@ static __global__ void scan_add_kernel(int* out, const int* __restrict__ add, lo
 // -------------------------------------------------------- import / export
 // Device-side compaction of live slots for export: flags -> scan -> rows.
 template <typename real>
-__global__ void live_flag_kernel(const int* __restrict__ cell, int n, int* flag) {
+__global__ void live_flag_kernel(Parts<real> P, int n, int* flag) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) flag[t] = cell[t] >= 0 ? 1 : 0;
+  if (t < n) flag[t] = P.cell[t] >= 0 ? 1 : 0;
 }
 
 template <typename real>

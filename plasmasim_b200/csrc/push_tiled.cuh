@@ -20,9 +20,8 @@ struct PushSmem {
   static constexpr int kWarps = kTileX * kTileY;
   static constexpr bool kFieldWin = sizeof(real) == 4;
   static constexpr size_t win_bytes = 4 * WN * sizeof(real);
-  static constexpr size_t pcell_off = (win_bytes + 15) & ~(size_t)15;
-  static constexpr size_t pdat_off = pcell_off + (size_t)kWarps * kStages * kLanes * sizeof(int);
-  static constexpr size_t fwin_off = pdat_off + (size_t)kWarps * kStages * 6 * kLanes * sizeof(real);
+  static constexpr size_t prec_off = (win_bytes + 15) & ~(size_t)15;  // records A, B of each slot: 8 reals
+  static constexpr size_t fwin_off = prec_off + (size_t)kWarps * kStages * kLanes * 8 * sizeof(real);
   static constexpr size_t bytes = fwin_off + (kFieldWin ? (size_t)6 * WN * sizeof(real) : 0);
 };
 
@@ -158,13 +157,39 @@ struct HomeJ<float> {
   __device__ __forceinline__ float z(int a, int b, int c) const { return c ? jz[a][b].y : jz[a][b].x; }
 };
 
-template <int BYTES>
-__device__ __forceinline__ void cp_async_n(void* smem, const void* gmem) {
+__device__ __forceinline__ void cp_async_16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  if (BYTES == 4)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(s), "l"(gmem) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(s), "l"(gmem) : "memory");
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(s), "l"(gmem) : "memory");
+}
+
+// Records A and B of particle t into 8 reals of shared memory (16-byte copies).
+template <typename real>
+__device__ __forceinline__ void fetch_records(real* dst, const Parts<real>& P, long long t) {
+  constexpr int kPieces = 4 * (int)sizeof(real) / 16;  // 16-byte pieces per record
+  const char* a = reinterpret_cast<const char*>(P.ra + 4 * t);
+  const char* b = reinterpret_cast<const char*>(P.rb + 4 * t);
+  char* d = reinterpret_cast<char*>(dst);
+#pragma unroll
+  for (int q = 0; q < kPieces; ++q) {
+    cp_async_16(d + 16 * q, a + 16 * q);
+    cp_async_16(d + 16 * (kPieces + q), b + 16 * q);
+  }
+}
+
+// Particle t's records, written with vector stores.
+__device__ __forceinline__ void store_records(const Parts<float>& P, long long t, int c, float fx, float fy,
+                                              float fz, float vx, float vy, float vz) {
+  reinterpret_cast<float4*>(P.ra)[t] = make_float4(__int_as_float(c), fx, fy, fz);
+  reinterpret_cast<float4*>(P.rb)[t] = make_float4(vx, vy, vz, 0.f);
+}
+__device__ __forceinline__ void store_records(const Parts<double>& P, long long t, int c, double fx, double fy,
+                                              double fz, double vx, double vy, double vz) {
+  double2* a = reinterpret_cast<double2*>(P.ra + 4 * t);
+  double2* b = reinterpret_cast<double2*>(P.rb + 4 * t);
+  a[0] = make_double2(__hiloint2double(0, c), fx);
+  a[1] = make_double2(fy, fz);
+  b[0] = make_double2(vx, vy);
+  b[1] = make_double2(vz, 0.0);
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -243,19 +268,9 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   acc.zero();
   // ring of particle rows fetched ahead; each lane copies and reads only its
   // own slots, so the per-thread cp.async groups need no warp barrier
-  int* pcell = reinterpret_cast<int*>(smem_raw + S::pcell_off) + warp * kStages * kLanes;
-  real* pdat = reinterpret_cast<real*>(smem_raw + S::pdat_off) + warp * kStages * 6 * kLanes;
+  real* prec = reinterpret_cast<real*>(smem_raw + S::prec_off) + warp * kStages * kLanes * 8;
   auto fetch = [&](int row) {
-    if (row < jmax) {
-      const int t = base + row * kLanes + lane;
-      const int st = row % kStages;
-      cp_async_n<4>(pcell + st * kLanes + lane, P.cell + t);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        cp_async_n<sizeof(real)>(pdat + (st * 6 + a) * kLanes + lane, P.o[a] + t);
-        cp_async_n<sizeof(real)>(pdat + (st * 6 + 3 + a) * kLanes + lane, P.v[a] + t);
-      }
-    }
+    if (row < jmax) fetch_records(prec + ((row % kStages) * kLanes + lane) * 8, P, base + row * kLanes + lane);
     cp_async_commit();
   };
 #pragma unroll
@@ -266,16 +281,16 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     cp_async_wait<kStages - 1>();
     const int t = base + jj * kLanes + lane;
     const int st = jj % kStages;
-    const int c = pcell[st * kLanes + lane];
+    const real* rec = prec + (st * kLanes + lane) * 8;
+    const int c = reinterpret_cast<const int*>(rec)[0];
     const bool act = c >= 0;
     int i = 0, j = 0, k = 0;
     real fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
     if (act) {
       ++pushed;
       unpack_cell(c, i, j, k);
-      const real* d = pdat + st * 6 * kLanes + lane;
-      fx = d[0]; fy = d[kLanes]; fz = d[2 * kLanes];
-      vx = d[3 * kLanes]; vy = d[4 * kLanes]; vz = d[5 * kLanes];
+      fx = rec[1]; fy = rec[2]; fz = rec[3];
+      vx = rec[4]; vy = rec[5]; vz = rec[6];
       bool bal = ballistic(pc, i, j, k, fx, fy, fz);
       if (!bal && !stencil_ok(g, i, j, k)) {
         count_err(err, ERR_DEPOSIT_OOB);
@@ -330,9 +345,7 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
           count_err(err, ERR_DEPOSIT_OOB);
         }
       }
-      P.cell[t] = settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
-      P.o[0][t] = fx; P.o[1][t] = fy; P.o[2][t] = fz;
-      P.v[0][t] = vx; P.v[1][t] = vy; P.v[2][t] = vz;
+      store_records(P, t, settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err), fx, fy, fz, vx, vy, vz);
     }
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);

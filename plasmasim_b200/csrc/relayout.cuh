@@ -29,12 +29,7 @@ constexpr int kAppendBlock = 64;
 
 template <typename real>
 __device__ __forceinline__ void copy_slot(const Parts<real>& S, int s, const Parts<real>& D, int d, int c) {
-  D.cell[d] = c;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    D.o[a][d] = S.o[a][s];
-    D.v[a][d] = S.v[a][s];
-  }
+  copy_record(S, s, D, d, c);
 }
 
 template <typename real>

@@ -157,9 +157,10 @@ __global__ void group_size_kernel(Geom g, TileGeom t, const int* __restrict__ st
 }
 
 // Marks the padding slots of every lane column empty.
+template <typename CellArray>
 __global__ void group_pad_kernel(Geom g, TileGeom t, const int* __restrict__ stay,
                                  const int* __restrict__ moved, const int* __restrict__ goff,
-                                 const int* __restrict__ gmax, int* cell) {
+                                 const int* __restrict__ gmax, CellArray cell) {
   const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (G >= t.ngroups) return;
@@ -172,12 +173,7 @@ __global__ void group_pad_kernel(Geom g, TileGeom t, const int* __restrict__ sta
 template <typename real>
 __device__ __forceinline__ void copy_particle(const Parts<real>& P, int s, const Parts<real>& Q, int d,
                                               int c) {
-  Q.cell[d] = c;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    Q.o[a][d] = P.o[a][s];
-    Q.v[a][d] = P.v[a][s];
-  }
+  copy_record(P, s, Q, d, c);
 }
 
 // Scatter over the tiled slots: a stayer keeps its place in its column order;
