@@ -61,6 +61,7 @@ struct pic_ctx {
   int* total_dev = nullptr;
   int* append_dev = nullptr;          // end of the append region during a re-layout
   int* holes = nullptr;               // per-slot scratch: hole rows of every lane column
+  int* rank = nullptr;                // per-slot scratch: placement rank of every appended particle
   int* cnt = nullptr;
   int* offs = nullptr;
   int* cursor = nullptr;
@@ -730,9 +731,11 @@ int do_relayout_species(pic_ctx* c, int s) {
   CKL();
   const long long first = c->tiled_end[s];
   const Parts<real> Q = parts<real>(c, s, 1 - st.cur);
-  place_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
-      P, (int)first, st.count_dev, c->g, tg, c->goff[s][c->lay[s]], c->holes, nholes, c->cursor, Q,
-      c->total_dev);
+  place_rank_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
+      P, (int)first, st.count_dev, c->g, nholes, c->cursor, c->total_dev, c->rank);
+  CKL();
+  place_move_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
+      P, (int)first, st.count_dev, c->g, tg, c->goff[s][c->lay[s]], c->holes, c->rank, Q);
   CKL();
   unspill_kernel<real><<<particle_blocks(st.cap), kThreads, 0, c->stream>>>(Q, c->total_dev, P, (int)first);
   CKL();
@@ -1378,6 +1381,7 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
     if (cudaMalloc(&c->total_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->append_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->holes, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    if (cudaMalloc(&c->rank, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaFuncSetAttribute(push_tiled_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)PushSmem<double>::bytes) != cudaSuccess ||
         cudaFuncSetAttribute(push_tiled_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1419,6 +1423,7 @@ int pic_destroy(pic_ctx* c) {
   cudaFree(c->total_dev);
   cudaFree(c->append_dev);
   cudaFree(c->holes);
+  cudaFree(c->rank);
   cudaFree(c->cnt);
   cudaFree(c->offs);
   cudaFree(c->cursor);

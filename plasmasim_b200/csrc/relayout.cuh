@@ -110,94 +110,57 @@ __global__ void clamp_count_kernel(const int* append_at, int cap, int* count_dev
   *count_dev = min(*append_at, cap);
 }
 
-// Each appended particle takes the next hole of its cell's column; the rest
-// go, compacted, to the spare buffer Q. A warp takes U rows of 32 appended
-// slots at a time and issues their loads, cursor atomics and hole lookups
-// together, so that the chain of dependent memory accesses of one particle
-// overlaps those of the others.
+// Placement: each appended particle takes the next hole of its cell's column;
+// the rest go, compacted, to the spare buffer Q. Two streaming passes, each
+// with one kind of scattered access, so that many of them are in flight at
+// once (one kernel doing the whole chain -- cell, cursor atomic, hole lookup,
+// record copy -- per particle ran at 8 % issue).
+// Pass 1: the particle's rank among the appended particles of its new cell,
+// or, when its column has no hole left, -2 - (its index in the spare buffer
+// Q); -1 for an empty slot or a particle outside the interior (dropped).
 template <typename real>
-__global__ void place_kernel(Parts<real> P, int first, const int* __restrict__ count, Geom g, TileGeom t,
-                             const int* __restrict__ goff, const int* __restrict__ holes,
-                             const int* __restrict__ nholes, int* cursor, Parts<real> Q, int* nspill) {
-  constexpr int U = 4;
-  const int n = *count;
-  const int span = n - first;
+__global__ void __launch_bounds__(256) place_rank_kernel(Parts<real> P, int first, const int* __restrict__ count,
+                                                         Geom g, const int* __restrict__ nholes, int* cursor,
+                                                         int* nspill, int* rank) {
+  const int span = *count - first;
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int w0 = warp * (U * kLanes); w0 < span; w0 += nwarps * (U * kLanes)) {  // warp-uniform
-    int s[U], c[U], key[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int q = w0 + u * kLanes + lane;
-      s[u] = first + q;
-      c[u] = q < span ? P.cell[s[u]] : -1;
-    }
-    real o[U][3], v[U][3];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      key[u] = interior_key(g, c[u]);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        o[u][a] = key[u] >= 0 ? P.o[a][s[u]] : (real)0;
-        v[u][a] = key[u] >= 0 ? P.v[a][s[u]] : (real)0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int w0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; w0 < span; w0 += stride) {  // warp-uniform
+    const int q = w0 + lane;
+    const int key = q < span ? interior_key(g, P.cell[first + q]) : -1;
+    const int r = warp_aggregated_inc(cursor, key < 0 ? 0 : key, key >= 0);
+    const bool spill = key >= 0 && r >= nholes[key];
+    const unsigned ms = __ballot_sync(0xffffffffu, spill);
+    int sb = 0;
+    if (lane == 0 && ms) sb = atomicAdd(nspill, __popc(ms));
+    sb = __shfl_sync(0xffffffffu, sb, 0);
+    if (q < span) rank[q] = key < 0 ? -1 : (spill ? -2 - (sb + __popc(ms & below)) : r);
+  }
+}
+
+// Pass 2: each appended particle to its hole (or to Q), its slot emptied.
+template <typename real>
+__global__ void __launch_bounds__(256) place_move_kernel(Parts<real> P, int first, const int* __restrict__ count,
+                                                         Geom g, TileGeom t, const int* __restrict__ goff,
+                                                         const int* __restrict__ holes, const int* __restrict__ rank,
+                                                         Parts<real> Q) {
+  const int span = *count - first;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < span; q += gridDim.x * blockDim.x) {
+    const int s = first + q;
+    const int r = rank[q];
+    if (r != -1) {
+      const int c = P.cell[s];
+      if (r >= 0) {
+        int l2;
+        const int G = group_of_key(g, t, interior_key(g, c), l2);
+        const int gb = goff[G];
+        copy_record(P, s, P, gb + holes[gb + r * kLanes + l2] * kLanes + l2, c);
+      } else {
+        copy_record(P, s, Q, -2 - r, c);
       }
     }
-    // per slot: holes of the destination cell and its column's first slot
-    int nh[U], gb[U], l2[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      nh[u] = 0;
-      gb[u] = 0;
-      l2[u] = 0;
-      if (key[u] >= 0) {
-        nh[u] = nholes[key[u]];
-        gb[u] = goff[group_of_key(g, t, key[u], l2[u])];
-      }
-    }
-    // warp-aggregated cursor increments: one atomic per distinct key and row
-    unsigned peers[U];
-    int old[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      peers[u] = __match_any_sync(0xffffffffu, key[u] >= 0 ? key[u] : -1 - lane);
-      old[u] = 0;
-      if (key[u] >= 0 && lane == __ffs(peers[u]) - 1) old[u] = atomicAdd(cursor + key[u], __popc(peers[u]));
-    }
-    int rank[U], sb[U];
-    unsigned ms[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      rank[u] = __shfl_sync(0xffffffffu, old[u], __ffs(peers[u]) - 1) + __popc(peers[u] & below);
-      const bool spill = key[u] >= 0 && rank[u] >= nh[u];
-      ms[u] = __ballot_sync(0xffffffffu, spill);
-      sb[u] = 0;
-      if (lane == 0 && ms[u]) sb[u] = atomicAdd(nspill, __popc(ms[u]));
-    }
-    int hrow[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      sb[u] = __shfl_sync(0xffffffffu, sb[u], 0);
-      const bool spill = (ms[u] >> lane) & 1u;
-      hrow[u] = (key[u] >= 0 && !spill) ? holes[gb[u] + rank[u] * kLanes + l2[u]] : 0;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (w0 + u * kLanes + lane >= span) continue;
-      if (key[u] >= 0) {
-        const bool spill = (ms[u] >> lane) & 1u;
-        const Parts<real>& D = spill ? Q : P;
-        const int d = spill ? sb[u] + __popc(ms[u] & below) : gb[u] + hrow[u] * kLanes + l2[u];
-        D.cell[d] = c[u];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          D.o[a][d] = o[u][a];
-          D.v[a][d] = v[u][a];
-        }
-      }
-      P.cell[s[u]] = -1;  // empty slot, outside the interior (dropped), or moved
-    }
+    P.cell[s] = -1;
   }
 }
 
