@@ -82,7 +82,9 @@ typedef struct pic_config {
   int procs_x, procs_y;    /* PROCESS_Nx, PROCESS_Ny (:100-101): the x-y decomposition, 1 x 1 by default;
                               nx, ny are then the cells of one rank (Grid_Nx, Grid_Ny) */
   int rank_x, rank_y;      /* myrank_x, myrank_y (:205-206) of this context */
-  int reserved1;
+  int plain_fields;        /* 0: renew_b4_2 / renew_e4_2 with TMA-staged stencil operands wherever the
+                              row pitch (nz + 4 values) is a multiple of 16 bytes; 1: the per-node
+                              kernels everywhere (same arithmetic, for comparison) */
 } pic_config;
 
 typedef struct pic_ctx pic_ctx;
@@ -255,9 +257,15 @@ int pic_rng_counters(pic_ctx *ctx, long long *ctr_p, long long *ctr_v, int set);
 /* Device counters: errors [0] deposits or gathers skipped because the stencil
  * left the array, [1] particles dropped with a cell outside the index range,
  * [2] non-finite velocities after a push; work [3] particle pushes made by
- * the push kernels since creation; [4..7] reserved. Returns PIC_ERR_DEVICE
- * when any error counter is non-zero. */
+ * the push kernels since creation; errors [4] sr_particle packets lost to a
+ * full exchange list, [5] field tiles whose TMA-staged operands did not arrive
+ * within the wait limit (the tile is left unchanged); [6..7] reserved.
+ * Returns PIC_ERR_DEVICE when any error counter is non-zero. */
 int pic_status(pic_ctx *ctx, long long *counters8);
+/* *staged = 1 when renew_b4_2 / renew_e4_2 run the TMA-staged stencil kernels,
+ * 0 when they run the per-node kernels (pic_config.plain_fields, or a row
+ * pitch that is not a multiple of 16 bytes). */
+int pic_field_path(pic_ctx *ctx, int *staged);
 int pic_synchronize(pic_ctx *ctx);
 /* The context's cudaStream_t, for callers that time or order work around it. */
 int pic_get_stream(pic_ctx *ctx, void **stream);

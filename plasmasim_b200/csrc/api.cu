@@ -9,10 +9,13 @@
 #include <new>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "../../include/plasma_b200.h"
 #include "common.cuh"
 #include "diag.cuh"
 #include "fields.cuh"
+#include "fields_tma.cuh"
 #include "particles.cuh"
 #include "tiled.cuh"
 #include "push_tiled.cuh"
@@ -47,6 +50,10 @@ struct pic_ctx {
   void* field_mem = nullptr;
   size_t plane_bytes = 0;
   double* ramps = nullptr;  // rx[2gx], ry[2gy], rz[2gz]
+  // tensor maps of the staged field kernels: E (the B half-step's curl
+  // operands) and DB (the E step's), each plane with its own box
+  CUtensorMap tm_e[3], tm_db[3];
+  bool staged = false;
   Store sp[2];
   // sort and scan scratch
   TileGeom tg{};
@@ -225,6 +232,63 @@ int phase_mark(pic_ctx* c, int ph) {
   }
   CK(cudaEventRecord(p.ev[p.used++], c->stream));
   return PIC_OK;
+}
+
+// Tile shape of the staged field kernels: 4 x 8 x 32 nodes in FP32 (25.6 KB
+// of staged planes), 4 x 4 x 32 in FP64 (30.7 KB).
+template <typename real> struct StShape;
+template <> struct StShape<float> { static constexpr int TX = 4, TY = 8; };
+template <> struct StShape<double> { static constexpr int TX = 4, TY = 4; };
+
+template <typename real>
+using StTile = StencilTile<real, StShape<real>::TX, StShape<real>::TY>;
+
+// Tensor maps of planes first, first + 1, first + 2 over the whole padded
+// array (z fastest), each with its plane's box of StencilTile.
+template <typename real>
+bool make_stencil_maps(const pic_ctx* c, PFN_cuTensorMapEncodeTiled_v12000 encode, int first, CUtensorMap* out) {
+  using T = StTile<real>;
+  const cuuint32_t ex[3] = {T::EX0, T::EX1, T::EX2}, ey[3] = {T::EY0, T::EY1, T::EY2};
+  const cuuint64_t dims[3] = {(cuuint64_t)c->g.gz, (cuuint64_t)c->g.gy, (cuuint64_t)c->g.gx};
+  const cuuint64_t strides[2] = {(cuuint64_t)c->g.gz * sizeof(real), (cuuint64_t)c->g.sx * sizeof(real)};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  for (int q = 0; q < 3; ++q) {
+    const cuuint32_t box[3] = {(cuuint32_t)kStBoxZ, ey[q], ex[q]};
+    void* base = (char*)c->field_mem + (size_t)(first + q) * c->plane_bytes;
+    if (encode(&out[q], sizeof(real) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+               base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  return true;
+}
+
+// Chooses the staged field kernels when the row pitch (gz values) is a
+// multiple of 16 bytes and the driver encodes the tensor maps; the per-node
+// kernels otherwise, or when the configuration asks for them.
+template <typename real>
+void setup_staged_fields(pic_ctx* c) {
+  using T = StTile<real>;
+  c->staged = false;
+  if (c->cfg.plain_fields || ((size_t)c->g.gz * sizeof(real)) % 16 != 0) return;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q{};
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
+      q != cudaDriverEntryPointSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  const auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  if (!make_stencil_maps<real>(c, encode, F_EX, c->tm_e) || !make_stencil_maps<real>(c, encode, F_DBX, c->tm_db))
+    return;
+  if (cudaFuncSetAttribute(renew_b_tma_kernel<real, StShape<real>::TX, StShape<real>::TY>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(renew_e_tma_kernel<real, StShape<real>::TX, StShape<real>::TY>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  c->staged = true;
 }
 
 Ramps ramps(const pic_ctx* c) {
@@ -434,8 +498,15 @@ int wrap_planes(pic_ctx* c, const int* ids, int n) {
 template <typename real>
 int do_renew_b(pic_ctx* c) {
   BParams p{1. / c->cfg.e0 * c->cfg.dt * 0.5 * 0.5, 0.5 * c->cfg.dt, 1.0 / (24.0 * c->cfg.dx)};
-  const long long nint = (long long)c->g.nx * c->g.ny * c->g.nz;
-  renew_b_kernel<real><<<grid_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, ramps(c), p);
+  if (c->staged) {
+    constexpr int TX = StShape<real>::TX, TY = StShape<real>::TY;
+    const int ty = (c->g.ny + TY - 1) / TY, tz = (c->g.nz + kStZ - 1) / kStZ, tx = (c->g.nx + TX - 1) / TX;
+    renew_b_tma_kernel<real, TX, TY><<<tx * ty * tz, kStThreads, StTile<real>::bytes, c->stream>>>(
+        c->tm_e[0], c->tm_e[1], c->tm_e[2], fields<real>(c), c->g, ramps(c), p, ty, tz, c->err);
+  } else {
+    const long long nint = (long long)c->g.nx * c->g.ny * c->g.nz;
+    renew_b_kernel<real><<<grid_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, ramps(c), p);
+  }
   CKL();
   if (c->has_xport) {
     Fields<real> F = fields<real>(c);
@@ -459,8 +530,15 @@ int do_renew_b(pic_ctx* c) {
 template <typename real>
 int do_renew_e(pic_ctx* c) {
   EParams p{c->cfg.c * c->cfg.c * c->cfg.dt, c->cfg.mu0, 1.0 / (24.0 * c->cfg.dx)};
-  const long long nint = (long long)c->g.nx * c->g.ny * c->g.nz;
-  renew_e_kernel<real><<<grid_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, ramps(c), p);
+  if (c->staged) {
+    constexpr int TX = StShape<real>::TX, TY = StShape<real>::TY;
+    const int ty = (c->g.ny + TY - 1) / TY, tz = (c->g.nz + kStZ - 1) / kStZ, tx = (c->g.nx + TX - 1) / TX;
+    renew_e_tma_kernel<real, TX, TY><<<tx * ty * tz, kStThreads, StTile<real>::bytes, c->stream>>>(
+        c->tm_db[0], c->tm_db[1], c->tm_db[2], fields<real>(c), c->g, ramps(c), p, ty, tz, c->err);
+  } else {
+    const long long nint = (long long)c->g.nx * c->g.ny * c->g.nz;
+    renew_e_kernel<real><<<grid_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, ramps(c), p);
+  }
   CKL();
   static const int ids[3] = {F_EX, F_EY, F_EZ};
   return wrap_planes<real>(c, ids, 3);
@@ -1344,6 +1422,8 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
     if (cudaMemcpy(c->ramps, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(PIC_ERR_CUDA);
   }
+  if (c->prec == 64) setup_staged_fields<double>(c);
+  else setup_staged_fields<float>(c);
   long long cap = k.capacity;
   if (cap <= 0) {
     // the tiled layout gives every lane column room for its fullest cell plus
@@ -1652,6 +1732,13 @@ int pic_rng_counters(pic_ctx* c, long long* ctr_p, long long* ctr_v, int set) {
   return PIC_OK;
 }
 
+int pic_field_path(pic_ctx* c, int* staged) {
+  CKR(check_ctx(c));
+  if (!staged) return PIC_ERR_ARG;
+  *staged = c->staged ? 1 : 0;
+  return PIC_OK;
+}
+
 int pic_status(pic_ctx* c, long long* counters8) {
   CKR(check_ctx(c));
   unsigned long long h[ERR_COUNT];
@@ -1660,7 +1747,7 @@ int pic_status(pic_ctx* c, long long* counters8) {
   int any = 0;
   for (int q = 0; q < ERR_COUNT; ++q) {
     if (counters8) counters8[q] = (long long)h[q];
-    if (q < ERR_FIRST_INFO || q == ERR_MIGRATION) any |= h[q] != 0;
+    if (q < ERR_FIRST_INFO || q == ERR_MIGRATION || q == ERR_FIELD_WAIT) any |= h[q] != 0;
   }
   return any ? PIC_ERR_DEVICE : PIC_OK;
 }

@@ -99,6 +99,7 @@ enum ErrId {
   ERR_DEPOSIT_OOB = 0, ERR_CELL_RANGE = 1, ERR_NONFINITE = 2,
   ERR_FIRST_INFO = 3, CNT_PUSHED = 3,  // slots from here on count work, not errors
   ERR_MIGRATION = 4,  // sr_particle packets lost to a full exchange buffer (an error)
+  ERR_FIELD_WAIT = 5,  // staged field tiles whose tensor loads did not arrive in time (an error)
   ERR_COUNT = 8
 };
 

@@ -81,6 +81,23 @@ struct EParams {
   double inv24dx;
 };
 
+// Damping coefficients of renew_b4_2 at sigma s: ca = (1 - s t)/(1 + s t),
+// cb = (dt/2)/(1 + s t); s = 0 gives exactly (1, dt/2) without the divisions.
+__device__ __forceinline__ void b_coeffs(double s, const BParams& p, double& ca, double& cb) {
+  if (s == 0.0) { ca = 1.0; cb = p.dth; return; }
+  ca = (1. - s * p.temp) / (1. + s * p.temp);
+  cb = p.dth / (1. + s * p.temp);
+}
+
+// Damping coefficients of renew_e4_2 at sigma s: with h = mu0 s t / 2,
+// ca = (1 - h)/(1 + h), cb = t/(1 + h); s = 0 gives exactly (1, t).
+__device__ __forceinline__ void e_coeffs(double s, const EParams& p, double& ca, double& cb) {
+  if (s == 0.0) { ca = 1.0; cb = p.temp; return; }
+  const double h = 0.5 * p.mu0 * s * p.temp;
+  ca = (1. - h) / (1. + h);
+  cb = p.temp / (1. + h);
+}
+
 // renew_b4_2 (:2580-2611) on the induced field: DB <- ca DB - cb curl4(E),
 // B = B0 + DB, with ca = (1 - s t)/(1 + s t), cb = (dt/2)/(1 + s t).
 template <typename real>
@@ -98,31 +115,31 @@ __global__ void __launch_bounds__(256) renew_b_kernel(Fields<real> F, Geom g, Ra
   // x component at (k+1/2, l, m): sigma[2k+1][2l][2m]
   {
     const double s = sigma_of(rp.a, rp.rx[2 * k + 1], rp.ry[2 * l], rp.rz[2 * m]);
-    const real ca = (real)((1. - s * p.temp) / (1. + s * p.temp));
-    const real cb = (real)(p.dth / (1. + s * p.temp));
+    double ca, cb;
+    b_coeffs(s, p, ca, cb);
     const real curl = ((real)27 * (ez[n] - ez[n - sy] - ey[n] + ey[n - 1]) -
                        (ez[n + sy] - ez[n - 2 * sy] - ey[n + 1] + ey[n - 2])) * c24;
-    const real db = ca * F.f[F_DBX][n] - cb * curl;
+    const real db = (real)ca * F.f[F_DBX][n] - (real)cb * curl;
     F.f[F_DBX][n] = db;
     F.f[F_BX][n] = F.f[F_B0X][n] + db;
   }
   {
     const double s = sigma_of(rp.a, rp.rx[2 * k], rp.ry[2 * l + 1], rp.rz[2 * m]);
-    const real ca = (real)((1. - s * p.temp) / (1. + s * p.temp));
-    const real cb = (real)(p.dth / (1. + s * p.temp));
+    double ca, cb;
+    b_coeffs(s, p, ca, cb);
     const real curl = ((real)27 * (ex[n] - ex[n - 1] - ez[n] + ez[n - sx]) -
                        (ex[n + 1] - ex[n - 2] - ez[n + sx] + ez[n - 2 * sx])) * c24;
-    const real db = ca * F.f[F_DBY][n] - cb * curl;
+    const real db = (real)ca * F.f[F_DBY][n] - (real)cb * curl;
     F.f[F_DBY][n] = db;
     F.f[F_BY][n] = F.f[F_B0Y][n] + db;
   }
   {
     const double s = sigma_of(rp.a, rp.rx[2 * k], rp.ry[2 * l], rp.rz[2 * m + 1]);
-    const real ca = (real)((1. - s * p.temp) / (1. + s * p.temp));
-    const real cb = (real)(p.dth / (1. + s * p.temp));
+    double ca, cb;
+    b_coeffs(s, p, ca, cb);
     const real curl = ((real)27 * (ey[n] - ey[n - sx] - ex[n] + ex[n - sy]) -
                        (ey[n + sx] - ey[n - 2 * sx] - ex[n + sy] + ex[n - 2 * sy])) * c24;
-    const real db = ca * F.f[F_DBZ][n] - cb * curl;
+    const real db = (real)ca * F.f[F_DBZ][n] - (real)cb * curl;
     F.f[F_DBZ][n] = db;
     F.f[F_BZ][n] = F.f[F_B0Z][n] + db;
   }
@@ -145,27 +162,27 @@ __global__ void __launch_bounds__(256) renew_e_kernel(Fields<real> F, Geom g, Ra
   const real mu0 = (real)p.mu0;
   {
     const double s = sigma_of(rp.a, rp.rx[2 * k], rp.ry[2 * l + 1], rp.rz[2 * m + 1]);
-    const double h = 0.5 * p.mu0 * s * p.temp;
-    const real ca = (real)((1. - h) / (1. + h)), cb = (real)(p.temp / (1. + h));
+    double ca, cb;
+    e_coeffs(s, p, ca, cb);
     const real curl = ((real)27 * ((bz[n + sy] - bz[n]) - (by[n + 1] - by[n])) -
                        ((bz[n + 2 * sy] - bz[n - sy]) - (by[n + 2] - by[n - 1]))) * c24;
-    F.f[F_EX][n] = ca * F.f[F_EX][n] + cb * (curl - mu0 * (F.f[F_JIX][n] - F.f[F_JEX][n]));
+    F.f[F_EX][n] = (real)ca * F.f[F_EX][n] + (real)cb * (curl - mu0 * (F.f[F_JIX][n] - F.f[F_JEX][n]));
   }
   {
     const double s = sigma_of(rp.a, rp.rx[2 * k + 1], rp.ry[2 * l], rp.rz[2 * m + 1]);
-    const double h = 0.5 * p.mu0 * s * p.temp;
-    const real ca = (real)((1. - h) / (1. + h)), cb = (real)(p.temp / (1. + h));
+    double ca, cb;
+    e_coeffs(s, p, ca, cb);
     const real curl = ((real)27 * ((bx[n + 1] - bx[n]) - (bz[n + sx] - bz[n])) -
                        ((bx[n + 2] - bx[n - 1]) - (bz[n + 2 * sx] - bz[n - sx]))) * c24;
-    F.f[F_EY][n] = ca * F.f[F_EY][n] + cb * (curl - mu0 * (F.f[F_JIY][n] - F.f[F_JEY][n]));
+    F.f[F_EY][n] = (real)ca * F.f[F_EY][n] + (real)cb * (curl - mu0 * (F.f[F_JIY][n] - F.f[F_JEY][n]));
   }
   {
     const double s = sigma_of(rp.a, rp.rx[2 * k + 1], rp.ry[2 * l + 1], rp.rz[2 * m]);
-    const double h = 0.5 * p.mu0 * s * p.temp;
-    const real ca = (real)((1. - h) / (1. + h)), cb = (real)(p.temp / (1. + h));
+    double ca, cb;
+    e_coeffs(s, p, ca, cb);
     const real curl = ((real)27 * ((by[n + sx] - by[n]) - (bx[n + sy] - bx[n])) -
                        ((by[n + 2 * sx] - by[n - sx]) - (bx[n + 2 * sy] - bx[n - sy]))) * c24;
-    F.f[F_EZ][n] = ca * F.f[F_EZ][n] + cb * (curl - mu0 * (F.f[F_JIZ][n] - F.f[F_JEZ][n]));
+    F.f[F_EZ][n] = (real)ca * F.f[F_EZ][n] + (real)cb * (curl - mu0 * (F.f[F_JIZ][n] - F.f[F_JEZ][n]));
   }
 }
 

@@ -51,7 +51,7 @@ class _CConfig(C.Structure):
         ("diag_every_step", C.c_int), ("poisson_clean", C.c_int),
         ("capacity", C.c_longlong), ("seed_p", C.c_ulonglong), ("seed_v", C.c_ulonglong),
         ("absorb_grid3", C.c_int), ("procs_x", C.c_int), ("procs_y", C.c_int),
-        ("rank_x", C.c_int), ("rank_y", C.c_int), ("reserved1", C.c_int),
+        ("rank_x", C.c_int), ("rank_y", C.c_int), ("plain_fields", C.c_int),
     ]
 
 
@@ -99,6 +99,7 @@ class PicConfig:
     procs_y: int = 1
     rank_x: int = 0
     rank_y: int = 0
+    plain_fields: int = 0
 
     @classmethod
     def normalized(cls, nx, ny, nz, np_, **kw) -> "PicConfig":
@@ -137,7 +138,7 @@ EXPORTED = [
     "pic_drift_deposit_n", "pic_reduce_current", "pic_sr_particle", "pic_add_flat", "pic_sort",
     "pic_thrust_f", "pic_thrust_fave", "pic_gauss_residual", "pic_step", "pic_fdtd",
     "pic_set_particles", "pic_get_particles", "pic_particle_count", "pic_get_grid",
-    "pic_set_grid", "pic_rng_counters", "pic_status", "pic_synchronize", "pic_get_stream",
+    "pic_set_grid", "pic_rng_counters", "pic_status", "pic_field_path", "pic_synchronize", "pic_get_stream",
     "pic_error_string", "pic_set_timing", "pic_read_timing", "pic_gauss_residual_noalloc",
     "pic_objective", "pic_adjoint", "pic_save_checkpoint", "pic_load_checkpoint", "pic_write_output",
     "pic_append_thrust", "pic_append_thrust_ave", "pic_poisson_clean",
@@ -198,6 +199,7 @@ def load_library(path: str = LIB_PATH):
     L.pic_set_grid.argtypes = [vp, _dp]
     L.pic_rng_counters.argtypes = [vp, _llp, _llp, C.c_int]
     L.pic_status.argtypes = [vp, _llp]
+    L.pic_field_path.argtypes = [vp, C.POINTER(C.c_int)]
     L.pic_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.pic_set_timing.argtypes = [vp, C.c_int]
     L.pic_read_timing.argtypes = [vp, _dp, _llp, _llp]
@@ -398,6 +400,12 @@ class Pic3D:
         out = np.zeros(8, dtype=np.int64)
         rc = self.L.pic_status(self.h, _ptr(out, _llp))
         return rc, out
+
+    def staged_fields(self) -> bool:
+        """True when renew_b4_2 / renew_e4_2 run the TMA-staged stencil kernels."""
+        v = C.c_int()
+        self._call("pic_field_path", C.byref(v))
+        return bool(v.value)
 
     def synchronize(self):
         self._call("pic_synchronize")
