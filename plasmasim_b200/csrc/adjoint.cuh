@@ -79,19 +79,80 @@ struct AdjConst {
 // atomics do not depend on the order of the particles): each term
 // v_q W / c is scaled by 2^40, which leaves 23 bits of headroom for the
 // number of particles per node; jconvert_kernel turns the sums into
-// J = q n c (sum / 2^40).
+// J = q n c (sum / 2^40). The warp-aggregated scatter below keeps this: its
+// group sums are exact.
 constexpr double kJFixed = 1099511627776.0;  // 2^40
 
+// ------------------------------------------------------------ warp-aggregated scatters
+// Slots keep the order of the initial load and of each refill, which is cell
+// order, so the lanes of a warp mostly share a few stencil bases. Lanes with
+// the same base (found with match.any) sum their eight terms first and the
+// group's first lane issues the atomics. `key` is the base node, or -1 for a
+// lane that adds nothing. Every lane of the warp calls these together.
+
+constexpr unsigned kFullWarp = 0xffffffffu;
+
+// Sums w over each group of lanes (grp: this lane's group) by pointer jumping
+// along the group's lanes: after step s a lane holds the sum of 2^s members
+// from itself on, so the group's first lane has the total after
+// ceil(log2(largest group)) steps of nine shuffles.
+template <typename T>
+__device__ __forceinline__ void group_sum8(T (&w)[8], unsigned grp) {
+  const int lane = threadIdx.x & 31;
+  int nxt = __ffs(grp & ~((2u << lane) - 1u)) - 1;  // the group's next lane above this one
+  const int m = __popc(grp);
+  const int steps = (int)__reduce_max_sync(kFullWarp, m > 1 ? 32u - (unsigned)__clz(m - 1) : 0u);
+  for (int it = 0; it < steps; ++it) {
+    const int src = nxt < 0 ? lane : nxt;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const T u = __shfl_sync(kFullWarp, w[q], src);
+      if (nxt >= 0) w[q] += u;
+    }
+    const int nn = __shfl_sync(kFullWarp, nxt, src);
+    nxt = nxt < 0 ? -1 : nn;
+  }
+}
+
+// Fixed-point terms: integer group sums are exact and independent of the
+// order of the terms, so the planes receive the same totals, modulo 2^64, as
+// from one atomic per lane.
+__device__ __forceinline__ void scatter8_fixed_agg(unsigned long long* F, int key, int sx, int sy,
+                                                   unsigned long long (&w)[8]) {
+  const unsigned grp = __match_any_sync(kFullWarp, key);
+  group_sum8(w, grp);
+  if (key >= 0 && (int)(threadIdx.x & 31) == __ffs(grp) - 1) {
+    const int o[8] = {0, 1, sy, sy + 1, sx, sx + 1, sx + sy, sx + sy + 1};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) atomicAdd(F + key + o[q], w[q]);
+  }
+}
+
+// The fixed-point terms of one trilinear scatter of v.
 template <typename real>
-__device__ __forceinline__ void scatter8_fixed(unsigned long long* F, int n, int sx, int sy, real v,
-                                               real x0, real x1, real y0, real y1, real z0, real z1) {
+__device__ __forceinline__ void fixed_terms(real v, real x0, real x1, real y0, real y1, real z0, real z1,
+                                            unsigned long long (&w)[8]) {
   const real a0 = v * x0, a1 = v * x1;
   const real a00 = a0 * y0, a01 = a0 * y1, a10 = a1 * y0, a11 = a1 * y1;
-  const real w[8] = {a00 * z0, a00 * z1, a01 * z0, a01 * z1, a10 * z0, a10 * z1, a11 * z0, a11 * z1};
-  const int o[8] = {0, 1, sy, sy + 1, sx, sx + 1, sx + sy, sx + sy + 1};
+  const real t[8] = {a00 * z0, a00 * z1, a01 * z0, a01 * z1, a10 * z0, a10 * z1, a11 * z0, a11 * z1};
 #pragma unroll
-  for (int q = 0; q < 8; ++q)
-    atomicAdd(F + n + o[q], (unsigned long long)__double2ll_rn((double)w[q]));
+  for (int q = 0; q < 8; ++q) w[q] = (unsigned long long)__double2ll_rn((double)t[q]);
+}
+
+// Floating-point terms: one atomic per group and node.
+template <typename real>
+__device__ __forceinline__ void scatter8_agg(real* F, int key, int sx, int sy, real v, real x0, real x1, real y0,
+                                             real y1, real z0, real z1) {
+  const unsigned grp = __match_any_sync(kFullWarp, key);
+  const real a0 = v * x0, a1 = v * x1;
+  const real a00 = a0 * y0, a01 = a0 * y1, a10 = a1 * y0, a11 = a1 * y1;
+  real w[8] = {a00 * z0, a00 * z1, a01 * z0, a01 * z1, a10 * z0, a10 * z1, a11 * z0, a11 * z1};
+  group_sum8(w, grp);
+  if (key >= 0 && (int)(threadIdx.x & 31) == __ffs(grp) - 1) {
+    const int o[8] = {0, 1, sy, sy + 1, sx, sx + 1, sx + sy, sx + sy + 1};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) atomicAdd(F + key + o[q], w[q]);
+  }
 }
 
 // push_kernel<real, PUSH_FUSED> with the J deposit into fixed-point planes
@@ -103,51 +164,65 @@ __global__ void __launch_bounds__(256) push_fixed_kernel(Parts<real> P, int n, F
                                                          real vscale, unsigned long long* err) {
   unsigned pushed = 0;
   const int sx = g.sx, sy = g.gz;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int c = P.cell[t];
-    if (c < 0) continue;
-    ++pushed;
-    int i, j, k;
-    unpack_cell(c, i, j, k);
-    real fx = P.o[0][t], fy = P.o[1][t], fz = P.o[2][t];
-    real vx = P.v[0][t], vy = P.v[1][t], vz = P.v[2][t];
-    bool bal = ballistic(pc, i, j, k, fx, fy, fz);
-    if (!bal && !stencil_ok(g, i, j, k)) {
-      count_err(err, ERR_DEPOSIT_OOB);
-      bal = true;
-    }
-    if (!bal) {
-      const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-      boris4(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
-      if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) count_err(err, ERR_NONFINITE);
-    }
-    advance(i, fx, vx * pc.hdt);
-    advance(j, fy, vy * pc.hdt);
-    advance(k, fz, vz * pc.hdt);
-    if (in_array(g, i, j, k)) {
-      if (stencil_ok(g, i, j, k)) {
-        const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-        scatter8_fixed(J64x, X.a * sx + Y.b * sy + Z.b, sx, sy, vx * vscale, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
-        scatter8_fixed(J64y, X.b * sx + Y.a * sy + Z.b, sx, sy, vy * vscale, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
-        scatter8_fixed(J64z, X.b * sx + Y.b * sy + Z.a, sx, sy, vz * vscale, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
-      } else {
+  const int lane = threadIdx.x & 31;
+  // warp-uniform trip count: the J deposit is aggregated across the warp
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += gridDim.x * blockDim.x) {
+    const int t = base + lane;
+    Rec<real> r{};
+    r.cell = -1;
+    if (t < n) r = load_records(P, t);
+    const bool live = r.cell >= 0;
+    int i = 0, j = 0, k = 0;
+    real fx = r.o[0], fy = r.o[1], fz = r.o[2];
+    real vx = r.v[0], vy = r.v[1], vz = r.v[2];
+    bool dep = false;
+    Axis<real> X{}, Y{}, Z{};
+    if (live) {
+      ++pushed;
+      unpack_cell(r.cell, i, j, k);
+      bool bal = ballistic(pc, i, j, k, fx, fy, fz);
+      if (!bal && !stencil_ok(g, i, j, k)) {
         count_err(err, ERR_DEPOSIT_OOB);
+        bal = true;
+      }
+      if (!bal) {
+        const Axis<real> X0 = axis_weights(i, fx), Y0 = axis_weights(j, fy), Z0 = axis_weights(k, fz);
+        boris4(pc, gather6(F, g, X0, Y0, Z0), vx, vy, vz);
+        if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) count_err(err, ERR_NONFINITE);
+      }
+      advance(i, fx, vx * pc.hdt);
+      advance(j, fy, vy * pc.hdt);
+      advance(k, fz, vz * pc.hdt);
+      if (in_array(g, i, j, k)) {
+        if (stencil_ok(g, i, j, k)) {
+          dep = true;
+          X = axis_weights(i, fx); Y = axis_weights(j, fy); Z = axis_weights(k, fz);
+        } else {
+          count_err(err, ERR_DEPOSIT_OOB);
+        }
       }
     }
-    advance(i, fx, vx * pc.hdt);
-    advance(j, fy, vy * pc.hdt);
-    advance(k, fz, vz * pc.hdt);
-    if (in_array(g, i, j, k)) {
-      if (stencil_ok(g, i, j, k)) {
-        const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-        deposit_n(F, g, pc, X, Y, Z);
-      } else {
-        count_err(err, ERR_DEPOSIT_OOB);
+    unsigned long long w[8];
+    fixed_terms(dep ? vx * vscale : (real)0, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1, w);
+    scatter8_fixed_agg(J64x, dep ? X.a * sx + Y.b * sy + Z.b : -1, sx, sy, w);
+    fixed_terms(dep ? vy * vscale : (real)0, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1, w);
+    scatter8_fixed_agg(J64y, dep ? X.b * sx + Y.a * sy + Z.b : -1, sx, sy, w);
+    fixed_terms(dep ? vz * vscale : (real)0, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1, w);
+    scatter8_fixed_agg(J64z, dep ? X.b * sx + Y.b * sy + Z.a : -1, sx, sy, w);
+    if (live) {
+      advance(i, fx, vx * pc.hdt);
+      advance(j, fy, vy * pc.hdt);
+      advance(k, fz, vz * pc.hdt);
+      if (in_array(g, i, j, k)) {
+        if (stencil_ok(g, i, j, k)) {
+          const Axis<real> X1 = axis_weights(i, fx), Y1 = axis_weights(j, fy), Z1 = axis_weights(k, fz);
+          deposit_n(F, g, pc, X1, Y1, Z1);
+        } else {
+          count_err(err, ERR_DEPOSIT_OOB);
+        }
       }
+      store_records(P, t, boundary(g, i, j, k) ? repack(i, j, k, err) : -1, fx, fy, fz, vx, vy, vz);
     }
-    P.cell[t] = boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
-    P.o[0][t] = fx; P.o[1][t] = fy; P.o[2][t] = fz;
-    P.v[0][t] = vx; P.v[1][t] = vy; P.v[2][t] = vz;
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
   if ((threadIdx.x & 31) == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
@@ -171,16 +246,16 @@ __global__ void __launch_bounds__(256) objective_kernel(Parts<real> P, int n, Fi
                                                         AdjConst a, double* acc) {
   double s[1] = {0.0};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int c = P.cell[t];
-    if (c < 0) continue;
+    const Rec<real> r = load_records(P, t);
+    if (r.cell < 0) continue;
     int i, j, k;
-    unpack_cell(c, i, j, k);
+    unpack_cell(r.cell, i, j, k);
     if (!stencil_ok(g, i, j, k)) continue;
-    const Axis<real> X = axis_weights(i, P.o[0][t]), Y = axis_weights(j, P.o[1][t]), Z = axis_weights(k, P.o[2][t]);
+    const Axis<real> X = axis_weights(i, r.o[0]), Y = axis_weights(j, r.o[1]), Z = axis_weights(k, r.o[2]);
     const Stagger<real> sx = stagger(g, X, Y, Z, 3), sy = stagger(g, X, Y, Z, 4);
     const double b0x = trilerp(F.f[F_B0X], sx.n, g.sx, g.gz, sx.x0, sx.x1, sx.y0, sx.y1, sx.z0, sx.z1);
     const double b0y = trilerp(F.f[F_B0Y], sy.n, g.sx, g.gz, sy.x0, sy.x1, sy.y0, sy.y1, sy.z0, sy.z1);
-    s[0] -= (double)P.v[0][t] * b0y - (double)P.v[1][t] * b0x;
+    s[0] -= (double)r.v[0] * b0y - (double)r.v[1] * b0x;
   }
   const int idx[1] = {0};
   const double scale[1] = {a.K * a.dt};
@@ -282,105 +357,125 @@ __global__ void __launch_bounds__(256) push_adjoint_kernel(Parts<real> P, int n,
   double s[2] = {0.0, 0.0};
   const int sx = g.sx, sy = g.gz;
   const real js = (real)a.jsign;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int c = P.cell[t];
-    if (c < 0) {
+  const int lane = threadIdx.x & 31;
+  // warp-uniform trip count: the field adjoints' scatter is aggregated across the warp
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += gridDim.x * blockDim.x) {
+    const int t = base + lane;
+    Rec<real> r{};
+    r.cell = -1;
+    if (t < n) r = load_records(P, t);
+    const bool live = r.cell >= 0;
+    if (t < n && !live) {
 #pragma unroll
       for (int q = 0; q < 3; ++q) { A.lx[q][t] = (real)0; A.lv[q][t] = (real)0; }
-      continue;
     }
-    int i0, j0, k0;
-    unpack_cell(c, i0, j0, k0);
-    const real f0x = P.o[0][t], f0y = P.o[1][t], f0z = P.o[2][t];
-    const real v0x = P.v[0][t], v0y = P.v[1][t], v0z = P.v[2][t];
-    // ---- forward recompute
-    bool bal = ballistic(pc, i0, j0, k0, f0x, f0y, f0z);
-    if (!bal && !stencil_ok(g, i0, j0, k0)) bal = true;
-    Axis<real> X0, Y0, Z0;
-    Gathered<real> G{};
-    real vx = v0x, vy = v0y, vz = v0z;
-    if (!bal) {
-      X0 = axis_weights(i0, f0x); Y0 = axis_weights(j0, f0y); Z0 = axis_weights(k0, f0z);
-      G = gather6(F, g, X0, Y0, Z0);
-      boris4(pc, G, vx, vy, vz);
-    }
-    int ih = i0, jh = j0, kh = k0;
-    real fhx = f0x, fhy = f0y, fhz = f0z;
-    advance(ih, fhx, vx * pc.hdt);
-    advance(jh, fhy, vy * pc.hdt);
-    advance(kh, fhz, vz * pc.hdt);
-    const bool dep = in_array(g, ih, jh, kh) && stencil_ok(g, ih, jh, kh);
-    int i1 = ih, j1 = jh, k1 = kh;
-    real f1x = fhx, f1y = fhy, f1z = fhz;
-    advance(i1, f1x, vx * pc.hdt);
-    advance(j1, f1y, vy * pc.hdt);
-    advance(k1, f1z, vz * pc.hdt);
-    const bool alive = boundary(g, i1, j1, k1);
-    // ---- reverse
-    real ax[3] = {0, 0, 0}, av[3] = {0, 0, 0};
-    if (alive) {
-#pragma unroll
-      for (int q = 0; q < 3; ++q) { ax[q] = A.lx[q][t]; av[q] = A.lv[q][t]; }
-      if (stencil_ok(g, i1, j1, k1)) {
-        // objective: F_p = -K (vx B0y - vy B0x) at the new (wrapped) position, times dt
-        const Axis<real> X = axis_weights(i1, f1x), Y = axis_weights(j1, f1y), Z = axis_weights(k1, f1z);
-        const Stagger<real> bxs = stagger(g, X, Y, Z, 3), bys = stagger(g, X, Y, Z, 4);
-        const VG<real> b0x = trilerp_vg(F.f[F_B0X], bxs.n, sx, sy, bxs.x0, bxs.x1, bxs.y0, bxs.y1, bxs.z0, bxs.z1);
-        const VG<real> b0y = trilerp_vg(F.f[F_B0Y], bys.n, sx, sy, bys.x0, bys.x1, bys.y0, bys.y1, bys.z0, bys.z1);
-        const real w = (real)(-a.K * a.dt);
-        av[0] += w * b0y.v;
-        av[1] -= w * b0x.v;
-        ax[0] += w * (vx * b0y.gx - vy * b0x.gx);
-        ax[1] += w * (vx * b0y.gy - vy * b0x.gy);
-        ax[2] += w * (vx * b0y.gz - vy * b0x.gz);
-        s[0] += (double)w * ((double)vx * ((double)b0y.v - a.imf[1]) - (double)vy * ((double)b0x.v - a.imf[0])) * a.inv_I;
+    bool bal = true;
+    Axis<real> X0{}, Y0{}, Z0{};
+    real ax[3] = {0, 0, 0};
+    real af[6] = {0, 0, 0, 0, 0, 0};  // adjoints of the gathered E and B
+    if (live) {
+      int i0, j0, k0;
+      unpack_cell(r.cell, i0, j0, k0);
+      const real f0x = r.o[0], f0y = r.o[1], f0z = r.o[2];
+      const real v0x = r.v[0], v0y = r.v[1], v0z = r.v[2];
+      // ---- forward recompute
+      bal = ballistic(pc, i0, j0, k0, f0x, f0y, f0z);
+      if (!bal && !stencil_ok(g, i0, j0, k0)) bal = true;
+      Gathered<real> G{};
+      real vx = v0x, vy = v0y, vz = v0z;
+      if (!bal) {
+        X0 = axis_weights(i0, f0x); Y0 = axis_weights(j0, f0y); Z0 = axis_weights(k0, f0z);
+        G = gather6(F, g, X0, Y0, Z0);
+        boris4(pc, G, vx, vy, vz);
       }
-    }
-    // drift: xi1 = xih + hdt v
+      int ih = i0, jh = j0, kh = k0;
+      real fhx = f0x, fhy = f0y, fhz = f0z;
+      advance(ih, fhx, vx * pc.hdt);
+      advance(jh, fhy, vy * pc.hdt);
+      advance(kh, fhz, vz * pc.hdt);
+      const bool dep = in_array(g, ih, jh, kh) && stencil_ok(g, ih, jh, kh);
+      int i1 = ih, j1 = jh, k1 = kh;
+      real f1x = fhx, f1y = fhy, f1z = fhz;
+      advance(i1, f1x, vx * pc.hdt);
+      advance(j1, f1y, vy * pc.hdt);
+      advance(k1, f1z, vz * pc.hdt);
+      const bool alive = boundary(g, i1, j1, k1);
+      // ---- reverse
+      real av[3] = {0, 0, 0};
+      if (alive) {
 #pragma unroll
-    for (int q = 0; q < 3; ++q) av[q] += pc.hdt * ax[q];
-    // J deposit at xih: J_q += qn v_q W_q(xih)
-    if (dep) {
-      const Axis<real> X = axis_weights(ih, fhx), Y = axis_weights(jh, fhy), Z = axis_weights(kh, fhz);
-      const real vq[3] = {vx, vy, vz};
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const Stagger<real> st = stagger(g, X, Y, Z, q);
-        const VG<real> l = trilerp_vg(A.lj[q], st.n, sx, sy, st.x0, st.x1, st.y0, st.y1, st.z0, st.z1);
-        const real k = js * pc.qn;
-        av[q] += k * l.v;
-        ax[0] += k * vq[q] * l.gx;
-        ax[1] += k * vq[q] * l.gy;
-        ax[2] += k * vq[q] * l.gz;
+        for (int q = 0; q < 3; ++q) { ax[q] = A.lx[q][t]; av[q] = A.lv[q][t]; }
+        if (stencil_ok(g, i1, j1, k1)) {
+          // objective: F_p = -K (vx B0y - vy B0x) at the new (wrapped) position, times dt
+          const Axis<real> X = axis_weights(i1, f1x), Y = axis_weights(j1, f1y), Z = axis_weights(k1, f1z);
+          const Stagger<real> bxs = stagger(g, X, Y, Z, 3), bys = stagger(g, X, Y, Z, 4);
+          const VG<real> b0x = trilerp_vg(F.f[F_B0X], bxs.n, sx, sy, bxs.x0, bxs.x1, bxs.y0, bxs.y1, bxs.z0, bxs.z1);
+          const VG<real> b0y = trilerp_vg(F.f[F_B0Y], bys.n, sx, sy, bys.x0, bys.x1, bys.y0, bys.y1, bys.z0, bys.z1);
+          const real w = (real)(-a.K * a.dt);
+          av[0] += w * b0y.v;
+          av[1] -= w * b0x.v;
+          ax[0] += w * (vx * b0y.gx - vy * b0x.gx);
+          ax[1] += w * (vx * b0y.gy - vy * b0x.gy);
+          ax[2] += w * (vx * b0y.gz - vy * b0x.gz);
+          s[0] += (double)w * ((double)vx * ((double)b0y.v - a.imf[1]) - (double)vy * ((double)b0x.v - a.imf[0])) * a.inv_I;
+        }
       }
+      // drift: xi1 = xih + hdt v
+#pragma unroll
+      for (int q = 0; q < 3; ++q) av[q] += pc.hdt * ax[q];
+      // J deposit at xih: J_q += qn v_q W_q(xih)
+      if (dep) {
+        const Axis<real> X = axis_weights(ih, fhx), Y = axis_weights(jh, fhy), Z = axis_weights(kh, fhz);
+        const real vq[3] = {vx, vy, vz};
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const Stagger<real> st = stagger(g, X, Y, Z, q);
+          const VG<real> l = trilerp_vg(A.lj[q], st.n, sx, sy, st.x0, st.x1, st.y0, st.y1, st.z0, st.z1);
+          const real k = js * pc.qn;
+          av[q] += k * l.v;
+          ax[0] += k * vq[q] * l.gx;
+          ax[1] += k * vq[q] * l.gy;
+          ax[2] += k * vq[q] * l.gz;
+        }
+      }
+      // xih = xi0 + hdt v
+#pragma unroll
+      for (int q = 0; q < 3; ++q) av[q] += pc.hdt * ax[q];
+      if (!bal) {
+        real ae[3], ab[3];
+        boris4_adjoint(pc, G, v0x, v0y, v0z, av, ae, ab);
+        s[1] += (double)ae[0] * a.imf[1] - (double)ae[1] * a.imf[0];  // E += (V IMF_y, -V IMF_x, 0)
+        af[0] = ae[0]; af[1] = ae[1]; af[2] = ae[2];
+        af[3] = ab[0]; af[4] = ab[1]; af[5] = ab[2];
+      }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) A.lv[q][t] = av[q];
     }
-    // xih = xi0 + hdt v
-#pragma unroll
-    for (int q = 0; q < 3; ++q) av[q] += pc.hdt * ax[q];
-    if (!bal) {
-      real ae[3], ab[3];
-      boris4_adjoint(pc, G, v0x, v0y, v0z, av, ae, ab);
-      s[1] += (double)ae[0] * a.imf[1] - (double)ae[1] * a.imf[0];  // E += (V IMF_y, -V IMF_x, 0)
-      // gather at xi0: scatter the field adjoints, add the interpolants' gradients
-      const real af[6] = {ae[0], ae[1], ae[2], ab[0], ab[1], ab[2]};
-      real* const dst[6] = {A.le[0], A.le[1], A.le[2], A.ldb[0], A.ldb[1], A.ldb[2]};
-      const int src[6] = {F_EX, F_EY, F_EZ, F_BX, F_BY, F_BZ};
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        const Stagger<real> st = stagger(g, X0, Y0, Z0, q);
+    // gather at xi0: scatter the field adjoints, add the interpolants' gradients
+    const bool gat = live && !bal;
+    real* const dst[6] = {A.le[0], A.le[1], A.le[2], A.ldb[0], A.ldb[1], A.ldb[2]};
+    const int src[6] = {F_EX, F_EY, F_EZ, F_BX, F_BY, F_BZ};
+#pragma unroll 1
+    for (int q = 0; q < 6; ++q) {
+      Stagger<real> st{};
+      if (gat) {
+        st = stagger(g, X0, Y0, Z0, q);
         const VG<real> fv = trilerp_vg(F.f[src[q]], st.n, sx, sy, st.x0, st.x1, st.y0, st.y1, st.z0, st.z1);
         ax[0] += af[q] * fv.gx;
         ax[1] += af[q] * fv.gy;
         ax[2] += af[q] * fv.gz;
-        scatter8(dst[q], st.n, sx, sy, af[q], st.x0, st.x1, st.y0, st.y1, st.z0, st.z1);
         if (q >= 3) {  // B = B0 + DB: the dipole part of B0 is proportional to I
           const real b0 = trilerp(F.f[F_B0X + q - 3], st.n, sx, sy, st.x0, st.x1, st.y0, st.y1, st.z0, st.z1);
           s[0] += (double)af[q] * ((double)b0 - a.imf[q - 3]) * a.inv_I;
         }
       }
+      scatter8_agg(dst[q], gat ? st.n : -1, sx, sy, gat ? af[q] : (real)0, st.x0, st.x1, st.y0, st.y1, st.z0,
+                   st.z1);
     }
+    if (live) {
 #pragma unroll
-    for (int q = 0; q < 3; ++q) { A.lx[q][t] = ax[q]; A.lv[q][t] = av[q]; }
+      for (int q = 0; q < 3; ++q) A.lx[q][t] = ax[q];
+    }
   }
   const int idx[2] = {1, 2};
   const double scale[2] = {1.0, 1.0};
@@ -515,7 +610,7 @@ __global__ void __launch_bounds__(256) renew_b_adjoint_curl(AdjField<real> A, Ge
   A.le[2][n] += -dminus_t(A.w[0], g, i, j, k, 1) + dminus_t(A.w[1], g, i, j, k, 0);
 }
 
-// Reverse of wrap_x_kernel / wrap_y_kernel (ghost copies): the adjoint of a
+// Reverse of wrap_kernel (ghost copies): the adjoint of a
 // ghost goes to its source and the ghost's own adjoint is cleared.
 template <typename real>
 __global__ void wrap_x_adjoint(PlaneSet<real> s, Geom g) {
@@ -549,7 +644,7 @@ __global__ void wrap_y_adjoint(PlaneSet<real> s, Geom g) {
   }
 }
 
-// Reverse of wrap_b_x_kernel / wrap_b_y_kernel on the induced field:
+// Reverse of wrap_b_kernel on the induced field:
 // DB[dst] = DB[src] + B0[src] - B0[dst], so besides the copy's transpose the
 // ghost adjoints add lDB[dst] (B0[src] - B0[dst]) / I to dJ/dI (acc[1]).
 template <typename real>
@@ -590,7 +685,7 @@ __global__ void __launch_bounds__(256) wrap_b_adjoint(Fields<real> F, AdjField<r
   block_reduce_add<1>(s, acc, idx, scale);
 }
 
-// Reverse of fold_x_kernel / fold_y_kernel: the ghosts' adjoints take those
+// Reverse of fold_kernel: the ghosts' adjoints take those
 // of the interior planes they were added to.
 template <typename real>
 __global__ void fold_x_adjoint(PlaneSet<real> s, Geom g) {

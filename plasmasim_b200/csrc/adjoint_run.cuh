@@ -27,6 +27,11 @@ struct AdjSnap {
 
 struct AdjRun {
   std::vector<void*> owned;
+  // snapshot blocks: allocated on first need, returned to `spare` when a
+  // snapshot is released and handed out again, freed with the run
+  std::vector<std::pair<void*, size_t>> spare;
+  std::vector<void*> snaps;
+  std::map<void*, size_t> snap_size;
   int* scan_tmp = nullptr;
   size_t scan_len = 0;
   void* lam[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [species][buffer]: lx[3] lv[3]
@@ -51,23 +56,46 @@ int adj_alloc(pic_ctx* c, AdjRun& R, void** p, size_t bytes) {
 void adj_free(AdjRun& R) {
   for (void* p : R.owned) cudaFree(p);
   R.owned.clear();
+  for (void* p : R.snaps) cudaFree(p);
+  R.snaps.clear();
+  R.spare.clear();
 }
 
-// Snapshot memory is returned as soon as a segment is done with it.
-int snap_alloc(pic_ctx* c, void** p, size_t bytes) {
-  CK(cudaMalloc(p, bytes < 256 ? 256 : bytes));
+// Snapshot memory: the smallest spare block that holds `bytes`, else a new
+// block with 1/16 headroom (particle counts drift by a little between steps)
+// rounded to 2 MB. A run allocates each block once: cudaMalloc and cudaFree
+// inside the loop would stall the stream at every step.
+int snap_alloc(pic_ctx* c, AdjRun& R, void** p, size_t bytes) {
+  size_t best = R.spare.size();
+  for (size_t q = 0; q < R.spare.size(); ++q)
+    if (R.spare[q].second >= bytes && (best == R.spare.size() || R.spare[q].second < R.spare[best].second)) best = q;
+  if (best < R.spare.size()) {
+    *p = R.spare[best].first;
+    R.snap_size[*p] = R.spare[best].second;
+    R.spare.erase(R.spare.begin() + (long)best);
+    return PIC_OK;
+  }
+  const size_t want = ((bytes + bytes / 16) + ((size_t)1 << 21) - 1) & ~(((size_t)1 << 21) - 1);
+  CK(cudaMalloc(p, want));
+  R.snaps.push_back(*p);
+  R.snap_size[*p] = want;
   return PIC_OK;
 }
 
-void snap_free(AdjSnap& S) {
+void snap_release(AdjRun& R, void*& p) {
+  if (!p) return;
+  R.spare.emplace_back(p, R.snap_size[p]);
+  p = nullptr;
+}
+
+void snap_free(AdjRun& R, AdjSnap& S) {
   for (int s = 0; s < 2; ++s) {
-    cudaFree(S.part[s]);
-    cudaFree(S.map[s]);
-    S.part[s] = nullptr;
+    snap_release(R, S.part[s]);
+    void* m = S.map[s];
+    snap_release(R, m);
     S.map[s] = nullptr;
   }
-  cudaFree(S.planes);
-  S.planes = nullptr;
+  snap_release(R, S.planes);
 }
 
 template <typename real>
@@ -87,14 +115,14 @@ int copy_parts(pic_ctx* c, Parts<real> dst, Parts<real> src, long long n) {
 // The context's particles, fields (E, B, DB), random-stream counters and step
 // counters into a new snapshot.
 template <typename real>
-int adj_save(pic_ctx* c, AdjSnap& S) {
+int adj_save(pic_ctx* c, AdjRun& R, AdjSnap& S) {
   for (int s = 0; s < 2; ++s) {
     S.count[s] = c->sp[s].count;
-    CKR(snap_alloc(c, &S.part[s], store_bytes(S.count[s] > 0 ? S.count[s] : 1, c->rsize)));
+    CKR(snap_alloc(c, R, &S.part[s], store_bytes(S.count[s] > 0 ? S.count[s] : 1, c->rsize)));
     CKR(copy_parts<real>(c, parts_at<real>(S.part[s], S.count[s] > 0 ? S.count[s] : 1), parts<real>(c, s),
                          S.count[s]));
   }
-  CKR(snap_alloc(c, &S.planes, kSnapPlanes * c->plane_bytes));
+  CKR(snap_alloc(c, R, &S.planes, kSnapPlanes * c->plane_bytes));
   CK(cudaMemcpyAsync(S.planes, (char*)c->field_mem + (size_t)F_EX * c->plane_bytes,
                      kSnapPlanes * c->plane_bytes, cudaMemcpyDeviceToDevice, c->stream));
   S.ctr_p = c->ctr_p;
@@ -175,7 +203,7 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
       }
       int* map = nullptr;
       if (rec && st.count > 0) {
-        CKR(snap_alloc(c, (void**)&map, sizeof(int) * (size_t)st.count));
+        CKR(snap_alloc(c, R, (void**)&map, sizeof(int) * (size_t)st.count));
         rec->map[s] = map;
         rec->map_n[s] = st.count;
       }
@@ -186,7 +214,7 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
     c->c_add = 0;
   }
   if (rec) {
-    CKR(adj_save<real>(c, *rec));
+    CKR(adj_save<real>(c, R, *rec));
     rec->kept[0] = kept[0];
     rec->kept[1] = kept[1];
   }

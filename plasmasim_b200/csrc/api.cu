@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <new>
 #include <vector>
 
@@ -488,9 +489,9 @@ int wrap_planes(pic_ctx* c, const int* ids, int n) {
   for (int q = 0; q < n; ++q) s.p[q] = F.f[ids[q]];
   s.count = n;
   if (c->has_xport) return halo_ghosts<real>(c, s, s, HALO_COPY);
-  wrap_x_kernel<real><<<grid_blocks((long long)c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
+  wrap_kernel<real><<<grid_blocks(4LL * n * c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(s, c->g, 0);
   CKL();
-  wrap_y_kernel<real><<<grid_blocks((long long)c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
+  wrap_kernel<real><<<grid_blocks(4LL * n * c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(s, c->g, 1);
   CKL();
   return PIC_OK;
 }
@@ -520,9 +521,9 @@ int do_renew_b(pic_ctx* c) {
     aux.count = 6;
     return halo_ghosts<real>(c, s, aux, HALO_BTOTAL);
   }
-  wrap_b_x_kernel<real><<<grid_blocks((long long)c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(fields<real>(c), c->g);
+  wrap_b_kernel<real><<<grid_blocks(12LL * c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(fields<real>(c), c->g, 0);
   CKL();
-  wrap_b_y_kernel<real><<<grid_blocks((long long)c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(fields<real>(c), c->g);
+  wrap_b_kernel<real><<<grid_blocks(12LL * c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(fields<real>(c), c->g, 1);
   CKL();
   return PIC_OK;
 }
@@ -551,9 +552,9 @@ int do_fold(pic_ctx* c) {
   for (int q = 0; q < 8; ++q) s.p[q] = F.f[F_JIX + q];
   s.count = 8;
   if (c->has_xport) return halo_fold<real>(c, s);
-  fold_x_kernel<real><<<grid_blocks((long long)c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
+  fold_kernel<real><<<grid_blocks(32LL * c->g.gy * c->g.gz), kThreads, 0, c->stream>>>(s, c->g, 0);
   CKL();
-  fold_y_kernel<real><<<grid_blocks((long long)c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(s, c->g);
+  fold_kernel<real><<<grid_blocks(32LL * c->g.gx * c->g.gz), kThreads, 0, c->stream>>>(s, c->g, 1);
   CKL();
   return PIC_OK;
 }
@@ -1242,7 +1243,7 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
     for (int n = 0; n < nsteps; ++n) {
       if (grad && n % every == 0) {
         ck.emplace_back();
-        CKR(adj_save<real>(c, ck.back()));
+        CKR(adj_save<real>(c, R, ck.back()));
       }
       CKR(adj_forward_step<real>(c, R, nullptr));
     }
@@ -1251,7 +1252,7 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
     CK(cudaStreamSynchronize(c->stream));
     out[0] = h[0];
     if (!grad) return PIC_OK;
-    CKR(adj_save<real>(c, fin));
+    CKR(adj_save<real>(c, R, fin));
     // adjoint state: zero for the final state (the objective terms enter in the reverse kernels)
     for (int s = 0; s < 2; ++s)
       for (int b = 0; b < 2; ++b) {
@@ -1272,8 +1273,8 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
         rc = adj_reverse_step<real>(c, R, rec[n - n0]);
         if (rc == PIC_OK) rc = adj_unrefill<real>(c, R, rec[n - n0]);
       }
-      CK(cudaStreamSynchronize(c->stream));
-      for (auto& S : rec) snap_free(S);
+      for (auto& S : rec) snap_free(R, S);
+      if (seg > 0) snap_free(R, ck[seg]);  // the first checkpoint's particles serve the drift gradient below
       if (rc != PIC_OK) return rc;
     }
     // the initial particles were created with vz = V + thermal
@@ -1293,8 +1294,6 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
   };
   const int rc = run();
   cudaStreamSynchronize(c->stream);
-  for (auto& S : ck) snap_free(S);
-  snap_free(fin);
   adj_free(R);
   return rc;
 }

@@ -193,40 +193,37 @@ struct PlaneSet {
   int count;
 };
 
-// sr_b / sr_e at size 1, x pass (:1016-1101): ghosts 0,1 <- N, N+1 and
-// N+2, N+3 <- 2, 3 for every (l, m).
-template <typename real>
-__global__ void wrap_x_kernel(PlaneSet<real> s, Geom g) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.gy * g.gz) return;
-  const int N = g.nx, sx = g.sx;
-  for (int q = 0; q < s.count; ++q) {
-    real* a = s.p[q];
-    const real v0 = a[N * sx + t], v1 = a[(N + 1) * sx + t];
-    const real v2 = a[2 * sx + t], v3 = a[3 * sx + t];
-    a[t] = v0;
-    a[sx + t] = v1;
-    a[(N + 2) * sx + t] = v2;
-    a[(N + 3) * sx + t] = v3;
-  }
+// One thread per (plane, ghost layer, in-layer node): the ghost layers are
+// thin (two on each side), so the parallelism comes from the planes and the
+// layers as well as the nodes. Sources (interior layers 2, 3, N, N+1) and
+// targets (ghost layers 0, 1, N+2, N+3) are disjoint for N >= 2, so the
+// threads are independent.
+__device__ __forceinline__ void ghost_pair(int r, int N, int& dst, int& src) {
+  // r: 0, 1 -> ghosts 0, 1 <- N, N+1; 2, 3 -> ghosts N+2, N+3 <- 2, 3
+  dst = r < 2 ? r : N + r;
+  src = r < 2 ? N + r : r;
 }
 
-// y pass (:1103-1190): ghosts 0,1 <- N, N+1 and N+2, N+3 <- 2, 3 for every (k, m).
+// Offset of node e of layer `layer` of an x pass (a whole k plane) or of a y
+// pass (row l of every k plane, ghosts included).
+__device__ __forceinline__ long long layer_node(const Geom& g, int axis, int layer, int e) {
+  if (axis == 0) return (long long)layer * g.sx + e;
+  return (long long)(e / g.gz) * g.sx + (long long)layer * g.gz + e % g.gz;
+}
+
+// sr_b / sr_e at size 1: x pass (:1016-1101) then y pass (:1103-1190);
+// ghosts 0,1 <- N, N+1 and N+2, N+3 <- 2, 3.
 template <typename real>
-__global__ void wrap_y_kernel(PlaneSet<real> s, Geom g) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.gx * g.gz) return;
-  const int k = t / g.gz, m = t % g.gz;
-  const int N = g.ny, sy = g.gz;
-  const int base = k * g.sx + m;
-  for (int q = 0; q < s.count; ++q) {
+__global__ void wrap_kernel(PlaneSet<real> s, Geom g, int axis) {
+  const int per = axis == 0 ? g.gy * g.gz : g.gx * g.gz;
+  const int N = axis == 0 ? g.nx : g.ny;
+  const long long total = (long long)s.count * 4 * per;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(t / (4LL * per)), r = (int)((t / per) % 4), e = (int)(t % per);
+    int dst, src;
+    ghost_pair(r, N, dst, src);
     real* a = s.p[q];
-    const real v0 = a[base + N * sy], v1 = a[base + (N + 1) * sy];
-    const real v2 = a[base + 2 * sy], v3 = a[base + 3 * sy];
-    a[base] = v0;
-    a[base + sy] = v1;
-    a[base + (N + 2) * sy] = v2;
-    a[base + (N + 3) * sy] = v3;
+    a[layer_node(g, axis, dst, e)] = a[layer_node(g, axis, src, e)];
   }
 }
 
@@ -234,85 +231,35 @@ __global__ void wrap_y_kernel(PlaneSet<real> s, Geom g) {
 // periodic images of B, while B0 keeps its own (non-periodic) dipole values, so
 // the induced field there is B_image - B0_ghost, which the E update then sees.
 template <typename real>
-__global__ void wrap_b_x_kernel(Fields<real> F, Geom g) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.gy * g.gz) return;
-  const int N = g.nx, sx = g.sx;
-  const int dst[4] = {t, sx + t, (N + 2) * sx + t, (N + 3) * sx + t};
-  const int src[4] = {N * sx + t, (N + 1) * sx + t, 2 * sx + t, 3 * sx + t};
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    real* b = F.f[F_BX + q];
-    real* db = F.f[F_DBX + q];
-    const real* b0 = F.f[F_B0X + q];
-    real v[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) v[r] = b[src[r]];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      b[dst[r]] = v[r];
-      db[dst[r]] = v[r] - b0[dst[r]];
-    }
+__global__ void wrap_b_kernel(Fields<real> F, Geom g, int axis) {
+  const int per = axis == 0 ? g.gy * g.gz : g.gx * g.gz;
+  const int N = axis == 0 ? g.nx : g.ny;
+  const long long total = 3LL * 4 * per;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(t / (4LL * per)), r = (int)((t / per) % 4), e = (int)(t % per);
+    int dst, src;
+    ghost_pair(r, N, dst, src);
+    const long long d = layer_node(g, axis, dst, e);
+    const real v = F.f[F_BX + q][layer_node(g, axis, src, e)];
+    F.f[F_BX + q][d] = v;
+    F.f[F_DBX + q][d] = v - F.f[F_B0X + q][d];
   }
 }
 
+// sr_current2 at size 1: x pass (:1815-1935), then y pass over every k
+// including the x ghosts (:1937-2036); layers 2,3 += N+2, N+3 and
+// N, N+1 += 0, 1 (the sources are ghosts, the targets interior).
 template <typename real>
-__global__ void wrap_b_y_kernel(Fields<real> F, Geom g) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.gx * g.gz) return;
-  const int k = t / g.gz, m = t % g.gz;
-  const int N = g.ny, sy = g.gz;
-  const int base = k * g.sx + m;
-  const int dst[4] = {base, base + sy, base + (N + 2) * sy, base + (N + 3) * sy};
-  const int src[4] = {base + N * sy, base + (N + 1) * sy, base + 2 * sy, base + 3 * sy};
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    real* b = F.f[F_BX + q];
-    real* db = F.f[F_DBX + q];
-    const real* b0 = F.f[F_B0X + q];
-    real v[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) v[r] = b[src[r]];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      b[dst[r]] = v[r];
-      db[dst[r]] = v[r] - b0[dst[r]];
-    }
-  }
-}
-
-// sr_current2 at size 1, x pass (:1815-1935): planes 2,3 += N+2, N+3 and
-// N, N+1 += 0, 1 (sources are ghosts, targets interior: disjoint for N >= 2).
-template <typename real>
-__global__ void fold_x_kernel(PlaneSet<real> s, Geom g) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.gy * g.gz) return;
-  const int N = g.nx, sx = g.sx;
-  for (int q = 0; q < s.count; ++q) {
+__global__ void fold_kernel(PlaneSet<real> s, Geom g, int axis) {
+  const int per = axis == 0 ? g.gy * g.gz : g.gx * g.gz;
+  const int N = axis == 0 ? g.nx : g.ny;
+  const long long total = (long long)s.count * 4 * per;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(t / (4LL * per)), r = (int)((t / per) % 4), e = (int)(t % per);
+    int ghost, target;
+    ghost_pair(r, N, ghost, target);  // the wrap's targets are the fold's sources
     real* a = s.p[q];
-    const real g0 = a[t], g1 = a[sx + t], g2 = a[(N + 2) * sx + t], g3 = a[(N + 3) * sx + t];
-    a[2 * sx + t] += g2;
-    a[3 * sx + t] += g3;
-    a[N * sx + t] += g0;
-    a[(N + 1) * sx + t] += g1;
-  }
-}
-
-// y pass (:1937-2036), over every k including the x ghosts.
-template <typename real>
-__global__ void fold_y_kernel(PlaneSet<real> s, Geom g) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.gx * g.gz) return;
-  const int k = t / g.gz, m = t % g.gz;
-  const int N = g.ny, sy = g.gz;
-  const int base = k * g.sx + m;
-  for (int q = 0; q < s.count; ++q) {
-    real* a = s.p[q];
-    const real g0 = a[base], g1 = a[base + sy], g2 = a[base + (N + 2) * sy], g3 = a[base + (N + 3) * sy];
-    a[base + 2 * sy] += g2;
-    a[base + 3 * sy] += g3;
-    a[base + N * sy] += g0;
-    a[base + (N + 1) * sy] += g1;
+    a[layer_node(g, axis, target, e)] += a[layer_node(g, axis, ghost, e)];
   }
 }
 

@@ -89,6 +89,40 @@ __device__ __forceinline__ Gathered<real> gather6(const Fields<real>& F, const G
   return r;
 }
 
+// Particle t's records, read with vector loads.
+template <typename real>
+struct Rec {
+  int cell;
+  real o[3];
+  real v[3];
+};
+__device__ __forceinline__ Rec<float> load_records(const Parts<float>& P, long long t) {
+  const float4 a = reinterpret_cast<const float4*>(P.ra)[t];
+  const float4 b = reinterpret_cast<const float4*>(P.rb)[t];
+  return Rec<float>{__float_as_int(a.x), {a.y, a.z, a.w}, {b.x, b.y, b.z}};
+}
+__device__ __forceinline__ Rec<double> load_records(const Parts<double>& P, long long t) {
+  const double2* a = reinterpret_cast<const double2*>(P.ra + 4 * t);
+  const double2* b = reinterpret_cast<const double2*>(P.rb + 4 * t);
+  const double2 a0 = a[0], a1 = a[1], b0 = b[0], b1 = b[1];
+  return Rec<double>{__double2loint(a0.x), {a0.y, a1.x, a1.y}, {b0.x, b0.y, b1.x}};
+}
+
+// Particle t's records, written with vector stores.
+__device__ __forceinline__ void store_records(const Parts<float>& P, long long t, int c, float fx, float fy,
+                                              float fz, float vx, float vy, float vz) {
+  reinterpret_cast<float4*>(P.ra)[t] = make_float4(__int_as_float(c), fx, fy, fz);
+  reinterpret_cast<float4*>(P.rb)[t] = make_float4(vx, vy, vz, 0.f);
+}
+__device__ __forceinline__ void store_records(const Parts<double>& P, long long t, int c, double fx, double fy,
+                                              double fz, double vx, double vy, double vz) {
+  double2* a = reinterpret_cast<double2*>(P.ra + 4 * t);
+  double2* b = reinterpret_cast<double2*>(P.rb + 4 * t);
+  a[0] = make_double2(__hiloint2double(0, c), fx);
+  a[1] = make_double2(fy, fz);
+  b[0] = make_double2(vx, vy);
+  b[1] = make_double2(vz, 0.0);
+}
 // Particle s of S to slot d of D with cell index c: two vector copies.
 __device__ __forceinline__ void copy_record(const Parts<float>& S, long long s, const Parts<float>& D, long long d,
                                             int c) {
@@ -286,13 +320,13 @@ __global__ void __launch_bounds__(256) push_kernel(Parts<real> P, int first, con
   const int n = *count;
   unsigned pushed = 0;
   for (int t = first + blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int c = P.cell[t];
-    if (c < 0) continue;
+    const Rec<real> r = load_records(P, t);
+    if (r.cell < 0) continue;
     ++pushed;
     int i, j, k;
-    unpack_cell(c, i, j, k);
-    real fx = P.o[0][t], fy = P.o[1][t], fz = P.o[2][t];
-    real vx = P.v[0][t], vy = P.v[1][t], vz = P.v[2][t];
+    unpack_cell(r.cell, i, j, k);
+    real fx = r.o[0], fy = r.o[1], fz = r.o[2];
+    real vx = r.v[0], vy = r.v[1], vz = r.v[2];
     bool bal = ballistic(pc, i, j, k, fx, fy, fz);
     if (!bal && !stencil_ok(g, i, j, k)) {
       count_err(err, ERR_DEPOSIT_OOB);
@@ -331,9 +365,7 @@ __global__ void __launch_bounds__(256) push_kernel(Parts<real> P, int first, con
     } else {
       cell = repack(i, j, k, err);
     }
-    P.cell[t] = cell;
-    P.o[0][t] = fx; P.o[1][t] = fy; P.o[2][t] = fz;
-    P.v[0][t] = vx; P.v[1][t] = vy; P.v[2][t] = vz;
+    store_records(P, t, cell, fx, fy, fz, vx, vy, vz);
   }
   // particle pushes of this warp, one atomic per warp
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);

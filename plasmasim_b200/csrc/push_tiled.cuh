@@ -176,21 +176,6 @@ __device__ __forceinline__ void fetch_records(real* dst, const Parts<real>& P, l
   }
 }
 
-// Particle t's records, written with vector stores.
-__device__ __forceinline__ void store_records(const Parts<float>& P, long long t, int c, float fx, float fy,
-                                              float fz, float vx, float vy, float vz) {
-  reinterpret_cast<float4*>(P.ra)[t] = make_float4(__int_as_float(c), fx, fy, fz);
-  reinterpret_cast<float4*>(P.rb)[t] = make_float4(vx, vy, vz, 0.f);
-}
-__device__ __forceinline__ void store_records(const Parts<double>& P, long long t, int c, double fx, double fy,
-                                              double fz, double vx, double vy, double vz) {
-  double2* a = reinterpret_cast<double2*>(P.ra + 4 * t);
-  double2* b = reinterpret_cast<double2*>(P.rb + 4 * t);
-  a[0] = make_double2(__hiloint2double(0, c), fx);
-  a[1] = make_double2(fy, fz);
-  b[0] = make_double2(vx, vy);
-  b[1] = make_double2(vz, 0.0);
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
