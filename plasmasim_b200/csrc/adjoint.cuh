@@ -79,8 +79,8 @@ struct AdjConst {
 // atomics do not depend on the order of the particles): each term
 // v_q W / c is scaled by 2^40, which leaves 23 bits of headroom for the
 // number of particles per node; jconvert_kernel turns the sums into
-// J = q n c (sum / 2^40). The warp-aggregated scatter below keeps this: its
-// group sums are exact.
+// J = q n c (sum / 2^40). The warp-aggregated scatter below keeps this: it
+// converts deterministic per-group sums.
 constexpr double kJFixed = 1099511627776.0;  // 2^40
 
 // ------------------------------------------------------------ warp-aggregated scatters
@@ -114,29 +114,24 @@ __device__ __forceinline__ void group_sum8(T (&w)[8], unsigned grp) {
   }
 }
 
-// Fixed-point terms: integer group sums are exact and independent of the
-// order of the terms, so the planes receive the same totals, modulo 2^64, as
-// from one atomic per lane.
-__device__ __forceinline__ void scatter8_fixed_agg(unsigned long long* F, int key, int sx, int sy,
-                                                   unsigned long long (&w)[8]) {
+// Fixed-point J: each group's terms are summed in the engine's precision by
+// group_sum8, whose order of additions depends only on which slots share the
+// warp and the base, and the first lane adds the sums as 64-bit integers.
+// A replayed segment has the same slots in the same warps, so it adds the
+// same integers, and integer atomics do not depend on their order.
+template <typename real>
+__device__ __forceinline__ void scatter8_fixed_agg(unsigned long long* F, int key, int sx, int sy, real v, real x0,
+                                                   real x1, real y0, real y1, real z0, real z1) {
   const unsigned grp = __match_any_sync(kFullWarp, key);
+  const real a0 = v * x0, a1 = v * x1;
+  const real a00 = a0 * y0, a01 = a0 * y1, a10 = a1 * y0, a11 = a1 * y1;
+  real w[8] = {a00 * z0, a00 * z1, a01 * z0, a01 * z1, a10 * z0, a10 * z1, a11 * z0, a11 * z1};
   group_sum8(w, grp);
   if (key >= 0 && (int)(threadIdx.x & 31) == __ffs(grp) - 1) {
     const int o[8] = {0, 1, sy, sy + 1, sx, sx + 1, sx + sy, sx + sy + 1};
 #pragma unroll
-    for (int q = 0; q < 8; ++q) atomicAdd(F + key + o[q], w[q]);
+    for (int q = 0; q < 8; ++q) atomicAdd(F + key + o[q], (unsigned long long)__double2ll_rn((double)w[q]));
   }
-}
-
-// The fixed-point terms of one trilinear scatter of v.
-template <typename real>
-__device__ __forceinline__ void fixed_terms(real v, real x0, real x1, real y0, real y1, real z0, real z1,
-                                            unsigned long long (&w)[8]) {
-  const real a0 = v * x0, a1 = v * x1;
-  const real a00 = a0 * y0, a01 = a0 * y1, a10 = a1 * y0, a11 = a1 * y1;
-  const real t[8] = {a00 * z0, a00 * z1, a01 * z0, a01 * z1, a10 * z0, a10 * z1, a11 * z0, a11 * z1};
-#pragma unroll
-  for (int q = 0; q < 8; ++q) w[q] = (unsigned long long)__double2ll_rn((double)t[q]);
 }
 
 // Floating-point terms: one atomic per group and node.
@@ -158,7 +153,7 @@ __device__ __forceinline__ void scatter8_agg(real* F, int key, int sx, int sy, r
 // push_kernel<real, PUSH_FUSED> with the J deposit into fixed-point planes
 // J64[3] (v scaled by 2^40 / c).
 template <typename real>
-__global__ void __launch_bounds__(256) push_fixed_kernel(Parts<real> P, int n, Fields<real> F, Geom g,
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_fixed_kernel(Parts<real> P, int n, Fields<real> F, Geom g,
                                                          PushConst<real> pc, unsigned long long* J64x,
                                                          unsigned long long* J64y, unsigned long long* J64z,
                                                          real vscale, unsigned long long* err) {
@@ -202,27 +197,30 @@ __global__ void __launch_bounds__(256) push_fixed_kernel(Parts<real> P, int n, F
         }
       }
     }
-    unsigned long long w[8];
-    fixed_terms(dep ? vx * vscale : (real)0, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1, w);
-    scatter8_fixed_agg(J64x, dep ? X.a * sx + Y.b * sy + Z.b : -1, sx, sy, w);
-    fixed_terms(dep ? vy * vscale : (real)0, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1, w);
-    scatter8_fixed_agg(J64y, dep ? X.b * sx + Y.a * sy + Z.b : -1, sx, sy, w);
-    fixed_terms(dep ? vz * vscale : (real)0, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1, w);
-    scatter8_fixed_agg(J64z, dep ? X.b * sx + Y.b * sy + Z.a : -1, sx, sy, w);
+    scatter8_fixed_agg(J64x, dep ? X.a * sx + Y.b * sy + Z.b : -1, sx, sy, dep ? vx * vscale : (real)0, X.a0, X.a1,
+                       Y.b0, Y.b1, Z.b0, Z.b1);
+    scatter8_fixed_agg(J64y, dep ? X.b * sx + Y.a * sy + Z.b : -1, sx, sy, dep ? vy * vscale : (real)0, X.b0, X.b1,
+                       Y.a0, Y.a1, Z.b0, Z.b1);
+    scatter8_fixed_agg(J64z, dep ? X.b * sx + Y.b * sy + Z.a : -1, sx, sy, dep ? vz * vscale : (real)0, X.b0, X.b1,
+                       Y.b0, Y.b1, Z.a0, Z.a1);
+    bool depn = false;
     if (live) {
       advance(i, fx, vx * pc.hdt);
       advance(j, fy, vy * pc.hdt);
       advance(k, fz, vz * pc.hdt);
       if (in_array(g, i, j, k)) {
         if (stencil_ok(g, i, j, k)) {
-          const Axis<real> X1 = axis_weights(i, fx), Y1 = axis_weights(j, fy), Z1 = axis_weights(k, fz);
-          deposit_n(F, g, pc, X1, Y1, Z1);
+          depn = true;
+          X = axis_weights(i, fx); Y = axis_weights(j, fy); Z = axis_weights(k, fz);
         } else {
           count_err(err, ERR_DEPOSIT_OOB);
         }
       }
-      store_records(P, t, boundary(g, i, j, k) ? repack(i, j, k, err) : -1, fx, fy, fz, vx, vy, vz);
     }
+    // the density deposit (deposit_n), aggregated like J
+    scatter8_agg(F.f[pc.pn], depn ? X.b * sx + Y.b * sy + Z.b : -1, sx, sy, depn ? pc.nw : (real)0, X.b0, X.b1,
+                 Y.b0, Y.b1, Z.b0, Z.b1);
+    if (live) store_records(P, t, boundary(g, i, j, k) ? repack(i, j, k, err) : -1, fx, fy, fz, vx, vy, vz);
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
   if ((threadIdx.x & 31) == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
@@ -351,7 +349,7 @@ struct AdjPart {
 // push found them; F the fields it gathered (E at the step start, B after the
 // first half-step) and B0. acc[1] += dJ/dI, acc[2] += dJ/dV.
 template <typename real>
-__global__ void __launch_bounds__(256) push_adjoint_kernel(Parts<real> P, int n, Fields<real> F, Geom g,
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_adjoint_kernel(Parts<real> P, int n, Fields<real> F, Geom g,
                                                            PushConst<real> pc, AdjPart<real> A, AdjConst a,
                                                            double* acc) {
   double s[2] = {0.0, 0.0};
