@@ -347,16 +347,24 @@ def run_adjoint(nsteps: int = 200, every: int = 20):
         torch.cuda.synchronize()
         return r, time.perf_counter() - t0
 
-    P = ctx()
-    P.step(3)
-    _, t_step = timed(lambda: P.step(nsteps))
-    P.close()
-    P = ctx()
-    _, t_fwd = timed(lambda: P.objective(nsteps))
-    P.close()
-    P = ctx()
-    out, t_adj = timed(lambda: P.adjoint(nsteps, every))
-    P.close()
+    def best_of(reps, run, prep=None):
+        """Wall time of `run` on a fresh context, the fastest of `reps` runs
+        (single wall-clock runs of the adjoint, which reads the particle
+        counts back at every refill, varied by up to 2x on one box)."""
+        best, res = None, None
+        for _ in range(reps):
+            P = ctx()
+            if prep:
+                prep(P)
+            r, t = timed(lambda: run(P))
+            P.close()
+            if best is None or t < best:
+                best, res = t, r
+        return res, best
+
+    _, t_step = best_of(3, lambda P: P.step(nsteps), prep=lambda P: P.step(3))
+    _, t_fwd = best_of(3, lambda P: P.objective(nsteps))
+    out, t_adj = best_of(3, lambda P: P.adjoint(nsteps, every))
     checks = []
     h = 1e-3
     for T in (5, 20, 50, nsteps):
@@ -373,6 +381,7 @@ def run_adjoint(nsteps: int = 200, every: int = 20):
         checks.append({"steps": T, "dJ_dI": dI, "fd_dJ_dI": fdI, "rel_err_I": abs(dI / fdI - 1),
                        "dJ_dV": dV, "fd_dJ_dV": fdV, "rel_err_V": abs(dV / fdV - 1)})
     return {"workload": f"64^3 cells x 16 ppc/species, {nsteps} steps, checkpoint every {every}, FP32",
+            "timing": "wall clock, fastest of 3 runs on fresh contexts",
             "objective": "impulse along z delivered to the dipole", "J": out[0], "dJ_dI": out[1], "dJ_dV": out[2],
             "step_ms": t_step / nsteps * 1e3, "forward_ms": t_fwd / nsteps * 1e3, "adjoint_ms": t_adj / nsteps * 1e3,
             "adjoint_over_step": t_adj / t_step, "adjoint_over_forward": t_adj / t_fwd,
