@@ -364,10 +364,11 @@ def run_adjoint(nsteps: int = 200, every: int = 20):
 
     _, t_step = best_of(3, lambda P: P.step(nsteps), prep=lambda P: P.step(3))
     _, t_fwd = best_of(3, lambda P: P.objective(nsteps))
-    out, t_adj = best_of(3, lambda P: P.adjoint(nsteps, every))
+    # each timed adjoint follows one on the same context, whose snapshot and work memory it reuses
+    out, t_adj = best_of(3, lambda P: P.adjoint(nsteps, every), prep=lambda P: P.adjoint(nsteps, every))
     checks = []
     h = 1e-3
-    for T in (5, 20, 50, nsteps):
+    for T in sorted({T for T in (5, 20, 50, nsteps) if T <= nsteps}):
         P = ctx()
         J, dI, dV = P.adjoint(T, min(every, T))
         P.close()
@@ -381,8 +382,10 @@ def run_adjoint(nsteps: int = 200, every: int = 20):
         checks.append({"steps": T, "dJ_dI": dI, "fd_dJ_dI": fdI, "rel_err_I": abs(dI / fdI - 1),
                        "dJ_dV": dV, "fd_dJ_dV": fdV, "rel_err_V": abs(dV / fdV - 1)})
     return {"workload": f"64^3 cells x 16 ppc/species, {nsteps} steps, checkpoint every {every}, FP32",
-            "timing": "wall clock, fastest of 3 runs on fresh contexts",
-            "objective": "impulse along z delivered to the dipole", "J": out[0], "dJ_dI": out[1], "dJ_dV": out[2],
+            "timing": "wall clock, fastest of 3 runs on fresh contexts; the adjoint after a first adjoint on its context",
+            "objective": "impulse along z delivered to the dipole",
+            "timed_run": {"J": out[0], "dJ_dI": out[1], "dJ_dV": out[2],
+                          "start": f"the state after a first {nsteps}-step adjoint"},
             "step_ms": t_step / nsteps * 1e3, "forward_ms": t_fwd / nsteps * 1e3, "adjoint_ms": t_adj / nsteps * 1e3,
             "adjoint_over_step": t_adj / t_step, "adjoint_over_forward": t_adj / t_fwd,
             "fd_checks": checks}
@@ -454,6 +457,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--no-poisson", action="store_true", help="skip the Poisson cleaning measurement")
     ap.add_argument("--runs2d", type=int, default=256, help="runs of the batched 2D workload")
+    ap.add_argument("--adjoint-steps", type=int, default=200, help="steps of the adjoint measurement")
+    ap.add_argument("--adjoint-every", type=int, default=20, help="its checkpoint interval")
     args = ap.parse_args()
     global NX, NY, NZ, PPC
     NX = NY = NZ = args.grid
@@ -548,7 +553,7 @@ def main():
     adjoint = None
     if not args.no_adjoint and world == 1:
         try:
-            adjoint = run_adjoint()
+            adjoint = run_adjoint(args.adjoint_steps, args.adjoint_every)
         except Exception as exc:
             log("adjoint failed:", exc)
             adjoint = {"error": str(exc)[:200]}

@@ -215,8 +215,10 @@ int pic_fdtd(pic_ctx *ctx, int nsteps);
  * call it after pic_init_grid, pic_init_particle_flat and pic_fdtd(ctx, 0)).
  * The reverse pass keeps a checkpoint every checkpoint_every steps and
  * recomputes each segment, so device memory holds nsteps/checkpoint_every
- * full states plus checkpoint_every step inputs. The context ends in the state
- * after the nsteps loop bodies. */
+ * full states plus checkpoint_every step inputs. That memory and the
+ * adjoint's work arrays stay with the context after the call, for the next
+ * pic_objective / pic_adjoint to reuse, until pic_destroy. The context ends in
+ * the state after the nsteps loop bodies. */
 int pic_objective(pic_ctx *ctx, int nsteps, double *J);
 int pic_adjoint(pic_ctx *ctx, int nsteps, int checkpoint_every, double *out3);
 

@@ -26,12 +26,7 @@ struct AdjSnap {
 };
 
 struct AdjRun {
-  std::vector<void*> owned;
-  // snapshot blocks: allocated on first need, returned to `spare` when a
-  // snapshot is released and handed out again, freed with the run
-  std::vector<std::pair<void*, size_t>> spare;
-  std::vector<void*> snaps;
-  std::map<void*, size_t> snap_size;
+  std::vector<void*> owned;  // work blocks taken from the context's pool
   int* scan_tmp = nullptr;
   size_t scan_len = 0;
   void* lam[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [species][buffer]: lx[3] lv[3]
@@ -47,55 +42,54 @@ static_assert(F_EY == F_EX + 1 && F_EZ == F_EX + 2 && F_BX == F_EX + 3 && F_DBX 
                   F_DBZ == F_EX + 8,
               "E, B and DB planes are consecutive");
 
-int adj_alloc(pic_ctx* c, AdjRun& R, void** p, size_t bytes) {
-  CK(cudaMalloc(p, bytes < 256 ? 256 : bytes));
-  R.owned.push_back(*p);
-  return PIC_OK;
-}
-
-void adj_free(AdjRun& R) {
-  for (void* p : R.owned) cudaFree(p);
-  R.owned.clear();
-  for (void* p : R.snaps) cudaFree(p);
-  R.snaps.clear();
-  R.spare.clear();
-}
-
-// Snapshot memory: the smallest spare block that holds `bytes`, else a new
-// block with 1/16 headroom (particle counts drift by a little between steps)
-// rounded to 2 MB. A run allocates each block once: cudaMalloc and cudaFree
-// inside the loop would stall the stream at every step.
-int snap_alloc(pic_ctx* c, AdjRun& R, void** p, size_t bytes) {
-  size_t best = R.spare.size();
-  for (size_t q = 0; q < R.spare.size(); ++q)
-    if (R.spare[q].second >= bytes && (best == R.spare.size() || R.spare[q].second < R.spare[best].second)) best = q;
-  if (best < R.spare.size()) {
-    *p = R.spare[best].first;
-    R.snap_size[*p] = R.spare[best].second;
-    R.spare.erase(R.spare.begin() + (long)best);
+// A block of at least `bytes` from the context's pool: the smallest spare
+// block that holds it, else a new one with 1/16 headroom (particle counts
+// drift a little between steps) rounded to 2 MB.
+int pool_get(pic_ctx* c, void** p, size_t bytes) {
+  DevPool& P = c->adj_pool;
+  size_t best = P.spare.size();
+  for (size_t q = 0; q < P.spare.size(); ++q)
+    if (P.spare[q].second >= bytes && (best == P.spare.size() || P.spare[q].second < P.spare[best].second)) best = q;
+  if (best < P.spare.size()) {
+    *p = P.spare[best].first;
+    P.spare.erase(P.spare.begin() + (long)best);
     return PIC_OK;
   }
   const size_t want = ((bytes + bytes / 16) + ((size_t)1 << 21) - 1) & ~(((size_t)1 << 21) - 1);
   CK(cudaMalloc(p, want));
-  R.snaps.push_back(*p);
-  R.snap_size[*p] = want;
+  P.all.push_back(*p);
+  P.size[*p] = want;
   return PIC_OK;
 }
 
-void snap_release(AdjRun& R, void*& p) {
+void pool_put(pic_ctx* c, void*& p) {
   if (!p) return;
-  R.spare.emplace_back(p, R.snap_size[p]);
+  c->adj_pool.spare.emplace_back(p, c->adj_pool.size[p]);
   p = nullptr;
 }
 
-void snap_free(AdjRun& R, AdjSnap& S) {
+int adj_alloc(pic_ctx* c, AdjRun& R, void** p, size_t bytes) {
+  CKR(pool_get(c, p, bytes));
+  R.owned.push_back(*p);
+  return PIC_OK;
+}
+
+// Work memory back to the pool; the stream orders its reuse after this run.
+void adj_free(pic_ctx* c, AdjRun& R) {
+  for (void*& p : R.owned) pool_put(c, p);
+  R.owned.clear();
+}
+
+int snap_alloc(pic_ctx* c, void** p, size_t bytes) { return pool_get(c, p, bytes); }
+
+void snap_free(pic_ctx* c, AdjSnap& S) {
   for (int s = 0; s < 2; ++s) {
-    snap_release(R, S.part[s]);
+    pool_put(c, S.part[s]);
     void* m = S.map[s];
-    snap_release(R, m);
+    pool_put(c, m);
     S.map[s] = nullptr;
   }
-  snap_release(R, S.planes);
+  pool_put(c, S.planes);
 }
 
 template <typename real>
@@ -115,14 +109,14 @@ int copy_parts(pic_ctx* c, Parts<real> dst, Parts<real> src, long long n) {
 // The context's particles, fields (E, B, DB), random-stream counters and step
 // counters into a new snapshot.
 template <typename real>
-int adj_save(pic_ctx* c, AdjRun& R, AdjSnap& S) {
+int adj_save(pic_ctx* c, AdjSnap& S) {
   for (int s = 0; s < 2; ++s) {
     S.count[s] = c->sp[s].count;
-    CKR(snap_alloc(c, R, &S.part[s], store_bytes(S.count[s] > 0 ? S.count[s] : 1, c->rsize)));
+    CKR(snap_alloc(c, &S.part[s], store_bytes(S.count[s] > 0 ? S.count[s] : 1, c->rsize)));
     CKR(copy_parts<real>(c, parts_at<real>(S.part[s], S.count[s] > 0 ? S.count[s] : 1), parts<real>(c, s),
                          S.count[s]));
   }
-  CKR(snap_alloc(c, R, &S.planes, kSnapPlanes * c->plane_bytes));
+  CKR(snap_alloc(c, &S.planes, kSnapPlanes * c->plane_bytes));
   CK(cudaMemcpyAsync(S.planes, (char*)c->field_mem + (size_t)F_EX * c->plane_bytes,
                      kSnapPlanes * c->plane_bytes, cudaMemcpyDeviceToDevice, c->stream));
   S.ctr_p = c->ctr_p;
@@ -203,7 +197,7 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
       }
       int* map = nullptr;
       if (rec && st.count > 0) {
-        CKR(snap_alloc(c, R, (void**)&map, sizeof(int) * (size_t)st.count));
+        CKR(snap_alloc(c, (void**)&map, sizeof(int) * (size_t)st.count));
         rec->map[s] = map;
         rec->map_n[s] = st.count;
       }
@@ -214,7 +208,7 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
     c->c_add = 0;
   }
   if (rec) {
-    CKR(adj_save<real>(c, R, *rec));
+    CKR(adj_save<real>(c, *rec));
     rec->kept[0] = kept[0];
     rec->kept[1] = kept[1];
   }

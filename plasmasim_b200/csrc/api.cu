@@ -39,6 +39,16 @@ struct Store {
   int* count_dev = nullptr;
 };
 
+// Device blocks of the adjoint runs: each block is allocated on first need,
+// handed back to `spare` when a run releases it and reused by later runs of
+// the same context; pic_destroy frees them. cudaMalloc and cudaFree inside
+// the adjoint's loop would stall the stream at every step.
+struct DevPool {
+  std::vector<std::pair<void*, size_t>> spare;
+  std::vector<void*> all;
+  std::map<void*, size_t> size;
+};
+
 }  // namespace
 
 struct pic_ctx {
@@ -95,6 +105,8 @@ struct pic_ctx {
   int* mig_cnt = nullptr;
   int mig_cap = 0;
   unsigned long long* err = nullptr;  // ERR_COUNT
+  DevPool adj_pool;                   // the adjoint's work and snapshot memory
+  int* host_pin = nullptr;            // pinned read-back slots (re-layout spill counts)
   // import/export staging
   void* stage = nullptr;
   size_t stage_bytes = 0;
@@ -788,12 +800,15 @@ int do_sort_species(pic_ctx* c, int s) {
 }
 
 // In-place re-layout (relayout.cuh): movers and appended particles into the
-// holes of their columns; a full sort when there is no layout yet or some
-// column overflows.
+// holes of their columns. relayout_launch issues the kernels and the read-back
+// of the spill count into pinned host memory; relayout_finish, after the
+// stream has reached that read-back, sets the count and falls back to a full
+// sort when many particles found no hole. Both species are launched before
+// the one wait, so the second species' kernels cover the first one's
+// read-back.
 template <typename real>
-int do_relayout_species(pic_ctx* c, int s) {
+int relayout_launch(pic_ctx* c, int s) {
   Store& st = c->sp[s];
-  if (!c->layout[s]) return do_sort_species<real>(c, s);
   const TileGeom& tg = c->tg;
   const int gblocks = grid_blocks((long long)tg.ngroups * 32);
   const Parts<real> P = parts<real>(c, s);
@@ -818,9 +833,14 @@ int do_relayout_species(pic_ctx* c, int s) {
   CKL();
   unspill_kernel<real><<<particle_blocks(st.cap), kThreads, 0, c->stream>>>(Q, c->total_dev, P, (int)first);
   CKL();
-  int nspill = 0;
-  CK(cudaMemcpyAsync(&nspill, c->total_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpyAsync(c->host_pin + s, c->total_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  return PIC_OK;
+}
+
+template <typename real>
+int relayout_finish(pic_ctx* c, int s) {
+  const long long first = c->tiled_end[s];
+  const int nspill = c->host_pin[s];
   CKR(set_count(c, s, first + nspill));
   c->tiled[s] = true;
   // particles without a hole are pushed in slot order; many of them call for a sort
@@ -829,8 +849,23 @@ int do_relayout_species(pic_ctx* c, int s) {
 }
 
 template <typename real>
+int do_relayout_species(pic_ctx* c, int s) {
+  if (!c->layout[s]) return do_sort_species<real>(c, s);
+  CKR(relayout_launch<real>(c, s));
+  CK(cudaStreamSynchronize(c->stream));
+  return relayout_finish<real>(c, s);
+}
+
+template <typename real>
 int do_sort(pic_ctx* c) {
-  for (int s = 0; s < 2; ++s) CKR(do_relayout_species<real>(c, s));
+  bool launched[2] = {false, false};
+  for (int s = 0; s < 2; ++s) {
+    if (!c->layout[s]) continue;
+    CKR(relayout_launch<real>(c, s));
+    launched[s] = true;
+  }
+  if (launched[0] || launched[1]) CK(cudaStreamSynchronize(c->stream));
+  for (int s = 0; s < 2; ++s) CKR(launched[s] ? relayout_finish<real>(c, s) : do_sort_species<real>(c, s));
   return PIC_OK;
 }
 
@@ -1243,7 +1278,7 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
     for (int n = 0; n < nsteps; ++n) {
       if (grad && n % every == 0) {
         ck.emplace_back();
-        CKR(adj_save<real>(c, R, ck.back()));
+        CKR(adj_save<real>(c, ck.back()));
       }
       CKR(adj_forward_step<real>(c, R, nullptr));
     }
@@ -1252,7 +1287,7 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
     CK(cudaStreamSynchronize(c->stream));
     out[0] = h[0];
     if (!grad) return PIC_OK;
-    CKR(adj_save<real>(c, R, fin));
+    CKR(adj_save<real>(c, fin));
     // adjoint state: zero for the final state (the objective terms enter in the reverse kernels)
     for (int s = 0; s < 2; ++s)
       for (int b = 0; b < 2; ++b) {
@@ -1273,8 +1308,8 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
         rc = adj_reverse_step<real>(c, R, rec[n - n0]);
         if (rc == PIC_OK) rc = adj_unrefill<real>(c, R, rec[n - n0]);
       }
-      for (auto& S : rec) snap_free(R, S);
-      if (seg > 0) snap_free(R, ck[seg]);  // the first checkpoint's particles serve the drift gradient below
+      for (auto& S : rec) snap_free(c, S);
+      if (seg > 0) snap_free(c, ck[seg]);  // the first checkpoint's particles serve the drift gradient below
       if (rc != PIC_OK) return rc;
     }
     // the initial particles were created with vz = V + thermal
@@ -1294,7 +1329,9 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
   };
   const int rc = run();
   cudaStreamSynchronize(c->stream);
-  adj_free(R);
+  for (auto& S : ck) snap_free(c, S);
+  snap_free(c, fin);
+  adj_free(c, R);
   return rc;
 }
 
@@ -1407,6 +1444,7 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
     return code;
   };
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  if (cudaMallocHost(&c->host_pin, sizeof(int) * 16) != cudaSuccess) return fail(PIC_ERR_CUDA);
   c->plane_bytes = align256((size_t)g.nodes * c->rsize);
   if (cudaMalloc(&c->field_mem, c->plane_bytes * F_COUNT) != cudaSuccess) return fail(PIC_ERR_CUDA);
   cudaMemsetAsync(c->field_mem, 0, c->plane_bytes * F_COUNT, c->stream);
@@ -1487,6 +1525,8 @@ int pic_destroy(pic_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   cudaFree(c->field_mem);
   cudaFree(c->ramps);
+  for (void* p : c->adj_pool.all) cudaFree(p);
+  if (c->host_pin) cudaFreeHost(c->host_pin);
   for (int s = 0; s < 2; ++s) {
     cudaFree(c->sp[s].mem[0]);
     cudaFree(c->sp[s].mem[1]);
