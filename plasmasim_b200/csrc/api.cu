@@ -37,6 +37,10 @@ struct Store {
   long long cap = 0;
   long long count = 0;  // slots in use (live and empty), mirrored in *count_dev
   int* count_dev = nullptr;
+  // a re-layout has set *count_dev and is reading the spill count back into
+  // pinned memory; `count` is stale until relayout_resolve
+  bool pending = false;
+  cudaEvent_t readback = nullptr;
 };
 
 // Device blocks of the adjoint runs: each block is allocated on first need,
@@ -668,8 +672,11 @@ int do_renew_grid(pic_ctx* c) {
 // The slot-order push over slots [first, count) (global-memory atomics).
 template <typename real, int MODE>
 int do_push(pic_ctx* c, int s, long long first = 0) {
-  if (c->sp[s].count <= first) return PIC_OK;
-  push_kernel<real, MODE><<<particle_blocks(c->sp[s].count - first), kThreads, 0, c->stream>>>(
+  // with a re-layout's count still pending, the grid covers every slot up to
+  // the capacity and the kernel stops at *count_dev
+  const long long end = c->sp[s].pending ? c->sp[s].cap : c->sp[s].count;
+  if (end <= first) return PIC_OK;
+  push_kernel<real, MODE><<<particle_blocks(end - first), kThreads, 0, c->stream>>>(
       parts<real>(c, s), (int)first, c->sp[s].count_dev, fields<real>(c), c->g, push_const<real>(c, s),
       c->err);
   CKL();
@@ -800,12 +807,14 @@ int do_sort_species(pic_ctx* c, int s) {
 }
 
 // In-place re-layout (relayout.cuh): movers and appended particles into the
-// holes of their columns. relayout_launch issues the kernels and the read-back
-// of the spill count into pinned host memory; relayout_finish, after the
-// stream has reached that read-back, sets the count and falls back to a full
-// sort when many particles found no hole. Both species are launched before
-// the one wait, so the second species' kernels cover the first one's
-// read-back.
+// holes of their columns. relayout_launch issues the kernels, sets the new
+// count on the device and reads the spill count back into pinned memory
+// without waiting; relayout_resolve waits for that read-back, sets the host
+// count and falls back to a full sort when many particles found no hole.
+// do_step resolves after it has issued the push, so the wait overlaps the
+// push instead of leaving the GPU idle.
+__global__ void spill_count_kernel(int* count, int first, const int* nspill) { *count = first + *nspill; }
+
 template <typename real>
 int relayout_launch(pic_ctx* c, int s) {
   Store& st = c->sp[s];
@@ -833,40 +842,59 @@ int relayout_launch(pic_ctx* c, int s) {
   CKL();
   unspill_kernel<real><<<particle_blocks(st.cap), kThreads, 0, c->stream>>>(Q, c->total_dev, P, (int)first);
   CKL();
+  spill_count_kernel<<<1, 1, 0, c->stream>>>(st.count_dev, (int)first, c->total_dev);
+  CKL();
   CK(cudaMemcpyAsync(c->host_pin + s, c->total_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaEventRecord(st.readback, c->stream));
+  st.pending = true;
+  c->tiled[s] = true;
   return PIC_OK;
 }
 
 template <typename real>
-int relayout_finish(pic_ctx* c, int s) {
+int relayout_resolve(pic_ctx* c, int s) {
+  Store& st = c->sp[s];
+  if (!st.pending) return PIC_OK;
+  CK(cudaEventSynchronize(st.readback));
+  st.pending = false;
   const long long first = c->tiled_end[s];
   const int nspill = c->host_pin[s];
-  CKR(set_count(c, s, first + nspill));
-  c->tiled[s] = true;
+  st.count = first + nspill;  // *count_dev holds it already
   // particles without a hole are pushed in slot order; many of them call for a sort
   if (nspill > first / 50) return do_sort_species<real>(c, s);
   return PIC_OK;
 }
 
+// Re-layout of every species that needs one (a full sort for a species with
+// no layout yet), leaving the counts pending.
+template <typename real>
+int relayout_species(pic_ctx* c, const bool (&which)[2]) {
+  for (int s = 0; s < 2; ++s) {
+    if (!which[s]) continue;
+    if (c->layout[s]) CKR(relayout_launch<real>(c, s));
+    else CKR(do_sort_species<real>(c, s));
+  }
+  return PIC_OK;
+}
+
+template <typename real>
+int resolve_counts(pic_ctx* c) {
+  for (int s = 0; s < 2; ++s) CKR(relayout_resolve<real>(c, s));
+  return PIC_OK;
+}
+
 template <typename real>
 int do_relayout_species(pic_ctx* c, int s) {
-  if (!c->layout[s]) return do_sort_species<real>(c, s);
-  CKR(relayout_launch<real>(c, s));
-  CK(cudaStreamSynchronize(c->stream));
-  return relayout_finish<real>(c, s);
+  const bool which[2] = {s == 0, s == 1};
+  CKR(relayout_species<real>(c, which));
+  return resolve_counts<real>(c);
 }
 
 template <typename real>
 int do_sort(pic_ctx* c) {
-  bool launched[2] = {false, false};
-  for (int s = 0; s < 2; ++s) {
-    if (!c->layout[s]) continue;
-    CKR(relayout_launch<real>(c, s));
-    launched[s] = true;
-  }
-  if (launched[0] || launched[1]) CK(cudaStreamSynchronize(c->stream));
-  for (int s = 0; s < 2; ++s) CKR(launched[s] ? relayout_finish<real>(c, s) : do_sort_species<real>(c, s));
-  return PIC_OK;
+  const bool both[2] = {true, true};
+  CKR(relayout_species<real>(c, both));
+  return resolve_counts<real>(c);
 }
 
 // Generates `total` particles of species s from the slabs into slots
@@ -1077,13 +1105,15 @@ int do_step(pic_ctx* c) {
   CKR(phase_mark(c, PH_FIELD));
   if (!c->tiled[0] || !c->tiled[1]) {  // after a refill or an import
     CKR(phase_mark(c, PH_SORT));
-    for (int s = 0; s < 2; ++s)
-      if (!c->tiled[s]) CKR(do_relayout_species<real>(c, s));
+    const bool which[2] = {!c->tiled[0], !c->tiled[1]};
+    CKR(relayout_species<real>(c, which));
     CKR(phase_mark(c, PH_SORT));
   }
   CKR(phase_mark(c, PH_PUSH));
+  if (c->has_xport) CKR(resolve_counts<real>(c));  // the exchange lists are sized from the counts
   if (c->has_xport) CKR(ensure_mig<real>(c));
   for (int s = 0; s < 2; ++s) CKR(do_push_tiled<real>(c, s));
+  CKR(resolve_counts<real>(c));  // waits for the re-layout's read-back while the GPU pushes
   if (c->has_xport) CKR(do_migrate<real>(c));  // sr_particle's exchange between ranks
   CKR(phase_mark(c, PH_PUSH));
   CKR(phase_mark(c, PH_FIELD));
@@ -1445,6 +1475,8 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
   };
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PIC_ERR_CUDA);
   if (cudaMallocHost(&c->host_pin, sizeof(int) * 16) != cudaSuccess) return fail(PIC_ERR_CUDA);
+  for (int s = 0; s < 2; ++s)
+    if (cudaEventCreateWithFlags(&c->sp[s].readback, cudaEventDisableTiming) != cudaSuccess) return fail(PIC_ERR_CUDA);
   c->plane_bytes = align256((size_t)g.nodes * c->rsize);
   if (cudaMalloc(&c->field_mem, c->plane_bytes * F_COUNT) != cudaSuccess) return fail(PIC_ERR_CUDA);
   cudaMemsetAsync(c->field_mem, 0, c->plane_bytes * F_COUNT, c->stream);
@@ -1527,6 +1559,8 @@ int pic_destroy(pic_ctx* c) {
   cudaFree(c->ramps);
   for (void* p : c->adj_pool.all) cudaFree(p);
   if (c->host_pin) cudaFreeHost(c->host_pin);
+  for (int s = 0; s < 2; ++s)
+    if (c->sp[s].readback) cudaEventDestroy(c->sp[s].readback);
   for (int s = 0; s < 2; ++s) {
     cudaFree(c->sp[s].mem[0]);
     cudaFree(c->sp[s].mem[1]);
