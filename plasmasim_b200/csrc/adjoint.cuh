@@ -153,10 +153,11 @@ __device__ __forceinline__ void scatter8_agg(real* F, int key, int sx, int sy, r
 // push_kernel<real, PUSH_FUSED> with the J deposit into fixed-point planes
 // J64[3] (v scaled by 2^40 / c).
 template <typename real>
-__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_fixed_kernel(Parts<real> P, int n, Fields<real> F, Geom g,
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_fixed_kernel(Parts<real> P, const int* count, Fields<real> F, Geom g,
                                                          PushConst<real> pc, unsigned long long* J64x,
                                                          unsigned long long* J64y, unsigned long long* J64z,
                                                          real vscale, unsigned long long* err) {
+  const int n = *count;
   unsigned pushed = 0;
   const int sx = g.sx, sy = g.gz;
   const int lane = threadIdx.x & 31;
@@ -717,6 +718,13 @@ __global__ void fold_y_adjoint(PlaneSet<real> s, Geom g) {
 // Stable compaction with its slot map (the adjoint run's refill): map[t] is
 // the new slot of live slot t, -1 for an empty one. pos = exclusive scan of
 // the live flags.
+// The count after compact_kernel: the last slot's position plus its flag.
+__global__ void compact_count_kernel(int* count, const int* __restrict__ pos, const int* __restrict__ flag, int n) {
+  *count = pos[n - 1] + flag[n - 1];
+}
+
+__global__ void add_count_kernel(int* count, int add) { *count += add; }
+
 template <typename real>
 __global__ void compact_kernel(Parts<real> P, int n, const int* __restrict__ pos, Parts<real> Q, int* map) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;

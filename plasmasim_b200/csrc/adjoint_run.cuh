@@ -16,6 +16,7 @@
 
 struct AdjSnap {
   long long count[2] = {0, 0};
+  long long slots[2] = {0, 0};       // record slots of part[s] (>= count[s]): the layout parts_at needs
   void* part[2] = {nullptr, nullptr};
   void* planes = nullptr;            // E, B, DB (nine consecutive planes from F_EX)
   int* map[2] = {nullptr, nullptr};  // the refill's compaction map (old slot -> new slot), or null
@@ -27,6 +28,10 @@ struct AdjSnap {
 
 struct AdjRun {
   std::vector<void*> owned;  // work blocks taken from the context's pool
+  // a refill's compaction count is read back without waiting: until
+  // adj_resolve, sp[s].count is an upper bound and *count_dev the count
+  bool pend[2] = {false, false};
+  long long pend_added[2] = {0, 0};  // particles appended after the compaction
   int* scan_tmp = nullptr;
   size_t scan_len = 0;
   void* lam[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [species][buffer]: lx[3] lv[3]
@@ -112,9 +117,9 @@ template <typename real>
 int adj_save(pic_ctx* c, AdjSnap& S) {
   for (int s = 0; s < 2; ++s) {
     S.count[s] = c->sp[s].count;
-    CKR(snap_alloc(c, &S.part[s], store_bytes(S.count[s] > 0 ? S.count[s] : 1, c->rsize)));
-    CKR(copy_parts<real>(c, parts_at<real>(S.part[s], S.count[s] > 0 ? S.count[s] : 1), parts<real>(c, s),
-                         S.count[s]));
+    S.slots[s] = S.count[s] > 0 ? S.count[s] : 1;
+    CKR(snap_alloc(c, &S.part[s], store_bytes(S.slots[s], c->rsize)));
+    CKR(copy_parts<real>(c, parts_at<real>(S.part[s], S.slots[s]), parts<real>(c, s), S.count[s]));
   }
   CKR(snap_alloc(c, &S.planes, kSnapPlanes * c->plane_bytes));
   CK(cudaMemcpyAsync(S.planes, (char*)c->field_mem + (size_t)F_EX * c->plane_bytes,
@@ -130,8 +135,7 @@ template <typename real>
 int adj_restore(pic_ctx* c, const AdjSnap& S) {
   for (int s = 0; s < 2; ++s) {
     if (S.count[s] > c->sp[s].cap) return PIC_ERR_CAPACITY;
-    CKR(copy_parts<real>(c, parts<real>(c, s), parts_at<real>(S.part[s], S.count[s] > 0 ? S.count[s] : 1),
-                         S.count[s]));
+    CKR(copy_parts<real>(c, parts<real>(c, s), parts_at<real>(S.part[s], S.slots[s]), S.count[s]));
     CKR(set_count(c, s, S.count[s]));
     c->tiled[s] = false;
     c->layout[s] = false;
@@ -157,7 +161,8 @@ AdjConst adj_const(const pic_ctx* c, int s) {
 }
 
 // Removes the empty slots of species s, keeping the order of the rest, and
-// records the slot map in `map` when it is not null.
+// records the slot map in `map` when it is not null. The new count is set on
+// the device and read back into pinned memory without waiting (adj_resolve).
 template <typename real>
 int adj_compact(pic_ctx* c, AdjRun& R, int s, int* map) {
   Store& st = c->sp[s];
@@ -172,12 +177,56 @@ int adj_compact(pic_ctx* c, AdjRun& R, int s, int* map) {
   compact_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, c->pos,
                                                                     parts<real>(c, s, 1 - st.cur), map);
   CKL();
-  int h[2] = {0, 0};
-  CK(cudaMemcpyAsync(&h[0], c->pos + n - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(&h[1], c->flags + n - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  compact_count_kernel<<<1, 1, 0, c->stream>>>(st.count_dev, c->pos, c->flags, (int)n);
+  CKL();
+  CK(cudaMemcpyAsync(c->host_pin + 2 + s, st.count_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaEventRecord(st.readback, c->stream));
   st.cur = 1 - st.cur;
-  return set_count(c, s, (long long)h[0] + h[1]);
+  c->tiled[s] = false;
+  c->layout[s] = false;
+  R.pend[s] = true;
+  R.pend_added[s] = 0;
+  return PIC_OK;
+}
+
+// The refill's appended particles after a pending compaction: placed from the
+// device count, which they then extend; the host count stays an upper bound.
+template <typename real>
+int adj_source(pic_ctx* c, AdjRun& R, int s, const Slab* slabs, int nslab) {
+  if (!R.pend[s]) return do_source<real>(c, s, slabs, nslab);
+  SourceParams sp = source_params(c, s, slabs, nslab, 0);
+  const long long total = sp.total;
+  if (total == 0) return PIC_OK;
+  Store& st = c->sp[s];
+  if (st.count + total > st.cap) return PIC_ERR_CAPACITY;
+  sp.dst_dev = st.count_dev;
+  source_kernel<real><<<grid_blocks(total), kThreads, 0, c->stream>>>(parts<real>(c, s), sp, c->err);
+  CKL();
+  add_count_kernel<<<1, 1, 0, c->stream>>>(st.count_dev, (int)total);
+  CKL();
+  c->ctr_p += 3 * total;
+  c->ctr_v += 6 * total;
+  st.count += total;
+  R.pend_added[s] += total;
+  return PIC_OK;
+}
+
+// Waits for pending compaction counts and sets the host counts (and, with
+// `rec`, the recorded step input's counts and kept slots).
+int adj_resolve(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
+  for (int s = 0; s < 2; ++s) {
+    if (!R.pend[s]) continue;
+    Store& st = c->sp[s];
+    CK(cudaEventSynchronize(st.readback));
+    R.pend[s] = false;
+    const long long kept = c->host_pin[2 + s];  // read back before the appends
+    st.count = kept + R.pend_added[s];
+    if (rec) {
+      rec->kept[s] = kept;
+      rec->count[s] = st.count;
+    }
+  }
+  return PIC_OK;
 }
 
 // One slot-stable loop body; with `rec`, the step input goes into it.
@@ -202,8 +251,7 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
         rec->map_n[s] = st.count;
       }
       CKR(adj_compact<real>(c, R, s, map));
-      kept[s] = st.count;
-      CKR(do_source<real>(c, s, slabs, 5));
+      CKR(adj_source<real>(c, R, s, slabs, 5));
     }
     c->c_add = 0;
   }
@@ -216,18 +264,19 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
   const int nodes = c->g.nodes;
   Fields<real> F = fields<real>(c);
   for (int s = 0; s < 2; ++s) {
-    const long long n = c->sp[s].count;
+    const long long n = c->sp[s].count;  // an upper bound while a compaction count is pending
     if (n == 0) continue;
     const PushConst<real> pc = push_const<real>(c, s);
     CK(cudaMemsetAsync(R.j64, 0, sizeof(unsigned long long) * 3 * (size_t)nodes, c->stream));
     push_fixed_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
-        parts<real>(c, s), (int)n, F, c->g, pc, R.j64, R.j64 + nodes, R.j64 + 2 * (size_t)nodes,
+        parts<real>(c, s), c->sp[s].count_dev, F, c->g, pc, R.j64, R.j64 + nodes, R.j64 + 2 * (size_t)nodes,
         (real)(kJFixed / c->cfg.c), c->err);
     CKL();
     jconvert_kernel<real><<<grid_blocks(nodes), kThreads, 0, c->stream>>>(
         R.j64, nodes, F.f[pc.pjx], F.f[pc.pjy], F.f[pc.pjz], c->cfg.q * species_weight(c) * c->cfg.c / kJFixed);
     CKL();
   }
+  CKR(adj_resolve(c, R, rec));  // waits for the refill's counts while the GPU pushes
   CKR(do_renew_b<real>(c));
   CKR(do_fold<real>(c));
   CKR(do_renew_e<real>(c));
@@ -341,7 +390,7 @@ int adj_reverse_step(pic_ctx* c, AdjRun& R, const AdjSnap& in) {
     const long long n = in.count[s];
     if (n == 0) continue;
     push_adjoint_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
-        parts_at<real>(in.part[s], n), (int)n, fields<real>(c), c->g, push_const<real>(c, s),
+        parts_at<real>(in.part[s], in.slots[s]), (int)n, fields<real>(c), c->g, push_const<real>(c, s),
         adj_part<real>(c, R, s, R.lcur[s]), adj_const(c, s), R.acc);
     CKL();
   }
@@ -358,7 +407,7 @@ int adj_unrefill(pic_ctx* c, AdjRun& R, const AdjSnap& in) {
     if (in.count[s] > in.kept[s]) {
       const AdjPart<real> A = adj_part<real>(c, R, s, R.lcur[s]);
       drift_grad_kernel<real><<<particle_blocks(in.count[s] - in.kept[s]), kThreads, 0, c->stream>>>(
-          parts_at<real>(in.part[s], in.count[s]), A.lv[2], (int)in.kept[s], (int)in.count[s], R.acc);
+          parts_at<real>(in.part[s], in.slots[s]), A.lv[2], (int)in.kept[s], (int)in.count[s], R.acc);
       CKL();
     }
     if (in.map[s]) {

@@ -1348,7 +1348,7 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
       if (n == 0) continue;
       const AdjPart<real> A = adj_part<real>(c, R, s, R.lcur[s]);
       drift_grad_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
-          parts_at<real>(ck[0].part[s], n), A.lv[2], 0, (int)n, R.acc);
+          parts_at<real>(ck[0].part[s], ck[0].slots[s]), A.lv[2], 0, (int)n, R.acc);
       CKL();
     }
     CK(cudaMemcpyAsync(h, R.acc, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));

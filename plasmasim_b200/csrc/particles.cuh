@@ -455,6 +455,7 @@ struct SourceParams {
   uint64_t seed_p, seed_v;
   long long base_p, base_v;  // first draw index on each stream
   int dst;                // first slot written
+  const int* dst_dev;     // when set, the first slot is *dst_dev (a count known only on the device)
   int init_form;          // 1: cell bounds as init_particle_flat writes them, 2dx + k dx (:475)
 };
 
@@ -535,7 +536,7 @@ __global__ void source_kernel(Parts<real> P, SourceParams sp, unsigned long long
   const int l = (int)(r % sl.nl);
   const int k = (int)(r / sl.nl);
   const int cc[3] = {k + sl.k0, l + sl.l0, m + sl.m0};
-  make_particle(P, sp, t, cc, sp.dst + (int)t, err);
+  make_particle(P, sp, t, cc, (sp.dst_dev ? *sp.dst_dev : sp.dst) + (int)t, err);
 }
 
 // ------------------------------------------------------------------- sort
