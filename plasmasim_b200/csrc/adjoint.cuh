@@ -718,30 +718,35 @@ __global__ void fold_y_adjoint(PlaneSet<real> s, Geom g) {
 // Stable compaction with its slot map (the adjoint run's refill): map[t] is
 // the new slot of live slot t, -1 for an empty one. pos = exclusive scan of
 // the live flags.
-// The count after compact_kernel: the last slot's position plus its flag.
-__global__ void compact_count_kernel(int* count, const int* __restrict__ pos, const int* __restrict__ flag, int n) {
-  *count = pos[n - 1] + flag[n - 1];
+// Sort keys of the refill's compaction: the cell index of a live slot, past
+// every cell for an empty one; the values are the slot indices.
+constexpr int kDeadKey = 0x7fffffff;
+
+template <typename real>
+__global__ void cell_key_kernel(Parts<real> P, int n, int* key, int* slot) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int c = P.cell[t];
+  key[t] = c >= 0 ? c : kDeadKey;
+  slot[t] = t;
+}
+
+// Slot j of Q takes the particle of sorted position j; map[old slot] = j, or
+// -1 for an empty slot; *count = the live particles (the first dead key).
+template <typename real>
+__global__ void cell_gather_kernel(Parts<real> P, int n, const int* __restrict__ key, const int* __restrict__ slot,
+                                   Parts<real> Q, int* map, int* count) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int k = key[j], old = slot[j];
+  const bool live = k != kDeadKey;
+  if (live) copy_record(P, old, Q, j, k);
+  if (map) map[old] = live ? j : -1;
+  if (live && (j == n - 1 || key[j + 1] == kDeadKey)) *count = j + 1;
+  if (j == 0 && !live) *count = 0;
 }
 
 __global__ void add_count_kernel(int* count, int add) { *count += add; }
 
-template <typename real>
-__global__ void compact_kernel(Parts<real> P, int n, const int* __restrict__ pos, Parts<real> Q, int* map) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int c = P.cell[t];
-  if (c < 0) {
-    if (map) map[t] = -1;
-    return;
-  }
-  const int d = pos[t];
-  if (map) map[t] = d;
-  Q.cell[d] = c;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    Q.o[a][d] = P.o[a][t];
-    Q.v[a][d] = P.v[a][t];
-  }
-}
 
 }  // namespace pb

@@ -1,5 +1,6 @@
 // Host side of the adjoint run (pic_adjoint / pic_objective), included by
-// api.cu after the step functions it reuses.
+// api.cu after the step functions it reuses (api.cu includes CUB's radix sort
+// at file scope for adj_compact).
 //
 // Forward: the loop body of fdtd (:687-949) in slot-stable form: the push is
 // the one-thread-per-particle fused kernel over the slots, sorting is left out
@@ -28,6 +29,12 @@ struct AdjSnap {
 
 struct AdjRun {
   std::vector<void*> owned;  // work blocks taken from the context's pool
+  // the refill's cell sort: keys and slots (double-buffered) and the radix
+  // sort's temporary storage
+  int* skey[2] = {nullptr, nullptr};
+  int* sslot[2] = {nullptr, nullptr};
+  void* sort_tmp = nullptr;
+  size_t sort_bytes = 0;
   // a refill's compaction count is read back without waiting: until
   // adj_resolve, sp[s].count is an upper bound and *count_dev the count
   bool pend[2] = {false, false};
@@ -160,24 +167,27 @@ AdjConst adj_const(const pic_ctx* c, int s) {
   return a;
 }
 
-// Removes the empty slots of species s, keeping the order of the rest, and
-// records the slot map in `map` when it is not null. The new count is set on
-// the device and read back into pinned memory without waiting (adj_resolve).
+// Removes the empty slots of species s and orders the rest by cell (a stable
+// radix sort on the cell index, so a replayed segment gets the same order),
+// recording the slot map in `map` when it is not null. Cell order keeps the
+// lanes of a warp on few stencil bases, which the aggregated scatters of the
+// adjoint kernels need; between refills the slots drift apart as particles
+// move. The new count is set on the device and read back into pinned memory
+// without waiting (adj_resolve).
 template <typename real>
 int adj_compact(pic_ctx* c, AdjRun& R, int s, int* map) {
   Store& st = c->sp[s];
   const long long n = st.count;
   if (n == 0) return PIC_OK;
-  CKR(ensure_flags(c, (size_t)n));
-  live_flag_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, c->flags);
+  cell_key_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, R.skey[0], R.sslot[0]);
   CKL();
-  const long long tiles = (n + kScanTile - 1) / kScanTile;
-  if ((size_t)(2 * tiles + 64) > R.scan_len) return PIC_ERR_STATE;
-  CKR(scan_exclusive(c, c->flags, c->pos, n, R.scan_tmp, R.scan_len));
-  compact_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, c->pos,
-                                                                    parts<real>(c, s, 1 - st.cur), map);
-  CKL();
-  compact_count_kernel<<<1, 1, 0, c->stream>>>(st.count_dev, c->pos, c->flags, (int)n);
+  size_t bytes = R.sort_bytes;
+  CK(cub::DeviceRadixSort::SortPairs(R.sort_tmp, bytes, R.skey[0], R.skey[1], R.sslot[0], R.sslot[1], (int)n, 0, 31,
+                                     c->stream));
+  ++c->launches;
+  cell_gather_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, R.skey[1],
+                                                                        R.sslot[1], parts<real>(c, s, 1 - st.cur),
+                                                                        map, st.count_dev);
   CKL();
   CK(cudaMemcpyAsync(c->host_pin + 2 + s, st.count_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaEventRecord(st.readback, c->stream));

@@ -10,6 +10,7 @@
 #include <new>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cudaTypedefs.h>
 
 #include "../../include/plasma_b200.h"
@@ -1301,6 +1302,13 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
     const long long capmax = c->sp[0].cap > c->sp[1].cap ? c->sp[0].cap : c->sp[1].cap;
     R.scan_len = (size_t)(2 * ((capmax + kScanTile - 1) / kScanTile) + 64);
     CKR(adj_alloc(c, R, (void**)&R.scan_tmp, sizeof(int) * R.scan_len));
+    for (int b = 0; b < 2; ++b) {
+      CKR(adj_alloc(c, R, (void**)&R.skey[b], sizeof(int) * (size_t)capmax));
+      CKR(adj_alloc(c, R, (void**)&R.sslot[b], sizeof(int) * (size_t)capmax));
+    }
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, R.sort_bytes, R.skey[0], R.skey[1], R.sslot[0], R.sslot[1],
+                                       (int)capmax, 0, 31, c->stream));
+    CKR(adj_alloc(c, R, &R.sort_tmp, R.sort_bytes));
     CKR(adj_alloc(c, R, (void**)&R.acc, sizeof(double) * 4));
     CKR(adj_alloc(c, R, (void**)&R.j64, sizeof(unsigned long long) * 3 * (size_t)c->g.nodes));
     CK(cudaMemsetAsync(R.acc, 0, sizeof(double) * 4, c->stream));
