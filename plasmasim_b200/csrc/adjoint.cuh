@@ -156,7 +156,7 @@ template <typename real>
 __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_fixed_kernel(Parts<real> P, const int* count, Fields<real> F, Geom g,
                                                          PushConst<real> pc, unsigned long long* J64x,
                                                          unsigned long long* J64y, unsigned long long* J64z,
-                                                         real vscale, unsigned long long* err) {
+                                                         real vscale, int with_n, unsigned long long* err) {
   const int n = *count;
   unsigned pushed = 0;
   const int sx = g.sx, sy = g.gz;
@@ -218,9 +218,10 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_fixed_ker
         }
       }
     }
-    // the density deposit (deposit_n), aggregated like J
-    scatter8_agg(F.f[pc.pn], depn ? X.b * sx + Y.b * sy + Z.b : -1, sx, sy, depn ? pc.nw : (real)0, X.b0, X.b1,
-                 Y.b0, Y.b1, Z.b0, Z.b1);
+    // the density deposit (deposit_n), aggregated like J; a recomputed step skips it (no adjoint reads n)
+    if (with_n)
+      scatter8_agg(F.f[pc.pn], depn ? X.b * sx + Y.b * sy + Z.b : -1, sx, sy, depn ? pc.nw : (real)0, X.b0, X.b1,
+                   Y.b0, Y.b1, Z.b0, Z.b1);
     if (live) store_records(P, t, boundary(g, i, j, k) ? repack(i, j, k, err) : -1, fx, fy, fz, vx, vy, vz);
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
@@ -342,7 +343,8 @@ struct AdjPart {
   real* lv[3];          // dJ/dv
   const real* lj[3];    // dJ/dJ_ion of the three current planes (after the fold's transpose)
   real* le[3];          // dJ/dE at the step start (accumulated)
-  real* ldb[3];         // dJ/dDB after the first B half-step (accumulated)
+  real* ldb[3];         // this step's particle terms of dJ/dDB (three zeroed planes; ldb_merge_kernel adds
+                        // them to dJ/dDB after the first B half-step)
 };
 
 // Reverse of push_kernel<real, PUSH_FUSED> for one species, plus the
@@ -463,10 +465,6 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_adjoint_k
         ax[0] += af[q] * fv.gx;
         ax[1] += af[q] * fv.gy;
         ax[2] += af[q] * fv.gz;
-        if (q >= 3) {  // B = B0 + DB: the dipole part of B0 is proportional to I
-          const real b0 = trilerp(F.f[F_B0X + q - 3], st.n, sx, sy, st.x0, st.x1, st.y0, st.y1, st.z0, st.z1);
-          s[0] += (double)af[q] * ((double)b0 - a.imf[q - 3]) * a.inv_I;
-        }
       }
       scatter8_agg(dst[q], gat ? st.n : -1, sx, sy, gat ? af[q] : (real)0, st.x0, st.x1, st.y0, st.y1, st.z0,
                    st.z1);
@@ -540,6 +538,31 @@ struct AdjField {
   real* lj[3];
   real* w[3];   // scratch planes (zero outside the interior)
 };
+
+// The particles' dJ/dDB terms T of one reverse step into lDB, T zeroed for
+// the next step, and acc[1] += sum over nodes of T (B0 - IMF) / I: B = B0 +
+// DB, and the dipole part of B0 is proportional to I. Summing T (B0 - IMF) per
+// node equals summing each particle's term with B0 interpolated at the
+// particle, because the interpolation weights of a particle are the weights
+// of its scatter and add up to one.
+template <typename real>
+__global__ void __launch_bounds__(256) ldb_merge_kernel(Fields<real> F, AdjPart<real> T, AdjField<real> A, int nodes,
+                                                        AdjConst a, double* acc) {
+  double s[1] = {0.0};
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nodes; n += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const real t = T.ldb[q][n];
+      if (t == (real)0) continue;
+      A.ldb[q][n] += t;
+      T.ldb[q][n] = (real)0;
+      s[0] += (double)t * ((double)F.f[F_B0X + q][n] - a.imf[q]);
+    }
+  }
+  const int idx[1] = {1};
+  const double scale[1] = {a.inv_I};
+  block_reduce_add<1>(s, acc, idx, scale);
+}
 
 // Reverse of renew_e_kernel, part 1 (pointwise on interior nodes):
 // W = cb c24 lE, lJ_ion = -cb mu0 lE, lE = ca lE.

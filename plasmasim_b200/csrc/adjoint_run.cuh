@@ -35,6 +35,8 @@ struct AdjRun {
   int* sslot[2] = {nullptr, nullptr};
   void* sort_tmp = nullptr;
   size_t sort_bytes = 0;
+  void* jn_final = nullptr;  // J_i, J_e, n_i, n_e after the forward sweep
+  void* tdb = nullptr;       // three planes: one reverse step's particle terms of dJ/dDB
   // a refill's compaction count is read back without waiting: until
   // adj_resolve, sp[s].count is an upper bound and *count_dev the count
   bool pend[2] = {false, false};
@@ -280,7 +282,7 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
     CK(cudaMemsetAsync(R.j64, 0, sizeof(unsigned long long) * 3 * (size_t)nodes, c->stream));
     push_fixed_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
         parts<real>(c, s), c->sp[s].count_dev, F, c->g, pc, R.j64, R.j64 + nodes, R.j64 + 2 * (size_t)nodes,
-        (real)(kJFixed / c->cfg.c), c->err);
+        (real)(kJFixed / c->cfg.c), rec ? 0 : 1, c->err);
     CKL();
     jconvert_kernel<real><<<grid_blocks(nodes), kThreads, 0, c->stream>>>(
         R.j64, nodes, F.f[pc.pjx], F.f[pc.pjy], F.f[pc.pjz], c->cfg.q * species_weight(c) * c->cfg.c / kJFixed);
@@ -290,7 +292,8 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
   CKR(do_renew_b<real>(c));
   CKR(do_fold<real>(c));
   CKR(do_renew_e<real>(c));
-  for (int s = 0; s < 2; ++s) {
+  // the objective: in the forward sweep only (a recomputed step's terms are known)
+  for (int s = 0; s < 2 && !rec; ++s) {
     const long long n = c->sp[s].count;
     if (n == 0) continue;
     objective_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n,
@@ -399,9 +402,18 @@ int adj_reverse_step(pic_ctx* c, AdjRun& R, const AdjSnap& in) {
   for (int s = 0; s < 2; ++s) {
     const long long n = in.count[s];
     if (n == 0) continue;
+    AdjPart<real> A = adj_part<real>(c, R, s, R.lcur[s]);
+    for (int q = 0; q < 3; ++q) A.ldb[q] = (real*)((char*)R.tdb + (size_t)q * c->plane_bytes);
     push_adjoint_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
-        parts_at<real>(in.part[s], in.slots[s]), (int)n, fields<real>(c), c->g, push_const<real>(c, s),
-        adj_part<real>(c, R, s, R.lcur[s]), adj_const(c, s), R.acc);
+        parts_at<real>(in.part[s], in.slots[s]), (int)n, fields<real>(c), c->g, push_const<real>(c, s), A,
+        adj_const(c, s), R.acc);
+    CKL();
+  }
+  {
+    AdjPart<real> T{};
+    for (int q = 0; q < 3; ++q) T.ldb[q] = (real*)((char*)R.tdb + (size_t)q * c->plane_bytes);
+    ldb_merge_kernel<real><<<particle_blocks(c->g.nodes), kThreads, 0, c->stream>>>(
+        fields<real>(c), T, adj_field<real>(c, R), c->g.nodes, adj_const(c, 0), R.acc);
     CKL();
   }
   CKR(adj_renew_b<real>(c, R));  // first B half-step

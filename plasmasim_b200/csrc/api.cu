@@ -1326,6 +1326,10 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
     out[0] = h[0];
     if (!grad) return PIC_OK;
     CKR(adj_save<real>(c, fin));
+    // the final J and n planes, which the recomputed segments overwrite
+    CKR(adj_alloc(c, R, &R.jn_final, 8 * c->plane_bytes));
+    CK(cudaMemcpyAsync(R.jn_final, (char*)c->field_mem + (size_t)F_JIX * c->plane_bytes, 8 * c->plane_bytes,
+                       cudaMemcpyDeviceToDevice, c->stream));
     // adjoint state: zero for the final state (the objective terms enter in the reverse kernels)
     for (int s = 0; s < 2; ++s)
       for (int b = 0; b < 2; ++b) {
@@ -1335,6 +1339,8 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
       }
     CKR(adj_alloc(c, R, &R.lfield, 12 * c->plane_bytes));
     CK(cudaMemsetAsync(R.lfield, 0, 12 * c->plane_bytes, c->stream));
+    CKR(adj_alloc(c, R, &R.tdb, 3 * c->plane_bytes));
+    CK(cudaMemsetAsync(R.tdb, 0, 3 * c->plane_bytes, c->stream));
     CK(cudaMemsetAsync(R.acc, 0, sizeof(double) * 4, c->stream));
     for (int seg = (int)ck.size() - 1; seg >= 0; --seg) {
       const int n0 = seg * every, n1 = n0 + every < nsteps ? n0 + every : nsteps;
@@ -1363,6 +1369,8 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
     CK(cudaStreamSynchronize(c->stream));
     out[1] = h[1];
     out[2] = h[2];
+    CK(cudaMemcpyAsync((char*)c->field_mem + (size_t)F_JIX * c->plane_bytes, R.jn_final, 8 * c->plane_bytes,
+                       cudaMemcpyDeviceToDevice, c->stream));
     return adj_restore<real>(c, fin);
   };
   const int rc = run();
