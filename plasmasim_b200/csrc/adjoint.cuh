@@ -156,9 +156,11 @@ template <typename real>
 __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_fixed_kernel(Parts<real> P, const int* count, Fields<real> F, Geom g,
                                                          PushConst<real> pc, unsigned long long* J64x,
                                                          unsigned long long* J64y, unsigned long long* J64z,
-                                                         real vscale, int with_n, unsigned long long* err) {
+                                                         real vscale, int with_n, AdjConst a, double* obj,
+                                                         unsigned long long* err) {
   const int n = *count;
   unsigned pushed = 0;
+  double fobj = 0.0;
   const int sx = g.sx, sy = g.gz;
   const int lane = threadIdx.x & 31;
   // warp-uniform trip count: the J deposit is aggregated across the warp
@@ -218,14 +220,31 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_fixed_ker
         }
       }
     }
-    // the density deposit (deposit_n), aggregated like J; a recomputed step skips it (no adjoint reads n)
+    // the density deposit (deposit_n), aggregated like J; only where the caller asks for n
     if (with_n)
       scatter8_agg(F.f[pc.pn], depn ? X.b * sx + Y.b * sy + Z.b : -1, sx, sy, depn ? pc.nw : (real)0, X.b0, X.b1,
                    Y.b0, Y.b1, Z.b0, Z.b1);
-    if (live) store_records(P, t, boundary(g, i, j, k) ? repack(i, j, k, err) : -1, fx, fy, fz, vx, vy, vz);
+    if (live) {
+      const int cell = boundary(g, i, j, k) ? repack(i, j, k, err) : -1;
+      store_records(P, t, cell, fx, fy, fz, vx, vy, vz);
+      // F of this particle after the step (times K dt in the block sum) when obj is given: the objective
+      if (obj && cell >= 0 && stencil_ok(g, i, j, k)) {
+        const Axis<real> X2 = axis_weights(i, fx), Y2 = axis_weights(j, fy), Z2 = axis_weights(k, fz);
+        const Stagger<real> bxs = stagger(g, X2, Y2, Z2, 3), bys = stagger(g, X2, Y2, Z2, 4);
+        const double b0x = trilerp(F.f[F_B0X], bxs.n, sx, sy, bxs.x0, bxs.x1, bxs.y0, bxs.y1, bxs.z0, bxs.z1);
+        const double b0y = trilerp(F.f[F_B0Y], bys.n, sx, sy, bys.x0, bys.x1, bys.y0, bys.y1, bys.z0, bys.z1);
+        fobj -= (double)vx * b0y - (double)vy * b0x;
+      }
+    }
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
   if ((threadIdx.x & 31) == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
+  if (obj) {
+    double sv[1] = {fobj};
+    const int idx[1] = {0};
+    const double scale[1] = {a.K * a.dt};
+    block_reduce_add<1>(sv, obj, idx, scale);
+  }
 }
 
 // J planes of one species from the fixed-point sums.
@@ -239,28 +258,6 @@ __global__ void jconvert_kernel(const unsigned long long* __restrict__ J64, int 
   jz[n] = (real)((double)(long long)J64[2 * nodes + n] * scale);
 }
 
-// F of the particles of one species after a step, summed in FP64 into acc[0]
-// (times dt).
-template <typename real>
-__global__ void __launch_bounds__(256) objective_kernel(Parts<real> P, int n, Fields<real> F, Geom g,
-                                                        AdjConst a, double* acc) {
-  double s[1] = {0.0};
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const Rec<real> r = load_records(P, t);
-    if (r.cell < 0) continue;
-    int i, j, k;
-    unpack_cell(r.cell, i, j, k);
-    if (!stencil_ok(g, i, j, k)) continue;
-    const Axis<real> X = axis_weights(i, r.o[0]), Y = axis_weights(j, r.o[1]), Z = axis_weights(k, r.o[2]);
-    const Stagger<real> sx = stagger(g, X, Y, Z, 3), sy = stagger(g, X, Y, Z, 4);
-    const double b0x = trilerp(F.f[F_B0X], sx.n, g.sx, g.gz, sx.x0, sx.x1, sx.y0, sx.y1, sx.z0, sx.z1);
-    const double b0y = trilerp(F.f[F_B0Y], sy.n, g.sx, g.gz, sy.x0, sy.x1, sy.y0, sy.y1, sy.z0, sy.z1);
-    s[0] -= (double)r.v[0] * b0y - (double)r.v[1] * b0x;
-  }
-  const int idx[1] = {0};
-  const double scale[1] = {a.K * a.dt};
-  block_reduce_add<1>(s, acc, idx, scale);
-}
 
 // Reverse of boris4 (cal_track4, :2804-2870): recomputes the forward from
 // (v, E, B) and maps the adjoint of the new velocity av to the adjoints of
@@ -352,7 +349,7 @@ struct AdjPart {
 // push found them; F the fields it gathered (E at the step start, B after the
 // first half-step) and B0. acc[1] += dJ/dI, acc[2] += dJ/dV.
 template <typename real>
-__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_adjoint_kernel(Parts<real> P, int n, Fields<real> F, Geom g,
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) push_adjoint_kernel(Parts<real> P, int n, Fields<real> F, Geom g,
                                                            PushConst<real> pc, AdjPart<real> A, AdjConst a,
                                                            double* acc) {
   double s[2] = {0.0, 0.0};
@@ -372,6 +369,8 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_adjoint_k
     }
     bool bal = true;
     Axis<real> X0{}, Y0{}, Z0{};
+    const int src[6] = {F_EX, F_EY, F_EZ, F_BX, F_BY, F_BZ};
+    real fg[6][3] = {};  // gradients of the six interpolants at xi0, kept from the recompute's gather
     real ax[3] = {0, 0, 0};
     real af[6] = {0, 0, 0, 0, 0, 0};  // adjoints of the gathered E and B
     if (live) {
@@ -386,7 +385,16 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_adjoint_k
       real vx = v0x, vy = v0y, vz = v0z;
       if (!bal) {
         X0 = axis_weights(i0, f0x); Y0 = axis_weights(j0, f0y); Z0 = axis_weights(k0, f0z);
-        G = gather6(F, g, X0, Y0, Z0);
+        // gather6 with the gradients: the same interpolants, read once for the recompute and the reverse
+        real gv[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const Stagger<real> st = stagger(g, X0, Y0, Z0, q);
+          const VG<real> f = trilerp_vg(F.f[src[q]], st.n, sx, sy, st.x0, st.x1, st.y0, st.y1, st.z0, st.z1);
+          gv[q] = f.v;
+          fg[q][0] = f.gx; fg[q][1] = f.gy; fg[q][2] = f.gz;
+        }
+        G = Gathered<real>{gv[0], gv[1], gv[2], gv[3], gv[4], gv[5]};
         boris4(pc, G, vx, vy, vz);
       }
       int ih = i0, jh = j0, kh = k0;
@@ -455,16 +463,14 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 4 : 2) push_adjoint_k
     // gather at xi0: scatter the field adjoints, add the interpolants' gradients
     const bool gat = live && !bal;
     real* const dst[6] = {A.le[0], A.le[1], A.le[2], A.ldb[0], A.ldb[1], A.ldb[2]};
-    const int src[6] = {F_EX, F_EY, F_EZ, F_BX, F_BY, F_BZ};
-#pragma unroll 1
+#pragma unroll
     for (int q = 0; q < 6; ++q) {
       Stagger<real> st{};
       if (gat) {
         st = stagger(g, X0, Y0, Z0, q);
-        const VG<real> fv = trilerp_vg(F.f[src[q]], st.n, sx, sy, st.x0, st.x1, st.y0, st.y1, st.z0, st.z1);
-        ax[0] += af[q] * fv.gx;
-        ax[1] += af[q] * fv.gy;
-        ax[2] += af[q] * fv.gz;
+        ax[0] += af[q] * fg[q][0];
+        ax[1] += af[q] * fg[q][1];
+        ax[2] += af[q] * fg[q][2];
       }
       scatter8_agg(dst[q], gat ? st.n : -1, sx, sy, gat ? af[q] : (real)0, st.x0, st.x1, st.y0, st.y1, st.z0,
                    st.z1);

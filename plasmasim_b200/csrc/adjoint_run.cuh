@@ -4,10 +4,10 @@
 //
 // Forward: the loop body of fdtd (:687-949) in slot-stable form: the push is
 // the one-thread-per-particle fused kernel over the slots, sorting is left out
-// (it only reorders particles) and the refill compacts the slots before it
-// appends, so that a particle keeps its slot from one refill to the next and
-// the compaction's slot map is all the reverse pass needs. After every step
-// the objective kernel adds dt * F.
+// (it only reorders particles) and the refill compacts the slots, in cell
+// order, before it appends, so that a particle keeps its slot from one refill
+// to the next and the compaction's slot map is all the reverse pass needs.
+// The forward sweep's push also adds each step's dt * F to the objective.
 //
 // Reverse: checkpoint/recompute. The forward sweep keeps the full state every
 // `every` steps; the reverse pass restores each segment's checkpoint, replays
@@ -241,9 +241,12 @@ int adj_resolve(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
   return PIC_OK;
 }
 
-// One slot-stable loop body; with `rec`, the step input goes into it.
+// One slot-stable loop body; with `rec`, the step input goes into it. The
+// density deposit runs only with `density` (the last step of the forward
+// sweep): no step of the adjoint run reads n, and the run ends with that
+// step's n.
 template <typename real>
-int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
+int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec, bool density = false) {
   CKR(do_renew_grid(c));
   long long kept[2] = {c->sp[0].count, c->sp[1].count};
   if (c->c_add > c->cfg.add_interval - 1) {
@@ -282,7 +285,7 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
     CK(cudaMemsetAsync(R.j64, 0, sizeof(unsigned long long) * 3 * (size_t)nodes, c->stream));
     push_fixed_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
         parts<real>(c, s), c->sp[s].count_dev, F, c->g, pc, R.j64, R.j64 + nodes, R.j64 + 2 * (size_t)nodes,
-        (real)(kJFixed / c->cfg.c), rec ? 0 : 1, c->err);
+        (real)(kJFixed / c->cfg.c), density ? 1 : 0, adj_const(c, s), rec ? nullptr : R.acc, c->err);
     CKL();
     jconvert_kernel<real><<<grid_blocks(nodes), kThreads, 0, c->stream>>>(
         R.j64, nodes, F.f[pc.pjx], F.f[pc.pjy], F.f[pc.pjz], c->cfg.q * species_weight(c) * c->cfg.c / kJFixed);
@@ -292,15 +295,7 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
   CKR(do_renew_b<real>(c));
   CKR(do_fold<real>(c));
   CKR(do_renew_e<real>(c));
-  // the objective: in the forward sweep only (a recomputed step's terms are known)
-  for (int s = 0; s < 2 && !rec; ++s) {
-    const long long n = c->sp[s].count;
-    if (n == 0) continue;
-    objective_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n,
-                                                                          fields<real>(c), c->g,
-                                                                          adj_const(c, s), R.acc);
-    CKL();
-  }
+  // the objective's terms came with the forward sweep's push; a recomputed step's are known
   c->c_add++;
   c->c_thrust++;
   return PIC_OK;

@@ -1318,7 +1318,7 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
         ck.emplace_back();
         CKR(adj_save<real>(c, ck.back()));
       }
-      CKR(adj_forward_step<real>(c, R, nullptr));
+      CKR(adj_forward_step<real>(c, R, nullptr, n == nsteps - 1));
     }
     double h[4] = {0, 0, 0, 0};
     CK(cudaMemcpyAsync(h, R.acc, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
