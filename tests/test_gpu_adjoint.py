@@ -106,3 +106,31 @@ def test_adjoint_argument_errors():
         for bad in [(0, 1), (4, 0)]:
             with pytest.raises(Exception):
                 P.adjoint(*bad)
+
+
+def restore(P, rows, grid, ctr):
+    for s in (ION, ELECTRON):
+        P.set_particles(s, rows[s])
+    P.set_grid(grid)
+    P.rng_counters(set_to=ctr)
+
+
+def test_adjoint_reuses_context_memory():
+    """pic_adjoint keeps its snapshot and work memory with the context. A second
+    call that starts from an imported state must give what a context that never
+    ran an adjoint gives from the same state. That context first runs the same
+    number of production steps, so that its refill counter is in the same
+    phase as the first context's after its first adjoint."""
+    p = oracle_params("tiny")
+    with gpu_ctx(p, 64) as P:
+        rows = {s: P.particles(s) for s in (ION, ELECTRON)}
+        grid, ctr = P.grid(), tuple(P.rng_counters())
+        P.adjoint(10, 3)
+        restore(P, rows, grid, ctr)
+        second = P.adjoint(10, 3)
+        assert P.status()[0] == 0
+    with gpu_ctx(p, 64) as Q:
+        Q.step(10)
+        restore(Q, rows, grid, ctr)
+        fresh = Q.adjoint(10, 3)
+    np.testing.assert_allclose(second, fresh, rtol=1e-10)
