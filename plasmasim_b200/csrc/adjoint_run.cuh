@@ -241,12 +241,13 @@ int adj_resolve(pic_ctx* c, AdjRun& R, AdjSnap* rec) {
   return PIC_OK;
 }
 
-// One slot-stable loop body; with `rec`, the step input goes into it. The
-// density deposit runs only with `density` (the last step of the forward
-// sweep): no step of the adjoint run reads n, and the run ends with that
-// step's n.
+// One slot-stable loop body; with `rec`, the step input goes into it. With
+// `objective` the push adds the step's dt * F to the objective (the forward
+// sweep; a recomputed step's terms are known). The density deposit runs only
+// with `density` (the last step of the forward sweep): no step of the adjoint
+// run reads n, and the run ends with that step's n.
 template <typename real>
-int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec, bool density = false) {
+int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec, bool objective, bool density) {
   CKR(do_renew_grid(c));
   long long kept[2] = {c->sp[0].count, c->sp[1].count};
   if (c->c_add > c->cfg.add_interval - 1) {
@@ -285,7 +286,7 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec, bool density = false) 
     CK(cudaMemsetAsync(R.j64, 0, sizeof(unsigned long long) * 3 * (size_t)nodes, c->stream));
     push_fixed_kernel<real><<<particle_blocks(n), kThreads, 0, c->stream>>>(
         parts<real>(c, s), c->sp[s].count_dev, F, c->g, pc, R.j64, R.j64 + nodes, R.j64 + 2 * (size_t)nodes,
-        (real)(kJFixed / c->cfg.c), density ? 1 : 0, adj_const(c, s), rec ? nullptr : R.acc, c->err);
+        (real)(kJFixed / c->cfg.c), density ? 1 : 0, adj_const(c, s), objective ? R.acc : nullptr, c->err);
     CKL();
     jconvert_kernel<real><<<grid_blocks(nodes), kThreads, 0, c->stream>>>(
         R.j64, nodes, F.f[pc.pjx], F.f[pc.pjy], F.f[pc.pjz], c->cfg.q * species_weight(c) * c->cfg.c / kJFixed);
@@ -295,7 +296,6 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec, bool density = false) 
   CKR(do_renew_b<real>(c));
   CKR(do_fold<real>(c));
   CKR(do_renew_e<real>(c));
-  // the objective's terms came with the forward sweep's push; a recomputed step's are known
   c->c_add++;
   c->c_thrust++;
   return PIC_OK;

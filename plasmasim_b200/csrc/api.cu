@@ -1297,6 +1297,7 @@ template <typename real>
 int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
   AdjRun R;
   std::vector<AdjSnap> ck;
+  std::vector<AdjSnap> last;  // the last segment's step inputs, kept by the forward sweep
   AdjSnap fin;
   auto run = [&]() -> int {
     const long long capmax = c->sp[0].cap > c->sp[1].cap ? c->sp[0].cap : c->sp[1].cap;
@@ -1312,13 +1313,17 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
     CKR(adj_alloc(c, R, (void**)&R.acc, sizeof(double) * 4));
     CKR(adj_alloc(c, R, (void**)&R.j64, sizeof(unsigned long long) * 3 * (size_t)c->g.nodes));
     CK(cudaMemsetAsync(R.acc, 0, sizeof(double) * 4, c->stream));
-    // forward sweep, keeping a checkpoint every `every` steps
+    // forward sweep, keeping a checkpoint every `every` steps and the step
+    // inputs of the last segment, which the reverse pass then need not recompute
+    const int last0 = ((nsteps - 1) / every) * every;
+    if (grad) last.resize((size_t)(nsteps - last0));
     for (int n = 0; n < nsteps; ++n) {
       if (grad && n % every == 0) {
         ck.emplace_back();
         CKR(adj_save<real>(c, ck.back()));
       }
-      CKR(adj_forward_step<real>(c, R, nullptr, n == nsteps - 1));
+      AdjSnap* rec = grad && n >= last0 ? &last[(size_t)(n - last0)] : nullptr;
+      CKR(adj_forward_step<real>(c, R, rec, true, n == nsteps - 1));
     }
     double h[4] = {0, 0, 0, 0};
     CK(cudaMemcpyAsync(h, R.acc, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
@@ -1344,10 +1349,15 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
     CK(cudaMemsetAsync(R.acc, 0, sizeof(double) * 4, c->stream));
     for (int seg = (int)ck.size() - 1; seg >= 0; --seg) {
       const int n0 = seg * every, n1 = n0 + every < nsteps ? n0 + every : nsteps;
-      CKR(adj_restore<real>(c, ck[seg]));
-      std::vector<AdjSnap> rec((size_t)(n1 - n0));
+      std::vector<AdjSnap> rec;
       int rc = PIC_OK;
-      for (int n = n0; n < n1 && rc == PIC_OK; ++n) rc = adj_forward_step<real>(c, R, &rec[n - n0]);
+      if (n0 == last0) {
+        rec.swap(last);
+      } else {
+        CKR(adj_restore<real>(c, ck[seg]));
+        rec.resize((size_t)(n1 - n0));
+        for (int n = n0; n < n1 && rc == PIC_OK; ++n) rc = adj_forward_step<real>(c, R, &rec[n - n0], false, false);
+      }
       for (int n = n1 - 1; n >= n0 && rc == PIC_OK; --n) {
         rc = adj_reverse_step<real>(c, R, rec[n - n0]);
         if (rc == PIC_OK) rc = adj_unrefill<real>(c, R, rec[n - n0]);
@@ -1376,6 +1386,7 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
   const int rc = run();
   cudaStreamSynchronize(c->stream);
   for (auto& S : ck) snap_free(c, S);
+  for (auto& S : last) snap_free(c, S);
   snap_free(c, fin);
   adj_free(c, R);
   return rc;
