@@ -747,31 +747,37 @@ __global__ void fold_y_adjoint(PlaneSet<real> s, Geom g) {
 // Stable compaction with its slot map (the adjoint run's refill): map[t] is
 // the new slot of live slot t, -1 for an empty one. pos = exclusive scan of
 // the live flags.
-// Sort keys of the refill's compaction: the cell index of a live slot, past
-// every cell for an empty one; the values are the slot indices.
-constexpr int kDeadKey = 0x7fffffff;
-
+// Sort keys of the refill's compaction: the linear node index of a live
+// slot's cell ((i gy + j) gz + k, below the node count), `dead` for an empty
+// slot; the values are the slot indices. The keys span few bits, so the radix
+// sort makes few passes.
 template <typename real>
-__global__ void cell_key_kernel(Parts<real> P, int n, int* key, int* slot) {
+__global__ void cell_key_kernel(Parts<real> P, int n, Geom g, int dead, int* key, int* slot) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const int c = P.cell[t];
-  key[t] = c >= 0 ? c : kDeadKey;
+  int v = dead;
+  if (c >= 0) {
+    int i, j, k;
+    unpack_cell(c, i, j, k);
+    v = (i * g.gy + j) * g.gz + k;
+  }
+  key[t] = v;
   slot[t] = t;
 }
 
 // Slot j of Q takes the particle of sorted position j; map[old slot] = j, or
 // -1 for an empty slot; *count = the live particles (the first dead key).
 template <typename real>
-__global__ void cell_gather_kernel(Parts<real> P, int n, const int* __restrict__ key, const int* __restrict__ slot,
-                                   Parts<real> Q, int* map, int* count) {
+__global__ void cell_gather_kernel(Parts<real> P, int n, int dead, const int* __restrict__ key,
+                                   const int* __restrict__ slot, Parts<real> Q, int* map, int* count) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const int k = key[j], old = slot[j];
-  const bool live = k != kDeadKey;
-  if (live) copy_record(P, old, Q, j, k);
+  const bool live = k != dead;
+  if (live) copy_record(P, old, Q, j, P.cell[old]);
   if (map) map[old] = live ? j : -1;
-  if (live && (j == n - 1 || key[j + 1] == kDeadKey)) *count = j + 1;
+  if (live && (j == n - 1 || key[j + 1] == dead)) *count = j + 1;
   if (j == 0 && !live) *count = 0;
 }
 

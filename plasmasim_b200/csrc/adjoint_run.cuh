@@ -11,8 +11,9 @@
 //
 // Reverse: checkpoint/recompute. The forward sweep keeps the full state every
 // `every` steps; the reverse pass restores each segment's checkpoint, replays
-// its steps while keeping each step's input (particles after the refill, E,
-// B, DB), and then runs the transposed step backwards over the segment. Memory
+// its steps while keeping each step's push input (particles after the refill,
+// E, and B and DB after the first half-step), and then runs the transposed
+// step backwards over the segment. Memory
 // is bounded by (nsteps / every) checkpoints plus `every` step inputs.
 
 struct AdjSnap {
@@ -169,6 +170,13 @@ AdjConst adj_const(const pic_ctx* c, int s) {
   return a;
 }
 
+// Bits of the compaction's sort keys: node indices and one dead key above them.
+int key_bits(const pic_ctx* c) {
+  int b = 1;
+  while ((1LL << b) - 1 < (long long)c->g.nodes + 1) ++b;
+  return b;
+}
+
 // Removes the empty slots of species s and orders the rest by cell (a stable
 // radix sort on the cell index, so a replayed segment gets the same order),
 // recording the slot map in `map` when it is not null. Cell order keeps the
@@ -181,13 +189,16 @@ int adj_compact(pic_ctx* c, AdjRun& R, int s, int* map) {
   Store& st = c->sp[s];
   const long long n = st.count;
   if (n == 0) return PIC_OK;
-  cell_key_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, R.skey[0], R.sslot[0]);
+  const int bits = key_bits(c);
+  const int dead = (1 << bits) - 1;
+  cell_key_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, c->g, dead, R.skey[0],
+                                                                     R.sslot[0]);
   CKL();
   size_t bytes = R.sort_bytes;
-  CK(cub::DeviceRadixSort::SortPairs(R.sort_tmp, bytes, R.skey[0], R.skey[1], R.sslot[0], R.sslot[1], (int)n, 0, 31,
-                                     c->stream));
+  CK(cub::DeviceRadixSort::SortPairs(R.sort_tmp, bytes, R.skey[0], R.skey[1], R.sslot[0], R.sslot[1], (int)n, 0,
+                                     bits, c->stream));
   ++c->launches;
-  cell_gather_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, R.skey[1],
+  cell_gather_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, dead, R.skey[1],
                                                                         R.sslot[1], parts<real>(c, s, 1 - st.cur),
                                                                         map, st.count_dev);
   CKL();
@@ -271,12 +282,12 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec, bool objective, bool d
     }
     c->c_add = 0;
   }
-  if (rec) {
+  CKR(do_renew_b<real>(c));
+  if (rec) {  // the push's inputs: particles, E at the step start, B and DB after the first half-step
     CKR(adj_save<real>(c, *rec));
     rec->kept[0] = kept[0];
     rec->kept[1] = kept[1];
   }
-  CKR(do_renew_b<real>(c));
   const int nodes = c->g.nodes;
   Fields<real> F = fields<real>(c);
   for (int s = 0; s < 2; ++s) {
@@ -388,10 +399,9 @@ int adj_renew_e(pic_ctx* c, AdjRun& R) {
 // step's recorded input.
 template <typename real>
 int adj_reverse_step(pic_ctx* c, AdjRun& R, const AdjSnap& in) {
-  // the fields the push gathered: E at the step start, B after the first half-step
+  // the fields the push gathered, as recorded: E at the step start, B after the first half-step
   CK(cudaMemcpyAsync((char*)c->field_mem + (size_t)F_EX * c->plane_bytes, in.planes, kSnapPlanes * c->plane_bytes,
                      cudaMemcpyDeviceToDevice, c->stream));
-  CKR(do_renew_b<real>(c));
   CKR(adj_renew_e<real>(c, R));
   CKR(adj_renew_b<real>(c, R));  // second B half-step
   for (int s = 0; s < 2; ++s) {

@@ -1308,7 +1308,7 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
       CKR(adj_alloc(c, R, (void**)&R.sslot[b], sizeof(int) * (size_t)capmax));
     }
     CK(cub::DeviceRadixSort::SortPairs(nullptr, R.sort_bytes, R.skey[0], R.skey[1], R.sslot[0], R.sslot[1],
-                                       (int)capmax, 0, 31, c->stream));
+                                       (int)capmax, 0, key_bits(c), c->stream));
     CKR(adj_alloc(c, R, &R.sort_tmp, R.sort_bytes));
     CKR(adj_alloc(c, R, (void**)&R.acc, sizeof(double) * 4));
     CKR(adj_alloc(c, R, (void**)&R.j64, sizeof(unsigned long long) * 3 * (size_t)c->g.nodes));
