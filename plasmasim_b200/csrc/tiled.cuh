@@ -138,7 +138,9 @@ __device__ __forceinline__ int refill_reserve(const SourceParams& sp, const Geom
 }
 
 // One warp per group: gmax = largest (stayers + movers) count of its 32
-// lanes, or a lane's refill reserve when that is larger.
+// lanes, or a lane's refill reserve when that is larger, plus a sixteenth and
+// two rows of slack: the fullest columns then take the next re-layouts'
+// arrivals in holes instead of spilling them to the slot-order tail.
 __global__ void group_size_kernel(Geom g, TileGeom t, const int* __restrict__ stay,
                                   const int* __restrict__ moved, SourceParams refill, int* gmax,
                                   int* gcap) {
@@ -150,6 +152,7 @@ __global__ void group_size_kernel(Geom g, TileGeom t, const int* __restrict__ st
   c = max(c, refill_reserve(refill, g, t, G, lane));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
+  if (c > 0) c += c / 16 + 2;
   if (lane == 0) {
     gmax[G] = c;
     gcap[G] = c * kLanes;
