@@ -122,6 +122,7 @@ struct pic_ctx {
   long long ctr_p = 0, ctr_v = 0;
   int c_add = 0, c_thrust = 0;
   bool grid_ready = false;
+  int since_layout = 0;         // steps since the last re-layout or full sort (both species)
   bool particles_ready = false;
   // kernel launches issued by this context, and optional per-phase event timing
   long long launches = 0;
@@ -895,6 +896,7 @@ template <typename real>
 int do_sort(pic_ctx* c) {
   const bool both[2] = {true, true};
   CKR(relayout_species<real>(c, both));
+  c->since_layout = 0;
   return resolve_counts<real>(c);
 }
 
@@ -1091,9 +1093,15 @@ int do_step(pic_ctx* c) {
   CKR(phase_mark(c, PH_FIELD));
   if (c->c_thrust > c->cfg.sort_interval - 1) {
     c->c_thrust = 0;
-    CKR(phase_mark(c, PH_SORT));
-    CKR(do_sort<real>(c));
-    CKR(phase_mark(c, PH_SORT));
+    // sorting (:696-697) only reorders particles, for locality. The tiled
+    // layout is already refreshed by the re-layout after every refill, so the
+    // periodic sort runs only when that has not happened for half a sort
+    // interval.
+    if (c->since_layout >= std::max(1, c->cfg.sort_interval / 2)) {
+      CKR(phase_mark(c, PH_SORT));
+      CKR(do_sort<real>(c));
+      CKR(phase_mark(c, PH_SORT));
+    }
   }
   if (c->c_add > c->cfg.add_interval - 1) {
     CKR(phase_mark(c, PH_ADD));
@@ -1108,6 +1116,7 @@ int do_step(pic_ctx* c) {
     CKR(phase_mark(c, PH_SORT));
     const bool which[2] = {!c->tiled[0], !c->tiled[1]};
     CKR(relayout_species<real>(c, which));
+    if (which[0] && which[1]) c->since_layout = 0;
     CKR(phase_mark(c, PH_SORT));
   }
   CKR(phase_mark(c, PH_PUSH));
@@ -1132,6 +1141,7 @@ int do_step(pic_ctx* c) {
   }
   c->c_add++;
   c->c_thrust++;
+  c->since_layout++;
   return PIC_OK;
 }
 
