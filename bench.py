@@ -233,7 +233,7 @@ def run_e2e(P, steps: int):
 # from the ncu capture of a 64^3 x 64 ppc launch
 # (profiles/push_tiled_kernel_grid64_64ppc.md); at a fixed number of particles
 # per cell the traffic of a launch grows with its particles.
-PUSH_TRAFFIC_PER_PARTICLE = 69.8
+PUSH_TRAFFIC_PER_PARTICLE = 73.1
 
 
 def roofline(out, npart_species, cells, rsize):
