@@ -139,7 +139,10 @@ __global__ void __launch_bounds__(256) place_rank_kernel(Parts<real> P, int firs
   }
 }
 
-// Pass 2: each appended particle to its hole (or to Q), its slot emptied.
+// Pass 2: each appended particle to its hole (or to Q). Its old slot is left
+// as it is: the count after the re-layout ends at first + (spilled
+// particles), and unspill_kernel rewrites exactly those slots, so no later
+// pass reads the others before a refill or the next re-layout writes them.
 template <typename real>
 __global__ void __launch_bounds__(256) place_move_kernel(Parts<real> P, int first, const int* __restrict__ count,
                                                          Geom g, TileGeom t, const int* __restrict__ goff,
@@ -160,7 +163,6 @@ __global__ void __launch_bounds__(256) place_move_kernel(Parts<real> P, int firs
         copy_record(P, s, Q, -2 - r, c);
       }
     }
-    P.cell[s] = -1;
   }
 }
 
