@@ -886,13 +886,6 @@ int resolve_counts(pic_ctx* c) {
 }
 
 template <typename real>
-int do_relayout_species(pic_ctx* c, int s) {
-  const bool which[2] = {s == 0, s == 1};
-  CKR(relayout_species<real>(c, which));
-  return resolve_counts<real>(c);
-}
-
-template <typename real>
 int do_sort(pic_ctx* c) {
   const bool both[2] = {true, true};
   CKR(relayout_species<real>(c, both));
