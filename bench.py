@@ -391,6 +391,45 @@ def run_adjoint(nsteps: int = 200, every: int = 20):
             "fd_checks": checks}
 
 
+def run_thrust_error(steps: int = 200, seed: int = 0):
+    """The thrust error the metric is quoted at: the FP32 path against the FP64
+    path on the same seed and the benchmark grid, after `steps` steps of fdtd
+    (refill every 5, sort every 20). Compares thrust_f's F[27] after the last
+    step and thrust_fave's running mean over all steps (27 components each,
+    normwise), and the total force (F[0..2]). A second FP32 run from another
+    seed gives the sampling noise of the same quantities: the spread between
+    two equally valid runs of the plasma."""
+    import numpy as np
+
+    from plasmasim_b200 import Pic3D
+
+    def run(precision, s):
+        cfg = make_config(precision, s)
+        cfg.diag_every_step = 1
+        with Pic3D(cfg) as P:
+            P.init_grid()
+            P.init_particle_flat()
+            P.fdtd(steps)
+            F, E = P.thrust_f()
+            return np.asarray(F), np.asarray(E), np.asarray(P.thrust_fave())
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    t0 = time.perf_counter()
+    F64, E64, A64 = run(64, seed)
+    F32, E32, A32 = run(32, seed)
+    G32, _, B32 = run(32, seed + 1)
+    return {"workload": f"{NX}x{NY}x{NZ} cells x {PPC} ppc/species, {steps} steps, FP32 vs FP64 from the same seed",
+            "thrust_rel_err": rel(F32, F64), "thrust_total_rel_err": rel(F32[:3], F64[:3]),
+            "fave_rel_err": rel(A32, A64), "fave_total_rel_err": rel(A32[:3], A64[:3]),
+            "energy_rel_err": [abs(E32[q] / E64[q] - 1) for q in range(4)],
+            "seed_spread": {"thrust": rel(G32, F32), "thrust_total": rel(G32[:3], F32[:3]),
+                            "fave": rel(B32, A32), "fave_total": rel(B32[:3], A32[:3])},
+            "F64_total": [float(x) for x in F64[:3]], "fave64_total": [float(x) for x in A64[:3]],
+            "wall_s": time.perf_counter() - t0}
+
+
 def combine_over_ranks(ms: float, pushed: float, dist=None, device: str = "cuda"):
     """Whole-job numbers of the replicas: the slowest rank's time and the
     particle pushes of all ranks (max and sum over the process group)."""
@@ -456,6 +495,8 @@ def main():
     ap.add_argument("--no-batch2d", action="store_true", help="skip the batched 2D runs")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--no-poisson", action="store_true", help="skip the Poisson cleaning measurement")
+    ap.add_argument("--no-thrust", action="store_true", help="skip the FP32-vs-FP64 thrust error leg")
+    ap.add_argument("--thrust-steps", type=int, default=200, help="steps of the thrust error leg")
     ap.add_argument("--runs2d", type=int, default=256, help="runs of the batched 2D workload")
     ap.add_argument("--adjoint-steps", type=int, default=200, help="steps of the adjoint measurement")
     ap.add_argument("--adjoint-every", type=int, default=20, help="its checkpoint interval")
@@ -567,6 +608,14 @@ def main():
             log("poisson failed:", exc)
             poisson = {"error": str(exc)[:200]}
 
+    thrust = None
+    if not args.no_thrust and world == 1:
+        try:
+            thrust = run_thrust_error(args.thrust_steps)
+        except Exception as exc:
+            log("thrust error leg failed:", exc)
+            thrust = {"error": str(exc)[:200]}
+
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         if ensure_reference_lib("cube64"):
@@ -605,6 +654,7 @@ def main():
             "clocks": out["clocks"], "gpu_launches": out["launches"],
             "device_errors": out["errors"], "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu,
             "batch2d": batch2d, "adjoint": adjoint, "poisson": poisson,
+            "thrust_rel_err": thrust.get("thrust_rel_err") if thrust else None, "thrust": thrust,
         }
         print(json.dumps(line))
     if dist is not None:

@@ -123,6 +123,11 @@ typedef struct pic_group pic_group;
 int pic_group_create(int nranks, pic_group **out);
 int pic_group_destroy(pic_group *group);
 int pic_group_transport(pic_group *group, int rank, pic_transport *out);
+/* The host rendezvous limit of the group's exchanges in milliseconds (60 s
+ * by default); an exchange whose partner does not arrive within it fails with
+ * PIC_ERR_COMM, and the group is unusable afterwards. No reference
+ * counterpart: MPI_Sendrecv and MPI_Allreduce (:1001-2531, :5103) block. */
+int pic_group_set_timeout(pic_group *group, int ms);
 
 /* NCCL transport: one process (or thread) per GPU. pic_nccl_unique_id fills
  * the 128-byte id on one rank; the caller shares it (e.g. through
@@ -289,9 +294,11 @@ int pic_read_timing(pic_ctx *ctx, double *ms8, long long *pairs8, long long *lau
  * `stream` (a cudaStream_t, NULL for the default stream) and allocates
  * nothing: its scratch is a static device array of 2048 x 4 doubles, which
  * caps the input at 2048 * 256 * 64 = 33,554,432 interior cells (larger inputs
- * return PIC_ERR_TOO_LARGE). The first call on each device sets up the
- * scratch address; make it before any stream capture. All calls share the
- * scratch: calls whose kernels overlap on the GPU race and must be ordered. */
+ * return PIC_ERR_TOO_LARGE; non-finite dx, q or e0 return PIC_ERR_ARG). Each
+ * call looks the scratch address up in the calling thread's current CUDA
+ * context; the first call in a context also loads the library's device code
+ * into it, so make that first call before any stream capture. All calls share
+ * the scratch: calls whose kernels overlap on the GPU race and must be ordered. */
 int pic_gauss_residual_noalloc(const float *ex, const float *ey, const float *ez,
                                const float *ni, const float *ne, int nx, int ny, int nz,
                                double dx, double q, double e0, void *stream, double *out4);

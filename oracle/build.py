@@ -23,7 +23,10 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("PLASMA_REFERENCE_ROOT", "/root/reference")
+# The reference checkout: PLASMA_REFERENCE_ROOT, else a "reference" directory
+# beside this repository's root.
+REF_ROOT = os.environ.get("PLASMA_REFERENCE_ROOT",
+                          os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 REF_SRC = os.path.join(REF_ROOT, "PIC", "3d_pic458_domain.c")
 REF_OUT = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(HERE, "liboracle3d.so")

@@ -202,6 +202,11 @@ int set_count(pic_ctx* c, int s, long long n) {
   return PIC_OK;
 }
 
+// Slots a kernel over species s covers: the host count, or the capacity while
+// a re-layout's new count is still on its way back to the host (such kernels
+// stop at *count_dev).
+long long slot_bound(const pic_ctx* c, int s) { return c->sp[s].pending ? c->sp[s].cap : c->sp[s].count; }
+
 double species_mass(const pic_ctx* c, int s) { return s == 0 ? c->cfg.mi : c->cfg.me; }
 double species_weight(const pic_ctx* c) { return c->cfg.n_all / c->cfg.np; }
 
@@ -676,7 +681,7 @@ template <typename real, int MODE>
 int do_push(pic_ctx* c, int s, long long first = 0) {
   // with a re-layout's count still pending, the grid covers every slot up to
   // the capacity and the kernel stops at *count_dev
-  const long long end = c->sp[s].pending ? c->sp[s].cap : c->sp[s].count;
+  const long long end = slot_bound(c, s);
   if (end <= first) return PIC_OK;
   push_kernel<real, MODE><<<particle_blocks(end - first), kThreads, 0, c->stream>>>(
       parts<real>(c, s), (int)first, c->sp[s].count_dev, fields<real>(c), c->g, push_const<real>(c, s),
@@ -958,6 +963,7 @@ int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0
 
 template <typename real>
 int do_add_flat(pic_ctx* c) {
+  CKR(resolve_counts<real>(c));  // the refill appends after the last re-layout's count
   Slab slabs[5];
   const int nslab = refill_slabs(c, slabs);
   for (int s = 0; s < 2; ++s) {
@@ -1032,7 +1038,7 @@ int do_thrust_sums(pic_ctx* c) {
   field_energy_kernel<real><<<particle_blocks(nint), kThreads, 0, c->stream>>>(fields<real>(c), c->g, b, c->acc);
   CKL();
   for (int s = 0; s < 2; ++s) {
-    if (c->sp[s].count == 0) continue;
+    if (slot_bound(c, s) == 0) continue;
     ThrustParams tp{};
     tp.xlo = (double)c->g.gnx * k.dx * 0.2; tp.xhi = (double)c->g.gnx * k.dx * 0.8;
     tp.ylo = (double)c->g.gny * k.dx * 0.2; tp.yhi = (double)c->g.gny * k.dx * 0.8;
@@ -1047,7 +1053,7 @@ int do_thrust_sums(pic_ctx* c) {
     for (int q = 0; q < 6; ++q) { tp.idx[3 + q] = o + q; tp.scale[3 + q] = sg * w; }
     tp.idx[9] = 27 + (s == 0 ? 2 : 3);
     tp.scale[9] = 0.5 * species_mass(c, s) * species_weight(c) * k.dx * k.dx * k.dx;
-    thrust_particles_kernel<real><<<particle_blocks(c->sp[s].count), kThreads, 0, c->stream>>>(
+    thrust_particles_kernel<real><<<particle_blocks(slot_bound(c, s)), kThreads, 0, c->stream>>>(
         parts<real>(c, s), c->sp[s].count_dev, fields<real>(c), c->g, tp, c->acc);
     CKL();
   }
@@ -1081,6 +1087,14 @@ int do_gauss(pic_ctx* c, double* out4) {
 // ------------------------------------------------------------ a step
 template <typename real>
 int do_step(pic_ctx* c) {
+  // a pending re-layout count whose read-back has landed is taken without waiting
+  for (int s = 0; s < 2; ++s) {
+    if (!c->sp[s].pending) continue;
+    const cudaError_t q = cudaEventQuery(c->sp[s].readback);
+    if (q == cudaSuccess) CKR(relayout_resolve<real>(c, s));
+    else if (q == cudaErrorNotReady) cudaGetLastError();  // not an error: the read-back is still on its way
+    else CK(q);
+  }
   CKR(phase_mark(c, PH_FIELD));
   CKR(do_renew_grid(c));
   CKR(phase_mark(c, PH_FIELD));
@@ -1115,8 +1129,11 @@ int do_step(pic_ctx* c) {
   CKR(phase_mark(c, PH_PUSH));
   if (c->has_xport) CKR(resolve_counts<real>(c));  // the exchange lists are sized from the counts
   if (c->has_xport) CKR(ensure_mig<real>(c));
+  // a re-layout's count stays pending: the push and the diagnostics cover the
+  // slots up to the capacity and stop at the device count, and the host reads
+  // the count back only when it needs it (the next refill, or any other call),
+  // by when the GPU has long passed the re-layout
   for (int s = 0; s < 2; ++s) CKR(do_push_tiled<real>(c, s));
-  CKR(resolve_counts<real>(c));  // waits for the re-layout's read-back while the GPU pushes
   if (c->has_xport) CKR(do_migrate<real>(c));  // sr_particle's exchange between ranks
   CKR(phase_mark(c, PH_PUSH));
   CKR(phase_mark(c, PH_FIELD));
@@ -1399,9 +1416,12 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
 #define DISPATCH(c, call)                      \
   ((c)->prec == 64 ? call<double> : call<float>)
 
+// Every entry point starts here: the context's device, and the particle
+// counts of a re-layout that pic_step left pending read back first.
 int check_ctx(pic_ctx* c) {
   if (!c) return PIC_ERR_ARG;
   if (cudaSetDevice(c->cfg.device) != cudaSuccess) return PIC_ERR_CUDA;
+  if (c->sp[0].pending || c->sp[1].pending) CKR(DISPATCH(c, resolve_counts)(c));
   return PIC_OK;
 }
 
@@ -1501,6 +1521,7 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
   c->ncells = (long long)k.nx * k.ny * k.nz;
   auto fail = [&](int code) {
     pic_destroy(c);
+    cudaGetLastError();  // a failed allocation must not fail the next context's launch checks
     return code;
   };
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PIC_ERR_CUDA);

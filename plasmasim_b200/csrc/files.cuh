@@ -93,8 +93,9 @@ int pic_load_checkpoint(pic_ctx* c, const char* dir, int rank, int nthreads) {
     FILE* fp = fopen(f.c_str(), "rb");
     if (!fp) return PIC_ERR_ARG;
     const size_t r = fread(rec.data(), sizeof(double) * PIC_GRID_RECORD, (size_t)nodes, fp);
+    const bool extra = fgetc(fp) != EOF;  // a field file of another grid size
     fclose(fp);
-    if (r != (size_t)nodes) return PIC_ERR_ARG;
+    if (r != (size_t)nodes || extra) return PIC_ERR_ARG;
   }
   const char* names[2] = {"ion", "electron"};
   std::vector<double> rows[2];
@@ -104,6 +105,12 @@ int pic_load_checkpoint(pic_ctx* c, const char* dir, int rank, int nthreads) {
           join(dir, "suspend-" + std::to_string(rank) + "-" + std::to_string(t) + "-" + names[s] + ".dat");
       FILE* fp = fopen(f.c_str(), "rb");
       if (!fp) return PIC_ERR_ARG;
+      // a file cut inside a record is rejected before anything is loaded
+      if (fseek(fp, 0, SEEK_END) != 0 || ftell(fp) < 0 || ftell(fp) % (long)sizeof(FileParticle) != 0 ||
+          fseek(fp, 0, SEEK_SET) != 0) {
+        fclose(fp);
+        return PIC_ERR_ARG;
+      }
       FileParticle p;
       while (fread(&p, sizeof(p), 1, fp) == 1) {
         const double r[PIC_PARTICLE_ROW] = {p.x, p.y, p.z, p.vx, p.vy, p.vz, p.n};

@@ -11,10 +11,12 @@
 // threads, each thread covering up to kCellsPerThread cells.
 //
 // Host code must not pass `g_noalloc_partials` itself to a kernel: in host code
-// that name is a host-side stand-in, not a device address. The first call on
-// each device does a one-time set-up: with that device current it looks the
-// device address up with cudaGetSymbolAddress and caches it. Make that first
-// call on a device before any stream capture.
+// that name is a host-side stand-in, not a device address. Every call looks the
+// device address up with cudaGetSymbolAddress in the calling thread's current
+// context and passes that to the kernels, so a context the host application
+// created itself, or one re-created after cudaDeviceReset, gets its own
+// address. The first call in a context also loads the library's device code
+// into it (a one-time set-up); make that first call before any stream capture.
 //
 // Every call reuses the same array and leaves its partial sums there. Each
 // call overwrites every partial slot it later reads, so nothing has to be
@@ -23,8 +25,8 @@
 // caller.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/plasma_b200.h"
 
@@ -33,13 +35,10 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kCellsPerThread = 64;
 constexpr int kMaxBlocks = 2048;
-constexpr int kMaxDevices = 64;
+constexpr int kFinalThreads = 256;
 
 // [kMaxBlocks][4]: sum r^2, sum (rho/e0)^2, max |r|, cells of each block
 __device__ __align__(256) double g_noalloc_partials[kMaxBlocks * 4];
-
-double* g_partials_addr[kMaxDevices] = {nullptr};
-std::mutex g_addr_mutex;
 
 struct Planes {
   const float *ex, *ey, *ez, *ni, *ne;
@@ -87,30 +86,45 @@ __global__ void __launch_bounds__(kThreads) gauss_partials_kernel(Planes p, int 
   }
 }
 
-__global__ void gauss_final_kernel(const double* partials, int nblocks, double* out4) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// The block partials summed by one block: thread t takes partials t,
+// t + kFinalThreads, ... in turn, then the threads' sums are combined in a
+// fixed tree, so that repeated calls on the same input give the same bits.
+__global__ void __launch_bounds__(kFinalThreads) gauss_final_kernel(const double* partials, int nblocks,
+                                                                    double* out4) {
   double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
-  for (int q = 0; q < nblocks; ++q) {
+  for (int q = threadIdx.x; q < nblocks; q += kFinalThreads) {
     a += partials[4 * q]; b += partials[4 * q + 1]; c = fmax(c, partials[4 * q + 2]); d += partials[4 * q + 3];
   }
-  out4[0] = a; out4[1] = b; out4[2] = c; out4[3] = d;
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+    c = fmax(c, __shfl_down_sync(0xffffffffu, c, o));
+    d += __shfl_down_sync(0xffffffffu, d, o);
+  }
+  __shared__ double sm[4][kFinalThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    sm[0][wid] = a; sm[1][wid] = b; sm[2][wid] = c; sm[3][wid] = d;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = b = c = d = 0.0;
+    for (int w = 0; w < kFinalThreads / 32; ++w) {
+      a += sm[0][w]; b += sm[1][w]; c = fmax(c, sm[2][w]); d += sm[3][w];
+    }
+    out4[0] = a; out4[1] = b; out4[2] = c; out4[3] = d;
+  }
 }
 
-// Device address of the scratch array on the current device, looked up once.
+// Device address of the scratch array in the current context.
 int partials_address(double** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PIC_ERR_CUDA;
-  std::lock_guard<std::mutex> lock(g_addr_mutex);
-  if (!g_partials_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-    if (e != cudaSuccess) {
-      fprintf(stderr, "plasma_b200: cudaGetSymbolAddress: %s\n", cudaGetErrorString(e));
-      return PIC_ERR_CUDA;
-    }
-    g_partials_addr[dev] = static_cast<double*>(p);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "plasma_b200: cudaGetSymbolAddress: %s\n", cudaGetErrorString(e));
+    return PIC_ERR_CUDA;
   }
-  *out = g_partials_addr[dev];
+  *out = static_cast<double*>(p);
   return PIC_OK;
 }
 
@@ -119,7 +133,8 @@ int partials_address(double** out) {
 extern "C" int pic_gauss_residual_noalloc(const float* ex, const float* ey, const float* ez,
                                           const float* ni, const float* ne, int nx, int ny, int nz,
                                           double dx, double q, double e0, void* stream, double* out4) {
-  if (!ex || !ey || !ez || !ni || !ne || !out4 || nx < 1 || ny < 1 || nz < 1 || !(dx > 0) || !(e0 != 0))
+  if (!ex || !ey || !ez || !ni || !ne || !out4 || nx < 1 || ny < 1 || nz < 1 || !std::isfinite(dx) ||
+      !(dx > 0) || !std::isfinite(q) || !std::isfinite(e0) || e0 == 0)
     return PIC_ERR_ARG;
   const long long ncells = (long long)nx * ny * nz;
   const long long per_block = (long long)kThreads * kCellsPerThread;
@@ -138,7 +153,7 @@ extern "C" int pic_gauss_residual_noalloc(const float* ex, const float* ey, cons
   Planes p{ex, ey, ez, ni, ne};
   gauss_partials_kernel<<<(unsigned)nblocks, kThreads, 0, s>>>(p, nx, ny, nz, 1.0 / (24.0 * dx), q / e0, partials);
   if (cudaGetLastError() != cudaSuccess) return PIC_ERR_CUDA;
-  gauss_final_kernel<<<1, 32, 0, s>>>(partials, (int)nblocks, out4);
+  gauss_final_kernel<<<1, kFinalThreads, 0, s>>>(partials, (int)nblocks, out4);
   if (cudaGetLastError() != cudaSuccess) return PIC_ERR_CUDA;
   return PIC_OK;
 }

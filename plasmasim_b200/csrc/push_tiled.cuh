@@ -10,55 +10,88 @@ namespace pb {
 constexpr int kStages = 3;   // particle rows in flight per warp
 
 // Shared-memory plan of one CTA (8 warps): the J/n window, per warp a ring of
-// kStages particle rows fetched ahead with cp.async (cell words, then the six
-// coordinate arrays) and, in FP32, the tile's E and B over the same window
-// (the gather reads them there; FP64 gathers from global memory, its window
-// would not leave room for two CTAs per SM).
+// kStages particle rows fetched ahead with cp.async (records A and B of each
+// slot) and, in FP32, the tile's E and B as node quads (FieldQuads below; the
+// gather reads them there; FP64 gathers from global memory, its window would
+// not leave room for two CTAs per SM).
+//
+// FieldQuads: for each of ex, ey, ez, bx, by, bz and each base node (x, y, z)
+// of the tile's gather stencils, the float4
+//   (f(x, y, z), f(x+1, y, z), f(x, y, z+1), f(x+1, y, z+1)),
+// so that the 2x2x2 nodes of one component are two 16-byte loads (rows y and
+// y+1). A particle in cell (i, j, k) of the tile interpolates from bases
+// i-1 .. i, j-1 .. j (and row j+1), k-1 .. k, so the quads cover bases
+// [c0 - 1, c0 + T - 1] of each axis for the tile's first cell c0 and extent T,
+// plus the row above on y: QX = TX + 1, QY = TY + 2, QZ = 32 + 1. Particles
+// that have left the tile gather from global memory.
 template <typename real>
 struct PushSmem {
   static constexpr int WX = kTileX + 4, WY = kTileY + 4, WZ = kWinZ, WN = WX * WY * WZ;
+  static constexpr int QX = kTileX + 1, QY = kTileY + 2, QZ = kLanes + 1, QN = QX * QY * QZ;
   static constexpr int kWarps = kTileX * kTileY;
   static constexpr bool kFieldWin = sizeof(real) == 4;
   static constexpr size_t win_bytes = 4 * WN * sizeof(real);
   static constexpr size_t prec_off = (win_bytes + 15) & ~(size_t)15;  // records A, B of each slot: 8 reals
   static constexpr size_t fwin_off = prec_off + (size_t)kWarps * kStages * kLanes * 8 * sizeof(real);
-  static constexpr size_t bytes = fwin_off + (kFieldWin ? (size_t)6 * WN * sizeof(real) : 0);
+  static constexpr size_t bytes = fwin_off + (kFieldWin ? (size_t)6 * QN * sizeof(float4) : 0);
 };
 
-// Trilinear interpolation from a window plane with compile-time strides (the
-// 2x2x2 nodes at window index n). The two x planes travel as one packed pair
-// through the z and y steps, two-wide multiplies and FMAs of sm_100 (one
-// instruction for both planes); Z0 = (z0, z0) and so on.
-template <int WY, int WZ>
-__device__ __forceinline__ float trilerp_win(const float* __restrict__ w, int n, float x0, float x1, float2 Y0,
-                                             float2 Y1, float2 Z0, float2 Z1) {
-  constexpr int P = WY * WZ;  // next x plane
-  const float2 n00 = make_float2(w[n], w[n + P]), n01 = make_float2(w[n + 1], w[n + P + 1]);
-  const float2 n10 = make_float2(w[n + WZ], w[n + P + WZ]), n11 = make_float2(w[n + WZ + 1], w[n + P + WZ + 1]);
-  const float2 cy0 = __ffma2_rn(n01, Z1, __fmul2_rn(n00, Z0));  // (c00, c10)
-  const float2 cy1 = __ffma2_rn(n11, Z1, __fmul2_rn(n10, Z0));  // (c01, c11)
-  const float2 cx = __ffma2_rn(cy1, Y1, __fmul2_rn(cy0, Y0));   // the two x planes
+// Fills the tile's FieldQuads from planes F_EX .. F_BZ; nodes outside the
+// array read as zero. (ci0, cj0, ck0): the tile's first cell.
+template <int QX, int QY, int QZ>
+__device__ __forceinline__ void fill_quads(float4* __restrict__ fq, const Fields<float>& F, const Geom& g, int ci0,
+                                           int cj0, int ck0) {
+  constexpr int QN = QX * QY * QZ;
+  const int x0 = ci0 - 1, y0 = cj0 - 1, z0 = ck0 - 1;
+  for (int q = threadIdx.x; q < 6 * QN; q += blockDim.x) {
+    const int p = q / QN, r = q % QN;
+    const int x = x0 + r / (QY * QZ), y = y0 + (r / QZ) % QY, z = z0 + r % QZ;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    if (y < g.gy) {
+      const float* src = F.f[p] + (long long)x * g.sx + y * g.gz + z;
+      const bool x1 = x + 1 < g.gx, zin = z < g.gz, z1 = z + 1 < g.gz;
+      if (x < g.gx && zin) v[0] = __ldg(src);
+      if (x1 && zin) v[1] = __ldg(src + g.sx);
+      if (x < g.gx && z1) v[2] = __ldg(src + 1);
+      if (x1 && z1) v[3] = __ldg(src + g.sx + 1);
+    }
+    fq[q] = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+// One component from its quads: base quad index n (rows n and n + QZ), the
+// weights of its x, y and z bases. The two x nodes travel as one packed pair
+// through the z and y steps (two-wide multiplies and FMAs of sm_100).
+template <int QZ>
+__device__ __forceinline__ float quad_lerp(const float4* __restrict__ fq, int n, float x0, float x1, float2 Y0,
+                                           float2 Y1, float2 Z0, float2 Z1) {
+  const float4 r0 = fq[n], r1 = fq[n + QZ];
+  const float2 c0 = __ffma2_rn(make_float2(r0.z, r0.w), Z1, __fmul2_rn(make_float2(r0.x, r0.y), Z0));
+  const float2 c1 = __ffma2_rn(make_float2(r1.z, r1.w), Z1, __fmul2_rn(make_float2(r1.x, r1.y), Z0));
+  const float2 cx = __ffma2_rn(c1, Y1, __fmul2_rn(c0, Y0));
   return cx.x * x0 + cx.y * x1;
 }
 
-// gather6 from the tile's field window (planes ex ey ez bx by bz of WN nodes,
-// origin (wx0, wy0, wz0)); the caller checks that the stencil lies inside.
-template <int WY, int WZ, int WN>
-__device__ __forceinline__ Gathered<float> gather6_win(const float* __restrict__ fw, int wx0, int wy0, int wz0,
-                                                       const Axis<float>& X, const Axis<float>& Y,
-                                                       const Axis<float>& Z) {
-  const int ax = X.a - wx0, bx = X.b - wx0, ay = Y.a - wy0, by = Y.b - wy0, az = Z.a - wz0, bz = Z.b - wz0;
+// gather6 from the tile's FieldQuads for a particle in the tile's cells.
+template <int QY, int QZ>
+__device__ __forceinline__ Gathered<float> gather6_quads(const float4* __restrict__ fq, int ci0, int cj0, int ck0,
+                                                         const Axis<float>& X, const Axis<float>& Y,
+                                                         const Axis<float>& Z) {
+  constexpr int QN = (kTileX + 1) * QY * QZ;
+  const int xa = (X.a - ci0 + 1) * (QY * QZ), xb = (X.b - ci0 + 1) * (QY * QZ);
+  const int ya = (Y.a - cj0 + 1) * QZ, yb = (Y.b - cj0 + 1) * QZ;
+  const int za = Z.a - ck0 + 1, zb = Z.b - ck0 + 1;
   const float2 ya0 = make_float2(Y.a0, Y.a0), ya1 = make_float2(Y.a1, Y.a1);
   const float2 yb0 = make_float2(Y.b0, Y.b0), yb1 = make_float2(Y.b1, Y.b1);
   const float2 za0 = make_float2(Z.a0, Z.a0), za1 = make_float2(Z.a1, Z.a1);
   const float2 zb0 = make_float2(Z.b0, Z.b0), zb1 = make_float2(Z.b1, Z.b1);
   Gathered<float> r;
-  r.ex = trilerp_win<WY, WZ>(fw, (ax * WY + by) * WZ + bz, X.a0, X.a1, yb0, yb1, zb0, zb1);
-  r.ey = trilerp_win<WY, WZ>(fw + WN, (bx * WY + ay) * WZ + bz, X.b0, X.b1, ya0, ya1, zb0, zb1);
-  r.ez = trilerp_win<WY, WZ>(fw + 2 * WN, (bx * WY + by) * WZ + az, X.b0, X.b1, yb0, yb1, za0, za1);
-  r.bx = trilerp_win<WY, WZ>(fw + 3 * WN, (bx * WY + ay) * WZ + az, X.b0, X.b1, ya0, ya1, za0, za1);
-  r.by = trilerp_win<WY, WZ>(fw + 4 * WN, (ax * WY + by) * WZ + az, X.a0, X.a1, yb0, yb1, za0, za1);
-  r.bz = trilerp_win<WY, WZ>(fw + 5 * WN, (ax * WY + ay) * WZ + bz, X.a0, X.a1, ya0, ya1, zb0, zb1);
+  r.ex = quad_lerp<QZ>(fq, xa + yb + zb, X.a0, X.a1, yb0, yb1, zb0, zb1);
+  r.ey = quad_lerp<QZ>(fq + QN, xb + ya + zb, X.b0, X.b1, ya0, ya1, zb0, zb1);
+  r.ez = quad_lerp<QZ>(fq + 2 * QN, xb + yb + za, X.b0, X.b1, yb0, yb1, za0, za1);
+  r.bx = quad_lerp<QZ>(fq + 3 * QN, xb + ya + za, X.b0, X.b1, ya0, ya1, za0, za1);
+  r.by = quad_lerp<QZ>(fq + 4 * QN, xa + yb + za, X.a0, X.a1, yb0, yb1, za0, za1);
+  r.bz = quad_lerp<QZ>(fq + 5 * QN, xa + ya + zb, X.a0, X.a1, ya0, ya1, zb0, zb1);
   return r;
 }
 
@@ -205,32 +238,10 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   // window origin: two nodes below the tile's first interior cell (2 + tx*TX)
   const int wx0 = tx * kTileX, wy0 = ty * kTileY, wz0 = tz * kLanes;
   for (int q = threadIdx.x; q < 4 * WN; q += blockDim.x) win[q] = (real)0;
-  // FP32: E and B (planes F_EX..F_BZ) over the window, zero outside the array
-  float* fw = reinterpret_cast<float*>(smem_raw + S::fwin_off);
-  if constexpr (S::kFieldWin) {
-    constexpr int NZ4 = WZ / 4;
-    for (int q4 = threadIdx.x; q4 < 6 * WX * WY * NZ4; q4 += blockDim.x) {
-      const int p = q4 / (WX * WY * NZ4);
-      const int r = q4 % (WX * WY * NZ4);
-      const int a = r / (WY * NZ4), b = (r / NZ4) % WY, c4 = r % NZ4;
-      const int ga = wx0 + a, gb = wy0 + b, gc = wz0 + 4 * c4;
-      float v[4] = {0.f, 0.f, 0.f, 0.f};
-      if (ga < g.gx && gb < g.gy) {
-        const real* src = F.f[p] + ga * g.sx + gb * g.gz + gc;
-        if (VEC_FLUSH && gc + 3 < g.gz) {
-          const float4 f4 = __ldg(reinterpret_cast<const float4*>(src));
-          v[0] = f4.x; v[1] = f4.y; v[2] = f4.z; v[3] = f4.w;
-        } else {
-#pragma unroll
-          for (int e = 0; e < 4; ++e)
-            if (gc + e < g.gz) v[e] = (float)src[e];
-        }
-      }
-      float* dst = fw + p * WN + (a * WY + b) * WZ + 4 * c4;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) dst[e] = v[e];
-    }
-  }
+  // FP32: E and B of the tile's gather stencils as node quads
+  float4* fq = reinterpret_cast<float4*>(smem_raw + S::fwin_off);
+  const int ci0 = wx0 + 2, cj0 = wy0 + 2, ck0 = wz0 + 2;  // the tile's first cell
+  if constexpr (S::kFieldWin) fill_quads<S::QX, S::QY, S::QZ>(fq, F, g, ci0, cj0, ck0);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int G = tile * (kTileX * kTileY) + warp;
@@ -284,11 +295,11 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       if (!bal) {
         const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
         if constexpr (S::kFieldWin) {
-          // the stencil spans nodes i-1 .. i+1 on each axis
-          const bool inside = i - 1 >= wx0 && i + 1 < wx0 + WX && j - 1 >= wy0 && j + 1 < wy0 + WY &&
-                              k - 1 >= wz0 && k + 1 < wz0 + WZ;
+          // the quads cover the stencils of particles in the tile's cells
+          const bool inside = (unsigned)(i - ci0) < (unsigned)kTileX && (unsigned)(j - cj0) < (unsigned)kTileY &&
+                              (unsigned)(k - ck0) < (unsigned)kLanes;
           if (inside)
-            boris4_fast(pc, gather6_win<WY, WZ, WN>(fw, wx0, wy0, wz0, X, Y, Z), vx, vy, vz);
+            boris4_fast(pc, gather6_quads<S::QY, S::QZ>(fq, ci0, cj0, ck0, X, Y, Z), vx, vy, vz);
           else
             boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
         } else {

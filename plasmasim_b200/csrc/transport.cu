@@ -27,7 +27,7 @@
 namespace {
 
 constexpr int kMaxRanks = 64;
-constexpr int kTimeoutMs = 60000;
+constexpr int kDefaultTimeoutMs = 60000;
 
 struct Msg {
   const void* ptr = nullptr;
@@ -43,6 +43,7 @@ struct Member;
 
 struct pic_group {
   int n = 0;
+  int timeout_ms = kDefaultTimeoutMs;  // host rendezvous limit of every exchange
   std::mutex mu;
   std::condition_variable cv;
   std::deque<Msg*> box[kMaxRanks][kMaxRanks];  // box[dest][src], FIFO per pair
@@ -75,7 +76,7 @@ int group_sendrecv(void* user, const void* send, size_t send_bytes, int dest, vo
     delete out;
     return 1;
   }
-  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(kTimeoutMs);
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(g->timeout_ms);
   {
     std::lock_guard<std::mutex> lk(g->mu);
     g->box[dest][me->rank].push_back(out);
@@ -87,7 +88,7 @@ int group_sendrecv(void* user, const void* send, size_t send_bytes, int dest, vo
     std::unique_lock<std::mutex> lk(g->mu);
     auto& q = g->box[me->rank][src];
     if (!g->cv.wait_until(lk, deadline, [&] { return !q.empty(); })) {
-      fprintf(stderr, "plasma_b200: rank %d: no message from rank %d within %d ms\n", me->rank, src, kTimeoutMs);
+      fprintf(stderr, "plasma_b200: rank %d: no message from rank %d within %d ms\n", me->rank, src, g->timeout_ms);
       return 1;
     }
     in = q.front();
@@ -112,7 +113,7 @@ int group_sendrecv(void* user, const void* send, size_t send_bytes, int dest, vo
     std::unique_lock<std::mutex> lk(g->mu);
     if (!g->cv.wait_until(lk, deadline, [&] { return out->taken; })) {
       fprintf(stderr, "plasma_b200: rank %d: rank %d did not take its message within %d ms\n", me->rank, dest,
-              kTimeoutMs);
+              g->timeout_ms);
       return 1;  // `out` stays queued; the group is unusable after a timeout
     }
   }
@@ -131,7 +132,7 @@ int group_allreduce(void* user, double* buf, int n, void* stream_p) {
   if (cudaMemcpyAsync(h.data(), buf, sizeof(double) * n, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
       cudaStreamSynchronize(stream) != cudaSuccess)
     return 1;
-  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(kTimeoutMs);
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(g->timeout_ms);
   std::vector<double> sum((size_t)n, 0.0);
   {
     std::unique_lock<std::mutex> lk(g->mu);
@@ -142,7 +143,7 @@ int group_allreduce(void* user, double* buf, int n, void* stream_p) {
     ++g->arrived;
     g->cv.notify_all();
     if (!g->cv.wait_until(lk, deadline, [&] { return g->arrived == g->n || g->gen != gen; })) {
-      fprintf(stderr, "plasma_b200: rank %d: allreduce partners missing after %d ms\n", me->rank, kTimeoutMs);
+      fprintf(stderr, "plasma_b200: rank %d: allreduce partners missing after %d ms\n", me->rank, g->timeout_ms);
       return 1;
     }
     for (int r = 0; r < g->n; ++r)  // rank order: the same bits on every rank
@@ -248,6 +249,13 @@ int pic_group_destroy(pic_group* g) {
       }
   for (Member* m : g->members) delete m;
   delete g;
+  return PIC_OK;
+}
+
+int pic_group_set_timeout(pic_group* g, int ms) {
+  if (!g || ms < 1) return PIC_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g->mu);
+  g->timeout_ms = ms;
   return PIC_OK;
 }
 

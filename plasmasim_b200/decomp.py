@@ -56,6 +56,12 @@ class LocalGroup:
     def transport(self, rank: int) -> _CTransport:
         return self._transports[rank]
 
+    def set_timeout(self, ms: int):
+        """pic_group_set_timeout: the host rendezvous limit of every exchange."""
+        rc = self.L.pic_group_set_timeout(self.h, int(ms))
+        if rc:
+            raise PicError(rc, "pic_group_set_timeout")
+
     def close(self):
         if self.h:
             self.L.pic_group_destroy(self.h)

@@ -2,11 +2,14 @@
  * pic3d_main.c -- host driver in C for the B200 PIC step, in the shape of the
  * reference's main()/main_func()/fdtd() (PIC/3d_pic458_domain.c:192-289,
  * 627-952) at MPI size 1: set up the domain, initialise grid and particles,
- * run the time loop through the C ABI, and print the thrust_f / thrust_fave
- * diagnostics every `thrust_every` steps in the reference's thrust458.txt
- * column layout (:5111-5119) to stdout.
+ * run the time loop through the C ABI, and print the thrust_f diagnostics
+ * every `thrust_every` steps in the reference's thrust458.txt column layout
+ * (:5111-5119) to stdout. As fdtd does (:913-926), it also appends those lines
+ * to thrust458.txt in `outdir` and, after every step, hands thrust_fave's
+ * running mean to pic_append_thrust_ave, which writes thrust458_ave.txt and
+ * restarts the mean at steps that are multiples of 500 (:5267-5280).
  *
- * usage: pic3d_main [nx ny nz np steps precision sort_every thrust_every]
+ * usage: pic3d_main [nx ny nz np steps precision sort_every thrust_every outdir]
  * (normalized units: c = e0 = mu0 = q = m_e = dx = 1, m_i = 100)
  */
 #include <math.h>
@@ -34,6 +37,7 @@ int main(int argc, char **argv)
   int precision = argc > 6 ? atoi(argv[6]) : 32;
   int sort_every = argc > 7 ? atoi(argv[7]) : 20;
   int thrust_every = argc > 8 ? atoi(argv[8]) : 10;
+  const char *outdir = argc > 9 ? argv[9] : ".";
 
   pic_config cfg;
   CHECK(pic_config_default(&cfg, nx, ny, nz));
@@ -57,14 +61,15 @@ int main(int argc, char **argv)
   for (int c = 0; c < steps; ++c) {
     CHECK(pic_step(ctx, 1));
     if (c % thrust_every == 0) {
-      double F[PIC_NUM_THRUST], E[PIC_NUM_ENERGY], Fave[PIC_NUM_THRUST];
+      double F[PIC_NUM_THRUST], E[PIC_NUM_ENERGY];
       CHECK(pic_thrust_f(ctx, F, E));
-      CHECK(pic_thrust_fave(ctx, Fave, 0));
+      CHECK(pic_append_thrust(ctx, outdir, c));
       printf("%d", c);
       for (int q = 0; q < PIC_NUM_THRUST; ++q) printf(" %.3E", F[q]);
       for (int q = 0; q < PIC_NUM_ENERGY; ++q) printf(" %.8E", E[q]);
       printf("\n");
     }
+    CHECK(pic_append_thrust_ave(ctx, outdir, c));
   }
   long long status[8];
   int rc = pic_status(ctx, status);

@@ -26,7 +26,8 @@ GRID_FIELDS = ["bx", "by", "bz", "b0x", "b0y", "b0z", "ex", "ey", "ez",
 
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "particle capacity exceeded",
           4: "call out of order", 5: "device counters report lost work",
-          6: "input larger than the fixed-size scratch allows"}
+          6: "input larger than the fixed-size scratch allows",
+          7: "an exchange between ranks failed"}
 
 
 class PicError(RuntimeError):
@@ -143,6 +144,7 @@ EXPORTED = [
     "pic_objective", "pic_adjoint", "pic_save_checkpoint", "pic_load_checkpoint", "pic_write_output",
     "pic_append_thrust", "pic_append_thrust_ave", "pic_poisson_clean",
     "pic_set_transport", "pic_group_create", "pic_group_destroy", "pic_group_transport",
+    "pic_group_set_timeout",
     "pic_nccl_unique_id", "pic_nccl_transport_create", "pic_nccl_transport_destroy",
     "pic2d_config_normalized", "pic2d_create", "pic2d_destroy", "pic2d_init", "pic2d_step",
     "pic2d_thrust", "pic2d_particle_count", "pic2d_get_particles", "pic2d_get_grid",
@@ -181,6 +183,7 @@ def load_library(path: str = LIB_PATH):
     L.pic_group_create.argtypes = [C.c_int, C.POINTER(vp)]
     L.pic_group_destroy.argtypes = [vp]
     L.pic_group_transport.argtypes = [vp, C.c_int, C.POINTER(_CTransport)]
+    L.pic_group_set_timeout.argtypes = [vp, C.c_int]
     L.pic_nccl_unique_id.argtypes = [C.c_char_p]
     L.pic_nccl_transport_create.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(_CTransport)]
     L.pic_nccl_transport_destroy.argtypes = [C.POINTER(_CTransport)]

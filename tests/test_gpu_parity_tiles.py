@@ -1,0 +1,210 @@
+"""Parity of pic_step at the benchmark's own shapes and horizons.
+
+The tiled push (one CTA per 2 x 4 x 32-cell tile, with shared-memory field
+and deposit windows) is checked here on grids of several tiles along every
+axis, so that particles whose home cell, gather stencil or deposit stencil
+crosses a tile seam are compared with the FP64 oracle (oracle/pic_oracle.c,
+pinned bit for bit to the reference program by tests/test_oracle_golden.py):
+
+* one step on 64^3 cells (2 x 16 x 2 tiles, whole tiles) and on 41 x 22 x 70
+  cells (ragged tiles on every axis, and a row pitch that rules out the staged
+  field path), from the same particle state on both sides. Particles are
+  paired by position and compared by their displacement and velocity
+  (tests.util.step_errors), the grid planes field by field, F[27] and E[6];
+* the configuration the reference runs on a CPU: 32^3 cells x 8 particles per
+  cell per species for 100 steps of fdtd (refill every 5 steps), compared by
+  the thrust sums F[27] (thrust_f :4940-5122), the energies E[6], the running
+  thrust mean (thrust_fave :5124-5285), the density moments and the particle
+  counts;
+* thrust_fave against the reference program's own ten-step output, with the
+  reference's window: thrust_fave restarts its mean after step c = 0
+  (c % 500 == 0 :5267-5280), so the ten-step mean holds steps 1-9;
+* the FP32 path against the FP64 path from the same seed after 100 steps.
+
+Tolerances are stated per test. FP64 runs differ from the oracle only by the
+order of the deposit sums and libm ulps; FP32 runs carry the offsets of each
+particle in FP32 (2^-24 cells) and the fields in FP32, and after many steps
+the two sides' particle noise decorrelates, so N-step FP32 checks compare
+integrated quantities at tolerances measured on the GPU with a margin.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle.pyoracle import Oracle
+from plasmasim_b200 import ELECTRON, ION, Pic3D
+from tests.util import (config_from_oracle_params, density_moments, field_rel_err, load_golden,
+                        make_oracle, match_rows, oracle_params, oracle_params_for, rel_norm, step_errors)
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = {"cube64": (64, 64, 64, 8), "ragged": (41, 22, 70, 4)}
+
+# one step, from identical particle state
+STEP_TOL = {
+    64: dict(disp=1e-11, vel=1e-12, max_dx_cells=1e-12, max_dv_rel=1e-11, grid=1e-10, F=1e-10, E=1e-12),
+    32: dict(disp=3e-6, vel=1e-6, max_dx_cells=1e-6, max_dv_rel=1e-5, grid=2e-5, F=2e-4, E=1e-5),
+}
+
+
+def _initial_rows(O: Oracle):
+    """The oracle's initial load without init_particle_flat's extra particle in
+    ghost cell x = N + 2 (fdtd's first add_*_flat deletes it; pic_step's first
+    sort drops it, as sorting() drops ghost-cell particles)."""
+    nx = O.p["nx"]
+    rows = [O.particles(s)[0] for s in (0, 1)]
+    return [r[r[:, 0] < nx + 2] for r in rows]
+
+
+@pytest.mark.parametrize("shape", list(SHAPES))
+@pytest.mark.parametrize("precision", [64, 32])
+def test_one_step_across_tiles(shape, precision, record):
+    nx, ny, nz, np_ = SHAPES[shape]
+    p = oracle_params_for(nx, ny, nz, np_)
+    O = Oracle(p)
+    O.call("init_grid")
+    O.call("init_particle_flat")
+    rows = _initial_rows(O)
+    cfg = config_from_oracle_params(p, precision=precision, diag_every_step=0)
+    tol = STEP_TOL[precision]
+    with Pic3D(cfg) as P:
+        P.init_grid()
+        for s in (ION, ELECTRON):
+            P.set_particles(s, rows[s])
+        # the oracle starts from the particle state exactly as the GPU holds it
+        for s in (ION, ELECTRON):
+            O.set_particles(s, P.particles(s))
+        O.step()
+        P.step(1)
+        errs = {}
+        for s in (ION, ELECTRON):
+            mine, ref = match_rows(P.particles(s), O.particles(s)[0])
+            e = step_errors(mine, ref, p["dt"], p["dx"])
+            errs[("ion", "electron")[s]] = e
+            for k, v in e.items():
+                assert v <= tol[k], (shape, s, k, v)
+        g = field_rel_err(P.grid(), O.grid(), range(17))
+        F, E = P.thrust_f()
+        ref = O.thrust()
+        errs["grid"] = max(g.values())
+        errs["F"] = rel_norm(F, ref[:27])
+        errs["E"] = rel_norm(E, ref[27:])
+        record.update(shape=shape, precision=precision, errors=errs, particles=int(sum(len(r) for r in rows)))
+        assert errs["grid"] <= tol["grid"], g
+        assert errs["F"] <= tol["F"]
+        assert errs["E"] <= tol["E"]
+        assert P.status()[0] == 0
+        # the staged field path needs a row pitch (nz + 4 values) of whole 16-byte units
+        assert P.staged_fields() == (precision == 32 and (nz + 4) % 4 == 0 or
+                                     precision == 64 and (nz + 4) % 2 == 0)
+
+
+# 100 steps of the configuration the reference runs on a CPU
+HUNDRED_TOL = {
+    64: dict(count=0, F=1e-6, E=1e-9, fave=1e-6, moments=1e-10),
+    32: dict(count=0.005, F=5e-2, E=1e-2, fave=5e-2, moments=1e-3),
+}
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_cube32_hundred_steps(precision, record):
+    O = make_oracle("cube32")
+    O.call("init_grid")
+    O.call("init_particle_flat")
+    O.fdtd(100)
+    cfg = config_from_oracle_params(oracle_params("cube32"), precision=precision, diag_every_step=1)
+    tol = HUNDRED_TOL[precision]
+    with Pic3D(cfg) as P:
+        P.init_grid()
+        P.init_particle_flat()
+        P.fdtd(100)
+        counts = [P.particle_count(s) for s in (ION, ELECTRON)]
+        ref_counts = [O.particles(s)[0].shape[0] for s in (0, 1)]
+        F, E = P.thrust_f()
+        fave = P.thrust_fave()
+        grid = P.grid()
+        assert P.status()[0] == 0
+    ref = O.thrust()
+    og = O.grid()
+    errs = dict(
+        count=max(abs(a - b) / b for a, b in zip(counts, ref_counts)),
+        F=rel_norm(F, ref[:27]),
+        F_total=rel_norm(F[:3], ref[:3]),
+        E=[abs(E[q] / ref[27 + q] - 1) for q in range(4)],
+        fave=rel_norm(fave, O.fave()),
+        moments=float(np.max(np.abs(density_moments(grid) / density_moments(og) - 1))),
+        field_energy=abs((grid[..., 6:9] ** 2).sum() / (og[..., 6:9] ** 2).sum() - 1),
+    )
+    record.update(precision=precision, errors=errs, counts=counts, ref_counts=ref_counts)
+    assert errs["count"] <= tol["count"] + (2 / min(ref_counts) if precision == 64 else 0)
+    assert errs["F"] <= tol["F"]
+    assert max(errs["E"]) <= tol["E"]
+    assert errs["fave"] <= tol["fave"]
+    assert errs["moments"] <= tol["moments"]
+
+
+FAVE_TOL = {64: dict(reference=3e-3, oracle=1e-9), 32: dict(reference=5e-3, oracle=1e-3)}
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_thrust_fave_against_reference_output(precision, record):
+    """Ten steps of fdtd on the tiny cube, thrust_fave's mean as the reference
+    program left it (tests/golden/ref_tiny_fdtd10.npz). The ABI keeps the mean
+    until pic_append_thrust_ave restarts it at a step that is a multiple of
+    500, as the reference does after printing; the C driver calls it after
+    every step, and so does this test. The reference's mean then holds steps
+    1-9. Against the reference the difference is its list walks: thrust_fave
+    skips the last particle of each list and its deletions skip the particle
+    after a deleted list head (both measured on the CPU oracle at 1.4e-3
+    normwise); against the oracle the FP64 path agrees to summation order."""
+    g = load_golden("fdtd10")
+    cfg = config_from_oracle_params(oracle_params("tiny"), precision=precision, diag_every_step=1)
+    with Pic3D(cfg) as P, tempfile.TemporaryDirectory() as d:
+        P.init_grid()
+        P.init_particle_flat()
+        P.fdtd(1)
+        P.append_thrust_ave(d, 0)
+        assert os.path.exists(os.path.join(d, "thrust458_ave.txt"))
+        for c in range(1, 10):
+            P.step(1)
+            P.append_thrust_ave(d, c)
+        fave = P.thrust_fave()
+    runs = []
+    for n in (1, 10):
+        O = make_oracle("tiny")
+        O.call("init_grid")
+        O.call("init_particle_flat")
+        O.fdtd(n)
+        runs.append(O.fave())
+    fo = runs[1] - runs[0]
+    errs = dict(reference=rel_norm(fave, g["fave"]), oracle=rel_norm(fave, fo))
+    record.update(precision=precision, errors=errs)
+    assert errs["reference"] <= FAVE_TOL[precision]["reference"]
+    assert errs["oracle"] <= FAVE_TOL[precision]["oracle"]
+
+
+def test_fp32_against_fp64_hundred_steps(record):
+    """The FP32 path against the FP64 path from the same seed, 32^3 x 8 ppc,
+    100 steps: thrust F[27] normwise, the total force, energies. The two runs
+    start from the same draws (FP32 stores them rounded), so this measures
+    what FP32 arithmetic and storage do to the diagnostics the metric is
+    quoted at."""
+    res = {}
+    for precision in (64, 32):
+        cfg = config_from_oracle_params(oracle_params("cube32"), precision=precision, diag_every_step=1)
+        with Pic3D(cfg) as P:
+            P.init_grid()
+            P.init_particle_flat()
+            P.fdtd(100)
+            F, E = P.thrust_f()
+            res[precision] = (F, E, P.thrust_fave())
+    F64, E64, A64 = res[64]
+    F32, E32, A32 = res[32]
+    errs = dict(F=rel_norm(F32, F64), F_total=rel_norm(F32[:3], F64[:3]), fave=rel_norm(A32, A64),
+                E=[abs(E32[q] / E64[q] - 1) for q in range(4)])
+    record.update(errors=errs)
+    assert errs["F"] <= 5e-2
+    assert errs["fave"] <= 5e-2
+    assert max(errs["E"]) <= 1e-2

@@ -86,3 +86,68 @@ def random_fields(shape, rng, scale_e=1e-2, scale_b=0.1, smooth=True):
     e = [scale_e * f for f in out[:3]]
     b = [scale_b * f for f in out[3:]]
     return e, b
+
+
+def match_rows(mine: np.ndarray, ref: np.ndarray):
+    """Pairs each row of `mine` with the row of `ref` nearest in position.
+
+    Rows of the two sides come in different orders (the GPU keeps particles in
+    its tiled cell order). One step moves a particle about 0.025 cells and the
+    FP32 path places it within a few 1e-7 cells of the FP64 oracle, while
+    neighbouring particles lie tenths of a cell apart, so the nearest position
+    identifies the particle. Returns (mine, ref[idx]) after checking that the
+    pairing is one to one."""
+    from scipy.spatial import cKDTree
+
+    assert mine.shape == ref.shape, (mine.shape, ref.shape)
+    if mine.shape[0] == 0:
+        return mine, ref
+    tree = cKDTree(ref[:, :3])
+    dist, idx = tree.query(mine[:, :3], k=1)
+    assert np.bincount(idx, minlength=ref.shape[0]).max() == 1, "position matching is not one to one"
+    return mine, ref[idx]
+
+
+def step_errors(mine: np.ndarray, ref: np.ndarray, dt: float, dx: float) -> dict:
+    """Per-particle errors of one step, rows already paired (match_rows).
+
+    disp: ||x_mine - x_ref|| / ||v_ref dt|| over all particles, i.e. the error
+          of the displacement relative to the displacement (a step moves each
+          particle by v^{n+1/2} dt, so x_mine - x_ref is the displacement error)
+    vel:  ||v_mine - v_ref|| / ||v_ref||
+    max_dx_cells: the largest position difference of one particle, in cells
+    max_dv_rel:   the largest |v_mine - v_ref| / |v_ref| of one particle"""
+    dxv = mine[:, :3] - ref[:, :3]
+    dvv = mine[:, 3:6] - ref[:, 3:6]
+    vref = ref[:, 3:6]
+    vn = np.linalg.norm(vref, axis=1)
+    return dict(
+        disp=float(np.linalg.norm(dxv) / max(np.linalg.norm(vref) * dt, 1e-300)),
+        vel=float(np.linalg.norm(dvv) / max(np.linalg.norm(vref), 1e-300)),
+        max_dx_cells=float(np.abs(dxv).max() / dx) if len(dxv) else 0.0,
+        max_dv_rel=float((np.linalg.norm(dvv, axis=1) / np.maximum(vn, 1e-300)).max()) if len(dvv) else 0.0,
+    )
+
+
+def oracle_params_for(nx: int, ny: int, nz: int, np_: int, base: str = "tiny") -> dict:
+    """Run-time oracle parameters of the normalized plasma on an nx x ny x nz
+    grid with np_ particles per cell per species (the restatement takes its
+    geometry at run time; no compiled reference is needed)."""
+    p = dict(oracle_params(base))
+    p.update(nx=nx, ny=ny, nz=nz, np=np_)
+    return p
+
+
+def density_moments(grid: np.ndarray) -> np.ndarray:
+    """Sum n and the first moments sum n x, n y, n z of both species' density
+    planes (node indices as coordinates): 8 numbers."""
+    gx, gy, gz = grid.shape[:3]
+    ax = [np.arange(gx, dtype=np.float64), np.arange(gy, dtype=np.float64), np.arange(gz, dtype=np.float64)]
+    out = []
+    for f in (NI, NE):
+        n = grid[..., f]
+        out.append(n.sum())
+        out.append((n.sum(axis=(1, 2)) * ax[0]).sum())
+        out.append((n.sum(axis=(0, 2)) * ax[1]).sum())
+        out.append((n.sum(axis=(0, 1)) * ax[2]).sum())
+    return np.array(out)
