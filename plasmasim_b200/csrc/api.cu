@@ -85,6 +85,7 @@ struct pic_ctx {
   int* append_dev = nullptr;          // end of the append region during a re-layout
   int* holes = nullptr;               // per-slot scratch: hole rows of every lane column
   int* rank = nullptr;                // per-slot scratch: placement rank of every appended particle
+  int* bucket = nullptr;              // per-slot scratch: appended particles bucketed by their new cell
   int* cnt = nullptr;
   int* offs = nullptr;
   int* cursor = nullptr;
@@ -841,11 +842,18 @@ int relayout_launch(pic_ctx* c, int s) {
   CKL();
   const long long first = c->tiled_end[s];
   const Parts<real> Q = parts<real>(c, s, 1 - st.cur);
-  place_rank_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
-      P, (int)first, st.count_dev, c->g, nholes, c->cursor, c->total_dev, c->rank);
+  place_count_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
+      P, (int)first, st.count_dev, c->g, c->cursor, c->rank);
   CKL();
-  place_move_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
-      P, (int)first, st.count_dev, c->g, tg, c->goff[s][c->lay[s]], c->holes, c->rank, Q);
+  int* off = c->offs;  // per cell: arrivals that fit, then their bucket offset
+  place_fit_kernel<<<particle_blocks(c->ncells), kThreads, 0, c->stream>>>(c->cursor, nholes, off, c->ncells);
+  CKL();
+  CKR(scan_exclusive(c, off, off, c->ncells, c->scan_tmp, c->scan_tmp_len));
+  place_bucket_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
+      P, (int)first, st.count_dev, c->g, nholes, off, c->rank, c->bucket, c->total_dev, Q);
+  CKL();
+  place_fill_kernel<real><<<gblocks, kThreads, 0, c->stream>>>(P, (int)first, c->g, tg, c->goff[s][c->lay[s]],
+                                                               c->holes, c->cursor, nholes, off, c->bucket);
   CKL();
   unspill_kernel<real><<<particle_blocks(st.cap), kThreads, 0, c->stream>>>(Q, c->total_dev, P, (int)first);
   CKL();
@@ -1582,6 +1590,7 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
     if (cudaMalloc(&c->append_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->holes, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->rank, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    if (cudaMalloc(&c->bucket, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaFuncSetAttribute(push_tiled_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)PushSmem<double>::bytes) != cudaSuccess ||
         cudaFuncSetAttribute(push_tiled_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1628,6 +1637,7 @@ int pic_destroy(pic_ctx* c) {
   cudaFree(c->append_dev);
   cudaFree(c->holes);
   cudaFree(c->rank);
+  cudaFree(c->bucket);
   cudaFree(c->cnt);
   cudaFree(c->offs);
   cudaFree(c->cursor);

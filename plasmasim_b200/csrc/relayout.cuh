@@ -9,9 +9,14 @@
 //     A warp takes append slots 64 at a time from the shared counter and
 //     marks the slots of its last block it does not use empty, so the counter
 //     sees one atomic per 64 movers instead of one per row;
-//  2. place (one thread per appended slot: movers and refilled particles):
-//     the particle takes the next hole of its new cell's column; a particle
-//     that finds no hole is copied, compacted, into the spare buffer;
+//  2. place (movers and refilled particles, all appended after `count`): the
+//     particles are bucketed by their new cell -- a rank per particle from a
+//     per-cell counter, an exclusive scan of the arrivals that find a hole,
+//     the particle's index written to its bucket slot -- and then one warp
+//     per group fills each lane's holes, in row order, from its cell's
+//     bucket. A particle ranked past its cell's holes is copied, compacted,
+//     into the spare buffer instead. Every pass streams its input, so its
+//     scattered accesses are independent of one another;
 //  3. the particles without a hole are copied back right after the layout,
 //     where the slot-order push handles them until a later re-layout finds
 //     them a hole (or a full sort, when they become too many).
@@ -77,27 +82,16 @@ __global__ void classify_kernel(Parts<real> P, Geom g, TileGeom t, const int* __
         ++nh;
       }
     }
-    // the movers of the U rows: their loads issued together, then the copies
-    real o[U][3], v[U][3];
+    // the movers of the U rows: their record loads issued together, then the copies
+    Rec<real> rec[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (moved[u]) rec[u] = load_records(P, base + (r0 + u) * kLanes + lane);
 #pragma unroll
     for (int u = 0; u < U; ++u)
       if (moved[u]) {
-        const int s = base + (r0 + u) * kLanes + lane;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          o[u][a] = P.o[a][s];
-          v[u][a] = P.v[a][s];
-        }
-      }
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      if (moved[u]) {
-        P.cell[d[u]] = c[u];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          P.o[a][d[u]] = o[u][a];
-          P.v[a][d[u]] = v[u][a];
-        }
+        const Rec<real>& q = rec[u];
+        store_records(P, d[u], c[u], q.o[0], q.o[1], q.o[2], q.v[0], q.v[1], q.v[2]);
         P.cell[base + (r0 + u) * kLanes + lane] = -1;
       }
   }
@@ -110,59 +104,89 @@ __global__ void clamp_count_kernel(const int* append_at, int cap, int* count_dev
   *count_dev = min(*append_at, cap);
 }
 
-// Placement: each appended particle takes the next hole of its cell's column;
-// the rest go, compacted, to the spare buffer Q. Two streaming passes, each
-// with one kind of scattered access, so that many of them are in flight at
-// once (one kernel doing the whole chain -- cell, cursor atomic, hole lookup,
-// record copy -- per particle ran at 8 % issue).
-// Pass 1: the particle's rank among the appended particles of its new cell,
-// or, when its column has no hole left, -2 - (its index in the spare buffer
-// Q); -1 for an empty slot or a particle outside the interior (dropped).
+// Placement, pass 1: the particle's rank among the appended particles of its
+// new cell (from the per-cell counter `cursor`); -1 for an empty slot or a
+// particle outside the interior (dropped).
 template <typename real>
-__global__ void __launch_bounds__(256) place_rank_kernel(Parts<real> P, int first, const int* __restrict__ count,
-                                                         Geom g, const int* __restrict__ nholes, int* cursor,
-                                                         int* nspill, int* rank) {
+__global__ void __launch_bounds__(256) place_count_kernel(Parts<real> P, int first, const int* __restrict__ count,
+                                                          Geom g, int* cursor, int* rank) {
+  const int span = *count - first;
+  const int lane = threadIdx.x & 31;
+  const int stride = gridDim.x * blockDim.x;
+  for (int w0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; w0 < span; w0 += stride) {  // warp-uniform
+    const int q = w0 + lane;
+    const int key = q < span ? interior_key(g, P.cell[first + q]) : -1;
+    const int r = warp_aggregated_inc(cursor, key < 0 ? 0 : key, key >= 0);
+    if (q < span) rank[q] = key < 0 ? -1 : r;
+  }
+}
+
+// Pass 2, per interior cell: the arrivals that find a hole, min(arrivals, holes)
+// (exclusive-scanned afterwards into each cell's bucket offset).
+__global__ void place_fit_kernel(const int* __restrict__ arrivals, const int* __restrict__ nholes, int* fit,
+                                 long long ncells) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells;
+       c += (long long)gridDim.x * blockDim.x)
+    fit[c] = min(arrivals[c], nholes[c]);
+}
+
+// Pass 3: a particle ranked below its cell's holes writes its index to its
+// bucket slot; the others are copied, compacted, into the spare buffer Q.
+template <typename real>
+__global__ void __launch_bounds__(256) place_bucket_kernel(Parts<real> P, int first, const int* __restrict__ count,
+                                                           Geom g, const int* __restrict__ nholes,
+                                                           const int* __restrict__ off, const int* __restrict__ rank,
+                                                           int* bucket, int* nspill, Parts<real> Q) {
   const int span = *count - first;
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
   const int stride = gridDim.x * blockDim.x;
   for (int w0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; w0 < span; w0 += stride) {  // warp-uniform
     const int q = w0 + lane;
-    const int key = q < span ? interior_key(g, P.cell[first + q]) : -1;
-    const int r = warp_aggregated_inc(cursor, key < 0 ? 0 : key, key >= 0);
-    const bool spill = key >= 0 && r >= nholes[key];
+    const int c = q < span ? P.cell[first + q] : -1;
+    const int key = interior_key(g, c);
+    const int r = q < span ? rank[q] : -1;
+    const bool fits = key >= 0 && r < nholes[key];
+    const bool spill = key >= 0 && !fits;
+    if (fits) bucket[off[key] + r] = q;
     const unsigned ms = __ballot_sync(0xffffffffu, spill);
     int sb = 0;
     if (lane == 0 && ms) sb = atomicAdd(nspill, __popc(ms));
     sb = __shfl_sync(0xffffffffu, sb, 0);
-    if (q < span) rank[q] = key < 0 ? -1 : (spill ? -2 - (sb + __popc(ms & below)) : r);
+    if (spill) copy_record(P, first + q, Q, sb + __popc(ms & below), c);
   }
 }
 
-// Pass 2: each appended particle to its hole (or to Q). Its old slot is left
-// as it is: the count after the re-layout ends at first + (spilled
-// particles), and unspill_kernel rewrites exactly those slots, so no later
-// pass reads the others before a refill or the next re-layout writes them.
+// Pass 4, one warp per group: lane l copies the k-th particle of its home
+// cell's bucket into the slot of its k-th hole. U holes per lane are in
+// flight at once; their slots lie in the lane's own column.
 template <typename real>
-__global__ void __launch_bounds__(256) place_move_kernel(Parts<real> P, int first, const int* __restrict__ count,
-                                                         Geom g, TileGeom t, const int* __restrict__ goff,
-                                                         const int* __restrict__ holes, const int* __restrict__ rank,
-                                                         Parts<real> Q) {
-  const int span = *count - first;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < span; q += gridDim.x * blockDim.x) {
-    const int s = first + q;
-    const int r = rank[q];
-    if (r != -1) {
-      const int c = P.cell[s];
-      if (r >= 0) {
-        int l2;
-        const int G = group_of_key(g, t, interior_key(g, c), l2);
-        const int gb = goff[G];
-        copy_record(P, s, P, gb + holes[gb + r * kLanes + l2] * kLanes + l2, c);
-      } else {
-        copy_record(P, s, Q, -2 - r, c);
-      }
+__global__ void place_fill_kernel(Parts<real> P, int first, Geom g, TileGeom t, const int* __restrict__ goff,
+                                  const int* __restrict__ holes, const int* __restrict__ arrivals,
+                                  const int* __restrict__ nholes, const int* __restrict__ off,
+                                  const int* __restrict__ bucket) {
+  constexpr int U = 4;
+  const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (G >= t.ngroups) return;  // warp-uniform
+  const int home = home_key(g, t, G, lane);
+  const int n = home >= 0 ? min(arrivals[home], nholes[home]) : 0;
+  const int o = home >= 0 ? off[home] : 0;
+  const int base = goff[G];
+  int nmax = n;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, s));
+  for (int k0 = 0; k0 < nmax; k0 += U) {
+    int src[U], dst[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = k0 + u;
+      src[u] = k < n ? first + bucket[o + k] : -1;
+      dst[u] = k < n ? base + holes[base + k * kLanes + lane] * kLanes + lane : -1;
     }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (src[u] >= 0) copy_record(P, src[u], P, dst[u], P.cell[src[u]]);
   }
 }
 
