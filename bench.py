@@ -96,43 +96,60 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU side
-def reference_sample(name: str, nsteps: int, warm: int, workdir: str):
-    """Times the reference program (compiled from its own source, oracle/_ref)
-    on one host core: init, the initial refill, `warm` untimed loop bodies,
-    then `nsteps` timed ones. Returns (particle-steps, seconds, particles)."""
+def _reference_threaded_worker(name, phases, warm, budget_s, q):
     from oracle.pyoracle import Reference
 
-    os.chdir(workdir)
-    R = Reference(name)
-    R.init_grid()
-    R.init_particle_flat()
-    R.op("add_flat")
-    if warm:
-        R.L.ref_loop(warm, SORT_EVERY, ADD_EVERY)
-    n0 = R.L.ref_count(0) + R.L.ref_count(1)
-    t0 = time.perf_counter()
-    R.L.ref_loop(nsteps, SORT_EVERY, ADD_EVERY)
-    dt = time.perf_counter() - t0
-    n1 = R.L.ref_count(0) + R.L.ref_count(1)
-    return 0.5 * (n0 + n1) * nsteps, dt, n0
-
-
-def _reference_worker(args):
-    name, nsteps, warm = args
     with tempfile.TemporaryDirectory() as d:
-        return reference_sample(name, nsteps, warm, d)
+        os.chdir(d)
+        R = Reference(name)
+        lists = R.L.ref_set_threads(phases[0][0])
+        t0 = time.perf_counter()
+        R.init_grid()
+        R.init_particle_flat()
+        R.op("add_flat")              # fdtd's refill before its loop
+        init_s = time.perf_counter() - t0
+        if warm:
+            R.L.ref_loop(warm, SORT_EVERY, ADD_EVERY)
+        out = []
+        for threads, steps in phases:
+            R.L.ref_set_threads(threads)
+            n0 = R.L.ref_count(0) + R.L.ref_count(1)
+            done, secs = 0, 0.0
+            while done < steps and (done == 0 or secs < budget_s):
+                t1 = time.perf_counter()
+                R.L.ref_loop(1, SORT_EVERY, ADD_EVERY)
+                secs += time.perf_counter() - t1
+                done += 1
+            n1 = R.L.ref_count(0) + R.L.ref_count(1)
+            out.append({"psteps": 0.5 * (n0 + n1) * done, "secs": secs, "steps": done, "particles": n0,
+                        "init_s": init_s, "lists": lists, "threads": threads})
+        q.put(out)
 
 
-def reference_baseline(name: str, nsteps: int, warm: int, procs: int):
-    """`procs` independent single-core reference processes (spawned), summed."""
+def reference_threaded(name: str, phases, warm: int, budget_s: float = 150.0):
+    """The reference program compiled with OpenMP (oracle/_ref, THREAD_N = 64
+    particle lists) at geometry `name`, in a spawned process: init, the
+    initial refill and `warm` untimed loop bodies on the first phase's
+    threads, then for each (threads, steps) of `phases` up to `steps` timed
+    loop bodies on that many host threads (fewer when they pass `budget_s`).
+    Its loop is fdtd's body (:687-949): the particle loops run one list per
+    thread (:731, :818), the field loops split over x. One result per phase."""
     import multiprocessing as mp
 
     ctx = mp.get_context("spawn")
-    with ctx.Pool(procs) as pool:
-        res = pool.map(_reference_worker, [(name, nsteps, warm)] * procs)
-    psteps = sum(r[0] for r in res)
-    wall = max(r[1] for r in res)
-    return psteps / wall, res
+    q = ctx.Queue()
+    p = ctx.Process(target=_reference_threaded_worker, args=(name, list(phases), warm, budget_s, q))
+    p.start()
+    res = q.get()
+    p.join()
+    return res
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
 
 
 def ensure_reference_lib(name: str) -> bool:
@@ -430,6 +447,65 @@ def run_thrust_error(steps: int = 200, seed: int = 0):
             "wall_s": time.perf_counter() - t0}
 
 
+def run_configs2(steps: int = 100, grid: int = 256, ppc: int = 32):
+    """The large-grid workload: `grid`^3 cells x `ppc` particles/cell/species
+    (256^3 x 32: 1.07 G particles), the dipole moment at 0.5, 1 and 2 times
+    the benchmark's (coil current I = 16, 32, 64). For each, the FP32 path
+    (tiled layout) and the FP64 path from the same seed -- in slot order, one
+    record buffer per species, which is what lets 1.07 G FP64 particles fit
+    next to nothing else -- advance `steps` steps of fdtd; their thrust_f
+    F[27] and E[6], thrust_fave's running mean and the Gauss-law residual are
+    compared (the FP64 run as the reference), and the FP32 steps are timed
+    with CUDA events."""
+    import numpy as np
+    import torch
+
+    from plasmasim_b200 import Pic3D, PicConfig
+
+    def run(precision, coil_i, slot_order):
+        cfg = PicConfig.normalized(grid, grid, grid, ppc, precision=precision, sort_interval=SORT_EVERY,
+                                   add_interval=ADD_EVERY, diag_every_step=1, slot_order=slot_order)
+        cfg.coil_i = coil_i
+        with Pic3D(cfg) as P:
+            P.init_grid()
+            P.init_particle_flat()
+            P.fdtd(0)
+            stream = torch.cuda.ExternalStream(P.stream_handle())
+            _, c0 = P.status()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            P.synchronize()
+            e0.record(stream)
+            P.step(steps)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            rc, c1 = P.status()
+            F, E = P.thrust_f()
+            return dict(F=np.asarray(F), E=np.asarray(E), fave=np.asarray(P.thrust_fave()),
+                        gauss=np.asarray(P.gauss_residual()), ms=ms, pushed=int(c1[3] - c0[3]), rc=int(rc))
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    out = []
+    for mult in (0.5, 1.0, 2.0):
+        r64 = run(64, 32.0 * mult, 1)
+        r32 = run(32, 32.0 * mult, 0)
+        out.append({"dipole": mult, "coil_i": 32.0 * mult,
+                    "F_rel_err": rel(r32["F"], r64["F"]), "F_total_rel_err": rel(r32["F"][:3], r64["F"][:3]),
+                    "fave_rel_err": rel(r32["fave"], r64["fave"]),
+                    "E_rel_err": [abs(r32["E"][q] / r64["E"][q] - 1) for q in range(4)],
+                    "gauss_rel_err": [abs(r32["gauss"][q] / r64["gauss"][q] - 1) for q in range(3)],
+                    "fp32": {"value": r32["pushed"] / (r32["ms"] / 1e3), "ms_per_step": r32["ms"] / steps,
+                             "status": r32["rc"]},
+                    "fp64_slot_order": {"value": r64["pushed"] / (r64["ms"] / 1e3), "ms_per_step": r64["ms"] / steps,
+                                        "status": r64["rc"]},
+                    "particles": r32["pushed"] // max(steps, 1)})
+        log(json.dumps(out[-1]))
+    return {"workload": f"{grid}^3 cells x {ppc} ppc/species, {steps} steps, dipole x0.5 / x1 / x2, "
+                        "FP32 (tiled) against FP64 (slot order) from the same seed", "runs": out}
+
+
 def combine_over_ranks(ms: float, pushed: float, dist=None, device: str = "cuda"):
     """Whole-job numbers of the replicas: the slowest rank's time and the
     particle pushes of all ranks (max and sum over the process group)."""
@@ -496,6 +572,9 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--no-poisson", action="store_true", help="skip the Poisson cleaning measurement")
     ap.add_argument("--no-thrust", action="store_true", help="skip the FP32-vs-FP64 thrust error leg")
+    ap.add_argument("--configs2", action="store_true",
+                    help="only the 256^3 x 32 ppc FP32-vs-FP64 comparison at three dipole moments (minutes)")
+    ap.add_argument("--configs2-steps", type=int, default=100)
     ap.add_argument("--thrust-steps", type=int, default=200, help="steps of the thrust error leg")
     ap.add_argument("--runs2d", type=int, default=256, help="runs of the batched 2D workload")
     ap.add_argument("--adjoint-steps", type=int, default=200, help="steps of the adjoint measurement")
@@ -512,24 +591,36 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        name = "cube32"
-        if not ensure_reference_lib(name):
-            print(json.dumps({"impl": "reference", "unavailable": "compiled reference library missing"}))
+        name = "cube128_t64"
+        if (NX, NY, NZ, PPC) != (128, 128, 128, 64) or not ensure_reference_lib(name):
+            print(json.dumps({"impl": "reference", "unavailable": "compiled reference library missing "
+                                                                   "or not built for this grid"}))
             return
-        procs = max(1, min(os.cpu_count() or 1, 64))
-        value, res = reference_baseline(name, max(args.steps // 4, 2), min(args.warmup, 2), procs)
-        cfg = {"workload": "3D PIC solar wind + dipole, 128^3 cells x 64 ppc/species",
-               "sample": f"{procs} processes x 32^3 cells x 8 ppc/species",
-               "grid": [NX, NY, NZ], "ppc_per_species": PPC}
+        threads = min(host_threads(), 64)
+        r = reference_threaded(name, [(threads, args.steps)], min(args.warmup, 3))[0]
+        value = r["psteps"] / r["secs"]
+        cfg = {"workload": f"3D PIC solar wind + dipole (normalized units), {NX}x{NY}x{NZ} cells x "
+                           f"{PPC} particles/cell/species, sort every 20, refill every 5",
+               "grid": [NX, NY, NZ], "ppc_per_species": PPC, "particles": r["particles"],
+               "sample": f"the full workload; {r['steps']} timed fdtd loop bodies after "
+                         f"{min(args.warmup, 3)} untimed ones (init {r['init_s']:.0f} s, untimed)",
+               "threads": threads, "particle_lists": r["lists"]}
         print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
-                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "n_gpus": args.gpus, "steps": r["steps"], "warmup": min(args.warmup, 3),
+                          "ms_per_step": r["secs"] / max(r["steps"], 1) * 1e3,
                           "higher_is_better": True, "scaling": "weak", "dtype": "f64",
                           "data": "synthetic", "config": cfg,
-                          "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs,
-                                           "kind": "reference",
-                                           "sample": cfg["sample"] + ", fdtd loop body"},
+                          "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                                           "kind": "reference", "sample": cfg["sample"]},
                           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": 0}}))
+        return
+
+    if args.configs2:
+        import torch
+
+        torch.cuda.set_device(0)
+        print(json.dumps({"configs2": run_configs2(args.configs2_steps)}))
         return
 
     import torch
@@ -618,13 +709,15 @@ def main():
 
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
-        if ensure_reference_lib("cube64"):
-            with tempfile.TemporaryDirectory() as d:
-                cwd = os.getcwd()
-                psteps, secs, n = reference_sample("cube64", 4, 1, d)
-                os.chdir(cwd)
-            cpu = {"value": psteps / secs, "unit": UNIT, "cores": 1, "kind": "reference",
-                   "sample": f"reference fdtd loop body, 64^3 cells x 16 ppc/species ({n} particles), 4 steps"}
+        if ensure_reference_lib("quarter128_t64"):
+            threads = min(host_threads(), 64)
+            r, r1 = reference_threaded("quarter128_t64", [(threads, 2), (1, 1)], 1, budget_s=30.0)
+            cpu = {"value": r["psteps"] / r["secs"], "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"the reference with OpenMP on a quarter of the workload's volume, 64x64x128 cells x "
+                             f"64 ppc/species ({r['particles']} particles), {r['steps']} fdtd loop bodies",
+                   "one_core": {"value": r1["psteps"] / r1["secs"], "cores": 1,
+                                "sample": f"the same, one thread (the reference as shipped, active_thread 1), "
+                                          f"{r1['steps']} loop body"}}
         else:
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": "compiled reference library missing"}

@@ -85,6 +85,13 @@ typedef struct pic_config {
   int plain_fields;        /* 0: renew_b4_2 / renew_e4_2 with TMA-staged stencil operands wherever the
                               row pitch (nz + 4 values) is a multiple of 16 bytes; 1: the per-node
                               kernels everywhere (same arithmetic, for comparison) */
+  int slot_order;          /* 0 (default): the tiled, cell-sorted particle layout and its sort, two
+                              record buffers per species; 1: particles in slot order, never sorted
+                              (sorting only reorders, :7475-7590), one record buffer per species: half
+                              the particle memory, the one-thread-per-particle push. Refills append
+                              and removed particles leave empty slots, so the capacity bounds the
+                              number of refills a run can take (the default capacity, 1.8 np per
+                              cell, holds about 100 steps of refills). The adjoint needs 0 */
 } pic_config;
 
 typedef struct pic_ctx pic_ctx;

@@ -86,7 +86,21 @@ REF_CONFIGS = {
     "wide16": {**NORMALIZED, **_geom(16, 8, 8, 4)},
     "tiny_2x2": {**NORMALIZED, **_geom(8, 8, 8, 4, pnx=2, pny=2)},
     "damped_2x2": {**NORMALIZED, **_geom(8, 8, 10, 2, absorb=2, absorb2=3, pnx=2, pny=2), "ORACLE_SIGMA_A": 0.05},
+    # the benchmark workload, 128^3 cells x 64 particles/cell/species, with
+    # OpenMP on: THREAD_N = active_thread = 64 particle lists and threads (the
+    # reference ships THREAD_N 4 and active_thread 1 and is built with -h omp);
+    # ref_set_threads picks the threads of a run, 1 for the shipped setting
+    "cube128_t64": {**NORMALIZED, **_geom(128, 128, 128, 64, threads=64, pack=20000),
+                    "ORACLE_ACTIVE_THREADS": 64},
 }
+
+# a quarter of that volume, 64 x 64 x 128 cells x 64 particles/cell/species:
+# a bounded CPU sample of the same workload
+REF_CONFIGS["quarter128_t64"] = {**NORMALIZED, **_geom(64, 64, 128, 64, threads=64, pack=20000),
+                                 "ORACLE_ACTIVE_THREADS": 64}
+
+# geometries that are large to build or run and are built only on request
+ON_REQUEST = {"cube128_t64", "quarter128_t64"}
 
 
 # The 2D reference (PIC2D/2d_pic278_mpi.c) in normalized units: c = e0 = mu0 =
@@ -171,9 +185,12 @@ def build_ref(name: str, force: bool = False) -> str:
                          check=True, capture_output=True)
     with open(os.path.join(HERE, "ref_harness.c"), "rb") as f:
         tu = sed.stdout + b"\n" + f.read()
+    # OpenMP for the threaded configurations; their static per-thread grids
+    # (grid_thread[THREAD_N][...], :149) pass 2 GB, beyond the small code model
+    omp = (["-fopenmp", "-mcmodel=medium"] if REF_CONFIGS[name].get("ORACLE_ACTIVE_THREADS", 1) > 1 else [])
     cmd = ["gcc", "-x", "c", "-", "-x", "none",
            os.path.join(HERE, "shim", "gsl_shim.c"), os.path.join(HERE, "shim", "mpi_shim.c"),
-           "-std=gnu11", "-O2", "-ffp-contract=off", "-fgnu89-inline", "-fPIC", "-shared", "-w",
+           "-std=gnu11", "-O2", "-ffp-contract=off", "-fgnu89-inline", "-fPIC", "-shared", "-w", *omp,
            "-I", os.path.join(HERE, "shim"), "-include", os.path.join(HERE, "ref_pre.h"),
            *defs, "-lm", "-lpthread", "-o", out]
     subprocess.run(cmd, input=tu, check=True)
@@ -199,7 +216,7 @@ def build_all(force: bool = False) -> None:
     build_oracle(force)
     if reference_available():
         for name in REF_CONFIGS:
-            build_ref(name, force)
+            build_ref(name, force and name not in ON_REQUEST)
     if os.path.isfile(REF2D_SRC):
         for name in REF2D_CONFIGS:
             build_ref2d(name, force)

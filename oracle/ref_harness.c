@@ -243,11 +243,13 @@ static void h_drift_n_list(Particle *start, int thread, int electron)
   }
 }
 
-/* Thread-accumulator reduction, restated from fdtd :869-886. */
+/* Thread-accumulator reduction, restated from fdtd :869-886 (parallel over k,
+ * as there, when built with OpenMP). */
 static void h_reduce_threads(void)
 {
   int i, k, l, m;
   for (i = 0; i < THREAD_N; i++)
+#pragma omp parallel for private(l, m)
     for (k = 0; k < Grid_Nx + 4; k++)
       for (l = 0; l < Grid_Ny + 4; l++)
         for (m = 0; m < Grid_Nz + 4; m++) {
@@ -413,12 +415,15 @@ static void h_loop(void *a)
     }
     renew_b4_2();
     sr_b(h_rx(), h_ry());
+    /* one list per thread, as fdtd's parallel loops (:731, :818) */
+#pragma omp parallel for num_threads(active_thread)
     for (i = 0; i < THREAD_N; i++) {
       h_push_j_list(h_ion_start[i], i, 0);
       h_push_j_list(h_el_start[i], i, 1);
     }
     renew_b4_2();
     sr_b(h_rx(), h_ry());
+#pragma omp parallel for num_threads(active_thread)
     for (i = 0; i < THREAD_N; i++) {
       h_drift_n_list(h_ion_start[i], i, 0);
       h_drift_n_list(h_el_start[i], i, 1);
@@ -442,6 +447,19 @@ int ref_loop(int nsteps, int sort_every, int add_every)
 }
 
 void ref_fave(double *out) { memcpy(out, Fave, sizeof(Fave)); }
+
+/* Threads of the OpenMP loops (active_thread, :110, and the default team
+ * size, as main_func's omp_set_num_threads(active_thread) :214 sets it);
+ * returns THREAD_N, the number of particle lists. Without OpenMP every loop
+ * runs on the calling thread. */
+int ref_set_threads(int n)
+{
+  active_thread = n;
+#ifdef _OPENMP
+  omp_set_num_threads(n);
+#endif
+  return THREAD_N;
+}
 int ref_unmatched_sends(void) { return oracle_mpi_unmatched(); }
 
 /* --- the reference's own file writers and reader ----------------------- */

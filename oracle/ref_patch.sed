@@ -20,6 +20,7 @@ s|^#define Step 300001$|#define Step oracle_steps|
 s|^#define Absorb_grid 32 .*|#define Absorb_grid ORACLE_ABSORB|
 s|^#define Absorb_grid2 40 .*|#define Absorb_grid2 ORACLE_ABSORB2|
 s|^#define THREAD_N 4$|#define THREAD_N ORACLE_THREADS|
+s|^int active_thread=1;$|int active_thread=ORACLE_ACTIVE_THREADS;|
 s|^#define PROCESS_Nx 128$|#define PROCESS_Nx ORACLE_PNX|
 s|^#define PROCESS_Ny 128$|#define PROCESS_Ny ORACLE_PNY|
 s|^#define PACK_N 80000$|#define PACK_N ORACLE_PACK_N|

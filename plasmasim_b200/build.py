@@ -24,17 +24,20 @@ def _newest_input() -> float:
     return max(os.path.getmtime(f) for f in files)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and os.path.isfile(LIB) and os.path.getmtime(LIB) >= _newest_input():
-        return LIB
+def build(force: bool = False, verbose: bool = False, out: str = LIB, defines=()) -> str:
+    """nvcc of the library sources for sm_100a into `out` (the in-tree
+    library by default); `defines` are extra -D flags of a variant build."""
+    if not force and os.path.isfile(out) and os.path.getmtime(out) >= _newest_input():
+        return out
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
-           "-I", os.path.join(ROOT, "include"),
-           "-o", LIB, *SOURCES]
+           "-I", os.path.join(ROOT, "include"), *(f"-D{d}" for d in defines),
+           "-o", out, *SOURCES]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)
-    build_driver()
-    return LIB
+    if out == LIB:
+        build_driver()
+    return out
 
 
 DRIVER = os.path.join(HERE, "pic3d_main")

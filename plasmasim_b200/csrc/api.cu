@@ -231,6 +231,10 @@ PushConst<real> push_const(const pic_ctx* c, int s) {
   pc.bal_hx = g.gnx + 4 - k.absorb_grid2 - g.ox;
   pc.bal_hy = g.gny + 4 - k.absorb_grid2 - g.oy;
   pc.bal_hz = k.nz + 4 - k.absorb_grid2;
+  // interior cells are [2, n + 2) on each axis; a particle there is ballistic
+  // when it lies below bal_l* or at or above bal_h* (fdtd :733-735)
+  pc.bal_interior = pc.bal_lx > 2 || pc.bal_ly > 2 || pc.bal_lz > 2 || pc.bal_hx < k.nx + 2 ||
+                    pc.bal_hy < k.ny + 2 || pc.bal_hz < k.nz + 2;
   pc.out = Outbox<real>{nullptr, 0, nullptr};
   if (c->has_xport && c->mig) {  // list s of the packet lists is species s's outbox
     pc.out.count = c->mig_cnt + s;
@@ -1112,7 +1116,7 @@ int do_step(pic_ctx* c) {
     // layout is already refreshed by the re-layout after every refill, so the
     // periodic sort runs only when that has not happened for half a sort
     // interval.
-    if (c->since_layout >= std::max(1, c->cfg.sort_interval / 2)) {
+    if (!c->cfg.slot_order && c->since_layout >= std::max(1, c->cfg.sort_interval / 2)) {
       CKR(phase_mark(c, PH_SORT));
       CKR(do_sort<real>(c));
       CKR(phase_mark(c, PH_SORT));
@@ -1127,7 +1131,7 @@ int do_step(pic_ctx* c) {
   CKR(phase_mark(c, PH_FIELD));
   CKR(do_renew_b<real>(c));
   CKR(phase_mark(c, PH_FIELD));
-  if (!c->tiled[0] || !c->tiled[1]) {  // after a refill or an import
+  if (!c->cfg.slot_order && (!c->tiled[0] || !c->tiled[1])) {  // after a refill or an import
     CKR(phase_mark(c, PH_SORT));
     const bool which[2] = {!c->tiled[0], !c->tiled[1]};
     CKR(relayout_species<real>(c, which));
@@ -1453,6 +1457,7 @@ const char* pic_error_string(int code) {
     case PIC_ERR_STATE: return "call out of order";
     case PIC_ERR_DEVICE: return "device counters report lost work";
     case PIC_ERR_TOO_LARGE: return "input larger than the fixed-size scratch allows";
+    case PIC_ERR_COMM: return "an exchange between ranks failed";
     default: return "unknown error";
   }
 }
@@ -1501,6 +1506,7 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
     return PIC_ERR_ARG;
   if (k.np < 1 || !(k.dx > 0) || !(k.dt > 0) || !(k.c > 0) || !(k.mi > 0) || !(k.me > 0)) return PIC_ERR_ARG;
   if (k.precision != 32 && k.precision != 64) return PIC_ERR_ARG;
+  if (k.slot_order != 0 && k.slot_order != 1) return PIC_ERR_ARG;
   if (k.add_interval < 1 || k.sort_interval < 1) return PIC_ERR_ARG;
   if (k.absorb_grid3 < 0 || (k.poisson_clean != 0 && k.poisson_clean != 1)) return PIC_ERR_ARG;
   if (k.procs_x < 1 || k.procs_y < 1 || k.rank_x < 0 || k.rank_y < 0 || k.rank_x >= k.procs_x ||
@@ -1552,18 +1558,20 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
   }
   if (c->prec == 64) setup_staged_fields<double>(c);
   else setup_staged_fields<float>(c);
+  const bool tiled = k.slot_order == 0;
   long long cap = k.capacity;
   if (cap <= 0) {
     // the tiled layout gives every lane column room for its fullest cell plus
     // a refill reserve (refill_reserve): about np + 3 sqrt(np) + 2 slots per
-    // cell, plus an eighth, plus 4; a few more for the unplaced tail
-    const double per_cell = 1.125 * (k.np + 3.0 * std::sqrt((double)k.np) + 2.0) + 6.0;
+    // cell, plus an eighth, plus 4; a few more for the unplaced tail. Slot
+    // order keeps the initial load and the refills of about 100 steps.
+    const double per_cell = tiled ? 1.125 * (k.np + 3.0 * std::sqrt((double)k.np) + 2.0) + 6.0 : 1.8 * k.np;
     cap = (long long)(per_cell * k.nx * k.ny * k.nz) + 65536;
   }
   if (cap > 0x7fffffffLL) return fail(PIC_ERR_ARG);
   for (int s = 0; s < 2; ++s) {
     c->sp[s].cap = cap;
-    for (int b = 0; b < 2; ++b)
+    for (int b = 0; b < (tiled ? 2 : 1); ++b)
       if (cudaMalloc(&c->sp[s].mem[b], store_bytes(cap, c->rsize)) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->sp[s].count_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
     cudaMemsetAsync(c->sp[s].count_dev, 0, sizeof(int), c->stream);
@@ -1588,9 +1596,11 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
     if (cudaMalloc(&c->gcap, sizeof(int) * t.ngroups) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->total_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->append_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
-    if (cudaMalloc(&c->holes, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
-    if (cudaMalloc(&c->rank, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
-    if (cudaMalloc(&c->bucket, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    if (tiled) {  // re-layout scratch
+      if (cudaMalloc(&c->holes, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
+      if (cudaMalloc(&c->rank, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
+      if (cudaMalloc(&c->bucket, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
+    }
     if (cudaFuncSetAttribute(push_tiled_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)PushSmem<double>::bytes) != cudaSuccess ||
         cudaFuncSetAttribute(push_tiled_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1729,6 +1739,7 @@ int pic_add_flat(pic_ctx* c) {
 
 int pic_sort(pic_ctx* c) {
   CKR(check_ctx(c));
+  if (c->cfg.slot_order) return PIC_OK;  // slot order: sorting only reorders, so there is nothing to do
   return DISPATCH(c, do_sort)(c);
 }
 
@@ -1772,6 +1783,7 @@ int pic_poisson_clean(pic_ctx* c) {
 int pic_objective(pic_ctx* c, int nsteps, double* J) {
   CKR(check_ctx(c));
   if (!J || nsteps < 0) return PIC_ERR_ARG;
+  if (c->cfg.slot_order) return PIC_ERR_ARG;  // its compaction needs the second record buffer
   if (c->cfg.poisson_clean) return PIC_ERR_ARG;  // the adjoint does not differentiate the cleaning
   if (c->has_xport || c->cfg.procs_x * c->cfg.procs_y > 1) return PIC_ERR_ARG;  // single domain only
   if (!c->grid_ready) return PIC_ERR_STATE;
@@ -1784,6 +1796,7 @@ int pic_objective(pic_ctx* c, int nsteps, double* J) {
 int pic_adjoint(pic_ctx* c, int nsteps, int checkpoint_every, double* out3) {
   CKR(check_ctx(c));
   if (!out3 || nsteps < 1 || checkpoint_every < 1) return PIC_ERR_ARG;
+  if (c->cfg.slot_order) return PIC_ERR_ARG;
   if (c->cfg.poisson_clean) return PIC_ERR_ARG;
   if (c->has_xport || c->cfg.procs_x * c->cfg.procs_y > 1) return PIC_ERR_ARG;
   if (!c->grid_ready) return PIC_ERR_STATE;

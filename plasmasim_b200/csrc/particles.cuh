@@ -177,6 +177,7 @@ struct PushConst {
   // Absorb_grid2 - offset below, N_global + 4 - Absorb_grid2 - offset above
   int bal_lx, bal_ly, bal_lz;
   int bal_hx, bal_hy, bal_hz;
+  int bal_interior;            // the ballistic region reaches an interior cell of this rank
   int pjx, pjy, pjz, pn;       // deposit planes of this species
   Outbox<real> out;            // decomposed runs: particles leaving the rank's x-y interior
 };

@@ -9,6 +9,20 @@ namespace pb {
 
 constexpr int kStages = 3;   // particle rows in flight per warp
 
+#ifndef PB_TILE_FASTPATH
+#define PB_TILE_FASTPATH 1
+#endif
+
+// The tile's interior cells: first cell (ci0, cj0, ck0) and extents (the
+// nominal tile clipped at the last interior cell, n + 1, of each axis).
+struct TileBox {
+  int ci0, cj0, ck0;
+  unsigned ex, ey, ez;
+  __device__ __forceinline__ bool has(int i, int j, int k) const {
+    return (unsigned)(i - ci0) < ex && (unsigned)(j - cj0) < ey && (unsigned)(k - ck0) < ez;
+  }
+};
+
 // Shared-memory plan of one CTA (8 warps): the J/n window, per warp a ring of
 // kStages particle rows fetched ahead with cp.async (records A and B of each
 // slot) and, in FP32, the tile's E and B as node quads (FieldQuads below; the
@@ -241,6 +255,8 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   // FP32: E and B of the tile's gather stencils as node quads
   float4* fq = reinterpret_cast<float4*>(smem_raw + S::fwin_off);
   const int ci0 = wx0 + 2, cj0 = wy0 + 2, ck0 = wz0 + 2;  // the tile's first cell
+  const TileBox tb{ci0, cj0, ck0, (unsigned)min(kTileX, g.nx + 2 - ci0), (unsigned)min(kTileY, g.ny + 2 - cj0),
+                   (unsigned)min(kLanes, g.nz + 2 - ck0)};
   if constexpr (S::kFieldWin) fill_quads<S::QX, S::QY, S::QZ>(fq, F, g, ci0, cj0, ck0);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -287,8 +303,17 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       unpack_cell(c, i, j, k);
       fx = rec[1]; fy = rec[2]; fz = rec[3];
       vx = rec[4]; vy = rec[5]; vz = rec[6];
+      // a particle in one of the tile's cells is in an interior cell: its
+      // stencils lie in the array, and it is ballistic only when the
+      // Absorb_grid2 layer reaches interior cells
+      const bool inside = tb.has(i, j, k);
+#if PB_TILE_FASTPATH
+      bool bal = (pc.bal_interior || !inside) && ballistic(pc, i, j, k, fx, fy, fz);
+      if (!bal && !inside && !stencil_ok(g, i, j, k)) {
+#else
       bool bal = ballistic(pc, i, j, k, fx, fy, fz);
       if (!bal && !stencil_ok(g, i, j, k)) {
+#endif
         count_err(err, ERR_DEPOSIT_OOB);
         bal = true;
       }
@@ -296,8 +321,6 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
         const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
         if constexpr (S::kFieldWin) {
           // the quads cover the stencils of particles in the tile's cells
-          const bool inside = (unsigned)(i - ci0) < (unsigned)kTileX && (unsigned)(j - cj0) < (unsigned)kTileY &&
-                              (unsigned)(k - ck0) < (unsigned)kLanes;
           if (inside)
             boris4_fast(pc, gather6_quads<S::QY, S::QZ>(fq, ci0, cj0, ck0, X, Y, Z), vx, vy, vz);
           else
@@ -329,8 +352,14 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       advance(j, fy, vy * pc.hdt);
       advance(k, fz, vz * pc.hdt);
       // n at x^{n+1}
+#if PB_TILE_FASTPATH
+      const bool inside1 = tb.has(i, j, k);
+      if (inside1 || in_array(g, i, j, k)) {
+        if (inside1 || stencil_ok(g, i, j, k)) {
+#else
       if (in_array(g, i, j, k)) {
         if (stencil_ok(g, i, j, k)) {
+#endif
           const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
           if constexpr (kFixedN)
             scatter8_win_fixed(reinterpret_cast<unsigned*>(wn), wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b,
@@ -341,7 +370,13 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
           count_err(err, ERR_DEPOSIT_OOB);
         }
       }
-      store_records(P, t, settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err), fx, fy, fz, vx, vy, vz);
+#if PB_TILE_FASTPATH
+      // sr_particle keeps a particle of an interior cell where it is
+      const int cnew = inside1 ? pack_cell(i, j, k) : settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
+#else
+      const int cnew = settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
+#endif
+      store_records(P, t, cnew, fx, fy, fz, vx, vy, vz);
     }
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);

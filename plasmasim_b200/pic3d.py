@@ -52,7 +52,7 @@ class _CConfig(C.Structure):
         ("diag_every_step", C.c_int), ("poisson_clean", C.c_int),
         ("capacity", C.c_longlong), ("seed_p", C.c_ulonglong), ("seed_v", C.c_ulonglong),
         ("absorb_grid3", C.c_int), ("procs_x", C.c_int), ("procs_y", C.c_int),
-        ("rank_x", C.c_int), ("rank_y", C.c_int), ("plain_fields", C.c_int),
+        ("rank_x", C.c_int), ("rank_y", C.c_int), ("plain_fields", C.c_int), ("slot_order", C.c_int),
     ]
 
 
@@ -101,6 +101,7 @@ class PicConfig:
     rank_x: int = 0
     rank_y: int = 0
     plain_fields: int = 0
+    slot_order: int = 0
 
     @classmethod
     def normalized(cls, nx, ny, nz, np_, **kw) -> "PicConfig":
@@ -156,11 +157,14 @@ PHASES = ["push", "field", "sort", "add", "diag"]
 _lib = None
 
 
-def load_library(path: str = LIB_PATH):
-    """Loads the CUDA library; raises if it has not been built."""
+def load_library(path: str = ""):
+    """Loads the CUDA library; raises if it has not been built. The path is
+    the in-tree build unless PLASMA_B200_LIB names another build of the same
+    sources (for comparing builds side by side)."""
     global _lib
     if _lib is not None:
         return _lib
+    path = path or os.environ.get("PLASMA_B200_LIB") or LIB_PATH
     if not os.path.isfile(path):
         raise FileNotFoundError(
             f"{path} is missing: build it with `python -m plasmasim_b200.build` "

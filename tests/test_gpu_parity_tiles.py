@@ -208,3 +208,61 @@ def test_fp32_against_fp64_hundred_steps(record):
     assert errs["F"] <= 5e-2
     assert errs["fave"] <= 5e-2
     assert max(errs["E"]) <= 1e-2
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_slot_order_matches_oracle(precision, record):
+    """pic_config.slot_order = 1 (one record buffer per species, never sorted,
+    the one-thread-per-particle push): one step from the same state as the
+    oracle on 41 x 22 x 70 cells, then 20 steps of fdtd (four refills) against
+    the oracle's integrated quantities, as the tiled path is checked."""
+    nx, ny, nz, np_ = SHAPES["ragged"]
+    p = oracle_params_for(nx, ny, nz, np_)
+    O = Oracle(p)
+    O.call("init_grid")
+    O.call("init_particle_flat")
+    rows = _initial_rows(O)
+    cfg = config_from_oracle_params(p, precision=precision, diag_every_step=0, slot_order=1)
+    tol = STEP_TOL[precision]
+    with Pic3D(cfg) as P:
+        P.init_grid()
+        for s in (ION, ELECTRON):
+            P.set_particles(s, rows[s])
+        for s in (ION, ELECTRON):
+            O.set_particles(s, P.particles(s))
+        O.step()
+        P.step(1)
+        errs = {}
+        for s in (ION, ELECTRON):
+            mine, ref = match_rows(P.particles(s), O.particles(s)[0])
+            e = step_errors(mine, ref, p["dt"], p["dx"])
+            errs[("ion", "electron")[s]] = e
+            for k, v in e.items():
+                assert v <= tol[k], (s, k, v)
+        errs["grid"] = max(field_rel_err(P.grid(), O.grid(), range(17)).values())
+        assert errs["grid"] <= tol["grid"]
+        P.sorting()  # nothing to reorder in slot order
+        assert P.status()[0] == 0
+    O = make_oracle("tiny")
+    O.call("init_grid")
+    O.call("init_particle_flat")
+    O.fdtd(20)
+    cfg = config_from_oracle_params(oracle_params("tiny"), precision=precision, diag_every_step=0, slot_order=1)
+    with Pic3D(cfg) as P:
+        P.init_grid()
+        P.init_particle_flat()
+        P.fdtd(20)
+        counts = [P.particle_count(s) for s in (ION, ELECTRON)]
+        F, E = P.thrust_f()
+        g = P.grid()
+        assert P.status()[0] == 0
+    ref = O.thrust()
+    og = O.grid()
+    errs["count20"] = max(abs(a - O.particles(s)[0].shape[0]) / O.particles(s)[0].shape[0]
+                          for s, a in zip((0, 1), counts))
+    errs["E20"] = [abs(E[q] / ref[27 + q] - 1) for q in (2, 3)]
+    errs["density20"] = [abs(g[..., f].sum() / og[..., f].sum() - 1) for f in (15, 16)]
+    record.update(precision=precision, errors=errs)
+    tol20 = 1e-9 if precision == 64 else 1e-3
+    assert errs["count20"] <= (2 / 2000 if precision == 64 else 0.005)
+    assert max(errs["E20"]) <= tol20 and max(errs["density20"]) <= tol20
