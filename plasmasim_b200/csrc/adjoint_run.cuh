@@ -149,6 +149,7 @@ int adj_restore(pic_ctx* c, const AdjSnap& S) {
     CKR(set_count(c, s, S.count[s]));
     c->tiled[s] = false;
     c->layout[s] = false;
+    c->sp[s].listed = false;
   }
   CK(cudaMemcpyAsync((char*)c->field_mem + (size_t)F_EX * c->plane_bytes, S.planes,
                      kSnapPlanes * c->plane_bytes, cudaMemcpyDeviceToDevice, c->stream));
@@ -207,6 +208,7 @@ int adj_compact(pic_ctx* c, AdjRun& R, int s, int* map) {
   st.cur = 1 - st.cur;
   c->tiled[s] = false;
   c->layout[s] = false;
+  c->sp[s].listed = false;
   R.pend[s] = true;
   R.pend_added[s] = 0;
   return PIC_OK;
@@ -267,7 +269,7 @@ int adj_forward_step(pic_ctx* c, AdjRun& R, AdjSnap* rec, bool objective, bool d
     for (int s = 0; s < 2; ++s) {
       Store& st = c->sp[s];
       if (st.count > 0) {
-        delete_shell_kernel<real><<<particle_blocks(st.count), kThreads, 0, c->stream>>>(parts<real>(c, s),
+        delete_shell_kernel<real><<<particle_blocks(st.count), kThreads, 0, c->stream>>>(parts<real>(c, s), 0,
                                                                                          st.count_dev, c->g);
         CKL();
       }

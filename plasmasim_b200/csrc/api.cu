@@ -28,6 +28,13 @@
 
 using namespace pb;
 
+// 1: pic_step's push lists the holes and moves particles that left their home
+// cells out of the layout, and every step places them (no classify pass);
+// 0: a classify pass re-lays the particles after each refill
+#ifndef PB_RELIST
+#define PB_RELIST 1
+#endif
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -36,12 +43,23 @@ struct Store {
   void* mem[2] = {nullptr, nullptr};  // double-buffered for the sort
   int cur = 0;
   long long cap = 0;
-  long long count = 0;  // slots in use (live and empty), mirrored in *count_dev
+  long long count = 0;  // slots in use (live and empty); the host's copy of *count_dev unless `pending`
   int* count_dev = nullptr;
-  // a re-layout has set *count_dev and is reading the spill count back into
-  // pinned memory; `count` is stale until relayout_resolve
+  // *count_dev has moved on without the host (a placement, a re-listing push,
+  // a refill appended on the device): kernels cover the slots up to the
+  // capacity and stop at *count_dev, and sync_count reads it back when the
+  // host needs it
   bool pending = false;
+  // a placement's spill count and non-home flag are on their way into pinned
+  // memory (event `readback`); check_spill acts on them
+  bool spill_pending = false;
   cudaEvent_t readback = nullptr;
+  // the layout's holes are those the last push listed (its RELIST form), so
+  // the next placement needs no classify pass
+  bool listed = false;
+  int* holes = nullptr;   // per-slot scratch: hole rows of every lane column
+  int* nholes = nullptr;  // per interior cell: holes of its lane column
+  int* nonhome = nullptr; // a particle outside its home cell stayed in the layout
 };
 
 // Device blocks of the adjoint runs: each block is allocated on first need,
@@ -83,7 +101,6 @@ struct pic_ctx {
   int* gcap = nullptr;
   int* total_dev = nullptr;
   int* append_dev = nullptr;          // end of the append region during a re-layout
-  int* holes = nullptr;               // per-slot scratch: hole rows of every lane column
   int* rank = nullptr;                // per-slot scratch: placement rank of every appended particle
   int* bucket = nullptr;              // per-slot scratch: appended particles bucketed by their new cell
   int* cnt = nullptr;
@@ -112,7 +129,7 @@ struct pic_ctx {
   int mig_cap = 0;
   unsigned long long* err = nullptr;  // ERR_COUNT
   DevPool adj_pool;                   // the adjoint's work and snapshot memory
-  int* host_pin = nullptr;            // pinned read-back slots (re-layout spill counts)
+  int* host_pin = nullptr;            // pinned read-back slots: per species the spill count, the non-home flag
   // import/export staging
   void* stage = nullptr;
   size_t stage_bytes = 0;
@@ -196,8 +213,9 @@ int particle_blocks(long long n) {
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
 
 int set_count(pic_ctx* c, int s, long long n) {
-  if (n != c->sp[s].count) c->tiled[s] = false;  // appended or imported slots break the layout
+  if (n != c->sp[s].count || c->sp[s].pending) c->tiled[s] = false;  // appended or imported slots break the layout
   c->sp[s].count = n;
+  c->sp[s].pending = false;
   set_int_kernel<<<1, 1, 0, c->stream>>>(c->sp[s].count_dev, (int)n);
   CKL();
   return PIC_OK;
@@ -695,22 +713,43 @@ int do_push(pic_ctx* c, int s, long long first = 0) {
   return PIC_OK;
 }
 
+__global__ void copy_int_kernel(int* dst, const int* src) { *dst = *src; }
+
+// The push of species s: the slots after the layout (particles a placement
+// could not place) with the slot-order kernel, then the tiled kernel. With
+// `relist` (pic_step), the tiled push lists every lane's holes and moves the
+// particles that left their home cell to the append region after *count_dev
+// (push_tiled.cuh, Relist), for the next step's placement.
 template <typename real>
-int do_push_tiled(pic_ctx* c, int s) {
+int do_push_tiled(pic_ctx* c, int s, bool relist = false) {
   if (!c->layout[s]) return do_push<real, PUSH_FUSED>(c, s);
-  // the slots after the layout (particles a re-layout could not place) first
+  Store& st = c->sp[s];
   CKR((do_push<real, PUSH_FUSED>(c, s, c->tiled_end[s])));
   const int ntiles = c->tg.ntx * c->tg.nty * c->tg.ntz;
   TileArgs ta{c->tg, c->goff[s][c->lay[s]], c->gmax[s][c->lay[s]]};
   const size_t smem = PushSmem<real>::bytes;
   const bool vec = sizeof(real) == 4 && c->g.gz % 4 == 0;
-  if (vec)
-    push_tiled_kernel<real, true><<<ntiles, kTileX * kTileY * 32, smem, c->stream>>>(
-        parts<real>(c, s), ta, fields<real>(c), c->g, push_const<real>(c, s), c->err);
-  else
-    push_tiled_kernel<real, false><<<ntiles, kTileX * kTileY * 32, smem, c->stream>>>(
-        parts<real>(c, s), ta, fields<real>(c), c->g, push_const<real>(c, s), c->err);
-  CKL();
+  Relist rl{st.holes, st.nholes, c->append_dev, st.nonhome, (int)st.cap};
+  const Parts<real> P = parts<real>(c, s);
+  const Fields<real> F = fields<real>(c);
+  const PushConst<real> pc = push_const<real>(c, s);
+  const dim3 grid(ntiles), block(kTileX * kTileY * 32);
+  if (relist) {
+    copy_int_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, st.count_dev);  // movers go after the current end
+    CKL();
+    if (vec) push_tiled_kernel<real, true, true><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, c->err);
+    else push_tiled_kernel<real, false, true><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, c->err);
+    CKL();
+    clamp_count_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.cap, st.count_dev);
+    CKL();
+    st.pending = true;
+    st.listed = true;
+    c->tiled[s] = false;  // the appended particles await the next placement
+  } else {
+    if (vec) push_tiled_kernel<real, true, false><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, c->err);
+    else push_tiled_kernel<real, false, false><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, c->err);
+    CKL();
+  }
   return PIC_OK;
 }
 
@@ -812,6 +851,8 @@ int do_sort_species(pic_ctx* c, int s) {
   st.cur = 1 - st.cur;
   c->lay[s] = nw;
   CKR(set_count(c, s, total));
+  CK(cudaMemsetAsync(st.nonhome, 0, sizeof(int), c->stream));
+  st.listed = false;
   c->layout[s] = true;
   c->tiled_end[s] = total;
   c->tiled[s] = true;
@@ -819,68 +860,108 @@ int do_sort_species(pic_ctx* c, int s) {
 }
 
 // In-place re-layout (relayout.cuh): movers and appended particles into the
-// holes of their columns. relayout_launch issues the kernels, sets the new
-// count on the device and reads the spill count back into pinned memory
-// without waiting; relayout_resolve waits for that read-back, sets the host
-// count and falls back to a full sort when many particles found no hole.
-// do_step resolves after it has issued the push, so the wait overlaps the
-// push instead of leaving the GPU idle.
+// holes of their columns. The hole lists come from a classify pass
+// (relayout_launch) or from the last push (its RELIST form, place_launch).
+// Both issue the placement, set the new count on the device and read the
+// spill count back into pinned memory without waiting; check_spill acts on
+// that read-back when it has landed (a full sort when many particles found no
+// hole), sync_count reads the count itself when the host needs it.
 __global__ void spill_count_kernel(int* count, int first, const int* nspill) { *count = first + *nspill; }
 
+// The placement of the particles in [tiled_end, *count_dev) into the holes
+// that st.holes / st.nholes list.
 template <typename real>
-int relayout_launch(pic_ctx* c, int s) {
+int place_launch(pic_ctx* c, int s) {
   Store& st = c->sp[s];
   const TileGeom& tg = c->tg;
   const int gblocks = grid_blocks((long long)tg.ngroups * 32);
   const Parts<real> P = parts<real>(c, s);
-  int* nholes = c->cnt;
-  CK(cudaMemsetAsync(c->cursor, 0, sizeof(int) * c->ncells, c->stream));
-  CK(cudaMemsetAsync(c->total_dev, 0, sizeof(int), c->stream));  // overflow count
-  set_int_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.count);
-  CKL();
-  classify_kernel<real><<<gblocks, kThreads, 0, c->stream>>>(P, c->g, tg, c->goff[s][c->lay[s]],
-                                                             c->gmax[s][c->lay[s]], (int)st.cap, c->holes,
-                                                             nholes, c->append_dev);
-  CKL();
-  clamp_count_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.cap, st.count_dev);
-  CKL();
   const long long first = c->tiled_end[s];
   const Parts<real> Q = parts<real>(c, s, 1 - st.cur);
+  CK(cudaMemsetAsync(c->cursor, 0, sizeof(int) * c->ncells, c->stream));
+  CK(cudaMemsetAsync(c->total_dev, 0, sizeof(int), c->stream));  // spill count
   place_count_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
       P, (int)first, st.count_dev, c->g, c->cursor, c->rank);
   CKL();
   int* off = c->offs;  // per cell: arrivals that fit, then their bucket offset
-  place_fit_kernel<<<particle_blocks(c->ncells), kThreads, 0, c->stream>>>(c->cursor, nholes, off, c->ncells);
+  place_fit_kernel<<<particle_blocks(c->ncells), kThreads, 0, c->stream>>>(c->cursor, st.nholes, off, c->ncells);
   CKL();
   CKR(scan_exclusive(c, off, off, c->ncells, c->scan_tmp, c->scan_tmp_len));
   place_bucket_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
-      P, (int)first, st.count_dev, c->g, nholes, off, c->rank, c->bucket, c->total_dev, Q);
+      P, (int)first, st.count_dev, c->g, st.nholes, off, c->rank, c->bucket, c->total_dev, Q);
   CKL();
   place_fill_kernel<real><<<gblocks, kThreads, 0, c->stream>>>(P, (int)first, c->g, tg, c->goff[s][c->lay[s]],
-                                                               c->holes, c->cursor, nholes, off, c->bucket);
+                                                               st.holes, c->cursor, st.nholes, off, c->bucket);
   CKL();
   unspill_kernel<real><<<particle_blocks(st.cap), kThreads, 0, c->stream>>>(Q, c->total_dev, P, (int)first);
   CKL();
   spill_count_kernel<<<1, 1, 0, c->stream>>>(st.count_dev, (int)first, c->total_dev);
   CKL();
   CK(cudaMemcpyAsync(c->host_pin + s, c->total_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->host_pin + 2 + s, st.nonhome, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaEventRecord(st.readback, c->stream));
   st.pending = true;
+  st.spill_pending = true;
+  st.listed = false;
   c->tiled[s] = true;
   return PIC_OK;
 }
 
+// The classify pass (every slot of the layout), then the placement.
 template <typename real>
-int relayout_resolve(pic_ctx* c, int s) {
+int relayout_launch(pic_ctx* c, int s) {
+  Store& st = c->sp[s];
+  const TileGeom& tg = c->tg;
+  const int gblocks = grid_blocks((long long)tg.ngroups * 32);
+  const Parts<real> P = parts<real>(c, s);
+  CK(cudaMemsetAsync(st.nonhome, 0, sizeof(int), c->stream));
+  copy_int_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, st.count_dev);
+  CKL();
+  classify_kernel<real><<<gblocks, kThreads, 0, c->stream>>>(P, c->g, tg, c->goff[s][c->lay[s]],
+                                                             c->gmax[s][c->lay[s]], (int)st.cap, st.holes,
+                                                             st.nholes, c->append_dev, st.nonhome);
+  CKL();
+  clamp_count_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.cap, st.count_dev);
+  CKL();
+  return place_launch<real>(c, s);
+}
+
+// The host's copy of the count, read back from the device when it moved on.
+int sync_count(pic_ctx* c, int s) {
   Store& st = c->sp[s];
   if (!st.pending) return PIC_OK;
-  CK(cudaEventSynchronize(st.readback));
+  int n = 0;
+  CK(cudaMemcpyAsync(&n, st.count_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  st.count = n;
   st.pending = false;
+  return PIC_OK;
+}
+
+// A placement's spill count (waiting for its read-back when `wait`): many
+// particles without a hole, or particles outside their home cells left in
+// the layout, call for a full sort (particles without a hole are pushed in
+// slot order meanwhile).
+template <typename real>
+int check_spill(pic_ctx* c, int s, bool wait) {
+  Store& st = c->sp[s];
+  if (!st.spill_pending) return PIC_OK;
+  if (wait) {
+    CK(cudaEventSynchronize(st.readback));
+  } else {
+    const cudaError_t q = cudaEventQuery(st.readback);
+    if (q == cudaErrorNotReady) {
+      cudaGetLastError();  // not an error: the read-back is still on its way
+      return PIC_OK;
+    }
+    CK(q);
+  }
+  st.spill_pending = false;
   const long long first = c->tiled_end[s];
-  const int nspill = c->host_pin[s];
-  st.count = first + nspill;  // *count_dev holds it already
-  // particles without a hole are pushed in slot order; many of them call for a sort
-  if (nspill > first / 50) return do_sort_species<real>(c, s);
+  if (c->host_pin[s] > first / 50 || c->host_pin[2 + s]) {
+    CKR(sync_count(c, s));
+    return do_sort_species<real>(c, s);
+  }
   return PIC_OK;
 }
 
@@ -890,15 +971,24 @@ template <typename real>
 int relayout_species(pic_ctx* c, const bool (&which)[2]) {
   for (int s = 0; s < 2; ++s) {
     if (!which[s]) continue;
-    if (c->layout[s]) CKR(relayout_launch<real>(c, s));
-    else CKR(do_sort_species<real>(c, s));
+    if (c->sp[s].listed) {
+      CKR(place_launch<real>(c, s));
+    } else if (c->layout[s]) {
+      CKR(relayout_launch<real>(c, s));
+    } else {
+      CKR(sync_count(c, s));
+      CKR(do_sort_species<real>(c, s));
+    }
   }
   return PIC_OK;
 }
 
 template <typename real>
 int resolve_counts(pic_ctx* c) {
-  for (int s = 0; s < 2; ++s) CKR(relayout_resolve<real>(c, s));
+  for (int s = 0; s < 2; ++s) {
+    CKR(check_spill<real>(c, s, true));
+    CKR(sync_count(c, s));
+  }
   return PIC_OK;
 }
 
@@ -973,16 +1063,58 @@ int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0
 }
 
 
+// The count after a refill of `add` particles, stopping at the capacity.
+__global__ void count_add_kernel(int* count, long long add, int cap) {
+  *count = (int)min((long long)*count + add, (long long)cap);
+}
+
+// The refill's particles appended after *count_dev, which the host need not
+// know: the source kernel reads its first slot there, and particles that
+// would pass the capacity are counted as lost (ERR_STORE_FULL) instead.
+template <typename real>
+int do_source_dev(pic_ctx* c, int s, const Slab* slabs, int nslab) {
+  Store& st = c->sp[s];
+  SourceParams sp = source_params(c, s, slabs, nslab, 0);
+  if (sp.total == 0) return PIC_OK;
+  sp.dst_dev = st.count_dev;
+  sp.cap = (int)st.cap;
+  source_kernel<real><<<grid_blocks(sp.total), kThreads, 0, c->stream>>>(parts<real>(c, s), sp, c->err);
+  CKL();
+  count_add_kernel<<<1, 1, 0, c->stream>>>(st.count_dev, sp.total, (int)st.cap);
+  CKL();
+  c->ctr_p += 3 * sp.total;
+  c->ctr_v += 6 * sp.total;
+  st.pending = true;
+  c->tiled[s] = false;
+  return PIC_OK;
+}
+
+// add_*_flat: the shell deletion, then the refill appended (the next step's
+// placement moves it into the layout). On a layout whose holes the last push
+// listed, the count stays on the device: the layout's shell particles are
+// deleted with their rows listed as holes, those after the layout by a scan.
 template <typename real>
 int do_add_flat(pic_ctx* c) {
-  CKR(resolve_counts<real>(c));  // the refill appends after the last re-layout's count
   Slab slabs[5];
   const int nslab = refill_slabs(c, slabs);
   for (int s = 0; s < 2; ++s) {
     Store& st = c->sp[s];
+    const Parts<real> P = parts<real>(c, s);
+    if (st.listed) {
+      shell_relist_kernel<real><<<grid_blocks((long long)c->tg.ngroups * 32), kThreads, 0, c->stream>>>(
+          P, c->g, c->tg, c->goff[s][c->lay[s]], c->gmax[s][c->lay[s]], st.holes, st.nholes, st.nonhome);
+      CKL();
+      const long long first = c->tiled_end[s];
+      delete_shell_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
+          P, (int)first, st.count_dev, c->g);
+      CKL();
+      CKR(do_source_dev<real>(c, s, slabs, nslab));
+      continue;
+    }
+    CKR(check_spill<real>(c, s, true));
+    CKR(sync_count(c, s));
     if (st.count > 0) {
-      delete_shell_kernel<real><<<particle_blocks(st.count), kThreads, 0, c->stream>>>(
-          parts<real>(c, s), st.count_dev, c->g);
+      delete_shell_kernel<real><<<particle_blocks(st.count), kThreads, 0, c->stream>>>(P, 0, st.count_dev, c->g);
       CKL();
     }
     CKR(do_source<real>(c, s, slabs, nslab));  // appended; the next step's re-layout places them
@@ -1001,6 +1133,7 @@ int do_init_particles(pic_ctx* c) {
     CKR(set_count(c, s, 0));
     c->tiled[s] = false;
     c->layout[s] = false;
+    c->sp[s].listed = false;
     const Slab body = {2, c->cfg.nx, 2, c->cfg.ny, 2, c->cfg.nz, 0};
     const Slab extra_cell = {2 + c->cfg.nx, 1, 2, 1, 2, 1, 0};
     CKR(do_source<real>(c, s, &body, 1, 1));
@@ -1099,14 +1232,8 @@ int do_gauss(pic_ctx* c, double* out4) {
 // ------------------------------------------------------------ a step
 template <typename real>
 int do_step(pic_ctx* c) {
-  // a pending re-layout count whose read-back has landed is taken without waiting
-  for (int s = 0; s < 2; ++s) {
-    if (!c->sp[s].pending) continue;
-    const cudaError_t q = cudaEventQuery(c->sp[s].readback);
-    if (q == cudaSuccess) CKR(relayout_resolve<real>(c, s));
-    else if (q == cudaErrorNotReady) cudaGetLastError();  // not an error: the read-back is still on its way
-    else CK(q);
-  }
+  // a placement's spill count that has landed is acted on without waiting
+  for (int s = 0; s < 2; ++s) CKR(check_spill<real>(c, s, false));
   CKR(phase_mark(c, PH_FIELD));
   CKR(do_renew_grid(c));
   CKR(phase_mark(c, PH_FIELD));
@@ -1131,9 +1258,12 @@ int do_step(pic_ctx* c) {
   CKR(phase_mark(c, PH_FIELD));
   CKR(do_renew_b<real>(c));
   CKR(phase_mark(c, PH_FIELD));
-  if (!c->cfg.slot_order && (!c->tiled[0] || !c->tiled[1])) {  // after a refill or an import
+  // placement of the particles the last push moved out of their home cells
+  // (with the holes it listed), or a re-layout after a refill or an import
+  const bool which[2] = {!c->cfg.slot_order && (c->sp[0].listed || !c->tiled[0]),
+                         !c->cfg.slot_order && (c->sp[1].listed || !c->tiled[1])};
+  if (which[0] || which[1]) {
     CKR(phase_mark(c, PH_SORT));
-    const bool which[2] = {!c->tiled[0], !c->tiled[1]};
     CKR(relayout_species<real>(c, which));
     if (which[0] && which[1]) c->since_layout = 0;
     CKR(phase_mark(c, PH_SORT));
@@ -1141,11 +1271,13 @@ int do_step(pic_ctx* c) {
   CKR(phase_mark(c, PH_PUSH));
   if (c->has_xport) CKR(resolve_counts<real>(c));  // the exchange lists are sized from the counts
   if (c->has_xport) CKR(ensure_mig<real>(c));
-  // a re-layout's count stays pending: the push and the diagnostics cover the
+  // the counts stay on the device: the push and the diagnostics cover the
   // slots up to the capacity and stop at the device count, and the host reads
-  // the count back only when it needs it (the next refill, or any other call),
-  // by when the GPU has long passed the re-layout
-  for (int s = 0; s < 2; ++s) CKR(do_push_tiled<real>(c, s));
+  // a count back only when an entry point needs it. A single domain's push
+  // lists the holes and moves the particles that leave their home cells out
+  // of the layout for the next step's placement; a decomposed run's
+  // exchanges append to its counts, and it re-lays its particles after them.
+  for (int s = 0; s < 2; ++s) CKR(do_push_tiled<real>(c, s, PB_RELIST && !c->has_xport));
   if (c->has_xport) CKR(do_migrate<real>(c));  // sr_particle's exchange between ranks
   CKR(phase_mark(c, PH_PUSH));
   CKR(phase_mark(c, PH_FIELD));
@@ -1266,6 +1398,7 @@ int do_import(pic_ctx* c, int s, const double* rows, const int* flag, long long 
   CKR(set_count(c, s, n));
   c->tiled[s] = false;
   c->layout[s] = false;
+  c->sp[s].listed = false;
   CK(cudaStreamSynchronize(c->stream));
   return PIC_OK;
 }
@@ -1428,12 +1561,14 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
 #define DISPATCH(c, call)                      \
   ((c)->prec == 64 ? call<double> : call<float>)
 
-// Every entry point starts here: the context's device, and the particle
-// counts of a re-layout that pic_step left pending read back first.
-int check_ctx(pic_ctx* c) {
+// Every entry point starts here: the context's device, and, unless the entry
+// point works with counts that only the device knows (pic_step, pic_fdtd),
+// the particle counts that earlier steps left on the device read back.
+int check_ctx(pic_ctx* c, bool resolve = true) {
   if (!c) return PIC_ERR_ARG;
   if (cudaSetDevice(c->cfg.device) != cudaSuccess) return PIC_ERR_CUDA;
-  if (c->sp[0].pending || c->sp[1].pending) CKR(DISPATCH(c, resolve_counts)(c));
+  if (resolve && (c->sp[0].pending || c->sp[1].pending || c->sp[0].spill_pending || c->sp[1].spill_pending))
+    CKR(DISPATCH(c, resolve_counts)(c));
   return PIC_OK;
 }
 
@@ -1489,6 +1624,7 @@ int pic_config_default(pic_config* k, int nx, int ny, int nz) {
   k->dipole_cutoff = 210.;
   k->add_interval = 5;
   k->sort_interval = 500;
+  k->procs_x = k->procs_y = 1;  // PROCESS_Nx x PROCESS_Ny = 1 x 1: a single domain
   k->diag_every_step = 1;
   k->poisson_clean = 0;
   k->absorb_grid3 = 40;
@@ -1597,16 +1733,28 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
     if (cudaMalloc(&c->total_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (cudaMalloc(&c->append_dev, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
     if (tiled) {  // re-layout scratch
-      if (cudaMalloc(&c->holes, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
+      for (int s = 0; s < 2; ++s) {  // each species' hole lists live from its push to its next placement
+        if (cudaMalloc(&c->sp[s].holes, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
+        if (cudaMalloc(&c->sp[s].nholes, sizeof(int) * c->ncells) != cudaSuccess) return fail(PIC_ERR_CUDA);
+        if (cudaMalloc(&c->sp[s].nonhome, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
+        cudaMemsetAsync(c->sp[s].nonhome, 0, sizeof(int), c->stream);
+      }
       if (cudaMalloc(&c->rank, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
       if (cudaMalloc(&c->bucket, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
     }
-    if (cudaFuncSetAttribute(push_tiled_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)PushSmem<double>::bytes) != cudaSuccess ||
-        cudaFuncSetAttribute(push_tiled_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)PushSmem<float>::bytes) != cudaSuccess ||
-        cudaFuncSetAttribute(push_tiled_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)PushSmem<float>::bytes) != cudaSuccess)
+    const int pb_f = (int)PushSmem<float>::bytes, pb_d = (int)PushSmem<double>::bytes;
+    if (cudaFuncSetAttribute(push_tiled_kernel<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             pb_d) != cudaSuccess ||
+        cudaFuncSetAttribute(push_tiled_kernel<double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             pb_d) != cudaSuccess ||
+        cudaFuncSetAttribute(push_tiled_kernel<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             pb_f) != cudaSuccess ||
+        cudaFuncSetAttribute(push_tiled_kernel<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             pb_f) != cudaSuccess ||
+        cudaFuncSetAttribute(push_tiled_kernel<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             pb_f) != cudaSuccess ||
+        cudaFuncSetAttribute(push_tiled_kernel<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             pb_f) != cudaSuccess)
       return fail(PIC_ERR_CUDA);
   }
   if (cudaMalloc(&c->acc, sizeof(double) * 64) != cudaSuccess) return fail(PIC_ERR_CUDA);
@@ -1645,7 +1793,11 @@ int pic_destroy(pic_ctx* c) {
   cudaFree(c->gcap);
   cudaFree(c->total_dev);
   cudaFree(c->append_dev);
-  cudaFree(c->holes);
+  for (int s = 0; s < 2; ++s) {
+    cudaFree(c->sp[s].holes);
+    cudaFree(c->sp[s].nholes);
+    cudaFree(c->sp[s].nonhome);
+  }
   cudaFree(c->rank);
   cudaFree(c->bucket);
   cudaFree(c->cnt);
@@ -1708,6 +1860,7 @@ int pic_push_deposit_j(pic_ctx* c, int species) {
   for (int s = 0; s < 2; ++s) {
     if (species >= 0 && s != species) continue;
     CKR((c->prec == 64 ? do_push<double, PUSH_J>(c, s) : do_push<float, PUSH_J>(c, s)));
+    c->sp[s].listed = false;  // particles moved without their holes listed
   }
   return PIC_OK;
 }
@@ -1718,6 +1871,7 @@ int pic_drift_deposit_n(pic_ctx* c, int species) {
   for (int s = 0; s < 2; ++s) {
     if (species >= 0 && s != species) continue;
     CKR((c->prec == 64 ? do_drift_n<double>(c, s) : do_drift_n<float>(c, s)));
+    c->sp[s].listed = false;
   }
   return PIC_OK;
 }
@@ -1729,6 +1883,7 @@ int pic_reduce_current(pic_ctx* c) {
 
 int pic_sr_particle(pic_ctx* c) {
   CKR(check_ctx(c));
+  c->sp[0].listed = c->sp[1].listed = false;
   return DISPATCH(c, do_sr_particle)(c);
 }
 
@@ -1813,14 +1968,14 @@ int pic_gauss_residual(pic_ctx* c, double* out4) {
 }
 
 int pic_step(pic_ctx* c, int nsteps) {
-  CKR(check_ctx(c));
+  CKR(check_ctx(c, false));
   if (!c->grid_ready) return PIC_ERR_STATE;
   for (int i = 0; i < nsteps; ++i) CKR(DISPATCH(c, do_step)(c));
   return PIC_OK;
 }
 
 int pic_fdtd(pic_ctx* c, int nsteps) {
-  CKR(check_ctx(c));
+  CKR(check_ctx(c, false));
   if (!c->grid_ready) return PIC_ERR_STATE;
   c->c_add = 0;
   c->c_thrust = 0;
@@ -1894,7 +2049,7 @@ int pic_status(pic_ctx* c, long long* counters8) {
   int any = 0;
   for (int q = 0; q < ERR_COUNT; ++q) {
     if (counters8) counters8[q] = (long long)h[q];
-    if (q < ERR_FIRST_INFO || q == ERR_MIGRATION || q == ERR_FIELD_WAIT) any |= h[q] != 0;
+    if (q < ERR_FIRST_INFO || q == ERR_MIGRATION || q == ERR_FIELD_WAIT || q == ERR_STORE_FULL) any |= h[q] != 0;
   }
   return any ? PIC_ERR_DEVICE : PIC_OK;
 }

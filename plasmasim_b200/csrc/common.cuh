@@ -100,6 +100,7 @@ enum ErrId {
   ERR_FIRST_INFO = 3, CNT_PUSHED = 3,  // slots from here on count work, not errors
   ERR_MIGRATION = 4,  // sr_particle packets lost to a full exchange buffer (an error)
   ERR_FIELD_WAIT = 5,  // staged field tiles whose tensor loads did not arrive in time (an error)
+  ERR_STORE_FULL = 6,  // refilled particles lost to a full particle store (an error)
   ERR_COUNT = 8
 };
 

@@ -419,21 +419,30 @@ __global__ void sr_particle_kernel(Parts<real> P, const int* __restrict__ count,
 // Shell deletion of add_*_flat (:6015-6031): x < 4dx on the rank of the
 // global low x face, x > Nx dx on the rank of the high face, the same in y;
 // z < 4dx or z > Nz dx everywhere (at size 1 the one rank holds every face).
+// Whether the particle in slot t (cell c) lies in such a shell.
 template <typename real>
-__global__ void delete_shell_kernel(Parts<real> P, const int* __restrict__ count, Geom g) {
+__device__ __forceinline__ bool in_refill_shell(const Parts<real>& P, const Geom& g, int c, long long t) {
+  int i, j, k;
+  unpack_cell(c, i, j, k);
+  const bool xl = g.xlo && i < 4, yl = g.ylo && j < 4;
+  const bool xh = g.xhi && (i > g.nx || (i == g.nx && P.o[0][t] > (real)0));
+  const bool yh = g.yhi && (j > g.ny || (j == g.ny && P.o[1][t] > (real)0));
+  const bool zs = k < 4 || k > g.nz || (k == g.nz && P.o[2][t] > (real)0);
+  return xl || yl || xh || yh || zs;
+}
+
+// Whether cell (i, j, k) can hold a particle of a refill shell (any offset).
+__device__ __forceinline__ bool shell_cell(const Geom& g, int i, int j, int k) {
+  return (g.xlo && i < 4) || (g.ylo && j < 4) || (g.xhi && i >= g.nx) || (g.yhi && j >= g.ny) || k < 4 ||
+         k >= g.nz;
+}
+
+template <typename real>
+__global__ void delete_shell_kernel(Parts<real> P, int first, const int* __restrict__ count, Geom g) {
   const int n = *count;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+  for (int t = first + blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int c = P.cell[t];
-    if (c < 0) continue;
-    int i, j, k;
-    unpack_cell(c, i, j, k);
-    // the x and y shells only on the ranks that hold that face of the global domain
-    const bool xl = g.xlo && i < 4, yl = g.ylo && j < 4;
-    const bool xh = g.xhi && (i > g.nx || (i == g.nx && P.o[0][t] > (real)0));
-    const bool yh = g.yhi && (j > g.ny || (j == g.ny && P.o[1][t] > (real)0));
-    const bool zs = k < 4 || k > g.nz || (k == g.nz && P.o[2][t] > (real)0);
-    const bool del = xl || yl || xh || yh || zs;
-    if (del) P.cell[t] = -1;
+    if (c >= 0 && in_refill_shell(P, g, c, t)) P.cell[t] = -1;
   }
 }
 
@@ -457,6 +466,7 @@ struct SourceParams {
   long long base_p, base_v;  // first draw index on each stream
   int dst;                // first slot written
   const int* dst_dev;     // when set, the first slot is *dst_dev (a count known only on the device)
+  int cap;                // when set, slots from cap on are not written (counted as ERR_STORE_FULL)
   int init_form;          // 1: cell bounds as init_particle_flat writes them, 2dx + k dx (:475)
 };
 
@@ -537,7 +547,12 @@ __global__ void source_kernel(Parts<real> P, SourceParams sp, unsigned long long
   const int l = (int)(r % sl.nl);
   const int k = (int)(r / sl.nl);
   const int cc[3] = {k + sl.k0, l + sl.l0, m + sl.m0};
-  make_particle(P, sp, t, cc, (sp.dst_dev ? *sp.dst_dev : sp.dst) + (int)t, err);
+  const long long d = (long long)(sp.dst_dev ? *sp.dst_dev : sp.dst) + t;
+  if (sp.cap && d >= sp.cap) {
+    count_err(err, ERR_STORE_FULL);
+    return;
+  }
+  make_particle(P, sp, t, cc, (int)d, err);
 }
 
 // ------------------------------------------------------------------- sort

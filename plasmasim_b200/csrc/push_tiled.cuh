@@ -48,28 +48,50 @@ struct PushSmem {
   static constexpr size_t prec_off = (win_bytes + 15) & ~(size_t)15;  // records A, B of each slot: 8 reals
   static constexpr size_t fwin_off = prec_off + (size_t)kWarps * kStages * kLanes * 8 * sizeof(real);
   static constexpr size_t bytes = fwin_off + (kFieldWin ? (size_t)6 * QN * sizeof(float4) : 0);
+  // fill_quads stages 6 x (QX + 1) x QY x kWinZ values in the ring's memory
+  static_assert(!kFieldWin || (size_t)6 * (QX + 1) * QY * kWinZ * 4 <= fwin_off - prec_off, "stage fits the ring");
 };
 
-// Fills the tile's FieldQuads from planes F_EX .. F_BZ; nodes outside the
-// array read as zero. (ci0, cj0, ck0): the tile's first cell.
-template <int QX, int QY, int QZ>
-__device__ __forceinline__ void fill_quads(float4* __restrict__ fq, const Fields<float>& F, const Geom& g, int ci0,
-                                           int cj0, int ck0) {
+// Fills the tile's FieldQuads from planes F_EX .. F_BZ in two passes over
+// shared memory: the window's node rows (x planes c0x - 1 .. c0x + TX,
+// y rows c0y - 1 .. c0y + TY, z from the tile's 16-byte-aligned start wz0,
+// WZ values) are copied into `stage` with 16-byte loads where the row pitch
+// allows (VEC), many in flight per thread; then each quad is gathered from
+// `stage`. Nodes outside the array read as zero. (ci0, cj0, ck0): the tile's
+// first cell, ck0 = wz0 + 2.
+template <int QX, int QY, int QZ, bool VEC>
+__device__ __forceinline__ void fill_quads(float4* __restrict__ fq, float* __restrict__ stage, const Fields<float>& F,
+                                           const Geom& g, int ci0, int cj0, int ck0) {
+  constexpr int SX = QX + 1, SY = QY, SZ = kWinZ, NZ4 = SZ / 4, SN = SX * SY * SZ;
   constexpr int QN = QX * QY * QZ;
-  const int x0 = ci0 - 1, y0 = cj0 - 1, z0 = ck0 - 1;
+  const int x0 = ci0 - 1, y0 = cj0 - 1, wz0 = ck0 - 2;
+  for (int q4 = threadIdx.x; q4 < 6 * SX * SY * NZ4; q4 += blockDim.x) {
+    const int p = q4 / (SX * SY * NZ4), r = q4 % (SX * SY * NZ4);
+    const int a = r / (SY * NZ4), b = (r / NZ4) % SY, c4 = r % NZ4;
+    const int x = x0 + a, y = y0 + b, z = wz0 + 4 * c4;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    if (x < g.gx && y < g.gy) {
+      const float* src = F.f[p] + (long long)x * g.sx + y * g.gz + z;
+      if (VEC && z + 3 < g.gz) {
+        const float4 f4 = __ldg(reinterpret_cast<const float4*>(src));
+        v[0] = f4.x; v[1] = f4.y; v[2] = f4.z; v[3] = f4.w;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (z + e < g.gz) v[e] = __ldg(src + e);
+      }
+    }
+    *reinterpret_cast<float4*>(stage + p * SN + (a * SY + b) * SZ + 4 * c4) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+  __syncthreads();
+  // quad (xb, yr, zb) of component p: nodes (xb, xb + 1) x (zb, zb + 1) of
+  // row yr, at stage z index zb + 1 (the stage starts one node below z0)
   for (int q = threadIdx.x; q < 6 * QN; q += blockDim.x) {
     const int p = q / QN, r = q % QN;
-    const int x = x0 + r / (QY * QZ), y = y0 + (r / QZ) % QY, z = z0 + r % QZ;
-    float v[4] = {0.f, 0.f, 0.f, 0.f};
-    if (y < g.gy) {
-      const float* src = F.f[p] + (long long)x * g.sx + y * g.gz + z;
-      const bool x1 = x + 1 < g.gx, zin = z < g.gz, z1 = z + 1 < g.gz;
-      if (x < g.gx && zin) v[0] = __ldg(src);
-      if (x1 && zin) v[1] = __ldg(src + g.sx);
-      if (x < g.gx && z1) v[2] = __ldg(src + 1);
-      if (x1 && z1) v[3] = __ldg(src + g.sx + 1);
-    }
-    fq[q] = make_float4(v[0], v[1], v[2], v[3]);
+    const int xb = r / (QY * QZ), yr = (r / QZ) % QY, zb = r % QZ;
+    const float* s0 = stage + p * SN + (xb * SY + yr) * SZ + zb + 1;
+    const float* s1 = s0 + SY * SZ;  // plane xb + 1
+    fq[q] = make_float4(s0[0], s1[0], s0[1], s1[1]);
   }
 }
 
@@ -209,23 +231,52 @@ __device__ __forceinline__ void cp_async_16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(s), "l"(gmem) : "memory");
 }
 
-// Records A and B of particle t into 8 reals of shared memory (16-byte copies).
+// Records A and B of particle t into 4 reals of shared memory each (16-byte copies).
 template <typename real>
-__device__ __forceinline__ void fetch_records(real* dst, const Parts<real>& P, long long t) {
+__device__ __forceinline__ void fetch_records(real* dst_a, real* dst_b, const Parts<real>& P, long long t) {
   constexpr int kPieces = 4 * (int)sizeof(real) / 16;  // 16-byte pieces per record
   const char* a = reinterpret_cast<const char*>(P.ra + 4 * t);
   const char* b = reinterpret_cast<const char*>(P.rb + 4 * t);
-  char* d = reinterpret_cast<char*>(dst);
 #pragma unroll
   for (int q = 0; q < kPieces; ++q) {
-    cp_async_16(d + 16 * q, a + 16 * q);
-    cp_async_16(d + 16 * (kPieces + q), b + 16 * q);
+    cp_async_16(reinterpret_cast<char*>(dst_a) + 16 * q, a + 16 * q);
+    cp_async_16(reinterpret_cast<char*>(dst_b) + 16 * q, b + 16 * q);
   }
+}
+
+// Four reals of one record from shared memory, as vector loads.
+__device__ __forceinline__ void read_record(const float* p, float (&r)[4]) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = v.w;
+}
+__device__ __forceinline__ void read_record(const double* p, double (&r)[4]) {
+  const double2 v0 = reinterpret_cast<const double2*>(p)[0], v1 = reinterpret_cast<const double2*>(p)[1];
+  r[0] = v0.x; r[1] = v0.y; r[2] = v1.x; r[3] = v1.y;
 }
 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+
+// Per-step re-listing, the RELIST form of the push: every slot of the layout
+// that the push leaves without a particle of its lane's home cell -- an empty
+// slot, a particle that sr_particle removed, a particle that ended the step in
+// another cell -- is listed as a hole of its lane, in row order, in the
+// per-slot scratch `holes` (laid out like the slots), with the lane's count in
+// `nholes` (indexed by the home cell's interior key). A particle that ended the
+// step in another cell is written to the append region instead of its slot,
+// at slots [*append_at, cap) taken by one atomic per warp and row; when that
+// region is full it stays in its slot. The next step's placement
+// (relayout.cuh) then moves the appended particles into the holes of their
+// new cells, so the push never meets a particle outside its home cell unless
+// the append region ran out.
+struct Relist {
+  int* holes;
+  int* nholes;
+  int* append_at;
+  int* nonhome;  // set when a particle outside its home cell had to stay in the layout
+  int cap;
+};
 
 // The fused particle part of one step (push, J deposit at x^{n+1/2}, drift,
 // n deposit at x^{n+1}, sr_particle) for one species over the tiled layout;
@@ -238,9 +289,9 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // would be compare-and-swap loops). The density goes to the window with shared
 // reductions (every active lane at once): integer ones on fixed-point sums in
 // FP32, FP64 atomics in FP64.
-template <typename real, bool VEC_FLUSH>
+template <typename real, bool VEC_FLUSH, bool RELIST>
 __global__ void __launch_bounds__(kTileX * kTileY * 32, 2)
-push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc,
+push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc, Relist rl,
                   unsigned long long* err) {
   using S = PushSmem<real>;
   constexpr int WY = S::WY, WZ = S::WZ, WN = S::WN, WX = S::WX;
@@ -257,13 +308,19 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   const int ci0 = wx0 + 2, cj0 = wy0 + 2, ck0 = wz0 + 2;  // the tile's first cell
   const TileBox tb{ci0, cj0, ck0, (unsigned)min(kTileX, g.nx + 2 - ci0), (unsigned)min(kTileY, g.ny + 2 - cj0),
                    (unsigned)min(kLanes, g.nz + 2 - ck0)};
-  if constexpr (S::kFieldWin) fill_quads<S::QX, S::QY, S::QZ>(fq, F, g, ci0, cj0, ck0);
+  // the ring's memory, not in use yet, stages the window's rows
+  if constexpr (S::kFieldWin)
+    fill_quads<S::QX, S::QY, S::QZ, VEC_FLUSH>(fq, reinterpret_cast<float*>(smem_raw + S::prec_off), F, g, ci0, cj0,
+                                               ck0);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int G = tile * (kTileX * kTileY) + warp;
   const int base = ta.goff[G], jmax = ta.gmax[G];
   // home cell of this lane
   const int hi = wx0 + 2 + warp / kTileY, hj = wy0 + 2 + warp % kTileY, hk = wz0 + 2 + lane;
+  const int home_c = pack_cell(hi, hj, hk);
+  const bool home_in = hi < g.nx + 2 && hj < g.ny + 2 && hk < g.nz + 2;  // the lane has an interior cell
+  int nh = 0;  // RELIST: holes listed by this lane
   real* wn = win + 3 * WN;
   // FP32: the density window holds fixed-point sums (scatter8_win_fixed) at a
   // scale that no node of this tile can overflow
@@ -279,10 +336,15 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   HomeJ<real> acc;
   acc.zero();
   // ring of particle rows fetched ahead; each lane copies and reads only its
-  // own slots, so the per-thread cp.async groups need no warp barrier
+  // own slots, so the per-thread cp.async groups need no warp barrier. A
+  // stage holds the row's 32 records A, then its 32 records B, so that the
+  // lanes' 16-byte reads of one record fall on consecutive banks.
   real* prec = reinterpret_cast<real*>(smem_raw + S::prec_off) + warp * kStages * kLanes * 8;
   auto fetch = [&](int row) {
-    if (row < jmax) fetch_records(prec + ((row % kStages) * kLanes + lane) * 8, P, base + row * kLanes + lane);
+    if (row < jmax) {
+      real* stage = prec + (row % kStages) * kLanes * 8;
+      fetch_records(stage + lane * 4, stage + (kLanes + lane) * 4, P, base + row * kLanes + lane);
+    }
     cp_async_commit();
   };
 #pragma unroll
@@ -293,16 +355,21 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     cp_async_wait<kStages - 1>();
     const int t = base + jj * kLanes + lane;
     const int st = jj % kStages;
-    const real* rec = prec + (st * kLanes + lane) * 8;
-    const int c = reinterpret_cast<const int*>(rec)[0];
+    real ra[4], rb[4];
+    read_record(prec + st * kLanes * 8 + lane * 4, ra);
+    read_record(prec + st * kLanes * 8 + (kLanes + lane) * 4, rb);
+    int c;
+    if constexpr (sizeof(real) == 4) c = __float_as_int((float)ra[0]);
+    else c = __double2loint((double)ra[0]);
     const bool act = c >= 0;
     int i = 0, j = 0, k = 0;
     real fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
+    int cnew = -1;
     if (act) {
       ++pushed;
       unpack_cell(c, i, j, k);
-      fx = rec[1]; fy = rec[2]; fz = rec[3];
-      vx = rec[4]; vy = rec[5]; vz = rec[6];
+      fx = ra[1]; fy = ra[2]; fz = ra[3];
+      vx = rb[0]; vy = rb[1]; vz = rb[2];
       // a particle in one of the tile's cells is in an interior cell: its
       // stencils lie in the array, and it is ballistic only when the
       // Absorb_grid2 layer reaches interior cells
@@ -372,13 +439,38 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       }
 #if PB_TILE_FASTPATH
       // sr_particle keeps a particle of an interior cell where it is
-      const int cnew = inside1 ? pack_cell(i, j, k) : settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
+      cnew = inside1 ? pack_cell(i, j, k) : settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
 #else
-      const int cnew = settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
+      cnew = settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
 #endif
-      store_records(P, t, cnew, fx, fy, fz, vx, vy, vz);
+      if constexpr (!RELIST) store_records(P, t, cnew, fx, fy, fz, vx, vy, vz);
+    }
+    if constexpr (RELIST) {
+      const bool away = act && cnew >= 0 && cnew != home_c;
+      bool mover = away;
+      const unsigned mm = __ballot_sync(0xffffffffu, mover);
+      int d = 0;
+      if (mm) {  // warp-uniform: the row's movers take consecutive append slots
+        int b = 0;
+        if (lane == 0) b = atomicAdd(rl.append_at, __popc(mm));
+        b = __shfl_sync(0xffffffffu, b, 0);
+        d = b + __popc(mm & ((1u << lane) - 1u));
+        mover = mover && d < rl.cap;  // a full append region keeps the particle in its slot
+        if (away && !mover) *rl.nonhome = 1;
+      }
+      if (mover) {
+        store_records(P, d, cnew, fx, fy, fz, vx, vy, vz);
+        P.cell[t] = -1;
+      } else if (act) {
+        store_records(P, t, cnew, fx, fy, fz, vx, vy, vz);
+      }
+      if (home_in && (!act || cnew < 0 || mover)) {
+        rl.holes[base + nh * kLanes + lane] = jj;
+        ++nh;
+      }
     }
   }
+  if (RELIST && home_in) rl.nholes[((hi - 2) * g.ny + (hj - 2)) * g.nz + (hk - 2)] = nh;
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
   if (lane == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
   // the lane's home-cell sums into the window (nodes h-1 .. h+1 around it)

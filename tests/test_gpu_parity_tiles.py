@@ -43,9 +43,13 @@ pytestmark = pytest.mark.gpu
 SHAPES = {"cube64": (64, 64, 64, 8), "ragged": (41, 22, 70, 4)}
 
 # one step, from identical particle state
+# (measured on a B200: FP64 disp 3e-13, vel 2e-17, max_dx 1.4e-14 cells, max_dv 7e-16,
+# grid 1e-14, F 2e-14, E 1.2e-14; FP32 disp 1.8e-6, vel 7.3e-8, max_dx 7.3e-8 cells,
+# max_dv 4e-7, grid 8.6e-7, F 4e-8, E 3e-10. FP32 stores offsets to 2^-24 cells,
+# so a 0.025-cell step carries about 1e-6 of displacement error from storage alone)
 STEP_TOL = {
-    64: dict(disp=1e-11, vel=1e-12, max_dx_cells=1e-12, max_dv_rel=1e-11, grid=1e-10, F=1e-10, E=1e-12),
-    32: dict(disp=3e-6, vel=1e-6, max_dx_cells=1e-6, max_dv_rel=1e-5, grid=2e-5, F=2e-4, E=1e-5),
+    64: dict(disp=3e-12, vel=1e-15, max_dx_cells=1e-13, max_dv_rel=1e-14, grid=1e-12, F=1e-12, E=1e-13),
+    32: dict(disp=3e-6, vel=3e-7, max_dx_cells=3e-7, max_dv_rel=2e-6, grid=5e-6, F=1e-6, E=1e-8),
 }
 
 
@@ -102,9 +106,13 @@ def test_one_step_across_tiles(shape, precision, record):
 
 
 # 100 steps of the configuration the reference runs on a CPU
+# (measured: FP64 F 1.8e-8, E 2e-11, fave 2e-10, moments 5e-14; FP32 F 2.7e-3, E 5.5e-6,
+# fave 2.7e-4, moments 1.3e-7, equal particle counts. The FP32 run's particles
+# decorrelate from the FP64 oracle's over 100 steps, so its instantaneous thrust
+# differs at the 1e-3 level while the running mean and the energies stay close)
 HUNDRED_TOL = {
-    64: dict(count=0, F=1e-6, E=1e-9, fave=1e-6, moments=1e-10),
-    32: dict(count=0.005, F=5e-2, E=1e-2, fave=5e-2, moments=1e-3),
+    64: dict(count=0, F=2e-7, E=5e-10, fave=5e-9, moments=1e-12),
+    32: dict(count=0.005, F=1e-2, E=5e-5, fave=2e-3, moments=1e-6),
 }
 
 
@@ -145,7 +153,8 @@ def test_cube32_hundred_steps(precision, record):
     assert errs["moments"] <= tol["moments"]
 
 
-FAVE_TOL = {64: dict(reference=3e-3, oracle=1e-9), 32: dict(reference=5e-3, oracle=1e-3)}
+# (measured: 1.45e-3 of the reference in both precisions; 3e-15 / 1.4e-7 of the oracle)
+FAVE_TOL = {64: dict(reference=3e-3, oracle=1e-12), 32: dict(reference=3e-3, oracle=1e-5)}
 
 
 @pytest.mark.parametrize("precision", [64, 32])
@@ -205,9 +214,10 @@ def test_fp32_against_fp64_hundred_steps(record):
     errs = dict(F=rel_norm(F32, F64), F_total=rel_norm(F32[:3], F64[:3]), fave=rel_norm(A32, A64),
                 E=[abs(E32[q] / E64[q] - 1) for q in range(4)])
     record.update(errors=errs)
-    assert errs["F"] <= 5e-2
-    assert errs["fave"] <= 5e-2
-    assert max(errs["E"]) <= 1e-2
+    # measured: F 2.7e-3, fave 2.7e-4, E 5.5e-6
+    assert errs["F"] <= 1e-2
+    assert errs["fave"] <= 2e-3
+    assert max(errs["E"]) <= 5e-5
 
 
 @pytest.mark.parametrize("precision", [64, 32])
@@ -263,6 +273,6 @@ def test_slot_order_matches_oracle(precision, record):
     errs["E20"] = [abs(E[q] / ref[27 + q] - 1) for q in (2, 3)]
     errs["density20"] = [abs(g[..., f].sum() / og[..., f].sum() - 1) for f in (15, 16)]
     record.update(precision=precision, errors=errs)
-    tol20 = 1e-9 if precision == 64 else 1e-3
+    tol20 = 1e-12 if precision == 64 else 1e-6  # measured 1e-15 / 2.3e-8
     assert errs["count20"] <= (2 / 2000 if precision == 64 else 0.005)
     assert max(errs["E20"]) <= tol20 and max(errs["density20"]) <= tol20
