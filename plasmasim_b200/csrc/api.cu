@@ -103,6 +103,9 @@ struct pic_ctx {
   int* append_dev = nullptr;          // end of the append region during a re-layout
   int* rank = nullptr;                // per-slot scratch: placement rank of every appended particle
   int* bucket = nullptr;              // per-slot scratch: appended particles bucketed by their new cell
+  void* jtask_mem = nullptr;          // J deposits queued by the push (JTasks), records A then B
+  long long jtask_cap = 0;
+  int* jtask_count = nullptr;
   int* cnt = nullptr;
   int* offs = nullptr;
   int* cursor = nullptr;
@@ -730,6 +733,10 @@ int do_push_tiled(pic_ctx* c, int s, bool relist = false) {
   const size_t smem = PushSmem<real>::bytes;
   const bool vec = sizeof(real) == 4 && c->g.gz % 4 == 0;
   Relist rl{st.holes, st.nholes, c->append_dev, st.nonhome, (int)st.cap};
+  JTasks<real> jt{make_parts<real>((real*)c->jtask_mem,
+                                   (real*)((char*)c->jtask_mem + parts_record_bytes(c->jtask_cap, sizeof(real)))),
+                  c->jtask_count, (int)c->jtask_cap};
+  CK(cudaMemsetAsync(c->jtask_count, 0, sizeof(int), c->stream));
   const Parts<real> P = parts<real>(c, s);
   const Fields<real> F = fields<real>(c);
   const PushConst<real> pc = push_const<real>(c, s);
@@ -737,8 +744,8 @@ int do_push_tiled(pic_ctx* c, int s, bool relist = false) {
   if (relist) {
     copy_int_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, st.count_dev);  // movers go after the current end
     CKL();
-    if (vec) push_tiled_kernel<real, true, true><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, c->err);
-    else push_tiled_kernel<real, false, true><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, c->err);
+    if (vec) push_tiled_kernel<real, true, true><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, jt, c->err);
+    else push_tiled_kernel<real, false, true><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, jt, c->err);
     CKL();
     clamp_count_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.cap, st.count_dev);
     CKL();
@@ -746,8 +753,12 @@ int do_push_tiled(pic_ctx* c, int s, bool relist = false) {
     st.listed = true;
     c->tiled[s] = false;  // the appended particles await the next placement
   } else {
-    if (vec) push_tiled_kernel<real, true, false><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, c->err);
-    else push_tiled_kernel<real, false, false><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, c->err);
+    if (vec) push_tiled_kernel<real, true, false><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, jt, c->err);
+    else push_tiled_kernel<real, false, false><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, jt, c->err);
+    CKL();
+  }
+  if (PB_JTASK) {
+    jtask_kernel<real><<<particle_blocks(c->jtask_cap), kThreads, 0, c->stream>>>(jt, F, c->g, pc);
     CKL();
   }
   return PIC_OK;
@@ -1741,6 +1752,10 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
       }
       if (cudaMalloc(&c->rank, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
       if (cudaMalloc(&c->bucket, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
+      // the push's queue of J deposits off their home cells: a sixteenth of the capacity
+      c->jtask_cap = cap / 16 + 4096;
+      if (cudaMalloc(&c->jtask_mem, store_bytes(c->jtask_cap, c->rsize)) != cudaSuccess) return fail(PIC_ERR_CUDA);
+      if (cudaMalloc(&c->jtask_count, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
     }
     const int pb_f = (int)PushSmem<float>::bytes, pb_d = (int)PushSmem<double>::bytes;
     if (cudaFuncSetAttribute(push_tiled_kernel<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1800,6 +1815,8 @@ int pic_destroy(pic_ctx* c) {
   }
   cudaFree(c->rank);
   cudaFree(c->bucket);
+  cudaFree(c->jtask_mem);
+  cudaFree(c->jtask_count);
   cudaFree(c->cnt);
   cudaFree(c->offs);
   cudaFree(c->cursor);

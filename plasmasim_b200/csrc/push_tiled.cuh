@@ -278,6 +278,34 @@ struct Relist {
   int cap;
 };
 
+// The J deposits of particles outside their lane's home cell at x^{n+1/2}
+// (mostly particles that crossed a cell face in the step's first half drift),
+// queued as records (cell, offsets | velocities) at slots [0, *count) of T,
+// up to cap; jtask_kernel deposits them afterwards, one thread each, so that
+// the push's warps do not all take the global-reduction path whenever one of
+// their lanes needs it. A full queue falls back to depositing in place.
+#ifndef PB_JTASK
+#define PB_JTASK 1
+#endif
+template <typename real>
+struct JTasks {
+  Parts<real> T;
+  int* count;
+  int cap;
+};
+
+template <typename real>
+__global__ void __launch_bounds__(256) jtask_kernel(JTasks<real> jt, Fields<real> F, Geom g, PushConst<real> pc) {
+  const int n = min(*jt.count, jt.cap);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const Rec<real> r = load_records(jt.T, t);
+    int i, j, k;
+    unpack_cell(r.cell, i, j, k);
+    const Axis<real> X = axis_weights(i, r.o[0]), Y = axis_weights(j, r.o[1]), Z = axis_weights(k, r.o[2]);
+    deposit_j(F, g, pc, X, Y, Z, r.v[0], r.v[1], r.v[2]);
+  }
+}
+
 // The fused particle part of one step (push, J deposit at x^{n+1/2}, drift,
 // n deposit at x^{n+1}, sr_particle) for one species over the tiled layout;
 // the same arithmetic as push_kernel<real, PUSH_FUSED> apart from the FP32
@@ -292,7 +320,7 @@ struct Relist {
 template <typename real, bool VEC_FLUSH, bool RELIST>
 __global__ void __launch_bounds__(kTileX * kTileY * 32, 2)
 push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc, Relist rl,
-                  unsigned long long* err) {
+                  JTasks<real> jt, unsigned long long* err) {
   using S = PushSmem<real>;
   constexpr int WY = S::WY, WZ = S::WZ, WN = S::WN, WX = S::WX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -407,8 +435,22 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
         acc.add(pc.qn * vx, pc.qn * vy, pc.qn * vz, X, Y, Z, bx, by, bz);
       } else if (in_array(g, i, j, k)) {
         if (stencil_ok(g, i, j, k)) {
-          const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-          deposit_j(F, g, pc, X, Y, Z, vx, vy, vz);
+#if PB_JTASK
+          // queued for jtask_kernel: one append per warp, the deposit in full warps later
+          const unsigned am = __activemask();
+          const unsigned tm = __ballot_sync(am, true);
+          const int leader = __ffs(tm) - 1;
+          int b = 0;
+          if (lane == leader) b = atomicAdd(jt.count, __popc(tm));
+          b = __shfl_sync(am, b, leader) + __popc(tm & ((1u << lane) - 1u));
+          if (b < jt.cap) {
+            store_records(jt.T, b, pack_cell(i, j, k), fx, fy, fz, vx, vy, vz);
+          } else
+#endif
+          {
+            const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+            deposit_j(F, g, pc, X, Y, Z, vx, vy, vz);
+          }
         } else {
           count_err(err, ERR_DEPOSIT_OOB);
         }
