@@ -12,6 +12,11 @@ constexpr int kStages = 3;   // particle rows in flight per warp
 #ifndef PB_TILE_FASTPATH
 #define PB_TILE_FASTPATH 1
 #endif
+// The FP32 gather's window: 1, node quads (FieldQuads); 0, one plane per
+// component over the tile and two halo nodes (trilerp_win)
+#ifndef PB_QUADS
+#define PB_QUADS 1
+#endif
 
 // The tile's interior cells: first cell (ci0, cj0, ck0) and extents (the
 // nominal tile clipped at the last interior cell, n + 1, of each axis).
@@ -47,7 +52,8 @@ struct PushSmem {
   static constexpr size_t win_bytes = 4 * WN * sizeof(real);
   static constexpr size_t prec_off = (win_bytes + 15) & ~(size_t)15;  // records A, B of each slot: 8 reals
   static constexpr size_t fwin_off = prec_off + (size_t)kWarps * kStages * kLanes * 8 * sizeof(real);
-  static constexpr size_t bytes = fwin_off + (kFieldWin ? (size_t)6 * QN * sizeof(float4) : 0);
+  static constexpr size_t bytes =
+      fwin_off + (kFieldWin ? (PB_QUADS ? (size_t)6 * QN * sizeof(float4) : (size_t)6 * WN * sizeof(float)) : 0);
   // fill_quads stages 6 x (QX + 1) x QY x kWinZ values in the ring's memory
   static_assert(!kFieldWin || (size_t)6 * (QX + 1) * QY * kWinZ * 4 <= fwin_off - prec_off, "stage fits the ring");
 };
@@ -129,6 +135,67 @@ __device__ __forceinline__ Gathered<float> gather6_quads(const float4* __restric
   r.by = quad_lerp<QZ>(fq + 4 * QN, xa + yb + za, X.a0, X.a1, yb0, yb1, za0, za1);
   r.bz = quad_lerp<QZ>(fq + 5 * QN, xa + ya + zb, X.a0, X.a1, ya0, ya1, zb0, zb1);
   return r;
+}
+
+// Trilinear interpolation from a window plane with compile-time strides (the
+// 2x2x2 nodes at window index n), the two x planes as one packed pair.
+template <int WY, int WZ>
+__device__ __forceinline__ float trilerp_win(const float* __restrict__ w, int n, float x0, float x1, float2 Y0,
+                                             float2 Y1, float2 Z0, float2 Z1) {
+  constexpr int P = WY * WZ;  // next x plane
+  const float2 n00 = make_float2(w[n], w[n + P]), n01 = make_float2(w[n + 1], w[n + P + 1]);
+  const float2 n10 = make_float2(w[n + WZ], w[n + P + WZ]), n11 = make_float2(w[n + WZ + 1], w[n + P + WZ + 1]);
+  const float2 cy0 = __ffma2_rn(n01, Z1, __fmul2_rn(n00, Z0));
+  const float2 cy1 = __ffma2_rn(n11, Z1, __fmul2_rn(n10, Z0));
+  const float2 cx = __ffma2_rn(cy1, Y1, __fmul2_rn(cy0, Y0));
+  return cx.x * x0 + cx.y * x1;
+}
+
+// gather6 from a window of one plane per component (ex ey ez bx by bz, WN
+// nodes each, origin (wx0, wy0, wz0)); the caller checks that the stencil lies inside.
+template <int WY, int WZ, int WN>
+__device__ __forceinline__ Gathered<float> gather6_win(const float* __restrict__ fw, int wx0, int wy0, int wz0,
+                                                       const Axis<float>& X, const Axis<float>& Y,
+                                                       const Axis<float>& Z) {
+  const int ax = X.a - wx0, bx = X.b - wx0, ay = Y.a - wy0, by = Y.b - wy0, az = Z.a - wz0, bz = Z.b - wz0;
+  const float2 ya0 = make_float2(Y.a0, Y.a0), ya1 = make_float2(Y.a1, Y.a1);
+  const float2 yb0 = make_float2(Y.b0, Y.b0), yb1 = make_float2(Y.b1, Y.b1);
+  const float2 za0 = make_float2(Z.a0, Z.a0), za1 = make_float2(Z.a1, Z.a1);
+  const float2 zb0 = make_float2(Z.b0, Z.b0), zb1 = make_float2(Z.b1, Z.b1);
+  Gathered<float> r;
+  r.ex = trilerp_win<WY, WZ>(fw, (ax * WY + by) * WZ + bz, X.a0, X.a1, yb0, yb1, zb0, zb1);
+  r.ey = trilerp_win<WY, WZ>(fw + WN, (bx * WY + ay) * WZ + bz, X.b0, X.b1, ya0, ya1, zb0, zb1);
+  r.ez = trilerp_win<WY, WZ>(fw + 2 * WN, (bx * WY + by) * WZ + az, X.b0, X.b1, yb0, yb1, za0, za1);
+  r.bx = trilerp_win<WY, WZ>(fw + 3 * WN, (bx * WY + ay) * WZ + az, X.b0, X.b1, ya0, ya1, za0, za1);
+  r.by = trilerp_win<WY, WZ>(fw + 4 * WN, (ax * WY + by) * WZ + az, X.a0, X.a1, yb0, yb1, za0, za1);
+  r.bz = trilerp_win<WY, WZ>(fw + 5 * WN, (ax * WY + ay) * WZ + bz, X.a0, X.a1, ya0, ya1, zb0, zb1);
+  return r;
+}
+
+// The window's planes from F_EX .. F_BZ (16-byte loads where the row pitch
+// allows), zero outside the array.
+template <int WX, int WY, int WZ, bool VEC>
+__device__ __forceinline__ void fill_win(float* __restrict__ fw, const Fields<float>& F, const Geom& g, int wx0,
+                                         int wy0, int wz0) {
+  constexpr int NZ4 = WZ / 4, WN = WX * WY * WZ;
+  for (int q4 = threadIdx.x; q4 < 6 * WX * WY * NZ4; q4 += blockDim.x) {
+    const int p = q4 / (WX * WY * NZ4), r = q4 % (WX * WY * NZ4);
+    const int a = r / (WY * NZ4), b = (r / NZ4) % WY, c4 = r % NZ4;
+    const int ga = wx0 + a, gb = wy0 + b, gc = wz0 + 4 * c4;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    if (ga < g.gx && gb < g.gy) {
+      const float* src = F.f[p] + (long long)ga * g.sx + gb * g.gz + gc;
+      if (VEC && gc + 3 < g.gz) {
+        const float4 f4 = __ldg(reinterpret_cast<const float4*>(src));
+        v[0] = f4.x; v[1] = f4.y; v[2] = f4.z; v[3] = f4.w;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (gc + e < g.gz) v[e] = __ldg(src + e);
+      }
+    }
+    *reinterpret_cast<float4*>(fw + p * WN + (a * WY + b) * WZ + 4 * c4) = make_float4(v[0], v[1], v[2], v[3]);
+  }
 }
 
 // The current of the particles that are in a lane's home cell, summed in
@@ -337,9 +404,13 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   const TileBox tb{ci0, cj0, ck0, (unsigned)min(kTileX, g.nx + 2 - ci0), (unsigned)min(kTileY, g.ny + 2 - cj0),
                    (unsigned)min(kLanes, g.nz + 2 - ck0)};
   // the ring's memory, not in use yet, stages the window's rows
-  if constexpr (S::kFieldWin)
-    fill_quads<S::QX, S::QY, S::QZ, VEC_FLUSH>(fq, reinterpret_cast<float*>(smem_raw + S::prec_off), F, g, ci0, cj0,
-                                               ck0);
+  if constexpr (S::kFieldWin) {
+    if (PB_QUADS)
+      fill_quads<S::QX, S::QY, S::QZ, VEC_FLUSH>(fq, reinterpret_cast<float*>(smem_raw + S::prec_off), F, g, ci0,
+                                                 cj0, ck0);
+    else
+      fill_win<WX, WY, WZ, VEC_FLUSH>(reinterpret_cast<float*>(fq), F, g, wx0, wy0, wz0);
+  }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int G = tile * (kTileX * kTileY) + warp;
@@ -415,9 +486,16 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       if (!bal) {
         const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
         if constexpr (S::kFieldWin) {
-          // the quads cover the stencils of particles in the tile's cells
-          if (inside)
-            boris4_fast(pc, gather6_quads<S::QY, S::QZ>(fq, ci0, cj0, ck0, X, Y, Z), vx, vy, vz);
+          // the quads cover the stencils of particles in the tile's cells;
+          // the plane window those within two halo nodes of the tile
+          const bool in_win = PB_QUADS ? inside
+                                       : i - 1 >= wx0 && i + 1 < wx0 + WX && j - 1 >= wy0 && j + 1 < wy0 + WY &&
+                                             k - 1 >= wz0 && k + 1 < wz0 + WZ;
+          if (in_win)
+            boris4_fast(pc,
+                        PB_QUADS ? gather6_quads<S::QY, S::QZ>(fq, ci0, cj0, ck0, X, Y, Z)
+                                 : gather6_win<WY, WZ, WN>(reinterpret_cast<const float*>(fq), wx0, wy0, wz0, X, Y, Z),
+                        vx, vy, vz);
           else
             boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
         } else {

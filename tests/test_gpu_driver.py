@@ -5,7 +5,6 @@ step. Its printed thrust lines and the files it writes (thrust458.txt, and
 thrust458_ave.txt at step 0, a multiple of 500) are checked against the same
 run made through the Python binding: F to the printed three decimals
 (4 significant digits), E to the printed eight."""
-import math
 import os
 import subprocess
 
@@ -53,4 +52,4 @@ def test_c_driver_runs_the_loop(tmp_path):
     assert [int(l.split()[0]) for l in thrust] == list(range(steps))
     ave = (tmp_path / "thrust458_ave.txt").read_text().splitlines()
     assert len(ave) == 1 and ave[0].split()[0] == "0" and len(ave[0].split()) == 28
-    assert "steps 5" in res.stderr and not math.isnan(printed).any()
+    assert "steps 5" in res.stderr and not np.isnan(printed).any()
