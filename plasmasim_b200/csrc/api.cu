@@ -32,7 +32,12 @@ using namespace pb;
 // cells out of the layout, and every step places them (no classify pass);
 // 0: a classify pass re-lays the particles after each refill
 #ifndef PB_RELIST
-#define PB_RELIST 1
+#define PB_RELIST 0
+#endif
+// 1: the FP32 push sums J in the shared window (push_fixj_kernel, 3 CTAs per
+// SM); 0: in per-lane registers (push_tiled_kernel, 2 CTAs per SM)
+#ifndef PB_FIXJ
+#define PB_FIXJ 0
 #endif
 
 namespace {
@@ -741,6 +746,29 @@ int do_push_tiled(pic_ctx* c, int s, bool relist = false) {
   const Fields<real> F = fields<real>(c);
   const PushConst<real> pc = push_const<real>(c, s);
   const dim3 grid(ntiles), block(kTileX * kTileY * 32);
+  if (PB_FIXJ && sizeof(real) == 4) {
+    const Parts<float> Pf = parts<float>(c, s);
+    const Fields<float> Ff = fields<float>(c);
+    const PushConst<float> pf = push_const<float>(c, s);
+    const size_t sb = FixjSmem::bytes;
+    if (relist) {
+      copy_int_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, st.count_dev);
+      CKL();
+    }
+    if (vec && relist) push_fixj_kernel<true, true><<<grid, block, sb, c->stream>>>(Pf, ta, Ff, c->g, pf, rl, c->err);
+    else if (vec) push_fixj_kernel<true, false><<<grid, block, sb, c->stream>>>(Pf, ta, Ff, c->g, pf, rl, c->err);
+    else if (relist) push_fixj_kernel<false, true><<<grid, block, sb, c->stream>>>(Pf, ta, Ff, c->g, pf, rl, c->err);
+    else push_fixj_kernel<false, false><<<grid, block, sb, c->stream>>>(Pf, ta, Ff, c->g, pf, rl, c->err);
+    CKL();
+    if (relist) {
+      clamp_count_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.cap, st.count_dev);
+      CKL();
+      st.pending = true;
+      st.listed = true;
+      c->tiled[s] = false;
+    }
+    return PIC_OK;
+  }
   if (relist) {
     copy_int_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, st.count_dev);  // movers go after the current end
     CKL();
@@ -1769,7 +1797,15 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
         cudaFuncSetAttribute(push_tiled_kernel<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              pb_f) != cudaSuccess ||
         cudaFuncSetAttribute(push_tiled_kernel<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             pb_f) != cudaSuccess)
+                             pb_f) != cudaSuccess ||
+        (PB_FIXJ && (cudaFuncSetAttribute(push_fixj_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)FixjSmem::bytes) != cudaSuccess ||
+                     cudaFuncSetAttribute(push_fixj_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)FixjSmem::bytes) != cudaSuccess ||
+                     cudaFuncSetAttribute(push_fixj_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)FixjSmem::bytes) != cudaSuccess ||
+                     cudaFuncSetAttribute(push_fixj_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)FixjSmem::bytes) != cudaSuccess)))
       return fail(PIC_ERR_CUDA);
   }
   if (cudaMalloc(&c->acc, sizeof(double) * 64) != cudaSuccess) return fail(PIC_ERR_CUDA);

@@ -48,7 +48,7 @@ constexpr int kChunk = 2048;     // particle slots per work item
 // summed per cell in registers); 0: push2d_kernel (rows of the chunk,
 // deposits reduced across each warp)
 #ifndef PB_PUSH2D_SEQ
-#define PB_PUSH2D_SEQ 1
+#define PB_PUSH2D_SEQ 0
 #endif
 constexpr int kCellShift = 16;   // cell = (i << 16) | k
 

@@ -12,11 +12,6 @@ constexpr int kStages = 3;   // particle rows in flight per warp
 #ifndef PB_TILE_FASTPATH
 #define PB_TILE_FASTPATH 1
 #endif
-// The FP32 gather's window: 1, node quads (FieldQuads); 0, one plane per
-// component over the tile and two halo nodes (trilerp_win)
-#ifndef PB_QUADS
-#define PB_QUADS 1
-#endif
 
 // The tile's interior cells: first cell (ci0, cj0, ck0) and extents (the
 // nominal tile clipped at the last interior cell, n + 1, of each axis).
@@ -30,112 +25,19 @@ struct TileBox {
 
 // Shared-memory plan of one CTA (8 warps): the J/n window, per warp a ring of
 // kStages particle rows fetched ahead with cp.async (records A and B of each
-// slot) and, in FP32, the tile's E and B as node quads (FieldQuads below; the
-// gather reads them there; FP64 gathers from global memory, its window would
-// not leave room for two CTAs per SM).
-//
-// FieldQuads: for each of ex, ey, ez, bx, by, bz and each base node (x, y, z)
-// of the tile's gather stencils, the float4
-//   (f(x, y, z), f(x+1, y, z), f(x, y, z+1), f(x+1, y, z+1)),
-// so that the 2x2x2 nodes of one component are two 16-byte loads (rows y and
-// y+1). A particle in cell (i, j, k) of the tile interpolates from bases
-// i-1 .. i, j-1 .. j (and row j+1), k-1 .. k, so the quads cover bases
-// [c0 - 1, c0 + T - 1] of each axis for the tile's first cell c0 and extent T,
-// plus the row above on y: QX = TX + 1, QY = TY + 2, QZ = 32 + 1. Particles
-// that have left the tile gather from global memory.
+// slot) and, in FP32, the tile's E and B over the same window (the gather
+// reads them there; FP64 gathers from global memory, its window would not
+// leave room for two CTAs per SM).
 template <typename real>
 struct PushSmem {
   static constexpr int WX = kTileX + 4, WY = kTileY + 4, WZ = kWinZ, WN = WX * WY * WZ;
-  static constexpr int QX = kTileX + 1, QY = kTileY + 2, QZ = kLanes + 1, QN = QX * QY * QZ;
   static constexpr int kWarps = kTileX * kTileY;
   static constexpr bool kFieldWin = sizeof(real) == 4;
   static constexpr size_t win_bytes = 4 * WN * sizeof(real);
   static constexpr size_t prec_off = (win_bytes + 15) & ~(size_t)15;  // records A, B of each slot: 8 reals
   static constexpr size_t fwin_off = prec_off + (size_t)kWarps * kStages * kLanes * 8 * sizeof(real);
-  static constexpr size_t bytes =
-      fwin_off + (kFieldWin ? (PB_QUADS ? (size_t)6 * QN * sizeof(float4) : (size_t)6 * WN * sizeof(float)) : 0);
-  // fill_quads stages 6 x (QX + 1) x QY x kWinZ values in the ring's memory
-  static_assert(!kFieldWin || (size_t)6 * (QX + 1) * QY * kWinZ * 4 <= fwin_off - prec_off, "stage fits the ring");
+  static constexpr size_t bytes = fwin_off + (kFieldWin ? (size_t)6 * WN * sizeof(float) : 0);
 };
-
-// Fills the tile's FieldQuads from planes F_EX .. F_BZ in two passes over
-// shared memory: the window's node rows (x planes c0x - 1 .. c0x + TX,
-// y rows c0y - 1 .. c0y + TY, z from the tile's 16-byte-aligned start wz0,
-// WZ values) are copied into `stage` with 16-byte loads where the row pitch
-// allows (VEC), many in flight per thread; then each quad is gathered from
-// `stage`. Nodes outside the array read as zero. (ci0, cj0, ck0): the tile's
-// first cell, ck0 = wz0 + 2.
-template <int QX, int QY, int QZ, bool VEC>
-__device__ __forceinline__ void fill_quads(float4* __restrict__ fq, float* __restrict__ stage, const Fields<float>& F,
-                                           const Geom& g, int ci0, int cj0, int ck0) {
-  constexpr int SX = QX + 1, SY = QY, SZ = kWinZ, NZ4 = SZ / 4, SN = SX * SY * SZ;
-  constexpr int QN = QX * QY * QZ;
-  const int x0 = ci0 - 1, y0 = cj0 - 1, wz0 = ck0 - 2;
-  for (int q4 = threadIdx.x; q4 < 6 * SX * SY * NZ4; q4 += blockDim.x) {
-    const int p = q4 / (SX * SY * NZ4), r = q4 % (SX * SY * NZ4);
-    const int a = r / (SY * NZ4), b = (r / NZ4) % SY, c4 = r % NZ4;
-    const int x = x0 + a, y = y0 + b, z = wz0 + 4 * c4;
-    float v[4] = {0.f, 0.f, 0.f, 0.f};
-    if (x < g.gx && y < g.gy) {
-      const float* src = F.f[p] + (long long)x * g.sx + y * g.gz + z;
-      if (VEC && z + 3 < g.gz) {
-        const float4 f4 = __ldg(reinterpret_cast<const float4*>(src));
-        v[0] = f4.x; v[1] = f4.y; v[2] = f4.z; v[3] = f4.w;
-      } else {
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-          if (z + e < g.gz) v[e] = __ldg(src + e);
-      }
-    }
-    *reinterpret_cast<float4*>(stage + p * SN + (a * SY + b) * SZ + 4 * c4) = make_float4(v[0], v[1], v[2], v[3]);
-  }
-  __syncthreads();
-  // quad (xb, yr, zb) of component p: nodes (xb, xb + 1) x (zb, zb + 1) of
-  // row yr, at stage z index zb + 1 (the stage starts one node below z0)
-  for (int q = threadIdx.x; q < 6 * QN; q += blockDim.x) {
-    const int p = q / QN, r = q % QN;
-    const int xb = r / (QY * QZ), yr = (r / QZ) % QY, zb = r % QZ;
-    const float* s0 = stage + p * SN + (xb * SY + yr) * SZ + zb + 1;
-    const float* s1 = s0 + SY * SZ;  // plane xb + 1
-    fq[q] = make_float4(s0[0], s1[0], s0[1], s1[1]);
-  }
-}
-
-// One component from its quads: base quad index n (rows n and n + QZ), the
-// weights of its x, y and z bases. The two x nodes travel as one packed pair
-// through the z and y steps (two-wide multiplies and FMAs of sm_100).
-template <int QZ>
-__device__ __forceinline__ float quad_lerp(const float4* __restrict__ fq, int n, float x0, float x1, float2 Y0,
-                                           float2 Y1, float2 Z0, float2 Z1) {
-  const float4 r0 = fq[n], r1 = fq[n + QZ];
-  const float2 c0 = __ffma2_rn(make_float2(r0.z, r0.w), Z1, __fmul2_rn(make_float2(r0.x, r0.y), Z0));
-  const float2 c1 = __ffma2_rn(make_float2(r1.z, r1.w), Z1, __fmul2_rn(make_float2(r1.x, r1.y), Z0));
-  const float2 cx = __ffma2_rn(c1, Y1, __fmul2_rn(c0, Y0));
-  return cx.x * x0 + cx.y * x1;
-}
-
-// gather6 from the tile's FieldQuads for a particle in the tile's cells.
-template <int QY, int QZ>
-__device__ __forceinline__ Gathered<float> gather6_quads(const float4* __restrict__ fq, int ci0, int cj0, int ck0,
-                                                         const Axis<float>& X, const Axis<float>& Y,
-                                                         const Axis<float>& Z) {
-  constexpr int QN = (kTileX + 1) * QY * QZ;
-  const int xa = (X.a - ci0 + 1) * (QY * QZ), xb = (X.b - ci0 + 1) * (QY * QZ);
-  const int ya = (Y.a - cj0 + 1) * QZ, yb = (Y.b - cj0 + 1) * QZ;
-  const int za = Z.a - ck0 + 1, zb = Z.b - ck0 + 1;
-  const float2 ya0 = make_float2(Y.a0, Y.a0), ya1 = make_float2(Y.a1, Y.a1);
-  const float2 yb0 = make_float2(Y.b0, Y.b0), yb1 = make_float2(Y.b1, Y.b1);
-  const float2 za0 = make_float2(Z.a0, Z.a0), za1 = make_float2(Z.a1, Z.a1);
-  const float2 zb0 = make_float2(Z.b0, Z.b0), zb1 = make_float2(Z.b1, Z.b1);
-  Gathered<float> r;
-  r.ex = quad_lerp<QZ>(fq, xa + yb + zb, X.a0, X.a1, yb0, yb1, zb0, zb1);
-  r.ey = quad_lerp<QZ>(fq + QN, xb + ya + zb, X.b0, X.b1, ya0, ya1, zb0, zb1);
-  r.ez = quad_lerp<QZ>(fq + 2 * QN, xb + yb + za, X.b0, X.b1, yb0, yb1, za0, za1);
-  r.bx = quad_lerp<QZ>(fq + 3 * QN, xb + ya + za, X.b0, X.b1, ya0, ya1, za0, za1);
-  r.by = quad_lerp<QZ>(fq + 4 * QN, xa + yb + za, X.a0, X.a1, yb0, yb1, za0, za1);
-  r.bz = quad_lerp<QZ>(fq + 5 * QN, xa + ya + zb, X.a0, X.a1, ya0, ya1, zb0, zb1);
-  return r;
-}
 
 // Trilinear interpolation from a window plane with compile-time strides (the
 // 2x2x2 nodes at window index n), the two x planes as one packed pair.
@@ -352,7 +254,7 @@ struct Relist {
 // the push's warps do not all take the global-reduction path whenever one of
 // their lanes needs it. A full queue falls back to depositing in place.
 #ifndef PB_JTASK
-#define PB_JTASK 1
+#define PB_JTASK 0
 #endif
 template <typename real>
 struct JTasks {
@@ -634,6 +536,227 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
 #pragma unroll
       for (int e = 0; e < 4; ++e)
         if (gc + e < g.gz && v[e] != (real)0) atomicAdd(dst + e, v[e]);
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// The FP32 push with J summed in the shared window (push_fixj_kernel).
+//
+// push_tiled_kernel sums J of the particles in a lane's home cell in 54
+// registers per lane, which holds the kernel at 2 CTAs of 8 warps per SM. Here
+// every particle adds its 24 J weights to the tile's shared J window with FP32
+// atomic adds (the window is added to the planes once, at the end, as before),
+// so that the registers and the smaller windows allow 3 CTAs per SM, and
+// particles off their home cell take the same path as the others. The density
+// keeps its fixed-point window.
+//
+// Shared memory: J and n windows over the tile and two halo nodes (4 x 6 x 8 x
+// 36 words), E and B over the tile and one halo node (6 planes of 4 x 6 x 36
+// words, from a 16-byte-aligned z start) and a 2-stage particle ring: 64.7 KB.
+struct FixjSmem {
+  static constexpr int WX = kTileX + 4, WY = kTileY + 4, WZ = kWinZ, WN = WX * WY * WZ;      // J, n window
+  static constexpr int FX = kTileX + 2, FY = kTileY + 2, FZ = kWinZ, FN = FX * FY * FZ;      // field window
+  static constexpr int kStages = 2;
+  static constexpr int kWarps = kTileX * kTileY;
+  static constexpr size_t prec_off = (size_t)4 * WN * 4;
+  static constexpr size_t fwin_off = prec_off + (size_t)kWarps * kStages * kLanes * 8 * 4;
+  static constexpr size_t bytes = fwin_off + (size_t)6 * FN * 4;
+};
+
+// The 8 J weights of one component added to the window at node s (the
+// caller checks that the stencil lies inside): value v = q n v_x, the weights
+// of the three axes, the two x planes as a packed pair.
+__device__ __forceinline__ void scatter8_jwin(float* __restrict__ w, int s, float v, float x0, float x1, float y0,
+                                              float y1, float z0, float z1) {
+  constexpr int WY = FixjSmem::WY, WZ = FixjSmem::WZ;
+  const float2 ax = __fmul2_rn(make_float2(x0, x1), make_float2(v, v));
+  const float2 a0 = __fmul2_rn(ax, make_float2(y0, y0));  // (x0 y0, x1 y0)
+  const float2 a1 = __fmul2_rn(ax, make_float2(y1, y1));  // (x0 y1, x1 y1)
+  const float2 t00 = __fmul2_rn(a0, make_float2(z0, z0)), t01 = __fmul2_rn(a0, make_float2(z1, z1));
+  const float2 t10 = __fmul2_rn(a1, make_float2(z0, z0)), t11 = __fmul2_rn(a1, make_float2(z1, z1));
+  atomicAdd(w + s, t00.x);
+  atomicAdd(w + s + 1, t01.x);
+  atomicAdd(w + s + WZ, t10.x);
+  atomicAdd(w + s + WZ + 1, t11.x);
+  atomicAdd(w + s + WY * WZ, t00.y);
+  atomicAdd(w + s + WY * WZ + 1, t01.y);
+  atomicAdd(w + s + WY * WZ + WZ, t10.y);
+  atomicAdd(w + s + WY * WZ + WZ + 1, t11.y);
+}
+
+template <bool VEC_FLUSH, bool RELIST>
+__global__ void __launch_bounds__(kTileX * kTileY * 32, 3)
+push_fixj_kernel(Parts<float> P, TileArgs ta, Fields<float> F, Geom g, PushConst<float> pc, Relist rl,
+                 unsigned long long* err) {
+  using S = FixjSmem;
+  constexpr int WY = S::WY, WZ = S::WZ, WN = S::WN, WX = S::WX;
+  constexpr int FY = S::FY, FZ = S::FZ, FN = S::FN, FX = S::FX;
+  constexpr int kSt = S::kStages;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* win = reinterpret_cast<float*>(smem_raw);  // [4][WN]: jx, jy, jz (FP32), n (fixed point)
+  const int tile = blockIdx.x;
+  const TileGeom& t = ta.t;
+  const int tz = tile % t.ntz, ty = (tile / t.ntz) % t.nty, tx = tile / (t.ntz * t.nty);
+  const int wx0 = tx * kTileX, wy0 = ty * kTileY, wz0 = tz * kLanes;  // J/n window origin
+  for (int q = threadIdx.x; q < 4 * WN; q += blockDim.x) win[q] = 0.f;
+  const int ci0 = wx0 + 2, cj0 = wy0 + 2, ck0 = wz0 + 2;  // the tile's first cell
+  const TileBox tb{ci0, cj0, ck0, (unsigned)min(kTileX, g.nx + 2 - ci0), (unsigned)min(kTileY, g.ny + 2 - cj0),
+                   (unsigned)min(kLanes, g.nz + 2 - ck0)};
+  float* fw = reinterpret_cast<float*>(smem_raw + S::fwin_off);
+  const int fx0 = wx0 + 1, fy0 = wy0 + 1, fz0 = wz0;  // field window origin: one halo node in x, y
+  fill_win<FX, FY, FZ, VEC_FLUSH>(fw, F, g, fx0, fy0, fz0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int G = tile * (kTileX * kTileY) + warp;
+  const int base = ta.goff[G], jmax = ta.gmax[G];
+  const int hi = wx0 + 2 + warp / kTileY, hj = wy0 + 2 + warp % kTileY, hk = wz0 + 2 + lane;
+  const int home_c = pack_cell(hi, hj, hk);
+  const bool home_in = hi < g.nx + 2 && hj < g.ny + 2 && hk < g.nz + 2;
+  int nh = 0;
+  // n: as push_tiled_kernel's density window
+  int slots = 0;
+#pragma unroll
+  for (int w = 0; w < kTileX * kTileY; ++w) slots += ta.gmax[tile * (kTileX * kTileY) + w];
+  const float nscale = fminf(4294967295.f / (float)(slots * kLanes + 1), 8388607.f);
+  unsigned* wn = reinterpret_cast<unsigned*>(win + 3 * WN);
+  __syncthreads();
+  float* prec = reinterpret_cast<float*>(smem_raw + S::prec_off) + warp * kSt * kLanes * 8;
+  auto fetch = [&](int row) {
+    if (row < jmax) {
+      float* stage = prec + (row % kSt) * kLanes * 8;
+      fetch_records(stage + lane * 4, stage + (kLanes + lane) * 4, P, base + row * kLanes + lane);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int s = 0; s < kSt - 1; ++s) fetch(s);
+  unsigned pushed = 0;
+  for (int jj = 0; jj < jmax; ++jj) {
+    fetch(jj + kSt - 1);
+    cp_async_wait<kSt - 1>();
+    const int tslot = base + jj * kLanes + lane;
+    const int st = jj % kSt;
+    float ra[4], rb[4];
+    read_record(prec + st * kLanes * 8 + lane * 4, ra);
+    read_record(prec + st * kLanes * 8 + (kLanes + lane) * 4, rb);
+    const int c = __float_as_int(ra[0]);
+    const bool act = c >= 0;
+    int i = 0, j = 0, k = 0;
+    float fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
+    int cnew = -1;
+    if (act) {
+      ++pushed;
+      unpack_cell(c, i, j, k);
+      fx = ra[1]; fy = ra[2]; fz = ra[3];
+      vx = rb[0]; vy = rb[1]; vz = rb[2];
+      const bool inside = tb.has(i, j, k);
+      bool bal = (pc.bal_interior || !inside) && ballistic(pc, i, j, k, fx, fy, fz);
+      if (!bal && !inside && !stencil_ok(g, i, j, k)) {
+        count_err(err, ERR_DEPOSIT_OOB);
+        bal = true;
+      }
+      if (!bal) {
+        const Axis<float> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+        if (inside)
+          boris4_fast(pc, gather6_win<FY, FZ, FN>(fw, fx0, fy0, fz0, X, Y, Z), vx, vy, vz);
+        else
+          boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
+        if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) count_err(err, ERR_NONFINITE);
+      }
+      advance(i, fx, vx * pc.hdt);
+      advance(j, fy, vy * pc.hdt);
+      advance(k, fz, vz * pc.hdt);
+      // J at x^{n+1/2} into the fixed-point window, or to global memory when
+      // its stencil (nodes i-1 .. i+1 on each axis) leaves the window
+      if (in_array(g, i, j, k)) {
+        if (stencil_ok(g, i, j, k)) {
+          const Axis<float> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+          if (i - 1 >= wx0 && i + 1 < wx0 + WX && j - 1 >= wy0 && j + 1 < wy0 + WY && k - 1 >= wz0 &&
+              k + 1 < wz0 + WZ) {
+            const int ax = X.a - wx0, bx = X.b - wx0, ay = Y.a - wy0, by = Y.b - wy0, az = Z.a - wz0,
+                      bz = Z.b - wz0;
+            scatter8_jwin(win, (ax * WY + by) * WZ + bz, pc.qn * vx, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
+            scatter8_jwin(win + WN, (bx * WY + ay) * WZ + bz, pc.qn * vy, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
+            scatter8_jwin(win + 2 * WN, (bx * WY + by) * WZ + az, pc.qn * vz, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
+          } else {
+            deposit_j(F, g, pc, X, Y, Z, vx, vy, vz);
+          }
+        } else {
+          count_err(err, ERR_DEPOSIT_OOB);
+        }
+      }
+      advance(i, fx, vx * pc.hdt);
+      advance(j, fy, vy * pc.hdt);
+      advance(k, fz, vz * pc.hdt);
+      // n at x^{n+1}
+      const bool inside1 = tb.has(i, j, k);
+      if (inside1 || in_array(g, i, j, k)) {
+        if (inside1 || stencil_ok(g, i, j, k)) {
+          const Axis<float> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+          scatter8_win_fixed(wn, wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b, pc.nw, nscale, X.b0, X.b1, Y.b0,
+                             Y.b1, Z.b0, Z.b1);
+        } else {
+          count_err(err, ERR_DEPOSIT_OOB);
+        }
+      }
+      cnew = inside1 ? pack_cell(i, j, k) : settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
+      if constexpr (!RELIST) store_records(P, tslot, cnew, fx, fy, fz, vx, vy, vz);
+    }
+    if constexpr (RELIST) {
+      const bool away = act && cnew >= 0 && cnew != home_c;
+      bool mover = away;
+      const unsigned mm = __ballot_sync(0xffffffffu, mover);
+      int d = 0;
+      if (mm) {
+        int b = 0;
+        if (lane == 0) b = atomicAdd(rl.append_at, __popc(mm));
+        b = __shfl_sync(0xffffffffu, b, 0);
+        d = b + __popc(mm & ((1u << lane) - 1u));
+        mover = mover && d < rl.cap;
+        if (away && !mover) *rl.nonhome = 1;
+      }
+      if (mover) {
+        store_records(P, d, cnew, fx, fy, fz, vx, vy, vz);
+        P.cell[tslot] = -1;
+      } else if (act) {
+        store_records(P, tslot, cnew, fx, fy, fz, vx, vy, vz);
+      }
+      if (home_in && (!act || cnew < 0 || mover)) {
+        rl.holes[base + nh * kLanes + lane] = jj;
+        ++nh;
+      }
+    }
+  }
+  if (RELIST && home_in) rl.nholes[((hi - 2) * g.ny + (hj - 2)) * g.nz + (hk - 2)] = nh;
+  for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
+  if (lane == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
+  __syncthreads();
+  // flush the window: J as summed, n from its fixed-point sums
+  const int planes[4] = {pc.pjx, pc.pjy, pc.pjz, pc.pn};
+  const float nback = pc.nw / nscale;
+  constexpr int NZ4 = WZ / 4;
+  for (int q4 = threadIdx.x; q4 < 4 * WX * WY * NZ4; q4 += blockDim.x) {
+    const int q = q4 / (WX * WY * NZ4);
+    const int r = q4 % (WX * WY * NZ4);
+    const int a = r / (WY * NZ4), b = (r / NZ4) % WY, c4 = r % NZ4;
+    const int ga = wx0 + a, gb = wy0 + b, gc = wz0 + 4 * c4;
+    if (ga >= g.gx || gb >= g.gy || gc >= g.gz) continue;
+    const uint4 u = *reinterpret_cast<const uint4*>(win + q * WN + (a * WY + b) * WZ + 4 * c4);
+    if ((u.x | u.y | u.z | u.w) == 0u) continue;
+    float v[4];
+    if (q < 3) {
+      v[0] = __uint_as_float(u.x); v[1] = __uint_as_float(u.y); v[2] = __uint_as_float(u.z); v[3] = __uint_as_float(u.w);
+    } else {
+      v[0] = (float)u.x * nback; v[1] = (float)u.y * nback; v[2] = (float)u.z * nback; v[3] = (float)u.w * nback;
+    }
+    float* dst = F.f[planes[q]] + ga * g.sx + gb * g.gz + gc;
+    if (VEC_FLUSH) {
+      red_add_v4(dst, v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (gc + e < g.gz && v[e] != 0.f) atomicAdd(dst + e, v[e]);
     }
   }
 }
