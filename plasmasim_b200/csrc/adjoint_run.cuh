@@ -149,7 +149,6 @@ int adj_restore(pic_ctx* c, const AdjSnap& S) {
     CKR(set_count(c, s, S.count[s]));
     c->tiled[s] = false;
     c->layout[s] = false;
-    c->sp[s].listed = false;
   }
   CK(cudaMemcpyAsync((char*)c->field_mem + (size_t)F_EX * c->plane_bytes, S.planes,
                      kSnapPlanes * c->plane_bytes, cudaMemcpyDeviceToDevice, c->stream));
@@ -208,7 +207,6 @@ int adj_compact(pic_ctx* c, AdjRun& R, int s, int* map) {
   st.cur = 1 - st.cur;
   c->tiled[s] = false;
   c->layout[s] = false;
-  c->sp[s].listed = false;
   R.pend[s] = true;
   R.pend_added[s] = 0;
   return PIC_OK;

@@ -28,17 +28,6 @@
 
 using namespace pb;
 
-// 1: pic_step's push lists the holes and moves particles that left their home
-// cells out of the layout, and every step places them (no classify pass);
-// 0: a classify pass re-lays the particles after each refill
-#ifndef PB_RELIST
-#define PB_RELIST 0
-#endif
-// 1: the FP32 push sums J in the shared window (push_fixj_kernel, 3 CTAs per
-// SM); 0: in per-lane registers (push_tiled_kernel, 2 CTAs per SM)
-#ifndef PB_FIXJ
-#define PB_FIXJ 0
-#endif
 
 namespace {
 
@@ -59,9 +48,6 @@ struct Store {
   // memory (event `readback`); check_spill acts on them
   bool spill_pending = false;
   cudaEvent_t readback = nullptr;
-  // the layout's holes are those the last push listed (its RELIST form), so
-  // the next placement needs no classify pass
-  bool listed = false;
   int* holes = nullptr;   // per-slot scratch: hole rows of every lane column
   int* nholes = nullptr;  // per interior cell: holes of its lane column
   int* nonhome = nullptr; // a particle outside its home cell stayed in the layout
@@ -108,9 +94,6 @@ struct pic_ctx {
   int* append_dev = nullptr;          // end of the append region during a re-layout
   int* rank = nullptr;                // per-slot scratch: placement rank of every appended particle
   int* bucket = nullptr;              // per-slot scratch: appended particles bucketed by their new cell
-  void* jtask_mem = nullptr;          // J deposits queued by the push (JTasks), records A then B
-  long long jtask_cap = 0;
-  int* jtask_count = nullptr;
   int* cnt = nullptr;
   int* offs = nullptr;
   int* cursor = nullptr;
@@ -724,71 +707,22 @@ int do_push(pic_ctx* c, int s, long long first = 0) {
 __global__ void copy_int_kernel(int* dst, const int* src) { *dst = *src; }
 
 // The push of species s: the slots after the layout (particles a placement
-// could not place) with the slot-order kernel, then the tiled kernel. With
-// `relist` (pic_step), the tiled push lists every lane's holes and moves the
-// particles that left their home cell to the append region after *count_dev
-// (push_tiled.cuh, Relist), for the next step's placement.
+// could not place) with the slot-order kernel, then the tiled kernel.
 template <typename real>
-int do_push_tiled(pic_ctx* c, int s, bool relist = false) {
+int do_push_tiled(pic_ctx* c, int s) {
   if (!c->layout[s]) return do_push<real, PUSH_FUSED>(c, s);
-  Store& st = c->sp[s];
   CKR((do_push<real, PUSH_FUSED>(c, s, c->tiled_end[s])));
   const int ntiles = c->tg.ntx * c->tg.nty * c->tg.ntz;
   TileArgs ta{c->tg, c->goff[s][c->lay[s]], c->gmax[s][c->lay[s]]};
-  const size_t smem = PushSmem<real>::bytes;
   const bool vec = sizeof(real) == 4 && c->g.gz % 4 == 0;
-  Relist rl{st.holes, st.nholes, c->append_dev, st.nonhome, (int)st.cap};
-  JTasks<real> jt{make_parts<real>((real*)c->jtask_mem,
-                                   (real*)((char*)c->jtask_mem + parts_record_bytes(c->jtask_cap, sizeof(real)))),
-                  c->jtask_count, (int)c->jtask_cap};
-  CK(cudaMemsetAsync(c->jtask_count, 0, sizeof(int), c->stream));
   const Parts<real> P = parts<real>(c, s);
   const Fields<real> F = fields<real>(c);
   const PushConst<real> pc = push_const<real>(c, s);
   const dim3 grid(ntiles), block(kTileX * kTileY * 32);
-  if (PB_FIXJ && sizeof(real) == 4) {
-    const Parts<float> Pf = parts<float>(c, s);
-    const Fields<float> Ff = fields<float>(c);
-    const PushConst<float> pf = push_const<float>(c, s);
-    const size_t sb = FixjSmem::bytes;
-    if (relist) {
-      copy_int_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, st.count_dev);
-      CKL();
-    }
-    if (vec && relist) push_fixj_kernel<true, true><<<grid, block, sb, c->stream>>>(Pf, ta, Ff, c->g, pf, rl, c->err);
-    else if (vec) push_fixj_kernel<true, false><<<grid, block, sb, c->stream>>>(Pf, ta, Ff, c->g, pf, rl, c->err);
-    else if (relist) push_fixj_kernel<false, true><<<grid, block, sb, c->stream>>>(Pf, ta, Ff, c->g, pf, rl, c->err);
-    else push_fixj_kernel<false, false><<<grid, block, sb, c->stream>>>(Pf, ta, Ff, c->g, pf, rl, c->err);
-    CKL();
-    if (relist) {
-      clamp_count_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.cap, st.count_dev);
-      CKL();
-      st.pending = true;
-      st.listed = true;
-      c->tiled[s] = false;
-    }
-    return PIC_OK;
-  }
-  if (relist) {
-    copy_int_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, st.count_dev);  // movers go after the current end
-    CKL();
-    if (vec) push_tiled_kernel<real, true, true><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, jt, c->err);
-    else push_tiled_kernel<real, false, true><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, jt, c->err);
-    CKL();
-    clamp_count_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.cap, st.count_dev);
-    CKL();
-    st.pending = true;
-    st.listed = true;
-    c->tiled[s] = false;  // the appended particles await the next placement
-  } else {
-    if (vec) push_tiled_kernel<real, true, false><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, jt, c->err);
-    else push_tiled_kernel<real, false, false><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, rl, jt, c->err);
-    CKL();
-  }
-  if (PB_JTASK) {
-    jtask_kernel<real><<<particle_blocks(c->jtask_cap), kThreads, 0, c->stream>>>(jt, F, c->g, pc);
-    CKL();
-  }
+  const size_t smem = PushSmem<real>::bytes;
+  if (vec) push_tiled_kernel<real, true><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, c->err);
+  else push_tiled_kernel<real, false><<<grid, block, smem, c->stream>>>(P, ta, F, c->g, pc, c->err);
+  CKL();
   return PIC_OK;
 }
 
@@ -891,7 +825,6 @@ int do_sort_species(pic_ctx* c, int s) {
   c->lay[s] = nw;
   CKR(set_count(c, s, total));
   CK(cudaMemsetAsync(st.nonhome, 0, sizeof(int), c->stream));
-  st.listed = false;
   c->layout[s] = true;
   c->tiled_end[s] = total;
   c->tiled[s] = true;
@@ -899,16 +832,15 @@ int do_sort_species(pic_ctx* c, int s) {
 }
 
 // In-place re-layout (relayout.cuh): movers and appended particles into the
-// holes of their columns. The hole lists come from a classify pass
-// (relayout_launch) or from the last push (its RELIST form, place_launch).
-// Both issue the placement, set the new count on the device and read the
+// holes of their columns, which a classify pass lists (relayout_launch). It
+// issues the placement, set the new count on the device and read the
 // spill count back into pinned memory without waiting; check_spill acts on
 // that read-back when it has landed (a full sort when many particles found no
 // hole), sync_count reads the count itself when the host needs it.
 __global__ void spill_count_kernel(int* count, int first, const int* nspill) { *count = first + *nspill; }
 
 // The placement of the particles in [tiled_end, *count_dev) into the holes
-// that st.holes / st.nholes list.
+// that st.holes / st.nholes list (place_launch).
 template <typename real>
 int place_launch(pic_ctx* c, int s) {
   Store& st = c->sp[s];
@@ -941,7 +873,6 @@ int place_launch(pic_ctx* c, int s) {
   CK(cudaEventRecord(st.readback, c->stream));
   st.pending = true;
   st.spill_pending = true;
-  st.listed = false;
   c->tiled[s] = true;
   return PIC_OK;
 }
@@ -1010,9 +941,7 @@ template <typename real>
 int relayout_species(pic_ctx* c, const bool (&which)[2]) {
   for (int s = 0; s < 2; ++s) {
     if (!which[s]) continue;
-    if (c->sp[s].listed) {
-      CKR(place_launch<real>(c, s));
-    } else if (c->layout[s]) {
+    if (c->layout[s]) {
       CKR(relayout_launch<real>(c, s));
     } else {
       CKR(sync_count(c, s));
@@ -1102,36 +1031,8 @@ int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0
 }
 
 
-// The count after a refill of `add` particles, stopping at the capacity.
-__global__ void count_add_kernel(int* count, long long add, int cap) {
-  *count = (int)min((long long)*count + add, (long long)cap);
-}
-
-// The refill's particles appended after *count_dev, which the host need not
-// know: the source kernel reads its first slot there, and particles that
-// would pass the capacity are counted as lost (ERR_STORE_FULL) instead.
-template <typename real>
-int do_source_dev(pic_ctx* c, int s, const Slab* slabs, int nslab) {
-  Store& st = c->sp[s];
-  SourceParams sp = source_params(c, s, slabs, nslab, 0);
-  if (sp.total == 0) return PIC_OK;
-  sp.dst_dev = st.count_dev;
-  sp.cap = (int)st.cap;
-  source_kernel<real><<<grid_blocks(sp.total), kThreads, 0, c->stream>>>(parts<real>(c, s), sp, c->err);
-  CKL();
-  count_add_kernel<<<1, 1, 0, c->stream>>>(st.count_dev, sp.total, (int)st.cap);
-  CKL();
-  c->ctr_p += 3 * sp.total;
-  c->ctr_v += 6 * sp.total;
-  st.pending = true;
-  c->tiled[s] = false;
-  return PIC_OK;
-}
-
 // add_*_flat: the shell deletion, then the refill appended (the next step's
-// placement moves it into the layout). On a layout whose holes the last push
-// listed, the count stays on the device: the layout's shell particles are
-// deleted with their rows listed as holes, those after the layout by a scan.
+// re-layout moves it into the layout).
 template <typename real>
 int do_add_flat(pic_ctx* c) {
   Slab slabs[5];
@@ -1139,17 +1040,6 @@ int do_add_flat(pic_ctx* c) {
   for (int s = 0; s < 2; ++s) {
     Store& st = c->sp[s];
     const Parts<real> P = parts<real>(c, s);
-    if (st.listed) {
-      shell_relist_kernel<real><<<grid_blocks((long long)c->tg.ngroups * 32), kThreads, 0, c->stream>>>(
-          P, c->g, c->tg, c->goff[s][c->lay[s]], c->gmax[s][c->lay[s]], st.holes, st.nholes, st.nonhome);
-      CKL();
-      const long long first = c->tiled_end[s];
-      delete_shell_kernel<real><<<particle_blocks(st.cap - first), kThreads, 0, c->stream>>>(
-          P, (int)first, st.count_dev, c->g);
-      CKL();
-      CKR(do_source_dev<real>(c, s, slabs, nslab));
-      continue;
-    }
     CKR(check_spill<real>(c, s, true));
     CKR(sync_count(c, s));
     if (st.count > 0) {
@@ -1172,7 +1062,6 @@ int do_init_particles(pic_ctx* c) {
     CKR(set_count(c, s, 0));
     c->tiled[s] = false;
     c->layout[s] = false;
-    c->sp[s].listed = false;
     const Slab body = {2, c->cfg.nx, 2, c->cfg.ny, 2, c->cfg.nz, 0};
     const Slab extra_cell = {2 + c->cfg.nx, 1, 2, 1, 2, 1, 0};
     CKR(do_source<real>(c, s, &body, 1, 1));
@@ -1297,10 +1186,8 @@ int do_step(pic_ctx* c) {
   CKR(phase_mark(c, PH_FIELD));
   CKR(do_renew_b<real>(c));
   CKR(phase_mark(c, PH_FIELD));
-  // placement of the particles the last push moved out of their home cells
-  // (with the holes it listed), or a re-layout after a refill or an import
-  const bool which[2] = {!c->cfg.slot_order && (c->sp[0].listed || !c->tiled[0]),
-                         !c->cfg.slot_order && (c->sp[1].listed || !c->tiled[1])};
+  // a re-layout after a refill or an import
+  const bool which[2] = {!c->cfg.slot_order && !c->tiled[0], !c->cfg.slot_order && !c->tiled[1]};
   if (which[0] || which[1]) {
     CKR(phase_mark(c, PH_SORT));
     CKR(relayout_species<real>(c, which));
@@ -1312,11 +1199,8 @@ int do_step(pic_ctx* c) {
   if (c->has_xport) CKR(ensure_mig<real>(c));
   // the counts stay on the device: the push and the diagnostics cover the
   // slots up to the capacity and stop at the device count, and the host reads
-  // a count back only when an entry point needs it. A single domain's push
-  // lists the holes and moves the particles that leave their home cells out
-  // of the layout for the next step's placement; a decomposed run's
-  // exchanges append to its counts, and it re-lays its particles after them.
-  for (int s = 0; s < 2; ++s) CKR(do_push_tiled<real>(c, s, PB_RELIST && !c->has_xport));
+  // a count back only when an entry point needs it
+  for (int s = 0; s < 2; ++s) CKR(do_push_tiled<real>(c, s));
   if (c->has_xport) CKR(do_migrate<real>(c));  // sr_particle's exchange between ranks
   CKR(phase_mark(c, PH_PUSH));
   CKR(phase_mark(c, PH_FIELD));
@@ -1437,7 +1321,6 @@ int do_import(pic_ctx* c, int s, const double* rows, const int* flag, long long 
   CKR(set_count(c, s, n));
   c->tiled[s] = false;
   c->layout[s] = false;
-  c->sp[s].listed = false;
   CK(cudaStreamSynchronize(c->stream));
   return PIC_OK;
 }
@@ -1780,32 +1663,14 @@ int pic_create(const pic_config* cfg, pic_ctx** out) {
       }
       if (cudaMalloc(&c->rank, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
       if (cudaMalloc(&c->bucket, sizeof(int) * (size_t)cap) != cudaSuccess) return fail(PIC_ERR_CUDA);
-      // the push's queue of J deposits off their home cells: a sixteenth of the capacity
-      c->jtask_cap = cap / 16 + 4096;
-      if (cudaMalloc(&c->jtask_mem, store_bytes(c->jtask_cap, c->rsize)) != cudaSuccess) return fail(PIC_ERR_CUDA);
-      if (cudaMalloc(&c->jtask_count, sizeof(int)) != cudaSuccess) return fail(PIC_ERR_CUDA);
     }
     const int pb_f = (int)PushSmem<float>::bytes, pb_d = (int)PushSmem<double>::bytes;
-    if (cudaFuncSetAttribute(push_tiled_kernel<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             pb_d) != cudaSuccess ||
-        cudaFuncSetAttribute(push_tiled_kernel<double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             pb_d) != cudaSuccess ||
-        cudaFuncSetAttribute(push_tiled_kernel<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             pb_f) != cudaSuccess ||
-        cudaFuncSetAttribute(push_tiled_kernel<float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             pb_f) != cudaSuccess ||
-        cudaFuncSetAttribute(push_tiled_kernel<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             pb_f) != cudaSuccess ||
-        cudaFuncSetAttribute(push_tiled_kernel<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             pb_f) != cudaSuccess ||
-        (PB_FIXJ && (cudaFuncSetAttribute(push_fixj_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)FixjSmem::bytes) != cudaSuccess ||
-                     cudaFuncSetAttribute(push_fixj_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)FixjSmem::bytes) != cudaSuccess ||
-                     cudaFuncSetAttribute(push_fixj_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)FixjSmem::bytes) != cudaSuccess ||
-                     cudaFuncSetAttribute(push_fixj_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)FixjSmem::bytes) != cudaSuccess)))
+    if (cudaFuncSetAttribute(push_tiled_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, pb_d) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(push_tiled_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, pb_f) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(push_tiled_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, pb_f) !=
+            cudaSuccess)
       return fail(PIC_ERR_CUDA);
   }
   if (cudaMalloc(&c->acc, sizeof(double) * 64) != cudaSuccess) return fail(PIC_ERR_CUDA);
@@ -1851,8 +1716,6 @@ int pic_destroy(pic_ctx* c) {
   }
   cudaFree(c->rank);
   cudaFree(c->bucket);
-  cudaFree(c->jtask_mem);
-  cudaFree(c->jtask_count);
   cudaFree(c->cnt);
   cudaFree(c->offs);
   cudaFree(c->cursor);
@@ -1913,7 +1776,6 @@ int pic_push_deposit_j(pic_ctx* c, int species) {
   for (int s = 0; s < 2; ++s) {
     if (species >= 0 && s != species) continue;
     CKR((c->prec == 64 ? do_push<double, PUSH_J>(c, s) : do_push<float, PUSH_J>(c, s)));
-    c->sp[s].listed = false;  // particles moved without their holes listed
   }
   return PIC_OK;
 }
@@ -1924,7 +1786,6 @@ int pic_drift_deposit_n(pic_ctx* c, int species) {
   for (int s = 0; s < 2; ++s) {
     if (species >= 0 && s != species) continue;
     CKR((c->prec == 64 ? do_drift_n<double>(c, s) : do_drift_n<float>(c, s)));
-    c->sp[s].listed = false;
   }
   return PIC_OK;
 }
@@ -1936,7 +1797,6 @@ int pic_reduce_current(pic_ctx* c) {
 
 int pic_sr_particle(pic_ctx* c) {
   CKR(check_ctx(c));
-  c->sp[0].listed = c->sp[1].listed = false;
   return DISPATCH(c, do_sr_particle)(c);
 }
 

@@ -431,12 +431,6 @@ __device__ __forceinline__ bool in_refill_shell(const Parts<real>& P, const Geom
   return xl || yl || xh || yh || zs;
 }
 
-// Whether cell (i, j, k) can hold a particle of a refill shell (any offset).
-__device__ __forceinline__ bool shell_cell(const Geom& g, int i, int j, int k) {
-  return (g.xlo && i < 4) || (g.ylo && j < 4) || (g.xhi && i >= g.nx) || (g.yhi && j >= g.ny) || k < 4 ||
-         k >= g.nz;
-}
-
 template <typename real>
 __global__ void delete_shell_kernel(Parts<real> P, int first, const int* __restrict__ count, Geom g) {
   const int n = *count;

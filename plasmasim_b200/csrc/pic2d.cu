@@ -44,12 +44,6 @@ enum Plane {
 
 constexpr int kChunk = 2048;     // particle slots per work item
 
-// 1: push2d_seq_kernel (per-thread runs of the cell-sorted slots, deposits
-// summed per cell in registers); 0: push2d_kernel (rows of the chunk,
-// deposits reduced across each warp)
-#ifndef PB_PUSH2D_SEQ
-#define PB_PUSH2D_SEQ 0
-#endif
 constexpr int kCellShift = 16;   // cell = (i << 16) | k
 
 __host__ __device__ __forceinline__ int pack2(int i, int k) { return (i << kCellShift) | k; }
@@ -478,213 +472,6 @@ __global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, con
         P.cell[t] = keep ? pack2(i, k) : -1;
         P.ox[t] = fx; P.oz[t] = fz;
         P.vx[t] = vx; P.vy[t] = vy; P.vz[t] = vz;
-      }
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
-  if ((threadIdx.x & 31) == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
-}
-
-// The same particle part of one step, each thread walking kSeq consecutive
-// slots of the cell-sorted chunk (every slot of the chunk is visited by one
-// thread). Consecutive particles mostly share a cell, so a thread sums the
-// current and density deposits of its particles in registers, over the 3 x 3
-// nodes a particle of its current cell can touch, and adds them to the planes
-// when the cell changes and at the end, instead of reducing every deposit
-// across the warp. A particle gathers, moves and is removed exactly as in
-// push2d_kernel.
-constexpr int kSeq = 16;
-
-// Weights of one axis over the three nodes h-1, h, h+1 around cell h: the
-// half-shifted base is h-1 below the cell's middle, h above it (ax2).
-template <typename real>
-__device__ __forceinline__ void w3(const Ax2<real>& A, int h, real (&w)[3]) {
-  const bool up = A.b == h;
-  w[0] = up ? (real)0 : A.b0;
-  w[1] = up ? A.b0 : A.b1;
-  w[2] = up ? A.b1 : (real)0;
-}
-
-template <typename real>
-struct Patch2 {
-  real jx[2][3], jy[3][3], jz[3][2];  // jx: x nodes h, h+1 x z nodes h-1..h+1; jy: 3 x 3; jz: 3 x (h, h+1)
-  __device__ __forceinline__ void zero() {
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if (a < 2) jx[a][c] = (real)0;
-        jy[a][c] = (real)0;
-        if (c < 2) jz[a][c] = (real)0;
-      }
-  }
-};
-
-template <typename real>
-__device__ __forceinline__ void flush_j(const Patch2<real>& p, real* jx, real* jy, real* jz, int G, int i, int k) {
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (a < 2) atomicAdd(jx + (i + a) * G + (k - 1 + c), p.jx[a][c]);
-      atomicAdd(jy + (i - 1 + a) * G + (k - 1 + c), p.jy[a][c]);
-      if (c < 2) atomicAdd(jz + (i - 1 + a) * G + (k + c), p.jz[a][c]);
-    }
-}
-
-template <typename real>
-__device__ __forceinline__ void flush_n(const real (&n)[3][3], real* dn, int G, int i, int k) {
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) atomicAdd(dn + (i - 1 + a) * G + (k - 1 + c), n[a][c]);
-}
-
-template <typename real>
-__global__ void __launch_bounds__(128, sizeof(real) == 4 ? 4 : 2) push2d_seq_kernel(Pools pools, real* F, const Run<real>* __restrict__ runs,
-                                                         const State* __restrict__ st,
-                                                         const Item* __restrict__ items, int nitems, int chunk,
-                                                         unsigned long long* err) {
-  unsigned pushed = 0;
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const int rs = items[it].run;
-    const int r = rs >> 1, s = rs & 1;
-    const Run<real> R = runs[r];
-    const int n = st[r].count[s];
-    const int first = items[it].first;
-    if (first >= n) continue;  // block-uniform
-    const int last = min(first + chunk, n);
-    const PView<real> P = pview<real>(pools, s);
-    const int G = R.gz;
-    const real T = (real)R.T[s];
-    const real hdt = (real)(0.5 * R.dt / R.dx);
-    const real qn = (real)(R.q * R.nw);
-    const real nw = (real)R.nw;
-    real* jx = plane(F, R, s == 0 ? P_JIX : P_JEX);
-    real* jy = plane(F, R, s == 0 ? P_JIY : P_JEY);
-    real* jz = plane(F, R, s == 0 ? P_JIZ : P_JEZ);
-    real* dn = plane(F, R, s == 0 ? P_NI : P_NE);
-    const real* Ex = plane(F, R, P_EX);
-    const real* Ey = plane(F, R, P_EY);
-    const real* Ez = plane(F, R, P_EZ);
-    const real* Bx = plane(F, R, P_BX);
-    const real* By = plane(F, R, P_BY);
-    const real* Bz = plane(F, R, P_BZ);
-    const int hz = R.nz + 4 - R.a2, hx = R.nx + 4 - R.a2;
-    for (int q0 = first + threadIdx.x * kSeq; q0 < last; q0 += blockDim.x * kSeq) {
-      Patch2<real> pj;
-      real pn[3][3];
-      int cj = -1, cn = -1;  // cells of the two patches (packed), -1: empty
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) pn[a][c] = (real)0;
-      pj.zero();
-      const int q1 = min(q0 + kSeq, last);
-      for (int q = q0; q < q1; ++q) {
-        const long long t = R.poff + q;
-        const int c = P.cell[t];
-        if (c < 0) continue;
-        ++pushed;
-        int i, k;
-        unpack2(c, i, k);
-        real fx = P.ox[t], fz = P.oz[t];
-        real vx = P.vx[t], vy = P.vy[t], vz = P.vz[t];
-        // ballistic margins (:682-686)
-        const bool bal = k < R.a2 || i < R.a2 || k > hz || (k == hz && fz > (real)0) || i > hx ||
-                         (i == hx && fx > (real)0);
-        if (!bal) {
-          if (i < 1 || k < 1 || i > R.gx - 2 || k > R.gz - 2) {
-            atomicAdd(err + ERR_DEPOSIT_OOB, 1ull);
-          } else {
-            const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-            const real ex = bil(Ex, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1) + (real)R.ex_add;
-            const real bz = bil(Bz, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
-            const real ey = bil(Ey, G, X.b, Z.b, X.b0, X.b1, Z.b0, Z.b1) + (real)R.ey_add;
-            const real ez = bil(Ez, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
-            const real bx = bil(Bx, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
-            const real by = bil(By, G, X.a, Z.a, X.a0, X.a1, Z.a0, Z.a1);
-            // cal_track_c4 (:1520-1560)
-            const real S = (real)2 * T / ((real)1 + T * T * (bx * bx + by * by + bz * bz));
-            const real ux = vx + ex * T, uy = vy + ey * T, uz = vz + ez * T;
-            const real uox = ux + T * (uy * bz - uz * by);
-            const real uoy = uy + T * (uz * bx - ux * bz);
-            const real uoz = uz + T * (ux * by - uy * bx);
-            vx = ux + S * (uoy * bz - uoz * by) + ex * T;
-            vy = uy + S * (uoz * bx - uox * bz) + ey * T;
-            vz = uz + S * (uox * by - uoy * bx) + ez * T;
-          }
-        }
-        advance(i, fx, vx * hdt);
-        advance(k, fz, vz * hdt);
-        // J at x^{n+1/2} for dx <= x < (Nx+3) dx, 2 dx <= z < (Nz+2) dx, summed in the patch of its cell
-        if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
-          const int cc = pack2(i, k);
-          if (cc != cj) {
-            if (cj >= 0) {
-              int pi, pk;
-              unpack2(cj, pi, pk);
-              flush_j(pj, jx, jy, jz, G, pi, pk);
-            }
-            pj.zero();
-            cj = cc;
-          }
-          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-          real xb[3], zb[3];
-          w3(X, i, xb);
-          w3(Z, k, zb);
-          const real xa[2] = {X.a0, X.a1}, za[2] = {Z.a0, Z.a1};
-          const real qx = qn * vx, qy = qn * vy, qz = qn * vz;
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int cz = 0; cz < 3; ++cz) {
-              if (a < 2) pj.jx[a][cz] += qx * xa[a] * zb[cz];
-              pj.jy[a][cz] += qy * xb[a] * zb[cz];
-              if (cz < 2) pj.jz[a][cz] += qz * xb[a] * za[cz];
-            }
-        }
-        advance(i, fx, vx * hdt);
-        advance(k, fz, vz * hdt);
-        if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
-          const int cc = pack2(i, k);
-          if (cc != cn) {
-            if (cn >= 0) {
-              int pi, pk;
-              unpack2(cn, pi, pk);
-              flush_n(pn, dn, G, pi, pk);
-            }
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-              for (int cz = 0; cz < 3; ++cz) pn[a][cz] = (real)0;
-            cn = cc;
-          }
-          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-          real xb[3], zb[3];
-          w3(X, i, xb);
-          w3(Z, k, zb);
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int cz = 0; cz < 3; ++cz) pn[a][cz] += nw * xb[a] * zb[cz];
-        }
-        // x exchange at size 1: forward crossers wrap, backward ones are dropped; then removal
-        if (i == R.nx + 2 && k >= 2 && k < R.nz + 2) i -= R.nx;
-        const bool keep = i >= 2 && i < R.nx + 2 && k >= 2 && k < R.nz + 2;
-        P.cell[t] = keep ? pack2(i, k) : -1;
-        P.ox[t] = fx; P.oz[t] = fz;
-        P.vx[t] = vx; P.vy[t] = vy; P.vz[t] = vz;
-      }
-      if (cj >= 0) {
-        int pi, pk;
-        unpack2(cj, pi, pk);
-        flush_j(pj, jx, jy, jz, G, pi, pk);
-      }
-      if (cn >= 0) {
-        int pi, pk;
-        unpack2(cn, pi, pk);
-        flush_n(pn, dn, G, pi, pk);
       }
     }
   }
@@ -1153,8 +940,11 @@ struct pic2d_batch {
   int push_blocks = 148 * 8;
   // graphs
   bool use_graph = true;
-  cudaGraphExec_t graph[1] = {nullptr};  // the plain step on the current pool
-  long long graph_launches = 0;          // kernels in that graph
+  // one graph per kind of step (plain, sort, refill) and starting pool; a
+  // sort or refill step ends on the other pool (graph_cur)
+  cudaGraphExec_t graph[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+  long long graph_launches[3][2] = {{0, 0}, {0, 0}, {0, 0}};  // kernels in each graph
+  int graph_cur[3][2] = {{0, 0}, {0, 0}, {0, 0}};
   long long launches = 0;
 };
 
@@ -1412,12 +1202,6 @@ template <typename real>
 int push(pic2d_batch* b) {
   const Run<real>* R = runs_of<real>(b);
   real* F = (real*)b->field;
-#if PB_PUSH2D_SEQ
-  push2d_seq_kernel<real><<<b->push_blocks, 128, 0, b->stream>>>(b->pool[b->cur], F, R, b->st, b->part_items,
-                                                                  b->n_part, kChunk, b->err);
-  CKL2();
-  return PIC_OK;
-#endif
   switch (b->push_block) {
     case 128:
       push2d_kernel<real, 128><<<b->push_blocks, 128, 0, b->stream>>>(b->pool[b->cur], F, R, b->st, b->part_items,
@@ -1482,48 +1266,53 @@ int step_body(pic2d_batch* b, bool refill, bool sort = false) {
 }
 
 void drop_graphs(pic2d_batch* b) {
-  for (auto& g : b->graph)
-    if (g) {
-      cudaGraphExecDestroy(g);
-      g = nullptr;
-    }
+  for (auto& row : b->graph)
+    for (auto& g : row)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
 }
 
-// nsteps loop bodies. A plain step is replayed from a CUDA graph captured on
-// first use; a step with a refill (every add_interval steps) runs directly,
-// since its compaction moves the particles to the other pool, after which
-// the plain-step graph is captured again for the new pool.
+// nsteps loop bodies, each replayed from a CUDA graph captured on first use:
+// one graph per kind of step -- plain, with the cell sort (every
+// sort_interval steps), with the refill (every add_interval steps) -- and per
+// pool the step starts on, since the sort moves the particles to the other
+// pool. The launches of a step depend on nothing else the host holds (counts,
+// stream counters and the step number live on the device), so at most six
+// graphs cover a run.
 template <typename real>
 int run_steps(pic2d_batch* b, int nsteps) {
   for (int i = 0; i < nsteps; ++i) {
     const bool refill = b->c_add > b->cfg[0].add_interval - 1;
     const int si = b->cfg[0].sort_interval;
     const bool sort = !refill && si > 0 && b->step > 0 && b->step % si == 0;
-    if (refill || sort || !b->use_graph) {
+    if (!b->use_graph) {
       CKR2(step_body<real>(b, refill, sort));
-      if (refill || sort) drop_graphs(b);
     } else {
-      if (!b->graph[0]) {
-        cudaGraph_t graph;
+      const int kind = refill ? 2 : sort ? 1 : 0, cur = b->cur;
+      if (!b->graph[kind][cur]) {
         CK2(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         const long long l0 = b->launches;
-        const int rc = step_body<real>(b, false);
-        cudaGraph_t g = nullptr;
-        const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-        graph = g;
+        const int rc = step_body<real>(b, refill, sort);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+        b->graph_launches[kind][cur] = b->launches - l0;
+        b->launches = l0;
+        b->graph_cur[kind][cur] = b->cur;
+        b->cur = cur;
         if (rc != PIC_OK) {
           if (graph) cudaGraphDestroy(graph);
           return rc;
         }
         CK2(e);
-        b->graph_launches = b->launches - l0;
-        b->launches = l0;
-        const cudaError_t ei = cudaGraphInstantiate(&b->graph[0], graph, 0);
+        const cudaError_t ei = cudaGraphInstantiate(&b->graph[kind][cur], graph, 0);
         cudaGraphDestroy(graph);
         CK2(ei);
       }
-      CK2(cudaGraphLaunch(b->graph[0], b->stream));
-      b->launches += b->graph_launches;
+      CK2(cudaGraphLaunch(b->graph[kind][cur], b->stream));
+      b->launches += b->graph_launches[kind][cur];
+      b->cur = b->graph_cur[kind][cur];
     }
     if (refill) b->c_add = 0;
     b->c_add++;

@@ -9,10 +9,6 @@ namespace pb {
 
 constexpr int kStages = 3;   // particle rows in flight per warp
 
-#ifndef PB_TILE_FASTPATH
-#define PB_TILE_FASTPATH 1
-#endif
-
 // The tile's interior cells: first cell (ci0, cj0, ck0) and extents (the
 // nominal tile clipped at the last interior cell, n + 1, of each axis).
 struct TileBox {
@@ -227,54 +223,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
 
-// Per-step re-listing, the RELIST form of the push: every slot of the layout
-// that the push leaves without a particle of its lane's home cell -- an empty
-// slot, a particle that sr_particle removed, a particle that ended the step in
-// another cell -- is listed as a hole of its lane, in row order, in the
-// per-slot scratch `holes` (laid out like the slots), with the lane's count in
-// `nholes` (indexed by the home cell's interior key). A particle that ended the
-// step in another cell is written to the append region instead of its slot,
-// at slots [*append_at, cap) taken by one atomic per warp and row; when that
-// region is full it stays in its slot. The next step's placement
-// (relayout.cuh) then moves the appended particles into the holes of their
-// new cells, so the push never meets a particle outside its home cell unless
-// the append region ran out.
-struct Relist {
-  int* holes;
-  int* nholes;
-  int* append_at;
-  int* nonhome;  // set when a particle outside its home cell had to stay in the layout
-  int cap;
-};
-
-// The J deposits of particles outside their lane's home cell at x^{n+1/2}
-// (mostly particles that crossed a cell face in the step's first half drift),
-// queued as records (cell, offsets | velocities) at slots [0, *count) of T,
-// up to cap; jtask_kernel deposits them afterwards, one thread each, so that
-// the push's warps do not all take the global-reduction path whenever one of
-// their lanes needs it. A full queue falls back to depositing in place.
-#ifndef PB_JTASK
-#define PB_JTASK 0
-#endif
-template <typename real>
-struct JTasks {
-  Parts<real> T;
-  int* count;
-  int cap;
-};
-
-template <typename real>
-__global__ void __launch_bounds__(256) jtask_kernel(JTasks<real> jt, Fields<real> F, Geom g, PushConst<real> pc) {
-  const int n = min(*jt.count, jt.cap);
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const Rec<real> r = load_records(jt.T, t);
-    int i, j, k;
-    unpack_cell(r.cell, i, j, k);
-    const Axis<real> X = axis_weights(i, r.o[0]), Y = axis_weights(j, r.o[1]), Z = axis_weights(k, r.o[2]);
-    deposit_j(F, g, pc, X, Y, Z, r.v[0], r.v[1], r.v[2]);
-  }
-}
-
 // The fused particle part of one step (push, J deposit at x^{n+1/2}, drift,
 // n deposit at x^{n+1}, sr_particle) for one species over the tiled layout;
 // the same arithmetic as push_kernel<real, PUSH_FUSED> apart from the FP32
@@ -282,14 +230,14 @@ __global__ void __launch_bounds__(256) jtask_kernel(JTasks<real> jt, Fields<real
 // window. One CTA per tile, one warp per group.
 //
 // J of a particle in its lane's home cell at x^{n+1/2} is summed in registers;
-// the others add theirs to global memory with reductions (FP32 shared atomics
-// would be compare-and-swap loops). The density goes to the window with shared
+// the others add theirs to global memory with reductions (a shared J window
+// taking every particle's 24 weights by FP32 shared atomics, which frees the
+// registers for 3 CTAs per SM, measured 1.7x slower). The density goes to the window with shared
 // reductions (every active lane at once): integer ones on fixed-point sums in
 // FP32, FP64 atomics in FP64.
-template <typename real, bool VEC_FLUSH, bool RELIST>
+template <typename real, bool VEC_FLUSH>
 __global__ void __launch_bounds__(kTileX * kTileY * 32, 2)
-push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc, Relist rl,
-                  JTasks<real> jt, unsigned long long* err) {
+push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc, unsigned long long* err) {
   using S = PushSmem<real>;
   constexpr int WY = S::WY, WZ = S::WZ, WN = S::WN, WX = S::WX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -300,28 +248,18 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   // window origin: two nodes below the tile's first interior cell (2 + tx*TX)
   const int wx0 = tx * kTileX, wy0 = ty * kTileY, wz0 = tz * kLanes;
   for (int q = threadIdx.x; q < 4 * WN; q += blockDim.x) win[q] = (real)0;
-  // FP32: E and B of the tile's gather stencils as node quads
-  float4* fq = reinterpret_cast<float4*>(smem_raw + S::fwin_off);
+  // FP32: E and B over the window, one plane per component
+  float* fw = reinterpret_cast<float*>(smem_raw + S::fwin_off);
   const int ci0 = wx0 + 2, cj0 = wy0 + 2, ck0 = wz0 + 2;  // the tile's first cell
   const TileBox tb{ci0, cj0, ck0, (unsigned)min(kTileX, g.nx + 2 - ci0), (unsigned)min(kTileY, g.ny + 2 - cj0),
                    (unsigned)min(kLanes, g.nz + 2 - ck0)};
-  // the ring's memory, not in use yet, stages the window's rows
-  if constexpr (S::kFieldWin) {
-    if (PB_QUADS)
-      fill_quads<S::QX, S::QY, S::QZ, VEC_FLUSH>(fq, reinterpret_cast<float*>(smem_raw + S::prec_off), F, g, ci0,
-                                                 cj0, ck0);
-    else
-      fill_win<WX, WY, WZ, VEC_FLUSH>(reinterpret_cast<float*>(fq), F, g, wx0, wy0, wz0);
-  }
+  if constexpr (S::kFieldWin) fill_win<WX, WY, WZ, VEC_FLUSH>(fw, F, g, wx0, wy0, wz0);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int G = tile * (kTileX * kTileY) + warp;
   const int base = ta.goff[G], jmax = ta.gmax[G];
   // home cell of this lane
   const int hi = wx0 + 2 + warp / kTileY, hj = wy0 + 2 + warp % kTileY, hk = wz0 + 2 + lane;
-  const int home_c = pack_cell(hi, hj, hk);
-  const bool home_in = hi < g.nx + 2 && hj < g.ny + 2 && hk < g.nz + 2;  // the lane has an interior cell
-  int nh = 0;  // RELIST: holes listed by this lane
   real* wn = win + 3 * WN;
   // FP32: the density window holds fixed-point sums (scatter8_win_fixed) at a
   // scale that no node of this tile can overflow
@@ -365,7 +303,6 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     const bool act = c >= 0;
     int i = 0, j = 0, k = 0;
     real fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
-    int cnew = -1;
     if (act) {
       ++pushed;
       unpack_cell(c, i, j, k);
@@ -375,29 +312,19 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       // stencils lie in the array, and it is ballistic only when the
       // Absorb_grid2 layer reaches interior cells
       const bool inside = tb.has(i, j, k);
-#if PB_TILE_FASTPATH
       bool bal = (pc.bal_interior || !inside) && ballistic(pc, i, j, k, fx, fy, fz);
       if (!bal && !inside && !stencil_ok(g, i, j, k)) {
-#else
-      bool bal = ballistic(pc, i, j, k, fx, fy, fz);
-      if (!bal && !stencil_ok(g, i, j, k)) {
-#endif
         count_err(err, ERR_DEPOSIT_OOB);
         bal = true;
       }
       if (!bal) {
         const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
         if constexpr (S::kFieldWin) {
-          // the quads cover the stencils of particles in the tile's cells;
-          // the plane window those within two halo nodes of the tile
-          const bool in_win = PB_QUADS ? inside
-                                       : i - 1 >= wx0 && i + 1 < wx0 + WX && j - 1 >= wy0 && j + 1 < wy0 + WY &&
-                                             k - 1 >= wz0 && k + 1 < wz0 + WZ;
+          // the window covers the stencils of particles within two halo nodes of the tile
+          const bool in_win = i - 1 >= wx0 && i + 1 < wx0 + WX && j - 1 >= wy0 && j + 1 < wy0 + WY &&
+                              k - 1 >= wz0 && k + 1 < wz0 + WZ;
           if (in_win)
-            boris4_fast(pc,
-                        PB_QUADS ? gather6_quads<S::QY, S::QZ>(fq, ci0, cj0, ck0, X, Y, Z)
-                                 : gather6_win<WY, WZ, WN>(reinterpret_cast<const float*>(fq), wx0, wy0, wz0, X, Y, Z),
-                        vx, vy, vz);
+            boris4_fast(pc, gather6_win<WY, WZ, WN>(fw, wx0, wy0, wz0, X, Y, Z), vx, vy, vz);
           else
             boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
         } else {
@@ -415,22 +342,8 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
         acc.add(pc.qn * vx, pc.qn * vy, pc.qn * vz, X, Y, Z, bx, by, bz);
       } else if (in_array(g, i, j, k)) {
         if (stencil_ok(g, i, j, k)) {
-#if PB_JTASK
-          // queued for jtask_kernel: one append per warp, the deposit in full warps later
-          const unsigned am = __activemask();
-          const unsigned tm = __ballot_sync(am, true);
-          const int leader = __ffs(tm) - 1;
-          int b = 0;
-          if (lane == leader) b = atomicAdd(jt.count, __popc(tm));
-          b = __shfl_sync(am, b, leader) + __popc(tm & ((1u << lane) - 1u));
-          if (b < jt.cap) {
-            store_records(jt.T, b, pack_cell(i, j, k), fx, fy, fz, vx, vy, vz);
-          } else
-#endif
-          {
-            const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-            deposit_j(F, g, pc, X, Y, Z, vx, vy, vz);
-          }
+          const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+          deposit_j(F, g, pc, X, Y, Z, vx, vy, vz);
         } else {
           count_err(err, ERR_DEPOSIT_OOB);
         }
@@ -441,14 +354,9 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       advance(j, fy, vy * pc.hdt);
       advance(k, fz, vz * pc.hdt);
       // n at x^{n+1}
-#if PB_TILE_FASTPATH
       const bool inside1 = tb.has(i, j, k);
       if (inside1 || in_array(g, i, j, k)) {
         if (inside1 || stencil_ok(g, i, j, k)) {
-#else
-      if (in_array(g, i, j, k)) {
-        if (stencil_ok(g, i, j, k)) {
-#endif
           const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
           if constexpr (kFixedN)
             scatter8_win_fixed(reinterpret_cast<unsigned*>(wn), wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b,
@@ -459,40 +367,11 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
           count_err(err, ERR_DEPOSIT_OOB);
         }
       }
-#if PB_TILE_FASTPATH
       // sr_particle keeps a particle of an interior cell where it is
-      cnew = inside1 ? pack_cell(i, j, k) : settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
-#else
-      cnew = settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
-#endif
-      if constexpr (!RELIST) store_records(P, t, cnew, fx, fy, fz, vx, vy, vz);
-    }
-    if constexpr (RELIST) {
-      const bool away = act && cnew >= 0 && cnew != home_c;
-      bool mover = away;
-      const unsigned mm = __ballot_sync(0xffffffffu, mover);
-      int d = 0;
-      if (mm) {  // warp-uniform: the row's movers take consecutive append slots
-        int b = 0;
-        if (lane == 0) b = atomicAdd(rl.append_at, __popc(mm));
-        b = __shfl_sync(0xffffffffu, b, 0);
-        d = b + __popc(mm & ((1u << lane) - 1u));
-        mover = mover && d < rl.cap;  // a full append region keeps the particle in its slot
-        if (away && !mover) *rl.nonhome = 1;
-      }
-      if (mover) {
-        store_records(P, d, cnew, fx, fy, fz, vx, vy, vz);
-        P.cell[t] = -1;
-      } else if (act) {
-        store_records(P, t, cnew, fx, fy, fz, vx, vy, vz);
-      }
-      if (home_in && (!act || cnew < 0 || mover)) {
-        rl.holes[base + nh * kLanes + lane] = jj;
-        ++nh;
-      }
+      const int cnew = inside1 ? pack_cell(i, j, k) : settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
+      store_records(P, t, cnew, fx, fy, fz, vx, vy, vz);
     }
   }
-  if (RELIST && home_in) rl.nholes[((hi - 2) * g.ny + (hj - 2)) * g.nz + (hk - 2)] = nh;
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
   if (lane == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
   // the lane's home-cell sums into the window (nodes h-1 .. h+1 around it)
@@ -540,225 +419,5 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   }
 }
 
-
-// ---------------------------------------------------------------------------
-// The FP32 push with J summed in the shared window (push_fixj_kernel).
-//
-// push_tiled_kernel sums J of the particles in a lane's home cell in 54
-// registers per lane, which holds the kernel at 2 CTAs of 8 warps per SM. Here
-// every particle adds its 24 J weights to the tile's shared J window with FP32
-// atomic adds (the window is added to the planes once, at the end, as before),
-// so that the registers and the smaller windows allow 3 CTAs per SM, and
-// particles off their home cell take the same path as the others. The density
-// keeps its fixed-point window.
-//
-// Shared memory: J and n windows over the tile and two halo nodes (4 x 6 x 8 x
-// 36 words), E and B over the tile and one halo node (6 planes of 4 x 6 x 36
-// words, from a 16-byte-aligned z start) and a 2-stage particle ring: 64.7 KB.
-struct FixjSmem {
-  static constexpr int WX = kTileX + 4, WY = kTileY + 4, WZ = kWinZ, WN = WX * WY * WZ;      // J, n window
-  static constexpr int FX = kTileX + 2, FY = kTileY + 2, FZ = kWinZ, FN = FX * FY * FZ;      // field window
-  static constexpr int kStages = 2;
-  static constexpr int kWarps = kTileX * kTileY;
-  static constexpr size_t prec_off = (size_t)4 * WN * 4;
-  static constexpr size_t fwin_off = prec_off + (size_t)kWarps * kStages * kLanes * 8 * 4;
-  static constexpr size_t bytes = fwin_off + (size_t)6 * FN * 4;
-};
-
-// The 8 J weights of one component added to the window at node s (the
-// caller checks that the stencil lies inside): value v = q n v_x, the weights
-// of the three axes, the two x planes as a packed pair.
-__device__ __forceinline__ void scatter8_jwin(float* __restrict__ w, int s, float v, float x0, float x1, float y0,
-                                              float y1, float z0, float z1) {
-  constexpr int WY = FixjSmem::WY, WZ = FixjSmem::WZ;
-  const float2 ax = __fmul2_rn(make_float2(x0, x1), make_float2(v, v));
-  const float2 a0 = __fmul2_rn(ax, make_float2(y0, y0));  // (x0 y0, x1 y0)
-  const float2 a1 = __fmul2_rn(ax, make_float2(y1, y1));  // (x0 y1, x1 y1)
-  const float2 t00 = __fmul2_rn(a0, make_float2(z0, z0)), t01 = __fmul2_rn(a0, make_float2(z1, z1));
-  const float2 t10 = __fmul2_rn(a1, make_float2(z0, z0)), t11 = __fmul2_rn(a1, make_float2(z1, z1));
-  atomicAdd(w + s, t00.x);
-  atomicAdd(w + s + 1, t01.x);
-  atomicAdd(w + s + WZ, t10.x);
-  atomicAdd(w + s + WZ + 1, t11.x);
-  atomicAdd(w + s + WY * WZ, t00.y);
-  atomicAdd(w + s + WY * WZ + 1, t01.y);
-  atomicAdd(w + s + WY * WZ + WZ, t10.y);
-  atomicAdd(w + s + WY * WZ + WZ + 1, t11.y);
-}
-
-template <bool VEC_FLUSH, bool RELIST>
-__global__ void __launch_bounds__(kTileX * kTileY * 32, 3)
-push_fixj_kernel(Parts<float> P, TileArgs ta, Fields<float> F, Geom g, PushConst<float> pc, Relist rl,
-                 unsigned long long* err) {
-  using S = FixjSmem;
-  constexpr int WY = S::WY, WZ = S::WZ, WN = S::WN, WX = S::WX;
-  constexpr int FY = S::FY, FZ = S::FZ, FN = S::FN, FX = S::FX;
-  constexpr int kSt = S::kStages;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float* win = reinterpret_cast<float*>(smem_raw);  // [4][WN]: jx, jy, jz (FP32), n (fixed point)
-  const int tile = blockIdx.x;
-  const TileGeom& t = ta.t;
-  const int tz = tile % t.ntz, ty = (tile / t.ntz) % t.nty, tx = tile / (t.ntz * t.nty);
-  const int wx0 = tx * kTileX, wy0 = ty * kTileY, wz0 = tz * kLanes;  // J/n window origin
-  for (int q = threadIdx.x; q < 4 * WN; q += blockDim.x) win[q] = 0.f;
-  const int ci0 = wx0 + 2, cj0 = wy0 + 2, ck0 = wz0 + 2;  // the tile's first cell
-  const TileBox tb{ci0, cj0, ck0, (unsigned)min(kTileX, g.nx + 2 - ci0), (unsigned)min(kTileY, g.ny + 2 - cj0),
-                   (unsigned)min(kLanes, g.nz + 2 - ck0)};
-  float* fw = reinterpret_cast<float*>(smem_raw + S::fwin_off);
-  const int fx0 = wx0 + 1, fy0 = wy0 + 1, fz0 = wz0;  // field window origin: one halo node in x, y
-  fill_win<FX, FY, FZ, VEC_FLUSH>(fw, F, g, fx0, fy0, fz0);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int G = tile * (kTileX * kTileY) + warp;
-  const int base = ta.goff[G], jmax = ta.gmax[G];
-  const int hi = wx0 + 2 + warp / kTileY, hj = wy0 + 2 + warp % kTileY, hk = wz0 + 2 + lane;
-  const int home_c = pack_cell(hi, hj, hk);
-  const bool home_in = hi < g.nx + 2 && hj < g.ny + 2 && hk < g.nz + 2;
-  int nh = 0;
-  // n: as push_tiled_kernel's density window
-  int slots = 0;
-#pragma unroll
-  for (int w = 0; w < kTileX * kTileY; ++w) slots += ta.gmax[tile * (kTileX * kTileY) + w];
-  const float nscale = fminf(4294967295.f / (float)(slots * kLanes + 1), 8388607.f);
-  unsigned* wn = reinterpret_cast<unsigned*>(win + 3 * WN);
-  __syncthreads();
-  float* prec = reinterpret_cast<float*>(smem_raw + S::prec_off) + warp * kSt * kLanes * 8;
-  auto fetch = [&](int row) {
-    if (row < jmax) {
-      float* stage = prec + (row % kSt) * kLanes * 8;
-      fetch_records(stage + lane * 4, stage + (kLanes + lane) * 4, P, base + row * kLanes + lane);
-    }
-    cp_async_commit();
-  };
-#pragma unroll
-  for (int s = 0; s < kSt - 1; ++s) fetch(s);
-  unsigned pushed = 0;
-  for (int jj = 0; jj < jmax; ++jj) {
-    fetch(jj + kSt - 1);
-    cp_async_wait<kSt - 1>();
-    const int tslot = base + jj * kLanes + lane;
-    const int st = jj % kSt;
-    float ra[4], rb[4];
-    read_record(prec + st * kLanes * 8 + lane * 4, ra);
-    read_record(prec + st * kLanes * 8 + (kLanes + lane) * 4, rb);
-    const int c = __float_as_int(ra[0]);
-    const bool act = c >= 0;
-    int i = 0, j = 0, k = 0;
-    float fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
-    int cnew = -1;
-    if (act) {
-      ++pushed;
-      unpack_cell(c, i, j, k);
-      fx = ra[1]; fy = ra[2]; fz = ra[3];
-      vx = rb[0]; vy = rb[1]; vz = rb[2];
-      const bool inside = tb.has(i, j, k);
-      bool bal = (pc.bal_interior || !inside) && ballistic(pc, i, j, k, fx, fy, fz);
-      if (!bal && !inside && !stencil_ok(g, i, j, k)) {
-        count_err(err, ERR_DEPOSIT_OOB);
-        bal = true;
-      }
-      if (!bal) {
-        const Axis<float> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-        if (inside)
-          boris4_fast(pc, gather6_win<FY, FZ, FN>(fw, fx0, fy0, fz0, X, Y, Z), vx, vy, vz);
-        else
-          boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
-        if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) count_err(err, ERR_NONFINITE);
-      }
-      advance(i, fx, vx * pc.hdt);
-      advance(j, fy, vy * pc.hdt);
-      advance(k, fz, vz * pc.hdt);
-      // J at x^{n+1/2} into the fixed-point window, or to global memory when
-      // its stencil (nodes i-1 .. i+1 on each axis) leaves the window
-      if (in_array(g, i, j, k)) {
-        if (stencil_ok(g, i, j, k)) {
-          const Axis<float> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-          if (i - 1 >= wx0 && i + 1 < wx0 + WX && j - 1 >= wy0 && j + 1 < wy0 + WY && k - 1 >= wz0 &&
-              k + 1 < wz0 + WZ) {
-            const int ax = X.a - wx0, bx = X.b - wx0, ay = Y.a - wy0, by = Y.b - wy0, az = Z.a - wz0,
-                      bz = Z.b - wz0;
-            scatter8_jwin(win, (ax * WY + by) * WZ + bz, pc.qn * vx, X.a0, X.a1, Y.b0, Y.b1, Z.b0, Z.b1);
-            scatter8_jwin(win + WN, (bx * WY + ay) * WZ + bz, pc.qn * vy, X.b0, X.b1, Y.a0, Y.a1, Z.b0, Z.b1);
-            scatter8_jwin(win + 2 * WN, (bx * WY + by) * WZ + az, pc.qn * vz, X.b0, X.b1, Y.b0, Y.b1, Z.a0, Z.a1);
-          } else {
-            deposit_j(F, g, pc, X, Y, Z, vx, vy, vz);
-          }
-        } else {
-          count_err(err, ERR_DEPOSIT_OOB);
-        }
-      }
-      advance(i, fx, vx * pc.hdt);
-      advance(j, fy, vy * pc.hdt);
-      advance(k, fz, vz * pc.hdt);
-      // n at x^{n+1}
-      const bool inside1 = tb.has(i, j, k);
-      if (inside1 || in_array(g, i, j, k)) {
-        if (inside1 || stencil_ok(g, i, j, k)) {
-          const Axis<float> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-          scatter8_win_fixed(wn, wx0, wy0, wz0, F.f[pc.pn], g, X.b, Y.b, Z.b, pc.nw, nscale, X.b0, X.b1, Y.b0,
-                             Y.b1, Z.b0, Z.b1);
-        } else {
-          count_err(err, ERR_DEPOSIT_OOB);
-        }
-      }
-      cnew = inside1 ? pack_cell(i, j, k) : settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
-      if constexpr (!RELIST) store_records(P, tslot, cnew, fx, fy, fz, vx, vy, vz);
-    }
-    if constexpr (RELIST) {
-      const bool away = act && cnew >= 0 && cnew != home_c;
-      bool mover = away;
-      const unsigned mm = __ballot_sync(0xffffffffu, mover);
-      int d = 0;
-      if (mm) {
-        int b = 0;
-        if (lane == 0) b = atomicAdd(rl.append_at, __popc(mm));
-        b = __shfl_sync(0xffffffffu, b, 0);
-        d = b + __popc(mm & ((1u << lane) - 1u));
-        mover = mover && d < rl.cap;
-        if (away && !mover) *rl.nonhome = 1;
-      }
-      if (mover) {
-        store_records(P, d, cnew, fx, fy, fz, vx, vy, vz);
-        P.cell[tslot] = -1;
-      } else if (act) {
-        store_records(P, tslot, cnew, fx, fy, fz, vx, vy, vz);
-      }
-      if (home_in && (!act || cnew < 0 || mover)) {
-        rl.holes[base + nh * kLanes + lane] = jj;
-        ++nh;
-      }
-    }
-  }
-  if (RELIST && home_in) rl.nholes[((hi - 2) * g.ny + (hj - 2)) * g.nz + (hk - 2)] = nh;
-  for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
-  if (lane == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
-  __syncthreads();
-  // flush the window: J as summed, n from its fixed-point sums
-  const int planes[4] = {pc.pjx, pc.pjy, pc.pjz, pc.pn};
-  const float nback = pc.nw / nscale;
-  constexpr int NZ4 = WZ / 4;
-  for (int q4 = threadIdx.x; q4 < 4 * WX * WY * NZ4; q4 += blockDim.x) {
-    const int q = q4 / (WX * WY * NZ4);
-    const int r = q4 % (WX * WY * NZ4);
-    const int a = r / (WY * NZ4), b = (r / NZ4) % WY, c4 = r % NZ4;
-    const int ga = wx0 + a, gb = wy0 + b, gc = wz0 + 4 * c4;
-    if (ga >= g.gx || gb >= g.gy || gc >= g.gz) continue;
-    const uint4 u = *reinterpret_cast<const uint4*>(win + q * WN + (a * WY + b) * WZ + 4 * c4);
-    if ((u.x | u.y | u.z | u.w) == 0u) continue;
-    float v[4];
-    if (q < 3) {
-      v[0] = __uint_as_float(u.x); v[1] = __uint_as_float(u.y); v[2] = __uint_as_float(u.z); v[3] = __uint_as_float(u.w);
-    } else {
-      v[0] = (float)u.x * nback; v[1] = (float)u.y * nback; v[2] = (float)u.z * nback; v[3] = (float)u.w * nback;
-    }
-    float* dst = F.f[planes[q]] + ga * g.sx + gb * g.gz + gc;
-    if (VEC_FLUSH) {
-      red_add_v4(dst, v[0], v[1], v[2], v[3]);
-    } else {
-#pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if (gc + e < g.gz && v[e] != 0.f) atomicAdd(dst + e, v[e]);
-    }
-  }
-}
 
 }  // namespace pb

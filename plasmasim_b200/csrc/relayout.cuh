@@ -101,43 +101,6 @@ __global__ void classify_kernel(Parts<real> P, Geom g, TileGeom t, const int* __
   if (home >= 0) nholes[home] = nh;
 }
 
-// The shell deletion of a refill (add_*_flat :6015-6031) on a layout whose
-// holes the last push listed (the RELIST push of push_tiled.cuh), one warp per
-// group. Only a lane whose home cell can hold shell particles reads its column
-// -- the push keeps every other particle of the layout in its home cell --
-// unless `nonhome` reports that a push left particles outside their home
-// cells, when every lane reads its column. A deleted particle's row joins its
-// lane's hole list, so the refill's particles find those slots.
-template <typename real>
-__global__ void shell_relist_kernel(Parts<real> P, Geom g, TileGeom t, const int* __restrict__ goff,
-                                    const int* __restrict__ gmax, int* holes, int* nholes,
-                                    const int* __restrict__ nonhome) {
-  constexpr int U = 4;  // rows whose loads are in flight together
-  const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (G >= t.ngroups) return;
-  int hi, hj, hk;
-  const bool own = home_cell(g, t, G, lane, hi, hj, hk);
-  if (!(*nonhome || (own && shell_cell(g, hi, hj, hk)))) return;  // no warp-wide operation follows
-  const int key = own ? ((hi - 2) * g.ny + (hj - 2)) * g.nz + (hk - 2) : -1;
-  int nh = own ? nholes[key] : 0;
-  const int base = goff[G], m = gmax[G];
-  for (int r0 = 0; r0 < m; r0 += U) {
-    int c[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) c[u] = r0 + u < m ? P.cell[base + (r0 + u) * kLanes + lane] : -1;
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int slot = base + (r0 + u) * kLanes + lane;
-      if (c[u] >= 0 && in_refill_shell(P, g, c[u], slot)) {
-        P.cell[slot] = -1;
-        if (own) holes[base + nh++ * kLanes + lane] = r0 + u;
-      }
-    }
-  }
-  if (own) nholes[key] = nh;
-}
-
 __global__ void clamp_count_kernel(const int* append_at, int cap, int* count_dev) {
   *count_dev = min(*append_at, cap);
 }

@@ -33,13 +33,9 @@
 namespace pb {
 
 // Layout slack of a full sort: rows added to a group beyond its fullest lane,
-// count / PB_SLACK_DIV + PB_SLACK_ROWS.
-#ifndef PB_SLACK_DIV
-#define PB_SLACK_DIV 16
-#endif
-#ifndef PB_SLACK_ROWS
-#define PB_SLACK_ROWS 2
-#endif
+// count / kSlackDiv + kSlackRows (a slack of count / 32 measured no faster).
+constexpr int kSlackDiv = 16;
+constexpr int kSlackRows = 2;
 
 constexpr int kTileX = 2;
 constexpr int kTileY = 4;
@@ -161,7 +157,7 @@ __global__ void group_size_kernel(Geom g, TileGeom t, const int* __restrict__ st
   c = max(c, refill_reserve(refill, g, t, G, lane));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
-  if (c > 0) c += c / PB_SLACK_DIV + PB_SLACK_ROWS;
+  if (c > 0) c += c / kSlackDiv + kSlackRows;
   if (lane == 0) {
     gmax[G] = c;
     gcap[G] = c * kLanes;
