@@ -309,10 +309,16 @@ def run_batch2d(nruns: int, steps: int, warmup: int):
     rc, c1 = B.status()
     pushed = int(c1[3] - c0[3])
     B.close()
+    # algorithmic bytes: every particle's cell and five FP32 values read and written
+    peak, kind = measured_peaks()
+    gbs = pushed * 48 / (ms / 1e3) / 1e9
     return {"workload": f"{nruns} independent x-z runs (PIC2D), grid sides uniform in [64, 256], "
                         "16-64 particles/cell/species, coil current and drift seeded-random",
             "value": pushed / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
-            "particles": pushed // max(steps, 1), "launch_shape": list(choice), "graph": True,
+            "particles": pushed // max(steps, 1),
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "bytes": "particles x 48 (cell + 5 FP32 values, read and written)", "peak_kind": kind},
+            "launch_shape": list(choice), "graph": True,
             "kernels_per_step": int(c1[5] - c0[5]) // max(steps, 1), "device_errors": [int(x) for x in c1[:3]]}
 
 

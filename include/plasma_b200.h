@@ -366,9 +366,14 @@ int pic2d_get_particles(pic2d_batch *b, int run, int species, double *rows6, lon
  * bz ex ey ez jix0 jiy0 jiz0 jex0 jey0 jez0 ni ne phi), (nx+4)*(nz+4) nodes,
  * z fastest. */
 int pic2d_get_grid(pic2d_batch *b, int run, double *records);
-/* No counterpart in the reference. Tunes the push launch shape on the batch's
- * next steps (ordinary steps of the runs); choice2 = {block size, blocks}. */
+/* No counterpart in the reference. Tunes the push tile shape on the batch's
+ * next 16 steps (ordinary steps of the runs): tiles of 1, 2, 4 or 8 rows of
+ * 32 cells, with 8 or 16 blocks per SM; choice2 = {tile rows, blocks}. */
 int pic2d_autotune(pic2d_batch *b, int *choice2);
+/* No counterpart in the reference. Sets the push tile shape that
+ * pic2d_autotune chooses (tile rows 1, 2, 4 or 8; persistent blocks >= 1), e.g.
+ * one tuned on an earlier batch of the same sizes. */
+int pic2d_set_push_shape(pic2d_batch *b, int tile_rows, int blocks);
 int pic2d_set_graph(pic2d_batch *b, int enable);
 /* counters8: [0..2] device errors as pic_status, [3] particle pushes,
  * [4] steps taken, [5] kernels launched. */

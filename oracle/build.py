@@ -128,6 +128,9 @@ REF2D_CONFIGS = {
     "sq64": {**NORMALIZED_2D, **_geom2d(64, 64, 4, 8, 4, 8)},
     # 32 x 128 cells, 3 x 3 particles per cell, a different current and drift
     "rect": {**NORMALIZED_2D, **_geom2d(32, 128, 3, 6, 3, 6), "ORACLE_I": 20.0, "ORACLE_V": 0.15},
+    # 32 x 16 cells, 3 x 3 particles per cell: half of a 32-cell z tile of the
+    # batched push (the reference's sine transform needs power-of-two sides)
+    "half": {**NORMALIZED_2D, **_geom2d(32, 16, 3, 4, 2, 4), "ORACLE_I": 12.0, "ORACLE_V": 0.2},
 }
 
 

@@ -16,8 +16,11 @@
 // Layout: runs are concatenated. Fields: per run 18 planes of (nx+4)(nz+4)
 // nodes, z fastest. Particles: per species one pool, run r owning slots
 // [poff_r, poff_r + cap_r): cell (i << 16 | k), the in-cell offsets along x
-// and z, and vx vy vz. Work lists map persistent blocks onto (run, chunk)
-// items so that one launch covers every run whatever its size.
+// and z, and vx vy vz, in the tiled layout of Layout2 (one lane column of 32
+// slot-wide rows per cell), which the cell sort rebuilds every sort_interval
+// steps and after each refill. Work lists map persistent blocks onto (run,
+// chunk) or (run, tile) items so that one launch covers every run whatever
+// its size.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -41,6 +44,8 @@ enum Plane {
   P_EX, P_EY, P_EZ, P_BX, P_BY, P_BZ, P_B0X, P_B0Y, P_B0Z,
   P_JIX, P_JIY, P_JIZ, P_JEX, P_JEY, P_JEZ, P_NI, P_NE, P_PHI, P_COUNT
 };
+static_assert(P_EY == P_EX + 1 && P_BZ == P_EX + 5 && P_JEX == P_JIX + 3 && P_NE == P_NI + 1,
+              "the push indexes E, B, J and n planes by offset");
 
 constexpr int kChunk = 2048;     // particle slots per work item
 
@@ -72,6 +77,9 @@ struct Run {
   int add_interval;
   int sz_dst;             // offset of the run's sine tables (Nx then Nz)
   long long roff;         // offset of the run's Poisson buffers (nx * nz)
+  // tiled layout: group (i, b) holds cells (i, 2 + 32 b + lane); the run's
+  // groups are [gbase, gbase + ngroups), nx rows of nzb = ceil(nz / 32)
+  int nzb, gbase, ngroups;
 };
 
 struct Pools {
@@ -329,97 +337,164 @@ __device__ __forceinline__ void dep4(real* P, int G, int i, int k, real v, real 
   atomicAdd(P + (i + 1) * G + k + 1, v * (x1 * z1));
 }
 
-// dep4 for a whole warp: runs of neighbouring lanes whose four nodes coincide
-// (particles of one cell and half-cell, adjacent after the cell sort) are
-// summed with a segmented shuffle reduction, and the first lane of each run
-// adds the sums to the plane. Every lane of the warp calls it; `active`
-// selects the lanes that deposit. A warp without such runs adds directly.
+// The particle layout the cell sort builds, per run and species: group
+// (i, b) holds the particles of cells (i, 2 + 32 b + l), l = 0 .. 31 the lane,
+// in gmax rows of 32 slots, slot = poff + goff[G] - goff[gbase] + 32 row + l.
+// After the sort every particle sits in its lane's home cell; between sorts a
+// particle keeps its slot wherever it moves. Empty slots hold cell -1.
+struct Layout2 {
+  const int* goff[2];  // per group: exclusive scan of 32 gmax over all groups (+ the total)
+  const int* gmax[2];  // per group: rows
+};
+
+// Rows of particles each warp of push2d_tiled_kernel fetches ahead with
+// cp.async (1: loads at the point of use)
+#ifndef PB_RING2D
+#define PB_RING2D 3
+#endif
+
+__device__ __forceinline__ void cp_async_ca(void* smem, const void* gmem, int bytes) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if (bytes == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(sa), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit2() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+
+// Sums of one lane's home cell (hi, hk) over the nodes its particles deposit
+// on: jx on x nodes hi, hi+1 and z nodes hk-1 .. hk+1 (node-aligned x,
+// half-shifted z); jy and n on x and z nodes hi-1 .. hi+1, hk-1 .. hk+1; jz on
+// x nodes hi-1 .. hi+1 and z nodes hk, hk+1.
 template <typename real>
-__device__ __forceinline__ void dep4_warp(real* P, int G, bool active, int i, int k, real v, real x0, real x1,
-                                          real z0, real z1) {
-  const int lane = threadIdx.x & 31;
-  const int key = active ? i * G + k : -1 - lane;
-  const int prev = __shfl_up_sync(0xffffffffu, key, 1);
-  const bool head = lane == 0 || prev != key;
-  const unsigned heads = __ballot_sync(0xffffffffu, head);
-  real w0 = v * (x0 * z0), w1 = v * (x1 * z0), w2 = v * (x0 * z1), w3 = v * (x1 * z1);
-  if (heads != 0xffffffffu) {  // warp-uniform
-    const unsigned after = lane == 31 ? 0u : heads & (0xffffffffu << (lane + 1));
-    const int end = after ? __ffs(after) - 2 : 31;  // last lane of this lane's run
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const real o0 = __shfl_down_sync(0xffffffffu, w0, off);
-      const real o1 = __shfl_down_sync(0xffffffffu, w1, off);
-      const real o2 = __shfl_down_sync(0xffffffffu, w2, off);
-      const real o3 = __shfl_down_sync(0xffffffffu, w3, off);
-      if (lane + off <= end) {
-        w0 += o0;
-        w1 += o1;
-        w2 += o2;
-        w3 += o3;
-      }
-    }
-  }
-  if (active && head) {
-    atomicAdd(P + i * G + k, w0);
-    atomicAdd(P + (i + 1) * G + k, w1);
-    atomicAdd(P + i * G + k + 1, w2);
-    atomicAdd(P + (i + 1) * G + k + 1, w3);
-  }
+struct Home2 {
+  real jx[2][3], jy[3][3], jz[3][2], n[3][3];
+};
+
+// The half-shifted weights (b0, b1) of a particle of home cell h over the
+// three nodes h-1 .. h+1 (its base is h-1 or h).
+template <typename real>
+__device__ __forceinline__ void spread3(const Ax2<real>& A, int h, real (&w)[3]) {
+  const bool lo = A.b < h;
+  w[0] = lo ? A.b0 : (real)0;
+  w[1] = lo ? A.b1 : A.b0;
+  w[2] = lo ? (real)0 : A.b1;
 }
 
 // The particle part of one step for every run and species (the push loop,
-// the drift loop and the x exchange + removal in one pass). item = (run*2 +
-// species, first slot relative to the run). A block walks its chunk in rows of
-// BLOCK slots with every lane present, so that the deposits can sum the lanes
-// of a warp that share nodes before their atomics: after the cell sort,
-// neighbouring lanes mostly deposit on the same nodes.
-template <typename real, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, const Run<real>* __restrict__ runs,
-                                                       const State* __restrict__ st, const Item* __restrict__ items,
-                                                       int nitems, int chunk, unsigned long long* err) {
+// the drift loop and the x exchange + removal in one pass) over the tiled
+// layout. item = (run * 2 + species, tile): a tile is TX x 32 cells (TX rows
+// of groups), one warp per group. The block stages the tile's E and B over a
+// window of two nodes around it in shared memory; a particle whose stencil
+// leaves the window (it moved more than a cell since the sort) gathers from
+// the planes. J (at x^{n+1/2}) and n (at x^{n+1}) of a particle in its lane's
+// home cell are summed in the lane's registers (Home2) and added to the planes
+// once per group; a particle elsewhere adds its terms to the planes directly.
+// 512 resident threads per SM in FP32 (128 registers: the 30 home sums and
+// the particle in flight fit without spills), 256 in FP64.
+template <typename real, int TX>
+__global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX * 32))
+    push2d_tiled_kernel(Pools pools, real* F, const Run<real>* __restrict__ runs, Layout2 L,
+                        const Item* __restrict__ items, int nitems, unsigned long long* err) {
+  constexpr int WX = TX + 4, WZ = 36, WN = WX * WZ;
+  constexpr int kSt = sizeof(real) == 4 || PB_RING2D < 2 ? PB_RING2D : 2;  // FP64: static shared memory
+  __shared__ real fw[6 * WN];  // ex ey ez bx by bz
+  // per warp and stage: the row's five reals and cells, lane-contiguous
+  __shared__ real ring_r[TX][kSt][5][32];
+  __shared__ int ring_c[TX][kSt][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned pushed = 0;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int rs = items[it].run;
     const int r = rs >> 1, s = rs & 1;
-    const Run<real> R = runs[r];
-    const int n = st[r].count[s];
-    const int first = items[it].first;
-    if (first >= n) continue;  // block-uniform
-    const int last = min(first + chunk, n);
-    const PView<real> P = pview<real>(pools, s);
+    // the run's constants as scalars (a copy of the whole Run, indexed by the
+    // species, would live in local memory)
+    const Run<real>& RR = runs[r];
+    struct {
+      int nx, nz, gx, gz, nzb, gbase, a2;
+      long long nodes, poff, foff;
+    } R{RR.nx, RR.nz, RR.gx, RR.gz, RR.nzb, RR.gbase, RR.a2, RR.nodes, RR.poff, RR.foff};
+    const double Ts = s == 0 ? RR.T[0] : RR.T[1];
+    const int tile = items[it].first;
+    const int i0 = 2 + (tile / R.nzb) * TX, k0 = 2 + 32 * (tile % R.nzb);
+    const int wx0 = i0 - 2, wz0 = k0 - 2;  // window origin (node)
     const int G = R.gz;
-    const real T = (real)R.T[s];
-    const real hdt = (real)(0.5 * R.dt / R.dx);
-    const real qn = (real)(R.q * R.nw);
-    const real nw = (real)R.nw;
-    real* jx = plane(F, R, s == 0 ? P_JIX : P_JEX);
-    real* jy = plane(F, R, s == 0 ? P_JIY : P_JEY);
-    real* jz = plane(F, R, s == 0 ? P_JIZ : P_JEZ);
-    real* dn = plane(F, R, s == 0 ? P_NI : P_NE);
-    const real* Ex = plane(F, R, P_EX);
-    const real* Ey = plane(F, R, P_EY);
-    const real* Ez = plane(F, R, P_EZ);
-    const real* Bx = plane(F, R, P_BX);
-    const real* By = plane(F, R, P_BY);
-    const real* Bz = plane(F, R, P_BZ);
-    for (int qb = first; qb < last; qb += BLOCK) {  // block-uniform
-      const int q = qb + threadIdx.x;
-      const long long t = R.poff + q;
-      const int c = q < last ? P.cell[t] : -1;
-      const bool act = c >= 0;
-      int i = 0, k = 0;
-      real fx = 0, fz = 0, vx = 0, vy = 0, vz = 0;
-      if (act) {
+    real* const F0 = F + R.foff;
+    // planes of this species' J (p = 0..2) and n (p = 3)
+    auto pj = [&](int p) { return F0 + (long long)(p < 3 ? P_JIX + 3 * s + p : P_NI + s) * R.nodes; };
+    __syncthreads();  // the last item's gathers are done
+    for (int q = threadIdx.x; q < 6 * WN; q += blockDim.x) {
+      const int p = q / WN, a = (q / WZ) % WX, c = q % WZ;
+      const int gi = wx0 + a, gk = wz0 + c;
+      fw[q] = gi < R.gx && gk < G ? F0[(long long)(P_EX + p) * R.nodes + gi * G + gk] : (real)0;
+    }
+    __syncthreads();
+    const int hi = i0 + warp, hk = k0 + lane;  // this lane's home cell
+    if (hi < R.nx + 2) {  // warp-uniform
+      const PView<real> P = pview<real>(pools, s);
+      const int Gi = R.gbase + (hi - 2) * R.nzb + (tile % R.nzb);
+      const long long base = R.poff + L.goff[s][Gi] - L.goff[s][R.gbase] + lane;
+      const long long end = R.poff + RR.cap;  // rows of a layout that overflowed the run were not written
+      const int m = L.gmax[s][Gi];
+      const real T = (real)Ts;
+      const real hdt = (real)(0.5 * RR.dt / RR.dx);
+      const real qn = (real)(RR.q * RR.nw);
+      const real nw = (real)RR.nw;
+      const real ex_add = (real)RR.ex_add, ey_add = (real)RR.ey_add;
+      const int hz = R.nz + 4 - R.a2, hx = R.nx + 4 - R.a2;
+      Home2<real> h;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          h.jy[a][c] = h.n[a][c] = (real)0;
+          if (a < 2) h.jx[a][c] = (real)0;
+          if (c < 2) h.jz[a][c] = (real)0;
+        }
+      // each lane copies and reads only its own slots, so the per-thread
+      // cp.async groups need no warp barrier
+      auto fetch = [&](int row) {
+        const long long t = base + 32LL * row;
+        if (kSt > 1 && row < m && t < end) {
+          const int st = row % kSt;
+          cp_async_ca(&ring_c[warp][st][lane], P.cell + t, 4);
+          cp_async_ca(&ring_r[warp][st][0][lane], P.ox + t, sizeof(real));
+          cp_async_ca(&ring_r[warp][st][1][lane], P.oz + t, sizeof(real));
+          cp_async_ca(&ring_r[warp][st][2][lane], P.vx + t, sizeof(real));
+          cp_async_ca(&ring_r[warp][st][3][lane], P.vy + t, sizeof(real));
+          cp_async_ca(&ring_r[warp][st][4][lane], P.vz + t, sizeof(real));
+        }
+        if (kSt > 1) cp_async_commit2();
+      };
+#pragma unroll
+      for (int q = 0; q < kSt - 1; ++q) fetch(q);
+      for (int row = 0; row < m; ++row) {
+        fetch(row + kSt - 1);
+        const long long t = base + 32LL * row;
+        if (t >= end) break;
+        int c;
+        real fx, fz, vx, vy, vz;
+        if (kSt > 1) {
+          cp_async_wait2<kSt - 1>();
+          const int st = row % kSt;
+          c = ring_c[warp][st][lane];
+          fx = ring_r[warp][st][0][lane];
+          fz = ring_r[warp][st][1][lane];
+          vx = ring_r[warp][st][2][lane];
+          vy = ring_r[warp][st][3][lane];
+          vz = ring_r[warp][st][4][lane];
+        } else {
+          c = P.cell[t];
+          fx = P.ox[t]; fz = P.oz[t];
+          vx = P.vx[t]; vy = P.vy[t]; vz = P.vz[t];
+        }
+        if (c < 0) continue;
         ++pushed;
+        int i, k;
         unpack2(c, i, k);
-        fx = P.ox[t];
-        fz = P.oz[t];
-        vx = P.vx[t];
-        vy = P.vy[t];
-        vz = P.vz[t];
         // ballistic margins (:682-686): z < A2, z > Nz+4-A2, x < A2, x > Nx+4-A2 (cells)
-        const int hz = R.nz + 4 - R.a2, hx = R.nx + 4 - R.a2;
         const bool bal = k < R.a2 || i < R.a2 || k > hz || (k == hz && fz > (real)0) || i > hx ||
                          (i == hx && fx > (real)0);
         if (!bal) {
@@ -428,12 +503,25 @@ __global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, con
           } else {
             const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
             // ex, bz: x aligned, z shifted; ez, bx: x shifted, z aligned; ey: both shifted; by: both aligned
-            real ex = bil(Ex, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1) + (real)R.ex_add;
-            real bz = bil(Bz, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
-            real ey = bil(Ey, G, X.b, Z.b, X.b0, X.b1, Z.b0, Z.b1) + (real)R.ey_add;
-            real ez = bil(Ez, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
-            real bx = bil(Bx, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
-            real by = bil(By, G, X.a, Z.a, X.a0, X.a1, Z.a0, Z.a1);
+            real ex, ey, ez, bx, by, bz;
+            if (i - 1 >= wx0 && i + 1 < wx0 + WX && k - 1 >= wz0 && k + 1 < wz0 + WZ) {
+              const int xa = X.a - wx0, xb = X.b - wx0, za = Z.a - wz0, zb = Z.b - wz0;
+              ex = bil(fw + 0 * WN, WZ, xa, zb, X.a0, X.a1, Z.b0, Z.b1);
+              ey = bil(fw + 1 * WN, WZ, xb, zb, X.b0, X.b1, Z.b0, Z.b1);
+              ez = bil(fw + 2 * WN, WZ, xb, za, X.b0, X.b1, Z.a0, Z.a1);
+              bx = bil(fw + 3 * WN, WZ, xb, za, X.b0, X.b1, Z.a0, Z.a1);
+              by = bil(fw + 4 * WN, WZ, xa, za, X.a0, X.a1, Z.a0, Z.a1);
+              bz = bil(fw + 5 * WN, WZ, xa, zb, X.a0, X.a1, Z.b0, Z.b1);
+            } else {
+              ex = bil(F0 + (long long)P_EX * R.nodes, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
+              ey = bil(F0 + (long long)P_EY * R.nodes, G, X.b, Z.b, X.b0, X.b1, Z.b0, Z.b1);
+              ez = bil(F0 + (long long)P_EZ * R.nodes, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
+              bx = bil(F0 + (long long)P_BX * R.nodes, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
+              by = bil(F0 + (long long)P_BY * R.nodes, G, X.a, Z.a, X.a0, X.a1, Z.a0, Z.a1);
+              bz = bil(F0 + (long long)P_BZ * R.nodes, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
+            }
+            ex += ex_add;
+            ey += ey_add;
             // cal_track_c4 (:1520-1560)
             const real S = (real)2 * T / ((real)1 + T * T * (bx * bx + by * by + bz * bz));
             const real ux = vx + ex * T, uy = vy + ey * T, uz = vz + ez * T;
@@ -447,25 +535,50 @@ __global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, con
         }
         advance(i, fx, vx * hdt);
         advance(k, fz, vz * hdt);
-      }
-      // J deposit at x^{n+1/2} for dx <= x < (Nx+3) dx, 2 dx <= z < (Nz+2) dx
-      {
-        const bool dep = act && i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2;
-        const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-        dep4_warp(jx, G, dep, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1);
-        dep4_warp(jy, G, dep, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1);
-        dep4_warp(jz, G, dep, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1);
-      }
-      if (act) {
+        // J deposit at x^{n+1/2} for dx <= x < (Nx+3) dx, 2 dx <= z < (Nz+2) dx
+        if (i == hi && k == hk) {
+          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+          real xb[3], zb[3];
+          spread3(X, hi, xb);
+          spread3(Z, hk, zb);
+          const real px0 = qn * vx * X.a0, px1 = qn * vx * X.a1;
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            h.jx[0][cc] += px0 * zb[cc];
+            h.jx[1][cc] += px1 * zb[cc];
+          }
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            const real py = qn * vy * xb[b], pz = qn * vz * xb[b];
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) h.jy[b][cc] += py * zb[cc];
+            h.jz[b][0] += pz * Z.a0;
+            h.jz[b][1] += pz * Z.a1;
+          }
+        } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
+          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+          dep4(pj(0), G, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1);
+          dep4(pj(1), G, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1);
+          dep4(pj(2), G, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1);
+        }
         advance(i, fx, vx * hdt);
         advance(k, fz, vz * hdt);
-      }
-      {
-        const bool dep = act && i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2;
-        const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-        dep4_warp(dn, G, dep, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1);
-      }
-      if (act) {
+        // n at x^{n+1}, same range
+        if (i == hi && k == hk) {
+          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+          real xb[3], zb[3];
+          spread3(X, hi, xb);
+          spread3(Z, hk, zb);
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            const real pn = nw * xb[b];
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) h.n[b][cc] += pn * zb[cc];
+          }
+        } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
+          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+          dep4(pj(3), G, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1);
+        }
         // x exchange at size 1: forward crossers wrap, backward ones are dropped; then removal
         if (i == R.nx + 2 && k >= 2 && k < R.nz + 2) i -= R.nx;
         const bool keep = i >= 2 && i < R.nx + 2 && k >= 2 && k < R.nz + 2;
@@ -473,10 +586,25 @@ __global__ void __launch_bounds__(BLOCK) push2d_kernel(Pools pools, real* F, con
         P.ox[t] = fx; P.oz[t] = fz;
         P.vx[t] = vx; P.vy[t] = vy; P.vz[t] = vz;
       }
+      if (kSt > 1) cp_async_wait2<0>();  // the next item refills the ring
+      // the home sums into the planes (home cells are interior, so every
+      // node lies in the array); untouched nodes are skipped
+      if (hk < R.nz + 2) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            const int node = (hi - 1 + a) * G + (hk - 1 + cc);
+            if (a < 2 && h.jx[a][cc] != (real)0) atomicAdd(pj(0) + node + G, h.jx[a][cc]);
+            if (h.jy[a][cc] != (real)0) atomicAdd(pj(1) + node, h.jy[a][cc]);
+            if (cc < 2 && h.jz[a][cc] != (real)0) atomicAdd(pj(2) + node + 1, h.jz[a][cc]);
+            if (h.n[a][cc] != (real)0) atomicAdd(pj(3) + node, h.n[a][cc]);
+          }
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
-  if ((threadIdx.x & 31) == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
+  if (lane == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
 }
 
 // Density deposit of every particle (fdtd's set-up, :583-607).
@@ -604,60 +732,6 @@ __global__ void delete5_kernel(Pools pools, const Run<real>* __restrict__ runs, 
       if (del) P.cell[t] = -1;
     }
   }
-}
-
-// Stable compaction of every run's slots: flags -> per-run exclusive scan ->
-// scatter into the second pool; counts become the live totals.
-template <typename real>
-__global__ void live2d_kernel(Pools pools, const Run<real>* __restrict__ runs, const State* __restrict__ st,
-                              const Item* __restrict__ items, int nitems, int chunk, int s, int* flags, long long pool_cap) {
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const int rs = items[it].run;
-    if ((rs & 1) != s) continue;
-    const int r = rs >> 1;
-    const Run<real> R = runs[r];
-    const int n = st[r].count[s];
-    const int first = items[it].first;
-    const int last = (int)min((long long)first + chunk, R.cap);
-    for (int q = first + threadIdx.x; q < last; q += blockDim.x) {
-      const long long t = R.poff + q;
-      flags[t] = (q < n && pools.cell[s][t] >= 0) ? 1 : 0;
-    }
-  }
-}
-
-template <typename real>
-__global__ void compact2d_kernel(Pools src, Pools dst, const Run<real>* __restrict__ runs, State* st,
-                                 const Item* __restrict__ items, int nitems, int chunk, int s, const int* __restrict__ pos,
-                                 const int* __restrict__ flags) {
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const int rs = items[it].run;
-    if ((rs & 1) != s) continue;
-    const int r = rs >> 1;
-    const Run<real> R = runs[r];
-    const int base = pos[R.poff];
-    const int first = items[it].first;
-    const int last = (int)min((long long)first + chunk, R.cap);
-    const PView<real> A = pview<real>(src, s), B = pview<real>(dst, s);
-    for (int q = first + threadIdx.x; q < last; q += blockDim.x) {
-      const long long t = R.poff + q;
-      if (!flags[t]) continue;
-      const long long d = R.poff + (pos[t] - base);
-      B.cell[d] = A.cell[t];
-      B.ox[d] = A.ox[t]; B.oz[d] = A.oz[t];
-      B.vx[d] = A.vx[t]; B.vy[d] = A.vy[t]; B.vz[d] = A.vz[t];
-    }
-  }
-}
-
-template <typename real>
-__global__ void compact2d_count_kernel(const Run<real>* __restrict__ runs, State* st, int nruns, int s,
-                                       const int* __restrict__ pos, const int* __restrict__ flags) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nruns) return;
-  const Run<real> R = runs[r];
-  const long long e = R.poff + R.cap - 1;
-  st[r].count[s] = pos[e] + flags[e] - pos[R.poff];
 }
 
 // ------------------------------------------------------------ renew_phi
@@ -927,9 +1001,16 @@ struct pic2d_batch {
   int* pos = nullptr;
   int* scan_tmp = nullptr;
   size_t scan_len = 0;
-  int* ccnt = nullptr;   // cell sort: particles per cell, first slot per cell, cursors (rho_len each)
-  int* coffs = nullptr;
+  int* ccnt = nullptr;   // cell sort: particles per cell and cursors (rho_len each)
   int* ccur = nullptr;
+  // tiled layout (Layout2): groups of every run, their run, rows and offsets
+  int ngroups = 0;
+  int* grun = nullptr;
+  int* gsz = nullptr;                   // ngroups + 1 (the last stays 0)
+  int* goff[2] = {nullptr, nullptr};    // ngroups + 1
+  int* gmax[2] = {nullptr, nullptr};
+  Item* ptile_items = nullptr; int n_ptile = 0;  // (run*2+s, tile) of the push
+  int tile_x = 4;                       // group rows per push tile (tuned)
   int* step_dev = nullptr;
   unsigned long long* err = nullptr;
   int c_add = 0;
@@ -1037,12 +1118,12 @@ int scan_excl(pic2d_batch* b, const int* in, int* out, long long n, int* tmp, si
 
 // ---------------------------------------------------------- cell sort
 // The reference draws its particles uniformly over each source slab, so their
-// order in the lists says nothing about where they are; deposited in that
-// order, every lane of a warp adds to different nodes and the L2 reductions
-// bound the step. A counting sort of every run's particles by cell (into the
-// other pool, empty slots dropped) lets neighbouring lanes share nodes, which
-// push2d_kernel's deposits then sum before their atomics. Keys index the
-// run's interior cells from R.roff (the nx * nz layout of its Poisson buffer).
+// order in the lists says nothing about where they are. A counting sort of
+// every run's particles by cell into the tiled layout of the other pool
+// (Layout2; empty and deleted slots dropped) puts the particles of one cell in
+// one lane's column, so that push2d_tiled_kernel's warps read whole rows and
+// their lanes deposit on different nodes. Keys index the run's interior cells
+// from R.roff (the nx * nz layout of its Poisson buffer).
 __device__ __forceinline__ int warp_add_count(int* counter, int key, bool active) {
   const int lane = threadIdx.x & 31;
   const unsigned peers = __match_any_sync(0xffffffffu, active ? key : -1 - lane);
@@ -1084,11 +1165,33 @@ __global__ void cellcount2d_kernel(Pools pools, const Run<real>* __restrict__ ru
   }
 }
 
-// Each particle to slot (cell's first slot + its rank) of the other pool.
+// Rows of every group: its fullest lane's count (one warp per group); gsz =
+// 32 rows, scanned into the groups' offsets.
+template <typename real>
+__global__ void group_rows2d_kernel(const Run<real>* __restrict__ runs, const int* __restrict__ grun, int ngroups,
+                                    const int* __restrict__ cnt, int* gmax, int* gsz) {
+  const int G = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (G >= ngroups) return;  // warp-uniform
+  const Run<real> R = runs[grun[G]];
+  const int q = G - R.gbase;
+  const int i = q / R.nzb, k = (q % R.nzb) * 32 + lane;
+  int m = k < R.nz ? cnt[R.roff + i * R.nz + k] : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) {
+    gmax[G] = m;
+    gsz[G] = 32 * m;
+  }
+}
+
+// Each particle to row (its rank in its cell) of its cell's lane column in the
+// other pool. A particle past the run's capacity is lost (ERR_STORE_FULL).
 template <typename real>
 __global__ void cellscatter2d_kernel(Pools src, Pools dst, const Run<real>* __restrict__ runs,
                                      const State* __restrict__ st, const Item* __restrict__ items, int nitems,
-                                     int chunk, int s, const int* __restrict__ offs, int* cursor) {
+                                     int chunk, int s, const int* __restrict__ goff, int* cursor,
+                                     unsigned long long* err) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int rs = items[it].run;
     if ((rs & 1) != s) continue;
@@ -1097,7 +1200,7 @@ __global__ void cellscatter2d_kernel(Pools src, Pools dst, const Run<real>* __re
     const int first = items[it].first;
     const int last = min(first + chunk, n);
     const PView<real> A = pview<real>(src, s), B = pview<real>(dst, s);
-    const int base = offs[R.roff];
+    const int base = goff[R.gbase];
     for (int qb = first; qb < last; qb += blockDim.x) {  // block-uniform
       const int q = qb + threadIdx.x;
       const long long t = R.poff + q;
@@ -1105,7 +1208,13 @@ __global__ void cellscatter2d_kernel(Pools src, Pools dst, const Run<real>* __re
       const int key = q < last ? sort_key(R, c) : -1;
       const int rank = warp_add_count(cursor, key < 0 ? 0 : key, key >= 0);
       if (key < 0) continue;
-      const long long d = R.poff + (offs[key] - base) + rank;
+      const int i = (int)((key - R.roff) / R.nz), k = (int)((key - R.roff) % R.nz);
+      const long long rel = (long long)goff[R.gbase + i * R.nzb + (k >> 5)] - base + 32LL * rank + (k & 31);
+      if (rel >= R.cap) {
+        atomicAdd(err + ERR_STORE_FULL, 1ull);
+        continue;
+      }
+      const long long d = R.poff + rel;
       B.cell[d] = c;
       B.ox[d] = A.ox[t]; B.oz[d] = A.oz[t];
       B.vx[d] = A.vx[t]; B.vy[d] = A.vy[t]; B.vz[d] = A.vz[t];
@@ -1113,57 +1222,57 @@ __global__ void cellscatter2d_kernel(Pools src, Pools dst, const Run<real>* __re
   }
 }
 
-// Live particles of every run after the sort.
+// The empty slots of every group (rows past its lane's count) to cell -1.
 template <typename real>
-__global__ void cellsort_count_kernel(const Run<real>* __restrict__ runs, State* st, int nruns, int s,
-                                      const int* __restrict__ offs, const int* __restrict__ cnt) {
+__global__ void pad2d_kernel(int* cell, const Run<real>* __restrict__ runs, const int* __restrict__ grun, int ngroups,
+                             const int* __restrict__ goff, const int* __restrict__ gmax, const int* __restrict__ cnt) {
+  const int G = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (G >= ngroups) return;
+  const Run<real> R = runs[grun[G]];
+  const int q = G - R.gbase;
+  const int i = q / R.nzb, k = (q % R.nzb) * 32 + lane;
+  const int have = k < R.nz ? cnt[R.roff + i * R.nz + k] : 0;
+  const long long rel0 = (long long)goff[G] - goff[R.gbase] + lane;
+  for (int row = have; row < gmax[G]; ++row) {
+    const long long rel = rel0 + 32LL * row;
+    if (rel < R.cap) cell[R.poff + rel] = -1;
+  }
+}
+
+// Slots in use of every run after the sort: the end of its last group.
+template <typename real>
+__global__ void layout_count2d_kernel(const Run<real>* __restrict__ runs, State* st, int nruns, int s,
+                                      const int* __restrict__ goff) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nruns) return;
   const Run<real> R = runs[r];
-  const long long e = R.roff + (long long)R.nx * R.nz - 1;
-  st[r].count[s] = offs[e] + cnt[e] - offs[R.roff];
+  st[r].count[s] = (int)min((long long)goff[R.gbase + R.ngroups] - goff[R.gbase], R.cap);
 }
 
-// Every run's particles by cell into the other pool, empty slots dropped.
+// Every run's particles by cell into the tiled layout of the other pool.
 template <typename real>
 int cellsort(pic2d_batch* b) {
   const int nb = 1 - b->cur;
   const long long nc = b->rho_len;
   const Run<real>* R = runs_of<real>(b);
+  const int gblocks = (int)((32LL * b->ngroups + 255) / 256);
   for (int s = 0; s < 2; ++s) {
     CK2(cudaMemsetAsync(b->ccnt, 0, sizeof(int) * (size_t)nc, b->stream));
     CK2(cudaMemsetAsync(b->ccur, 0, sizeof(int) * (size_t)nc, b->stream));
     cellcount2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], R, b->st, b->part_items,
                                                                             b->n_part, kChunk, s, b->ccnt);
     CKL2();
-    CKR2(scan_excl(b, b->ccnt, b->coffs, nc, b->scan_tmp, b->scan_len));
+    group_rows2d_kernel<real><<<gblocks, 256, 0, b->stream>>>(R, b->grun, b->ngroups, b->ccnt, b->gmax[s], b->gsz);
+    CKL2();
+    CKR2(scan_excl(b, b->gsz, b->goff[s], b->ngroups + 1, b->scan_tmp, b->scan_len));
     cellscatter2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(
-        b->pool[b->cur], b->pool[nb], R, b->st, b->part_items, b->n_part, kChunk, s, b->coffs, b->ccur);
+        b->pool[b->cur], b->pool[nb], R, b->st, b->part_items, b->n_part, kChunk, s, b->goff[s], b->ccur, b->err);
     CKL2();
-    cellsort_count_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(R, b->st, b->nruns, s, b->coffs,
-                                                                               b->ccnt);
+    pad2d_kernel<real><<<gblocks, 256, 0, b->stream>>>(b->pool[nb].cell[s], R, b->grun, b->ngroups, b->goff[s],
+                                                       b->gmax[s], b->ccnt);
     CKL2();
-  }
-  b->cur = nb;
-  return PIC_OK;
-}
-
-// Removes every run's empty slots, keeping order (into the other pool).
-template <typename real>
-int compact(pic2d_batch* b) {
-  const int nb = 1 - b->cur;
-  for (int s = 0; s < 2; ++s) {
-    live2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], runs_of<real>(b), b->st,
-                                                                      b->part_items, b->n_part, kChunk, s, b->flags,
-                                                                      b->pool_slots);
-    CKL2();
-    CKR2(scan_excl(b, b->flags, b->pos, b->pool_slots, b->scan_tmp, b->scan_len));
-    compact2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], b->pool[nb], runs_of<real>(b),
-                                                                         b->st, b->part_items, b->n_part, kChunk, s,
-                                                                         b->pos, b->flags);
-    CKL2();
-    compact2d_count_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(runs_of<real>(b), b->st, b->nruns, s,
-                                                                                b->pos, b->flags);
+    layout_count2d_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(R, b->st, b->nruns, s, b->goff[s]);
     CKL2();
   }
   b->cur = nb;
@@ -1202,20 +1311,40 @@ template <typename real>
 int push(pic2d_batch* b) {
   const Run<real>* R = runs_of<real>(b);
   real* F = (real*)b->field;
-  switch (b->push_block) {
-    case 128:
-      push2d_kernel<real, 128><<<b->push_blocks, 128, 0, b->stream>>>(b->pool[b->cur], F, R, b->st, b->part_items,
-                                                                       b->n_part, kChunk, b->err);
+  Layout2 L{{b->goff[0], b->goff[1]}, {b->gmax[0], b->gmax[1]}};
+  const Pools P = b->pool[b->cur];
+  switch (b->tile_x) {
+    case 1:
+      push2d_tiled_kernel<real, 1><<<b->push_blocks, 32, 0, b->stream>>>(P, F, R, L, b->ptile_items, b->n_ptile, b->err);
       break;
-    case 512:
-      push2d_kernel<real, 512><<<b->push_blocks, 512, 0, b->stream>>>(b->pool[b->cur], F, R, b->st, b->part_items,
-                                                                       b->n_part, kChunk, b->err);
+    case 2:
+      push2d_tiled_kernel<real, 2><<<b->push_blocks, 64, 0, b->stream>>>(P, F, R, L, b->ptile_items, b->n_ptile, b->err);
+      break;
+    case 8:
+      push2d_tiled_kernel<real, 8><<<b->push_blocks, 256, 0, b->stream>>>(P, F, R, L, b->ptile_items, b->n_ptile, b->err);
       break;
     default:
-      push2d_kernel<real, 256><<<b->push_blocks, 256, 0, b->stream>>>(b->pool[b->cur], F, R, b->st, b->part_items,
-                                                                       b->n_part, kChunk, b->err);
+      push2d_tiled_kernel<real, 4><<<b->push_blocks, 128, 0, b->stream>>>(P, F, R, L, b->ptile_items, b->n_ptile, b->err);
   }
   CKL2();
+  return PIC_OK;
+}
+
+// The push's work list for tiles of tx group rows: per run and species, the
+// tiles in row-major order (consecutive items share the run's fields in L2).
+int set_tiles(pic2d_batch* b, int tx) {
+  std::vector<Item> v;
+  for (int r = 0; r < b->nruns; ++r) {
+    const int nx = b->cfg[r].nx, nzb = (b->cfg[r].nz + 31) / 32, tn = (nx + tx - 1) / tx;
+    for (int s = 0; s < 2; ++s)
+      for (int t = 0; t < tn * nzb; ++t) v.push_back({2 * r + s, t});
+  }
+  cudaFree(b->ptile_items);
+  b->ptile_items = nullptr;
+  b->n_ptile = (int)v.size();
+  CK2(cudaMalloc(&b->ptile_items, sizeof(Item) * std::max<size_t>(v.size(), 1)));
+  CK2(cudaMemcpy(b->ptile_items, v.data(), sizeof(Item) * v.size(), cudaMemcpyHostToDevice));
+  b->tile_x = tx;
   return PIC_OK;
 }
 
@@ -1237,8 +1366,8 @@ int step_body(pic2d_batch* b, bool refill, bool sort = false) {
     delete5_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], R, b->st, b->part_items,
                                                                         b->n_part, kChunk);
     CKL2();
-    CKR2(cellsort<real>(b));  // drops the deleted slots as a compaction would
-    CKR2(run_sources<real>(b, 1));
+    CKR2(run_sources<real>(b, 1));  // appended after the layout
+    CKR2(cellsort<real>(b));        // everything into a new layout, the deleted slots dropped
   } else if (sort) {
     CKR2(cellsort<real>(b));
   }
@@ -1383,6 +1512,7 @@ int do_create(pic2d_batch* b) {
   b->runs_host.assign(sizeof(Run<real>) * n, 0);
   Run<real>* H = runs_host<real>(b);
   long long foff = 0, poff = 0, roff = 0;
+  int ngroups = 0;
   std::vector<int> sine_sizes;
   std::vector<std::pair<int, long long>> sine_off;  // size -> offset
   std::vector<double> sines;
@@ -1403,9 +1533,18 @@ int do_create(pic2d_batch* b) {
     R.foff = foff;
     foff += (long long)P_COUNT * R.nodes;
     foff = (foff + 63) & ~63LL;
-    const long long load = (long long)k.np * k.np * k.nx * k.nz + 1;
     const long long refill = 2LL * k.np * k.nx * k.np + 2LL * (k.np * (long long)k.nz - 2) * k.np;
-    R.cap = k.capacity > 0 ? k.capacity : (long long)(load * 1.25) + 2 * refill + 4096;
+    R.nzb = (k.nz + 31) / 32;
+    R.ngroups = k.nx * R.nzb;
+    R.gbase = ngroups;
+    ngroups += R.ngroups;
+    // the tiled layout takes 32 slots per group row, as many rows as the
+    // group's fullest cell: with m = Np^2 particles per cell on average (about
+    // Poisson-distributed), room for 1.25 m + 4 sqrt(m) + 4 in every lane,
+    // then a refill appended before the next sort
+    const double m = (double)k.np * k.np;
+    const long long layout = 32LL * R.ngroups * (long long)std::ceil(1.25 * m + 4 * std::sqrt(m) + 4);
+    R.cap = k.capacity > 0 ? k.capacity : layout + 2 * refill + 4096;
     R.cap = (R.cap + kChunk - 1) / kChunk * kChunk;
     R.poff = poff;
     poff += R.cap;
@@ -1442,6 +1581,23 @@ int do_create(pic2d_batch* b) {
   b->field_nodes = foff;
   b->pool_slots = poff;
   b->rho_len = roff;
+  b->ngroups = ngroups;
+  if (poff >= (1LL << 31) - kChunk) return PIC_ERR_CAPACITY;  // slot offsets are 32-bit
+  {
+    std::vector<int> grun(ngroups);
+    for (int r = 0; r < n; ++r)
+      for (int q = 0; q < H[r].ngroups; ++q) grun[H[r].gbase + q] = r;
+    CK2(cudaMalloc(&b->grun, sizeof(int) * std::max(ngroups, 1)));
+    CK2(cudaMemcpy(b->grun, grun.data(), sizeof(int) * ngroups, cudaMemcpyHostToDevice));
+    CK2(cudaMalloc(&b->gsz, sizeof(int) * (ngroups + 1)));
+    CK2(cudaMemset(b->gsz, 0, sizeof(int) * (ngroups + 1)));
+    for (int s = 0; s < 2; ++s) {
+      CK2(cudaMalloc(&b->goff[s], sizeof(int) * (ngroups + 1)));
+      CK2(cudaMemset(b->goff[s], 0, sizeof(int) * (ngroups + 1)));
+      CK2(cudaMalloc(&b->gmax[s], sizeof(int) * std::max(ngroups, 1)));
+      CK2(cudaMemset(b->gmax[s], 0, sizeof(int) * std::max(ngroups, 1)));
+    }
+  }
   CK2(cudaMalloc(&b->runs_dev, sizeof(Run<real>) * n));
   CK2(cudaMemcpy(b->runs_dev, H, sizeof(Run<real>) * n, cudaMemcpyHostToDevice));
   CK2(cudaMalloc(&b->st, sizeof(State) * n));
@@ -1495,13 +1651,13 @@ int do_create(pic2d_batch* b) {
   b->scan_len = (size_t)(2 * ((poff + kScanTile - 1) / kScanTile) + 64);
   CK2(cudaMalloc(&b->scan_tmp, sizeof(int) * b->scan_len));
   CK2(cudaMalloc(&b->ccnt, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
-  CK2(cudaMalloc(&b->coffs, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
   CK2(cudaMalloc(&b->ccur, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
   CK2(cudaMalloc(&b->step_dev, sizeof(int)));
   CK2(cudaMemset(b->step_dev, 0, sizeof(int)));
   CK2(cudaMalloc(&b->err, sizeof(unsigned long long) * ERR_COUNT));
   CK2(cudaMemset(b->err, 0, sizeof(unsigned long long) * ERR_COUNT));
-  b->push_blocks = persistent(b->n_part, 8);
+  CKR2(set_tiles(b, 4));
+  b->push_blocks = persistent(b->n_ptile, 8);
   return PIC_OK;
 }
 
@@ -1519,7 +1675,9 @@ void free_batch(pic2d_batch* b) {
   for (int w = 0; w < 2; ++w)
     for (int s = 0; s < 2; ++s) { cudaFree(b->src_items[w][s]); cudaFree(b->sets[w][s]); }
   cudaFree(b->flags); cudaFree(b->pos); cudaFree(b->scan_tmp); cudaFree(b->step_dev); cudaFree(b->err);
-  cudaFree(b->ccnt); cudaFree(b->coffs); cudaFree(b->ccur);
+  cudaFree(b->ccnt); cudaFree(b->ccur);
+  cudaFree(b->grun); cudaFree(b->gsz); cudaFree(b->ptile_items);
+  for (int s = 0; s < 2; ++s) { cudaFree(b->goff[s]); cudaFree(b->gmax[s]); }
   if (b->stream) cudaStreamDestroy(b->stream);
 }
 
@@ -1599,23 +1757,26 @@ int do_thrust(pic2d_batch* b, double* out) {
   return PIC_OK;
 }
 
-// Online tuning: the next steps of the run itself try each push launch shape
-// (block size x persistent blocks per SM), timing whole loop bodies, and the
-// fastest shape is kept; the steps taken are ordinary steps of the run.
+// Online tuning: the next steps of the run itself try each push tile shape
+// (1, 2, 4 or 8 group rows of 32 cells, one warp per row) with 8 or 16
+// resident blocks' worth of persistent blocks per SM, timing whole loop
+// bodies, and the fastest is kept; the steps taken are ordinary steps of the
+// run.
 template <typename real>
 int do_autotune(pic2d_batch* b, int* choice) {
-  const int blocks[3] = {128, 256, 512};
-  const int per_sm[3] = {2, 4, 8};  // resident blocks of 256 threads per SM
+  const int shapes[4] = {1, 2, 4, 8};
+  const int per_sm[2] = {8, 16};
   float best = 1e30f;
-  int bb = b->push_block, bs = b->push_blocks;
+  int bt = b->tile_x, bs = b->push_blocks;
   cudaEvent_t e0, e1;
   CK2(cudaEventCreate(&e0));
   CK2(cudaEventCreate(&e1));
   int rc = PIC_OK;
-  for (int i = 0; i < 3 && rc == PIC_OK; ++i)
-    for (int j = 0; j < 3 && rc == PIC_OK; ++j) {
-      b->push_block = blocks[i];
-      b->push_blocks = persistent(b->n_part, per_sm[j] * 256 / blocks[i]);
+  for (int i = 0; i < 4 && rc == PIC_OK; ++i)
+    for (int j = 0; j < 2 && rc == PIC_OK; ++j) {
+      rc = set_tiles(b, shapes[i]);
+      if (rc != PIC_OK) break;
+      b->push_blocks = persistent(b->n_ptile, per_sm[j]);
       const bool g = b->use_graph;
       b->use_graph = false;
       cudaEventRecord(e0, b->stream);
@@ -1627,17 +1788,17 @@ int do_autotune(pic2d_batch* b, int* choice) {
       cudaEventElapsedTime(&ms, e0, e1);
       if (rc == PIC_OK && ms < best) {
         best = ms;
-        bb = blocks[i];
+        bt = shapes[i];
         bs = b->push_blocks;
       }
     }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  b->push_block = bb;
+  if (rc == PIC_OK) rc = set_tiles(b, bt);
   b->push_blocks = bs;
   drop_graphs(b);
   if (choice) {
-    choice[0] = bb;
+    choice[0] = bt;
     choice[1] = bs;
   }
   return rc;
@@ -1736,6 +1897,14 @@ int pic2d_get_grid(pic2d_batch* b, int run, double* records) {
   return (b->prec == 64 ? do_get_grid<double> : do_get_grid<float>)(b, run, records);
 }
 
+int pic2d_set_push_shape(pic2d_batch* b, int tile_rows, int blocks) {
+  if (!b || (tile_rows != 1 && tile_rows != 2 && tile_rows != 4 && tile_rows != 8) || blocks < 1) return PIC_ERR_ARG;
+  CKR2(set_tiles(b, tile_rows));
+  b->push_blocks = blocks;
+  drop_graphs(b);
+  return PIC_OK;
+}
+
 int pic2d_autotune(pic2d_batch* b, int* choice2) {
   if (!b) return PIC_ERR_ARG;
   if (!b->ready) return PIC_ERR_STATE;
@@ -1751,12 +1920,16 @@ int pic2d_set_graph(pic2d_batch* b, int enable) {
 
 int pic2d_status(pic2d_batch* b, long long* counters8) {
   if (!b || !counters8) return PIC_ERR_ARG;
+  // read on the batch's stream, after the work queued before this call (the
+  // stream does not synchronise with the legacy default stream)
   unsigned long long h[ERR_COUNT];
-  if (cudaMemcpy(h, b->err, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return PIC_ERR_CUDA;
+  if (cudaMemcpyAsync(h, b->err, sizeof(h), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess ||
+      cudaStreamSynchronize(b->stream) != cudaSuccess)
+    return PIC_ERR_CUDA;
   for (int q = 0; q < 8; ++q) counters8[q] = (long long)h[q];
   counters8[4] = b->step;
   counters8[5] = b->launches;
-  return (h[0] | h[1] | h[2]) ? PIC_ERR_DEVICE : PIC_OK;
+  return (h[0] | h[1] | h[2] | h[ERR_STORE_FULL]) ? PIC_ERR_DEVICE : PIC_OK;
 }
 
 int pic2d_get_stream(pic2d_batch* b, void** stream) {

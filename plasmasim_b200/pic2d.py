@@ -88,6 +88,7 @@ def _bind(L):
     L.pic2d_get_grid.argtypes = [vp, C.c_int, _dp]
     L.pic2d_autotune.argtypes = [vp, _ip]
     L.pic2d_set_graph.argtypes = [vp, C.c_int]
+    L.pic2d_set_push_shape.argtypes = [vp, C.c_int, C.c_int]
     L.pic2d_status.argtypes = [vp, _llp]
     L.pic2d_get_stream.argtypes = [vp, C.POINTER(vp)]
     _bound = True
@@ -160,6 +161,9 @@ class Pic2DBatch:
         out = np.zeros(2, dtype=np.int32)
         self._check(self.L.pic2d_autotune(self.h, out.ctypes.data_as(_ip)), "pic2d_autotune")
         return int(out[0]), int(out[1])
+
+    def set_push_shape(self, tile_rows: int, blocks: int):
+        self._check(self.L.pic2d_set_push_shape(self.h, tile_rows, blocks), "pic2d_set_push_shape")
 
     def set_graph(self, enable: bool):
         self._check(self.L.pic2d_set_graph(self.h, int(enable)), "pic2d_set_graph")

@@ -149,7 +149,7 @@ EXPORTED = [
     "pic_nccl_unique_id", "pic_nccl_transport_create", "pic_nccl_transport_destroy",
     "pic2d_config_normalized", "pic2d_create", "pic2d_destroy", "pic2d_init", "pic2d_step",
     "pic2d_thrust", "pic2d_particle_count", "pic2d_get_particles", "pic2d_get_grid",
-    "pic2d_autotune", "pic2d_set_graph", "pic2d_status", "pic2d_get_stream",
+    "pic2d_autotune", "pic2d_set_push_shape", "pic2d_set_graph", "pic2d_status", "pic2d_get_stream",
 ]
 
 PHASES = ["push", "field", "sort", "add", "diag"]

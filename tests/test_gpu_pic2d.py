@@ -145,8 +145,87 @@ def test_graph_and_direct_steps_agree():
 def test_autotune_keeps_the_run_on_the_reference():
     with Pic2DBatch([cfg_from("strip", 5)], precision=64) as B:
         B.init()
-        block, blocks = B.autotune()  # nine shapes x two steps of the run itself
-        assert block in (128, 256, 512) and blocks >= 1
+        tiles, blocks = B.autotune()  # eight shapes x two steps of the run itself
+        assert tiles in (1, 2, 4, 8) and blocks >= 1
         B.step(2)
-        R = reference("strip", 20, 5)
+        steps = int(B.status()[1][4])
+        assert steps == 18
+        R = reference("strip", steps, 5)
         compare(B, 0, R, 64, "after tuning")
+
+
+def test_half_tile_geometry_with_frequent_sorts():
+    """32 x 16 cells: every z tile of the push has 16 of its 32 lanes.
+    Sorting every 3 steps and refilling every 5 re-lays the particles four
+    times in 12 steps."""
+    R = reference("half", 12, 5)
+    cfg = cfg_from("half", 5)
+    cfg.sort_interval = 3
+    with Pic2DBatch([cfg], precision=64) as B:
+        B.init()
+        B.step(12)
+        compare(B, 0, R, 64, "half tile 12 steps")
+        assert B.status()[0] == 0
+
+
+def ragged_cfg(nx, nz, np_, seed):
+    cfg = cfg_from("rect", 5)
+    cfg.nx, cfg.nz, cfg.np = nx, nz, np_
+    cfg.seed_p, cfg.seed_v = seed, seed + 50
+    cfg.sort_interval = 3
+    return cfg
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_tile_shapes_agree(prec):
+    """Sides that no tile divides (22 x 70 and 37 x 45 cells; the reference's
+    sine transform cannot take them, so the check is against the engine with
+    one-row tiles): every tile shape gives the same run, to the rounding of
+    the deposit sums, through sorts, refills and particles leaving their
+    tiles."""
+    cfgs = [ragged_cfg(22, 70, 3, 11), ragged_cfg(37, 45, 4, 23)]
+    out = {}
+    for rows in (1, 4, 8):
+        with Pic2DBatch(cfgs, precision=prec) as B:
+            B.init()
+            B.set_push_shape(rows, 148 * 4)
+            B.step(11)
+            assert B.status()[0] == 0
+            out[rows] = ([[B.particles(r, s) for s in (0, 1)] for r in range(2)], [B.grid(r) for r in range(2)])
+    ptol, gtol = (1e-12, 1e-10) if prec == 64 else (1e-4, 1e-3)
+    for rows in (4, 8):
+        for r in range(2):
+            for s in (0, 1):
+                check_particles(out[rows][0][r][s], out[1][0][r][s], ptol, f"{rows} rows run {r} species {s}")
+            check_grid(out[rows][1][r], out[1][1][r], gtol, f"{rows} rows run {r}", loose=("phi",) if prec == 32 else ())
+
+
+def test_sort_interval_changes_only_the_order():
+    """The same run sorted every step and only at refills: the particle sets
+    agree to the rounding of the deposit sums (FP64)."""
+    out = []
+    for every in (1, 0):
+        cfg = cfg_from("rect", 5)
+        cfg.sort_interval = every
+        with Pic2DBatch([cfg], precision=64) as B:
+            B.init()
+            B.step(8)
+            out.append([B.particles(0, s) for s in (0, 1)])
+            assert B.status()[0] == 0
+    for s in (0, 1):
+        check_particles(out[0][s], out[1][s], 1e-12, f"sort every step vs at refills, species {s}")
+
+
+def test_layout_overflow_is_reported():
+    """A capacity that holds the initial load but not its tiled layout: the
+    particles the layout cannot place are counted (counter 6) and the status
+    is an error, with nothing written past the run's slots."""
+    cfg = cfg_from("sq64")
+    load = cfg.np * cfg.np * cfg.nx * cfg.nz + 1
+    cfg.capacity = load + 64
+    with Pic2DBatch([cfg, cfg_from("strip")], precision=32) as B:
+        B.init()
+        rc, counters = B.status()
+        assert rc != 0 and counters[6] > 0
+        # the neighbouring run's slots are intact
+        assert B.count(1, 0) == cfg_from("strip").np ** 2 * 16 * 32 + 1
