@@ -125,9 +125,11 @@ __device__ __forceinline__ double ramp2(int idx, int n, int absorb) {
   return 0.;
 }
 
-// init_grid's damping profile (:252-276) on the doubled grid.
+// init_grid's damping profile (:252-276) on the doubled grid; zero, without
+// the powers, away from the damping layers (most nodes).
 __device__ __forceinline__ double sigma2(double a, int kk, int mm, int nx, int nz, int absorb) {
   const double x = ramp2(kk, nx, absorb), z = ramp2(mm, nz, absorb);
+  if (x == 0. && z == 0.) return 0.;
   return a * (0.1 * sqrt(pow(x, 4) + pow(z, 4)) + 0.01 * sqrt(pow(x, 12) + pow(z, 12)));
 }
 
@@ -143,12 +145,22 @@ struct Item {
 };
 
 // ------------------------------------------------------------ grid
-// renew_b4 (:1391-1417) on the interior of every run; item = (run, row k).
+// Rows of one item of the field updates: a block of 256 threads takes
+// kFieldRows rows of a run, so that a thread updates several nodes per item.
+constexpr int kFieldRows = 4;
+
+// renew_b4 (:1391-1417) on the interior of every run; item = (run, first row
+// k0) for rows k0 .. k0 + kFieldRows - 1. Away from the damping layers s = 0,
+// where the two factors are exactly 1 and dt / 2 and are taken without their
+// divisions.
 template <typename real>
-__global__ void renew_b4_kernel(real* F, const Run<real>* __restrict__ runs, const Item* __restrict__ items, int nitems) {
+__global__ void __launch_bounds__(256) renew_b4_kernel(real* F, const Run<real>* __restrict__ runs,
+                                                       const Item* __restrict__ items, int nitems) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const Run<real> R = runs[items[it].run];
-    const int k = items[it].first;
+    const Run<real>& R = runs[items[it].run];
+    const int k0 = items[it].first;
+    const int nx = R.nx, nz = R.nz, G = R.gz, a1 = R.a1;
+    const double dt = R.dt, dx = R.dx, sa = R.sigma_a;
     const real* ex = plane(F, R, P_EX);
     const real* ey = plane(F, R, P_EY);
     const real* ez = plane(F, R, P_EZ);
@@ -158,33 +170,39 @@ __global__ void renew_b4_kernel(real* F, const Run<real>* __restrict__ runs, con
     const real* b0x = plane(F, R, P_B0X);
     const real* b0y = plane(F, R, P_B0Y);
     const real* b0z = plane(F, R, P_B0Z);
-    const int G = R.gz;
-    const double t = 1. / R.e0 * R.dt * 0.5 * 0.5;
-    for (int m = 2 + threadIdx.x; m < R.nz + 2; m += blockDim.x) {
+    const double t = 1. / R.e0 * dt * 0.5 * 0.5;
+    // (1 - s t) / (1 + s t) and dt / 2 / (1 + s t)
+    auto ca = [&](double s) { return s == 0. ? 1. : (1. - s * t) / (1. + s * t); };
+    auto cb = [&](double s) { return s == 0. ? 0.5 * dt : 0.5 * dt / (1. + s * t); };
+    for (int q = threadIdx.x; q < kFieldRows * nz; q += blockDim.x) {
+      const int k = k0 + q / nz, m = 2 + q % nz;
+      if (k >= nx + 2) break;
       const int n = k * G + m;
-      double s = sigma2(R.sigma_a, 2 * k + 1, 2 * m, R.nx, R.nz, R.a1);
-      bx[n] = (real)((double)b0x[n] + (1. - s * t) / (1. + s * t) * ((double)bx[n] - (double)b0x[n]) +
-                     0.5 * R.dt / (1. + s * t) * (1. / 24.) *
-                         (27. * ((double)ey[n] - (double)ey[n - 1]) - ((double)ey[n + 1] - (double)ey[n - 2])) / R.dx);
-      s = sigma2(R.sigma_a, 2 * k, 2 * m, R.nx, R.nz, R.a1);
-      by[n] = (real)((double)b0y[n] + (1. - s * t) / (1. + s * t) * ((double)by[n] - (double)b0y[n]) -
-                     R.dt * 0.5 / (1. + s * t) *
-                         ((1. / 24.) * (27. * ((double)ex[n] - (double)ex[n - 1]) - ((double)ex[n + 1] - (double)ex[n - 2])) / R.dx -
-                          (1. / 24.) * (27. * ((double)ez[n] - (double)ez[n - G]) - ((double)ez[n + G] - (double)ez[n - 2 * G])) / R.dx));
-      s = sigma2(R.sigma_a, 2 * k, 2 * m + 1, R.nx, R.nz, R.a1);
-      bz[n] = (real)((double)b0z[n] + (1. - s * t) / (1. + s * t) * ((double)bz[n] - (double)b0z[n]) -
-                     R.dt * 0.5 / (1. + s * t) * (1. / 24.) *
-                         (27. * ((double)ey[n] - (double)ey[n - G]) - ((double)ey[n + G] - (double)ey[n - 2 * G])) / R.dx);
+      double s = sigma2(sa, 2 * k + 1, 2 * m, nx, nz, a1);
+      bx[n] = (real)((double)b0x[n] + ca(s) * ((double)bx[n] - (double)b0x[n]) +
+                     cb(s) * (1. / 24.) * (27. * ((double)ey[n] - (double)ey[n - 1]) - ((double)ey[n + 1] - (double)ey[n - 2])) /
+                         dx);
+      s = sigma2(sa, 2 * k, 2 * m, nx, nz, a1);
+      by[n] = (real)((double)b0y[n] + ca(s) * ((double)by[n] - (double)b0y[n]) -
+                     cb(s) * ((1. / 24.) * (27. * ((double)ex[n] - (double)ex[n - 1]) - ((double)ex[n + 1] - (double)ex[n - 2])) / dx -
+                              (1. / 24.) * (27. * ((double)ez[n] - (double)ez[n - G]) - ((double)ez[n + G] - (double)ez[n - 2 * G])) / dx));
+      s = sigma2(sa, 2 * k, 2 * m + 1, nx, nz, a1);
+      bz[n] = (real)((double)b0z[n] + ca(s) * ((double)bz[n] - (double)b0z[n]) -
+                     cb(s) * (1. / 24.) *
+                         (27. * ((double)ey[n] - (double)ey[n - G]) - ((double)ey[n + G] - (double)ey[n - 2 * G])) / dx);
     }
   }
 }
 
-// renew_e4 (:1419-1449); item = (run, row k).
+// renew_e4 (:1419-1449); items as renew_b4_kernel's; s = 0 as there.
 template <typename real>
-__global__ void renew_e4_kernel(real* F, const Run<real>* __restrict__ runs, const Item* __restrict__ items, int nitems) {
+__global__ void __launch_bounds__(256) renew_e4_kernel(real* F, const Run<real>* __restrict__ runs,
+                                                       const Item* __restrict__ items, int nitems) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const Run<real> R = runs[items[it].run];
-    const int k = items[it].first;
+    const Run<real>& R = runs[items[it].run];
+    const int k0 = items[it].first;
+    const int nx = R.nx, nz = R.nz, G = R.gz, a1 = R.a1;
+    const double dx = R.dx, sa = R.sigma_a, mu0 = R.mu0;
     real* ex = plane(F, R, P_EX);
     real* ey = plane(F, R, P_EY);
     real* ez = plane(F, R, P_EZ);
@@ -200,32 +218,33 @@ __global__ void renew_e4_kernel(real* F, const Run<real>* __restrict__ runs, con
     const real* jex = plane(F, R, P_JEX);
     const real* jey = plane(F, R, P_JEY);
     const real* jez = plane(F, R, P_JEZ);
-    const int G = R.gz;
     const double cc = R.c * R.c * R.dt;
     auto dby = [&](int n) { return (double)by[n] - (double)b0y[n]; };
     auto dbx = [&](int n) { return (double)bx[n] - (double)b0x[n]; };
     auto dbz = [&](int n) { return (double)bz[n] - (double)b0z[n]; };
-    for (int m = 2 + threadIdx.x; m < R.nz + 2; m += blockDim.x) {
+    // h = mu0 s cc / 2: (1 - h) / (1 + h) and cc / (1 + h)
+    auto ca = [&](double s) {
+      const double h = 0.5 * mu0 * s * cc;
+      return s == 0. ? 1. : (1. - h) / (1. + h);
+    };
+    auto cb = [&](double s) { return s == 0. ? cc : cc / (1. + 0.5 * mu0 * s * cc); };
+    for (int q = threadIdx.x; q < kFieldRows * nz; q += blockDim.x) {
+      const int k = k0 + q / nz, m = 2 + q % nz;
+      if (k >= nx + 2) break;
       const int n = k * G + m;
-      double s = sigma2(R.sigma_a, 2 * k, 2 * m + 1, R.nx, R.nz, R.a1);
-      double h = 0.5 * R.mu0 * s * cc;
-      ex[n] = (real)((1. - h) / (1. + h) * (double)ex[n] +
-                     cc / (1. + h) *
-                         (-1. / 24. * (27. * (dby(n + 1) - dby(n)) - (dby(n + 2) - dby(n - 1))) / R.dx -
-                          R.mu0 * ((double)jix[n] - (double)jex[n])));
-      s = sigma2(R.sigma_a, 2 * k + 1, 2 * m, R.nx, R.nz, R.a1);
-      h = 0.5 * R.mu0 * s * cc;
-      ez[n] = (real)((1. - h) / (1. + h) * (double)ez[n] +
-                     cc / (1. + h) *
-                         (1. / 24. * (27. * (dby(n + G) - dby(n)) - (dby(n + 2 * G) - dby(n - G))) / R.dx -
-                          R.mu0 * ((double)jiz[n] - (double)jez[n])));
-      s = sigma2(R.sigma_a, 2 * k + 1, 2 * m + 1, R.nx, R.nz, R.a1);
-      h = 0.5 * R.mu0 * s * cc;
-      ey[n] = (real)((1. - h) / (1. + h) * (double)ey[n] +
-                     cc / (1. + h) *
-                         (1. / 24. * (27. * (dbx(n + 1) - dbx(n)) - (dbx(n + 2) - dbx(n - 1))) / R.dx -
-                          1. / 24. * (27. * (dbz(n + G) - dbz(n)) - (dbz(n + 2 * G) - dbz(n - G))) / R.dx -
-                          R.mu0 * ((double)jiy[n] - (double)jey[n])));
+      double s = sigma2(sa, 2 * k, 2 * m + 1, nx, nz, a1);
+      ex[n] = (real)(ca(s) * (double)ex[n] +
+                     cb(s) * (-1. / 24. * (27. * (dby(n + 1) - dby(n)) - (dby(n + 2) - dby(n - 1))) / dx -
+                              mu0 * ((double)jix[n] - (double)jex[n])));
+      s = sigma2(sa, 2 * k + 1, 2 * m, nx, nz, a1);
+      ez[n] = (real)(ca(s) * (double)ez[n] +
+                     cb(s) * (1. / 24. * (27. * (dby(n + G) - dby(n)) - (dby(n + 2 * G) - dby(n - G))) / dx -
+                              mu0 * ((double)jiz[n] - (double)jez[n])));
+      s = sigma2(sa, 2 * k + 1, 2 * m + 1, nx, nz, a1);
+      ey[n] = (real)(ca(s) * (double)ey[n] +
+                     cb(s) * (1. / 24. * (27. * (dbx(n + 1) - dbx(n)) - (dbx(n + 2) - dbx(n - 1))) / dx -
+                              1. / 24. * (27. * (dbz(n + G) - dbz(n)) - (dbz(n + 2 * G) - dbz(n - G))) / dx -
+                              mu0 * ((double)jiy[n] - (double)jey[n])));
     }
   }
 }
@@ -522,8 +541,11 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
             }
             ex += ex_add;
             ey += ey_add;
-            // cal_track_c4 (:1520-1560)
-            const real S = (real)2 * T / ((real)1 + T * T * (bx * bx + by * by + bz * bz));
+            // cal_track_c4 (:1520-1560); FP32 divides with __fdividef
+            const real den = (real)1 + T * T * (bx * bx + by * by + bz * bz);
+            real S;
+            if constexpr (sizeof(real) == 4) S = __fdividef(2.f * T, den);
+            else S = (real)2 * T / den;
             const real ux = vx + ex * T, uy = vy + ey * T, uz = vz + ez * T;
             const real uox = ux + T * (uy * bz - uz * by);
             const real uoy = uy + T * (uz * bx - ux * bz);
@@ -990,7 +1012,7 @@ struct pic2d_batch {
   void* rho2 = nullptr;
   long long rho_len = 0;
   // work lists
-  Item* row_items = nullptr;   int n_row = 0;    // (run, interior row k)
+  Item* row_items = nullptr;   int n_row = 0;    // (run, first of kFieldRows interior rows)
   Item* rho_items = nullptr;   int n_rhorow = 0; // (run, rho row 0..nx-1)
   Item* part_items = nullptr;  int n_part = 0;   // (run*2+s, first slot) over [0, cap)
   Item* tile_items = nullptr;  int n_tile = 0;   // (run, 32x32 tile of nx x nz)
@@ -1371,7 +1393,7 @@ int step_body(pic2d_batch* b, bool refill, bool sort = false) {
   } else if (sort) {
     CKR2(cellsort<real>(b));
   }
-  renew_b4_kernel<real><<<persistent(b->n_row), 128, 0, b->stream>>>(F, R, b->row_items, b->n_row);
+  renew_b4_kernel<real><<<persistent(b->n_row), 256, 0, b->stream>>>(F, R, b->row_items, b->n_row);
   CKL2();
   CKR2(sr_grid<real>(b));
   CKR2(push<real>(b));
@@ -1381,10 +1403,10 @@ int step_body(pic2d_batch* b, bool refill, bool sort = false) {
   CKL2();
   coil_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(F, R, b->nruns, b->step_dev);
   CKL2();
-  renew_b4_kernel<real><<<persistent(b->n_row), 128, 0, b->stream>>>(F, R, b->row_items, b->n_row);
+  renew_b4_kernel<real><<<persistent(b->n_row), 256, 0, b->stream>>>(F, R, b->row_items, b->n_row);
   CKL2();
   CKR2(sr_grid<real>(b));
-  renew_e4_kernel<real><<<persistent(b->n_row), 128, 0, b->stream>>>(F, R, b->row_items, b->n_row);
+  renew_e4_kernel<real><<<persistent(b->n_row), 256, 0, b->stream>>>(F, R, b->row_items, b->n_row);
   CKL2();
   CKR2(sr_grid<real>(b));
   CKR2(renew_phi<real>(b));
@@ -1617,7 +1639,7 @@ int do_create(pic2d_batch* b) {
   // work lists
   std::vector<Item> rows, rhos, parts, tiles;
   for (int r = 0; r < n; ++r) {
-    for (int k = 2; k < H[r].nx + 2; ++k) rows.push_back({r, k});
+    for (int k = 2; k < H[r].nx + 2; k += kFieldRows) rows.push_back({r, k});
     for (int k = 0; k < H[r].nx; ++k) rhos.push_back({r, k});
     for (int s = 0; s < 2; ++s)
       for (long long q = 0; q < H[r].cap; q += kChunk) parts.push_back({2 * r + s, (int)q});
