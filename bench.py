@@ -250,7 +250,7 @@ def run_e2e(P, steps: int):
 # from the ncu capture of a 64^3 x 64 ppc launch
 # (profiles/push_tiled_kernel_grid64_64ppc.md); at a fixed number of particles
 # per cell the traffic of a launch grows with its particles.
-PUSH_TRAFFIC_PER_PARTICLE = 73.1
+PUSH_TRAFFIC_PER_PARTICLE = 73.0
 
 
 def roofline(out, npart_species, cells, rsize):
@@ -320,6 +320,20 @@ def run_batch2d(nruns: int, steps: int, warmup: int):
                          "bytes": "particles x 48 (cell + 5 FP32 values, read and written)", "peak_kind": kind},
             "launch_shape": list(choice), "graph": True,
             "kernels_per_step": int(c1[5] - c0[5]) // max(steps, 1), "device_errors": [int(x) for x in c1[:3]]}
+
+
+def step_batch2d(nruns: int, steps: int, tile_rows: int = 2, blocks: int = 2368):
+    """The batched 2D workload stepped with a fixed push shape (no tuning, no
+    timing), for profiling the kernels of its steps."""
+    from plasmasim_b200 import Pic2DBatch
+
+    B = Pic2DBatch(batch2d_configs(nruns), precision=32)
+    B.init()
+    B.set_push_shape(tile_rows, blocks)
+    B.step(steps)
+    rc, counters = B.status()
+    B.close()
+    return rc, [int(x) for x in counters]
 
 
 def batch2d_cpu_sample(steps: int = 3):
