@@ -149,10 +149,17 @@ struct Item {
 // kFieldRows rows of a run, so that a thread updates several nodes per item.
 constexpr int kFieldRows = 4;
 
+// The 4th-order difference (27 (f[0] - f[-1]) - (f[1] - f[-2])) / 24 / dx with
+// the run's 1 / (24 dx), in the field's precision; d is the stride.
+template <typename real>
+__device__ __forceinline__ real d4(const real* f, int n, int d, real inv24dx) {
+  return ((real)27 * (f[n] - f[n - d]) - (f[n + d] - f[n - 2 * d])) * inv24dx;
+}
+
 // renew_b4 (:1391-1417) on the interior of every run; item = (run, first row
-// k0) for rows k0 .. k0 + kFieldRows - 1. Away from the damping layers s = 0,
-// where the two factors are exactly 1 and dt / 2 and are taken without their
-// divisions.
+// k0) for rows k0 .. k0 + kFieldRows - 1, in the field's precision. Away from
+// the damping layers s = 0, where the two factors are exactly 1 and dt / 2
+// and are taken without their divisions.
 template <typename real>
 __global__ void __launch_bounds__(256) renew_b4_kernel(real* F, const Run<real>* __restrict__ runs,
                                                        const Item* __restrict__ items, int nitems) {
@@ -160,7 +167,8 @@ __global__ void __launch_bounds__(256) renew_b4_kernel(real* F, const Run<real>*
     const Run<real>& R = runs[items[it].run];
     const int k0 = items[it].first;
     const int nx = R.nx, nz = R.nz, G = R.gz, a1 = R.a1;
-    const double dt = R.dt, dx = R.dx, sa = R.sigma_a;
+    const double sa = R.sigma_a;
+    const real inv24dx = (real)(1. / (24. * R.dx));
     const real* ex = plane(F, R, P_EX);
     const real* ey = plane(F, R, P_EY);
     const real* ez = plane(F, R, P_EZ);
@@ -170,31 +178,27 @@ __global__ void __launch_bounds__(256) renew_b4_kernel(real* F, const Run<real>*
     const real* b0x = plane(F, R, P_B0X);
     const real* b0y = plane(F, R, P_B0Y);
     const real* b0z = plane(F, R, P_B0Z);
-    const double t = 1. / R.e0 * dt * 0.5 * 0.5;
+    const double t = 1. / R.e0 * R.dt * 0.5 * 0.5;
+    const real hdt = (real)(0.5 * R.dt);
     // (1 - s t) / (1 + s t) and dt / 2 / (1 + s t)
-    auto ca = [&](double s) { return s == 0. ? 1. : (1. - s * t) / (1. + s * t); };
-    auto cb = [&](double s) { return s == 0. ? 0.5 * dt : 0.5 * dt / (1. + s * t); };
+    auto ca = [&](double s) { return s == 0. ? (real)1 : (real)((1. - s * t) / (1. + s * t)); };
+    auto cb = [&](double s) { return s == 0. ? hdt : (real)(0.5 * R.dt / (1. + s * t)); };
     for (int q = threadIdx.x; q < kFieldRows * nz; q += blockDim.x) {
       const int k = k0 + q / nz, m = 2 + q % nz;
       if (k >= nx + 2) break;
       const int n = k * G + m;
       double s = sigma2(sa, 2 * k + 1, 2 * m, nx, nz, a1);
-      bx[n] = (real)((double)b0x[n] + ca(s) * ((double)bx[n] - (double)b0x[n]) +
-                     cb(s) * (1. / 24.) * (27. * ((double)ey[n] - (double)ey[n - 1]) - ((double)ey[n + 1] - (double)ey[n - 2])) /
-                         dx);
+      bx[n] = b0x[n] + ca(s) * (bx[n] - b0x[n]) + cb(s) * d4(ey, n, 1, inv24dx);
       s = sigma2(sa, 2 * k, 2 * m, nx, nz, a1);
-      by[n] = (real)((double)b0y[n] + ca(s) * ((double)by[n] - (double)b0y[n]) -
-                     cb(s) * ((1. / 24.) * (27. * ((double)ex[n] - (double)ex[n - 1]) - ((double)ex[n + 1] - (double)ex[n - 2])) / dx -
-                              (1. / 24.) * (27. * ((double)ez[n] - (double)ez[n - G]) - ((double)ez[n + G] - (double)ez[n - 2 * G])) / dx));
+      by[n] = b0y[n] + ca(s) * (by[n] - b0y[n]) - cb(s) * (d4(ex, n, 1, inv24dx) - d4(ez, n, G, inv24dx));
       s = sigma2(sa, 2 * k, 2 * m + 1, nx, nz, a1);
-      bz[n] = (real)((double)b0z[n] + ca(s) * ((double)bz[n] - (double)b0z[n]) -
-                     cb(s) * (1. / 24.) *
-                         (27. * ((double)ey[n] - (double)ey[n - G]) - ((double)ey[n + G] - (double)ey[n - 2 * G])) / dx);
+      bz[n] = b0z[n] + ca(s) * (bz[n] - b0z[n]) - cb(s) * d4(ey, n, G, inv24dx);
     }
   }
 }
 
-// renew_e4 (:1419-1449); items as renew_b4_kernel's; s = 0 as there.
+// renew_e4 (:1419-1449); items and precision as renew_b4_kernel's; s = 0 as
+// there. dB = B - B0 on both sides of each difference.
 template <typename real>
 __global__ void __launch_bounds__(256) renew_e4_kernel(real* F, const Run<real>* __restrict__ runs,
                                                        const Item* __restrict__ items, int nitems) {
@@ -202,7 +206,9 @@ __global__ void __launch_bounds__(256) renew_e4_kernel(real* F, const Run<real>*
     const Run<real>& R = runs[items[it].run];
     const int k0 = items[it].first;
     const int nx = R.nx, nz = R.nz, G = R.gz, a1 = R.a1;
-    const double dx = R.dx, sa = R.sigma_a, mu0 = R.mu0;
+    const double sa = R.sigma_a, mu0 = R.mu0;
+    const real inv24dx = (real)(1. / (24. * R.dx));
+    const real rmu0 = (real)mu0;
     real* ex = plane(F, R, P_EX);
     real* ey = plane(F, R, P_EY);
     real* ez = plane(F, R, P_EZ);
@@ -219,32 +225,28 @@ __global__ void __launch_bounds__(256) renew_e4_kernel(real* F, const Run<real>*
     const real* jey = plane(F, R, P_JEY);
     const real* jez = plane(F, R, P_JEZ);
     const double cc = R.c * R.c * R.dt;
-    auto dby = [&](int n) { return (double)by[n] - (double)b0y[n]; };
-    auto dbx = [&](int n) { return (double)bx[n] - (double)b0x[n]; };
-    auto dbz = [&](int n) { return (double)bz[n] - (double)b0z[n]; };
+    const real rcc = (real)cc;
+    // the 4th-order difference of B - B0 at the half-shifted nodes n + d/2
+    auto db4 = [&](const real* b, const real* b0, int n, int d) {
+      auto v = [&](int o) { return b[n + o] - b0[n + o]; };
+      return ((real)27 * (v(d) - v(0)) - (v(2 * d) - v(-d))) * inv24dx;
+    };
     // h = mu0 s cc / 2: (1 - h) / (1 + h) and cc / (1 + h)
     auto ca = [&](double s) {
       const double h = 0.5 * mu0 * s * cc;
-      return s == 0. ? 1. : (1. - h) / (1. + h);
+      return s == 0. ? (real)1 : (real)((1. - h) / (1. + h));
     };
-    auto cb = [&](double s) { return s == 0. ? cc : cc / (1. + 0.5 * mu0 * s * cc); };
+    auto cb = [&](double s) { return s == 0. ? rcc : (real)(cc / (1. + 0.5 * mu0 * s * cc)); };
     for (int q = threadIdx.x; q < kFieldRows * nz; q += blockDim.x) {
       const int k = k0 + q / nz, m = 2 + q % nz;
       if (k >= nx + 2) break;
       const int n = k * G + m;
       double s = sigma2(sa, 2 * k, 2 * m + 1, nx, nz, a1);
-      ex[n] = (real)(ca(s) * (double)ex[n] +
-                     cb(s) * (-1. / 24. * (27. * (dby(n + 1) - dby(n)) - (dby(n + 2) - dby(n - 1))) / dx -
-                              mu0 * ((double)jix[n] - (double)jex[n])));
+      ex[n] = ca(s) * ex[n] + cb(s) * (-db4(by, b0y, n, 1) - rmu0 * (jix[n] - jex[n]));
       s = sigma2(sa, 2 * k + 1, 2 * m, nx, nz, a1);
-      ez[n] = (real)(ca(s) * (double)ez[n] +
-                     cb(s) * (1. / 24. * (27. * (dby(n + G) - dby(n)) - (dby(n + 2 * G) - dby(n - G))) / dx -
-                              mu0 * ((double)jiz[n] - (double)jez[n])));
+      ez[n] = ca(s) * ez[n] + cb(s) * (db4(by, b0y, n, G) - rmu0 * (jiz[n] - jez[n]));
       s = sigma2(sa, 2 * k + 1, 2 * m + 1, nx, nz, a1);
-      ey[n] = (real)(ca(s) * (double)ey[n] +
-                     cb(s) * (1. / 24. * (27. * (dbx(n + 1) - dbx(n)) - (dbx(n + 2) - dbx(n - 1))) / dx -
-                              1. / 24. * (27. * (dbz(n + G) - dbz(n)) - (dbz(n + 2 * G) - dbz(n - G))) / dx -
-                              mu0 * ((double)jiy[n] - (double)jey[n])));
+      ey[n] = ca(s) * ey[n] + cb(s) * (db4(bx, b0x, n, 1) - db4(bz, b0z, n, G) - rmu0 * (jiy[n] - jey[n]));
     }
   }
 }
@@ -418,11 +420,19 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
     push2d_tiled_kernel(Pools pools, real* F, const Run<real>* __restrict__ runs, Layout2 L,
                         const Item* __restrict__ items, int nitems, unsigned long long* err) {
   constexpr int WX = TX + 4, WZ = 36, WN = WX * WZ;
-  constexpr int kSt = sizeof(real) == 4 || PB_RING2D < 2 ? PB_RING2D : 2;  // FP64: static shared memory
+  // static shared memory: two stages in FP64 and with eight-row tiles
+  constexpr int kSt = (sizeof(real) == 4 && TX < 8) || PB_RING2D < 2 ? PB_RING2D : 2;
   __shared__ real fw[6 * WN];  // ex ey ez bx by bz
   // per warp and stage: the row's five reals and cells, lane-contiguous
   __shared__ real ring_r[TX][kSt][5][32];
   __shared__ int ring_c[TX][kSt][32];
+  // FP32: per warp, queues of the J (7 words: cell, offsets, q n v, a pad for
+  // the banks) and n (3 words: cell, offsets) deposits of particles off their
+  // lane's home cell, made 32 at a time by the whole warp
+  constexpr bool kQueue = sizeof(real) == 4;
+  constexpr int kQ = 64;
+  __shared__ float jq_s[kQueue ? TX : 1][kQueue ? kQ : 1][7];
+  __shared__ float nq_s[kQueue ? TX : 1][kQueue ? kQ : 1][3];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned pushed = 0;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -489,10 +499,26 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
       };
 #pragma unroll
       for (int q = 0; q < kSt - 1; ++q) fetch(q);
+      int njq = 0, nnq = 0;  // queue lengths (warp-uniform)
+      auto dep_j = [&](int q) {
+        const float* e = jq_s[kQueue ? warp : 0][q];
+        int qi, qk;
+        unpack2(__float_as_int(e[0]), qi, qk);
+        const Ax2<real> X = ax2(qi, (real)e[1]), Z = ax2(qk, (real)e[2]);
+        dep4(pj(0), G, X.a, Z.b, (real)e[3], X.a0, X.a1, Z.b0, Z.b1);
+        dep4(pj(1), G, X.b, Z.b, (real)e[4], X.b0, X.b1, Z.b0, Z.b1);
+        dep4(pj(2), G, X.b, Z.a, (real)e[5], X.b0, X.b1, Z.a0, Z.a1);
+      };
+      auto dep_n = [&](int q) {
+        const float* e = nq_s[kQueue ? warp : 0][q];
+        int qi, qk;
+        unpack2(__float_as_int(e[0]), qi, qk);
+        const Ax2<real> X = ax2(qi, (real)e[1]), Z = ax2(qk, (real)e[2]);
+        dep4(pj(3), G, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1);
+      };
       for (int row = 0; row < m; ++row) {
         fetch(row + kSt - 1);
         const long long t = base + 32LL * row;
-        if (t >= end) break;
         int c;
         real fx, fz, vx, vy, vz;
         if (kSt > 1) {
@@ -505,11 +531,17 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
           vy = ring_r[warp][st][3][lane];
           vz = ring_r[warp][st][4][lane];
         } else {
-          c = P.cell[t];
-          fx = P.ox[t]; fz = P.oz[t];
-          vx = P.vx[t]; vy = P.vy[t]; vz = P.vz[t];
+          c = t < end ? P.cell[t] : -1;
+          if (c >= 0) {
+            fx = P.ox[t]; fz = P.oz[t];
+            vx = P.vx[t]; vy = P.vy[t]; vz = P.vz[t];
+          }
         }
-        if (c < 0) continue;
+        if (t >= end) c = -1;  // rows of a layout that overflowed the run were not written
+        bool qj = false, qnn = false;  // J / n of this particle go to the warp's queues
+        int jc = 0, ncell = 0;
+        real jfx = 0, jfz = 0;
+        if (c >= 0) {
         ++pushed;
         int i, k;
         unpack2(c, i, k);
@@ -578,10 +610,17 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
             h.jz[b][1] += pz * Z.a1;
           }
         } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
-          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-          dep4(pj(0), G, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1);
-          dep4(pj(1), G, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1);
-          dep4(pj(2), G, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1);
+          if constexpr (kQueue) {
+            qj = true;
+            jc = pack2(i, k);
+            jfx = fx;
+            jfz = fz;
+          } else {
+            const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+            dep4(pj(0), G, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1);
+            dep4(pj(1), G, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1);
+            dep4(pj(2), G, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1);
+          }
         }
         advance(i, fx, vx * hdt);
         advance(k, fz, vz * hdt);
@@ -598,8 +637,13 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
             for (int cc = 0; cc < 3; ++cc) h.n[b][cc] += pn * zb[cc];
           }
         } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
-          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-          dep4(pj(3), G, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1);
+          if constexpr (kQueue) {
+            qnn = true;
+            ncell = pack2(i, k);
+          } else {
+            const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+            dep4(pj(3), G, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1);
+          }
         }
         // x exchange at size 1: forward crossers wrap, backward ones are dropped; then removal
         if (i == R.nx + 2 && k >= 2 && k < R.nz + 2) i -= R.nx;
@@ -607,6 +651,43 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
         P.cell[t] = keep ? pack2(i, k) : -1;
         P.ox[t] = fx; P.oz[t] = fz;
         P.vx[t] = vx; P.vy[t] = vy; P.vz[t] = vz;
+        }
+        if constexpr (kQueue) {
+          // warp-uniform: the row's queued lanes take consecutive entries, and
+          // a full warp's worth is deposited by all 32 lanes at once
+          const unsigned below = (1u << lane) - 1u;
+          const unsigned mj = __ballot_sync(0xffffffffu, qj), mn = __ballot_sync(0xffffffffu, qnn);
+          if (qj) {
+            float* e = jq_s[warp][njq + __popc(mj & below)];
+            e[0] = __int_as_float(jc);
+            e[1] = (float)jfx; e[2] = (float)jfz;
+            e[3] = (float)(qn * vx); e[4] = (float)(qn * vy); e[5] = (float)(qn * vz);
+          }
+          if (qnn) {
+            float* e = nq_s[warp][nnq + __popc(mn & below)];
+            e[0] = __int_as_float(ncell);
+            e[1] = (float)fx; e[2] = (float)fz;
+          }
+          njq += __popc(mj);
+          nnq += __popc(mn);
+          if (njq >= 32 || nnq >= 32) {
+            __syncwarp();
+            if (njq >= 32) {
+              dep_j(njq - 32 + lane);
+              njq -= 32;
+            }
+            if (nnq >= 32) {
+              dep_n(nnq - 32 + lane);
+              nnq -= 32;
+            }
+            __syncwarp();
+          }
+        }
+      }
+      if constexpr (kQueue) {
+        __syncwarp();
+        if (lane < njq) dep_j(lane);
+        if (lane < nnq) dep_n(lane);
       }
       if (kSt > 1) cp_async_wait2<0>();  // the next item refills the ring
       // the home sums into the planes (home cells are interior, so every

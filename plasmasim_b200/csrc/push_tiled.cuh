@@ -9,6 +9,7 @@ namespace pb {
 
 constexpr int kStages = 3;   // particle rows in flight per warp
 
+
 // The tile's interior cells: first cell (ci0, cj0, ck0) and extents (the
 // nominal tile clipped at the last interior cell, n + 1, of each axis).
 struct TileBox {
@@ -32,7 +33,14 @@ struct PushSmem {
   static constexpr size_t win_bytes = 4 * WN * sizeof(real);
   static constexpr size_t prec_off = (win_bytes + 15) & ~(size_t)15;  // records A, B of each slot: 8 reals
   static constexpr size_t fwin_off = prec_off + (size_t)kWarps * kStages * kLanes * 8 * sizeof(real);
-  static constexpr size_t bytes = fwin_off + (kFieldWin ? (size_t)6 * WN * sizeof(float) : 0);
+  // FP32: per warp a queue of kQ off-home J deposits, 7 words each (cell,
+  // offsets, velocities), made 32 at a time by the whole warp (1.7 % off the
+  // step against each particle depositing where it is found); FP64 has no
+  // room for it beside two CTAs per SM
+  static constexpr bool kJQueue = sizeof(real) == 4;
+  static constexpr int kQ = 2 * kLanes;
+  static constexpr size_t jq_off = fwin_off + (kFieldWin ? (size_t)6 * WN * sizeof(float) : 0);
+  static constexpr size_t bytes = jq_off + (kJQueue ? (size_t)kWarps * kQ * 7 * sizeof(float) : 0);
 };
 
 // Trilinear interpolation from a window plane with compile-time strides (the
@@ -274,6 +282,17 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   }
   HomeJ<real> acc;
   acc.zero();
+  // the warp's queue of J deposits off the home cells: entries [0, nq), 7
+  // words each (7 is odd, so the lanes' entries fall on different banks)
+  float* jq = reinterpret_cast<float*>(smem_raw + S::jq_off) + warp * S::kQ * 7;
+  int nq = 0;
+  auto deposit_queued = [&](int q) {
+    const float* e = jq + q * 7;
+    int qi, qj, qk;
+    unpack_cell(__float_as_int(e[0]), qi, qj, qk);
+    const Axis<real> X = axis_weights(qi, (real)e[1]), Y = axis_weights(qj, (real)e[2]), Z = axis_weights(qk, (real)e[3]);
+    deposit_j(F, g, pc, X, Y, Z, (real)e[4], (real)e[5], (real)e[6]);
+  };
   // ring of particle rows fetched ahead; each lane copies and reads only its
   // own slots, so the per-thread cp.async groups need no warp barrier. A
   // stage holds the row's 32 records A, then its 32 records B, so that the
@@ -303,6 +322,7 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     const bool act = c >= 0;
     int i = 0, j = 0, k = 0;
     real fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
+    bool enq = false;  // J at x^{n+1/2} goes to the warp's queue
     if (act) {
       ++pushed;
       unpack_cell(c, i, j, k);
@@ -342,10 +362,34 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
         acc.add(pc.qn * vx, pc.qn * vy, pc.qn * vz, X, Y, Z, bx, by, bz);
       } else if (in_array(g, i, j, k)) {
         if (stencil_ok(g, i, j, k)) {
-          const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
-          deposit_j(F, g, pc, X, Y, Z, vx, vy, vz);
+          if constexpr (S::kJQueue) {
+            enq = true;
+          } else {
+            const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
+            deposit_j(F, g, pc, X, Y, Z, vx, vy, vz);
+          }
         } else {
           count_err(err, ERR_DEPOSIT_OOB);
+        }
+      }
+    }
+    if constexpr (S::kJQueue) {
+      // warp-uniform: the row's queued lanes take consecutive entries; a full
+      // warp's worth is deposited by all 32 lanes at once
+      const unsigned em = __ballot_sync(0xffffffffu, enq);
+      if (em) {
+        if (enq) {
+          float* e = jq + (nq + __popc(em & ((1u << lane) - 1u))) * 7;
+          e[0] = __int_as_float(pack_cell(i, j, k));
+          e[1] = (float)fx; e[2] = (float)fy; e[3] = (float)fz;
+          e[4] = (float)vx; e[5] = (float)vy; e[6] = (float)vz;
+        }
+        nq += __popc(em);
+        if (nq >= kLanes) {
+          __syncwarp();
+          deposit_queued(nq - kLanes + lane);
+          nq -= kLanes;
+          __syncwarp();
         }
       }
     }
@@ -371,6 +415,10 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       const int cnew = inside1 ? pack_cell(i, j, k) : settle(g, pc.out, i, j, k, fx, fy, fz, vx, vy, vz, err);
       store_records(P, t, cnew, fx, fy, fz, vx, vy, vz);
     }
+  }
+  if constexpr (S::kJQueue) {
+    __syncwarp();
+    if (lane < nq) deposit_queued(lane);
   }
   for (int o = 16; o > 0; o >>= 1) pushed += __shfl_down_sync(0xffffffffu, pushed, o);
   if (lane == 0 && pushed) atomicAdd(err + CNT_PUSHED, (unsigned long long)pushed);
