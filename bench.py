@@ -47,18 +47,53 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock and throttle-reason samples while the timed region runs."""
+    """SM clock and throttle-reason samples while the timed region runs: NVML
+    read every 10 ms from a thread (reads only), else nvidia-smi at its
+    200 ms floor."""
 
     def __init__(self, index: int):
         self.index = index
-        self.rows = []
+        self.rows = []  # (sm MHz, max sm MHz, hw_slowdown, hw_thermal, sw_thermal, sw_power_cap)
         self.proc = None
+        self.stop = threading.Event()
+        self.thread = None
 
     def __enter__(self):
         try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = None
+            try:  # the CUDA device by its PCI address (NVML numbers all GPUs, CUDA the visible ones)
+                import torch
+
+                pr = torch.cuda.get_device_properties(self.index)
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(
+                    f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0")
+            except Exception:
+                h = None
+            if h is None:
+                h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            bits = [pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap]
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop.is_set():
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.rows.append((float(sm), float(mx), *[bool(r & b) for b in bits]))
+                    self.stop.wait(0.01)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
+        try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}",
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
                  "clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "200"],
@@ -72,27 +107,28 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 7:
-                self.rows.append(parts)
+            if len(parts) >= 6 and parts[0].replace(".", "").isdigit() and parts[1].replace(".", "").isdigit():
+                self.rows.append((float(parts[0]), float(parts[1]), *[p == "Active" for p in parts[2:6]]))
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
 
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.rows)}
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[2 + i]})
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows),
+                "sm_max_mhz": max(r[1] for r in self.rows), "reasons": reasons,
+                "samples": len(self.rows), "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 
 # ------------------------------------------------------------------ CPU side

@@ -868,25 +868,28 @@ __global__ void phi_rho_kernel(real* F, const Run<real>* __restrict__ runs, cons
 }
 
 // Batched small GEMM C = alpha * op(A B) over every run (row-major, the run's
-// sizes): 32x32 output tiles, K staged through shared memory. mode selects the
-// operands of the four sine transforms:
+// sizes): 64x64 output tiles, 256 threads of 4x4 outputs each, K staged
+// through shared memory 32 at a time. mode selects the operands of the four
+// sine transforms:
 //  0: C[nx][nz] = A[nx][nz] * S_nz        (transform along z)
 //  1: C[nx][nz] = S_nx * A[nx][nz], then / eigenvalue  (along x, solve)
 //  2: C[nx][nz] = (2/nx) S_nx * A          (inverse along x)
 //  3: C[nx][nz] = (2/nz) A * S_nz          (inverse along z)
 // S_n[i][j] = sin(pi i j / n); its row and column 0 vanish, so the transforms
 // skip the first element as the reference's sinft does (y[1] = 0, :2902).
+constexpr int kGemmTile = 64;
 template <typename real>
 __global__ void __launch_bounds__(256) dst_gemm_kernel(const Run<real>* __restrict__ runs, const Item* __restrict__ items,
                                                        int nitems, const real* __restrict__ A, real* C,
                                                        const real* __restrict__ sines, int mode) {
-  __shared__ real As[32][33];
-  __shared__ real Bs[32][33];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  constexpr int T = kGemmTile, KT = 32;
+  __shared__ real As[T][KT + 1];  // [row of C][k]
+  __shared__ real Bs[KT][T + 1];  // [k][col of C]
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16; outputs (ty + 16 u, tx + 16 v)
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const Run<real> R = runs[items[it].run];
+    const Run<real>& R = runs[items[it].run];
     const int nx = R.nx, nz = R.nz;
-    const int tiles_n = (nz + 31) / 32;
+    const int tiles_n = (nz + T - 1) / T;
     const int ti = items[it].first / tiles_n, tj = items[it].first % tiles_n;
     const real* a = A + R.roff;
     real* cmat = C + R.roff;
@@ -894,50 +897,68 @@ __global__ void __launch_bounds__(256) dst_gemm_kernel(const Run<real>* __restri
     const real* Sz = sines + R.sz_dst + (long long)nx * nx;
     const bool left = mode == 1 || mode == 2;  // S * A (K = nx) or A * S (K = nz)
     const int K = left ? nx : nz;
-    real acc[4] = {0, 0, 0, 0};
-    for (int k0 = 0; k0 < K; k0 += 32) {
-      // left operand tile [32 rows of C][32 of K], right operand tile [32 of K][32 cols of C]
-      for (int q = ty; q < 32; q += 8) {
-        const int row = ti * 32 + q, kc = k0 + tx;
-        real lv = 0, rv = 0;
+    real acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] = 0;
+    for (int k0 = 0; k0 < K; k0 += KT) {
+      __syncthreads();  // the last tile's reads are done
+      // left operand tile [T rows of C][KT of K], right operand tile [KT of K][T cols of C]
+      for (int q = threadIdx.x; q < T * KT; q += blockDim.x) {
+        const int r = q / KT, kc = q % KT;  // left: row r, column k0 + kc
+        const int row = ti * T + r, kk = k0 + kc;
+        real lv = 0;
         if (left) {
-          if (row < nx && kc < nx) lv = Sx[(long long)row * nx + kc];
-          const int kr = k0 + q, col = tj * 32 + tx;
-          if (kr < nx && col < nz) rv = a[(long long)kr * nz + col];
+          if (row < nx && kk < nx) lv = Sx[(long long)row * nx + kk];
         } else {
-          if (row < nx && kc < nz) lv = a[(long long)row * nz + kc];
-          const int kr = k0 + q, col = tj * 32 + tx;
-          if (kr < nz && col < nz) rv = Sz[(long long)kr * nz + col];
+          if (row < nx && kk < nz) lv = a[(long long)row * nz + kk];
         }
-        As[q][tx] = lv;
-        Bs[q][tx] = rv;
+        As[r][kc] = lv;
+        const int kr = q / T, cc = q % T;  // right: row k0 + kr, column cc
+        const int krow = k0 + kr, col = tj * T + cc;
+        real rv = 0;
+        if (left) {
+          if (krow < nx && col < nz) rv = a[(long long)krow * nz + col];
+        } else {
+          if (krow < nz && col < nz) rv = Sz[(long long)krow * nz + col];
+        }
+        Bs[kr][cc] = rv;
       }
       __syncthreads();
 #pragma unroll 8
-      for (int kk = 0; kk < 32; ++kk) {
-        const real b = Bs[kk][tx];
+      for (int kk = 0; kk < KT; ++kk) {
+        real av[4], bv[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) acc[u] += As[ty + 8 * u][kk] * b;
+        for (int u = 0; u < 4; ++u) av[u] = As[ty + 16 * u][kk];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) bv[v] = Bs[kk][tx + 16 * v];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[u][v] += av[u] * bv[v];
       }
-      __syncthreads();
     }
     const double Pi = 3.14159265358979323846;
-    for (int u = 0; u < 4; ++u) {
-      const int row = ti * 32 + ty + 8 * u, col = tj * 32 + tx;
-      if (row >= nx || col >= nz) continue;
-      real v = acc[u];
-      if (mode == 1) {
-        // renew_phi's eigenvalue (:2680-2690): row = x wave number, col = z wave number
-        const double sz = sin(Pi * (double)col / (double)nz / 2.), sx = sin(Pi * (double)row / (double)nx / 2.);
-        const double Aev = -(sz * sz + sx * sx) / ((R.dx / 2.) * (R.dx / 2.));
-        v = Aev == 0. ? (real)0 : (real)((double)v / Aev);
-      } else if (mode == 2) {
-        v = (real)(2. * (double)v / nx);
-      } else if (mode == 3) {
-        v = (real)(2. * (double)v / nz);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int row = ti * T + ty + 16 * u, col = tj * T + tx + 16 * v;
+        if (row >= nx || col >= nz) continue;
+        real w = acc[u][v];
+        if (mode == 1) {
+          // renew_phi's eigenvalue (:2680-2690): row = x wave number, col = z wave number
+          const double sz = sin(Pi * (double)col / (double)nz / 2.), sx = sin(Pi * (double)row / (double)nx / 2.);
+          const double Aev = -(sz * sz + sx * sx) / ((R.dx / 2.) * (R.dx / 2.));
+          w = Aev == 0. ? (real)0 : (real)((double)w / Aev);
+        } else if (mode == 2) {
+          w = (real)(2. * (double)w / nx);
+        } else if (mode == 3) {
+          w = (real)(2. * (double)w / nz);
+        }
+        cmat[(long long)row * nz + col] = w;
       }
-      cmat[(long long)row * nz + col] = v;
-    }
   }
 }
 
@@ -1096,7 +1117,7 @@ struct pic2d_batch {
   Item* row_items = nullptr;   int n_row = 0;    // (run, first of kFieldRows interior rows)
   Item* rho_items = nullptr;   int n_rhorow = 0; // (run, rho row 0..nx-1)
   Item* part_items = nullptr;  int n_part = 0;   // (run*2+s, first slot) over [0, cap)
-  Item* tile_items = nullptr;  int n_tile = 0;   // (run, 32x32 tile of nx x nz)
+  Item* tile_items = nullptr;  int n_tile = 0;   // (run, 64x64 tile of nx x nz)
   Item* src_items[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [init/add][species]
   int n_src[2][2] = {{0, 0}, {0, 0}};
   SourceSet* sets[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -1724,7 +1745,7 @@ int do_create(pic2d_batch* b) {
     for (int k = 0; k < H[r].nx; ++k) rhos.push_back({r, k});
     for (int s = 0; s < 2; ++s)
       for (long long q = 0; q < H[r].cap; q += kChunk) parts.push_back({2 * r + s, (int)q});
-    const int tn = (H[r].nz + 31) / 32, tm = (H[r].nx + 31) / 32;
+    const int tn = (H[r].nz + kGemmTile - 1) / kGemmTile, tm = (H[r].nx + kGemmTile - 1) / kGemmTile;
     for (int t = 0; t < tn * tm; ++t) tiles.push_back({r, t});
   }
   auto upload = [&](const std::vector<Item>& v, Item** dst, int* cnt) -> int {
