@@ -149,6 +149,29 @@ struct Item {
 // kFieldRows rows of a run, so that a thread updates several nodes per item.
 constexpr int kFieldRows = 4;
 
+// The nodes (k, m) of one item, k0 <= k < k0 + kFieldRows (and < nx + 2), 2 <=
+// m < nz + 2, flattened over the block's threads and walked without a
+// division per node.
+struct NodeWalk {
+  int k, m, dk, dm;
+  __device__ NodeWalk(int k0, int nz, int first, int stride)
+      : k(k0 + first / nz), m(2 + first % nz), dk(stride / nz), dm(stride % nz) {}
+  __device__ void next(int nz) {
+    k += dk;
+    m += dm;
+    if (m >= nz + 2) {
+      m -= nz;
+      ++k;
+    }
+  }
+};
+
+// Whether cells 2 idx and 2 idx + 1 of the doubled grid lie outside the
+// damping layers of an axis of n cells (ramp2 zero for both).
+__device__ __forceinline__ bool undamped(int idx, int n, int absorb) {
+  return 2 * idx - 4 > 2 * absorb && 2 * idx + 1 - 4 < 2 * n - 2 * absorb;
+}
+
 // The 4th-order difference (27 (f[0] - f[-1]) - (f[1] - f[-2])) / 24 / dx with
 // the run's 1 / (24 dx), in the field's precision; d is the stride.
 template <typename real>
@@ -183,16 +206,24 @@ __global__ void __launch_bounds__(256) renew_b4_kernel(real* F, const Run<real>*
     // (1 - s t) / (1 + s t) and dt / 2 / (1 + s t)
     auto ca = [&](double s) { return s == 0. ? (real)1 : (real)((1. - s * t) / (1. + s * t)); };
     auto cb = [&](double s) { return s == 0. ? hdt : (real)(0.5 * R.dt / (1. + s * t)); };
-    for (int q = threadIdx.x; q < kFieldRows * nz; q += blockDim.x) {
-      const int k = k0 + q / nz, m = 2 + q % nz;
-      if (k >= nx + 2) break;
+    const int kend = min(k0 + kFieldRows, nx + 2);
+    for (NodeWalk w(k0, nz, threadIdx.x, blockDim.x); w.k < kend; w.next(nz)) {
+      const int k = w.k, m = w.m;
       const int n = k * G + m;
+      const real dex = d4(ex, n, 1, inv24dx), dez = d4(ez, n, G, inv24dx);
+      const real deyx = d4(ey, n, 1, inv24dx), deyz = d4(ey, n, G, inv24dx);
+      if (undamped(k, nx, a1) && undamped(m, nz, a1)) {  // s = 0 for all three
+        bx[n] = b0x[n] + (bx[n] - b0x[n]) + hdt * deyx;
+        by[n] = b0y[n] + (by[n] - b0y[n]) - hdt * (dex - dez);
+        bz[n] = b0z[n] + (bz[n] - b0z[n]) - hdt * deyz;
+        continue;
+      }
       double s = sigma2(sa, 2 * k + 1, 2 * m, nx, nz, a1);
-      bx[n] = b0x[n] + ca(s) * (bx[n] - b0x[n]) + cb(s) * d4(ey, n, 1, inv24dx);
+      bx[n] = b0x[n] + ca(s) * (bx[n] - b0x[n]) + cb(s) * deyx;
       s = sigma2(sa, 2 * k, 2 * m, nx, nz, a1);
-      by[n] = b0y[n] + ca(s) * (by[n] - b0y[n]) - cb(s) * (d4(ex, n, 1, inv24dx) - d4(ez, n, G, inv24dx));
+      by[n] = b0y[n] + ca(s) * (by[n] - b0y[n]) - cb(s) * (dex - dez);
       s = sigma2(sa, 2 * k, 2 * m + 1, nx, nz, a1);
-      bz[n] = b0z[n] + ca(s) * (bz[n] - b0z[n]) - cb(s) * d4(ey, n, G, inv24dx);
+      bz[n] = b0z[n] + ca(s) * (bz[n] - b0z[n]) - cb(s) * deyz;
     }
   }
 }
@@ -237,16 +268,25 @@ __global__ void __launch_bounds__(256) renew_e4_kernel(real* F, const Run<real>*
       return s == 0. ? (real)1 : (real)((1. - h) / (1. + h));
     };
     auto cb = [&](double s) { return s == 0. ? rcc : (real)(cc / (1. + 0.5 * mu0 * s * cc)); };
-    for (int q = threadIdx.x; q < kFieldRows * nz; q += blockDim.x) {
-      const int k = k0 + q / nz, m = 2 + q % nz;
-      if (k >= nx + 2) break;
+    const int kend = min(k0 + kFieldRows, nx + 2);
+    for (NodeWalk w(k0, nz, threadIdx.x, blockDim.x); w.k < kend; w.next(nz)) {
+      const int k = w.k, m = w.m;
       const int n = k * G + m;
+      const real tx = -db4(by, b0y, n, 1) - rmu0 * (jix[n] - jex[n]);
+      const real tz = db4(by, b0y, n, G) - rmu0 * (jiz[n] - jez[n]);
+      const real ty = db4(bx, b0x, n, 1) - db4(bz, b0z, n, G) - rmu0 * (jiy[n] - jey[n]);
+      if (undamped(k, nx, a1) && undamped(m, nz, a1)) {  // s = 0 for all three
+        ex[n] = ex[n] + rcc * tx;
+        ez[n] = ez[n] + rcc * tz;
+        ey[n] = ey[n] + rcc * ty;
+        continue;
+      }
       double s = sigma2(sa, 2 * k, 2 * m + 1, nx, nz, a1);
-      ex[n] = ca(s) * ex[n] + cb(s) * (-db4(by, b0y, n, 1) - rmu0 * (jix[n] - jex[n]));
+      ex[n] = ca(s) * ex[n] + cb(s) * tx;
       s = sigma2(sa, 2 * k + 1, 2 * m, nx, nz, a1);
-      ez[n] = ca(s) * ez[n] + cb(s) * (db4(by, b0y, n, G) - rmu0 * (jiz[n] - jez[n]));
+      ez[n] = ca(s) * ez[n] + cb(s) * tz;
       s = sigma2(sa, 2 * k + 1, 2 * m + 1, nx, nz, a1);
-      ey[n] = ca(s) * ey[n] + cb(s) * (db4(bx, b0x, n, 1) - db4(bz, b0z, n, G) - rmu0 * (jiy[n] - jey[n]));
+      ey[n] = ca(s) * ey[n] + cb(s) * ty;
     }
   }
 }
@@ -356,6 +396,24 @@ __device__ __forceinline__ void dep4(real* P, int G, int i, int k, real v, real 
   atomicAdd(P + (i + 1) * G + k, v * (x1 * z0));
   atomicAdd(P + i * G + k + 1, v * (x0 * z1));
   atomicAdd(P + (i + 1) * G + k + 1, v * (x1 * z1));
+}
+
+// cal_track_c4 (:1520-1560) on (vx, vy, vz) with T = q dt / 2m; FP32
+// divides with __fdividef.
+template <typename real>
+__device__ __forceinline__ void rotate_c4(real T, real ex, real ey, real ez, real bx, real by, real bz, real& vx,
+                                          real& vy, real& vz) {
+  const real den = (real)1 + T * T * (bx * bx + by * by + bz * bz);
+  real S;
+  if constexpr (sizeof(real) == 4) S = __fdividef(2.f * T, den);
+  else S = (real)2 * T / den;
+  const real ux = vx + ex * T, uy = vy + ey * T, uz = vz + ez * T;
+  const real uox = ux + T * (uy * bz - uz * by);
+  const real uoy = uy + T * (uz * bx - ux * bz);
+  const real uoz = uz + T * (ux * by - uy * bx);
+  vx = ux + S * (uoy * bz - uoz * by) + ex * T;
+  vy = uy + S * (uoz * bx - uox * bz) + ey * T;
+  vz = uz + S * (uox * by - uoy * bx) + ez * T;
 }
 
 // The particle layout the cell sort builds, per run and species: group
@@ -571,20 +629,7 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
               by = bil(F0 + (long long)P_BY * R.nodes, G, X.a, Z.a, X.a0, X.a1, Z.a0, Z.a1);
               bz = bil(F0 + (long long)P_BZ * R.nodes, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
             }
-            ex += ex_add;
-            ey += ey_add;
-            // cal_track_c4 (:1520-1560); FP32 divides with __fdividef
-            const real den = (real)1 + T * T * (bx * bx + by * by + bz * bz);
-            real S;
-            if constexpr (sizeof(real) == 4) S = __fdividef(2.f * T, den);
-            else S = (real)2 * T / den;
-            const real ux = vx + ex * T, uy = vy + ey * T, uz = vz + ez * T;
-            const real uox = ux + T * (uy * bz - uz * by);
-            const real uoy = uy + T * (uz * bx - ux * bz);
-            const real uoz = uz + T * (ux * by - uy * bx);
-            vx = ux + S * (uoy * bz - uoz * by) + ex * T;
-            vy = uy + S * (uoz * bx - uox * bz) + ey * T;
-            vz = uz + S * (uox * by - uoy * bx) + ez * T;
+            rotate_c4(T, ex + ex_add, ey + ey_add, ez, bx, by, bz, vx, vy, vz);
           }
         }
         advance(i, fx, vx * hdt);
@@ -1127,12 +1172,16 @@ struct pic2d_batch {
   size_t scan_len = 0;
   int* ccnt = nullptr;   // cell sort: particles per cell and cursors (rho_len each)
   int* ccur = nullptr;
+  int* gfree = nullptr;  // cell sort: per group and lane, its first free slot number (32 ngroups)
+  int* gover = nullptr;  // cell sort: per group, the particles placed in other lanes' free slots
   // tiled layout (Layout2): groups of every run, their run, rows and offsets
   int ngroups = 0;
   int* grun = nullptr;
   int* gsz = nullptr;                   // ngroups + 1 (the last stays 0)
-  int* goff[2] = {nullptr, nullptr};    // ngroups + 1
-  int* gmax[2] = {nullptr, nullptr};
+  // the layout of each pool, per species: goff (ngroups + 1) and gmax
+  int* goff[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int* gmax[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  bool laid = false;                    // the current pool holds a layout (a sort has run since init)
   Item* ptile_items = nullptr; int n_ptile = 0;  // (run*2+s, tile) of the push
   int tile_x = 4;                       // group rows per push tile (tuned)
   int* step_dev = nullptr;
@@ -1289,33 +1338,62 @@ __global__ void cellcount2d_kernel(Pools pools, const Run<real>* __restrict__ ru
   }
 }
 
-// Rows of every group: its fullest lane's count (one warp per group); gsz =
-// 32 rows, scanned into the groups' offsets.
+// Rows of every group (one warp per group): the mean count of its cells,
+// rounded up (at most its fullest cell's count); gsz = 32 rows, scanned into
+// the groups' offsets. A row runs as long as its fullest lane's column, so
+// rows sized for the fullest cell of 32 left 30-40 % of the lanes idle at
+// 16-64 particles per cell (the whole 2D step took 19.9 ms against 17.8). The
+// particles of a cell past the group's rows take the free slots of the
+// group's other lanes (rows past their own cells' counts), so every particle
+// stays in its group and its tile's field window; they deposit as particles
+// off their lane's home cell do. gfree holds each lane's first free slot
+// number (an exclusive scan of the lanes' free rows). The rows cover the mean
+// of all 32 lanes, so the free slots hold every such particle. (Rows of the
+// mean plus half or one standard deviation of a Poisson count measured 18.4
+// and 18.9 ms.)
 template <typename real>
 __global__ void group_rows2d_kernel(const Run<real>* __restrict__ runs, const int* __restrict__ grun, int ngroups,
-                                    const int* __restrict__ cnt, int* gmax, int* gsz) {
+                                    const int* __restrict__ cnt, int* gmax, int* gsz, int* gfree) {
   const int G = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (G >= ngroups) return;  // warp-uniform
   const Run<real> R = runs[grun[G]];
   const int q = G - R.gbase;
   const int i = q / R.nzb, k = (q % R.nzb) * 32 + lane;
-  int m = k < R.nz ? cnt[R.roff + i * R.nz + k] : 0;
+  const int c = k < R.nz ? cnt[R.roff + i * R.nz + k] : 0;
+  int m = c, sum = c, nv = k < R.nz;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  for (int o = 16; o > 0; o >>= 1) {
+    m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    nv += __shfl_xor_sync(0xffffffffu, nv, o);
+  }
+  const int rows = min(m, (sum + max(nv, 1) - 1) / max(nv, 1));
+  // free rows of this lane, scanned over the warp
+  const int fr = max(rows - c, 0);
+  int pre = fr;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, pre, o);
+    if (lane >= o) pre += v;
+  }
+  gfree[32LL * G + lane] = pre - fr;
   if (lane == 0) {
-    gmax[G] = m;
-    gsz[G] = 32 * m;
+    gmax[G] = rows;
+    gsz[G] = 32 * rows;
   }
 }
 
 // Each particle to row (its rank in its cell) of its cell's lane column in the
-// other pool. A particle past the run's capacity is lost (ERR_STORE_FULL).
+// other pool, or, past its group's rows, to the next free slot of the group
+// (gover counts them; the free slots are numbered lane by lane, gfree). A
+// particle past the run's capacity is lost (ERR_STORE_FULL).
 template <typename real>
 __global__ void cellscatter2d_kernel(Pools src, Pools dst, const Run<real>* __restrict__ runs,
                                      const State* __restrict__ st, const Item* __restrict__ items, int nitems,
-                                     int chunk, int s, const int* __restrict__ goff, int* cursor,
-                                     unsigned long long* err) {
+                                     int chunk, int s, const int* __restrict__ goff, const int* __restrict__ gmax,
+                                     const int* __restrict__ gfree, const int* __restrict__ cnt, int* cursor,
+                                     int* gover, unsigned long long* err) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int rs = items[it].run;
     if ((rs & 1) != s) continue;
@@ -1332,8 +1410,31 @@ __global__ void cellscatter2d_kernel(Pools src, Pools dst, const Run<real>* __re
       const int key = q < last ? sort_key(R, c) : -1;
       const int rank = warp_add_count(cursor, key < 0 ? 0 : key, key >= 0);
       if (key < 0) continue;
-      const int i = (int)((key - R.roff) / R.nz), k = (int)((key - R.roff) % R.nz);
-      const long long rel = (long long)goff[R.gbase + i * R.nzb + (k >> 5)] - base + 32LL * rank + (k & 31);
+      const int rk = key - (int)R.roff;
+      const int i = rk / R.nz, k = rk % R.nz;
+      const int Gk = R.gbase + i * R.nzb + (k >> 5);
+      const int rows = gmax[Gk];
+      long long rel;
+      if (rank < rows) {
+        rel = (long long)goff[Gk] - base + 32LL * rank + (k & 31);
+      } else {
+        // the j-th free slot of the group: the last lane whose first free
+        // slot number is <= j, at the row after its own cell's particles
+        const int j = atomicAdd(gover + Gk, 1);
+        const int* f = gfree + 32LL * Gk;
+        int l = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
+          if (f[l + step] <= j) l += step;
+        const int kl = (k & ~31) + l;
+        const int cl = kl < R.nz ? min(cnt[R.roff + i * R.nz + kl], rows) : 0;
+        const int row = cl + (j - f[l]);
+        if (row >= rows) {  // the group's free slots are spent (cannot happen: the rows cover the mean)
+          atomicAdd(err + ERR_STORE_FULL, 1ull);
+          continue;
+        }
+        rel = (long long)goff[Gk] - base + 32LL * row + l;
+      }
       if (rel >= R.cap) {
         atomicAdd(err + ERR_STORE_FULL, 1ull);
         continue;
@@ -1374,7 +1475,60 @@ __global__ void layout_count2d_kernel(const Run<real>* __restrict__ runs, State*
   st[r].count[s] = (int)min((long long)goff[R.gbase + R.ngroups] - goff[R.gbase], R.cap);
 }
 
-// Every run's particles by cell into the tiled layout of the other pool.
+// The count of a pool that holds a layout (every sort after the first): one
+// warp per group of the old layout, lane l walking its column. The particles
+// still in the lane's home cell are counted in a register and added once; a
+// particle that moved adds itself to its new cell. (Ranking the stayers by
+// the same per-lane counter in the scatter made its stores land on different
+// rows of the lanes' columns and measured slower than ranking every particle
+// by the cell cursors of cellscatter2d_kernel.)
+template <typename real>
+__global__ void layout_count_kernel(Pools pools, const Run<real>* __restrict__ runs, const int* __restrict__ grun,
+                                    int ngroups, const int* __restrict__ goff, const int* __restrict__ gmax, int s,
+                                    int* cnt) {
+  const int G = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (G >= ngroups) return;  // warp-uniform
+  const Run<real>& R = runs[grun[G]];
+  const int q = G - R.gbase;
+  const int i = q / R.nzb, k = (q % R.nzb) * 32 + lane;
+  const bool valid = k < R.nz;
+  const int home = valid ? (int)R.roff + i * R.nz + k : -1;
+  const long long base = R.poff + goff[G] - goff[R.gbase] + lane, end = R.poff + R.cap;
+  const int* cell = pools.cell[s];
+  int stay = 0;
+  for (int row = 0; row < gmax[G]; ++row) {
+    const long long t = base + 32LL * row;
+    if (t >= end) break;
+    const int key = sort_key(R, cell[t]);
+    if (key < 0) continue;
+    if (key == home) ++stay;
+    else atomicAdd(cnt + key, 1);
+  }
+  if (valid && stay) atomicAdd(cnt + home, stay);
+}
+
+// Pass 1 for the slots after the old layout (a refill appended there).
+template <typename real>
+__global__ void tail_count_kernel(Pools pools, const Run<real>* __restrict__ runs, const State* __restrict__ st,
+                                  const Item* __restrict__ items, int nitems, int chunk, int s,
+                                  const int* __restrict__ goff, int* cnt) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int rs = items[it].run;
+    if ((rs & 1) != s) continue;
+    const Run<real>& R = runs[rs >> 1];
+    const int lay = goff[R.gbase + R.ngroups] - goff[R.gbase];  // the old layout's end
+    const int first = max(items[it].first, lay), last = min(items[it].first + chunk, st[rs >> 1].count[s]);
+    for (int q = first + threadIdx.x; q < last; q += blockDim.x) {
+      const int key = sort_key(R, pools.cell[s][R.poff + q]);
+      if (key >= 0) atomicAdd(cnt + key, 1);
+    }
+  }
+}
+
+// Every run's particles by cell into the tiled layout of the other pool: the
+// counts over every slot (the first sort after init) or by the layout-aware
+// passes above, then the ranks by per-cell cursors.
 template <typename real>
 int cellsort(pic2d_batch* b) {
   const int nb = 1 - b->cur;
@@ -1382,24 +1536,43 @@ int cellsort(pic2d_batch* b) {
   const Run<real>* R = runs_of<real>(b);
   const int gblocks = (int)((32LL * b->ngroups + 255) / 256);
   for (int s = 0; s < 2; ++s) {
+    int* goff_old = b->goff[b->cur][s];
+    int* gmax_old = b->gmax[b->cur][s];
+    int* goff = b->goff[nb][s];
+    int* gmax = b->gmax[nb][s];
     CK2(cudaMemsetAsync(b->ccnt, 0, sizeof(int) * (size_t)nc, b->stream));
     CK2(cudaMemsetAsync(b->ccur, 0, sizeof(int) * (size_t)nc, b->stream));
-    cellcount2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], R, b->st, b->part_items,
-                                                                            b->n_part, kChunk, s, b->ccnt);
+    if (b->laid) {
+      layout_count_kernel<real><<<gblocks, 256, 0, b->stream>>>(b->pool[b->cur], R, b->grun, b->ngroups, goff_old,
+                                                                gmax_old, s, b->ccnt);
+      CKL2();
+      tail_count_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], R, b->st, b->part_items,
+                                                                             b->n_part, kChunk, s, goff_old, b->ccnt);
+      CKL2();
+    } else {
+      cellcount2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], R, b->st,
+                                                                              b->part_items, b->n_part, kChunk, s,
+                                                                              b->ccnt);
+      CKL2();
+    }
+    group_rows2d_kernel<real><<<gblocks, 256, 0, b->stream>>>(R, b->grun, b->ngroups, b->ccnt, gmax, b->gsz,
+                                                               b->gfree);
     CKL2();
-    group_rows2d_kernel<real><<<gblocks, 256, 0, b->stream>>>(R, b->grun, b->ngroups, b->ccnt, b->gmax[s], b->gsz);
+    CKR2(scan_excl(b, b->gsz, goff, b->ngroups + 1, b->scan_tmp, b->scan_len));
+    // the empty slots first: the scatter then fills some of them with other cells' particles
+    pad2d_kernel<real><<<gblocks, 256, 0, b->stream>>>(b->pool[nb].cell[s], R, b->grun, b->ngroups, goff, gmax,
+                                                       b->ccnt);
     CKL2();
-    CKR2(scan_excl(b, b->gsz, b->goff[s], b->ngroups + 1, b->scan_tmp, b->scan_len));
+    CK2(cudaMemsetAsync(b->gover, 0, sizeof(int) * (size_t)std::max(b->ngroups, 1), b->stream));
     cellscatter2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(
-        b->pool[b->cur], b->pool[nb], R, b->st, b->part_items, b->n_part, kChunk, s, b->goff[s], b->ccur, b->err);
+        b->pool[b->cur], b->pool[nb], R, b->st, b->part_items, b->n_part, kChunk, s, goff, gmax, b->gfree, b->ccnt,
+        b->ccur, b->gover, b->err);
     CKL2();
-    pad2d_kernel<real><<<gblocks, 256, 0, b->stream>>>(b->pool[nb].cell[s], R, b->grun, b->ngroups, b->goff[s],
-                                                       b->gmax[s], b->ccnt);
-    CKL2();
-    layout_count2d_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(R, b->st, b->nruns, s, b->goff[s]);
+    layout_count2d_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(R, b->st, b->nruns, s, goff);
     CKL2();
   }
   b->cur = nb;
+  b->laid = true;
   return PIC_OK;
 }
 
@@ -1435,7 +1608,7 @@ template <typename real>
 int push(pic2d_batch* b) {
   const Run<real>* R = runs_of<real>(b);
   real* F = (real*)b->field;
-  Layout2 L{{b->goff[0], b->goff[1]}, {b->gmax[0], b->gmax[1]}};
+  Layout2 L{{b->goff[b->cur][0], b->goff[b->cur][1]}, {b->gmax[b->cur][0], b->gmax[b->cur][1]}};
   const Pools P = b->pool[b->cur];
   switch (b->tile_x) {
     case 1:
@@ -1609,6 +1782,7 @@ int do_init(pic2d_batch* b) {
   CK2(cudaMemsetAsync(b->st, 0, sizeof(State) * b->nruns, b->stream));
   for (int p = 0; p < 2; ++p) CK2(cudaMemsetAsync(b->pool[p].cell[0], 0xff, sizeof(int) * b->pool_slots, b->stream));
   for (int p = 0; p < 2; ++p) CK2(cudaMemsetAsync(b->pool[p].cell[1], 0xff, sizeof(int) * b->pool_slots, b->stream));
+  b->laid = false;  // the first sort goes from slot order
   CKR2(run_sources<real>(b, 0));
   CKR2(cellsort<real>(b));  // the particles by cell (only their order changes)
   // fdtd's set-up (:583-625)
@@ -1715,12 +1889,13 @@ int do_create(pic2d_batch* b) {
     CK2(cudaMemcpy(b->grun, grun.data(), sizeof(int) * ngroups, cudaMemcpyHostToDevice));
     CK2(cudaMalloc(&b->gsz, sizeof(int) * (ngroups + 1)));
     CK2(cudaMemset(b->gsz, 0, sizeof(int) * (ngroups + 1)));
-    for (int s = 0; s < 2; ++s) {
-      CK2(cudaMalloc(&b->goff[s], sizeof(int) * (ngroups + 1)));
-      CK2(cudaMemset(b->goff[s], 0, sizeof(int) * (ngroups + 1)));
-      CK2(cudaMalloc(&b->gmax[s], sizeof(int) * std::max(ngroups, 1)));
-      CK2(cudaMemset(b->gmax[s], 0, sizeof(int) * std::max(ngroups, 1)));
-    }
+    for (int p = 0; p < 2; ++p)
+      for (int s = 0; s < 2; ++s) {
+        CK2(cudaMalloc(&b->goff[p][s], sizeof(int) * (ngroups + 1)));
+        CK2(cudaMemset(b->goff[p][s], 0, sizeof(int) * (ngroups + 1)));
+        CK2(cudaMalloc(&b->gmax[p][s], sizeof(int) * std::max(ngroups, 1)));
+        CK2(cudaMemset(b->gmax[p][s], 0, sizeof(int) * std::max(ngroups, 1)));
+      }
   }
   CK2(cudaMalloc(&b->runs_dev, sizeof(Run<real>) * n));
   CK2(cudaMemcpy(b->runs_dev, H, sizeof(Run<real>) * n, cudaMemcpyHostToDevice));
@@ -1776,6 +1951,8 @@ int do_create(pic2d_batch* b) {
   CK2(cudaMalloc(&b->scan_tmp, sizeof(int) * b->scan_len));
   CK2(cudaMalloc(&b->ccnt, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
   CK2(cudaMalloc(&b->ccur, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
+  CK2(cudaMalloc(&b->gfree, sizeof(int) * 32 * (size_t)std::max(b->ngroups, 1)));
+  CK2(cudaMalloc(&b->gover, sizeof(int) * (size_t)std::max(b->ngroups, 1)));
   CK2(cudaMalloc(&b->step_dev, sizeof(int)));
   CK2(cudaMemset(b->step_dev, 0, sizeof(int)));
   CK2(cudaMalloc(&b->err, sizeof(unsigned long long) * ERR_COUNT));
@@ -1799,9 +1976,10 @@ void free_batch(pic2d_batch* b) {
   for (int w = 0; w < 2; ++w)
     for (int s = 0; s < 2; ++s) { cudaFree(b->src_items[w][s]); cudaFree(b->sets[w][s]); }
   cudaFree(b->flags); cudaFree(b->pos); cudaFree(b->scan_tmp); cudaFree(b->step_dev); cudaFree(b->err);
-  cudaFree(b->ccnt); cudaFree(b->ccur);
+  cudaFree(b->ccnt); cudaFree(b->ccur); cudaFree(b->gfree); cudaFree(b->gover);
   cudaFree(b->grun); cudaFree(b->gsz); cudaFree(b->ptile_items);
-  for (int s = 0; s < 2; ++s) { cudaFree(b->goff[s]); cudaFree(b->gmax[s]); }
+  for (int p = 0; p < 2; ++p)
+    for (int s = 0; s < 2; ++s) { cudaFree(b->goff[p][s]); cudaFree(b->gmax[p][s]); }
   if (b->stream) cudaStreamDestroy(b->stream);
 }
 

@@ -217,10 +217,12 @@ def test_sort_interval_changes_only_the_order():
 
 
 def test_layout_overflow_is_reported():
-    """A capacity that holds the initial load but not its tiled layout: the
-    particles the layout cannot place are counted (counter 6) and the status
-    is an error, with nothing written past the run's slots."""
-    cfg = cfg_from("sq64")
+    """A capacity that holds the initial load but not its tiled layout (32 x
+    16 cells: every group has 16 lanes without a cell, so its rows take about
+    twice the load): the particles the layout cannot place are counted
+    (counter 6) and the status is an error, with nothing written past the
+    run's slots."""
+    cfg = cfg_from("half")
     load = cfg.np * cfg.np * cfg.nx * cfg.nz + 1
     cfg.capacity = load + 64
     with Pic2DBatch([cfg, cfg_from("strip")], precision=32) as B:
