@@ -1174,6 +1174,7 @@ struct pic2d_batch {
   int* ccur = nullptr;
   int* gfree = nullptr;  // cell sort: per group and lane, its first free slot number (32 ngroups)
   int* gover = nullptr;  // cell sort: per group, the particles placed in other lanes' free slots
+  int* hcnt = nullptr;   // cell sort: per cell, the particles that stayed in it (rho_len)
   // tiled layout (Layout2): groups of every run, their run, rows and offsets
   int ngroups = 0;
   int* grun = nullptr;
@@ -1384,12 +1385,57 @@ __global__ void group_rows2d_kernel(const Run<real>* __restrict__ runs, const in
   }
 }
 
-// Each particle to row (its rank in its cell) of its cell's lane column in the
-// other pool, or, past its group's rows, to the next free slot of the group
-// (gover counts them; the free slots are numbered lane by lane, gfree). A
-// particle past the run's capacity is lost (ERR_STORE_FULL).
+// The destination of the particle of rank `rank` in cell `key`, relative to
+// the run's first slot: row `rank` of the cell's lane column in the new
+// layout, or, past its group's rows, the next free slot of the group (gover
+// counts them; the free slots are numbered lane by lane, gfree). -1 for a
+// particle past the run's capacity, which is lost (ERR_STORE_FULL).
 template <typename real>
-__global__ void cellscatter2d_kernel(Pools src, Pools dst, const Run<real>* __restrict__ runs,
+__device__ __forceinline__ long long dest_slot(const Run<real>& R, const int* __restrict__ goff,
+                                               const int* __restrict__ gmax, const int* __restrict__ gfree,
+                                               const int* __restrict__ cnt, int* gover, int key, int rank,
+                                               unsigned long long* err) {
+  const int rk = key - (int)R.roff;
+  const int i = rk / R.nz, k = rk % R.nz;
+  const int Gk = R.gbase + i * R.nzb + (k >> 5);
+  const int rows = gmax[Gk];
+  const long long base = goff[R.gbase];
+  long long rel;
+  if (rank < rows) {
+    rel = goff[Gk] - base + 32LL * rank + (k & 31);
+  } else {
+    // the j-th free slot of the group: the last lane whose first free slot
+    // number is <= j, at the row after its own cell's particles
+    const int j = atomicAdd(gover + Gk, 1);
+    const int* f = gfree + 32LL * Gk;
+    int l = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1)
+      if (f[l + step] <= j) l += step;
+    const int kl = (k & ~31) + l;
+    const int cl = kl < R.nz ? min(cnt[R.roff + i * R.nz + kl], rows) : 0;
+    const int row = cl + (j - f[l]);
+    if (row >= rows) {  // the group's free slots are spent (cannot happen: the rows cover the mean)
+      atomicAdd(err + ERR_STORE_FULL, 1ull);
+      return -1;
+    }
+    rel = goff[Gk] - base + 32LL * row + l;
+  }
+  if (rel >= R.cap) {
+    atomicAdd(err + ERR_STORE_FULL, 1ull);
+    return -1;
+  }
+  return rel;
+}
+
+// Each particle's destination (dest_slot), ranked by per-cell cursors over
+// every slot of the pool (the first sort after init). perm[destination] = the
+// particle's slot; layout_gather2d_kernel then moves the particles destination
+// by destination, so that the stores of its six arrays are whole rows (stores
+// of single particles to scattered rows cost the sort about eight times the
+// bytes it moves).
+template <typename real>
+__global__ void cellscatter2d_kernel(Pools src, int* perm, const Run<real>* __restrict__ runs,
                                      const State* __restrict__ st, const Item* __restrict__ items, int nitems,
                                      int chunk, int s, const int* __restrict__ goff, const int* __restrict__ gmax,
                                      const int* __restrict__ gfree, const int* __restrict__ cnt, int* cursor,
@@ -1401,53 +1447,50 @@ __global__ void cellscatter2d_kernel(Pools src, Pools dst, const Run<real>* __re
     const int n = st[rs >> 1].count[s];
     const int first = items[it].first;
     const int last = min(first + chunk, n);
-    const PView<real> A = pview<real>(src, s), B = pview<real>(dst, s);
-    const int base = goff[R.gbase];
+    const int* cell = src.cell[s];
     for (int qb = first; qb < last; qb += blockDim.x) {  // block-uniform
       const int q = qb + threadIdx.x;
       const long long t = R.poff + q;
-      const int c = q < last ? A.cell[t] : -1;
+      const int c = q < last ? cell[t] : -1;
       const int key = q < last ? sort_key(R, c) : -1;
       const int rank = warp_add_count(cursor, key < 0 ? 0 : key, key >= 0);
       if (key < 0) continue;
-      const int rk = key - (int)R.roff;
-      const int i = rk / R.nz, k = rk % R.nz;
-      const int Gk = R.gbase + i * R.nzb + (k >> 5);
-      const int rows = gmax[Gk];
-      long long rel;
-      if (rank < rows) {
-        rel = (long long)goff[Gk] - base + 32LL * rank + (k & 31);
-      } else {
-        // the j-th free slot of the group: the last lane whose first free
-        // slot number is <= j, at the row after its own cell's particles
-        const int j = atomicAdd(gover + Gk, 1);
-        const int* f = gfree + 32LL * Gk;
-        int l = 0;
-#pragma unroll
-        for (int step = 16; step > 0; step >>= 1)
-          if (f[l + step] <= j) l += step;
-        const int kl = (k & ~31) + l;
-        const int cl = kl < R.nz ? min(cnt[R.roff + i * R.nz + kl], rows) : 0;
-        const int row = cl + (j - f[l]);
-        if (row >= rows) {  // the group's free slots are spent (cannot happen: the rows cover the mean)
-          atomicAdd(err + ERR_STORE_FULL, 1ull);
-          continue;
-        }
-        rel = (long long)goff[Gk] - base + 32LL * row + l;
-      }
-      if (rel >= R.cap) {
-        atomicAdd(err + ERR_STORE_FULL, 1ull);
+      const long long rel = dest_slot(R, goff, gmax, gfree, cnt, gover, key, rank, err);
+      if (rel >= 0) perm[R.poff + rel] = (int)t;
+    }
+  }
+}
+
+// The move of the sort, destination by destination over every run's new
+// layout: perm[d] is the slot of the particle that goes to slot d, or -1 for
+// an empty slot.
+template <typename real>
+__global__ void layout_gather2d_kernel(Pools src, Pools dst, const Run<real>* __restrict__ runs,
+                                       const Item* __restrict__ items, int nitems, int chunk, int s,
+                                       const int* __restrict__ goff, const int* __restrict__ perm) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int rs = items[it].run;
+    if ((rs & 1) != s) continue;
+    const Run<real>& R = runs[rs >> 1];
+    const long long lay = min((long long)goff[R.gbase + R.ngroups] - goff[R.gbase], R.cap);
+    const int first = items[it].first, last = (int)min((long long)first + chunk, lay);
+    const PView<real> A = pview<real>(src, s), B = pview<real>(dst, s);
+    for (int q = first + threadIdx.x; q < last; q += blockDim.x) {
+      const long long d = R.poff + q;
+      const int t = perm[d];
+      if (t < 0) {
+        B.cell[d] = -1;
         continue;
       }
-      const long long d = R.poff + rel;
-      B.cell[d] = c;
+      B.cell[d] = A.cell[t];
       B.ox[d] = A.ox[t]; B.oz[d] = A.oz[t];
       B.vx[d] = A.vx[t]; B.vy[d] = A.vy[t]; B.vz[d] = A.vz[t];
     }
   }
 }
 
-// The empty slots of every group (rows past its lane's count) to cell -1.
+// The empty slots of every group (rows past its lane's count) to -1 in `cell`
+// (the sort's destination map).
 template <typename real>
 __global__ void pad2d_kernel(int* cell, const Run<real>* __restrict__ runs, const int* __restrict__ grun, int ngroups,
                              const int* __restrict__ goff, const int* __restrict__ gmax, const int* __restrict__ cnt) {
@@ -1475,17 +1518,18 @@ __global__ void layout_count2d_kernel(const Run<real>* __restrict__ runs, State*
   st[r].count[s] = (int)min((long long)goff[R.gbase + R.ngroups] - goff[R.gbase], R.cap);
 }
 
-// The count of a pool that holds a layout (every sort after the first): one
+// The sort of a pool that holds a layout (every sort after the first): one
 // warp per group of the old layout, lane l walking its column. The particles
-// still in the lane's home cell are counted in a register and added once; a
-// particle that moved adds itself to its new cell. (Ranking the stayers by
-// the same per-lane counter in the scatter made its stores land on different
-// rows of the lanes' columns and measured slower than ranking every particle
-// by the cell cursors of cellscatter2d_kernel.)
+// still in the lane's home cell (stayers) are counted in a register and added
+// once, hcnt[cell] = their number; a particle that moved adds itself to its
+// new cell. layout_perm_kernel then gives the stayers ranks in their old row
+// order from the same per-lane counter, so that the gather of the move reads
+// each new row from nearby old rows; the others take ranks after their new
+// cell's stayers from its cursor.
 template <typename real>
 __global__ void layout_count_kernel(Pools pools, const Run<real>* __restrict__ runs, const int* __restrict__ grun,
                                     int ngroups, const int* __restrict__ goff, const int* __restrict__ gmax, int s,
-                                    int* cnt) {
+                                    int* cnt, int* hcnt) {
   const int G = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (G >= ngroups) return;  // warp-uniform
@@ -1505,7 +1549,74 @@ __global__ void layout_count_kernel(Pools pools, const Run<real>* __restrict__ r
     if (key == home) ++stay;
     else atomicAdd(cnt + key, 1);
   }
-  if (valid && stay) atomicAdd(cnt + home, stay);
+  if (valid) {
+    hcnt[home] = stay;
+    if (stay) atomicAdd(cnt + home, stay);
+  }
+}
+
+// The destinations of the old layout's particles (see layout_count_kernel),
+// four rows in flight per lane.
+template <typename real>
+__global__ void layout_perm_kernel(Pools pools, const Run<real>* __restrict__ runs, const int* __restrict__ grun,
+                                   int ngroups, const int* __restrict__ goff_old, const int* __restrict__ gmax_old,
+                                   const int* __restrict__ goff, const int* __restrict__ gmax,
+                                   const int* __restrict__ gfree, const int* __restrict__ cnt,
+                                   const int* __restrict__ hcnt, int* cursor, int* gover, int s, int* perm,
+                                   unsigned long long* err) {
+  const int G = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (G >= ngroups) return;  // warp-uniform
+  const Run<real>& R = runs[grun[G]];
+  const int q = G - R.gbase;
+  const int i = q / R.nzb, k = (q % R.nzb) * 32 + lane;
+  const int home = k < R.nz ? (int)R.roff + i * R.nz + k : -1;
+  const long long base = R.poff + goff_old[G] - goff_old[R.gbase] + lane, end = R.poff + R.cap;
+  const int* cell = pools.cell[s];
+  constexpr int U = 4;
+  const int m = gmax_old[G];
+  int stay = 0;
+  for (int r0 = 0; r0 < m; r0 += U) {
+    int key[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const long long t = base + 32LL * (r0 + u);
+      key[u] = r0 + u < m && t < end ? sort_key(R, cell[t]) : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (key[u] < 0) continue;
+      const int rank = key[u] == home ? stay++ : hcnt[key[u]] + atomicAdd(cursor + key[u], 1);
+      const long long rel = dest_slot(R, goff, gmax, gfree, cnt, gover, key[u], rank, err);
+      if (rel >= 0) perm[R.poff + rel] = (int)(base + 32LL * (r0 + u));
+    }
+  }
+}
+
+// The destinations of the slots after the old layout (a refill appended
+// there): ranks after their cells' stayers.
+template <typename real>
+__global__ void tail_perm_kernel(Pools pools, const Run<real>* __restrict__ runs, const State* __restrict__ st,
+                                 const Item* __restrict__ items, int nitems, int chunk, int s,
+                                 const int* __restrict__ goff_old, const int* __restrict__ goff,
+                                 const int* __restrict__ gmax, const int* __restrict__ gfree,
+                                 const int* __restrict__ cnt, const int* __restrict__ hcnt, int* cursor, int* gover,
+                                 int* perm, unsigned long long* err) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int rs = items[it].run;
+    if ((rs & 1) != s) continue;
+    const Run<real>& R = runs[rs >> 1];
+    const int lay = goff_old[R.gbase + R.ngroups] - goff_old[R.gbase];
+    const int first = max(items[it].first, lay), last = min(items[it].first + chunk, st[rs >> 1].count[s]);
+    for (int q = first + threadIdx.x; q < last; q += blockDim.x) {
+      const long long t = R.poff + q;
+      const int key = sort_key(R, pools.cell[s][t]);
+      if (key < 0) continue;
+      const long long rel =
+          dest_slot(R, goff, gmax, gfree, cnt, gover, key, hcnt[key] + atomicAdd(cursor + key, 1), err);
+      if (rel >= 0) perm[R.poff + rel] = (int)t;
+    }
+  }
 }
 
 // Pass 1 for the slots after the old layout (a refill appended there).
@@ -1544,7 +1655,7 @@ int cellsort(pic2d_batch* b) {
     CK2(cudaMemsetAsync(b->ccur, 0, sizeof(int) * (size_t)nc, b->stream));
     if (b->laid) {
       layout_count_kernel<real><<<gblocks, 256, 0, b->stream>>>(b->pool[b->cur], R, b->grun, b->ngroups, goff_old,
-                                                                gmax_old, s, b->ccnt);
+                                                                gmax_old, s, b->ccnt, b->hcnt);
       CKL2();
       tail_count_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(b->pool[b->cur], R, b->st, b->part_items,
                                                                              b->n_part, kChunk, s, goff_old, b->ccnt);
@@ -1559,14 +1670,29 @@ int cellsort(pic2d_batch* b) {
                                                                b->gfree);
     CKL2();
     CKR2(scan_excl(b, b->gsz, goff, b->ngroups + 1, b->scan_tmp, b->scan_len));
-    // the empty slots first: the scatter then fills some of them with other cells' particles
-    pad2d_kernel<real><<<gblocks, 256, 0, b->stream>>>(b->pool[nb].cell[s], R, b->grun, b->ngroups, goff, gmax,
-                                                       b->ccnt);
+    // the destinations: the empty slots first (perm -1), since the scatter then
+    // fills some of them with other cells' particles; then the move
+    int* perm = b->flags;
+    pad2d_kernel<real><<<gblocks, 256, 0, b->stream>>>(perm, R, b->grun, b->ngroups, goff, gmax, b->ccnt);
     CKL2();
     CK2(cudaMemsetAsync(b->gover, 0, sizeof(int) * (size_t)std::max(b->ngroups, 1), b->stream));
-    cellscatter2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(
-        b->pool[b->cur], b->pool[nb], R, b->st, b->part_items, b->n_part, kChunk, s, goff, gmax, b->gfree, b->ccnt,
-        b->ccur, b->gover, b->err);
+    if (b->laid) {
+      layout_perm_kernel<real><<<gblocks, 256, 0, b->stream>>>(b->pool[b->cur], R, b->grun, b->ngroups, goff_old,
+                                                               gmax_old, goff, gmax, b->gfree, b->ccnt, b->hcnt,
+                                                               b->ccur, b->gover, s, perm, b->err);
+      CKL2();
+      tail_perm_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(
+          b->pool[b->cur], R, b->st, b->part_items, b->n_part, kChunk, s, goff_old, goff, gmax, b->gfree, b->ccnt,
+          b->hcnt, b->ccur, b->gover, perm, b->err);
+      CKL2();
+    } else {
+      cellscatter2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(
+          b->pool[b->cur], perm, R, b->st, b->part_items, b->n_part, kChunk, s, goff, gmax, b->gfree, b->ccnt,
+          b->ccur, b->gover, b->err);
+      CKL2();
+    }
+    layout_gather2d_kernel<real><<<persistent(b->n_part), 256, 0, b->stream>>>(
+        b->pool[b->cur], b->pool[nb], R, b->part_items, b->n_part, kChunk, s, goff, perm);
     CKL2();
     layout_count2d_kernel<real><<<(b->nruns + 127) / 128, 128, 0, b->stream>>>(R, b->st, b->nruns, s, goff);
     CKL2();
@@ -1953,6 +2079,7 @@ int do_create(pic2d_batch* b) {
   CK2(cudaMalloc(&b->ccur, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
   CK2(cudaMalloc(&b->gfree, sizeof(int) * 32 * (size_t)std::max(b->ngroups, 1)));
   CK2(cudaMalloc(&b->gover, sizeof(int) * (size_t)std::max(b->ngroups, 1)));
+  CK2(cudaMalloc(&b->hcnt, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
   CK2(cudaMalloc(&b->step_dev, sizeof(int)));
   CK2(cudaMemset(b->step_dev, 0, sizeof(int)));
   CK2(cudaMalloc(&b->err, sizeof(unsigned long long) * ERR_COUNT));
@@ -1976,7 +2103,7 @@ void free_batch(pic2d_batch* b) {
   for (int w = 0; w < 2; ++w)
     for (int s = 0; s < 2; ++s) { cudaFree(b->src_items[w][s]); cudaFree(b->sets[w][s]); }
   cudaFree(b->flags); cudaFree(b->pos); cudaFree(b->scan_tmp); cudaFree(b->step_dev); cudaFree(b->err);
-  cudaFree(b->ccnt); cudaFree(b->ccur); cudaFree(b->gfree); cudaFree(b->gover);
+  cudaFree(b->ccnt); cudaFree(b->ccur); cudaFree(b->gfree); cudaFree(b->gover); cudaFree(b->hcnt);
   cudaFree(b->grun); cudaFree(b->gsz); cudaFree(b->ptile_items);
   for (int p = 0; p < 2; ++p)
     for (int s = 0; s < 2; ++s) { cudaFree(b->goff[p][s]); cudaFree(b->gmax[p][s]); }
