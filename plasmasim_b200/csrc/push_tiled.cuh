@@ -10,9 +10,9 @@ namespace pb {
 constexpr int kStages = 3;   // particle rows in flight per warp
 
 
-// The tile's interior cells: first cell (ci0, cj0, ck0) and extents (the
-// nominal tile clipped at the last interior cell, n + 1, of each axis).
-struct TileBox {
+// A box of cells: first cell (ci0, cj0, ck0) and extents; the push uses the
+// domain's interior cells [2, n + 2) of each axis.
+struct InteriorBox {
   int ci0, cj0, ck0;
   unsigned ex, ey, ez;
   __device__ __forceinline__ bool has(int i, int j, int k) const {
@@ -258,9 +258,11 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   for (int q = threadIdx.x; q < 4 * WN; q += blockDim.x) win[q] = (real)0;
   // FP32: E and B over the window, one plane per component
   float* fw = reinterpret_cast<float*>(smem_raw + S::fwin_off);
-  const int ci0 = wx0 + 2, cj0 = wy0 + 2, ck0 = wz0 + 2;  // the tile's first cell
-  const TileBox tb{ci0, cj0, ck0, (unsigned)min(kTileX, g.nx + 2 - ci0), (unsigned)min(kTileY, g.ny + 2 - cj0),
-                   (unsigned)min(kLanes, g.nz + 2 - ck0)};
+  // the interior cells: a particle in one needs none of the array bounds,
+  // ballistic or sr_particle checks (below), wherever it sits relative to the
+  // tile (testing the tile's own cells instead sent every particle that had
+  // crossed into a neighbouring tile down those paths)
+  const InteriorBox tb{2, 2, 2, (unsigned)g.nx, (unsigned)g.ny, (unsigned)g.nz};
   if constexpr (S::kFieldWin) fill_win<WX, WY, WZ, VEC_FLUSH>(fw, F, g, wx0, wy0, wz0);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -331,9 +333,8 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       unpack_cell(c, i, j, k);
       fx = ra[1]; fy = ra[2]; fz = ra[3];
       vx = rb[0]; vy = rb[1]; vz = rb[2];
-      // a particle in one of the tile's cells is in an interior cell: its
-      // stencils lie in the array, and it is ballistic only when the
-      // Absorb_grid2 layer reaches interior cells
+      // a particle in an interior cell has its stencils in the array, and it
+      // is ballistic only when the Absorb_grid2 layer reaches interior cells
       const bool inside = tb.has(i, j, k);
       bool bal = (pc.bal_interior || !inside) && ballistic(pc, i, j, k, fx, fy, fz);
       if (!bal && !inside && !stencil_ok(g, i, j, k)) {
