@@ -600,102 +600,102 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
         int jc = 0, ncell = 0;
         real jfx = 0, jfz = 0;
         if (c >= 0) {
-        ++pushed;
-        int i, k;
-        unpack2(c, i, k);
-        // ballistic margins (:682-686): z < A2, z > Nz+4-A2, x < A2, x > Nx+4-A2 (cells)
-        const bool bal = k < R.a2 || i < R.a2 || k > hz || (k == hz && fz > (real)0) || i > hx ||
-                         (i == hx && fx > (real)0);
-        if (!bal) {
-          if (i < 1 || k < 1 || i > R.gx - 2 || k > R.gz - 2) {
-            atomicAdd(err + ERR_DEPOSIT_OOB, 1ull);
-          } else {
-            const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-            // ex, bz: x aligned, z shifted; ez, bx: x shifted, z aligned; ey: both shifted; by: both aligned
-            real ex, ey, ez, bx, by, bz;
-            if (i - 1 >= wx0 && i + 1 < wx0 + WX && k - 1 >= wz0 && k + 1 < wz0 + WZ) {
-              const int xa = X.a - wx0, xb = X.b - wx0, za = Z.a - wz0, zb = Z.b - wz0;
-              ex = bil(fw + 0 * WN, WZ, xa, zb, X.a0, X.a1, Z.b0, Z.b1);
-              ey = bil(fw + 1 * WN, WZ, xb, zb, X.b0, X.b1, Z.b0, Z.b1);
-              ez = bil(fw + 2 * WN, WZ, xb, za, X.b0, X.b1, Z.a0, Z.a1);
-              bx = bil(fw + 3 * WN, WZ, xb, za, X.b0, X.b1, Z.a0, Z.a1);
-              by = bil(fw + 4 * WN, WZ, xa, za, X.a0, X.a1, Z.a0, Z.a1);
-              bz = bil(fw + 5 * WN, WZ, xa, zb, X.a0, X.a1, Z.b0, Z.b1);
+          ++pushed;
+          int i, k;
+          unpack2(c, i, k);
+          // ballistic margins (:682-686): z < A2, z > Nz+4-A2, x < A2, x > Nx+4-A2 (cells)
+          const bool bal = k < R.a2 || i < R.a2 || k > hz || (k == hz && fz > (real)0) || i > hx ||
+                           (i == hx && fx > (real)0);
+          if (!bal) {
+            if (i < 1 || k < 1 || i > R.gx - 2 || k > R.gz - 2) {
+              atomicAdd(err + ERR_DEPOSIT_OOB, 1ull);
             } else {
-              ex = bil(F0 + (long long)P_EX * R.nodes, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
-              ey = bil(F0 + (long long)P_EY * R.nodes, G, X.b, Z.b, X.b0, X.b1, Z.b0, Z.b1);
-              ez = bil(F0 + (long long)P_EZ * R.nodes, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
-              bx = bil(F0 + (long long)P_BX * R.nodes, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
-              by = bil(F0 + (long long)P_BY * R.nodes, G, X.a, Z.a, X.a0, X.a1, Z.a0, Z.a1);
-              bz = bil(F0 + (long long)P_BZ * R.nodes, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
+              const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+              // ex, bz: x aligned, z shifted; ez, bx: x shifted, z aligned; ey: both shifted; by: both aligned
+              real ex, ey, ez, bx, by, bz;
+              if (i - 1 >= wx0 && i + 1 < wx0 + WX && k - 1 >= wz0 && k + 1 < wz0 + WZ) {
+                const int xa = X.a - wx0, xb = X.b - wx0, za = Z.a - wz0, zb = Z.b - wz0;
+                ex = bil(fw + 0 * WN, WZ, xa, zb, X.a0, X.a1, Z.b0, Z.b1);
+                ey = bil(fw + 1 * WN, WZ, xb, zb, X.b0, X.b1, Z.b0, Z.b1);
+                ez = bil(fw + 2 * WN, WZ, xb, za, X.b0, X.b1, Z.a0, Z.a1);
+                bx = bil(fw + 3 * WN, WZ, xb, za, X.b0, X.b1, Z.a0, Z.a1);
+                by = bil(fw + 4 * WN, WZ, xa, za, X.a0, X.a1, Z.a0, Z.a1);
+                bz = bil(fw + 5 * WN, WZ, xa, zb, X.a0, X.a1, Z.b0, Z.b1);
+              } else {
+                ex = bil(F0 + (long long)P_EX * R.nodes, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
+                ey = bil(F0 + (long long)P_EY * R.nodes, G, X.b, Z.b, X.b0, X.b1, Z.b0, Z.b1);
+                ez = bil(F0 + (long long)P_EZ * R.nodes, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
+                bx = bil(F0 + (long long)P_BX * R.nodes, G, X.b, Z.a, X.b0, X.b1, Z.a0, Z.a1);
+                by = bil(F0 + (long long)P_BY * R.nodes, G, X.a, Z.a, X.a0, X.a1, Z.a0, Z.a1);
+                bz = bil(F0 + (long long)P_BZ * R.nodes, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
+              }
+              rotate_c4(T, ex + ex_add, ey + ey_add, ez, bx, by, bz, vx, vy, vz);
             }
-            rotate_c4(T, ex + ex_add, ey + ey_add, ez, bx, by, bz, vx, vy, vz);
           }
-        }
-        advance(i, fx, vx * hdt);
-        advance(k, fz, vz * hdt);
-        // J deposit at x^{n+1/2} for dx <= x < (Nx+3) dx, 2 dx <= z < (Nz+2) dx
-        if (i == hi && k == hk) {
-          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-          real xb[3], zb[3];
-          spread3(X, hi, xb);
-          spread3(Z, hk, zb);
-          const real px0 = qn * vx * X.a0, px1 = qn * vx * X.a1;
-#pragma unroll
-          for (int cc = 0; cc < 3; ++cc) {
-            h.jx[0][cc] += px0 * zb[cc];
-            h.jx[1][cc] += px1 * zb[cc];
-          }
-#pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            const real py = qn * vy * xb[b], pz = qn * vz * xb[b];
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc) h.jy[b][cc] += py * zb[cc];
-            h.jz[b][0] += pz * Z.a0;
-            h.jz[b][1] += pz * Z.a1;
-          }
-        } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
-          if constexpr (kQueue) {
-            qj = true;
-            jc = pack2(i, k);
-            jfx = fx;
-            jfz = fz;
-          } else {
+          advance(i, fx, vx * hdt);
+          advance(k, fz, vz * hdt);
+          // J deposit at x^{n+1/2} for dx <= x < (Nx+3) dx, 2 dx <= z < (Nz+2) dx
+          if (i == hi && k == hk) {
             const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-            dep4(pj(0), G, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1);
-            dep4(pj(1), G, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1);
-            dep4(pj(2), G, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1);
+            real xb[3], zb[3];
+            spread3(X, hi, xb);
+            spread3(Z, hk, zb);
+            const real px0 = qn * vx * X.a0, px1 = qn * vx * X.a1;
+  #pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+              h.jx[0][cc] += px0 * zb[cc];
+              h.jx[1][cc] += px1 * zb[cc];
+            }
+  #pragma unroll
+            for (int b = 0; b < 3; ++b) {
+              const real py = qn * vy * xb[b], pz = qn * vz * xb[b];
+  #pragma unroll
+              for (int cc = 0; cc < 3; ++cc) h.jy[b][cc] += py * zb[cc];
+              h.jz[b][0] += pz * Z.a0;
+              h.jz[b][1] += pz * Z.a1;
+            }
+          } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
+            if constexpr (kQueue) {
+              qj = true;
+              jc = pack2(i, k);
+              jfx = fx;
+              jfz = fz;
+            } else {
+              const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+              dep4(pj(0), G, X.a, Z.b, qn * vx, X.a0, X.a1, Z.b0, Z.b1);
+              dep4(pj(1), G, X.b, Z.b, qn * vy, X.b0, X.b1, Z.b0, Z.b1);
+              dep4(pj(2), G, X.b, Z.a, qn * vz, X.b0, X.b1, Z.a0, Z.a1);
+            }
           }
-        }
-        advance(i, fx, vx * hdt);
-        advance(k, fz, vz * hdt);
-        // n at x^{n+1}, same range
-        if (i == hi && k == hk) {
-          const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-          real xb[3], zb[3];
-          spread3(X, hi, xb);
-          spread3(Z, hk, zb);
-#pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            const real pn = nw * xb[b];
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc) h.n[b][cc] += pn * zb[cc];
-          }
-        } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
-          if constexpr (kQueue) {
-            qnn = true;
-            ncell = pack2(i, k);
-          } else {
+          advance(i, fx, vx * hdt);
+          advance(k, fz, vz * hdt);
+          // n at x^{n+1}, same range
+          if (i == hi && k == hk) {
             const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
-            dep4(pj(3), G, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1);
+            real xb[3], zb[3];
+            spread3(X, hi, xb);
+            spread3(Z, hk, zb);
+  #pragma unroll
+            for (int b = 0; b < 3; ++b) {
+              const real pn = nw * xb[b];
+  #pragma unroll
+              for (int cc = 0; cc < 3; ++cc) h.n[b][cc] += pn * zb[cc];
+            }
+          } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
+            if constexpr (kQueue) {
+              qnn = true;
+              ncell = pack2(i, k);
+            } else {
+              const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
+              dep4(pj(3), G, X.b, Z.b, nw, X.b0, X.b1, Z.b0, Z.b1);
+            }
           }
-        }
-        // x exchange at size 1: forward crossers wrap, backward ones are dropped; then removal
-        if (i == R.nx + 2 && k >= 2 && k < R.nz + 2) i -= R.nx;
-        const bool keep = i >= 2 && i < R.nx + 2 && k >= 2 && k < R.nz + 2;
-        P.cell[t] = keep ? pack2(i, k) : -1;
-        P.ox[t] = fx; P.oz[t] = fz;
-        P.vx[t] = vx; P.vy[t] = vy; P.vz[t] = vz;
+          // x exchange at size 1: forward crossers wrap, backward ones are dropped; then removal
+          if (i == R.nx + 2 && k >= 2 && k < R.nz + 2) i -= R.nx;
+          const bool keep = i >= 2 && i < R.nx + 2 && k >= 2 && k < R.nz + 2;
+          P.cell[t] = keep ? pack2(i, k) : -1;
+          P.ox[t] = fx; P.oz[t] = fz;
+          P.vx[t] = vx; P.vy[t] = vy; P.vz[t] = vz;
         }
         if constexpr (kQueue) {
           // warp-uniform: the row's queued lanes take consecutive entries, and
