@@ -30,6 +30,11 @@
 
 namespace pb {
 
+// rows (classify) and holes per lane (place_fill) whose loads are in flight together
+#ifndef PB_RELAYOUT_U
+#define PB_RELAYOUT_U 4
+#endif
+
 constexpr int kAppendBlock = 64;
 
 template <typename real>
@@ -41,7 +46,7 @@ template <typename real>
 __global__ void classify_kernel(Parts<real> P, Geom g, TileGeom t, const int* __restrict__ goff,
                                 const int* __restrict__ gmax, int cap, int* holes, int* nholes,
                                 int* append_at, int* nonhome) {
-  constexpr int U = 4;  // rows whose loads are in flight together
+  constexpr int U = PB_RELAYOUT_U;  // rows whose loads are in flight together
   const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (G >= t.ngroups) return;  // warp-uniform
@@ -166,7 +171,7 @@ __global__ void place_fill_kernel(Parts<real> P, int first, Geom g, TileGeom t, 
                                   const int* __restrict__ holes, const int* __restrict__ arrivals,
                                   const int* __restrict__ nholes, const int* __restrict__ off,
                                   const int* __restrict__ bucket) {
-  constexpr int U = 4;
+  constexpr int U = PB_RELAYOUT_U;  // holes per lane in flight together
   const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (G >= t.ngroups) return;  // warp-uniform
