@@ -51,6 +51,8 @@ struct Store {
   int* holes = nullptr;   // per-slot scratch: hole rows of every lane column
   int* nholes = nullptr;  // per interior cell: holes of its lane column
   int* nonhome = nullptr; // a particle outside its home cell stayed in the layout
+  // a refill's shell deletion over the layout is left to the next classify pass
+  bool shell_pending = false;
 };
 
 // Device blocks of the adjoint runs: each block is allocated on first need,
@@ -889,8 +891,10 @@ int relayout_launch(pic_ctx* c, int s) {
   CKL();
   classify_kernel<real><<<gblocks, kThreads, 0, c->stream>>>(P, c->g, tg, c->goff[s][c->lay[s]],
                                                              c->gmax[s][c->lay[s]], (int)st.cap, st.holes,
-                                                             st.nholes, c->append_dev, st.nonhome);
+                                                             st.nholes, c->append_dev, st.nonhome,
+                                                             st.shell_pending ? 1 : 0);
   CKL();
+  st.shell_pending = false;
   clamp_count_kernel<<<1, 1, 0, c->stream>>>(c->append_dev, (int)st.cap, st.count_dev);
   CKL();
   return place_launch<real>(c, s);
@@ -1032,9 +1036,12 @@ int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0
 
 
 // add_*_flat: the shell deletion, then the refill appended (the next step's
-// re-layout moves it into the layout).
+// re-layout moves it into the layout). With `fused` (pic_step, whose re-layout
+// follows in the same step), the deletion over a species' layout is left to
+// that re-layout's classify pass, which reads every slot of the layout anyway;
+// the slots after the layout are cleared here.
 template <typename real>
-int do_add_flat(pic_ctx* c) {
+int do_add_flat(pic_ctx* c, bool fused = false) {
   Slab slabs[5];
   const int nslab = refill_slabs(c, slabs);
   for (int s = 0; s < 2; ++s) {
@@ -1042,9 +1049,16 @@ int do_add_flat(pic_ctx* c) {
     const Parts<real> P = parts<real>(c, s);
     CKR(check_spill<real>(c, s, true));
     CKR(sync_count(c, s));
-    if (st.count > 0) {
-      delete_shell_kernel<real><<<particle_blocks(st.count), kThreads, 0, c->stream>>>(P, 0, st.count_dev, c->g);
+    const bool defer = fused && c->layout[s] && !c->cfg.slot_order;
+    const long long first = defer ? c->tiled_end[s] : 0;
+    if (st.count > first) {
+      delete_shell_kernel<real><<<particle_blocks(st.count - first), kThreads, 0, c->stream>>>(P, (int)first,
+                                                                                              st.count_dev, c->g);
       CKL();
+    }
+    if (defer) {
+      st.shell_pending = true;
+      c->tiled[s] = false;  // the re-layout runs this step, refill or not
     }
     CKR(do_source<real>(c, s, slabs, nslab));  // appended; the next step's re-layout places them
   }
@@ -1179,7 +1193,7 @@ int do_step(pic_ctx* c) {
   }
   if (c->c_add > c->cfg.add_interval - 1) {
     CKR(phase_mark(c, PH_ADD));
-    CKR(do_add_flat<real>(c));
+    CKR(do_add_flat<real>(c, true));
     CKR(phase_mark(c, PH_ADD));
     c->c_add = 0;
   }
@@ -1802,7 +1816,7 @@ int pic_sr_particle(pic_ctx* c) {
 
 int pic_add_flat(pic_ctx* c) {
   CKR(check_ctx(c));
-  return DISPATCH(c, do_add_flat)(c);
+  return DISPATCH(c, do_add_flat)(c, false);
 }
 
 int pic_sort(pic_ctx* c) {
@@ -1892,7 +1906,7 @@ int pic_fdtd(pic_ctx* c, int nsteps) {
   if (!c->grid_ready) return PIC_ERR_STATE;
   c->c_add = 0;
   c->c_thrust = 0;
-  CKR(DISPATCH(c, do_add_flat)(c));
+  CKR(DISPATCH(c, do_add_flat)(c, false));
   if (c->cfg.poisson_clean) CKR(DISPATCH(c, do_poisson)(c));  // :676-681
   return pic_step(c, nsteps);
 }

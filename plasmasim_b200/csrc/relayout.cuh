@@ -30,11 +30,6 @@
 
 namespace pb {
 
-// rows (classify) and holes per lane (place_fill) whose loads are in flight together
-#ifndef PB_RELAYOUT_U
-#define PB_RELAYOUT_U 4
-#endif
-
 constexpr int kAppendBlock = 64;
 
 template <typename real>
@@ -42,11 +37,14 @@ __device__ __forceinline__ void copy_slot(const Parts<real>& S, int s, const Par
   copy_record(S, s, D, d, c);
 }
 
+// With `shell` set (the re-layout after a refill), a particle of the layout
+// that lies in a refill shell is deleted here, as add_*_flat's removal
+// (:6015-6031) would have: one pass over the layout for both.
 template <typename real>
 __global__ void classify_kernel(Parts<real> P, Geom g, TileGeom t, const int* __restrict__ goff,
                                 const int* __restrict__ gmax, int cap, int* holes, int* nholes,
-                                int* append_at, int* nonhome) {
-  constexpr int U = PB_RELAYOUT_U;  // rows whose loads are in flight together
+                                int* append_at, int* nonhome, int shell) {
+  constexpr int U = 4;  // rows whose loads are in flight together (8 measured no faster)
   const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (G >= t.ngroups) return;  // warp-uniform
@@ -60,6 +58,16 @@ __global__ void classify_kernel(Parts<real> P, Geom g, TileGeom t, const int* __
     bool moved[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) c[u] = r0 + u < m ? P.cell[base + (r0 + u) * kLanes + lane] : -1;
+    if (shell) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const long long tu = base + (r0 + u) * kLanes + lane;
+        if (c[u] >= 0 && in_refill_shell(P, g, c[u], tu)) {
+          P.cell[tu] = -1;
+          c[u] = -1;
+        }
+      }
+    }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int r = r0 + u;
@@ -171,7 +179,7 @@ __global__ void place_fill_kernel(Parts<real> P, int first, Geom g, TileGeom t, 
                                   const int* __restrict__ holes, const int* __restrict__ arrivals,
                                   const int* __restrict__ nholes, const int* __restrict__ off,
                                   const int* __restrict__ bucket) {
-  constexpr int U = PB_RELAYOUT_U;  // holes per lane in flight together
+  constexpr int U = 4;  // holes per lane in flight together
   const int G = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (G >= t.ngroups) return;  // warp-uniform
