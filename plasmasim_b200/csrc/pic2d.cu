@@ -1170,8 +1170,7 @@ struct pic2d_batch {
   Item* src_items[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [init/add][species]
   int n_src[2][2] = {{0, 0}, {0, 0}};
   SourceSet* sets[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-  int* flags = nullptr;
-  int* pos = nullptr;
+  int* perm = nullptr;   // cell sort: the source slot of every destination slot (pool_slots)
   int* scan_tmp = nullptr;
   size_t scan_len = 0;
   int* ccnt = nullptr;   // cell sort: particles per cell and cursors (rho_len each)
@@ -1676,7 +1675,7 @@ int cellsort(pic2d_batch* b) {
     CKR2(scan_excl(b, b->gsz, goff, b->ngroups + 1, b->scan_tmp, b->scan_len));
     // the destinations: the empty slots first (perm -1), since the scatter then
     // fills some of them with other cells' particles; then the move
-    int* perm = b->flags;
+    int* perm = b->perm;
     pad2d_kernel<real><<<gblocks, 256, 0, b->stream>>>(perm, R, b->grun, b->ngroups, goff, gmax, b->ccnt);
     CKL2();
     CK2(cudaMemsetAsync(b->gover, 0, sizeof(int) * (size_t)std::max(b->ngroups, 1), b->stream));
@@ -2075,8 +2074,7 @@ int do_create(pic2d_batch* b) {
       CKR2(upload(it, &b->src_items[which][s], &b->n_src[which][s]));
     }
   }
-  CK2(cudaMalloc(&b->flags, sizeof(int) * (size_t)poff));
-  CK2(cudaMalloc(&b->pos, sizeof(int) * (size_t)poff));
+  CK2(cudaMalloc(&b->perm, sizeof(int) * (size_t)poff));
   b->scan_len = (size_t)(2 * ((poff + kScanTile - 1) / kScanTile) + 64);
   CK2(cudaMalloc(&b->scan_tmp, sizeof(int) * b->scan_len));
   CK2(cudaMalloc(&b->ccnt, sizeof(int) * (size_t)std::max(b->rho_len, 1LL)));
@@ -2106,7 +2104,7 @@ void free_batch(pic2d_batch* b) {
   cudaFree(b->row_items); cudaFree(b->rho_items); cudaFree(b->part_items); cudaFree(b->tile_items);
   for (int w = 0; w < 2; ++w)
     for (int s = 0; s < 2; ++s) { cudaFree(b->src_items[w][s]); cudaFree(b->sets[w][s]); }
-  cudaFree(b->flags); cudaFree(b->pos); cudaFree(b->scan_tmp); cudaFree(b->step_dev); cudaFree(b->err);
+  cudaFree(b->perm); cudaFree(b->scan_tmp); cudaFree(b->step_dev); cudaFree(b->err);
   cudaFree(b->ccnt); cudaFree(b->ccur); cudaFree(b->gfree); cudaFree(b->gover); cudaFree(b->hcnt);
   cudaFree(b->grun); cudaFree(b->gsz); cudaFree(b->ptile_items);
   for (int p = 0; p < 2; ++p)
