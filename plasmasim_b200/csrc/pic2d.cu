@@ -390,6 +390,49 @@ __device__ __forceinline__ real bil(const real* P, int G, int i, int k, real x0,
          (P[i * G + k + 1] * (x0 * z1) + P[(i + 1) * G + k + 1] * (x1 * z1));
 }
 
+// E and B at a particle from a window of one plane per component (ex ey ez
+// bx by bz, WN nodes each, z rows of WZ nodes; window coordinates of the
+// stencil bases): bil's arithmetic in FP64. In FP32 the two x nodes of each
+// stencil row travel as one packed pair through two-wide multiplies and FMAs
+// (0.2 ms per step off the 256-run batch against bil's scalar form).
+template <typename real>
+struct EB2 {
+  real ex, ey, ez, bx, by, bz;
+};
+template <int WZ, int WN>
+__device__ __forceinline__ EB2<double> gather_win2(const double* fw, int xa, int xb, int za, int zb,
+                                                   const Ax2<double>& X, const Ax2<double>& Z) {
+  EB2<double> r;
+  r.ex = bil(fw + 0 * WN, WZ, xa, zb, X.a0, X.a1, Z.b0, Z.b1);
+  r.ey = bil(fw + 1 * WN, WZ, xb, zb, X.b0, X.b1, Z.b0, Z.b1);
+  r.ez = bil(fw + 2 * WN, WZ, xb, za, X.b0, X.b1, Z.a0, Z.a1);
+  r.bx = bil(fw + 3 * WN, WZ, xb, za, X.b0, X.b1, Z.a0, Z.a1);
+  r.by = bil(fw + 4 * WN, WZ, xa, za, X.a0, X.a1, Z.a0, Z.a1);
+  r.bz = bil(fw + 5 * WN, WZ, xa, zb, X.a0, X.a1, Z.b0, Z.b1);
+  return r;
+}
+template <int WZ>
+__device__ __forceinline__ float bil_pair(const float* P, int i, int k, float x0, float x1, float2 Z0, float2 Z1) {
+  const float2 n0 = make_float2(P[i * WZ + k], P[(i + 1) * WZ + k]);
+  const float2 n1 = make_float2(P[i * WZ + k + 1], P[(i + 1) * WZ + k + 1]);
+  const float2 cz = __ffma2_rn(n1, Z1, __fmul2_rn(n0, Z0));
+  return cz.x * x0 + cz.y * x1;
+}
+template <int WZ, int WN>
+__device__ __forceinline__ EB2<float> gather_win2(const float* fw, int xa, int xb, int za, int zb,
+                                                  const Ax2<float>& X, const Ax2<float>& Z) {
+  const float2 za0 = make_float2(Z.a0, Z.a0), za1 = make_float2(Z.a1, Z.a1);
+  const float2 zb0 = make_float2(Z.b0, Z.b0), zb1 = make_float2(Z.b1, Z.b1);
+  EB2<float> r;
+  r.ex = bil_pair<WZ>(fw + 0 * WN, xa, zb, X.a0, X.a1, zb0, zb1);
+  r.ey = bil_pair<WZ>(fw + 1 * WN, xb, zb, X.b0, X.b1, zb0, zb1);
+  r.ez = bil_pair<WZ>(fw + 2 * WN, xb, za, X.b0, X.b1, za0, za1);
+  r.bx = bil_pair<WZ>(fw + 3 * WN, xb, za, X.b0, X.b1, za0, za1);
+  r.by = bil_pair<WZ>(fw + 4 * WN, xa, za, X.a0, X.a1, za0, za1);
+  r.bz = bil_pair<WZ>(fw + 5 * WN, xa, zb, X.a0, X.a1, zb0, zb1);
+  return r;
+}
+
 template <typename real>
 __device__ __forceinline__ void dep4(real* P, int G, int i, int k, real v, real x0, real x1, real z0, real z1) {
   atomicAdd(P + i * G + k, v * (x0 * z0));
@@ -618,13 +661,8 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
               // ex, bz: x aligned, z shifted; ez, bx: x shifted, z aligned; ey: both shifted; by: both aligned
               real ex, ey, ez, bx, by, bz;
               if (i - 1 >= wx0 && i + 1 < wx0 + WX && k - 1 >= wz0 && k + 1 < wz0 + WZ) {
-                const int xa = X.a - wx0, xb = X.b - wx0, za = Z.a - wz0, zb = Z.b - wz0;
-                ex = bil(fw + 0 * WN, WZ, xa, zb, X.a0, X.a1, Z.b0, Z.b1);
-                ey = bil(fw + 1 * WN, WZ, xb, zb, X.b0, X.b1, Z.b0, Z.b1);
-                ez = bil(fw + 2 * WN, WZ, xb, za, X.b0, X.b1, Z.a0, Z.a1);
-                bx = bil(fw + 3 * WN, WZ, xb, za, X.b0, X.b1, Z.a0, Z.a1);
-                by = bil(fw + 4 * WN, WZ, xa, za, X.a0, X.a1, Z.a0, Z.a1);
-                bz = bil(fw + 5 * WN, WZ, xa, zb, X.a0, X.a1, Z.b0, Z.b1);
+                const EB2<real> e = gather_win2<WZ, WN>(fw, X.a - wx0, X.b - wx0, Z.a - wz0, Z.b - wz0, X, Z);
+                ex = e.ex; ey = e.ey; ez = e.ez; bx = e.bx; by = e.by; bz = e.bz;
               } else {
                 ex = bil(F0 + (long long)P_EX * R.nodes, G, X.a, Z.b, X.a0, X.a1, Z.b0, Z.b1);
                 ey = bil(F0 + (long long)P_EY * R.nodes, G, X.b, Z.b, X.b0, X.b1, Z.b0, Z.b1);
