@@ -960,8 +960,9 @@ __global__ void phi_rho_kernel(real* F, const Run<real>* __restrict__ runs, cons
 }
 
 // Batched small GEMM C = alpha * op(A B) over every run (row-major, the run's
-// sizes): 64x64 output tiles, 256 threads of 4x4 outputs each, K staged
-// through shared memory 32 at a time. mode selects the operands of the four
+// sizes): 64x64 output tiles, 256 threads of 4x4 outputs each (4 consecutive
+// rows by 4 consecutive columns, read from the staged tiles as 4-wide vector
+// loads), K staged through shared memory 32 at a time, both tiles k-major. mode selects the operands of the four
 // sine transforms:
 //  0: C[nx][nz] = A[nx][nz] * S_nz        (transform along z)
 //  1: C[nx][nz] = S_nx * A[nx][nz], then / eigenvalue  (along x, solve)
@@ -970,14 +971,22 @@ __global__ void phi_rho_kernel(real* F, const Run<real>* __restrict__ runs, cons
 // S_n[i][j] = sin(pi i j / n); its row and column 0 vanish, so the transforms
 // skip the first element as the reference's sinft does (y[1] = 0, :2902).
 constexpr int kGemmTile = 64;
+__device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
+  const float4 q = *reinterpret_cast<const float4*>(p);
+  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&v)[4]) {
+  const double2 q0 = reinterpret_cast<const double2*>(p)[0], q1 = reinterpret_cast<const double2*>(p)[1];
+  v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+}
 template <typename real>
 __global__ void __launch_bounds__(256) dst_gemm_kernel(const Run<real>* __restrict__ runs, const Item* __restrict__ items,
                                                        int nitems, const real* __restrict__ A, real* C,
                                                        const real* __restrict__ sines, int mode) {
   constexpr int T = kGemmTile, KT = 32;
-  __shared__ real As[T][KT + 1];  // [row of C][k]
-  __shared__ real Bs[KT][T + 1];  // [k][col of C]
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16; outputs (ty + 16 u, tx + 16 v)
+  __shared__ __align__(16) real As[KT][T + 4];  // [k][row of C]
+  __shared__ __align__(16) real Bs[KT][T + 4];  // [k][col of C]
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16; outputs (4 ty + u, 4 tx + v)
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const Run<real>& R = runs[items[it].run];
     const int nx = R.nx, nz = R.nz;
@@ -998,7 +1007,10 @@ __global__ void __launch_bounds__(256) dst_gemm_kernel(const Run<real>* __restri
       __syncthreads();  // the last tile's reads are done
       // left operand tile [T rows of C][KT of K], right operand tile [KT of K][T cols of C]
       for (int q = threadIdx.x; q < T * KT; q += blockDim.x) {
-        const int r = q / KT, kc = q % KT;  // left: row r, column k0 + kc
+        // left: a warp takes 4 rows x 8 consecutive k (coalesced reads; its
+        // transposed stores fall on 32 different banks)
+        const int ch = q >> 5, l = q & 31;
+        const int r = 4 * (ch % (T / 4)) + (l >> 3), kc = 8 * (ch / (T / 4)) + (l & 7);
         const int row = ti * T + r, kk = k0 + kc;
         real lv = 0;
         if (left) {
@@ -1006,7 +1018,7 @@ __global__ void __launch_bounds__(256) dst_gemm_kernel(const Run<real>* __restri
         } else {
           if (row < nx && kk < nz) lv = a[(long long)row * nz + kk];
         }
-        As[r][kc] = lv;
+        As[kc][r] = lv;
         const int kr = q / T, cc = q % T;  // right: row k0 + kr, column cc
         const int krow = k0 + kr, col = tj * T + cc;
         real rv = 0;
@@ -1021,10 +1033,8 @@ __global__ void __launch_bounds__(256) dst_gemm_kernel(const Run<real>* __restri
 #pragma unroll 8
       for (int kk = 0; kk < KT; ++kk) {
         real av[4], bv[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) av[u] = As[ty + 16 * u][kk];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) bv[v] = Bs[kk][tx + 16 * v];
+        ld4(&As[kk][4 * ty], av);
+        ld4(&Bs[kk][4 * tx], bv);
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
@@ -1036,7 +1046,7 @@ __global__ void __launch_bounds__(256) dst_gemm_kernel(const Run<real>* __restri
     for (int u = 0; u < 4; ++u)
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        const int row = ti * T + ty + 16 * u, col = tj * T + tx + 16 * v;
+        const int row = ti * T + 4 * ty + u, col = tj * T + 4 * tx + v;
         if (row >= nx || col >= nz) continue;
         real w = acc[u][v];
         if (mode == 1) {
