@@ -497,7 +497,94 @@ __device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_g
 // x nodes hi-1 .. hi+1 and z nodes hk, hk+1.
 template <typename real>
 struct Home2 {
-  real jx[2][3], jy[3][3], jz[3][2], n[3][3];
+  real jx_[2][3], jy_[3][3], jz_[3][2], n_[3][3];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        jy_[a][c] = n_[a][c] = (real)0;
+        if (a < 2) jx_[a][c] = (real)0;
+        if (c < 2) jz_[a][c] = (real)0;
+      }
+  }
+  // J of one particle with charge weight q, x-aligned weights (X.a0, X.a1),
+  // z-aligned (Z.a0, Z.a1) and half-shifted weights xb, zb over the 3 nodes
+  __device__ __forceinline__ void add_j(real q, real vx, real vy, real vz, const Ax2<real>& X, const Ax2<real>& Z,
+                                        const real (&xb)[3], const real (&zb)[3]) {
+    const real px0 = q * vx * X.a0, px1 = q * vx * X.a1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      jx_[0][c] += px0 * zb[c];
+      jx_[1][c] += px1 * zb[c];
+    }
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const real py = q * vy * xb[b], pz = q * vz * xb[b];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) jy_[b][c] += py * zb[c];
+      jz_[b][0] += pz * Z.a0;
+      jz_[b][1] += pz * Z.a1;
+    }
+  }
+  __device__ __forceinline__ void add_n(real w, const real (&xb)[3], const real (&zb)[3]) {
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const real pn = w * xb[b];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) n_[b][c] += pn * zb[c];
+    }
+  }
+  __device__ __forceinline__ real jx(int a, int c) const { return jx_[a][c]; }
+  __device__ __forceinline__ real jy(int b, int c) const { return jy_[b][c]; }
+  __device__ __forceinline__ real jz(int b, int c) const { return jz_[b][c]; }
+  __device__ __forceinline__ real n(int b, int c) const { return n_[b][c]; }
+};
+
+// FP32: pairs of sums updated with the two-wide multiplies and FMAs of sm_100
+// (jx over its two x nodes, jz over its two z nodes, jy and n over the first
+// two x nodes beside a scalar third).
+template <>
+struct Home2<float> {
+  float2 jx_[3], jy01_[3], jz_[3], n01_[3];  // jx_[c] = (a 0, a 1); jy01_[c] = (b 0, b 1); jz_[b] = (c 0, c 1)
+  float jy2_[3], n2_[3];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      jx_[c] = jy01_[c] = jz_[c] = n01_[c] = make_float2(0.f, 0.f);
+      jy2_[c] = n2_[c] = 0.f;
+    }
+  }
+  __device__ __forceinline__ void add_j(float q, float vx, float vy, float vz, const Ax2<float>& X,
+                                        const Ax2<float>& Z, const float (&xb)[3], const float (&zb)[3]) {
+    const float qx = q * vx, qy = q * vy, qz = q * vz;
+    const float2 px = __fmul2_rn(make_float2(qx, qx), make_float2(X.a0, X.a1));
+    const float2 py = __fmul2_rn(make_float2(qy, qy), make_float2(xb[0], xb[1]));
+    const float py2 = qy * xb[2];
+    const float2 za = make_float2(Z.a0, Z.a1);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float2 zc = make_float2(zb[c], zb[c]);
+      jx_[c] = __ffma2_rn(px, zc, jx_[c]);
+      jy01_[c] = __ffma2_rn(py, zc, jy01_[c]);
+      jy2_[c] = fmaf(py2, zb[c], jy2_[c]);
+      const float pz = qz * xb[c];
+      jz_[c] = __ffma2_rn(make_float2(pz, pz), za, jz_[c]);
+    }
+  }
+  __device__ __forceinline__ void add_n(float w, const float (&xb)[3], const float (&zb)[3]) {
+    const float2 pn = __fmul2_rn(make_float2(w, w), make_float2(xb[0], xb[1]));
+    const float pn2 = w * xb[2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      n01_[c] = __ffma2_rn(pn, make_float2(zb[c], zb[c]), n01_[c]);
+      n2_[c] = fmaf(pn2, zb[c], n2_[c]);
+    }
+  }
+  __device__ __forceinline__ float jx(int a, int c) const { return a ? jx_[c].y : jx_[c].x; }
+  __device__ __forceinline__ float jy(int b, int c) const { return b == 2 ? jy2_[c] : b ? jy01_[c].y : jy01_[c].x; }
+  __device__ __forceinline__ float jz(int b, int c) const { return c ? jz_[b].y : jz_[b].x; }
+  __device__ __forceinline__ float n(int b, int c) const { return b == 2 ? n2_[c] : b ? n01_[c].y : n01_[c].x; }
 };
 
 // The half-shifted weights (b0, b1) of a particle of home cell h over the
@@ -584,14 +671,7 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
       const real ex_add = (real)RR.ex_add, ey_add = (real)RR.ey_add;
       const int hz = R.nz + 4 - R.a2, hx = R.nx + 4 - R.a2;
       Home2<real> h;
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          h.jy[a][c] = h.n[a][c] = (real)0;
-          if (a < 2) h.jx[a][c] = (real)0;
-          if (c < 2) h.jz[a][c] = (real)0;
-        }
+      h.zero();
       // each lane copies and reads only its own slots, so the per-thread
       // cp.async groups need no warp barrier
       auto fetch = [&](int row) {
@@ -687,20 +767,7 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
             real xb[3], zb[3];
             spread3(X, hi, xb);
             spread3(Z, hk, zb);
-            const real px0 = qn * vx * X.a0, px1 = qn * vx * X.a1;
-  #pragma unroll
-            for (int cc = 0; cc < 3; ++cc) {
-              h.jx[0][cc] += px0 * zb[cc];
-              h.jx[1][cc] += px1 * zb[cc];
-            }
-  #pragma unroll
-            for (int b = 0; b < 3; ++b) {
-              const real py = qn * vy * xb[b], pz = qn * vz * xb[b];
-  #pragma unroll
-              for (int cc = 0; cc < 3; ++cc) h.jy[b][cc] += py * zb[cc];
-              h.jz[b][0] += pz * Z.a0;
-              h.jz[b][1] += pz * Z.a1;
-            }
+            h.add_j(qn, vx, vy, vz, X, Z, xb, zb);
           } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
             if constexpr (kQueue) {
               qj = true;
@@ -722,12 +789,7 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
             real xb[3], zb[3];
             spread3(X, hi, xb);
             spread3(Z, hk, zb);
-  #pragma unroll
-            for (int b = 0; b < 3; ++b) {
-              const real pn = nw * xb[b];
-  #pragma unroll
-              for (int cc = 0; cc < 3; ++cc) h.n[b][cc] += pn * zb[cc];
-            }
+            h.add_n(nw, xb, zb);
           } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
             if constexpr (kQueue) {
               qnn = true;
@@ -790,10 +852,10 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
 #pragma unroll
           for (int cc = 0; cc < 3; ++cc) {
             const int node = (hi - 1 + a) * G + (hk - 1 + cc);
-            if (a < 2 && h.jx[a][cc] != (real)0) atomicAdd(pj(0) + node + G, h.jx[a][cc]);
-            if (h.jy[a][cc] != (real)0) atomicAdd(pj(1) + node, h.jy[a][cc]);
-            if (cc < 2 && h.jz[a][cc] != (real)0) atomicAdd(pj(2) + node + 1, h.jz[a][cc]);
-            if (h.n[a][cc] != (real)0) atomicAdd(pj(3) + node, h.n[a][cc]);
+            if (a < 2 && h.jx(a, cc) != (real)0) atomicAdd(pj(0) + node + G, h.jx(a, cc));
+            if (h.jy(a, cc) != (real)0) atomicAdd(pj(1) + node, h.jy(a, cc));
+            if (cc < 2 && h.jz(a, cc) != (real)0) atomicAdd(pj(2) + node + 1, h.jz(a, cc));
+            if (h.n(a, cc) != (real)0) atomicAdd(pj(3) + node, h.n(a, cc));
           }
       }
     }
