@@ -508,11 +508,11 @@ struct Home2 {
         if (c < 2) jz_[a][c] = (real)0;
       }
   }
-  // J of one particle with charge weight q, x-aligned weights (X.a0, X.a1),
-  // z-aligned (Z.a0, Z.a1) and half-shifted weights xb, zb over the 3 nodes
-  __device__ __forceinline__ void add_j(real q, real vx, real vy, real vz, const Ax2<real>& X, const Ax2<real>& Z,
+  // J of one particle with charge weight q, x-aligned weights (xa0, xa1),
+  // z-aligned (za0, za1) and half-shifted weights xb, zb over the 3 nodes
+  __device__ __forceinline__ void add_j(real q, real vx, real vy, real vz, real xa0, real xa1, real za0, real za1,
                                         const real (&xb)[3], const real (&zb)[3]) {
-    const real px0 = q * vx * X.a0, px1 = q * vx * X.a1;
+    const real px0 = q * vx * xa0, px1 = q * vx * xa1;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       jx_[0][c] += px0 * zb[c];
@@ -523,8 +523,8 @@ struct Home2 {
       const real py = q * vy * xb[b], pz = q * vz * xb[b];
 #pragma unroll
       for (int c = 0; c < 3; ++c) jy_[b][c] += py * zb[c];
-      jz_[b][0] += pz * Z.a0;
-      jz_[b][1] += pz * Z.a1;
+      jz_[b][0] += pz * za0;
+      jz_[b][1] += pz * za1;
     }
   }
   __device__ __forceinline__ void add_n(real w, const real (&xb)[3], const real (&zb)[3]) {
@@ -555,13 +555,13 @@ struct Home2<float> {
       jy2_[c] = n2_[c] = 0.f;
     }
   }
-  __device__ __forceinline__ void add_j(float q, float vx, float vy, float vz, const Ax2<float>& X,
-                                        const Ax2<float>& Z, const float (&xb)[3], const float (&zb)[3]) {
+  __device__ __forceinline__ void add_j(float q, float vx, float vy, float vz, float xa0, float xa1, float za0,
+                                        float za1, const float (&xb)[3], const float (&zb)[3]) {
     const float qx = q * vx, qy = q * vy, qz = q * vz;
-    const float2 px = __fmul2_rn(make_float2(qx, qx), make_float2(X.a0, X.a1));
+    const float2 px = __fmul2_rn(make_float2(qx, qx), make_float2(xa0, xa1));
     const float2 py = __fmul2_rn(make_float2(qy, qy), make_float2(xb[0], xb[1]));
     const float py2 = qy * xb[2];
-    const float2 za = make_float2(Z.a0, Z.a1);
+    const float2 za = make_float2(za0, za1);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const float2 zc = make_float2(zb[c], zb[c]);
@@ -595,6 +595,20 @@ __device__ __forceinline__ void spread3(const Ax2<real>& A, int h, real (&w)[3])
   w[0] = lo ? A.b0 : (real)0;
   w[1] = lo ? A.b1 : A.b0;
   w[2] = lo ? (real)0 : A.b1;
+}
+// FP32: the same three weights straight from the offset f of a particle in
+// its home cell (an interior cell, so never cell 0): with g = f - 1/2 they are
+// (max(-g, 0), 1 - |g|, max(g, 0)), equal to spread3's to within a rounding.
+template <typename real>
+__device__ __forceinline__ void home_w3(int i, real f, int h, real (&w)[3]) {
+  if constexpr (sizeof(real) == 4) {
+    const float g = f - 0.5f;
+    w[0] = fmaxf(-g, 0.f);
+    w[1] = 1.f - fabsf(g);
+    w[2] = fmaxf(g, 0.f);
+  } else {
+    spread3(ax2(i, f), h, w);
+  }
 }
 
 // The particle part of one step for every run and species (the push loop,
@@ -763,11 +777,10 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
           advance(k, fz, vz * hdt);
           // J deposit at x^{n+1/2} for dx <= x < (Nx+3) dx, 2 dx <= z < (Nz+2) dx
           if (i == hi && k == hk) {
-            const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
             real xb[3], zb[3];
-            spread3(X, hi, xb);
-            spread3(Z, hk, zb);
-            h.add_j(qn, vx, vy, vz, X, Z, xb, zb);
+            home_w3(i, fx, hi, xb);
+            home_w3(k, fz, hk, zb);
+            h.add_j(qn, vx, vy, vz, (real)1 - fx, fx, (real)1 - fz, fz, xb, zb);
           } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
             if constexpr (kQueue) {
               qj = true;
@@ -785,10 +798,9 @@ __global__ void __launch_bounds__(TX * 32, (sizeof(real) == 4 ? 512 : 256) / (TX
           advance(k, fz, vz * hdt);
           // n at x^{n+1}, same range
           if (i == hi && k == hk) {
-            const Ax2<real> X = ax2(i, fx), Z = ax2(k, fz);
             real xb[3], zb[3];
-            spread3(X, hi, xb);
-            spread3(Z, hk, zb);
+            home_w3(i, fx, hi, xb);
+            home_w3(k, fz, hk, zb);
             h.add_n(nw, xb, zb);
           } else if (i >= 1 && i < R.nx + 3 && k >= 2 && k < R.nz + 2) {
             if constexpr (kQueue) {
