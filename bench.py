@@ -323,7 +323,8 @@ def batch2d_configs(nruns: int, seed: int = 7):
 
 def run_batch2d(nruns: int, steps: int, warmup: int):
     """Device-timed steps of the batched 2D workload (FP32), after init, the
-    online launch tuning and `warmup` further steps."""
+    online launch tuning and at least `warmup` further steps: at least `steps`
+    steps, rounded up to whole sort cycles."""
     import torch
 
     from plasmasim_b200 import Pic2DBatch
@@ -331,8 +332,12 @@ def run_batch2d(nruns: int, steps: int, warmup: int):
     cfgs = batch2d_configs(nruns)
     B = Pic2DBatch(cfgs, precision=32)
     B.init()
-    choice = B.autotune()
-    B.step(warmup)
+    choice = B.autotune()  # 16 steps of the runs themselves
+    # the timed window starts with a sort step and covers whole sort cycles,
+    # so that it holds each step of the cycle equally often
+    si = cfgs[0].sort_interval
+    B.step(warmup + (-(16 + warmup)) % si)
+    steps = -(-steps // si) * si
     stream = torch.cuda.ExternalStream(B.stream_handle())
     _, c0 = B.status()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

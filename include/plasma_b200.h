@@ -336,7 +336,8 @@ typedef struct pic2d_config {
   int absorb_grid3;        /* Absorb_grid3: margin left out of renew_phi's source (>= 2) */
   int sort_interval;       /* no reference counterpart: every run's particles are sorted by cell every
                               sort_interval steps (and at each refill), which changes only their order;
-                              0 sorts at refills only. The same for every run of a batch */
+                              0 sorts at refills only. The same for every run of a batch; 12 by
+                              default */
   double sigma_a;          /* damping amplitude a of init_grid (:228) */
   unsigned long long seed_p, seed_v;  /* position / velocity stream keys (:406-407: 0, 50) */
   long long capacity;      /* particle slots per species of this run; 0 sizes it */

@@ -57,7 +57,7 @@ class Pic2DConfig:
     absorb_grid: int = 32
     absorb_grid2: int = 16
     absorb_grid3: int = 32
-    sort_interval: int = 20
+    sort_interval: int = 12
     sigma_a: float = 1e-6
     seed_p: int = 0
     seed_v: int = 50
