@@ -336,8 +336,11 @@ def run_batch2d(nruns: int, steps: int, warmup: int):
     # the timed window starts with a sort step and covers whole sort cycles,
     # so that it holds each step of the cycle equally often
     si = cfgs[0].sort_interval
-    B.step(warmup + (-(16 + warmup)) % si)
-    steps = -(-steps // si) * si
+    if si > 0:
+        B.step(warmup + (-(16 + warmup)) % si)
+        steps = -(-steps // si) * si
+    else:  # sorts at refills only
+        B.step(warmup)
     stream = torch.cuda.ExternalStream(B.stream_handle())
     _, c0 = B.status()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
