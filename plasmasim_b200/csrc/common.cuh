@@ -167,11 +167,20 @@ __device__ __forceinline__ void split_coord(double xc, int& i, real& f) {
   }
 }
 
+// Whether t lies outside [0, 1) as one unsigned compare of its bits: every
+// value of [+0, 1) has a pattern below that of 1, every negative one a pattern
+// above, and so do -0 (which the slow path below turns into +0) and NaN
+// (which it leaves NaN).
+__device__ __forceinline__ bool off_unit(float t) { return __float_as_uint(t) >= 0x3f800000u; }
+__device__ __forceinline__ bool off_unit(double t) {
+  return (unsigned long long)__double_as_longlong(t) >= 0x3ff0000000000000ull;
+}
+
 // Adds a displacement d (in cells) to (i, f) keeping f in [0, 1).
 template <typename real>
 __device__ __forceinline__ void advance(int& i, real& f, real d) {
   real t = f + d;
-  if (t >= (real)1 || t < (real)0) {
+  if (off_unit(t)) {
     const real fl = floor(t);
     i += (int)fl;
     t -= fl;
