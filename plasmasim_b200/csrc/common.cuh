@@ -133,25 +133,58 @@ __host__ __device__ __forceinline__ double uniform53(uint64_t seed, uint64_t d) 
   return (double)m * (1.0 / 9007199254740992.0);
 }
 
+// The uniform53 values of draws d .. d + N - 1 of a stream with each Philox
+// block computed once: draw d is the 53 bits of words (0, 1) of block d >> 1
+// for even d and of words (2, 3) for odd d, so N consecutive draws need
+// N / 2 + 1 blocks at most instead of N. `odd` is d's parity; callers whose
+// d has the same parity in every thread of a launch keep the blocks uniform.
+__host__ __device__ __forceinline__ double u53_words(uint32_t a, uint32_t b) {
+  const uint64_t m = ((uint64_t)a << 21) | (uint64_t)(b >> 11);
+  return (double)m * (1.0 / 9007199254740992.0);
+}
+template <int N>
+__host__ __device__ __forceinline__ void uniform53_run(uint64_t seed, uint64_t d, double (&u)[N]) {
+  constexpr int kBlocks = N / 2 + 1;
+  uint32_t c[kBlocks][4];
+#pragma unroll
+  for (int q = 0; q < kBlocks; ++q) {
+    const uint64_t blk = (d >> 1) + (uint64_t)q;
+    c[q][0] = (uint32_t)blk;
+    c[q][1] = (uint32_t)(blk >> 32);
+    c[q][2] = 0u;
+    c[q][3] = 0u;
+    if (q < (N + (int)(d & 1) + 1) / 2) philox4x32_10(c[q], (uint32_t)seed, (uint32_t)(seed >> 32));
+  }
+  const int odd = (int)(d & 1);
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    const int w = q + odd;  // word pair of draw d + q, counted from block d >> 1
+    u[q] = (w & 1) ? u53_words(c[w >> 1][2], c[w >> 1][3]) : u53_words(c[w >> 1][0], c[w >> 1][1]);
+  }
+}
+
 #ifdef __CUDACC__
 // a*(1-u) + b*u rounded step by step (no contraction), as the host computes it.
 __device__ __forceinline__ double flat_rn(double a, double b, double u) {
   return __dadd_rn(__dmul_rn(a, __dadd_rn(1.0, -u)), __dmul_rn(b, u));
 }
 
-// Box-Muller from draws d and d+1 of a stream: sqrt(-2 ln(1-u1)) cos(2 pi u2).
-__device__ __forceinline__ double gauss_bm(uint64_t seed, uint64_t d) {
-  const double u1 = __dadd_rn(1.0, -uniform53(seed, d));
-  const double u2 = uniform53(seed, d + 1);
+// Box-Muller from two uniforms v1, v2 (draws d and d+1 of a stream):
+// sqrt(-2 ln(1-v1)) cos(2 pi v2).
+__device__ __forceinline__ double gauss_bm_u(double v1, double v2) {
+  const double u1 = __dadd_rn(1.0, -v1);
   const double r = sqrt(__dmul_rn(-2.0, log(u1)));
-  const double ang = __dmul_rn(__dmul_rn(2.0, 3.14159265358979323846), u2);
+  const double ang = __dmul_rn(__dmul_rn(2.0, 3.14159265358979323846), v2);
   return __dmul_rn(r, cos(ang));
+}
+__device__ __forceinline__ double gauss_bm(uint64_t seed, uint64_t d) {
+  return gauss_bm_u(uniform53(seed, d), uniform53(seed, d + 1));
 }
 
 // The same normal deviate from FP32 log/cos (for particles stored in FP32).
-__device__ __forceinline__ float gauss_bm_f32(uint64_t seed, uint64_t d) {
-  const float u1 = (float)__dadd_rn(1.0, -uniform53(seed, d));
-  const float u2 = (float)uniform53(seed, d + 1);
+__device__ __forceinline__ float gauss_bm_f32_u(double v1, double v2) {
+  const float u1 = (float)__dadd_rn(1.0, -v1);
+  const float u2 = (float)v2;
   return sqrtf(-2.0f * logf(u1)) * cosf(6.28318530717958647692f * u2);
 }
 

@@ -484,21 +484,24 @@ __device__ __forceinline__ void make_particle(const Parts<real>& P, const Source
       hi[a] = __dmul_rn((double)(cc[a] + 1), dx);
     }
   }
-  const double x = flat_rn(lo[0], hi[0], uniform53(sp.seed_p, dp));
-  const double y = flat_rn(lo[1], hi[1], uniform53(sp.seed_p, dp + 1));
-  const double z = flat_rn(lo[2], hi[2], uniform53(sp.seed_p, dp + 2));
+  double up[3], uv[6];  // the particle's 3 position and 6 velocity draws
+  uniform53_run<3>(sp.seed_p, dp, up);
+  const double x = flat_rn(lo[0], hi[0], up[0]);
+  const double y = flat_rn(lo[1], hi[1], up[1]);
+  const double z = flat_rn(lo[2], hi[2], up[2]);
   const uint64_t dv = (uint64_t)(sp.base_v + 6 * t);
+  uniform53_run<6>(sp.seed_v, dv, uv);
   real vx, vy, vz;
   if (sizeof(real) == 8) {  // the host's arithmetic, rounded step by step
-    const double g0 = gauss_bm(sp.seed_v, dv), g1 = gauss_bm(sp.seed_v, dv + 2), g2 = gauss_bm(sp.seed_v, dv + 4);
+    const double g0 = gauss_bm_u(uv[0], uv[1]), g1 = gauss_bm_u(uv[2], uv[3]), g2 = gauss_bm_u(uv[4], uv[5]);
     vx = (real)__dadd_rn(__dmul_rn(sp.lsig, g0), 0.0);
     vy = (real)__dadd_rn(__dmul_rn(sp.lsig, g1), 0.0);
     vz = (real)__dadd_rn(__dmul_rn(sp.lsig, g2), sp.vdrift);
   } else {  // the same draws through FP32 log/cos: the FP32 state's own precision
     const float ls = (float)sp.lsig;
-    vx = (real)(ls * gauss_bm_f32(sp.seed_v, dv));
-    vy = (real)(ls * gauss_bm_f32(sp.seed_v, dv + 2));
-    vz = (real)(ls * gauss_bm_f32(sp.seed_v, dv + 4) + (float)sp.vdrift);
+    vx = (real)(ls * gauss_bm_f32_u(uv[0], uv[1]));
+    vy = (real)(ls * gauss_bm_f32_u(uv[2], uv[3]));
+    vz = (real)(ls * gauss_bm_f32_u(uv[4], uv[5]) + (float)sp.vdrift);
   }
   int ci, cj, ck;
   real fx, fy, fz;
