@@ -273,7 +273,9 @@ int pic_rng_counters(pic_ctx *ctx, long long *ctr_p, long long *ctr_v, int set);
  * [2] non-finite velocities after a push; work [3] particle pushes made by
  * the push kernels since creation; errors [4] sr_particle packets lost to a
  * full exchange list, [5] field tiles whose TMA-staged operands did not arrive
- * within the wait limit (the tile is left unchanged); [6..7] reserved.
+ * within the wait limit (the tile is left unchanged), [6] refilled particles
+ * lost to a full particle store (pic_step places a refill after the count it
+ * holds on the device, without waiting for it); [7] reserved.
  * Returns PIC_ERR_DEVICE when any error counter is non-zero. */
 int pic_status(pic_ctx *ctx, long long *counters8);
 /* *staged = 1 when renew_b4_2 / renew_e4_2 run the TMA-staged stencil kernels,

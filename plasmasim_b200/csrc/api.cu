@@ -1034,6 +1034,32 @@ int do_source(pic_ctx* c, int s, const Slab* slabs, int nslab, int init_form = 0
   return set_count(c, s, st.count + total);
 }
 
+__global__ void grow_count_kernel(int* count, long long add, int cap) {
+  const long long n = (long long)*count + add;
+  *count = (int)(n < cap ? n : (long long)cap);
+}
+
+// do_source for a species whose count is known only on the device: the
+// particles go after the device count, a slot past the capacity is not written
+// (counted as ERR_STORE_FULL, which pic_status reports), and the count grows on
+// the device; the host's copy stays pending.
+template <typename real>
+int do_source_dev(pic_ctx* c, int s, const Slab* slabs, int nslab) {
+  SourceParams sp = source_params(c, s, slabs, nslab, 0);
+  const long long total = sp.total;
+  if (total == 0) return PIC_OK;
+  Store& st = c->sp[s];
+  sp.dst_dev = st.count_dev;
+  sp.cap = (int)st.cap;
+  source_kernel<real><<<grid_blocks(total), kThreads, 0, c->stream>>>(parts<real>(c, s), sp, c->err);
+  CKL();
+  grow_count_kernel<<<1, 1, 0, c->stream>>>(st.count_dev, total, (int)st.cap);
+  CKL();
+  c->ctr_p += 3 * total;
+  c->ctr_v += 6 * total;
+  return PIC_OK;
+}
+
 
 // add_*_flat: the shell deletion, then the refill appended (the next step's
 // re-layout moves it into the layout). With `fused` (pic_step, whose re-layout
@@ -1047,20 +1073,27 @@ int do_add_flat(pic_ctx* c, bool fused = false) {
   for (int s = 0; s < 2; ++s) {
     Store& st = c->sp[s];
     const Parts<real> P = parts<real>(c, s);
-    CKR(check_spill<real>(c, s, true));
-    CKR(sync_count(c, s));
     const bool defer = fused && c->layout[s] && !c->cfg.slot_order;
+    // in pic_step, with the count still on the device, nothing here needs the
+    // host's copy, so the step does not wait for the device to drain (a
+    // pending spill read-back is acted on at the start of a later step)
+    const bool nowait = defer && st.pending;
+    if (!nowait) {
+      CKR(check_spill<real>(c, s, true));
+      CKR(sync_count(c, s));
+    }
     const long long first = defer ? c->tiled_end[s] : 0;
-    if (st.count > first) {
-      delete_shell_kernel<real><<<particle_blocks(st.count - first), kThreads, 0, c->stream>>>(P, (int)first,
-                                                                                              st.count_dev, c->g);
+    if (nowait || st.count > first) {
+      delete_shell_kernel<real><<<particle_blocks((nowait ? st.cap : st.count) - first), kThreads, 0, c->stream>>>(
+          P, (int)first, st.count_dev, c->g);
       CKL();
     }
     if (defer) {
       st.shell_pending = true;
       c->tiled[s] = false;  // the re-layout runs this step, refill or not
     }
-    CKR(do_source<real>(c, s, slabs, nslab));  // appended; the next step's re-layout places them
+    // appended; the re-layout that follows places them
+    CKR(nowait ? do_source_dev<real>(c, s, slabs, nslab) : do_source<real>(c, s, slabs, nslab));
   }
   return PIC_OK;
 }
