@@ -270,6 +270,7 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
   const int base = ta.goff[G], jmax = ta.gmax[G];
   // home cell of this lane
   const int hi = wx0 + 2 + warp / kTileY, hj = wy0 + 2 + warp % kTileY, hk = wz0 + 2 + lane;
+  const int hcell = pack_cell(hi, hj, hk);
   real* wn = win + 3 * WN;
   // FP32: the density window holds fixed-point sums (scatter8_win_fixed) at a
   // scale that no node of this tile can overflow
@@ -328,6 +329,7 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
     int i = 0, j = 0, k = 0;
     real fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
     bool enq = false;  // J at x^{n+1/2} goes to the warp's queue
+    int chalf = 0;     // the packed cell at x^{n+1/2}
     if (act) {
       ++pushed;
       unpack_cell(c, i, j, k);
@@ -354,13 +356,18 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
         } else {
           boris4_fast(pc, gather6(F, g, X, Y, Z), vx, vy, vz);
         }
-        if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) count_err(err, ERR_NONFINITE);
+        // one test for the three: |v| < c, so the sum of finite components is finite
+        if (!isfinite(vx + vy + vz)) count_err(err, ERR_NONFINITE);
       }
       advance(i, fx, vx * pc.hdt);
       advance(j, fy, vy * pc.hdt);
       advance(k, fz, vz * pc.hdt);
       // J at x^{n+1/2}
-      if (i == hi && j == hj && k == hk) {
+      // compared packed: a half step moves an index at most a cell past the
+      // padded array, where a -1 packs negative and a kMaxDim sets a bit that
+      // only an index 0 or 1 next to it could match, and home cells have indices >= 2
+      chalf = pack_cell(i, j, k);
+      if (chalf == hcell) {
         const Axis<real> X = axis_weights(i, fx), Y = axis_weights(j, fy), Z = axis_weights(k, fz);
         const W3<real> bx = home3(X, hi), by = home3(Y, hj), bz = home3(Z, hk);
         acc.add(pc.qn * vx, pc.qn * vy, pc.qn * vz, X, Y, Z, bx, by, bz);
@@ -384,7 +391,7 @@ push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<
       if (em) {
         if (enq) {
           float* e = jq + (nq + __popc(em & ((1u << lane) - 1u))) * 7;
-          e[0] = __int_as_float(pack_cell(i, j, k));
+          e[0] = __int_as_float(chalf);
           e[1] = (float)fx; e[2] = (float)fy; e[3] = (float)fz;
           e[4] = (float)vx; e[5] = (float)vy; e[6] = (float)vz;
         }
