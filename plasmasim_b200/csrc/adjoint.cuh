@@ -766,6 +766,52 @@ __global__ void cell_key_kernel(Parts<real> P, int n, Geom g, int dead, int* key
   slot[t] = t;
 }
 
+// The compaction's stable sort on those keys is a counting sort: count the
+// slots of every key (the dead key counted in bucket `nodes`, after every
+// node), scan the counts, scatter each slot to its key's run, then order each
+// run by slot. The scatter's order within a run depends on the atomics; the
+// last pass makes it the slot order, so a replayed segment gets the same
+// result, which is the stable sort's. The dead run keeps the scatter's order:
+// none of its slots is copied, and every one of them maps to -1.
+__device__ __forceinline__ int key_bucket(int k, int dead, int nodes) { return k == dead ? nodes : k; }
+
+__global__ void key_count_kernel(const int* __restrict__ key, int n, int dead, int nodes, int* cnt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = t < n;
+  warp_aggregated_inc(cnt, in ? key_bucket(key[t], dead, nodes) : 0, in);
+}
+
+// pos[b] holds the start of run b on entry and its end on return.
+__global__ void key_scatter_kernel(const int* __restrict__ key, int n, int dead, int nodes, int* pos, int* okey,
+                                   int* oslot) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = t < n;
+  const int k = in ? key[t] : 0;
+  const int p = warp_aggregated_inc(pos, in ? key_bucket(k, dead, nodes) : 0, in);
+  if (in) {
+    okey[p] = k;
+    oslot[p] = t;
+  }
+}
+
+// Each live entry's place in its run is the number of entries of the run with
+// a lower slot (slots are distinct); `end` is the scatter's pos.
+__global__ void key_rank_kernel(const int* __restrict__ skey, const int* __restrict__ sslot, int n, int dead,
+                                const int* __restrict__ cnt, const int* __restrict__ end, int* okey, int* oslot) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int k = skey[p], v = sslot[p];
+  int dst = p;
+  if (k != dead) {
+    const int e = end[k], s0 = e - cnt[k];
+    int r = 0;
+    for (int q = s0; q < e; ++q) r += sslot[q] < v;
+    dst = s0 + r;
+  }
+  okey[dst] = k;
+  oslot[dst] = v;
+}
+
 // Slot j of Q takes the particle of sorted position j; map[old slot] = j, or
 // -1 for an empty slot; *count = the live particles (the first dead key).
 template <typename real>

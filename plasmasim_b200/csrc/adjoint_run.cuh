@@ -1,6 +1,5 @@
 // Host side of the adjoint run (pic_adjoint / pic_objective), included by
-// api.cu after the step functions it reuses (api.cu includes CUB's radix sort
-// at file scope for adj_compact).
+// api.cu after the step functions it reuses.
 //
 // Forward: the loop body of fdtd (:687-949) in slot-stable form: the push is
 // the one-thread-per-particle fused kernel over the slots, sorting is left out
@@ -34,8 +33,8 @@ struct AdjRun {
   // sort's temporary storage
   int* skey[2] = {nullptr, nullptr};
   int* sslot[2] = {nullptr, nullptr};
-  void* sort_tmp = nullptr;
-  size_t sort_bytes = 0;
+  int* kcnt = nullptr;  // the compaction's counting sort: slots per key (nodes + 1 buckets)
+  int* kpos = nullptr;  // and each key's run: start after the scan, end after the scatter
   void* jn_final = nullptr;  // J_i, J_e, n_i, n_e after the forward sweep
   void* tdb = nullptr;       // three planes: one reverse step's particle terms of dJ/dDB
   // a refill's compaction count is read back without waiting: until
@@ -178,7 +177,7 @@ int key_bits(const pic_ctx* c) {
 }
 
 // Removes the empty slots of species s and orders the rest by cell (a stable
-// radix sort on the cell index, so a replayed segment gets the same order),
+// counting sort on the node index, so a replayed segment gets the same order),
 // recording the slot map in `map` when it is not null. Cell order keeps the
 // lanes of a warp on few stencil bases, which the aggregated scatters of the
 // adjoint kernels need; between refills the slots drift apart as particles
@@ -191,15 +190,22 @@ int adj_compact(pic_ctx* c, AdjRun& R, int s, int* map) {
   if (n == 0) return PIC_OK;
   const int bits = key_bits(c);
   const int dead = (1 << bits) - 1;
+  const int nodes = c->g.nodes;
   cell_key_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, c->g, dead, R.skey[0],
                                                                      R.sslot[0]);
   CKL();
-  size_t bytes = R.sort_bytes;
-  CK(cub::DeviceRadixSort::SortPairs(R.sort_tmp, bytes, R.skey[0], R.skey[1], R.sslot[0], R.sslot[1], (int)n, 0,
-                                     bits, c->stream));
-  ++c->launches;
-  cell_gather_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, dead, R.skey[1],
-                                                                        R.sslot[1], parts<real>(c, s, 1 - st.cur),
+  CK(cudaMemsetAsync(R.kcnt, 0, sizeof(int) * (size_t)(nodes + 1), c->stream));
+  key_count_kernel<<<grid_blocks(n), kThreads, 0, c->stream>>>(R.skey[0], (int)n, dead, nodes, R.kcnt);
+  CKL();
+  CKR(scan_exclusive(c, R.kcnt, R.kpos, nodes + 1, R.scan_tmp, R.scan_len));
+  key_scatter_kernel<<<grid_blocks(n), kThreads, 0, c->stream>>>(R.skey[0], (int)n, dead, nodes, R.kpos, R.skey[1],
+                                                                 R.sslot[1]);
+  CKL();
+  key_rank_kernel<<<grid_blocks(n), kThreads, 0, c->stream>>>(R.skey[1], R.sslot[1], (int)n, dead, R.kcnt, R.kpos,
+                                                              R.skey[0], R.sslot[0]);
+  CKL();
+  cell_gather_kernel<real><<<grid_blocks(n), kThreads, 0, c->stream>>>(parts<real>(c, s), (int)n, dead, R.skey[0],
+                                                                        R.sslot[0], parts<real>(c, s, 1 - st.cur),
                                                                         map, st.count_dev);
   CKL();
   CK(cudaMemcpyAsync(c->host_pin + 2 + s, st.count_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));

@@ -10,7 +10,6 @@
 #include <new>
 #include <vector>
 
-#include <cub/device/device_radix_sort.cuh>
 #include <cudaTypedefs.h>
 
 #include "../../include/plasma_b200.h"
@@ -1435,15 +1434,16 @@ int do_adjoint(pic_ctx* c, int nsteps, int every, bool grad, double* out) {
   AdjSnap fin;
   auto run = [&]() -> int {
     const long long capmax = c->sp[0].cap > c->sp[1].cap ? c->sp[0].cap : c->sp[1].cap;
-    R.scan_len = (size_t)(2 * ((capmax + kScanTile - 1) / kScanTile) + 64);
+    // the scan serves the compaction's counts over nodes + 1 keys
+    const long long scan_n = capmax > (long long)c->g.nodes + 1 ? capmax : (long long)c->g.nodes + 1;
+    R.scan_len = (size_t)(2 * ((scan_n + kScanTile - 1) / kScanTile) + 64);
     CKR(adj_alloc(c, R, (void**)&R.scan_tmp, sizeof(int) * R.scan_len));
     for (int b = 0; b < 2; ++b) {
       CKR(adj_alloc(c, R, (void**)&R.skey[b], sizeof(int) * (size_t)capmax));
       CKR(adj_alloc(c, R, (void**)&R.sslot[b], sizeof(int) * (size_t)capmax));
     }
-    CK(cub::DeviceRadixSort::SortPairs(nullptr, R.sort_bytes, R.skey[0], R.skey[1], R.sslot[0], R.sslot[1],
-                                       (int)capmax, 0, key_bits(c), c->stream));
-    CKR(adj_alloc(c, R, &R.sort_tmp, R.sort_bytes));
+    CKR(adj_alloc(c, R, (void**)&R.kcnt, sizeof(int) * ((size_t)c->g.nodes + 1)));
+    CKR(adj_alloc(c, R, (void**)&R.kpos, sizeof(int) * ((size_t)c->g.nodes + 1)));
     CKR(adj_alloc(c, R, (void**)&R.acc, sizeof(double) * 4));
     CKR(adj_alloc(c, R, (void**)&R.j64, sizeof(unsigned long long) * 3 * (size_t)c->g.nodes));
     CK(cudaMemsetAsync(R.acc, 0, sizeof(double) * 4, c->stream));
