@@ -243,8 +243,14 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // registers for 3 CTAs per SM, measured 1.7x slower). The density goes to the window with shared
 // reductions (every active lane at once): integer ones on fixed-point sums in
 // FP32, FP64 atomics in FP64.
+// FP64 at one CTA per SM: 254 registers and no spills, against 528 bytes of
+// spill stores per thread at two CTAs per SM (128 registers); measured 30.6 ->
+// 27.2 ms per step for the FP64 push at 128^3 cells x 64 particles/cell/species.
+#ifndef PB_PUSH64_MIN_BLOCKS
+#define PB_PUSH64_MIN_BLOCKS 1
+#endif
 template <typename real, bool VEC_FLUSH>
-__global__ void __launch_bounds__(kTileX * kTileY * 32, 2)
+__global__ void __launch_bounds__(kTileX * kTileY * 32, sizeof(real) == 4 ? 2 : PB_PUSH64_MIN_BLOCKS)
 push_tiled_kernel(Parts<real> P, TileArgs ta, Fields<real> F, Geom g, PushConst<real> pc, unsigned long long* err) {
   using S = PushSmem<real>;
   constexpr int WY = S::WY, WZ = S::WZ, WN = S::WN, WX = S::WX;
